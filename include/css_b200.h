@@ -1,0 +1,173 @@
+/*
+ * css_b200.h -- C ABI of the B200 (sm_100a) implementation of the CSS
+ * (Compressible Spherical Segment) time-step hot path: compact 6th-order
+ * derivatives, hydro/MHD right-hand side, slope-limited diffusion (SLD) and
+ * the RK4 update.
+ *
+ * Every entry point takes plain pointers and sizes and returns an int status
+ * (CSS_OK == 0).  The reference has no return codes (errors print and call
+ * Graceful_Exit, parallel_mpi.f90:886-889); here the caller decides.
+ *
+ * Array layout (host and device): the reference's Fortran order
+ *   vars(it, ip, ir, iv)  ->  vars[it + nth*(ip + nphi*(ir + nr*iv))]
+ * (theta fastest, then phi, then r, then the field index), as allocated in
+ * Initialize_Physics (rhs_mpi.f90:24).  Field order: 0 rho, 1 w (u_theta),
+ * 2 v (u_phi), 3 u (u_r), 4 s, and for MHD 5..7 = the vector potential
+ * A_theta, A_phi, A_r in the state (B_theta, B_phi, B_r while an RHS runs),
+ * as rhs_mpi.f90:819-1027 and checkpoint.f90:289-296 name them.
+ *
+ * The reference runs one MPI rank per block of an (nnr, nnt, nnp) Cartesian
+ * decomposition and its derivative closures depend on the block faces
+ * (derivatives.f90:564-721).  Here the whole domain lives on one GPU and the
+ * decomposition is virtual: every block of the line is solved independently
+ * with the same halo-closed rows, so results equal the reference run on
+ * nnr*nnt*nnp ranks.
+ *
+ * Threading: one host thread per context; every call is stream-ordered on
+ * the context's own CUDA stream and synchronous unless documented otherwise.
+ */
+#ifndef CSS_B200_H
+#define CSS_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define CSS_OK           0
+#define CSS_ERR_ARG      1   /* bad argument / unsupported flag combination  */
+#define CSS_ERR_DECOMP   2   /* decomposition the reference cannot run       */
+#define CSS_ERR_CUDA     3   /* CUDA runtime error (message: css_last_error) */
+#define CSS_ERR_NAN      4   /* non-finite value in the state after a step   */
+#define CSS_ERR_NOMEM    5   /* device allocation failed                     */
+#define CSS_ERR_NODEV    6   /* no CUDA device                               */
+
+/* ---- radial profile slots: profiles[slot*nr + ir] ----------------------- */
+/* The reference keeps these as module globals (constants.f90:19-25,
+ * derivatives.f90:32); Read_Stellar_Model fills them (mhdsph_mpi.f90:317-397). */
+enum {
+  CSS_PROF_X = 0,     /* x_ind: uniform computational coordinate            */
+  CSS_PROF_R,         /* r_ind: radius at each grid point                    */
+  CSS_PROF_DR,        /* dr_ind: r(ir) - r(ir-1), dr_ind(1) extrapolated     */
+  CSS_PROF_DXDR,      /* dx/dr                                               */
+  CSS_PROF_D2XDR2,    /* d2x/dr2                                             */
+  CSS_PROF_RHO,       /* background density rhor                             */
+  CSS_PROF_S,         /* background entropy sr                               */
+  CSS_PROF_G,         /* gravity                                             */
+  CSS_PROF_KS,        /* entropy conductivity ks                             */
+  CSS_PROF_DLNKS,     /* d ln ks / dr                                        */
+  CSS_PROF_EPS,       /* internal heating eps                                */
+  CSS_NPROF
+};
+
+/* ---- run parameters (mirror of the four reference namelists,
+ *      mhdsph_mpi.f90:1142-1177; defaults constants.f90:31-82) ----------- */
+typedef struct css_params {
+  int nr, nth, nphi;          /* global grid                                   */
+  int nnr, nnt, nnp;          /* virtual block decomposition (MPI dims)        */
+  int magnetic;               /* 1: nv = 8 (MHD), 0: nv = 5                    */
+  int non_uniform;            /* 1: r from r_ind/dxdr/d2xdr2 profiles          */
+  double r1, r2;              /* radial extent                                 */
+  double th1, th2;            /* colatitude extent, radians                    */
+  double phi1, phi2;          /* azimuthal extent (periodic), radians          */
+  double gamma, cp, omega_0;  /* ratio of heats, Cp, frame rotation rate      */
+  double t0;                  /* top temperature (thermal damping target)      */
+  double xi_cs;               /* sound-speed reduction factor (1 = none)       */
+  double damping_time;        /* top thermal damping time                      */
+  double lumr1, lumr2;        /* luminosity for constant-flux boundaries       */
+  int slaplacian;             /* entropy diffusion ks*laplacian(s)             */
+  int sldiffusion;            /* slope-limited diffusion once per step         */
+  int top_stress_free, bottom_stress_free;       /* else no-slip               */
+  int top_constant_temp, bottom_constant_temp;   /* else constant flux         */
+  int theta_stress_free;
+  int theta_normal_field, theta_perf_conductor;
+  int top_radial_field, bottom_radial_field;
+  int top_perfect_cond, bottom_perfect_cond;
+  int set_stop;
+  /* slope-limited diffusion (diffusion.f90:8-11) */
+  double sld_coef, sld_speedh, sld_speedr, sld_exp, sld_pr, sld_prm;
+  double sld_tanh_coef, flux_cutoff;
+  int dstype;                 /* 1: add |u|^2 (+vA^2) to the diffusion speed^2 */
+  int mass_diffusion, magnetic_diffusion;
+  int do_viscous_heating, do_ohmic_heating;
+  int flux_limiter, ent_flux_limiter, mag_flux_limiter;  /* <= 0: off         */
+  int precision;              /* 0: FP64 (drop-in), 1: FP32 perturbation form  */
+} css_params;
+
+typedef struct css_ctx css_ctx;
+
+/* Human-readable message for the last failing call on this thread. */
+const char *css_last_error(void);
+
+/* Builds a device-resident context: derivative LU tables for every virtual
+ * block (Initialize_Derivatives, derivatives.f90:39-520), the SLD speed
+ * profile (Initialize_Diffusion, diffusion.f90:19-63), the BC integers
+ * (Read_Input, mhdsph_mpi.f90:1302-1462) and the state buffers.
+ * Replaces Setup's Initialize_* chain (mhdsph_mpi.f90:92-123).            */
+int css_create(const css_params *p, const double *profiles, css_ctx **out);
+void css_destroy(css_ctx *ctx);
+
+/* Host <-> device state copies; vars holds nth*nphi*nr*nv doubles in the
+ * layout above (vars0 of parallel_mpi.f90:41).                            */
+int css_upload_state(css_ctx *ctx, const double *vars);
+int css_download_state(css_ctx *ctx, double *vars);
+
+/* nsteps RK4 steps of size dt on the device-resident state.  Replaces the
+ * loop body of Program CSS2 (mhdsph_mpi.f90:28-48) calling Step_RK4
+ * (step_rk4.f90:339-493).  Returns CSS_ERR_NAN if the state became
+ * non-finite (the reference's Debug NaN abort, rhs_mpi.f90:288-322).      */
+int css_step_rk4(css_ctx *ctx, double dt, int nsteps);
+
+/* Host-buffer convenience: upload vars0, nsteps steps, download into vars0. */
+int css_step_rk4_host(css_ctx *ctx, double *vars0, double dt, int nsteps);
+
+/* RHS(call_num) (rhs_mpi.f90:279-783) on host buffers.  vars1 is in/out as
+ * in the reference: for MHD, slots 5..7 come back holding B = curl A when
+ * call_num == 1 and A otherwise (rhs_mpi.f90:325, :750-752).              */
+int css_rhs(css_ctx *ctx, double *vars1, double *dvars1, int call_num);
+
+/* Compute_Diffusion(1) (diffusion.f90:70-474) on host buffers: dvars1 gets
+ * the SLD tendency.  As in the reference, vars1 comes back with the mean
+ * state subtracted from rho and s (diffusion.f90:168-175).  For MHD, vars1
+ * slots 5..7 must hold B and avec the vector potential A (the reference's
+ * maga); avec may be NULL for hydro.                                      */
+int css_diffusion(css_ctx *ctx, double *vars1, const double *avec, double *dvars1);
+
+/* Whole-field compact derivative along one direction, every virtual block
+ * solved with its own closures.  dir: 0 = r (Dbydr/D2bydr2,
+ * derivatives.f90:547, :799), 1 = theta (Dbydt/D2bydt2, :1010, :1265),
+ * 2 = phi (Dbydp/D2bydp2, :1480, :1594).  order 1 or 2.  bdry = the
+ * reference's ibc 0..4 (its `var <= 0` form, derivatives.f90:558-562).
+ * bc_lo / bc_hi: the 1-deep boundary datum at the physical low/high face
+ * (r: nth*nphi values [it + nth*ip]; theta: nphi*nr values [ip + nphi*ir];
+ * phi: unused, may be NULL).  Non-uniform r is returned in x-space, as the
+ * reference returns it before the caller's dxdr multiply.
+ * Host pointers.                                                          */
+int css_deriv(css_ctx *ctx, int dir, int order, const double *x, double *dx,
+              const double *bc_lo, const double *bc_hi, int bdry);
+
+/* Same on device pointers, enqueued on `stream` (a cudaStream_t, NULL =
+ * the context stream); returns after enqueueing.                           */
+int css_deriv_dev(css_ctx *ctx, int dir, int order, const double *x, double *dx,
+                  const double *bc_lo, const double *bc_hi, int bdry, void *stream);
+
+/* Batched 1D whole-line first derivative Dbyd1_dt0 (derivatives.f90:2296)
+ * on nlines contiguous lines of n1 points, host pointers; bdat1/bdat2 per
+ * line.  Equals CSS-Python derivatives.py:32 compact_fd6(dtype=0) / dri.  */
+int css_dbyd1_dt0(const double *x, double *dxdy, const double *bdat1,
+                  const double *bdat2, int n1, int ibc, int nlines);
+
+/* Block until all work on the context stream is done. */
+int css_sync(css_ctx *ctx);
+
+/* Device pointer of the current state (vars0) and its element count, for
+ * zero-copy use from PyTorch or a CUDA-aware caller.                       */
+int css_state_device_ptr(css_ctx *ctx, double **dptr, long long *nelem);
+
+/* Number of kernels this library launched on ctx since creation. */
+long long css_kernel_launches(css_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* CSS_B200_H */

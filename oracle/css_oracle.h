@@ -1,0 +1,59 @@
+/*
+ * css_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * CPU FP64 restatement of the CSS reference hot path (orvedahl/CSS-Code,
+ * Fortran 90 + MPI) used as the parity oracle for the B200 library.  Only
+ * tests/, __graft_entry__.smoke() and bench.py's CPU-baseline / reference
+ * arm may load it.  It is never linked into the product library.
+ *
+ * The Fortran cannot be compiled in this environment (no Fortran compiler,
+ * no MPI, no LAPACK, Intel-only IFPORT in checkpoint.f90:3), so this file
+ * restates, routine by routine, the algorithm of
+ *   derivatives.f90 (Initialize_Derivatives, Dbydr..D2bydp2, VectorCurlA,
+ *                    Compute_B, Dbyd1_dt0),
+ *   parallel_mpi.f90 (Partition, the halo semantics of the exchanges),
+ *   rhs_mpi.f90     (RHS, Source_Theta_Terms, Phi_Terms, Radial_Terms,
+ *                    Density_Terms_Theta/_Radial, Induction_Terms, Bound),
+ *   diffusion.f90   (Initialize_Diffusion, Compute_Diffusion, Diffusion_R,
+ *                    Diffusion_Th, Diffusion_Phi),
+ *   step_rk4.f90    (Step_RK4),
+ * emulating the MPI ranks serially (one virtual rank per block).
+ *
+ * Pinning: Dbyd1_dt0 / the whole-line closures are checked against golden
+ * vectors produced by the reference's own CSS-Python derivatives.py
+ * compact_fd6 (tests/golden/); block operators against the analytic
+ * known-answer fields of validation.f90:17-28 and 6th-order convergence.
+ */
+#ifndef CSS_ORACLE_H
+#define CSS_ORACLE_H
+#include "../include/css_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct orc_ctx orc_ctx;
+
+int orc_create(const css_params *p, const double *profiles, orc_ctx **out);
+void orc_destroy(orc_ctx *c);
+const char *orc_last_error(void);
+void orc_set_threads(int n);
+
+/* same semantics as the css_* entry points of include/css_b200.h */
+int orc_deriv(orc_ctx *c, int dir, int order, const double *x, double *dx,
+              const double *bc_lo, const double *bc_hi, int bdry);
+int orc_rhs(orc_ctx *c, double *vars1, double *dvars1, int call_num);
+int orc_diffusion(orc_ctx *c, double *vars1, const double *avec, double *dvars1);
+int orc_step_rk4(orc_ctx *c, double *vars0, double dt, int nsteps);
+int orc_dbyd1_dt0(const double *x, double *dxdy, const double *bdat1,
+                  const double *bdat2, int n1, int ibc, int nlines);
+int orc_compact_lines(const double *x, double *dx, int n, int nlines, int order, int lphys, int rphys,
+                      int bdry, const double *bc_lo, const double *bc_hi, const double *halo_lo,
+                      const double *halo_hi, double dnum, double scale);
+/* curl of A (VectorCurlA + Compute_B boundary zeroing): b = curl(a), 3 fields */
+int orc_curl_b(orc_ctx *c, const double *a, double *b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

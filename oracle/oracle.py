@@ -1,0 +1,151 @@
+"""ctypes binding of the CPU oracle (liboracle.so).  TEST INFRASTRUCTURE
+ONLY: imported by tests/, __graft_entry__.smoke() and bench.py's CPU
+baseline arm, never by the product package.
+
+The oracle is a C restatement of the reference Fortran hot path; see
+css_oracle.h for what each entry point restates.
+"""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        L.orc_create.argtypes = [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_void_p)]
+        L.orc_create.restype = ctypes.c_int
+        L.orc_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_last_error.restype = ctypes.c_char_p
+        L.orc_set_threads.argtypes = [ctypes.c_int]
+        L.orc_deriv.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_int]
+        L.orc_rhs.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_int]
+        L.orc_diffusion.argtypes = [ctypes.c_void_p, _dp, _dp, _dp]
+        L.orc_step_rk4.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, ctypes.c_int]
+        L.orc_dbyd1_dt0.argtypes = [_dp, _dp, _dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.orc_curl_b.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_compact_lines.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double,
+                                        ctypes.c_double]
+        _LIB = L
+    return _LIB
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def _check(rc):
+    if rc != 0:
+        raise RuntimeError("oracle error %d: %s" % (rc, lib().orc_last_error().decode()))
+
+
+def set_threads(n):
+    lib().orc_set_threads(int(n))
+
+
+def dbyd1_dt0(x, bdat1, bdat2, ibc):
+    """Batched Dbyd1_dt0 (derivatives.f90:2296) over the last axis."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n1 = x.shape[-1]
+    lines = x.reshape(-1, n1)
+    nl = lines.shape[0]
+    out = np.zeros_like(lines)
+    b1 = np.ascontiguousarray(np.broadcast_to(np.asarray(bdat1, dtype=np.float64), (nl,)))
+    b2 = np.ascontiguousarray(np.broadcast_to(np.asarray(bdat2, dtype=np.float64), (nl,)))
+    _check(lib().orc_dbyd1_dt0(_ptr(lines), _ptr(out), _ptr(b1), _ptr(b2), n1, int(ibc), nl))
+    return out.reshape(x.shape)
+
+
+class Oracle:
+    """One emulated (nnr x nnt x nnp)-rank run of the reference on the CPU."""
+
+    def __init__(self, params, profiles):
+        self.p = params.copy()
+        self.prof = np.ascontiguousarray(profiles, dtype=np.float64)
+        h = ctypes.c_void_p()
+        _check(lib().orc_create(ctypes.byref(self.p), _ptr(self.prof), ctypes.byref(h)))
+        self.h = h
+        self.nv = 8 if self.p.magnetic else 5
+        self.shape = (self.nv, self.p.nr, self.p.nphi, self.p.nth)
+
+    def close(self):
+        if self.h:
+            lib().orc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def deriv(self, direction, order, x, bc_lo=None, bc_hi=None, bdry=1):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.zeros_like(x)
+        lo = None if bc_lo is None else np.ascontiguousarray(bc_lo, dtype=np.float64)
+        hi = None if bc_hi is None else np.ascontiguousarray(bc_hi, dtype=np.float64)
+        _check(lib().orc_deriv(self.h, direction, order, _ptr(x), _ptr(out), _ptr(lo), _ptr(hi), int(bdry)))
+        return out
+
+    def rhs(self, vars1, call_num=1):
+        v = np.array(vars1, dtype=np.float64, order="C", copy=True)
+        dv = np.zeros_like(v)
+        _check(lib().orc_rhs(self.h, _ptr(v), _ptr(dv), int(call_num)))
+        return v, dv
+
+    def diffusion(self, vars1, avec=None):
+        v = np.array(vars1, dtype=np.float64, order="C", copy=True)
+        dv = np.zeros_like(v)
+        a = None if avec is None else np.ascontiguousarray(avec, dtype=np.float64)
+        _check(lib().orc_diffusion(self.h, _ptr(v), _ptr(a), _ptr(dv)))
+        return v, dv
+
+    def curl_b(self, a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        b = np.zeros_like(a)
+        _check(lib().orc_curl_b(self.h, _ptr(a), _ptr(b)))
+        return b
+
+    def step(self, vars0, dt, nsteps=1):
+        v = np.array(vars0, dtype=np.float64, order="C", copy=True)
+        _check(lib().orc_step_rk4(self.h, _ptr(v), float(dt), int(nsteps)))
+        return v
+
+
+def compact_lines(x, order=1, lphys=True, rphys=True, bdry=1, bc_lo=None, bc_hi=None,
+                  halo_lo=None, halo_hi=None, dnum=1.0, scale=1.0):
+    """Independent compact-FD lines with explicit closures (orc_compact_lines)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[-1]
+    lines = x.reshape(-1, n)
+    nl = lines.shape[0]
+    out = np.zeros_like(lines)
+
+    def vec(a, k):
+        if a is None:
+            return None
+        return np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (nl, k) if k > 1 else (nl,)))
+
+    _check(lib().orc_compact_lines(_ptr(lines), _ptr(out), n, nl, int(order), int(bool(lphys)), int(bool(rphys)),
+                                   int(bdry), _ptr(vec(bc_lo, 1)), _ptr(vec(bc_hi, 1)), _ptr(vec(halo_lo, 4)),
+                                   _ptr(vec(halo_hi, 4)), float(dnum), float(scale)))
+    return out.reshape(x.shape)
