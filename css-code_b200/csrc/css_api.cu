@@ -1,0 +1,740 @@
+// css_api.cu -- C ABI of the CSS B200 library (include/css_b200.h): context
+// set-up (virtual decomposition, LU tables, profiles), device buffers, the
+// RK4 step loop and the parity entry points.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/css_b200.h"
+#include "css_kernels.cuh"
+
+using namespace css;
+
+static thread_local char g_err[512];
+static void set_err(const char *fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+}
+extern "C" const char *css_last_error(void) { return g_err; }
+
+#define CUDA_TRY(x)                                                                  \
+  do {                                                                               \
+    cudaError_t e_ = (x);                                                            \
+    if (e_ != cudaSuccess) {                                                         \
+      set_err("%s:%d %s: %s", __FILE__, __LINE__, #x, cudaGetErrorString(e_));       \
+      return e_ == cudaErrorMemoryAllocation ? CSS_ERR_NOMEM : CSS_ERR_CUDA;         \
+    }                                                                                \
+  } while (0)
+
+struct css_ctx {
+  css_params p;
+  CssGeo g;
+  int nv;
+  size_t ncell;
+  cudaStream_t stream;
+  // device buffers
+  double *tab, *prof, *theta_prof;
+  int *rblk;
+  double *v0, *vA, *vB, *dv, *vs;  // state, stage ping-pong, tendency, RK accumulator
+  double *bf;                       // B = curl A (MHD)
+  double *vcc;                      // SLD speed^2
+  double *cda;                      // curl of the A-tendency (MHD ohmic heating)
+  int *flag;
+  long long launches;
+  int tl_theta, tl_phi, tl_r;
+};
+
+// ---------------------------------------------------------------------------
+// LU tables (Initialize_Derivatives, derivatives.f90:106-287 for r/theta,
+// :172-219 for phi), 1-based arrays g1|g2|g3 per bdry.
+// ---------------------------------------------------------------------------
+static void tab_d1(int m, int lphys, int rphys, int iv, double *g1, double *g2, double *g3) {
+  double alpha = 1.0 / 3.0, a2 = 0.75, g2c = 0.125, a1 = 6.0, b1 = 3.0;
+  double cn = 1.0 / (a2 - b1 * g2c);
+  double up1 = (a1 * a2 - b1) * cn, up2;
+  up2 = ((iv != 1) && (iv != 2)) ? 0.0 : up1;
+  if (iv % 2 == 0) up1 = 0.0;
+  double c1 = 1.0, c2 = 1.0, c3;
+  g1[1] = g2[1] = g3[1] = c2;
+  if (lphys) {
+    c3 = up1 * c2; g1[2] = c3; c2 = c1 / (c1 - g2c * c3); g2[2] = c2;
+    c3 = a2 * c2; g1[3] = c3; c2 = c1 / (c1 - alpha * c3); g2[3] = c2;
+    g3[2] = -g2c * g2[2];
+  } else {
+    c3 = alpha * c2; g1[2] = c3; c2 = c1 / (c1 - alpha * c3); g2[2] = c2;
+    g3[2] = -alpha * g2[2];
+    c3 = alpha * c2; g1[3] = c3; c2 = c1 / (c1 - alpha * c3); g2[3] = c2;
+  }
+  for (int i = 4; i <= m - 2; i++) { c3 = alpha * c2; g1[i] = c3; c2 = c1 / (c1 - alpha * c3); g2[i] = c2; }
+  for (int i = 3; i <= m - 2; i++) g3[i] = -alpha * g2[i];
+  if (rphys) {
+    c3 = alpha * c2; g1[m - 1] = c3; c2 = c1 / (c1 - a2 * c3); g2[m - 1] = c2;
+    c3 = g2c * c2; g1[m] = c3; c2 = c1 / (c1 - up2 * c3); g2[m] = c2;
+    g3[m - 1] = -a2 * g2[m - 1];
+    g3[m] = -up2 * g2[m];
+  } else {
+    c3 = alpha * c2; g1[m - 1] = c3; c2 = c1 / (c1 - alpha * c3); g2[m - 1] = c2;
+    c3 = alpha * c2; g1[m] = c3; c2 = c1 / (c1 - alpha * c3); g2[m] = c2;
+    g3[m - 1] = -alpha * g2[m - 1];
+    g3[m] = -alpha * g2[m];
+  }
+  for (int j = 1; j <= m; j++) g1[j] = -g1[j];
+}
+
+static void tab_d2(int m, int lphys, int rphys, int iv, double *g1, double *g2, double *g3) {
+  static const double U1[5] = {707.0 / 193.0, 137.0 / 13.0, 707.0 / 193.0, 137.0 / 13.0, 707.0 / 193.0};
+  static const double U2[5] = {707.0 / 193.0, 137.0 / 13.0, 137.0 / 13.0, 707.0 / 193.0, 707.0 / 193.0};
+  double alpha = 2.0 / 11.0, up1 = U1[iv], up2 = U2[iv];
+  double a2 = -0.35, g2c = 0.1;
+  double c1 = 1.0, c2 = 1.0, c3;
+  g1[1] = g2[1] = g3[1] = c2;
+  if (lphys) {
+    c3 = up1; g1[2] = c3; c2 = c1 / (c1 - g2c * c3); g2[2] = c2;
+    c3 = a2 * c2; g1[3] = c3; c2 = c1 / (c1 - alpha * c3); g2[3] = c2;
+    g3[2] = -g2c * g2[2];
+  } else {
+    c3 = alpha * c2; g1[2] = c3; c2 = c1 / (c1 - alpha * c3); g2[2] = c2;
+    g3[2] = -alpha * g2[2];
+    c3 = alpha * c2; g1[3] = c3; c2 = c1 / (c1 - alpha * c3); g2[3] = c2;
+  }
+  for (int i = 4; i <= m - 2; i++) { c3 = alpha * c2; g1[i] = c3; c2 = c1 / (c1 - alpha * c3); g2[i] = c2; }
+  for (int i = 3; i <= m - 2; i++) g3[i] = -alpha * g2[i];
+  g2c = a2;
+  a2 = 0.1;
+  if (rphys) {
+    c3 = alpha * c2; g1[m - 1] = c3; c2 = c1 / (c1 - g2c * c3); g2[m - 1] = c2;
+    c3 = a2 * c2; g1[m] = c3; c2 = c1 / (c1 - up2 * c3); g2[m] = c2;
+    g3[m - 1] = -g2c * g2[m - 1];
+    g3[m] = -up2 * g2[m];
+  } else {
+    c3 = alpha * c2; g1[m - 1] = c3; c2 = c1 / (c1 - alpha * c3); g2[m - 1] = c2;
+    c3 = alpha * c2; g1[m] = c3; c2 = c1 / (c1 - alpha * c3); g2[m] = c2;
+    g3[m - 1] = -alpha * g2[m - 1];
+    g3[m] = -alpha * g2[m];
+  }
+  for (int j = 1; j <= m; j++) g1[j] = -g1[j];
+}
+
+static void tab_p(int m, double alpha, double *g1, double *g2, double *g3) {
+  double c1 = 1.0, c2 = 1.0, c3;
+  g1[1] = g2[1] = g3[1] = c1;
+  c3 = alpha * c2; g1[2] = c3; c2 = c1 / (c1 - alpha * c3); g2[2] = c2;
+  g3[2] = -alpha * g2[2];
+  for (int i = 3; i <= m; i++) { c3 = alpha * c2; g1[i] = c3; c2 = c1 / (c1 - alpha * c3); g2[i] = c2; }
+  for (int i = 3; i <= m; i++) g3[i] = -alpha * g2[i];
+  for (int j = 1; j <= m; j++) g1[j] = -g1[j];
+}
+
+// Partition (parallel_mpi.f90:236-343): the remainder goes to the first blocks
+static int partition(int n, int nn, int *start, int *size) {
+  int base = n / nn;
+  if (base < 9) return -1;
+  int irem = n % nn;
+  int pos = 0;
+  for (int i = 0; i < nn; i++) {
+    int sz = (irem > 0 && (i == 0 || i + 1 <= irem)) ? base + 1 : base;
+    start[i] = pos;
+    size[i] = sz;
+    pos += sz;
+  }
+  return 0;
+}
+
+static size_t smem_theta(int nh, int nd, int m, int TL) { return 8 * ((size_t)nh * TL * (m + 9) + (size_t)nd * TL * (m + 1)); }
+static size_t smem_line(int nh, int nd, int na, int m, int TL) {
+  return 8 * ((size_t)nh * (m + 8) * (TL + 1) + (size_t)(nd + na) * m * (TL + 1));
+}
+static const size_t kSmemCap = 100 * 1024;
+
+static int pick_tl(int kind, int nh, int nd, int na, int m) {
+  for (int tl = 16; tl >= 1; tl /= 2) {
+    size_t s = kind == 0 ? smem_theta(nh, nd, m, tl) : smem_line(nh, nd, na, m, tl);
+    if (s <= kSmemCap) return tl;
+  }
+  return 1;
+}
+
+extern "C" void css_destroy(css_ctx *c) {
+  if (!c) return;
+  cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk);
+  cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
+  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+static int setup_kernels() {
+  static bool done = false;
+  if (done) return CSS_OK;
+  int mx = 200 * 1024;
+  CUDA_TRY(cudaFuncSetAttribute(k_theta_terms, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_phi_terms, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_radial_terms, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_rhot_update, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_theta, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_phi, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_r, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  done = true;
+  return CSS_OK;
+}
+
+extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **out) {
+  if (!out) { set_err("css_create: NULL out"); return CSS_ERR_ARG; }
+  *out = nullptr;
+  if (!pp || !prof) { set_err("css_create: NULL argument"); return CSS_ERR_ARG; }
+  const css_params &p = *pp;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    set_err("css_create: no CUDA device");
+    return CSS_ERR_NODEV;
+  }
+  if (p.nnr < 2 || p.nnt < 2 || p.nnp < 3) {
+    set_err("css_create: the reference needs nnr>=2, nnt>=2 (no dtype 0 case, derivatives.f90:564) and nnp>=3 "
+            "(phi halos from distinct neighbours, parallel_mpi.f90:646-665)");
+    return CSS_ERR_DECOMP;
+  }
+  if (p.nnr > CSS_MAXBLK || p.nnt > CSS_MAXBLK || p.nnp > CSS_MAXBLK) {
+    set_err("css_create: at most %d blocks per direction", CSS_MAXBLK);
+    return CSS_ERR_DECOMP;
+  }
+  if (p.flux_limiter > 0 || p.ent_flux_limiter > 0 || p.mag_flux_limiter > 0 || p.bottom_constant_temp ||
+      (p.top_constant_temp && p.set_stop) || p.dstype != 1 || p.xi_cs > 1.0) {
+    set_err("css_create: unsupported option (SLD power flux limiter, bottom constant temperature, Set_Stop, "
+            "dstype != 1 or xi_cs > 1)");
+    return CSS_ERR_ARG;
+  }
+  if (p.magnetic && p.do_ohmic_heating && !p.magnetic_diffusion) {
+    set_err("css_create: ohmic heating needs magnetic diffusion");
+    return CSS_ERR_ARG;
+  }
+  if (p.precision != 0) {
+    set_err("css_create: precision %d not available in this build", p.precision);
+    return CSS_ERR_ARG;
+  }
+  css_ctx *c = new css_ctx();
+  memset(c, 0, sizeof(*c));
+  c->p = p;
+  c->nv = p.magnetic ? 8 : 5;
+  c->ncell = (size_t)p.nr * p.nth * p.nphi;
+  CssGeo &g = c->g;
+  memset(&g, 0, sizeof g);
+  g.nr = p.nr; g.nth = p.nth; g.nphi = p.nphi; g.nv = c->nv;
+  g.magnetic = p.magnetic; g.non_uniform = p.non_uniform;
+  g.ncell = (long long)c->ncell;
+  int ns[3] = {p.nr, p.nth, p.nphi}, nn[3] = {p.nnr, p.nnt, p.nnp};
+  for (int d = 0; d < 3; d++) {
+    CssDir &D = g.d[d];
+    D.nb = nn[d];
+    if (partition(ns[d], nn[d], D.start, D.size)) {
+      set_err("css_create: fewer than 9 points per block (parallel_mpi.f90:250-315)");
+      css_destroy(c);
+      return CSS_ERR_DECOMP;
+    }
+    D.maxm = 0;
+    for (int b = 0; b < nn[d]; b++) {
+      if (D.size[b] % 2 || D.size[b] < 10 || D.size[b] > CSS_MAXM) {
+        set_err("css_create: block sizes must be even and in [10, %d] (the reference's paired sweeps read an "
+                "unset row for odd sizes, derivatives.f90:755-792)", CSS_MAXM);
+        css_destroy(c);
+        return CSS_ERR_DECOMP;
+      }
+      D.maxm = D.size[b] > D.maxm ? D.size[b] : D.maxm;
+      D.lphys[b] = (d < 2) && b == 0;
+      D.rphys[b] = (d < 2) && b == nn[d] - 1;
+    }
+  }
+  // host copies of the profiles
+  const int nr = p.nr, nth = p.nth, nphi = p.nphi;
+  std::vector<double> P(prof, prof + (size_t)CSS_NPROF * nr);
+  const double *x_ind = &P[CSS_PROF_X * nr], *r_ind = &P[CSS_PROF_R * nr];
+  std::vector<double> dxdr(P.begin() + CSS_PROF_DXDR * nr, P.begin() + (CSS_PROF_DXDR + 1) * nr);
+  std::vector<double> d2xdr2(P.begin() + CSS_PROF_D2XDR2 * nr, P.begin() + (CSS_PROF_D2XDR2 + 1) * nr);
+  if (!p.non_uniform) for (int i = 0; i < nr; i++) { dxdr[i] = 1.0; d2xdr2[i] = 1.0; }
+  double dth = (p.th2 - p.th1) / (double)(nth - 1), dphi = (p.phi2 - p.phi1) / (double)nphi;
+  std::vector<double> theta(nth), phi(nphi), sines(nth), cosines(nth);
+  for (int i = 0; i < nth; i++) { theta[i] = dth * (double)i + p.th1; sines[i] = sin(theta[i]); cosines[i] = cos(theta[i]); }
+  for (int i = 0; i < nphi; i++) phi[i] = dphi * (double)i + p.phi1;
+  // block spacings (derivatives.f90:91-97)
+  const std::vector<double> *coords[3] = {nullptr, &theta, &phi};
+  for (int d = 0; d < 3; d++) {
+    CssDir &D = g.d[d];
+    for (int b = 0; b < D.nb; b++) {
+      int a0 = D.start[b], a1 = D.start[b] + D.size[b] - 1;
+      double v = d == 0 ? 1.0 / (x_ind[a1] - x_ind[a0]) : 1.0 / ((*coords[d])[a1] - (*coords[d])[a0]);
+      D.dnum[b] = (double)(D.size[b] - 1) * v;
+    }
+  }
+  // tables
+  int maxm = std::max(g.d[0].maxm, std::max(g.d[1].maxm, g.d[2].maxm));
+  g.tstride = maxm + 2;
+  const int ts = g.tstride;
+  std::vector<double> T;
+  for (int d = 0; d < 3; d++) {
+    CssDir &D = g.d[d];
+    for (int b = 0; b < D.nb; b++) {
+      int m = D.size[b];
+      for (int order = 1; order <= 2; order++) {
+        int nbd = (d == 2) ? 1 : 5;
+        int off = (int)T.size();
+        T.resize(T.size() + (size_t)nbd * 3 * ts, 0.0);
+        for (int iv = 0; iv < nbd; iv++) {
+          double *g1 = &T[off + (size_t)iv * 3 * ts], *g2 = g1 + ts, *g3 = g2 + ts;
+          if (d == 2) tab_p(m, order == 1 ? 1.0 / 3.0 : 2.0 / 11.0, g1, g2, g3);
+          else if (order == 1) tab_d1(m, D.lphys[b], D.rphys[b], iv, g1, g2, g3);
+          else tab_d2(m, D.lphys[b], D.rphys[b], iv, g1, g2, g3);
+        }
+        (order == 1 ? D.tab1 : D.tab2)[b] = off;
+      }
+    }
+  }
+  std::vector<int> rblk(nr);
+  for (int b = 0; b < g.d[0].nb; b++)
+    for (int i = g.d[0].start[b]; i < g.d[0].start[b] + g.d[0].size[b]; i++) rblk[i] = b;
+  // physics constants (rhs_mpi.f90:63-75)
+  g.gamma = p.gamma; g.gamm1 = p.gamma - 1.0; g.cp = p.cp; g.cv = p.cp / p.gamma;
+  g.invcv = 1.0 / g.cv;
+  double invcp = 1.0 / p.cp;
+  g.pconst = g.gamm1 * p.cp;
+  g.invpconst = invcp / g.gamm1;
+  g.invtconst = g.invcv / g.gamm1;
+  g.omega0 = p.omega_0; g.t0 = p.t0; g.damping_time = p.damping_time; g.lumr1 = p.lumr1; g.lumr2 = p.lumr2;
+  g.r1 = p.r1; g.r2 = p.r2; g.dth = dth; g.dphi = dphi; g.xi_cs = p.xi_cs;
+  g.slaplacian = p.slaplacian; g.sldiffusion = p.sldiffusion; g.set_stop = p.set_stop;
+  g.top_stress_free = p.top_stress_free; g.bottom_stress_free = p.bottom_stress_free;
+  g.top_constant_temp = p.top_constant_temp; g.bottom_constant_temp = p.bottom_constant_temp;
+  g.theta_stress_free = p.theta_stress_free; g.theta_normal_field = p.theta_normal_field;
+  g.theta_perf_conductor = p.theta_perf_conductor;
+  g.top_radial_field = p.top_radial_field; g.bottom_radial_field = p.bottom_radial_field;
+  g.top_perfect_cond = p.top_perfect_cond; g.bottom_perfect_cond = p.bottom_perfect_cond;
+  // BC integers (Read_Input, mhdsph_mpi.f90:1317-1461)
+  {
+    int tn = !p.top_stress_free, bn = !p.bottom_stress_free;
+    int lbcr_v = (tn && bn) ? 1 : (tn && !bn) ? 2 : (!tn && bn) ? 3 : 4;
+    int tt = p.top_constant_temp, bt = p.bottom_constant_temp;
+    int lbcr_s = (tt && bt) ? 1 : (tt && !bt) ? 2 : (!tt && bt) ? 3 : 4;
+    int lbcr_u = 1, lbcr_rho = 4, lbcr_t = 4;
+    int lbct_rho = 4, lbct_t = 0, lbct_w = 1, lbct_u = p.theta_stress_free ? 0 : 1, lbct_v = 4, lbct_s = 0;
+    int lbcr_br = 0, lbcr_bt = 0, lbcr_bp = 0, lbcr_ar = 0, lbcr_at = 0, lbcr_ap = 0;
+    int lbct_br = 0, lbct_bt = 0, lbct_bp = 0, lbct_ar = 0, lbct_at = 0, lbct_ap = 0;
+    if (p.magnetic) {
+      if (p.top_radial_field && p.bottom_radial_field) {
+        lbcr_br = 4; lbcr_bt = 1; lbcr_bp = 1; lbcr_ar = 1; lbcr_at = 0; lbcr_ap = 0;
+      }
+      if (p.top_perfect_cond && p.bottom_perfect_cond) {
+        lbcr_br = lbcr_bt = lbcr_bp = lbcr_ar = lbcr_at = lbcr_ap = 1;
+      }
+      if (p.theta_normal_field) { lbct_br = 1; lbct_bt = 4; lbct_bp = 1; lbct_ar = 0; lbct_at = 1; lbct_ap = 0; }
+      if (p.theta_perf_conductor) { lbct_br = lbct_bt = lbct_bp = lbct_ar = lbct_at = lbct_ap = 1; }
+    }
+    int ir_[13] = {0, lbcr_rho, lbcr_v, lbcr_v, lbcr_u, lbcr_s, lbcr_t, lbcr_bt, lbcr_bp, lbcr_br, lbcr_at, lbcr_ap, lbcr_ar};
+    int it_[13] = {0, lbct_rho, lbct_w, lbct_v, lbct_u, lbct_s, lbct_t, lbct_bt, lbct_bp, lbct_br, lbct_at, lbct_ap, lbct_ar};
+    memcpy(g.ibcr, ir_, sizeof ir_);
+    memcpy(g.ibct, it_, sizeof it_);
+    g.lbcr_rho = lbcr_rho;
+  }
+  const double one_over_4pi = 1.0 / 3.1415926535897932384626433832795028841972 / 4.0;
+  const double *ks = &P[CSS_PROF_KS * nr];
+  g.s_flux_lo = g.s_flux_hi = 0.0;
+  if (!p.bottom_constant_temp)
+    g.s_flux_lo = p.slaplacian ? -p.lumr1 * one_over_4pi / (p.r1 * p.r1 * ks[0] * dxdr[0]) : 0.0 / dxdr[0];
+  if (!p.top_constant_temp)
+    g.s_flux_hi = p.slaplacian ? -p.lumr2 * one_over_4pi / (p.r2 * p.r2 * ks[nr - 1] * dxdr[nr - 1]) : 0.0 / dxdr[nr - 1];
+  // SLD (diffusion.f90:76-114, :51-61)
+  g.sld_coef = p.sld_coef; g.sld_pr = p.sld_pr; g.sld_prm = p.sld_prm;
+  const double *rhor = &P[CSS_PROF_RHO * nr];
+  double tv[8] = {1e-8 * rhor[nr - 1], 1e-8, 1e-8, 1e-8, 1e-8 * 1e5, 1e-8 * 1e8, 1e-8 * 1e8, 1e-8 * 1e8};
+  memcpy(g.tinyvar, tv, sizeof tv);
+  g.nsld = 0;
+  if (p.mass_diffusion) g.varlist[g.nsld++] = 0;
+  for (int i = 1; i <= 4; i++) g.varlist[g.nsld++] = i;
+  if (p.magnetic && p.magnetic_diffusion) for (int i = 5; i <= 7; i++) g.varlist[g.nsld++] = i;
+  g.dstype = p.dstype; g.mass_diffusion = p.mass_diffusion;
+  g.do_viscous_heating = p.do_viscous_heating; g.do_ohmic_heating = p.magnetic && p.do_ohmic_heating;
+  std::vector<double> dspeed(nr);
+  for (int i = 0; i < nr; i++) {
+    double ds = p.sld_speedh * pow(rhor[i] / rhor[nr - 1], p.sld_exp) + p.sld_speedr;
+    ds = 0.5 * ds * (1.0 + tanh(p.sld_tanh_coef * (r_ind[i] - p.flux_cutoff) / (p.r2 - p.r1)));
+    dspeed[i] = ds * ds;
+  }
+  // device copies
+  int rc = setup_kernels();
+  if (rc) { css_destroy(c); return rc; }
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    set_err("css_create: stream creation failed");
+    css_destroy(c);
+    return CSS_ERR_CUDA;
+  }
+  // radial profile block: r_ind r_inv dr_ind dxdr d2xdr2 rhor sr grav ks dlnks eps dspeed
+  std::vector<double> R((size_t)12 * nr);
+  for (int i = 0; i < nr; i++) {
+    R[0 * nr + i] = r_ind[i];
+    R[1 * nr + i] = 1.0 / r_ind[i];
+    R[2 * nr + i] = P[CSS_PROF_DR * nr + i];
+    R[3 * nr + i] = dxdr[i];
+    R[4 * nr + i] = d2xdr2[i];
+    R[5 * nr + i] = rhor[i];
+    R[6 * nr + i] = P[CSS_PROF_S * nr + i];
+    R[7 * nr + i] = P[CSS_PROF_G * nr + i];
+    R[8 * nr + i] = ks[i];
+    R[9 * nr + i] = P[CSS_PROF_DLNKS * nr + i];
+    R[10 * nr + i] = P[CSS_PROF_EPS * nr + i];
+    R[11 * nr + i] = dspeed[i];
+  }
+  std::vector<double> TH((size_t)3 * nth);
+  for (int i = 0; i < nth; i++) { TH[i] = sines[i]; TH[nth + i] = cosines[i]; TH[2 * nth + i] = theta[i]; }
+#define ALLOC(ptr, bytes)                                                                \
+  do {                                                                                   \
+    if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) {                                     \
+      set_err("css_create: device allocation of %zu bytes failed", (size_t)(bytes));     \
+      css_destroy(c);                                                                    \
+      return CSS_ERR_NOMEM;                                                              \
+    }                                                                                    \
+  } while (0)
+  ALLOC(c->tab, T.size() * 8);
+  ALLOC(c->prof, R.size() * 8);
+  ALLOC(c->theta_prof, TH.size() * 8);
+  ALLOC(c->rblk, nr * sizeof(int));
+  size_t sb = c->ncell * c->nv * sizeof(double);
+  ALLOC(c->v0, sb); ALLOC(c->vA, sb); ALLOC(c->vB, sb); ALLOC(c->dv, sb); ALLOC(c->vs, sb);
+  ALLOC(c->vcc, c->ncell * sizeof(double));
+  if (p.magnetic) { ALLOC(c->bf, 3 * c->ncell * sizeof(double)); ALLOC(c->cda, 3 * c->ncell * sizeof(double)); }
+  ALLOC(c->flag, sizeof(int));
+  cudaMemcpy(c->tab, T.data(), T.size() * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->prof, R.data(), R.size() * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->theta_prof, TH.data(), TH.size() * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->rblk, rblk.data(), nr * sizeof(int), cudaMemcpyHostToDevice);
+  cudaMemset(c->flag, 0, sizeof(int));
+  cudaMemset(c->vs, 0, sb);
+  g.tab = c->tab; g.rblk = c->rblk;
+  g.r_ind = c->prof; g.r_inv = c->prof + nr; g.dr_ind = c->prof + 2 * nr; g.dxdr = c->prof + 3 * nr;
+  g.d2xdr2 = c->prof + 4 * nr; g.rhor = c->prof + 5 * nr; g.sr = c->prof + 6 * nr; g.grav = c->prof + 7 * nr;
+  g.ks = c->prof + 8 * nr; g.dlnks = c->prof + 9 * nr; g.eps = c->prof + 10 * nr; g.dspeed = c->prof + 11 * nr;
+  g.sines = c->theta_prof; g.cosines = c->theta_prof + nth; g.theta = c->theta_prof + 2 * nth;
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    set_err("css_create: %s", cudaGetErrorString(e));
+    css_destroy(c);
+    return CSS_ERR_CUDA;
+  }
+  int mag = p.magnetic;
+  c->tl_theta = pick_tl(0, mag ? 6 : 4, mag ? 7 : 5, 0, g.d[1].maxm);
+  c->tl_phi = pick_tl(1, mag ? 7 : 5, mag ? 8 : 6, 0, g.d[2].maxm);
+  c->tl_r = pick_tl(1, mag ? 7 : 5, mag ? 7 : 5, 5, g.d[0].maxm);
+  *out = c;
+  return CSS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// launch helpers
+// ---------------------------------------------------------------------------
+static int check_launch(css_ctx *c) {
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_err("kernel launch: %s", cudaGetErrorString(e));
+    return CSS_ERR_CUDA;
+  }
+  c->launches++;
+  return CSS_OK;
+}
+
+static int launch_curl(css_ctx *c, const double *a, double *out, int apply_bc) {
+  const CssGeo &g = c->g;
+  int mt = g.d[1].maxm, mp = g.d[2].maxm, mr = g.d[0].maxm;
+  int TL = c->tl_theta;
+  dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
+  k_curl_theta<<<gt, 128, smem_theta(2, 2, mt, TL), c->stream>>>(g, a, out, TL);
+  if (int rc = check_launch(c)) return rc;
+  TL = c->tl_phi;
+  dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
+  k_curl_phi<<<gp, 128, smem_line(2, 2, 0, mp, TL), c->stream>>>(g, a, out, TL);
+  if (int rc = check_launch(c)) return rc;
+  TL = c->tl_r;
+  dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
+  k_curl_r<<<gr, 128, smem_line(2, 2, 0, mr, TL), c->stream>>>(g, a, out, TL, apply_bc);
+  return check_launch(c);
+}
+
+// RHS of one stage on `cur`; if stage > 0 also the stage update into `nx`
+static int launch_rhs(css_ctx *c, const double *cur, double *nx, int stage, double dtcur) {
+  const CssGeo &g = c->g;
+  const int mag = g.magnetic;
+  if (mag) {
+    if (int rc = launch_curl(c, cur + 5 * c->ncell, c->bf, 1)) return rc;
+  }
+  int TL = c->tl_theta;
+  dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
+  k_theta_terms<<<gt, 128, smem_theta(mag ? 6 : 4, mag ? 7 : 5, g.d[1].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  if (int rc = check_launch(c)) return rc;
+  TL = c->tl_phi;
+  dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
+  k_phi_terms<<<gp, 128, smem_line(mag ? 7 : 5, mag ? 8 : 6, 0, g.d[2].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  if (int rc = check_launch(c)) return rc;
+  TL = c->tl_r;
+  dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
+  k_radial_terms<<<gr, 128, smem_line(mag ? 7 : 5, mag ? 7 : 5, 5, g.d[0].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  if (int rc = check_launch(c)) return rc;
+  TL = c->tl_theta;
+  dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
+  k_rhot_update<<<gu, 128, smem_theta(1, 1, g.d[1].maxm, TL), c->stream>>>(g, cur, c->dv, c->v0, c->vs, nx, stage,
+                                                                            dtcur, TL, c->flag);
+  return check_launch(c);
+}
+
+// slope-limited diffusion tendency of `v` (A in av for MHD; B must be in
+// c->bf) into dout
+static int launch_sld(css_ctx *c, const double *v, const double *av, double *dout) {
+  const CssGeo &g = c->g;
+  int nb = 148 * 16;
+  k_sld_vcc<<<nb, 256, 0, c->stream>>>(g, v, c->bf, c->vcc);
+  if (int rc = check_launch(c)) return rc;
+  k_sld<<<nb, 128, 0, c->stream>>>(g, v, av, c->vcc, dout);
+  if (int rc = check_launch(c)) return rc;
+  if (g.do_ohmic_heating) {
+    if (int rc = launch_curl(c, dout + 5 * c->ncell, c->cda, 0)) return rc;
+    k_sld_ohmic<<<nb, 256, 0, c->stream>>>(g, v, c->bf, c->cda, dout);
+    if (int rc = check_launch(c)) return rc;
+  }
+  return CSS_OK;
+}
+
+static int step_once(css_ctx *c, double dt) {
+  const size_t N = c->ncell * c->nv;
+  (void)N;
+  if (c->p.sldiffusion) {
+    if (c->g.magnetic) {
+      if (int rc = launch_curl(c, c->v0 + 5 * c->ncell, c->bf, 1)) return rc;
+    }
+    if (int rc = launch_sld(c, c->v0, c->v0 + 5 * c->ncell, c->vs)) return rc;
+  }
+  if (int rc = launch_rhs(c, c->v0, c->vA, 1, dt / 2.0)) return rc;
+  if (int rc = launch_rhs(c, c->vA, c->vB, 2, dt / 2.0)) return rc;
+  if (int rc = launch_rhs(c, c->vB, c->vA, 3, dt)) return rc;
+  if (int rc = launch_rhs(c, c->vA, c->v0, 4, dt)) return rc;
+  return CSS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" int css_upload_state(css_ctx *c, const double *vars) {
+  if (!c || !vars) { set_err("css_upload_state: NULL"); return CSS_ERR_ARG; }
+  CUDA_TRY(cudaMemcpyAsync(c->v0, vars, c->ncell * c->nv * 8, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+extern "C" int css_download_state(css_ctx *c, double *vars) {
+  if (!c || !vars) { set_err("css_download_state: NULL"); return CSS_ERR_ARG; }
+  CUDA_TRY(cudaMemcpyAsync(vars, c->v0, c->ncell * c->nv * 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+extern "C" int css_step_rk4(css_ctx *c, double dt, int nsteps) {
+  if (!c || nsteps < 0 || !(dt > 0.0)) { set_err("css_step_rk4: bad argument"); return CSS_ERR_ARG; }
+  CUDA_TRY(cudaMemsetAsync(c->flag, 0, sizeof(int), c->stream));
+  for (int s = 0; s < nsteps; s++)
+    if (int rc = step_once(c, dt)) return rc;
+  int h = 0;
+  CUDA_TRY(cudaMemcpyAsync(&h, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (h) { set_err("css_step_rk4: non-finite value in the state"); return CSS_ERR_NAN; }
+  return CSS_OK;
+}
+
+extern "C" int css_step_rk4_host(css_ctx *c, double *vars0, double dt, int nsteps) {
+  if (int rc = css_upload_state(c, vars0)) return rc;
+  int rc = css_step_rk4(c, dt, nsteps);
+  if (rc && rc != CSS_ERR_NAN) return rc;
+  if (int r2 = css_download_state(c, vars0)) return r2;
+  return rc;
+}
+
+extern "C" int css_rhs(css_ctx *c, double *vars1, double *dvars1, int call_num) {
+  if (!c || !vars1 || !dvars1) { set_err("css_rhs: NULL"); return CSS_ERR_ARG; }
+  size_t sb = c->ncell * c->nv * 8;
+  CUDA_TRY(cudaMemcpyAsync(c->vA, vars1, sb, cudaMemcpyHostToDevice, c->stream));
+  if (int rc = launch_rhs(c, c->vA, nullptr, 0, 0.0)) return rc;
+  CUDA_TRY(cudaMemcpyAsync(dvars1, c->dv, sb, cudaMemcpyDeviceToHost, c->stream));
+  if (c->g.magnetic && call_num == 1)
+    CUDA_TRY(cudaMemcpyAsync(vars1 + 5 * c->ncell, c->bf, 3 * c->ncell * 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+extern "C" int css_diffusion(css_ctx *c, double *vars1, const double *avec, double *dvars1) {
+  if (!c || !vars1 || !dvars1 || (c->g.magnetic && !avec)) { set_err("css_diffusion: NULL"); return CSS_ERR_ARG; }
+  size_t n = c->ncell, sb = n * c->nv * 8;
+  CUDA_TRY(cudaMemcpyAsync(c->vA, vars1, sb, cudaMemcpyHostToDevice, c->stream));
+  if (c->g.magnetic) {
+    CUDA_TRY(cudaMemcpyAsync(c->bf, vars1 + 5 * n, 3 * n * 8, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->vB, avec, 3 * n * 8, cudaMemcpyHostToDevice, c->stream));
+  }
+  if (int rc = launch_sld(c, c->vA, c->vB, c->dv)) return rc;
+  CUDA_TRY(cudaMemcpyAsync(dvars1, c->dv, sb, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  // the reference leaves rho and s with the mean state subtracted
+  std::vector<double> rhor(c->p.nr), sr(c->p.nr);
+  CUDA_TRY(cudaMemcpy(rhor.data(), c->g.rhor, c->p.nr * 8, cudaMemcpyDeviceToHost));
+  CUDA_TRY(cudaMemcpy(sr.data(), c->g.sr, c->p.nr * 8, cudaMemcpyDeviceToHost));
+  size_t plane = (size_t)c->p.nth * c->p.nphi;
+  for (int ir = 0; ir < c->p.nr; ir++)
+    for (size_t q = 0; q < plane; q++) {
+      vars1[ir * plane + q] = vars1[ir * plane + q] - rhor[ir];
+      vars1[4 * n + ir * plane + q] = vars1[4 * n + ir * plane + q] - sr[ir];
+    }
+  return CSS_OK;
+}
+
+extern "C" int css_deriv_dev(css_ctx *c, int dir, int order, const double *x, double *dx, const double *bc_lo,
+                             const double *bc_hi, int bdry, void *stream) {
+  if (!c || !x || !dx || dir < 0 || dir > 2 || order < 1 || order > 2 || bdry < 0 || bdry > 4) {
+    set_err("css_deriv: bad argument");
+    return CSS_ERR_ARG;
+  }
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const CssGeo &g = c->g;
+  if (dir == 1) {
+    int TL = c->tl_theta;
+    dim3 gr(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
+    size_t sm = smem_theta(1, 1, g.d[1].maxm, TL);
+    if (order == 1) k_deriv_theta<1><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
+    else k_deriv_theta<2><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
+  } else if (dir == 2) {
+    int TL = c->tl_phi;
+    dim3 gr(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
+    size_t sm = smem_line(1, 1, 0, g.d[2].maxm, TL);
+    if (order == 1) k_deriv_phi<1><<<gr, 128, sm, st>>>(g, x, dx, TL);
+    else k_deriv_phi<2><<<gr, 128, sm, st>>>(g, x, dx, TL);
+  } else {
+    int TL = c->tl_r;
+    dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
+    size_t sm = smem_line(1, 1, 0, g.d[0].maxm, TL);
+    if (order == 1) k_deriv_r<1><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
+    else k_deriv_r<2><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
+  }
+  return check_launch(c);
+}
+
+extern "C" int css_deriv(css_ctx *c, int dir, int order, const double *x, double *dx, const double *bc_lo,
+                         const double *bc_hi, int bdry) {
+  if (!c || !x || !dx) { set_err("css_deriv: NULL"); return CSS_ERR_ARG; }
+  size_t n = c->ncell;
+  size_t face = dir == 0 ? (size_t)c->p.nth * c->p.nphi : (size_t)c->p.nphi * c->p.nr;
+  double *bl = c->vB, *bh = c->vB + face;  // scratch
+  CUDA_TRY(cudaMemcpyAsync(c->vA, x, n * 8, cudaMemcpyHostToDevice, c->stream));
+  if (bc_lo) CUDA_TRY(cudaMemcpyAsync(bl, bc_lo, face * 8, cudaMemcpyHostToDevice, c->stream));
+  if (bc_hi) CUDA_TRY(cudaMemcpyAsync(bh, bc_hi, face * 8, cudaMemcpyHostToDevice, c->stream));
+  if (int rc = css_deriv_dev(c, dir, order, c->vA, c->dv, bc_lo ? bl : nullptr, bc_hi ? bh : nullptr, bdry, nullptr))
+    return rc;
+  CUDA_TRY(cudaMemcpyAsync(dx, c->dv, n * 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+// Lines with explicit closures; used by css_dbyd1_dt0 and css_compact_lines.
+static int run_lines(const double *x, double *dx, int n, int nlines, int order, int lphys, int rphys, int bdry,
+                     const double *bclo, const double *bchi, const double *hlo, const double *hhi, double dnum,
+                     double scale, int dt0_quirk) {
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) { set_err("no CUDA device"); return CSS_ERR_NODEV; }
+  int ts = n + 2;
+  std::vector<double> T((size_t)5 * 3 * ts, 0.0);
+  for (int iv = 0; iv < 5; iv++) {
+    double *g1 = &T[(size_t)iv * 3 * ts], *g2 = g1 + ts, *g3 = g2 + ts;
+    if (order == 1) tab_d1(n, lphys, rphys, iv, g1, g2, g3);
+    else tab_d2(n, lphys, rphys, iv, g1, g2, g3);
+  }
+  if (dt0_quirk && order == 1 && bdry == 2) {
+    // Dbyd1_dt0 zeroes up1 before copying it into up2 (derivatives.f90:
+    // 2355-2386), so for ibc = 2 its last row has no lower coefficient:
+    // pivot 1/(1 - 0*c3) = 1 and no elimination term
+    double *g2 = &T[(size_t)2 * 3 * ts] + ts, *g3 = g2 + ts;
+    g2[n] = 1.0;
+    g3[n] = 0.0;
+  }
+  int dtype = lphys ? (rphys ? 0 : 2) : (rphys ? 1 : 3);
+  double *dT = nullptr, *dx_ = nullptr, *dy = nullptr, *work = nullptr, *dbl = nullptr, *dbh = nullptr, *dhl = nullptr,
+         *dhh = nullptr;
+  size_t nb = (size_t)n * nlines * 8;
+  int rc = CSS_OK;
+  auto fail = [&](const char *what, cudaError_t e) {
+    set_err("%s: %s", what, cudaGetErrorString(e));
+    rc = CSS_ERR_CUDA;
+  };
+  cudaError_t e;
+  if ((e = cudaMalloc(&dT, T.size() * 8)) || (e = cudaMalloc(&dx_, nb)) || (e = cudaMalloc(&dy, nb)) ||
+      (e = cudaMalloc(&work, (size_t)(n + 8) * nlines * 8)) || (e = cudaMalloc(&dbl, nlines * 8)) ||
+      (e = cudaMalloc(&dbh, nlines * 8)) || (e = cudaMalloc(&dhl, (size_t)4 * nlines * 8)) ||
+      (e = cudaMalloc(&dhh, (size_t)4 * nlines * 8))) {
+    fail("lines alloc", e);
+  } else {
+    cudaMemcpy(dT, T.data(), T.size() * 8, cudaMemcpyHostToDevice);
+    cudaMemcpy(dx_, x, nb, cudaMemcpyHostToDevice);
+    if (bclo) cudaMemcpy(dbl, bclo, nlines * 8, cudaMemcpyHostToDevice);
+    if (bchi) cudaMemcpy(dbh, bchi, nlines * 8, cudaMemcpyHostToDevice);
+    if (hlo) cudaMemcpy(dhl, hlo, (size_t)4 * nlines * 8, cudaMemcpyHostToDevice);
+    if (hhi) cudaMemcpy(dhh, hhi, (size_t)4 * nlines * 8, cudaMemcpyHostToDevice);
+    k_lines<<<(nlines + 127) / 128, 128>>>(dx_, dy, n, nlines, order, dtype, bdry, bclo ? dbl : nullptr,
+                                           bchi ? dbh : nullptr, hlo ? dhl : nullptr, hhi ? dhh : nullptr, dT, ts, dnum,
+                                           scale, work);
+    if ((e = cudaGetLastError()) != cudaSuccess) fail("k_lines", e);
+    else if ((e = cudaMemcpy(dx, dy, nb, cudaMemcpyDeviceToHost)) != cudaSuccess) fail("lines copy", e);
+  }
+  cudaFree(dT); cudaFree(dx_); cudaFree(dy); cudaFree(work); cudaFree(dbl); cudaFree(dbh); cudaFree(dhl); cudaFree(dhh);
+  return rc;
+}
+
+extern "C" int css_dbyd1_dt0(const double *x, double *dxdy, const double *bdat1, const double *bdat2, int n1, int ibc,
+                             int nlines) {
+  if (!x || !dxdy || n1 < 14 || n1 > 100000 || ibc < 0 || ibc > 4 || nlines < 0) {
+    set_err("css_dbyd1_dt0: need n1 >= 14 and ibc in 0..4");
+    return CSS_ERR_ARG;
+  }
+  if (nlines == 0) return CSS_OK;
+  // Dbyd1_dt0 takes the Neumann datum already divided by the spacing and
+  // returns d/dx in grid units (the caller multiplies by 1/dx)
+  return run_lines(x, dxdy, n1, nlines, 1, 1, 1, ibc, bdat1, bdat2, nullptr, nullptr, 1.0, 1.0, 1);
+}
+
+extern "C" int css_compact_lines(const double *x, double *dx, int n, int nlines, int order, int lphys, int rphys,
+                                 int bdry, const double *bc_lo, const double *bc_hi, const double *halo_lo,
+                                 const double *halo_hi, double dnum, double scale) {
+  if (!x || !dx || n < 10 || n > 100000 || order < 1 || order > 2 || bdry < 0 || bdry > 4 || nlines < 0 ||
+      (!lphys && !halo_lo) || (!rphys && !halo_hi)) {
+    set_err("css_compact_lines: bad argument");
+    return CSS_ERR_ARG;
+  }
+  if (nlines == 0) return CSS_OK;
+  return run_lines(x, dx, n, nlines, order, lphys, rphys, bdry, bc_lo, bc_hi, halo_lo, halo_hi, dnum, scale, 0);
+}
+
+extern "C" int css_sync(css_ctx *c) {
+  if (!c) return CSS_ERR_ARG;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+extern "C" int css_state_device_ptr(css_ctx *c, double **dptr, long long *nelem) {
+  if (!c || !dptr || !nelem) return CSS_ERR_ARG;
+  *dptr = c->v0;
+  *nelem = (long long)(c->ncell * c->nv);
+  return CSS_OK;
+}
+
+extern "C" long long css_kernel_launches(css_ctx *c) { return c ? c->launches : 0; }

@@ -1,0 +1,53 @@
+// css_geo.cuh -- device-side description of one CSS run: grid, virtual block
+// decomposition, LU tables, radial profiles and physics constants.  Passed
+// to every kernel by value (it lands in the kernel parameter bank, so all
+// threads read it as uniform constants).
+#pragma once
+#include <cstddef>
+
+#define CSS_MAXBLK 64   // virtual blocks per direction
+#define CSS_MAXM 256    // points per block (the reference's LOOP COUNT MAX is 252)
+
+// One direction's blocks (Partition, parallel_mpi.f90:236-343).
+struct CssDir {
+  int nb;
+  int start[CSS_MAXBLK];
+  int size[CSS_MAXBLK];
+  unsigned char lphys[CSS_MAXBLK], rphys[CSS_MAXBLK];
+  double dnum[CSS_MAXBLK];   // dri / dti / dpi of the block (derivatives.f90:91-97)
+  int tab1[CSS_MAXBLK];      // offset of the first-derivative tables
+  int tab2[CSS_MAXBLK];      // offset of the second-derivative tables
+  int maxm;
+};
+
+struct CssGeo {
+  int nr, nth, nphi, nv, magnetic, non_uniform;
+  long long ncell;
+  CssDir d[3];              // 0 = r, 1 = theta, 2 = phi
+  int tstride;              // length of one 1-based table array (maxm + 2)
+  const double *tab;        // [.. bdry][g1|g2|g3][tstride]
+  const int *rblk;          // radial block index of each global ir
+  // radial profiles (length nr)
+  const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
+  // theta profiles (length nth)
+  const double *sines, *cosines, *theta;
+  // constants (Initialize_Physics, rhs_mpi.f90:63-75)
+  double gamma, gamm1, cp, cv, invcv, invtconst, pconst, invpconst;
+  double omega0, t0, damping_time, lumr1, lumr2, r1, r2, dth, dphi, xi_cs;
+  int slaplacian, sldiffusion, set_stop;
+  int top_stress_free, bottom_stress_free, top_constant_temp, bottom_constant_temp;
+  int theta_stress_free, theta_normal_field, theta_perf_conductor;
+  int top_radial_field, bottom_radial_field, top_perfect_cond, bottom_perfect_cond;
+  int ibcr[13], ibct[13];   // 1-based, as derivatives.f90:50-57
+  int lbcr_rho;
+  double s_flux_lo, s_flux_hi;  // entropy-gradient datum at constant-flux faces
+  // slope-limited diffusion
+  double sld_coef, sld_pr, sld_prm;
+  double tinyvar[8];
+  int nsld, varlist[8];
+  int dstype, mass_diffusion, do_viscous_heating, do_ohmic_heating;
+};
+
+__host__ __device__ inline size_t css_idx(const CssGeo &g, int it, int ip, int ir) {
+  return (size_t)it + (size_t)g.nth * ((size_t)ip + (size_t)g.nphi * (size_t)ir);
+}

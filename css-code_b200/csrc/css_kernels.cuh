@@ -1,0 +1,1100 @@
+// css_kernels.cuh -- the CSS right-hand side, slope-limited diffusion and RK4
+// stage kernels for sm_100a, FP64.
+//
+// Each RHS term group of the reference is one kernel over shared-memory
+// tiles: a tile is one virtual block segment along the sweep direction
+// (+4 halo points each side, exactly the reference's halo depth) times TL
+// lines.  The line solves run one thread per (field, line); the pointwise
+// physics then runs one thread per point with coalesced (theta-contiguous)
+// global reads/writes of the state and the tendency.
+//
+//   theta_terms   Source_Theta_Terms (+ its Lorentz part) + Induction_Terms
+//   phi_terms     Phi_Terms (+ Lorentz)
+//   radial_terms  Radial_Terms (+ Lorentz) fused with Density_Terms_Radial
+//   rhot_update   Density_Terms_Theta fused with the RK4 stage combination
+//                 of Step_RK4 and Bound
+//   curl_*        VectorCurlA (+ Compute_B's boundary zeroing)
+//   sld_*         Compute_Diffusion / Diffusion_R / _Th / _Phi
+#pragma once
+#include "css_geo.cuh"
+#include "css_lines.cuh"
+
+namespace css {
+
+#define ONE_OVER_4PI (1.0 / 3.14159265358979323846264338327950288 / 4.0)
+
+__device__ __forceinline__ const double *tabp(const CssGeo &g, int dir, int blk, int order, int bdry) {
+  int off = (order == 1 ? g.d[dir].tab1[blk] : g.d[dir].tab2[blk]);
+  return g.tab + off + (size_t)bdry * 3 * g.tstride;
+}
+
+__device__ __forceinline__ int dtype_of(const CssDir &d, int b) {
+  int lp = d.lphys[b], rp = d.rphys[b];
+  return lp ? (rp ? 0 : 2) : (rp ? 1 : 3);
+}
+
+// temperature (rhs_mpi.f90:376-385)
+__device__ __forceinline__ double temp_of(const CssGeo &g, double rho, double s) {
+  double a = pow(rho, g.gamm1);
+  double t = g.invtconst * a;
+  double e = exp(s * g.invcv);
+  return t * e;
+}
+
+__device__ __forceinline__ double dnum_d2_theta(const CssGeo &g, int ir) {
+  // D2bydt2 divides the theta Neumann datum by the rank's dri
+  // (derivatives.f90:1322, :1338)
+  return g.d[0].dnum[__ldg(g.rblk + ir)];
+}
+
+// ---------------------------------------------------------------------------
+// tile loaders
+// ---------------------------------------------------------------------------
+// theta tile: S[l*SR + j+4], j in [-4, m+4), lines = phi indices pb..pb+TL-1
+__device__ __forceinline__ void load_theta_tile(const CssGeo &g, const double *__restrict__ f, double *S, int SR,
+                                                int t0, int m, int pb, int TL, int ir, bool halo) {
+  int w = m + 8;
+  for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
+    int l = idx / w, jj = idx - l * w;
+    int gt = t0 + jj - 4, gp = pb + l;
+    if ((!halo && (jj < 4 || jj >= m + 4)) || gt < 0 || gt >= g.nth || gp >= g.nphi) continue;
+    S[l * SR + jj] = __ldg(f + css_idx(g, gt, gp, ir));
+  }
+}
+
+// phi tile: S[(j+4)*SR + l], lines = theta indices tb..tb+TL-1, periodic in phi
+__device__ __forceinline__ void load_phi_tile(const CssGeo &g, const double *__restrict__ f, double *S, int SR,
+                                              int p0, int m, int tb, int TL, int ir, bool halo) {
+  int w = m + 8;
+  for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
+    int jj = idx / TL, l = idx - jj * TL;
+    if (!halo && (jj < 4 || jj >= m + 4)) continue;
+    int gp = p0 + jj - 4;
+    gp = (gp + g.nphi) % g.nphi;
+    int gt = tb + l;
+    if (gt >= g.nth) continue;
+    S[jj * SR + l] = __ldg(f + css_idx(g, gt, gp, ir));
+  }
+}
+
+// r tile: S[(j+4)*SR + l], lines = theta indices tb..tb+TL-1 at fixed phi
+__device__ __forceinline__ void load_r_tile(const CssGeo &g, const double *__restrict__ f, double *S, int SR, int r0,
+                                            int m, int tb, int TL, int ip, bool halo) {
+  int w = m + 8;
+  for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
+    int jj = idx / TL, l = idx - jj * TL;
+    int gr = r0 + jj - 4, gt = tb + l;
+    if ((!halo && (jj < 4 || jj >= m + 4)) || gr < 0 || gr >= g.nr || gt >= g.nth) continue;
+    S[jj * SR + l] = __ldg(f + css_idx(g, gt, ip, gr));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Source_Theta_Terms (rhs_mpi.f90:786-1029) + Induction_Terms (:2340-2346)
+// grid: x = theta block * nchunk + phi chunk, y = r.  cur = stage input
+// (vars1), B = curl A (MHD) in bf, dv = dvars1 (written, not read).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__restrict__ cur,
+                                                     const double *__restrict__ bf, double *__restrict__ dv, int TL) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nphi + TL - 1) / TL;
+  const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
+  const int ir = blockIdx.y;
+  const CssDir &D = g.d[1];
+  const int t0 = D.start[bt], m = D.size[bt];
+  const int dtype = dtype_of(D, bt);
+  const int mag = g.magnetic;
+  const int SR = m + 9, SO = m + 1;
+  const size_t n = (size_t)g.ncell;
+  const int nh = mag ? 6 : 4;   // w v u s [bp br]
+  double *H = sm;                       // nh * TL * SR
+  double *O = H + (size_t)nh * TL * SR;  // nd * TL * SO
+  const double *fld[6] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, bf + n, bf + 2 * n};
+  for (int k = 0; k < nh; k++) load_theta_tile(g, fld[k], H + (size_t)k * TL * SR, SR, t0, m, pb, TL, ir, true);
+  __syncthreads();
+  // solves: 0 dw, 1 dv, 2 du, 3 ds, 4 d2s, 5 dbp, 6 dbr
+  const int nd = mag ? 7 : 5;
+  const double ri = g.r_inv[ir];
+  for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
+    int k = task / TL, l = task - k * TL;
+    if (pb + l >= g.nphi) continue;
+    if (k == 4 && !g.slaplacian) continue;
+    int hk = (k <= 3) ? k : (k == 4 ? 3 : k - 1);
+    const double *x = H + ((size_t)hk * TL + l) * SR + 4;
+    double *o = O + ((size_t)k * TL + l) * SO;
+    int var = (k == 0) ? 2 : (k == 1) ? 3 : (k == 2) ? 4 : (k <= 4) ? 5 : (k == 5) ? 8 : 9;
+    int bdry = g.ibct[var];
+    double lo = 0.0, hi = 0.0;
+    if (k == 1) {  // stress-free datum cot(theta)*v on the walls (rhs_mpi.f90:414, :444)
+      if (D.lphys[bt]) lo = (g.cosines[0] / g.sines[0]) * x[0];
+      if (D.rphys[bt]) hi = (g.cosines[g.nth - 1] / g.sines[g.nth - 1]) * x[m - 1];
+    }
+    if (k == 5 && g.theta_normal_field) {  // (rhs_mpi.f90:421, :451)
+      if (D.lphys[bt]) lo = -(g.cosines[0] / g.sines[0]) * x[0];
+      if (D.rphys[bt]) hi = -(g.cosines[g.nth - 1] / g.sines[g.nth - 1]) * x[m - 1];
+    }
+    if (k == 4)
+      line_solve<2>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 2, bdry), g.tstride, dnum_d2_theta(g, ir),
+                    D.dnum[bt] * D.dnum[bt], 0, o, 1);
+    else
+      line_solve<1>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, D.dnum[bt], D.dnum[bt], 0, o, 1);
+  }
+  __syncthreads();
+  const double rv = g.r_ind[ir], epsr = g.eps[ir];
+  const double omsq = rv * g.omega0 * g.omega0, om2 = 2.0 * g.omega0;
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int l = pt / m, j = pt - l * m;
+    int it = t0 + j, ip = pb + l;
+    if (ip >= g.nphi) continue;
+    size_t id = css_idx(g, it, ip, ir);
+    double sn = g.sines[it], cs = g.cosines[it], ct = cs / sn;
+    double rho = __ldg(cur + id);
+    const double *hl = H + (size_t)l * SR + 4 + j;
+    double w = hl[0], v = hl[(size_t)TL * SR], u = hl[(size_t)2 * TL * SR], s = hl[(size_t)3 * TL * SR];
+    const double *ol = O + (size_t)l * SO + j;
+    double dw = omsq * sn * cs;
+    double du = -g.grav[ir] + omsq * sn * sn;
+    double drho = -rho * w * ct * ri;
+    double dvv = -om2 * cs * w;
+    du = du + ri * w * w;
+    double w1 = ol[0] * ri;
+    drho = drho - rho * w1;
+    dw = dw - w * w1;
+    dw = dw + v * (ri * ct * v + om2 * cs);
+    dvv = dvv - ri * v * w * ct;
+    du = du + v * (ri * v + om2 * sn);
+    w1 = ol[(size_t)1 * TL * SO] * ri;
+    dvv = dvv - w * w1;
+    dv[id] = drho - 2.0 * ri * rho * u;
+    dvv = dvv - u * (ri * v + om2 * sn);
+    dw = dw - ri * u * w;
+    w1 = ol[(size_t)2 * TL * SO] * ri;
+    du = du - w * w1;
+    double t = temp_of(g, rho, s);
+    double invrho = 1.0 / rho;
+    double ds;
+    if (fabs(epsr) > 0.0) ds = epsr * invrho / t;
+    else ds = 0.0;
+    w1 = ol[(size_t)3 * TL * SO] * ri;
+    double dwfin = dw - g.gamm1 * t * w1;
+    ds = ds - w * w1;
+    if (g.slaplacian) {
+      double ddiff = ri * g.ks[ir];
+      double oorho = invrho / t;
+      w1 = ddiff * w1 * oorho;
+      ds = ds + ct * w1;
+      double dd2 = ddiff * ri * ri;  // ks/r^3 as rhs_mpi.f90:972 has it
+      ds = ds + dd2 * ol[(size_t)4 * TL * SO] * oorho;
+    }
+    dv[4 * n + id] = ds;
+    if (!mag) {
+      dv[n + id] = dwfin;
+      dv[2 * n + id] = dvv;
+      dv[3 * n + id] = du;
+    } else {
+      dw = dwfin;
+      double oo = invrho;
+      oo = oo * ONE_OVER_4PI * ri;
+      double bt_ = __ldg(bf + id), bp_ = hl[(size_t)4 * TL * SR], br_ = hl[(size_t)5 * TL * SR];
+      du = du - bt_ * bt_ * oo;
+      dw = dw - bp_ * bp_ * ct * oo;
+      dvv = dvv + bp_ * bt_ * ct * oo;
+      du = du - bp_ * bp_ * oo;
+      w1 = ol[(size_t)5 * TL * SO] * oo;
+      dvv = dvv + bt_ * w1;
+      dw = dw - bp_ * w1;
+      w1 = ol[(size_t)6 * TL * SO] * oo;
+      dv[n + id] = dw + br_ * (bt_ * oo - w1);
+      dv[2 * n + id] = dvv + br_ * bp_ * oo;
+      dv[3 * n + id] = du + bt_ * w1;
+      // Induction_Terms: dA/dt = v x B
+      dv[5 * n + id] = v * br_ - u * bp_;
+      dv[6 * n + id] = u * bt_ - w * br_;
+      dv[7 * n + id] = w * bp_ - v * bt_;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Phi_Terms (rhs_mpi.f90:1032-1261).  grid: x = phi block * nchunk + theta
+// chunk, y = r.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__restrict__ cur,
+                                                   const double *__restrict__ bf, double *__restrict__ dv, int TL) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nth + TL - 1) / TL;
+  const int bp = blockIdx.x / nchunk, tb = (blockIdx.x - bp * nchunk) * TL;
+  const int ir = blockIdx.y;
+  const CssDir &D = g.d[2];
+  const int p0 = D.start[bp], m = D.size[bp];
+  const int mag = g.magnetic;
+  const int SR = TL + 1;
+  const size_t n = (size_t)g.ncell;
+  const int nh = mag ? 7 : 5;  // rho v w u s [bt br]
+  double *H = sm;
+  double *O = H + (size_t)nh * (m + 8) * SR;
+  const double *fld[7] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n, bf, bf + 2 * n};
+  for (int k = 0; k < nh; k++) load_phi_tile(g, fld[k], H + (size_t)k * (m + 8) * SR, SR, p0, m, tb, TL, ir, true);
+  __syncthreads();
+  // solves: 0 drho 1 dv 2 dw 3 du 4 ds 5 d2s 6 dbt 7 dbr
+  const int nd = mag ? 8 : 6;
+  for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
+    int k = task / TL, l = task - k * TL;
+    if (tb + l >= g.nth) continue;
+    if (k == 5 && !g.slaplacian) continue;
+    int hk = (k <= 4) ? k : (k == 5 ? 4 : k - 1);
+    const double *x = H + (size_t)hk * (m + 8) * SR + 4 * SR + l;
+    double *o = O + (size_t)k * m * SR + l;
+    if (k == 5)
+      line_solve<2>(x, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 2, 0), g.tstride, D.dnum[bp], D.dnum[bp] * D.dnum[bp], 1,
+                    o, SR);
+    else
+      line_solve<1>(x, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, D.dnum[bp], D.dnum[bp], 1, o, SR);
+  }
+  __syncthreads();
+  const double ri = g.r_inv[ir];
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int j = pt / TL, l = pt - j * TL;
+    int it = tb + l, ip = p0 + j;
+    if (it >= g.nth) continue;
+    size_t id = css_idx(g, it, ip, ir);
+    const double *hl = H + (size_t)(j + 4) * SR + l;
+    const size_t HS = (size_t)(m + 8) * SR;
+    double rho = hl[0], v = hl[HS], s = hl[4 * HS];
+    const double *ol = O + (size_t)j * SR + l;
+    const size_t OS = (size_t)m * SR;
+    double cscth = 1.0 / g.sines[it];
+    double oors = ri * cscth;
+    double t = temp_of(g, rho, s), oorho = 1.0 / rho;
+    double w1 = ol[0] * oors;
+    double drho = dv[id];
+    double dvv = dv[2 * n + id];
+    drho = drho - v * w1;
+    dvv = dvv - g.pconst * w1 * t * oorho;
+    double ds = dv[4 * n + id];
+    w1 = ol[OS] * oors;
+    dvv = dvv - v * w1;
+    dv[id] = drho - rho * w1;
+    double dw = dv[n + id];
+    w1 = ol[2 * OS] * oors;
+    dw = dw - v * w1;
+    double du = dv[3 * n + id];
+    w1 = ol[3 * OS] * oors;
+    du = du - v * w1;
+    w1 = ol[4 * OS] * oors;
+    ds = ds - v * w1;
+    dvv = dvv - g.gamm1 * t * w1;
+    if (g.slaplacian) {
+      w1 = ol[5 * OS] * (oors * oors);
+      ds = ds + g.ks[ir] * w1 * (oorho / t);
+    }
+    dv[4 * n + id] = ds;
+    if (!mag) {
+      dv[n + id] = dw;
+      dv[3 * n + id] = du;
+      dv[2 * n + id] = dvv;
+    } else {
+      double oo = ONE_OVER_4PI * oorho * oors;
+      double bt_ = hl[5 * HS], br_ = hl[6 * HS], bp_ = __ldg(bf + n + id);
+      w1 = ol[6 * OS] * oo;
+      dvv = dvv - bt_ * w1;
+      dv[n + id] = dw + bp_ * w1;
+      w1 = ol[7 * OS] * oo;
+      dv[2 * n + id] = dvv - br_ * w1;
+      dv[3 * n + id] = du + bp_ * w1;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Radial_Terms (rhs_mpi.f90:1264-1519) + Density_Terms_Radial (:1710-1855)
+// grid: x = r block * nchunk + theta chunk, y = phi.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__restrict__ cur,
+                                                      const double *__restrict__ bf, double *__restrict__ dv, int TL) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nth + TL - 1) / TL;
+  const int br = blockIdx.x / nchunk, tb = (blockIdx.x - br * nchunk) * TL;
+  const int ip = blockIdx.y;
+  const CssDir &D = g.d[0];
+  const int r0 = D.start[br], m = D.size[br];
+  const int dtype = dtype_of(D, br);
+  const int mag = g.magnetic, nu = g.non_uniform;
+  const int SR = TL + 1;
+  const size_t n = (size_t)g.ncell;
+  const int nh = mag ? 7 : 5;  // w v u s rho [bt bp]
+  const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
+  double *H = sm;
+  double *O = H + nh * HS;            // nd derivative buffers
+  const int nd = mag ? 7 : 5;         // dw dv du ds d2s [dbt dbp]; slot 0 reused for drho
+  double *A = O + nd * OS;            // 5 accumulators (dvars 0..4)
+  const double *fld[7] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, cur, bf, bf + n};
+  for (int k = 0; k < nh; k++) load_r_tile(g, fld[k], H + k * HS, SR, r0, m, tb, TL, ip, true);
+  __syncthreads();
+  const int nr = g.nr;
+  for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
+    int k = task / TL, l = task - k * TL;
+    if (tb + l >= g.nth) continue;
+    if (k == 4 && !g.slaplacian) continue;
+    int hk = (k <= 3) ? k : (k == 4 ? 3 : k);  // d2s uses s; dbt -> 5, dbp -> 6
+    const double *x = H + hk * HS + 4 * SR + l;
+    double *o = O + k * OS + l;
+    int var = (k == 0) ? 2 : (k == 1) ? 3 : (k == 2) ? 4 : (k <= 4) ? 5 : (k == 5) ? 7 : 8;
+    int bdry = g.ibcr[var];
+    double lo = 0.0, hi = 0.0;
+    if (k == 0 || k == 1) {  // stress-free datum w/r/dxdr (rhs_mpi.f90:578-614)
+      if (D.lphys[br] && g.bottom_stress_free) lo = x[0] / g.r1 / g.dxdr[0];
+      if (D.rphys[br]) {
+        if (g.top_stress_free) hi = x[(m - 1) * SR] / g.r2 / g.dxdr[nr - 1];
+        else hi = x[(m - 1) * SR];
+      }
+    }
+    if (k == 3 || k == 4) {  // constant-flux datum (rhs_mpi.f90:584-592, :616-624)
+      lo = g.s_flux_lo;
+      hi = g.s_flux_hi;
+    }
+    if (k == 4)
+      line_solve<2>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 2, bdry), g.tstride, D.dnum[br],
+                    D.dnum[br] * D.dnum[br], 0, o, SR);
+    else
+      line_solve<1>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, D.dnum[br], D.dnum[br], 0, o,
+                    SR);
+  }
+  __syncthreads();
+  // radial terms
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int j = pt / TL, l = pt - j * TL;
+    int it = tb + l, ir = r0 + j;
+    if (it >= g.nth) continue;
+    size_t id = css_idx(g, it, ip, ir);
+    const double *hl = H + (size_t)(j + 4) * SR + l;
+    double u = hl[2 * HS], s = hl[3 * HS], rho = hl[4 * HS];
+    const double *ol = O + (size_t)j * SR + l;
+    double w3 = g.dxdr[ir];
+    double t = temp_of(g, rho, s), invrho = 1.0 / rho;
+    double w1 = ol[0];
+    if (nu) w1 = w1 * w3;
+    double dw = dv[n + id];
+    dw = dw - u * w1;
+    w1 = ol[OS];
+    if (nu) w1 = w1 * w3;
+    double dvv = dv[2 * n + id];
+    dvv = dvv - u * w1;
+    double du = dv[3 * n + id];
+    w1 = ol[2 * OS];
+    if (nu) w1 = w1 * w3;
+    du = du - u * w1;
+    double drho = dv[id];
+    drho = drho - rho * w1;
+    double ds = dv[4 * n + id];
+    w1 = ol[3 * OS];
+    if (nu) w1 = w1 * w3;
+    du = du - g.gamm1 * t * w1;
+    ds = ds - u * w1;
+    if (g.slaplacian) {
+      double oorho = invrho / t;
+      double work6 = (2.0 * g.r_inv[ir] + g.dlnks[ir]) * g.ks[ir];
+      w1 = w1 * oorho;
+      ds = ds + w1 * work6;
+      if (nu) ds = ds + (g.d2xdr2[ir] / w3) * w1 * g.ks[ir];
+      double d2 = ol[4 * OS];
+      if (nu) d2 = d2 * (w3 * w3);
+      ds = ds + g.ks[ir] * d2 * oorho;
+    }
+    if (mag) {
+      double oo = invrho * ONE_OVER_4PI;
+      double bt_ = hl[5 * HS], bp_ = hl[6 * HS], br_ = __ldg(bf + 2 * n + id);
+      w1 = ol[5 * OS];
+      if (nu) w1 = w1 * w3;
+      w1 = w1 * oo;
+      du = du - bt_ * w1;
+      dw = dw + br_ * w1;
+      w1 = ol[6 * OS];
+      if (nu) w1 = w1 * w3;
+      w1 = w1 * oo;
+      dvv = dvv + br_ * w1;
+      du = du - bp_ * w1;
+    }
+    double *al = A + (size_t)j * SR + l;
+    al[0] = drho;
+    al[OS] = dw;
+    al[2 * OS] = dvv;
+    al[3 * OS] = du;
+    al[4 * OS] = ds;
+  }
+  __syncthreads();
+  // density radial: BC datum from the completed du on the physical face
+  for (int l = threadIdx.x; l < TL; l += blockDim.x) {
+    if (tb + l >= g.nth) continue;
+    const double *x = H + 4 * HS + 4 * SR + l;  // rho
+    double lo = 0.0, hi = 0.0;
+    if (D.lphys[br]) {
+      double rho = x[0], t = temp_of(g, rho, H[3 * HS + 4 * SR + l]);
+      double du = A[3 * OS + l];
+      if (g.lbcr_rho == 2 || g.lbcr_rho == 4) lo = du * rho * g.invpconst / t;
+      else lo = rho;
+      if (nu) lo = lo / g.dxdr[0];
+    } else if (D.rphys[br]) {
+      double rho = x[(m - 1) * SR], t = temp_of(g, rho, H[3 * HS + (m + 3) * SR + l]);
+      double du = A[3 * OS + (size_t)(m - 1) * SR + l];
+      if (g.lbcr_rho == 3 || g.lbcr_rho == 4) hi = du * rho * g.invpconst / t;
+      else hi = rho;
+      if (nu) hi = hi / g.dxdr[nr - 1];
+    }
+    int bdry = g.ibcr[1];
+    line_solve<1>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, D.dnum[br], D.dnum[br], 0,
+                  O + l, SR);
+  }
+  __syncthreads();
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int j = pt / TL, l = pt - j * TL;
+    int it = tb + l, ir = r0 + j;
+    if (it >= g.nth) continue;
+    size_t id = css_idx(g, it, ip, ir);
+    const double *hl = H + (size_t)(j + 4) * SR + l;
+    double u = hl[2 * HS], s = hl[3 * HS], rho = hl[4 * HS];
+    double t = temp_of(g, rho, s), invrho = 1.0 / rho;
+    const double *al = A + (size_t)j * SR + l;
+    double w1 = O[(size_t)j * SR + l];
+    if (nu) w1 = w1 * g.dxdr[ir];
+    double drho = al[0] - u * w1;
+    w1 = w1 * invrho;
+    double du = al[3 * OS] - g.pconst * t * w1;
+    double ds = al[4 * OS];
+    if (D.rphys[br] && j == m - 1 && !g.set_stop) {  // rhs_mpi.f90:1807-1818
+      drho = drho + rho * (g.t0 - t) / (g.damping_time * (g.gamma - 2.0) * t);
+      ds = ds - g.cv * (g.t0 - t) / (g.damping_time * (g.gamma - 2.0) * t);
+    }
+    dv[id] = drho;
+    dv[n + id] = al[OS];
+    dv[2 * n + id] = al[2 * OS];
+    dv[3 * n + id] = du;
+    dv[4 * n + id] = ds;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Density_Terms_Theta (rhs_mpi.f90:1522-1605) fused with the RK4 stage
+// combination of Step_RK4 (step_rk4.f90:385-475) and Bound (rhs_mpi.f90:
+// 2395-2491).  stage 0 = no update (the RHS alone).  grid: x = theta block
+// * nchunk + phi chunk, y = r.
+//   stage 1: vs = (sld ? vs + dv/6 : dv); nx = v0 + dtcur*dv
+//   stage 2,3: vs = vs + dv/3;            nx = v0 + dtcur*dv
+//   stage 4: vs = vs + dv/6;              nx = v0 + dtcur*vs  (nx may be v0)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__restrict__ cur,
+                                                     double *__restrict__ dv, const double *v0, double *vs, double *nx,
+                                                     int stage, double dtcur, int TL, int *flag) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nphi + TL - 1) / TL;
+  const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
+  const int ir = blockIdx.y;
+  const CssDir &D = g.d[1];
+  const int t0 = D.start[bt], m = D.size[bt];
+  const int dtype = dtype_of(D, bt);
+  const int SR = m + 9, SO = m + 1;
+  const size_t n = (size_t)g.ncell;
+  double *H = sm;
+  double *O = H + (size_t)TL * SR;
+  load_theta_tile(g, cur, H, SR, t0, m, pb, TL, ir, true);
+  __syncthreads();
+  const double rvv = g.r_ind[ir] * g.invpconst, ri = g.r_inv[ir];
+  for (int l = threadIdx.x; l < TL; l += blockDim.x) {
+    if (pb + l >= g.nphi) continue;
+    const double *x = H + (size_t)l * SR + 4;
+    double lo = 0.0, hi = 0.0;
+    if (D.lphys[bt]) {  // rhs_mpi.f90:1553-1555: make dw = 0 on the wall
+      size_t id = css_idx(g, t0, pb + l, ir);
+      double rho = x[0], t = temp_of(g, rho, __ldg(cur + 4 * n + id));
+      lo = rvv * dv[n + id] * rho / t;
+    } else if (D.rphys[bt]) {
+      size_t id = css_idx(g, t0 + m - 1, pb + l, ir);
+      double rho = x[m - 1], t = temp_of(g, rho, __ldg(cur + 4 * n + id));
+      hi = rvv * dv[n + id] * rho / t;
+    }
+    int bdry = g.ibct[1];
+    line_solve<1>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, D.dnum[bt], D.dnum[bt], 0,
+                  O + (size_t)l * SO, 1);
+  }
+  __syncthreads();
+  const int nv = g.nv;
+  int bad = 0;
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int l = pt / m, j = pt - l * m;
+    int it = t0 + j, ip = pb + l;
+    if (ip >= g.nphi) continue;
+    size_t id = css_idx(g, it, ip, ir);
+    double rho = H[(size_t)l * SR + 4 + j];
+    double w = __ldg(cur + n + id), s = __ldg(cur + 4 * n + id);
+    double t = temp_of(g, rho, s);
+    double w1 = ri * O[(size_t)l * SO + j];
+    double d0 = dv[id] - w * w1;
+    w1 = w1 * (1.0 / rho);
+    double d1 = dv[n + id] - g.pconst * w1 * t;
+    if (g.xi_cs < 1.0) d0 = (g.xi_cs * g.xi_cs) * d0;
+    if (stage == 0) {
+      dv[id] = d0;
+      dv[n + id] = d1;
+      continue;
+    }
+    for (int iv = 0; iv < nv; iv++) {
+      size_t q = (size_t)iv * n + id;
+      double d = (iv == 0) ? d0 : (iv == 1) ? d1 : dv[q];
+      double a = v0[q], o;
+      if (stage == 1) {
+        double sv = g.sldiffusion ? vs[q] + d / 6.0 : d;
+        vs[q] = sv;
+        o = a + dtcur * d;
+      } else if (stage == 4) {
+        double sv = vs[q] + d / 6.0;
+        o = a + dtcur * sv;
+      } else {
+        double sv = vs[q] + d / 3.0;
+        vs[q] = sv;
+        o = a + dtcur * d;
+      }
+      // Bound (rhs_mpi.f90:2395-2491)
+      if (iv == 1 && (it == 0 || it == g.nth - 1)) o = 0.0;
+      if (iv == 3 && !g.theta_stress_free && (it == 0 || it == g.nth - 1)) o = 0.0;
+      if (ir == 0) {
+        if ((iv == 1 || iv == 2) && !g.bottom_stress_free) o = 0.0;
+        if (iv == 3) o = 0.0;
+      }
+      if (ir == g.nr - 1) {
+        if ((iv == 1 || iv == 2) && !g.top_stress_free) o = 0.0;
+        if (iv == 3) o = 0.0;
+      }
+      if (iv >= 5) {
+        if (g.theta_perf_conductor) {
+          if ((iv == 6 || iv == 7) && (it == 0 || it == g.nth - 1)) o = 0.0;
+        } else if (iv == 5 && (it == 0 || it == g.nth - 1)) {
+          o = 0.0;
+        }
+        if (ir == 0) {
+          if (g.bottom_radial_field) { if (iv == 7) o = 0.0; }
+          else if (g.bottom_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+        }
+        if (ir == g.nr - 1) {
+          if (g.top_radial_field) { if (iv == 7) o = 0.0; }
+          else if (g.top_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+        }
+      }
+      if (!isfinite(o)) bad = 1;
+      nx[q] = o;
+    }
+  }
+  if (bad && flag) atomicOr(flag, 1);
+}
+
+// ---------------------------------------------------------------------------
+// VectorCurlA (derivatives.f90:2106-2294): out = curl(a), fields ordered
+// (theta, phi, r).  Three kernels, one per sweep direction; the r sweep
+// optionally applies Compute_B's boundary zeroing (:1842-1883).
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
+                                                    int TL) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nphi + TL - 1) / TL;
+  const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
+  const int ir = blockIdx.y;
+  const CssDir &D = g.d[1];
+  const int t0 = D.start[bt], m = D.size[bt];
+  const int dtype = dtype_of(D, bt);
+  const int SR = m + 9, SO = m + 1;
+  const size_t n = (size_t)g.ncell;
+  double *H = sm;                      // 0: sin*A_phi, 1: A_r
+  double *O = H + (size_t)2 * TL * SR;
+  load_theta_tile(g, a + n, H, SR, t0, m, pb, TL, ir, true);
+  load_theta_tile(g, a + 2 * n, H + (size_t)TL * SR, SR, t0, m, pb, TL, ir, true);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < TL * (m + 8); idx += blockDim.x) {
+    int l = idx / (m + 8), jj = idx - l * (m + 8);
+    int gt = t0 + jj - 4;
+    if (gt < 0 || gt >= g.nth) continue;
+    H[(size_t)l * SR + jj] *= g.sines[gt];
+  }
+  __syncthreads();
+  for (int task = threadIdx.x; task < 2 * TL; task += blockDim.x) {
+    int k = task / TL, l = task - k * TL;
+    if (pb + l >= g.nphi) continue;
+    int bdry = g.ibct[k == 0 ? 11 : 12];
+    line_solve<1>(H + ((size_t)k * TL + l) * SR + 4, 1, m, dtype, bdry, 0.0, 0.0, tabp(g, 1, bt, 1, bdry), g.tstride,
+                  D.dnum[bt], D.dnum[bt], 0, O + ((size_t)k * TL + l) * SO, 1);
+  }
+  __syncthreads();
+  const double invr = g.r_inv[ir];
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int l = pt / m, j = pt - l * m;
+    int it = t0 + j, ip = pb + l;
+    if (ip >= g.nphi) continue;
+    size_t id = css_idx(g, it, ip, ir);
+    out[2 * n + id] = O[(size_t)l * SO + j] * (1.0 / g.sines[it]) * invr;
+    out[n + id] = -O[(size_t)(TL + l) * SO + j] * invr;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
+                                                  int TL) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nth + TL - 1) / TL;
+  const int bp = blockIdx.x / nchunk, tb = (blockIdx.x - bp * nchunk) * TL;
+  const int ir = blockIdx.y;
+  const CssDir &D = g.d[2];
+  const int p0 = D.start[bp], m = D.size[bp];
+  const int SR = TL + 1;
+  const size_t n = (size_t)g.ncell;
+  const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
+  double *H = sm;  // 0: A_r, 1: A_theta
+  double *O = H + 2 * HS;
+  load_phi_tile(g, a + 2 * n, H, SR, p0, m, tb, TL, ir, true);
+  load_phi_tile(g, a, H + HS, SR, p0, m, tb, TL, ir, true);
+  __syncthreads();
+  for (int task = threadIdx.x; task < 2 * TL; task += blockDim.x) {
+    int k = task / TL, l = task - k * TL;
+    if (tb + l >= g.nth) continue;
+    line_solve<1>(H + k * HS + 4 * SR + l, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, D.dnum[bp],
+                  D.dnum[bp], 1, O + k * OS + l, SR);
+  }
+  __syncthreads();
+  const double invr = g.r_inv[ir];
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int j = pt / TL, l = pt - j * TL;
+    int it = tb + l, ip = p0 + j;
+    if (it >= g.nth) continue;
+    size_t id = css_idx(g, it, ip, ir);
+    double csc = 1.0 / g.sines[it];
+    out[id] = invr * O[(size_t)j * SR + l] * csc;
+    out[2 * n + id] = out[2 * n + id] - invr * O[OS + (size_t)j * SR + l] * csc;
+  }
+}
+
+__global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
+                                                int TL, int apply_bc) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nth + TL - 1) / TL;
+  const int br = blockIdx.x / nchunk, tb = (blockIdx.x - br * nchunk) * TL;
+  const int ip = blockIdx.y;
+  const CssDir &D = g.d[0];
+  const int r0 = D.start[br], m = D.size[br];
+  const int dtype = dtype_of(D, br);
+  const int SR = TL + 1;
+  const size_t n = (size_t)g.ncell;
+  const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
+  double *H = sm;  // 0: r*A_theta, 1: r*A_phi
+  double *O = H + 2 * HS;
+  load_r_tile(g, a, H, SR, r0, m, tb, TL, ip, true);
+  load_r_tile(g, a + n, H + HS, SR, r0, m, tb, TL, ip, true);
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < TL * (m + 8); idx += blockDim.x) {
+    int jj = idx / TL, l = idx - jj * TL;
+    int gr = r0 + jj - 4;
+    if (gr < 0 || gr >= g.nr) continue;
+    H[(size_t)jj * SR + l] *= g.r_ind[gr];
+    H[HS + (size_t)jj * SR + l] *= g.r_ind[gr];
+  }
+  __syncthreads();
+  for (int task = threadIdx.x; task < 2 * TL; task += blockDim.x) {
+    int k = task / TL, l = task - k * TL;
+    if (tb + l >= g.nth) continue;
+    int bdry = g.ibcr[k == 0 ? 10 : 11];
+    line_solve<1>(H + k * HS + 4 * SR + l, SR, m, dtype, bdry, 0.0, 0.0, tabp(g, 0, br, 1, bdry), g.tstride,
+                  D.dnum[br], D.dnum[br], 0, O + k * OS + l, SR);
+  }
+  __syncthreads();
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int j = pt / TL, l = pt - j * TL;
+    int it = tb + l, ir = r0 + j;
+    if (it >= g.nth) continue;
+    size_t id = css_idx(g, it, ip, ir);
+    double d = O[(size_t)j * SR + l];
+    if (g.non_uniform) d = d * g.dxdr[ir];
+    double bp_ = out[n + id] + d * g.r_inv[ir];
+    d = O[OS + (size_t)j * SR + l];
+    if (g.non_uniform) d = d * g.dxdr[ir];
+    double bt_ = out[id] - d * g.r_inv[ir];
+    double br_ = out[2 * n + id];
+    if (apply_bc) {
+      if (it == 0 || it == g.nth - 1) {
+        if (g.theta_perf_conductor) bt_ = 0.0;
+        else { bp_ = 0.0; br_ = 0.0; }
+      }
+      if (ir == 0) {
+        if (g.bottom_radial_field) { bt_ = 0.0; bp_ = 0.0; }
+        else if (g.bottom_perfect_cond) br_ = 0.0;
+      }
+      if (ir == g.nr - 1) {
+        if (g.top_radial_field) { bt_ = 0.0; bp_ = 0.0; }
+        else if (g.top_perfect_cond) br_ = 0.0;
+      }
+      out[2 * n + id] = br_;
+    }
+    out[id] = bt_;
+    out[n + id] = bp_;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Slope-limited diffusion (diffusion.f90:70-474).  The block faces between
+// ranks only carry neighbour data here (halos and the ghost ring of vcc are
+// the neighbour's own values), so only the physical faces need the per-
+// variable ghost rules of Diffusion_R / Diffusion_Th.
+// ---------------------------------------------------------------------------
+// vcc = speed^2(r) + |u|^2 [+ vA^2] (diffusion.f90:177-286), dstype = 1
+__global__ void k_sld_vcc(CssGeo g, const double *__restrict__ v, const double *__restrict__ bf,
+                          double *__restrict__ vcc) {
+  size_t n = (size_t)g.ncell;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x) {
+    int ir = (int)(id / ((size_t)g.nth * g.nphi));
+    double c = g.dspeed[ir];
+    if (g.dstype == 1) {
+      for (int iv = 1; iv <= 3; iv++) {
+        double q = __ldg(v + iv * n + id);
+        c = c + q * q;
+      }
+      if (g.magnetic) {
+        double ir_ = 1.0 / __ldg(v + id);
+        for (int k = 0; k < 3; k++) {
+          double q = __ldg(bf + k * n + id);
+          c = c + ONE_OVER_4PI * ir_ * (q * q);
+        }
+      }
+    }
+    vcc[id] = c;
+  }
+}
+
+__device__ __forceinline__ double sld_limiter(double q, double qph, double tiny) {
+  double rtmp = fabs(q);
+  rtmp = 1.0 / fmax(rtmp, tiny);
+  rtmp = q * (rtmp * rtmp);
+  rtmp = rtmp * qph;
+  rtmp = fmin(1.0, rtmp);
+  return q * fmax(0.0, rtmp);
+}
+
+// limited face difference delta at the face whose neighbours are
+// x(-2..+1) around it: qmh = x_{-1}-x_{-2}, qph = x_0-x_{-1}, qp3h = x_1-x_0
+__device__ __forceinline__ double sld_face(double xm2, double xm1, double x0, double x1, double tiny) {
+  double qmh = xm1 - xm2, qph = x0 - xm1, qp3h = x1 - x0;
+  double pl = sld_limiter(qmh, qph, tiny), pr = sld_limiter(qp3h, qph, tiny);
+  return qph - 0.5 * (pr + pl);
+}
+
+// value of field iv (0-based) the SLD sees: rho - rhor, s - sr, A for iv>=5
+__device__ __forceinline__ double sld_val(const CssGeo &g, const double *__restrict__ v, const double *__restrict__ av,
+                                          int iv, int it, int ip, int ir) {
+  size_t id = css_idx(g, it, ip, ir);
+  size_t n = (size_t)g.ncell;
+  if (iv >= 5) return __ldg(av + (iv - 5) * n + id);
+  double q = __ldg(v + iv * n + id);
+  if (iv == 0) q = q - g.rhor[ir];
+  if (iv == 4) q = q - g.sr[ir];
+  return q;
+}
+
+__global__ void __launch_bounds__(128) k_sld(CssGeo g, const double *__restrict__ v, const double *__restrict__ av,
+                                             const double *__restrict__ vcc, double *__restrict__ dout) {
+  size_t n = (size_t)g.ncell;
+  const int nth = g.nth, nphi = g.nphi, nr = g.nr;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x) {
+    int it = (int)(id % nth);
+    int ip = (int)((id / nth) % nphi);
+    int ir = (int)(id / ((size_t)nth * nphi));
+    const double *r = g.r_ind, *dr = g.dr_ind;
+    // geometry of this cell
+    double rlo = (ir == 0) ? r[0] - 0.5 * dr[0] : 0.5 * (r[ir] + r[ir - 1]);
+    double rhi = (ir == nr - 1) ? r[nr - 1] + 0.5 * dr[nr - 1] : 0.5 * (r[ir + 1] + r[ir]);
+    double t3 = 3.0 / (rhi * rhi * rhi - rlo * rlo * rlo);
+    double rfac = 1.5 * (rhi * rhi - rlo * rlo) / (rhi * rhi * rhi - rlo * rlo * rlo);
+    const double *th = g.theta;
+    double dth = g.dth;
+    double sphl, cphl, sphh, cphh;
+    if (it == 0) { sphl = fabs(sin(th[0] - 0.5 * dth)); cphl = cos(th[0] - 0.5 * dth); }
+    else { double a = 0.5 * (th[it] + th[it - 1]); sphl = sin(a); cphl = cos(a); }
+    if (it == nth - 1) { sphh = sin(th[it] + 0.5 * dth); cphh = cos(th[it] + 0.5 * dth); }
+    else { double a = 0.5 * (th[it] + th[it + 1]); sphh = sin(a); cphh = cos(a); }
+    double geom;
+    {
+      double rt, st, ct;
+      if (it == 0) { rt = th[0] - 0.5 * dth; st = cos(rt); }
+      else { rt = 0.5 * (th[it] + th[it - 1]); st = cos(rt); }
+      if (it == nth - 1) { ct = th[it] + 0.5 * dth; rt = ct - rt; ct = cos(ct); }
+      else { ct = 0.5 * (th[it + 1] + th[it]); rt = ct - rt; ct = cos(ct); }
+      geom = rt / (st - ct);
+      geom = geom * (rfac / g.dphi);
+    }
+    // face speeds
+    double vc = __ldg(vcc + id);
+    auto vface = [&](double a, double b) { return g.sld_coef * sqrt(0.5 * (a + b)); };
+    double vr_lo = (ir > 0) ? vface(vc, __ldg(vcc + css_idx(g, it, ip, ir - 1))) : 0.0;
+    double vr_hi = (ir < nr - 1) ? vface(__ldg(vcc + css_idx(g, it, ip, ir + 1)), vc) : 0.0;
+    double vt_lo = (it > 0) ? vface(vc, __ldg(vcc + id - 1)) : 0.0;
+    double vt_hi = (it < nth - 1) ? vface(__ldg(vcc + id + 1), vc) : 0.0;
+    int ipm = (ip - 1 + nphi) % nphi, ipp = (ip + 1) % nphi;
+    double vp_lo = vface(__ldg(vcc + css_idx(g, it, ipm, ir)), vc);
+    double vp_hi = vface(vc, __ldg(vcc + css_idx(g, it, ipp, ir)));
+    double Dv[8];
+    for (int iv = 0; iv < g.nv; iv++) Dv[iv] = 0.0;
+    for (int isl = 0; isl < g.nsld; isl++) {
+      int iv = g.varlist[isl], iv1 = iv + 1;
+      double tiny = g.tinyvar[iv];
+      double prR = 1.0, prTP = 1.0;
+      if (g.sld_pr != 1.0 || g.sld_prm != 1.0) {
+        if (iv1 <= 3) prR = g.sld_pr; else if (iv1 >= 5) prR = g.sld_prm;
+        if (iv1 < 5) prTP = g.sld_pr; else if (iv1 > 5) prTP = g.sld_prm;
+      }
+      double x0 = sld_val(g, v, av, iv, it, ip, ir);
+      // ---- r ----
+      double xr[5];  // ir-2 .. ir+2
+      xr[2] = x0;
+      for (int k = -2; k <= 2; k++) {
+        if (k == 0) continue;
+        int q = ir + k;
+        if (q >= 0 && q < nr) xr[k + 2] = sld_val(g, v, av, iv, it, ip, q);
+        else xr[k + 2] = 0.0;
+      }
+      // ghost next to a physical radial face (diffusion.f90:582-728)
+      if (ir <= 1) {
+        double t1 = sld_val(g, v, av, iv, it, ip, 0), gl;
+        switch (iv1) {
+          case 1: gl = 0.0; break;
+          case 2: case 3:
+            gl = -10.0 * (1.0 / 3.0) * t1 / r[0] + 6.0 * sld_val(g, v, av, iv, it, ip, 1) / r[1] -
+                 2.0 * sld_val(g, v, av, iv, it, ip, 2) / r[2] + (1.0 / 3.0) * sld_val(g, v, av, iv, it, ip, 3) / r[3];
+            break;
+          case 5:
+            if (!g.bottom_constant_temp && g.slaplacian)
+              gl = t1 + dr[0] * (g.lumr1 * ONE_OVER_4PI / (g.r1 * g.r1 * g.ks[0] * g.dxdr[0]));
+            else gl = 0.0;
+            break;
+          case 6: case 7: gl = g.bottom_perfect_cond ? 0.0 : t1; break;
+          default: gl = t1; break;
+        }
+        xr[ir == 0 ? 1 : 0] = gl;
+      }
+      if (ir >= nr - 2) {
+        int m = nr - 1;
+        double tm = sld_val(g, v, av, iv, it, ip, m), gh;
+        switch (iv1) {
+          case 1: gh = 0.0; break;
+          case 2: case 3:
+            gh = -10.0 * (1.0 / 3.0) * tm / r[m] + 6.0 * sld_val(g, v, av, iv, it, ip, m - 1) / r[m - 1] -
+                 2.0 * sld_val(g, v, av, iv, it, ip, m - 2) / r[m - 2] +
+                 (1.0 / 3.0) * sld_val(g, v, av, iv, it, ip, m - 3) / r[m - 3];
+            break;
+          case 5:
+            if (!g.top_constant_temp && g.slaplacian)
+              gh = tm - dr[0] * (g.lumr2 * ONE_OVER_4PI / (g.r2 * g.r2 * g.ks[nr - 1] * g.dxdr[nr - 1]));
+            else gh = 0.0;
+            break;
+          case 6: case 7: gh = g.top_perfect_cond ? 0.0 : tm; break;
+          default: gh = tm; break;
+        }
+        xr[ir == nr - 1 ? 3 : 4] = gh;
+      }
+      double dlo = (ir == 0) ? 0.0 : sld_face(xr[0], xr[1], xr[2], xr[3], tiny) * (rlo * rlo);
+      double dhi = (ir == nr - 1) ? 0.0 : sld_face(xr[1], xr[2], xr[3], xr[4], tiny) * (rhi * rhi);
+      dlo = vr_lo * dlo;
+      dhi = vr_hi * dhi;
+      double flux = t3 * (dhi - dlo);
+      if (prR != 1.0) flux = prR * flux;
+      double acc = flux;
+      // ---- theta ----
+      double xt[5];
+      xt[2] = x0;
+      for (int k = -2; k <= 2; k++) {
+        if (k == 0) continue;
+        int q = it + k;
+        if (q >= 0 && q < nth) xt[k + 2] = sld_val(g, v, av, iv, q, ip, ir);
+        else xt[k + 2] = 0.0;
+      }
+      if (it <= 1) {
+        double t1 = sld_val(g, v, av, iv, 0, ip, ir), gl;
+        const double *sn = g.sines;
+        switch (iv1) {
+          case 2: gl = 0.0; break;
+          case 3:
+            gl = -10.0 * (1.0 / 3.0) * t1 / sn[0] + 6.0 * sld_val(g, v, av, iv, 1, ip, ir) / sn[1] -
+                 2.0 * sld_val(g, v, av, iv, 2, ip, ir) / sn[2] + (1.0 / 3.0) * sld_val(g, v, av, iv, 3, ip, ir) / sn[3];
+            break;
+          case 6: gl = g.theta_normal_field ? 0.0 : t1; break;
+          case 7: case 8: gl = g.theta_perf_conductor ? 0.0 : t1; break;
+          default: gl = t1; break;
+        }
+        xt[it == 0 ? 1 : 0] = gl;
+      }
+      if (it >= nth - 2) {
+        int m = nth - 1;
+        double tm = sld_val(g, v, av, iv, m, ip, ir), gh;
+        const double *sn = g.sines;
+        switch (iv1) {
+          case 2: gh = 0.0; break;
+          case 3:
+            gh = -10.0 * (1.0 / 3.0) * tm / sn[m] + 6.0 * sld_val(g, v, av, iv, m - 1, ip, ir) / sn[m - 1] -
+                 2.0 * sld_val(g, v, av, iv, m - 2, ip, ir) / sn[m - 2] +
+                 (1.0 / 3.0) * sld_val(g, v, av, iv, m - 3, ip, ir) / sn[m - 3];
+            break;
+          case 6: gh = g.theta_normal_field ? 0.0 : tm; break;
+          case 7: case 8: gh = g.theta_perf_conductor ? 0.0 : tm; break;
+          default: gh = tm; break;
+        }
+        xt[it == nth - 1 ? 3 : 4] = gh;
+      }
+      dlo = (it == 0) ? 0.0 : (vt_lo * sphl) * sld_face(xt[0], xt[1], xt[2], xt[3], tiny);
+      dhi = (it == nth - 1) ? 0.0 : (vt_hi * sphh) * sld_face(xt[1], xt[2], xt[3], xt[4], tiny);
+      flux = (rfac / (cphl - cphh)) * (dhi - dlo);
+      if (prTP != 1.0) flux = prTP * flux;
+      acc = acc + flux;
+      // ---- phi (periodic) ----
+      double xp[5];
+      for (int k = -2; k <= 2; k++) xp[k + 2] = (k == 0) ? x0 : sld_val(g, v, av, iv, it, (ip + k + nphi) % nphi, ir);
+      dlo = vp_lo * sld_face(xp[0], xp[1], xp[2], xp[3], tiny);
+      dhi = vp_hi * sld_face(xp[1], xp[2], xp[3], xp[4], tiny);
+      flux = dhi - dlo;
+      if (prTP != 1.0) flux = prTP * flux;
+      acc = acc + geom * flux;
+      Dv[iv] = acc;
+    }
+    // viscous heating and mass-diffusion corrections (diffusion.f90:375-428)
+    double invrho = 1.0 / __ldg(v + id);
+    double itemp = (pow(__ldg(v + id), -g.gamm1)) * exp(-__ldg(v + 4 * n + id) * g.invcv) / g.invtconst;
+    if (g.do_viscous_heating)
+      for (int iv = 1; iv <= 3; iv++) Dv[4] = Dv[4] - __ldg(v + iv * n + id) * Dv[iv] * itemp;
+    if (g.mass_diffusion) {
+      for (int iv = 1; iv <= 3; iv++) Dv[iv] = Dv[iv] - invrho * __ldg(v + iv * n + id) * Dv[0];
+      Dv[4] = Dv[4] - (g.gamm1 * g.cv) * invrho * Dv[0];
+    }
+    for (int iv = 0; iv < g.nv; iv++) dout[iv * n + id] = Dv[iv];
+  }
+}
+
+// ohmic heating (diffusion.f90:430-455): Ds -= B . curl(D_A) / (8 pi rho T)
+__global__ void k_sld_ohmic(CssGeo g, const double *__restrict__ v, const double *__restrict__ bf,
+                            const double *__restrict__ cda, double *__restrict__ dout) {
+  size_t n = (size_t)g.ncell;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x) {
+    double rho = __ldg(v + id);
+    double itemp = (pow(rho, -g.gamm1)) * exp(-__ldg(v + 4 * n + id) * g.invcv) / g.invtconst;
+    double f = (0.5 * ONE_OVER_4PI) * (1.0 / rho) * itemp;
+    double ds = dout[4 * n + id];
+    for (int k = 0; k < 3; k++) ds = ds - __ldg(bf + k * n + id) * __ldg(cda + k * n + id) * f;
+    dout[4 * n + id] = ds;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// generic single-field derivative (css_deriv): one kernel per direction
+// ---------------------------------------------------------------------------
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_deriv_theta(CssGeo g, const double *__restrict__ f, double *__restrict__ out,
+                                                     const double *__restrict__ bclo, const double *__restrict__ bchi,
+                                                     int bdry, int TL) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nphi + TL - 1) / TL;
+  const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
+  const int ir = blockIdx.y;
+  const CssDir &D = g.d[1];
+  const int t0 = D.start[bt], m = D.size[bt];
+  const int SR = m + 9, SO = m + 1;
+  double *H = sm, *O = H + (size_t)TL * SR;
+  load_theta_tile(g, f, H, SR, t0, m, pb, TL, ir, true);
+  __syncthreads();
+  for (int l = threadIdx.x; l < TL; l += blockDim.x) {
+    int ip = pb + l;
+    if (ip >= g.nphi) continue;
+    double lo = (D.lphys[bt] && bclo) ? bclo[ip + (size_t)g.nphi * ir] : 0.0;
+    double hi = (D.rphys[bt] && bchi) ? bchi[ip + (size_t)g.nphi * ir] : 0.0;
+    double dn = (ORDER == 1) ? D.dnum[bt] : dnum_d2_theta(g, ir);
+    double sc = (ORDER == 1) ? D.dnum[bt] : D.dnum[bt] * D.dnum[bt];
+    line_solve<ORDER>(H + (size_t)l * SR + 4, 1, m, dtype_of(D, bt), bdry, lo, hi, tabp(g, 1, bt, ORDER, bdry),
+                      g.tstride, dn, sc, 0, O + (size_t)l * SO, 1);
+  }
+  __syncthreads();
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int l = pt / m, j = pt - l * m;
+    if (pb + l >= g.nphi) continue;
+    out[css_idx(g, t0 + j, pb + l, ir)] = O[(size_t)l * SO + j];
+  }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_deriv_phi(CssGeo g, const double *__restrict__ f, double *__restrict__ out,
+                                                   int TL) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nth + TL - 1) / TL;
+  const int bp = blockIdx.x / nchunk, tb = (blockIdx.x - bp * nchunk) * TL;
+  const int ir = blockIdx.y;
+  const CssDir &D = g.d[2];
+  const int p0 = D.start[bp], m = D.size[bp];
+  const int SR = TL + 1;
+  double *H = sm, *O = H + (size_t)(m + 8) * SR;
+  load_phi_tile(g, f, H, SR, p0, m, tb, TL, ir, true);
+  __syncthreads();
+  for (int l = threadIdx.x; l < TL; l += blockDim.x) {
+    if (tb + l >= g.nth) continue;
+    double sc = (ORDER == 1) ? D.dnum[bp] : D.dnum[bp] * D.dnum[bp];
+    line_solve<ORDER>(H + 4 * SR + l, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, ORDER, 0), g.tstride, D.dnum[bp], sc, 1,
+                      O + l, SR);
+  }
+  __syncthreads();
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int j = pt / TL, l = pt - j * TL;
+    if (tb + l >= g.nth) continue;
+    out[css_idx(g, tb + l, p0 + j, ir)] = O[(size_t)j * SR + l];
+  }
+}
+
+template <int ORDER>
+__global__ void __launch_bounds__(128) k_deriv_r(CssGeo g, const double *__restrict__ f, double *__restrict__ out,
+                                                 const double *__restrict__ bclo, const double *__restrict__ bchi,
+                                                 int bdry, int TL) {
+  extern __shared__ double sm[];
+  const int nchunk = (g.nth + TL - 1) / TL;
+  const int br = blockIdx.x / nchunk, tb = (blockIdx.x - br * nchunk) * TL;
+  const int ip = blockIdx.y;
+  const CssDir &D = g.d[0];
+  const int r0 = D.start[br], m = D.size[br];
+  const int SR = TL + 1;
+  double *H = sm, *O = H + (size_t)(m + 8) * SR;
+  load_r_tile(g, f, H, SR, r0, m, tb, TL, ip, true);
+  __syncthreads();
+  for (int l = threadIdx.x; l < TL; l += blockDim.x) {
+    int it = tb + l;
+    if (it >= g.nth) continue;
+    double lo = (D.lphys[br] && bclo) ? bclo[it + (size_t)g.nth * ip] : 0.0;
+    double hi = (D.rphys[br] && bchi) ? bchi[it + (size_t)g.nth * ip] : 0.0;
+    double sc = (ORDER == 1) ? D.dnum[br] : D.dnum[br] * D.dnum[br];
+    line_solve<ORDER>(H + 4 * SR + l, SR, m, dtype_of(D, br), bdry, lo, hi, tabp(g, 0, br, ORDER, bdry), g.tstride,
+                      D.dnum[br], sc, 0, O + l, SR);
+  }
+  __syncthreads();
+  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+    int j = pt / TL, l = pt - j * TL;
+    if (tb + l >= g.nth) continue;
+    out[css_idx(g, tb + l, ip, r0 + j)] = O[(size_t)j * SR + l];
+  }
+}
+
+// independent lines with explicit closures (css_compact_lines /
+// Dbyd1_dt0): one thread per line on global memory, lines contiguous.
+__global__ void k_lines(const double *__restrict__ x, double *__restrict__ out, int n, int nlines, int order,
+                        int dtype, int bdry, const double *__restrict__ bclo, const double *__restrict__ bchi,
+                        const double *__restrict__ hlo, const double *__restrict__ hhi, const double *__restrict__ tab,
+                        int ts, double dnum, double scale, double *__restrict__ work) {
+  int l = blockIdx.x * blockDim.x + threadIdx.x;
+  if (l >= nlines) return;
+  double *xs = work + (size_t)l * (n + 8);
+  for (int k = 0; k < 4; k++) {
+    xs[k] = hlo ? hlo[(size_t)4 * l + k] : 0.0;
+    xs[n + 4 + k] = hhi ? hhi[(size_t)4 * l + k] : 0.0;
+  }
+  for (int j = 0; j < n; j++) xs[j + 4] = x[(size_t)l * n + j];
+  double lo = bclo ? bclo[l] : 0.0, hi = bchi ? bchi[l] : 0.0;
+  const double *G = tab + (size_t)bdry * 3 * ts;
+  if (order == 1)
+    line_solve<1>(xs + 4, 1, n, dtype, bdry, lo, hi, G, ts, dnum, scale, 0, out + (size_t)l * n, 1);
+  else
+    line_solve<2>(xs + 4, 1, n, dtype, bdry, lo, hi, G, ts, dnum, scale, 0, out + (size_t)l * n, 1);
+}
+
+}  // namespace css

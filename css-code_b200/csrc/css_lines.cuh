@@ -1,0 +1,213 @@
+// css_lines.cuh -- the compact sixth-order line operators on one block
+// segment, solved by one thread with the precomputed LU (Thomas) tables.
+//
+// x points at the first point of the segment in shared memory; point j
+// (1-based) sits at x[(j-1)*sx]; the four halo points below the segment at
+// j = -3..0 and the four above at j = m+1..m+4.  At a physical end the
+// boundary datum comes in bclo/bchi instead (the 1-deep BC slot of the
+// reference's binfo, parallel_mpi.f90:351-530).
+//
+// dtype follows Determine_Dtype (derivatives.f90:529-544): 1 = halo below /
+// physical above, 2 = physical below / halo above, 3 = halo both; 0 = both
+// ends physical (the whole-line case the reference only reaches through
+// Dbyd1_dt0 / CSS-Python compact_fd6).  The row formulas are those of
+// Dbydr/Dbydt (derivatives.f90:564-728, :1031-1194), D2bydr2/D2bydt2
+// (:816-939, :1286-1409) and Dbydp/D2bydp2 (:1491-1532, :1605-1627); the
+// sweeps are :730-795.
+#pragma once
+
+namespace css {
+
+// constants of the halo-closed rows (derivatives.f90:684-720)
+struct HaloD1 {
+  static constexpr double c1 = -1.0 / 180.0;
+  static constexpr double c2 = c1 * 9.0;
+  static constexpr double c3 = c1 * 45.0;
+  static constexpr double c5 = 1.0 / 36.0;
+  static constexpr double cnst = -(c3 + c5);
+  static constexpr double beta1 = 7.0 / 9.0 - c2;
+  static constexpr double alpha1 = c1 + c5;
+  // right end
+  static constexpr double r_c1 = 7.0 / 9.0, r_c2 = 1.0 / 36.0, r_c3 = -1.0 / 180.0;
+  static constexpr double r_cnst = r_c2 + r_c3 * 45.0;
+  static constexpr double r_beta1 = r_c3 * 9.0 - r_c1;
+  static constexpr double r_alpha1 = -(r_c2 + r_c3);
+  static constexpr double r_c4 = -r_c3 * 9.0;
+  static constexpr double r_c5 = -r_c3 * 45.0;
+  // preconditioned 5th-order physical row (derivatives.f90:604-619)
+  static constexpr double pc = 1.0 / (0.75 - 3.0 * 0.125);
+  static constexpr double pa2 = 0.75 * pc;
+  static constexpr double pb1 = -3.0 * pc;
+};
+
+#define CSS_X(j) x[((j)-1) * sx]
+
+// Right-hand side of the first-derivative system, rows written to d[] (a
+// per-thread scratch that aliases the output buffer).  Returns nothing; the
+// caller runs the sweeps.
+__device__ __forceinline__ double d1_row_lo1(const double *x, int sx, int dtype, int bdry, double bclo,
+                                             double dnum, double row2) {
+  if (dtype == 1 || dtype == 3) {
+    return (-HaloD1::c1) * CSS_X(-3) + HaloD1::c2 * CSS_X(-2) + HaloD1::cnst * CSS_X(-1) +
+           (-(7.0 / 9.0)) * CSS_X(0) + HaloD1::c3 * CSS_X(1) + HaloD1::beta1 * CSS_X(2) +
+           HaloD1::alpha1 * CSS_X(3);
+  }
+  double r = 0.0;
+  if (bdry % 2 == 0) r = bclo / dnum;
+  if (bdry == 0) r = 0.0;
+  if (bdry == 1 || bdry == 3) {
+    r = (-10.0 / 3.0) * CSS_X(1) + (-3.0) * CSS_X(2) + 6.0 * CSS_X(3) + (1.0 / 3.0) * CSS_X(4);
+    r = HaloD1::pa2 * r + HaloD1::pb1 * row2;
+  }
+  return r;
+}
+
+__device__ __forceinline__ double d1_row_lo2(const double *x, int sx, int dtype) {
+  if (dtype == 1 || dtype == 3)
+    return (7.0 / 9.0) * (CSS_X(3) - CSS_X(1)) + (1.0 / 36.0) * (CSS_X(4) - CSS_X(0));
+  return (-43.0 / 96.0) * CSS_X(1) + (-5.0 / 6.0) * CSS_X(2) + (9.0 / 8.0) * CSS_X(3) + (1.0 / 6.0) * CSS_X(4) +
+         (-1.0 / 96.0) * CSS_X(5);
+}
+
+__device__ __forceinline__ double d1_row_hi1(const double *x, int sx, int m, int dtype) {  // row m-1
+  if (dtype == 2 || dtype == 3)
+    return HaloD1::r_c1 * (CSS_X(m) - CSS_X(m - 2)) + HaloD1::r_c2 * (CSS_X(m + 1) - CSS_X(m - 3));
+  return (43.0 / 96.0) * CSS_X(m) + (5.0 / 6.0) * CSS_X(m - 1) + (-9.0 / 8.0) * CSS_X(m - 2) +
+         (-1.0 / 6.0) * CSS_X(m - 3) + (1.0 / 96.0) * CSS_X(m - 4);
+}
+
+__device__ __forceinline__ double d1_row_hi2(const double *x, int sx, int m, int dtype, int bdry, double bchi,
+                                             double dnum, double rowm1) {  // row m
+  if (dtype == 2 || dtype == 3)
+    return HaloD1::r_c1 * CSS_X(m + 1) + HaloD1::r_cnst * CSS_X(m + 2) + HaloD1::r_c4 * CSS_X(m + 3) +
+           HaloD1::r_c3 * CSS_X(m + 4) + HaloD1::r_beta1 * CSS_X(m - 1) + HaloD1::r_alpha1 * CSS_X(m - 2) +
+           HaloD1::r_c5 * CSS_X(m);
+  double r;
+  if (bdry == 3 || bdry == 4) r = bchi / dnum;
+  else r = 0.0;
+  if (bdry == 1 || bdry == 2) {
+    r = (10.0 / 3.0) * CSS_X(m) + 3.0 * CSS_X(m - 1) + (-6.0) * CSS_X(m - 2) + (-1.0 / 3.0) * CSS_X(m - 3);
+    r = HaloD1::pa2 * r + HaloD1::pb1 * rowm1;
+  }
+  return r;
+}
+
+__device__ __forceinline__ double d1_row_int(const double *x, int sx, int j) {
+  return (7.0 / 9.0) * (CSS_X(j + 1) - CSS_X(j - 1)) + (1.0 / 36.0) * (CSS_X(j + 2) - CSS_X(j - 2));
+}
+
+// ---- second derivative rows ----
+struct HaloD2 {
+  static constexpr double c1 = 12.0 / 11.0, c2 = 3.0 / 44.0, c3 = -1.0 / 990.0;
+};
+
+__device__ __forceinline__ double d2_row_lo1(const double *x, int sx, int dtype, int bdry, double bclo, double dnum) {
+  if (dtype == 1 || dtype == 3) {
+    double r = HaloD2::c3 * (2.0 * (CSS_X(-3) + CSS_X(3)) + (-27.0) * (CSS_X(-2) + CSS_X(2)) +
+                             270.0 * (CSS_X(-1) + CSS_X(1)) + (-490.0) * CSS_X(0));
+    return r + HaloD2::c1 * (CSS_X(2) - 2.0 * CSS_X(1) + CSS_X(0)) + HaloD2::c2 * (CSS_X(-1) - 2.0 * CSS_X(1) + CSS_X(3));
+  }
+  if (bdry % 2 == 0) {
+    double c1 = -575.0 / 193.0 / dnum;
+    if (bdry == 0) c1 = 0.0;
+    return c1 * bclo + (-5827.0 / 2316.0) * CSS_X(2) + (1987.0 / 1158.0) * CSS_X(3) + (465.0 / 386.0) * CSS_X(4) +
+           (-547.0 / 1158.0) * CSS_X(5) + (157.0 / 2316.0) * CSS_X(6);
+  }
+  return (1955.0 / 156.0) * CSS_X(1) + (-4057.0 / 156.0) * CSS_X(2) + (1117.0 / 78.0) * CSS_X(3) +
+         (-55.0 / 78.0) * CSS_X(4) + (-29.0 / 156.0) * CSS_X(5) + (7.0 / 156.0) * CSS_X(6);
+}
+
+__device__ __forceinline__ double d2_row_lo2(const double *x, int sx, int dtype) {
+  if (dtype == 1 || dtype == 3)
+    return HaloD2::c1 * (CSS_X(3) - 2.0 * CSS_X(2) + CSS_X(1)) + HaloD2::c2 * (CSS_X(0) - 2.0 * CSS_X(2) + CSS_X(4));
+  return 1.2375 * CSS_X(1) + (-3.0) * CSS_X(2) + 2.325 * CSS_X(3) + (-0.6) * CSS_X(4) + 0.0375 * CSS_X(5);
+}
+
+__device__ __forceinline__ double d2_row_hi1(const double *x, int sx, int m, int dtype) {
+  if (dtype == 2 || dtype == 3)
+    return HaloD2::c1 * (CSS_X(m) - 2.0 * CSS_X(m - 1) + CSS_X(m - 2)) +
+           HaloD2::c2 * (CSS_X(m - 3) - 2.0 * CSS_X(m - 1) + CSS_X(m + 1));
+  return 1.2375 * CSS_X(m) + (-3.0) * CSS_X(m - 1) + 2.325 * CSS_X(m - 2) + (-0.6) * CSS_X(m - 3) + 0.0375 * CSS_X(m - 4);
+}
+
+__device__ __forceinline__ double d2_row_hi2(const double *x, int sx, int m, int dtype, int bdry, double bchi,
+                                             double dnum) {
+  if (dtype == 2 || dtype == 3) {
+    double r = HaloD2::c1 * (CSS_X(m + 1) - 2.0 * CSS_X(m) + CSS_X(m - 1)) +
+               HaloD2::c2 * (CSS_X(m - 2) - 2.0 * CSS_X(m) + CSS_X(m + 2));
+    return r + HaloD2::c3 * (2.0 * (CSS_X(m - 2) + CSS_X(m + 4)) + (-27.0) * (CSS_X(m - 1) + CSS_X(m + 3)) +
+                             270.0 * (CSS_X(m) + CSS_X(m + 2)) + (-490.0) * CSS_X(m + 1));
+  }
+  if (bdry == 1 || bdry == 2)
+    return (1955.0 / 156.0) * CSS_X(m) + (-4057.0 / 156.0) * CSS_X(m - 1) + (1117.0 / 78.0) * CSS_X(m - 2) +
+           (-55.0 / 78.0) * CSS_X(m - 3) + (-29.0 / 156.0) * CSS_X(m - 4) + (7.0 / 156.0) * CSS_X(m - 5);
+  double c1 = 575.0 / 193.0 / dnum;
+  if (bdry == 0) c1 = 0.0;
+  return c1 * bchi + (-5827.0 / 2316.0) * CSS_X(m - 1) + (1987.0 / 1158.0) * CSS_X(m - 2) +
+         (465.0 / 386.0) * CSS_X(m - 3) + (-547.0 / 1158.0) * CSS_X(m - 4) + (157.0 / 2316.0) * CSS_X(m - 5);
+}
+
+__device__ __forceinline__ double d2_row_int(const double *x, int sx, int j) {
+  return HaloD2::c1 * (CSS_X(j + 1) - 2.0 * CSS_X(j) + CSS_X(j - 1)) +
+         HaloD2::c2 * (CSS_X(j - 2) - 2.0 * CSS_X(j) + CSS_X(j + 2));
+}
+
+// One line: ORDER 1 or 2.  G points at the 1-based tables of this block and
+// bdry: g1 = G, g2 = G + ts, g3 = G + 2 ts.  phi = 1 selects the Dbydp /
+// D2bydp2 sweep form (every row after the first as g2*(d + a*t)).
+// out[(j-1)*so] receives scale * solution.
+template <int ORDER>
+__device__ __forceinline__ void line_solve(const double *__restrict__ x, int sx, int m, int dtype, int bdry,
+                                           double bclo, double bchi, const double *__restrict__ G, int ts,
+                                           double dnum, double scale, int phi, double *__restrict__ out,
+                                           int so) {
+  const double *g1 = G, *g2 = G + ts, *g3 = G + 2 * ts;
+  const double a1 = (ORDER == 1) ? -1.0 / 3.0 : -2.0 / 11.0;
+  double r1, r2, rm1, rm;
+  if (ORDER == 1) {
+    r2 = d1_row_lo2(x, sx, dtype);
+    r1 = d1_row_lo1(x, sx, dtype, bdry, bclo, dnum, r2);
+    rm1 = d1_row_hi1(x, sx, m, dtype);
+    rm = d1_row_hi2(x, sx, m, dtype, bdry, bchi, dnum, rm1);
+  } else {
+    r1 = d2_row_lo1(x, sx, dtype, bdry, bclo, dnum);
+    r2 = d2_row_lo2(x, sx, dtype);
+    rm1 = d2_row_hi1(x, sx, m, dtype);
+    rm = d2_row_hi2(x, sx, m, dtype, bdry, bchi, dnum);
+  }
+  double t = __ldg(g2 + 1) * r1;
+  out[0] = t;
+  if (phi) {
+    t = __ldg(g2 + 2) * (r2 + a1 * t);
+    out[so] = t;
+    for (int j = 3; j <= m - 2; j++) {
+      double d = (ORDER == 1) ? d1_row_int(x, sx, j) : d2_row_int(x, sx, j);
+      t = __ldg(g2 + j) * (d + a1 * t);
+      out[(j - 1) * so] = t;
+    }
+    t = __ldg(g2 + m - 1) * (rm1 + a1 * t);
+    out[(m - 2) * so] = t;
+    t = __ldg(g2 + m) * (rm + a1 * t);
+  } else {
+    t = __ldg(g2 + 2) * r2 + __ldg(g3 + 2) * t;
+    out[so] = t;
+    for (int j = 3; j <= m - 2; j++) {
+      double d = (ORDER == 1) ? d1_row_int(x, sx, j) : d2_row_int(x, sx, j);
+      t = __ldg(g2 + j) * (d + a1 * t);
+      out[(j - 1) * so] = t;
+    }
+    t = __ldg(g2 + m - 1) * rm1 + __ldg(g3 + m - 1) * t;
+    out[(m - 2) * so] = t;
+    t = __ldg(g2 + m) * rm + __ldg(g3 + m) * t;
+  }
+  double sol = t;
+  out[(m - 1) * so] = scale * sol;
+  for (int j = m - 1; j >= 1; j--) {
+    sol = out[(j - 1) * so] + __ldg(g1 + j + 1) * sol;
+    out[(j - 1) * so] = scale * sol;
+  }
+}
+
+#undef CSS_X
+
+}  // namespace css

@@ -1,0 +1,62 @@
+"""Loader of the in-tree CUDA library libcss_b200.so (C ABI of
+include/css_b200.h).  There is no CPU fallback: if the library is missing or
+cannot be loaded, every entry point raises."""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBPATH = os.path.join(_HERE, "libcss_b200.so")
+_LIB = None
+
+dp = ctypes.POINTER(ctypes.c_double)
+
+
+class CssError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("css error %d: %s" % (code, msg))
+        self.code = code
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        if not os.path.exists(LIBPATH):
+            raise CssError(-1, "CUDA library %s not built (run __graft_entry__.build())" % LIBPATH)
+        L = ctypes.CDLL(LIBPATH)
+        L.css_last_error.restype = ctypes.c_char_p
+        L.css_create.argtypes = [ctypes.c_void_p, dp, ctypes.POINTER(ctypes.c_void_p)]
+        L.css_destroy.argtypes = [ctypes.c_void_p]
+        L.css_destroy.restype = None
+        L.css_upload_state.argtypes = [ctypes.c_void_p, dp]
+        L.css_download_state.argtypes = [ctypes.c_void_p, dp]
+        L.css_step_rk4.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.css_step_rk4_host.argtypes = [ctypes.c_void_p, dp, ctypes.c_double, ctypes.c_int]
+        L.css_rhs.argtypes = [ctypes.c_void_p, dp, dp, ctypes.c_int]
+        L.css_diffusion.argtypes = [ctypes.c_void_p, dp, dp, dp]
+        L.css_deriv.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, ctypes.c_int]
+        L.css_deriv_dev.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                    ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]
+        L.css_dbyd1_dt0.argtypes = [dp, dp, dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.css_compact_lines.argtypes = [dp, dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, dp, dp, dp, dp, ctypes.c_double, ctypes.c_double]
+        L.css_sync.argtypes = [ctypes.c_void_p]
+        L.css_state_device_ptr.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p),
+                                           ctypes.POINTER(ctypes.c_longlong)]
+        L.css_kernel_launches.argtypes = [ctypes.c_void_p]
+        L.css_kernel_launches.restype = ctypes.c_longlong
+        _LIB = L
+    return _LIB
+
+
+def check(rc):
+    if rc != 0:
+        raise CssError(rc, lib().css_last_error().decode())
+    return rc
+
+
+# exported symbols that include/css_b200.h declares
+EXPORTS = [
+    "css_last_error", "css_create", "css_destroy", "css_upload_state", "css_download_state", "css_step_rk4",
+    "css_step_rk4_host", "css_rhs", "css_diffusion", "css_deriv", "css_deriv_dev", "css_dbyd1_dt0",
+    "css_compact_lines", "css_sync", "css_state_device_ptr", "css_kernel_launches",
+]

@@ -1,0 +1,159 @@
+"""Host-side mirror of the reference's step / RHS / derivative interfaces on
+top of the C ABI.
+
+``Simulation`` plays the role of the Fortran driver's module state
+(vars0 of parallel_mpi.f90:41 plus the tables Setup builds): create it from
+parameters and radial profiles, upload an initial state, advance it with
+``step_rk4`` (Step_RK4, step_rk4.f90:339), or call ``rhs`` (RHS(call_num),
+rhs_mpi.f90:279), ``diffusion`` (Compute_Diffusion, diffusion.f90:70) and
+``deriv`` (Dbydr/Dbydt/Dbydp and the second derivatives) for one field.
+Arrays are numpy float64 of shape (nv, nr, nphi, nth), i.e. the Fortran
+vars(it, ip, ir, iv) in memory order.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import check, dp
+
+
+def _p(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(dp)
+
+
+class Simulation:
+    def __init__(self, params, profiles):
+        self.p = params.copy()
+        self.prof = np.ascontiguousarray(profiles, dtype=np.float64)
+        self.nv = 8 if self.p.magnetic else 5
+        self.shape = (self.nv, self.p.nr, self.p.nphi, self.p.nth)
+        h = ctypes.c_void_p()
+        check(_lib.lib().css_create(ctypes.byref(self.p), _p(self.prof), ctypes.byref(h)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().css_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # state ----------------------------------------------------------------
+    def upload(self, vars0):
+        v = np.ascontiguousarray(vars0, dtype=np.float64)
+        assert v.shape == self.shape, (v.shape, self.shape)
+        check(_lib.lib().css_upload_state(self.h, _p(v)))
+
+    def download(self):
+        out = np.empty(self.shape)
+        check(_lib.lib().css_download_state(self.h, _p(out)))
+        return out
+
+    def step_rk4(self, dt, nsteps=1):
+        check(_lib.lib().css_step_rk4(self.h, float(dt), int(nsteps)))
+
+    def step_host(self, vars0, dt, nsteps=1):
+        v = np.array(vars0, dtype=np.float64, order="C", copy=True)
+        check(_lib.lib().css_step_rk4_host(self.h, _p(v), float(dt), int(nsteps)))
+        return v
+
+    def sync(self):
+        check(_lib.lib().css_sync(self.h))
+
+    def device_state(self):
+        """(device pointer, element count) of the resident state."""
+        ptr = ctypes.c_void_p()
+        n = ctypes.c_longlong()
+        check(_lib.lib().css_state_device_ptr(self.h, ctypes.byref(ptr), ctypes.byref(n)))
+        return ptr.value, n.value
+
+    def launches(self):
+        return _lib.lib().css_kernel_launches(self.h)
+
+    # parity entry points ----------------------------------------------------
+    def rhs(self, vars1, call_num=1):
+        v = np.array(vars1, dtype=np.float64, order="C", copy=True)
+        dv = np.zeros_like(v)
+        check(_lib.lib().css_rhs(self.h, _p(v), _p(dv), int(call_num)))
+        return v, dv
+
+    def diffusion(self, vars1, avec=None):
+        v = np.array(vars1, dtype=np.float64, order="C", copy=True)
+        dv = np.zeros_like(v)
+        a = None if avec is None else np.ascontiguousarray(avec, dtype=np.float64)
+        check(_lib.lib().css_diffusion(self.h, _p(v), _p(a), _p(dv)))
+        return v, dv
+
+    def deriv(self, direction, order, x, bc_lo=None, bc_hi=None, bdry=1):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        out = np.zeros_like(x)
+        lo = None if bc_lo is None else np.ascontiguousarray(bc_lo, dtype=np.float64)
+        hi = None if bc_hi is None else np.ascontiguousarray(bc_hi, dtype=np.float64)
+        check(_lib.lib().css_deriv(self.h, int(direction), int(order), _p(x), _p(out), _p(lo), _p(hi), int(bdry)))
+        return out
+
+    def deriv_device(self, direction, order, x_ptr, out_ptr, bc_lo_ptr=None, bc_hi_ptr=None, bdry=1, stream=None):
+        check(_lib.lib().css_deriv_dev(self.h, int(direction), int(order), x_ptr, out_ptr, bc_lo_ptr, bc_hi_ptr,
+                                       int(bdry), stream))
+
+
+def dbyd1_dt0(x, bdat1, bdat2, ibc):
+    """Batched Dbyd1_dt0 (derivatives.f90:2296) over the last axis, on the GPU."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n1 = x.shape[-1]
+    lines = x.reshape(-1, n1)
+    nl = lines.shape[0]
+    out = np.zeros_like(lines)
+    b1 = np.ascontiguousarray(np.broadcast_to(np.asarray(bdat1, dtype=np.float64), (nl,)))
+    b2 = np.ascontiguousarray(np.broadcast_to(np.asarray(bdat2, dtype=np.float64), (nl,)))
+    check(_lib.lib().css_dbyd1_dt0(_p(lines), _p(out), _p(b1), _p(b2), n1, int(ibc), nl))
+    return out.reshape(x.shape)
+
+
+def compact_lines(x, order=1, lphys=True, rphys=True, bdry=1, bc_lo=None, bc_hi=None, halo_lo=None, halo_hi=None,
+                  dnum=1.0, scale=1.0):
+    """Independent compact-FD lines with explicit closures (css_compact_lines)."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[-1]
+    lines = x.reshape(-1, n)
+    nl = lines.shape[0]
+    out = np.zeros_like(lines)
+
+    def vec(a, k):
+        if a is None:
+            return None
+        return np.ascontiguousarray(np.broadcast_to(np.asarray(a, dtype=np.float64), (nl, k) if k > 1 else (nl,)))
+
+    check(_lib.lib().css_compact_lines(_p(lines), _p(out), n, nl, int(order), int(bool(lphys)), int(bool(rphys)),
+                                       int(bdry), _p(vec(bc_lo, 1)), _p(vec(bc_hi, 1)), _p(vec(halo_lo, 4)),
+                                       _p(vec(halo_hi, 4)), float(dnum), float(scale)))
+    return out.reshape(x.shape)
+
+
+def compact_fd6(dri, arr, b1, b2, ibc, dtype=0, darr=None):
+    """Drop-in for CSS-Python derivatives.py:32 compact_fd6 (dtype=0, the
+    whole-line form; the reference's dtype 1-3 closures do not converge).
+    For ibc 2/4 (3/4) the Neumann datum is darr[0] (darr[-1]) in the
+    reference's convention, f'(x_end)/dri.  Runs on the GPU."""
+    if dtype != 0:
+        raise ValueError("compact_fd6: only dtype=0 (whole line) is supported")
+    a = np.asarray(arr, dtype=np.float64)
+    n = a.shape[-1]
+    dli = float(n - 1)
+    drin = float(dri) * dli
+    lo = hi = 0.0
+    if darr is not None:
+        d = np.asarray(darr, dtype=np.float64)
+        if ibc in (2, 4):
+            lo = d[..., 0] / dli * drin
+        if ibc in (3, 4):
+            hi = d[..., -1] / dli * drin
+    return compact_lines(a, 1, True, True, int(ibc), lo, hi, dnum=drin, scale=drin)

@@ -153,9 +153,26 @@ int css_deriv_dev(css_ctx *ctx, int dir, int order, const double *x, double *dx,
 
 /* Batched 1D whole-line first derivative Dbyd1_dt0 (derivatives.f90:2296)
  * on nlines contiguous lines of n1 points, host pointers; bdat1/bdat2 per
- * line.  Equals CSS-Python derivatives.py:32 compact_fd6(dtype=0) / dri.  */
+ * line (may be NULL).  Returns d/dx in grid units, as the Fortran does.
+ * Equals CSS-Python compact_fd6(dtype=0)/dri except for ibc = 2, where the
+ * Fortran routine drops the last row's lower coefficient (its up2 is copied
+ * from an already zeroed up1, derivatives.f90:2355-2386) and this entry
+ * point reproduces that.                                                  */
 int css_dbyd1_dt0(const double *x, double *dxdy, const double *bdat1,
                   const double *bdat2, int n1, int ibc, int nlines);
+
+/* Independent compact-FD lines of n points (nlines, contiguous), order 1
+ * or 2, with explicit closures: lphys/rphys = 1 closes that end with the
+ * physical-boundary rows of bdry (datum bc_lo[l] / bc_hi[l]), 0 closes it
+ * with halo rows fed by halo_lo[4l..4l+3] (the four points below, farthest
+ * first) / halo_hi[4l..4l+3] (the four above, nearest first).  dx = scale *
+ * solution; dnum divides the Neumann datum (dri in Dbydr).  With both ends
+ * physical this is CSS-Python derivatives.py:32 compact_fd6(dtype=0).
+ * Host pointers.                                                          */
+int css_compact_lines(const double *x, double *dx, int n, int nlines, int order,
+                      int lphys, int rphys, int bdry, const double *bc_lo,
+                      const double *bc_hi, const double *halo_lo,
+                      const double *halo_hi, double dnum, double scale);
 
 /* Block until all work on the context stream is done. */
 int css_sync(css_ctx *ctx);
