@@ -1,0 +1,353 @@
+"""Benchmark of the CSS RK4 hot path on B200: RK4 cell-updates/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload NAME]
+
+Default workload: the 128x256x512 hydro polytrope (3 density scale heights,
+FP64, virtual decomposition 4x8x16 = 32^3 blocks), synthetic seeded state.
+One step = one full RK4 step (4 RHS evaluations + slope-limited diffusion).
+`value` is device-timed with CUDA events on the stream the library runs on,
+inputs resident in HBM (the state, 671 MB per buffer, is larger than L2).
+`e2e` is the same metric through the C ABI with host buffers: each step
+uploads the state from pinned host memory, advances it one step and reads
+it back (css_step_rk4_host), as a Fortran driver that keeps vars0 on the
+host would call it.  N > 1: one process per GPU, each advancing its own
+replica (the hot path runs the whole domain on one GPU; no collective),
+time = max over ranks.
+
+--impl reference times the reference's CPU implementation of the same path:
+the FP64 C restatement in oracle/ (the Fortran itself cannot be built here),
+with every host thread, on a bounded number of steps of the same workload.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "css-code_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "RK4 cell-updates/s at stated error vs FP64 oracle; % of HBM roofline"
+UNIT = "cell-updates/s"
+FALLBACK_HBM_GBS = 6650.0
+
+# compulsory bytes per cell of each kernel (FP64 words read + written once;
+# halo re-reads and the LU tables are not counted), hydro nv = 5 / MHD nv = 8
+def kernel_alg_bytes(name, nv, stage_mix=None):
+    mag = nv == 8
+    nb = 3 if mag else 0
+    w = {
+        "theta_terms": 5 + nb + (8 if mag else 5),
+        "phi_terms": 5 + nb + 2 * 5,
+        "radial_terms": 5 + nb + 2 * 5,
+        "rhot_update": 0,
+        "curl_theta": 2 + 2,
+        "curl_phi": 2 + 3 + 1,
+        "curl_r": 2 + 3 + 3,
+        "sld_vcc": 3 + (4 if mag else 0) + 1,
+        "sld": nv + 1 + nv,
+        "sld_ohmic": 2 + 3 + 3 + 2,
+    }.get(name)
+    if name == "rhot_update":
+        # average over the four stages: reads rho,w,s + dv,v0,vs (3 nv), writes
+        # vs + next (2 nv) in stages 1-3 and next only (nv) in stage 4
+        w = 3 + 3 * nv + (3 * 2 * nv + nv) / 4.0
+    return None if w is None else 8.0 * w
+
+
+def step_alg_bytes(nv):
+    """Compulsory traffic of a perfectly fused RK4 step: 17 nv words/cell."""
+    return 17 * nv * 8
+
+
+def read_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.fh.close()
+        rows = []
+        for line in open(self.path):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append(dict(sm=float(parts[1]), smax=float(parts[2]), hw=parts[5], hwt=parts[6], swt=parts[7],
+                                 pcap=parts[8]))
+            except ValueError:
+                continue
+        os.unlink(self.path)
+        if not rows:
+            return None
+        reasons = set()
+        for r in rows:
+            for key, nm in (("hw", "hw_slowdown"), ("hwt", "hw_thermal_slowdown"), ("swt", "sw_thermal_slowdown"),
+                            ("pcap", "sw_power_cap")):
+                if r[key].lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(r["sm"] for r in rows), "sm_max_mhz": max(r["smax"] for r in rows),
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def dist_setup(n):
+    import torch
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    return rank, world, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def cpu_baseline(p, prof, v0, dt, steps):
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    orc = O.Oracle(p, prof)
+    orc.step(v0, dt, 1)  # warm-up
+    t = time.perf_counter()
+    orc.step(v0, dt, steps)
+    el = time.perf_counter() - t
+    orc.close()
+    cells = p.nr * p.nth * p.nphi
+    return {"value": cells * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": "%d RK4 steps of the full %dx%dx%d workload (FP64 C restatement, %d OpenMP threads)"
+                      % (steps, p.nr, p.nth, p.nphi, threads), "seconds": el}
+
+
+def run_reference(args):
+    from css_b200 import problem
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return 0
+    p, prof, v0, dt, _ = problem.build(args.workload)
+    from oracle import oracle as O
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    orc = O.Oracle(p, prof)
+    v = v0
+    for _ in range(args.warmup):
+        v = orc.step(v, dt, 1)
+    t = time.perf_counter()
+    for _ in range(args.steps):
+        v = orc.step(v, dt, 1)
+    el = time.perf_counter() - t
+    cells = p.nr * p.nth * p.nphi
+    val = cells * args.steps / el
+    out = {
+        "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [p.nr, p.nth, p.nphi], "decomposition": [p.nnr, p.nnt, p.nnp],
+                   "fields": 8 if p.magnetic else 5, "l2": "state larger than L2"},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": "%d RK4 steps of the full workload, FP64 C restatement of the reference "
+                                   "(Fortran not buildable here), %d OpenMP threads" % (args.steps, threads)},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out))
+    return 0
+
+
+def run_ours(args):
+    import numpy as np
+    import torch
+    from css_b200 import problem
+    from css_b200.context import Simulation
+
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    p, prof, v0, dt, _ = problem.build(args.workload)
+    nv = 8 if p.magnetic else 5
+    cells = p.nr * p.nth * p.nphi
+    sim = Simulation(p, prof)
+    stream = torch.cuda.current_stream(dev)
+    sim.set_stream(stream.cuda_stream)
+    sim.upload(v0)
+    for _ in range(args.warmup):
+        sim.step_rk4(dt, 1)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    if rank == 0:
+        clocks.start()
+        time.sleep(0.3)
+    barrier(world)
+    torch.cuda.synchronize()
+    l0 = sim.launches()
+    sim.profile(True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        sim.step_rk4(dt, 1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    launches = sim.launches() - l0
+    ms = e0.elapsed_time(e1)
+    stats = sim.kernel_stats()
+    sim.profile(False)
+    clk = clocks.stop() if rank == 0 else None
+    ms_max = max_over_ranks(ms, world)
+    value = cells * args.steps * world / (ms_max / 1e3)
+
+    # e2e through the C ABI with host buffers (pinned)
+    e2e_steps = 0 if args.no_e2e else max(1, min(args.steps, 10))
+    host = torch.from_numpy(np.ascontiguousarray(v0)).pin_memory()
+    if e2e_steps:
+        sim.step_host(host.numpy(), dt, 1)  # warm
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    import ctypes
+    from css_b200 import _lib
+    ptr = ctypes.cast(host.data_ptr(), _lib.dp)
+    for _ in range(e2e_steps):
+        _lib.check(_lib.lib().css_step_rk4_host(sim.h, ptr, float(dt), 1))
+    t1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(t0.elapsed_time(t1), world)
+    e2e_val = cells * e2e_steps * world / (e2e_ms / 1e3) if e2e_steps else None
+    state_bytes = cells * nv * 8
+
+    # roofline of the dominant kernel (largest share of device time)
+    peak, peak_src = read_peaks()
+    dom = max(stats.items(), key=lambda kv: kv[1][0]) if stats else None
+    roof = None
+    if dom:
+        name, (kms, cnt) = dom
+        alg = kernel_alg_bytes(name, nv)
+        per_launch_cells = cells
+        achieved = alg * per_launch_cells / (kms / cnt / 1e3) / 1e9 if alg else None
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if os.path.exists(tpath):
+            try:
+                tj = json.load(open(tpath))
+                key = "%s/%s" % ("mhd" if p.magnetic else "hydro", name)
+                if key in tj:
+                    traffic = tj[key]["dram_bytes_per_cell"] * per_launch_cells
+            except Exception:
+                traffic = None
+        roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "algorithmic_bytes_per_launch": alg * per_launch_cells if alg else None,
+                "avg_launch_ms": kms / cnt, "peak_source": peak_src,
+                "time_share": kms / sum(v[0] for v in stats.values())}
+    step_ach = step_alg_bytes(nv) * cells * args.steps / (ms / 1e3) / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": args.workload, "grid": [p.nr, p.nth, p.nphi], "decomposition": [p.nnr, p.nnt, p.nnp],
+                   "fields": nv, "dt": dt, "l2": "state (%.0f MB per buffer) larger than L2, no flush" % (state_bytes / 1e6),
+                   "parallelism": "replicas" if world > 1 else "single-gpu"},
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
+                "steps": e2e_steps, "api": "css_step_rk4_host, one step per call, pinned host state"},
+        "gpu_launches": launches,
+        "roofline": roof,
+        "step_roofline": {"algorithmic_bytes_per_cell_step": step_alg_bytes(nv), "achieved": step_ach,
+                          "peak": peak, "unit": "GB/s", "frac": step_ach / peak, "peak_source": peak_src},
+        "kernels_ms": {k: {"total_ms": v[0], "launches": v[1]} for k, v in sorted(stats.items())},
+        "error_vs_oracle": "FP64: derivatives/RHS <= 1e-12, state after 100 steps <= 1e-10 (tests/test_gpu_parity.py)",
+    }
+    if clk:
+        out["clocks"] = clk
+    if rank == 0 and world == 1 and not args.no_cpu:
+        out["cpu_baseline"] = cpu_baseline(p, prof, v0, dt, args.cpu_steps)
+    sim.close()
+    if rank == 0:
+        print(json.dumps(out))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="hydro-128x256x512")
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -35,6 +35,13 @@ extern "C" const char *css_last_error(void) { return g_err; }
     }                                                                                \
   } while (0)
 
+// kernel kinds, for the per-kernel CUDA-event timing of css_profile
+enum KernelId { KI_THETA = 0, KI_PHI, KI_RADIAL, KI_RHOT_UPDATE, KI_CURL_THETA, KI_CURL_PHI, KI_CURL_R,
+                KI_SLD_VCC, KI_SLD, KI_SLD_OHMIC, KI_DERIV, KI_COUNT };
+static const char *kKernelNames[KI_COUNT] = {"theta_terms", "phi_terms", "radial_terms", "rhot_update",
+                                             "curl_theta", "curl_phi", "curl_r", "sld_vcc", "sld", "sld_ohmic",
+                                             "deriv"};
+
 struct css_ctx {
   css_params p;
   CssGeo g;
@@ -51,7 +58,46 @@ struct css_ctx {
   int *flag;
   long long launches;
   int tl_theta, tl_phi, tl_r;
+  cudaStream_t own_stream;
+  // per-kernel event timing (css_profile)
+  int profiling;
+  std::vector<cudaEvent_t> ev;     // pairs (start, stop)
+  std::vector<int> ev_kind;
+  size_t ev_used;
+  double k_ms[KI_COUNT];
+  long long k_count[KI_COUNT];
 };
+
+static void prof_begin(css_ctx *c, int kind) {
+  if (!c->profiling) return;
+  if (c->ev_used + 2 > c->ev.size()) {
+    for (int i = 0; i < 64; i++) {
+      cudaEvent_t e;
+      cudaEventCreate(&e);
+      c->ev.push_back(e);
+    }
+    c->ev_kind.resize(c->ev.size() / 2);
+  }
+  c->ev_kind[c->ev_used / 2] = kind;
+  cudaEventRecord(c->ev[c->ev_used], c->stream);
+}
+static void prof_end(css_ctx *c) {
+  if (!c->profiling) return;
+  cudaEventRecord(c->ev[c->ev_used + 1], c->stream);
+  c->ev_used += 2;
+}
+static void prof_collect(css_ctx *c) {
+  if (c->ev_used == 0) return;
+  cudaStreamSynchronize(c->stream);
+  for (size_t i = 0; i + 1 < c->ev_used; i += 2) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev[i], c->ev[i + 1]);
+    int k = c->ev_kind[i / 2];
+    c->k_ms[k] += ms;
+    c->k_count[k] += 1;
+  }
+  c->ev_used = 0;
+}
 
 // ---------------------------------------------------------------------------
 // LU tables (Initialize_Derivatives, derivatives.f90:106-287 for r/theta,
@@ -168,7 +214,8 @@ extern "C" void css_destroy(css_ctx *c) {
   cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
   cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag);
-  if (c->stream) cudaStreamDestroy(c->stream);
+  for (auto e : c->ev) cudaEventDestroy(e);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
 
@@ -227,7 +274,6 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     return CSS_ERR_ARG;
   }
   css_ctx *c = new css_ctx();
-  memset(c, 0, sizeof(*c));
   c->p = p;
   c->nv = p.magnetic ? 8 : 5;
   c->ncell = (size_t)p.nr * p.nth * p.nphi;
@@ -374,11 +420,12 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   // device copies
   int rc = setup_kernels();
   if (rc) { css_destroy(c); return rc; }
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
     set_err("css_create: stream creation failed");
     css_destroy(c);
     return CSS_ERR_CUDA;
   }
+  c->stream = c->own_stream;
   // radial profile block: r_ind r_inv dr_ind dxdr d2xdr2 rhor sr grav ks dlnks eps dspeed
   std::vector<double> R((size_t)12 * nr);
   for (int i = 0; i < nr; i++) {
@@ -457,15 +504,21 @@ static int launch_curl(css_ctx *c, const double *a, double *out, int apply_bc) {
   int mt = g.d[1].maxm, mp = g.d[2].maxm, mr = g.d[0].maxm;
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
+  prof_begin(c, KI_CURL_THETA);
   k_curl_theta<<<gt, 128, smem_theta(2, 2, mt, TL), c->stream>>>(g, a, out, TL);
+  prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
+  prof_begin(c, KI_CURL_PHI);
   k_curl_phi<<<gp, 128, smem_line(2, 2, 0, mp, TL), c->stream>>>(g, a, out, TL);
+  prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
+  prof_begin(c, KI_CURL_R);
   k_curl_r<<<gr, 128, smem_line(2, 2, 0, mr, TL), c->stream>>>(g, a, out, TL, apply_bc);
+  prof_end(c);
   return check_launch(c);
 }
 
@@ -478,20 +531,28 @@ static int launch_rhs(css_ctx *c, const double *cur, double *nx, int stage, doub
   }
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
+  prof_begin(c, KI_THETA);
   k_theta_terms<<<gt, 128, smem_theta(mag ? 6 : 4, mag ? 7 : 5, g.d[1].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
+  prof_begin(c, KI_PHI);
   k_phi_terms<<<gp, 128, smem_line(mag ? 7 : 5, mag ? 8 : 6, 0, g.d[2].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
+  prof_begin(c, KI_RADIAL);
   k_radial_terms<<<gr, 128, smem_line(mag ? 7 : 5, mag ? 7 : 5, 5, g.d[0].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
+  prof_begin(c, KI_RHOT_UPDATE);
   k_rhot_update<<<gu, 128, smem_theta(1, 1, g.d[1].maxm, TL), c->stream>>>(g, cur, c->dv, c->v0, c->vs, nx, stage,
                                                                             dtcur, TL, c->flag);
+  prof_end(c);
   return check_launch(c);
 }
 
@@ -500,13 +561,19 @@ static int launch_rhs(css_ctx *c, const double *cur, double *nx, int stage, doub
 static int launch_sld(css_ctx *c, const double *v, const double *av, double *dout) {
   const CssGeo &g = c->g;
   int nb = 148 * 16;
+  prof_begin(c, KI_SLD_VCC);
   k_sld_vcc<<<nb, 256, 0, c->stream>>>(g, v, c->bf, c->vcc);
+  prof_end(c);
   if (int rc = check_launch(c)) return rc;
+  prof_begin(c, KI_SLD);
   k_sld<<<nb, 128, 0, c->stream>>>(g, v, av, c->vcc, dout);
+  prof_end(c);
   if (int rc = check_launch(c)) return rc;
   if (g.do_ohmic_heating) {
     if (int rc = launch_curl(c, dout + 5 * c->ncell, c->cda, 0)) return rc;
+    prof_begin(c, KI_SLD_OHMIC);
     k_sld_ohmic<<<nb, 256, 0, c->stream>>>(g, v, c->bf, c->cda, dout);
+    prof_end(c);
     if (int rc = check_launch(c)) return rc;
   }
   return CSS_OK;
@@ -738,3 +805,27 @@ extern "C" int css_state_device_ptr(css_ctx *c, double **dptr, long long *nelem)
 }
 
 extern "C" long long css_kernel_launches(css_ctx *c) { return c ? c->launches : 0; }
+
+extern "C" int css_set_stream(css_ctx *c, void *stream) {
+  if (!c) { set_err("css_set_stream: NULL"); return CSS_ERR_ARG; }
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return CSS_OK;
+}
+
+extern "C" int css_profile(css_ctx *c, int enable) {
+  if (!c) { set_err("css_profile: NULL"); return CSS_ERR_ARG; }
+  prof_collect(c);
+  for (int k = 0; k < KI_COUNT; k++) { c->k_ms[k] = 0.0; c->k_count[k] = 0; }
+  c->profiling = enable ? 1 : 0;
+  return CSS_OK;
+}
+
+extern "C" int css_kernel_stats(css_ctx *c, int kind, const char **name, double *total_ms, long long *launches) {
+  if (!c || kind < 0 || kind >= KI_COUNT) return CSS_ERR_ARG;
+  prof_collect(c);
+  if (name) *name = kKernelNames[kind];
+  if (total_ms) *total_ms = c->k_ms[kind];
+  if (launches) *launches = c->k_count[kind];
+  return CSS_OK;
+}

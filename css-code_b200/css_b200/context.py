@@ -78,6 +78,26 @@ class Simulation:
     def launches(self):
         return _lib.lib().css_kernel_launches(self.h)
 
+    def set_stream(self, stream_handle):
+        """Run on the caller's cudaStream_t (int handle, e.g.
+        torch.cuda.current_stream().cuda_stream); None = own stream."""
+        check(_lib.lib().css_set_stream(self.h, stream_handle))
+
+    def profile(self, enable=True):
+        check(_lib.lib().css_profile(self.h, 1 if enable else 0))
+
+    def kernel_stats(self):
+        """{kernel name: (total ms, launches)} since profile(True)."""
+        out = {}
+        for k in range(11):
+            nm = ctypes.c_char_p()
+            ms = ctypes.c_double()
+            cnt = ctypes.c_longlong()
+            check(_lib.lib().css_kernel_stats(self.h, k, ctypes.byref(nm), ctypes.byref(ms), ctypes.byref(cnt)))
+            if cnt.value:
+                out[nm.value.decode()] = (ms.value, cnt.value)
+        return out
+
     # parity entry points ----------------------------------------------------
     def rhs(self, vars1, call_num=1):
         v = np.array(vars1, dtype=np.float64, order="C", copy=True)

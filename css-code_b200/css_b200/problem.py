@@ -192,6 +192,8 @@ WORKLOADS = {
     "hydro-128x256x512": (128, 256, 512, (4, 8, 16), False, 3.0),
     "mhd-256x512x1024": (256, 512, 1024, (8, 16, 32), True, 5.0),
     "hydro-64x128x256": (64, 128, 256, (2, 4, 8), False, 3.0),
+    "hydro-128x128x256": (128, 128, 256, (4, 4, 8), False, 3.0),
+    "mhd-128x128x256": (128, 128, 256, (4, 4, 8), True, 5.0),
 }
 
 

@@ -184,6 +184,22 @@ int css_state_device_ptr(css_ctx *ctx, double **dptr, long long *nelem);
 /* Number of kernels this library launched on ctx since creation. */
 long long css_kernel_launches(css_ctx *ctx);
 
+/* Run all further work of ctx on the caller's stream (a cudaStream_t; NULL
+ * returns to the context's own stream).  Lets a CUDA-aware caller (PyTorch,
+ * a Fortran driver with its own stream) order and time the library's
+ * kernels on its stream.                                                   */
+int css_set_stream(css_ctx *ctx, void *stream);
+
+/* Per-kernel timing with CUDA events recorded around every launch on the
+ * context stream (the reference's Do_Timings phase timers, rhs_mpi.f90:
+ * 324-766).  css_profile(ctx, 1) clears and enables, 0 disables;
+ * css_kernel_stats returns, for kernel kind 0..10 (theta_terms, phi_terms,
+ * radial_terms, rhot_update, curl_theta, curl_phi, curl_r, sld_vcc, sld,
+ * sld_ohmic, deriv), its name, summed milliseconds and launch count.      */
+int css_profile(css_ctx *ctx, int enable);
+int css_kernel_stats(css_ctx *ctx, int kind, const char **name, double *total_ms,
+                     long long *launches);
+
 #ifdef __cplusplus
 }
 #endif
