@@ -49,12 +49,14 @@ struct css_ctx {
   size_t ncell;
   cudaStream_t stream;
   // device buffers
-  double *tab, *prof, *theta_prof;
+  double *tab, *prof, *theta_prof, *sld_geo;
   int *rblk;
   double *v0, *vA, *vB, *dv, *vs;  // state, stage ping-pong, tendency, RK accumulator
   double *bf;                       // B = curl A (MHD)
   double *vcc;                      // SLD speed^2
   double *cda;                      // curl of the A-tendency (MHD ohmic heating)
+  double *tbuf;                     // temperature of the current stage input
+  int mt[3];                        // compile-time block length per direction (0 = generic)
   int *flag;
   long long launches;
   int tl_theta, tl_phi, tl_r;
@@ -211,34 +213,52 @@ static int pick_tl(int kind, int nh, int nd, int na, int m) {
 
 extern "C" void css_destroy(css_ctx *c) {
   if (!c) return;
-  cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk);
+  cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
-  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag);
+  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf);
   for (auto e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
 
+template <int MT>
+static int setup_mt() {
+  int mx = 200 * 1024;
+  CUDA_TRY(cudaFuncSetAttribute(k_theta_terms<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_phi_terms<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_radial_terms<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_rhot_update<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_theta<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_phi<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_r<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<1, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<2, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<1, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<2, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<1, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<2, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  return CSS_OK;
+}
+
 static int setup_kernels() {
   static bool done = false;
   if (done) return CSS_OK;
-  int mx = 200 * 1024;
-  CUDA_TRY(cudaFuncSetAttribute(k_theta_terms, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_phi_terms, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_radial_terms, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_rhot_update, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_theta, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_phi, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_r, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  if (int rc = setup_mt<0>()) return rc;
+  if (int rc = setup_mt<16>()) return rc;
+  if (int rc = setup_mt<32>()) return rc;
   done = true;
   return CSS_OK;
 }
+
+// launch KERNEL<MT> with MT = c->mt[DIR] chosen at run time
+#define LAUNCH_MT(DIR, KERNEL, GRID, SMEM, ...)                                          \
+  do {                                                                                    \
+    switch (c->mt[DIR]) {                                                                 \
+      case 16: KERNEL<16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;           \
+      case 32: KERNEL<32><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;           \
+      default: KERNEL<0><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;            \
+    }                                                                                     \
+  } while (0)
 
 extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **out) {
   if (!out) { set_err("css_create: NULL out"); return CSS_ERR_ARG; }
@@ -442,6 +462,35 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     R[10 * nr + i] = P[CSS_PROF_EPS * nr + i];
     R[11 * nr + i] = dspeed[i];
   }
+  // SLD geometry tables (diffusion.f90:806-849, :1196-1247, :1316-1351),
+  // the same expressions as the reference evaluates per rank
+  std::vector<double> SG((size_t)5 * nth + 4 * nr);
+  {
+    const double *dr = &P[CSS_PROF_DR * nr];
+    for (int it = 0; it < nth; it++) {
+      double sphl, cphl, sphh, cphh;
+      if (it == 0) { sphl = fabs(sin(theta[0] - 0.5 * dth)); cphl = cos(theta[0] - 0.5 * dth); }
+      else { sphl = sin(0.5 * (theta[it] + theta[it - 1])); cphl = cos(0.5 * (theta[it] + theta[it - 1])); }
+      if (it == nth - 1) { sphh = sin(theta[it] + 0.5 * dth); cphh = cos(theta[it] + 0.5 * dth); }
+      else { sphh = sin(0.5 * (theta[it] + theta[it + 1])); cphh = cos(0.5 * (theta[it] + theta[it + 1])); }
+      double rt, st, ct;
+      if (it == 0) { rt = theta[0] - 0.5 * dth; st = cos(rt); }
+      else { rt = 0.5 * (theta[it] + theta[it - 1]); st = cos(rt); }
+      if (it == nth - 1) { ct = theta[it] + 0.5 * dth; rt = ct - rt; ct = cos(ct); }
+      else { ct = 0.5 * (theta[it + 1] + theta[it]); rt = ct - rt; ct = cos(ct); }
+      SG[it] = sphl; SG[nth + it] = cphl; SG[2 * nth + it] = sphh; SG[3 * nth + it] = cphh;
+      SG[4 * nth + it] = rt / (st - ct);
+    }
+    double *R4 = &SG[5 * (size_t)nth];
+    for (int ir = 0; ir < nr; ir++) {
+      double rlo = (ir == 0) ? r_ind[0] - 0.5 * dr[0] : 0.5 * (r_ind[ir] + r_ind[ir - 1]);
+      double rhi = (ir == nr - 1) ? r_ind[nr - 1] + 0.5 * dr[nr - 1] : 0.5 * (r_ind[ir + 1] + r_ind[ir]);
+      R4[ir] = 3.0 / (rhi * rhi * rhi - rlo * rlo * rlo);
+      R4[nr + ir] = 1.5 * (rhi * rhi - rlo * rlo) / (rhi * rhi * rhi - rlo * rlo * rlo);
+      R4[2 * nr + ir] = rlo * rlo;
+      R4[3 * nr + ir] = rhi * rhi;
+    }
+  }
   std::vector<double> TH((size_t)3 * nth);
   for (int i = 0; i < nth; i++) { TH[i] = sines[i]; TH[nth + i] = cosines[i]; TH[2 * nth + i] = theta[i]; }
 #define ALLOC(ptr, bytes)                                                                \
@@ -455,15 +504,18 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   ALLOC(c->tab, T.size() * 8);
   ALLOC(c->prof, R.size() * 8);
   ALLOC(c->theta_prof, TH.size() * 8);
+  ALLOC(c->sld_geo, SG.size() * 8);
   ALLOC(c->rblk, nr * sizeof(int));
   size_t sb = c->ncell * c->nv * sizeof(double);
   ALLOC(c->v0, sb); ALLOC(c->vA, sb); ALLOC(c->vB, sb); ALLOC(c->dv, sb); ALLOC(c->vs, sb);
   ALLOC(c->vcc, c->ncell * sizeof(double));
+  ALLOC(c->tbuf, c->ncell * sizeof(double));
   if (p.magnetic) { ALLOC(c->bf, 3 * c->ncell * sizeof(double)); ALLOC(c->cda, 3 * c->ncell * sizeof(double)); }
   ALLOC(c->flag, sizeof(int));
   cudaMemcpy(c->tab, T.data(), T.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->prof, R.data(), R.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->theta_prof, TH.data(), TH.size() * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->sld_geo, SG.data(), SG.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->rblk, rblk.data(), nr * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemset(c->flag, 0, sizeof(int));
   cudaMemset(c->vs, 0, sb);
@@ -472,6 +524,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   g.d2xdr2 = c->prof + 4 * nr; g.rhor = c->prof + 5 * nr; g.sr = c->prof + 6 * nr; g.grav = c->prof + 7 * nr;
   g.ks = c->prof + 8 * nr; g.dlnks = c->prof + 9 * nr; g.eps = c->prof + 10 * nr; g.dspeed = c->prof + 11 * nr;
   g.sines = c->theta_prof; g.cosines = c->theta_prof + nth; g.theta = c->theta_prof + 2 * nth;
+  g.sld_th = c->sld_geo; g.sld_r = c->sld_geo + 5 * (size_t)nth;
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     set_err("css_create: %s", cudaGetErrorString(e));
@@ -482,6 +535,11 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   c->tl_theta = pick_tl(0, mag ? 6 : 4, mag ? 7 : 5, 0, g.d[1].maxm);
   c->tl_phi = pick_tl(1, mag ? 7 : 5, mag ? 8 : 6, 0, g.d[2].maxm);
   c->tl_r = pick_tl(1, mag ? 7 : 5, mag ? 7 : 5, 5, g.d[0].maxm);
+  for (int d = 0; d < 3; d++) {
+    int m0 = g.d[d].size[0], same = 1;
+    for (int b = 1; b < g.d[d].nb; b++) same &= (g.d[d].size[b] == m0);
+    c->mt[d] = (same && (m0 == 16 || m0 == 32)) ? m0 : 0;
+  }
   *out = c;
   return CSS_OK;
 }
@@ -505,19 +563,19 @@ static int launch_curl(css_ctx *c, const double *a, double *out, int apply_bc) {
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_CURL_THETA);
-  k_curl_theta<<<gt, 128, smem_theta(2, 2, mt, TL), c->stream>>>(g, a, out, TL);
+  LAUNCH_MT(1, k_curl_theta, gt, smem_theta(2, 2, mt, TL), g, a, out, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
   prof_begin(c, KI_CURL_PHI);
-  k_curl_phi<<<gp, 128, smem_line(2, 2, 0, mp, TL), c->stream>>>(g, a, out, TL);
+  LAUNCH_MT(2, k_curl_phi, gp, smem_line(2, 2, 0, mp, TL), g, a, out, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_CURL_R);
-  k_curl_r<<<gr, 128, smem_line(2, 2, 0, mr, TL), c->stream>>>(g, a, out, TL, apply_bc);
+  LAUNCH_MT(0, k_curl_r, gr, smem_line(2, 2, 0, mr, TL), g, a, out, TL, apply_bc);
   prof_end(c);
   return check_launch(c);
 }
@@ -532,26 +590,29 @@ static int launch_rhs(css_ctx *c, const double *cur, double *nx, int stage, doub
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_THETA);
-  k_theta_terms<<<gt, 128, smem_theta(mag ? 6 : 4, mag ? 7 : 5, g.d[1].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  LAUNCH_MT(1, k_theta_terms, gt, smem_theta(mag ? 6 : 4, mag ? 7 : 5, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+            TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
   prof_begin(c, KI_PHI);
-  k_phi_terms<<<gp, 128, smem_line(mag ? 7 : 5, mag ? 8 : 6, 0, g.d[2].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  LAUNCH_MT(2, k_phi_terms, gp, smem_line(mag ? 7 : 5, mag ? 8 : 6, 0, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+            TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_RADIAL);
-  k_radial_terms<<<gr, 128, smem_line(mag ? 7 : 5, mag ? 7 : 5, 5, g.d[0].maxm, TL), c->stream>>>(g, cur, c->bf, c->dv, TL);
+  LAUNCH_MT(0, k_radial_terms, gr, smem_line(mag ? 7 : 5, mag ? 7 : 5, 5, g.d[0].maxm, TL), g, cur, c->bf, c->dv,
+            c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_RHOT_UPDATE);
-  k_rhot_update<<<gu, 128, smem_theta(1, 1, g.d[1].maxm, TL), c->stream>>>(g, cur, c->dv, c->v0, c->vs, nx, stage,
-                                                                            dtcur, TL, c->flag);
+  LAUNCH_MT(1, k_rhot_update, gu, smem_theta(1, 1, g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf,
+            stage, dtcur, TL, c->flag);
   prof_end(c);
   return check_launch(c);
 }
@@ -566,7 +627,8 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   prof_begin(c, KI_SLD);
-  k_sld<<<nb, 128, 0, c->stream>>>(g, v, av, c->vcc, dout);
+  dim3 gs((g.nth + SLD_TT - 1) / SLD_TT, (g.nphi + SLD_TP - 1) / SLD_TP, (g.nr + SLD_RC - 1) / SLD_RC);
+  k_sld<<<gs, SLD_TT * SLD_TP, 0, c->stream>>>(g, v, av, c->vcc, dout);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   if (g.do_ohmic_heating) {
@@ -680,20 +742,20 @@ extern "C" int css_deriv_dev(css_ctx *c, int dir, int order, const double *x, do
     int TL = c->tl_theta;
     dim3 gr(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
     size_t sm = smem_theta(1, 1, g.d[1].maxm, TL);
-    if (order == 1) k_deriv_theta<1><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
-    else k_deriv_theta<2><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
+    if (order == 1) k_deriv_theta<1, 0><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
+    else k_deriv_theta<2, 0><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
   } else if (dir == 2) {
     int TL = c->tl_phi;
     dim3 gr(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
     size_t sm = smem_line(1, 1, 0, g.d[2].maxm, TL);
-    if (order == 1) k_deriv_phi<1><<<gr, 128, sm, st>>>(g, x, dx, TL);
-    else k_deriv_phi<2><<<gr, 128, sm, st>>>(g, x, dx, TL);
+    if (order == 1) k_deriv_phi<1, 0><<<gr, 128, sm, st>>>(g, x, dx, TL);
+    else k_deriv_phi<2, 0><<<gr, 128, sm, st>>>(g, x, dx, TL);
   } else {
     int TL = c->tl_r;
     dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
     size_t sm = smem_line(1, 1, 0, g.d[0].maxm, TL);
-    if (order == 1) k_deriv_r<1><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
-    else k_deriv_r<2><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
+    if (order == 1) k_deriv_r<1, 0><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
+    else k_deriv_r<2, 0><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
   }
   return check_launch(c);
 }

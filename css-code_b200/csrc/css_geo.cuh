@@ -31,6 +31,11 @@ struct CssGeo {
   const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
   // theta profiles (length nth)
   const double *sines, *cosines, *theta;
+  // SLD cell geometry (diffusion.f90:806-849, :1196-1247, :1316-1351):
+  // per theta: sin/cos of the lower and upper faces and the phi geometry
+  // factor; per r: 3/(r+^3 - r-^3), the volume-averaged 1/r factor, r-^2, r+^2
+  const double *sld_th;  // [5][nth]: sphl, cphl, sphh, cphh, geom
+  const double *sld_r;   // [4][nr]:  t3, rfac, rlo^2, rhi^2
   // constants (Initialize_Physics, rhs_mpi.f90:63-75)
   double gamma, gamm1, cp, cv, invcv, invtconst, pconst, invpconst;
   double omega0, t0, damping_time, lumr1, lumr2, r1, r2, dth, dphi, xi_cs;

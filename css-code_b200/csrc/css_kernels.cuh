@@ -94,8 +94,10 @@ __device__ __forceinline__ void load_r_tile(const CssGeo &g, const double *__res
 // grid: x = theta block * nchunk + phi chunk, y = r.  cur = stage input
 // (vars1), B = curl A (MHD) in bf, dv = dvars1 (written, not read).
 // ---------------------------------------------------------------------------
+template <int MT>
 __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__restrict__ cur,
-                                                     const double *__restrict__ bf, double *__restrict__ dv, int TL) {
+                                                     const double *__restrict__ bf, double *__restrict__ dv,
+                                                     double *__restrict__ tbuf, int TL) {
   extern __shared__ double sm[];
   const int nchunk = (g.nphi + TL - 1) / TL;
   const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
@@ -134,10 +136,10 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
       if (D.rphys[bt]) hi = -(g.cosines[g.nth - 1] / g.sines[g.nth - 1]) * x[m - 1];
     }
     if (k == 4)
-      line_solve<2>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 2, bdry), g.tstride, dnum_d2_theta(g, ir),
+      solve<2, MT>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 2, bdry), g.tstride, dnum_d2_theta(g, ir),
                     D.dnum[bt] * D.dnum[bt], 0, o, 1);
     else
-      line_solve<1>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, D.dnum[bt], D.dnum[bt], 0, o, 1);
+      solve<1, MT>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, D.dnum[bt], D.dnum[bt], 0, o, 1);
   }
   __syncthreads();
   const double rv = g.r_ind[ir], epsr = g.eps[ir];
@@ -171,6 +173,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
     w1 = ol[(size_t)2 * TL * SO] * ri;
     du = du - w * w1;
     double t = temp_of(g, rho, s);
+    tbuf[id] = t;  // the stage's temperature, read by the later kernels
     double invrho = 1.0 / rho;
     double ds;
     if (fabs(epsr) > 0.0) ds = epsr * invrho / t;
@@ -219,8 +222,10 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
 // Phi_Terms (rhs_mpi.f90:1032-1261).  grid: x = phi block * nchunk + theta
 // chunk, y = r.
 // ---------------------------------------------------------------------------
+template <int MT>
 __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__restrict__ cur,
-                                                   const double *__restrict__ bf, double *__restrict__ dv, int TL) {
+                                                   const double *__restrict__ bf, double *__restrict__ dv,
+                                                   const double *__restrict__ tbuf, int TL) {
   extern __shared__ double sm[];
   const int nchunk = (g.nth + TL - 1) / TL;
   const int bp = blockIdx.x / nchunk, tb = (blockIdx.x - bp * nchunk) * TL;
@@ -246,10 +251,10 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__res
     const double *x = H + (size_t)hk * (m + 8) * SR + 4 * SR + l;
     double *o = O + (size_t)k * m * SR + l;
     if (k == 5)
-      line_solve<2>(x, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 2, 0), g.tstride, D.dnum[bp], D.dnum[bp] * D.dnum[bp], 1,
+      solve<2, MT>(x, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 2, 0), g.tstride, D.dnum[bp], D.dnum[bp] * D.dnum[bp], 1,
                     o, SR);
     else
-      line_solve<1>(x, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, D.dnum[bp], D.dnum[bp], 1, o, SR);
+      solve<1, MT>(x, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, D.dnum[bp], D.dnum[bp], 1, o, SR);
   }
   __syncthreads();
   const double ri = g.r_inv[ir];
@@ -260,12 +265,12 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__res
     size_t id = css_idx(g, it, ip, ir);
     const double *hl = H + (size_t)(j + 4) * SR + l;
     const size_t HS = (size_t)(m + 8) * SR;
-    double rho = hl[0], v = hl[HS], s = hl[4 * HS];
+    double rho = hl[0], v = hl[HS];
     const double *ol = O + (size_t)j * SR + l;
     const size_t OS = (size_t)m * SR;
     double cscth = 1.0 / g.sines[it];
     double oors = ri * cscth;
-    double t = temp_of(g, rho, s), oorho = 1.0 / rho;
+    double t = __ldg(tbuf + id), oorho = 1.0 / rho;
     double w1 = ol[0] * oors;
     double drho = dv[id];
     double dvv = dv[2 * n + id];
@@ -310,8 +315,10 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__res
 // Radial_Terms (rhs_mpi.f90:1264-1519) + Density_Terms_Radial (:1710-1855)
 // grid: x = r block * nchunk + theta chunk, y = phi.
 // ---------------------------------------------------------------------------
+template <int MT>
 __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__restrict__ cur,
-                                                      const double *__restrict__ bf, double *__restrict__ dv, int TL) {
+                                                      const double *__restrict__ bf, double *__restrict__ dv,
+                                                      const double *__restrict__ tbuf, int TL) {
   extern __shared__ double sm[];
   const int nchunk = (g.nth + TL - 1) / TL;
   const int br = blockIdx.x / nchunk, tb = (blockIdx.x - br * nchunk) * TL;
@@ -354,10 +361,10 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
       hi = g.s_flux_hi;
     }
     if (k == 4)
-      line_solve<2>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 2, bdry), g.tstride, D.dnum[br],
+      solve<2, MT>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 2, bdry), g.tstride, D.dnum[br],
                     D.dnum[br] * D.dnum[br], 0, o, SR);
     else
-      line_solve<1>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, D.dnum[br], D.dnum[br], 0, o,
+      solve<1, MT>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, D.dnum[br], D.dnum[br], 0, o,
                     SR);
   }
   __syncthreads();
@@ -368,10 +375,10 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
     if (it >= g.nth) continue;
     size_t id = css_idx(g, it, ip, ir);
     const double *hl = H + (size_t)(j + 4) * SR + l;
-    double u = hl[2 * HS], s = hl[3 * HS], rho = hl[4 * HS];
+    double u = hl[2 * HS], rho = hl[4 * HS];
     const double *ol = O + (size_t)j * SR + l;
     double w3 = g.dxdr[ir];
-    double t = temp_of(g, rho, s), invrho = 1.0 / rho;
+    double t = __ldg(tbuf + id), invrho = 1.0 / rho;
     double w1 = ol[0];
     if (nu) w1 = w1 * w3;
     double dw = dv[n + id];
@@ -429,20 +436,20 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
     const double *x = H + 4 * HS + 4 * SR + l;  // rho
     double lo = 0.0, hi = 0.0;
     if (D.lphys[br]) {
-      double rho = x[0], t = temp_of(g, rho, H[3 * HS + 4 * SR + l]);
+      double rho = x[0], t = __ldg(tbuf + css_idx(g, tb + l, ip, r0));
       double du = A[3 * OS + l];
       if (g.lbcr_rho == 2 || g.lbcr_rho == 4) lo = du * rho * g.invpconst / t;
       else lo = rho;
       if (nu) lo = lo / g.dxdr[0];
     } else if (D.rphys[br]) {
-      double rho = x[(m - 1) * SR], t = temp_of(g, rho, H[3 * HS + (m + 3) * SR + l]);
+      double rho = x[(m - 1) * SR], t = __ldg(tbuf + css_idx(g, tb + l, ip, r0 + m - 1));
       double du = A[3 * OS + (size_t)(m - 1) * SR + l];
       if (g.lbcr_rho == 3 || g.lbcr_rho == 4) hi = du * rho * g.invpconst / t;
       else hi = rho;
       if (nu) hi = hi / g.dxdr[nr - 1];
     }
     int bdry = g.ibcr[1];
-    line_solve<1>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, D.dnum[br], D.dnum[br], 0,
+    solve<1, MT>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, D.dnum[br], D.dnum[br], 0,
                   O + l, SR);
   }
   __syncthreads();
@@ -452,8 +459,8 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
     if (it >= g.nth) continue;
     size_t id = css_idx(g, it, ip, ir);
     const double *hl = H + (size_t)(j + 4) * SR + l;
-    double u = hl[2 * HS], s = hl[3 * HS], rho = hl[4 * HS];
-    double t = temp_of(g, rho, s), invrho = 1.0 / rho;
+    double u = hl[2 * HS], rho = hl[4 * HS];
+    double t = __ldg(tbuf + id), invrho = 1.0 / rho;
     const double *al = A + (size_t)j * SR + l;
     double w1 = O[(size_t)j * SR + l];
     if (nu) w1 = w1 * g.dxdr[ir];
@@ -482,9 +489,11 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
 //   stage 2,3: vs = vs + dv/3;            nx = v0 + dtcur*dv
 //   stage 4: vs = vs + dv/6;              nx = v0 + dtcur*vs  (nx may be v0)
 // ---------------------------------------------------------------------------
+template <int MT>
 __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__restrict__ cur,
                                                      double *__restrict__ dv, const double *v0, double *vs, double *nx,
-                                                     int stage, double dtcur, int TL, int *flag) {
+                                                     const double *__restrict__ tbuf, int stage, double dtcur, int TL,
+                                                     int *flag) {
   extern __shared__ double sm[];
   const int nchunk = (g.nphi + TL - 1) / TL;
   const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
@@ -505,15 +514,15 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
     double lo = 0.0, hi = 0.0;
     if (D.lphys[bt]) {  // rhs_mpi.f90:1553-1555: make dw = 0 on the wall
       size_t id = css_idx(g, t0, pb + l, ir);
-      double rho = x[0], t = temp_of(g, rho, __ldg(cur + 4 * n + id));
+      double rho = x[0], t = __ldg(tbuf + id);
       lo = rvv * dv[n + id] * rho / t;
     } else if (D.rphys[bt]) {
       size_t id = css_idx(g, t0 + m - 1, pb + l, ir);
-      double rho = x[m - 1], t = temp_of(g, rho, __ldg(cur + 4 * n + id));
+      double rho = x[m - 1], t = __ldg(tbuf + id);
       hi = rvv * dv[n + id] * rho / t;
     }
     int bdry = g.ibct[1];
-    line_solve<1>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, D.dnum[bt], D.dnum[bt], 0,
+    solve<1, MT>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, D.dnum[bt], D.dnum[bt], 0,
                   O + (size_t)l * SO, 1);
   }
   __syncthreads();
@@ -525,8 +534,8 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
     if (ip >= g.nphi) continue;
     size_t id = css_idx(g, it, ip, ir);
     double rho = H[(size_t)l * SR + 4 + j];
-    double w = __ldg(cur + n + id), s = __ldg(cur + 4 * n + id);
-    double t = temp_of(g, rho, s);
+    double w = __ldg(cur + n + id);
+    double t = __ldg(tbuf + id);
     double w1 = ri * O[(size_t)l * SO + j];
     double d0 = dv[id] - w * w1;
     w1 = w1 * (1.0 / rho);
@@ -591,6 +600,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
 // (theta, phi, r).  Three kernels, one per sweep direction; the r sweep
 // optionally applies Compute_B's boundary zeroing (:1842-1883).
 // ---------------------------------------------------------------------------
+template <int MT>
 __global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
                                                     int TL) {
   extern __shared__ double sm[];
@@ -618,7 +628,7 @@ __global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__re
     int k = task / TL, l = task - k * TL;
     if (pb + l >= g.nphi) continue;
     int bdry = g.ibct[k == 0 ? 11 : 12];
-    line_solve<1>(H + ((size_t)k * TL + l) * SR + 4, 1, m, dtype, bdry, 0.0, 0.0, tabp(g, 1, bt, 1, bdry), g.tstride,
+    solve<1, MT>(H + ((size_t)k * TL + l) * SR + 4, 1, m, dtype, bdry, 0.0, 0.0, tabp(g, 1, bt, 1, bdry), g.tstride,
                   D.dnum[bt], D.dnum[bt], 0, O + ((size_t)k * TL + l) * SO, 1);
   }
   __syncthreads();
@@ -633,6 +643,7 @@ __global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__re
   }
 }
 
+template <int MT>
 __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
                                                   int TL) {
   extern __shared__ double sm[];
@@ -652,7 +663,7 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__rest
   for (int task = threadIdx.x; task < 2 * TL; task += blockDim.x) {
     int k = task / TL, l = task - k * TL;
     if (tb + l >= g.nth) continue;
-    line_solve<1>(H + k * HS + 4 * SR + l, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, D.dnum[bp],
+    solve<1, MT>(H + k * HS + 4 * SR + l, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, D.dnum[bp],
                   D.dnum[bp], 1, O + k * OS + l, SR);
   }
   __syncthreads();
@@ -668,6 +679,7 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__rest
   }
 }
 
+template <int MT>
 __global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
                                                 int TL, int apply_bc) {
   extern __shared__ double sm[];
@@ -697,7 +709,7 @@ __global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const double *__restri
     int k = task / TL, l = task - k * TL;
     if (tb + l >= g.nth) continue;
     int bdry = g.ibcr[k == 0 ? 10 : 11];
-    line_solve<1>(H + k * HS + 4 * SR + l, SR, m, dtype, bdry, 0.0, 0.0, tabp(g, 0, br, 1, bdry), g.tstride,
+    solve<1, MT>(H + k * HS + 4 * SR + l, SR, m, dtype, bdry, 0.0, 0.0, tabp(g, 0, br, 1, bdry), g.tstride,
                   D.dnum[br], D.dnum[br], 0, O + k * OS + l, SR);
   }
   __syncthreads();
@@ -792,179 +804,207 @@ __device__ __forceinline__ double sld_val(const CssGeo &g, const double *__restr
   return q;
 }
 
-__global__ void __launch_bounds__(128) k_sld(CssGeo g, const double *__restrict__ v, const double *__restrict__ av,
-                                             const double *__restrict__ vcc, double *__restrict__ dout) {
-  size_t n = (size_t)g.ncell;
-  const int nth = g.nth, nphi = g.nphi, nr = g.nr;
-  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x) {
-    int it = (int)(id % nth);
-    int ip = (int)((id / nth) % nphi);
-    int ir = (int)(id / ((size_t)nth * nphi));
-    const double *r = g.r_ind, *dr = g.dr_ind;
-    // geometry of this cell
-    double rlo = (ir == 0) ? r[0] - 0.5 * dr[0] : 0.5 * (r[ir] + r[ir - 1]);
-    double rhi = (ir == nr - 1) ? r[nr - 1] + 0.5 * dr[nr - 1] : 0.5 * (r[ir + 1] + r[ir]);
-    double t3 = 3.0 / (rhi * rhi * rhi - rlo * rlo * rlo);
-    double rfac = 1.5 * (rhi * rhi - rlo * rlo) / (rhi * rhi * rhi - rlo * rlo * rlo);
-    const double *th = g.theta;
-    double dth = g.dth;
-    double sphl, cphl, sphh, cphh;
-    if (it == 0) { sphl = fabs(sin(th[0] - 0.5 * dth)); cphl = cos(th[0] - 0.5 * dth); }
-    else { double a = 0.5 * (th[it] + th[it - 1]); sphl = sin(a); cphl = cos(a); }
-    if (it == nth - 1) { sphh = sin(th[it] + 0.5 * dth); cphh = cos(th[it] + 0.5 * dth); }
-    else { double a = 0.5 * (th[it] + th[it + 1]); sphh = sin(a); cphh = cos(a); }
-    double geom;
-    {
-      double rt, st, ct;
-      if (it == 0) { rt = th[0] - 0.5 * dth; st = cos(rt); }
-      else { rt = 0.5 * (th[it] + th[it - 1]); st = cos(rt); }
-      if (it == nth - 1) { ct = th[it] + 0.5 * dth; rt = ct - rt; ct = cos(ct); }
-      else { ct = 0.5 * (th[it + 1] + th[it]); rt = ct - rt; ct = cos(ct); }
-      geom = rt / (st - ct);
-      geom = geom * (rfac / g.dphi);
+// ghost value just outside a physical radial face (diffusion.f90:582-728):
+// lo = 1 for the bottom (x(-1) from x(0..3)), 0 for the top (x(nr) from
+// x(nr-1..nr-4)); iv1 is the reference's 1-based variable index
+__device__ double sld_ghost_r(const CssGeo &g, const double *__restrict__ v, const double *__restrict__ av, int iv,
+                              int it, int ip, int lo) {
+  const double *r = g.r_ind, *dr = g.dr_ind;
+  int iv1 = iv + 1, nr = g.nr;
+  if (lo) {
+    double t1 = sld_val(g, v, av, iv, it, ip, 0);
+    switch (iv1) {
+      case 1: return 0.0;
+      case 2: case 3:
+        return -10.0 * (1.0 / 3.0) * t1 / r[0] + 6.0 * sld_val(g, v, av, iv, it, ip, 1) / r[1] -
+               2.0 * sld_val(g, v, av, iv, it, ip, 2) / r[2] + (1.0 / 3.0) * sld_val(g, v, av, iv, it, ip, 3) / r[3];
+      case 5:
+        if (!g.bottom_constant_temp && g.slaplacian)
+          return t1 + dr[0] * (g.lumr1 * ONE_OVER_4PI / (g.r1 * g.r1 * g.ks[0] * g.dxdr[0]));
+        return 0.0;
+      case 6: case 7: return g.bottom_perfect_cond ? 0.0 : t1;
+      default: return t1;
     }
-    // face speeds
-    double vc = __ldg(vcc + id);
-    auto vface = [&](double a, double b) { return g.sld_coef * sqrt(0.5 * (a + b)); };
-    double vr_lo = (ir > 0) ? vface(vc, __ldg(vcc + css_idx(g, it, ip, ir - 1))) : 0.0;
-    double vr_hi = (ir < nr - 1) ? vface(__ldg(vcc + css_idx(g, it, ip, ir + 1)), vc) : 0.0;
-    double vt_lo = (it > 0) ? vface(vc, __ldg(vcc + id - 1)) : 0.0;
-    double vt_hi = (it < nth - 1) ? vface(__ldg(vcc + id + 1), vc) : 0.0;
-    int ipm = (ip - 1 + nphi) % nphi, ipp = (ip + 1) % nphi;
-    double vp_lo = vface(__ldg(vcc + css_idx(g, it, ipm, ir)), vc);
-    double vp_hi = vface(vc, __ldg(vcc + css_idx(g, it, ipp, ir)));
+  }
+  int m = nr - 1;
+  double tm = sld_val(g, v, av, iv, it, ip, m);
+  switch (iv1) {
+    case 1: return 0.0;
+    case 2: case 3:
+      return -10.0 * (1.0 / 3.0) * tm / r[m] + 6.0 * sld_val(g, v, av, iv, it, ip, m - 1) / r[m - 1] -
+             2.0 * sld_val(g, v, av, iv, it, ip, m - 2) / r[m - 2] +
+             (1.0 / 3.0) * sld_val(g, v, av, iv, it, ip, m - 3) / r[m - 3];
+    case 5:
+      if (!g.top_constant_temp && g.slaplacian)
+        return tm - dr[0] * (g.lumr2 * ONE_OVER_4PI / (g.r2 * g.r2 * g.ks[nr - 1] * g.dxdr[nr - 1]));
+      return 0.0;
+    case 6: case 7: return g.top_perfect_cond ? 0.0 : tm;
+    default: return tm;
+  }
+}
+
+// ghost just outside a physical theta face (diffusion.f90:1008-1118), from
+// the four tile values nearest the wall (q0 at the wall)
+__device__ __forceinline__ double sld_ghost_t(const CssGeo &g, int iv, double q0, double q1, double q2, double q3,
+                                              int lo) {
+  const double *sn = g.sines;
+  int iv1 = iv + 1, m = g.nth - 1;
+  switch (iv1) {
+    case 2: return 0.0;
+    case 3:
+      if (lo)
+        return -10.0 * (1.0 / 3.0) * q0 / sn[0] + 6.0 * q1 / sn[1] - 2.0 * q2 / sn[2] + (1.0 / 3.0) * q3 / sn[3];
+      return -10.0 * (1.0 / 3.0) * q0 / sn[m] + 6.0 * q1 / sn[m - 1] - 2.0 * q2 / sn[m - 2] + (1.0 / 3.0) * q3 / sn[m - 3];
+    case 6: return g.theta_normal_field ? 0.0 : q0;
+    case 7: case 8: return g.theta_perf_conductor ? 0.0 : q0;
+    default: return q0;
+  }
+}
+
+// Slope-limited diffusion, all three directions and all nsld fields in one
+// pass.  CTA = a 32 (theta) x 8 (phi) plane tile marching over an r chunk of
+// SLD_RC radii; each face's limited flux is computed once: theta and phi
+// faces of the plane from a shared tile with a 2-point halo, r faces carried
+// in registers from one radius to the next.  Then viscous heating and the
+// mass-diffusion corrections (diffusion.f90:375-428) per cell.
+#define SLD_TT 32
+#define SLD_TP 8
+#define SLD_RC 16
+__global__ void __launch_bounds__(SLD_TT * SLD_TP) k_sld(CssGeo g, const double *__restrict__ v,
+                                                         const double *__restrict__ av,
+                                                         const double *__restrict__ vcc, double *__restrict__ dout) {
+  __shared__ double X[SLD_TP + 4][SLD_TT + 5];   // field plane, halo 2
+  __shared__ double V[SLD_TP + 2][SLD_TT + 3];   // vcc plane, halo 1
+  __shared__ double FT[SLD_TP][SLD_TT + 1];      // theta faces
+  __shared__ double FP[SLD_TP + 1][SLD_TT + 1];  // phi faces
+  const size_t n = (size_t)g.ncell;
+  const int nth = g.nth, nphi = g.nphi, nr = g.nr;
+  const int tx = threadIdx.x % SLD_TT, ty = threadIdx.x / SLD_TT;
+  const int t0 = blockIdx.x * SLD_TT, p0 = blockIdx.y * SLD_TP;
+  const int r0 = blockIdx.z * SLD_RC, r1 = min(r0 + SLD_RC, nr);
+  const int it = t0 + tx, ip = p0 + ty;
+  const bool live = it < nth && ip < nphi;
+  const int itc = min(it, nth - 1), ipc = min(ip, nphi - 1);
+  // r-face carry per field: de of the lower r face of the current radius,
+  // and x(ir-1)
+  double carry[8], xprev[8];
+  for (int ir = r0; ir < r1; ir++) {
+    const double t3 = g.sld_r[ir], rfac = g.sld_r[nr + ir], rlo2 = g.sld_r[2 * nr + ir];
+    const double rhi2 = g.sld_r[3 * nr + ir];
+    const double cphl = g.sld_th[nth + itc], cphh = g.sld_th[3 * nth + itc];
+    const double geom = g.sld_th[4 * nth + itc] * (rfac / g.dphi);
+    // vcc plane with halo 1 (clamped at theta walls: those faces are zeroed)
+    __syncthreads();
+    for (int k = threadIdx.x; k < (SLD_TP + 2) * (SLD_TT + 2); k += blockDim.x) {
+      int a = k % (SLD_TT + 2), b = k / (SLD_TT + 2);
+      int gt = min(max(t0 + a - 1, 0), nth - 1), gp = (p0 + b - 1 + nphi) % nphi;
+      V[b][a] = __ldg(vcc + css_idx(g, gt, gp, ir));
+    }
+    const double vc = __ldg(vcc + css_idx(g, itc, ipc, ir));
+    const double vcm = ir > 0 ? __ldg(vcc + css_idx(g, itc, ipc, ir - 1)) : vc;
+    const double vcp = ir < nr - 1 ? __ldg(vcc + css_idx(g, itc, ipc, ir + 1)) : vc;
+    const double vr_lo = g.sld_coef * sqrt(0.5 * (vc + vcm));
+    const double vr_hi = g.sld_coef * sqrt(0.5 * (vcp + vc));
     double Dv[8];
-    for (int iv = 0; iv < g.nv; iv++) Dv[iv] = 0.0;
-    for (int isl = 0; isl < g.nsld; isl++) {
-      int iv = g.varlist[isl], iv1 = iv + 1;
-      double tiny = g.tinyvar[iv];
+    const int off = g.varlist[0];  // varlist is off, off+1, ..., contiguous
+#pragma unroll
+    for (int isl = 0; isl < 8; isl++) {
+      Dv[isl] = 0.0;
+      if (isl >= g.nsld) continue;
+      const int iv = isl + off, iv1 = iv + 1;
+      const double tiny = g.tinyvar[iv];
       double prR = 1.0, prTP = 1.0;
       if (g.sld_pr != 1.0 || g.sld_prm != 1.0) {
         if (iv1 <= 3) prR = g.sld_pr; else if (iv1 >= 5) prR = g.sld_prm;
         if (iv1 < 5) prTP = g.sld_pr; else if (iv1 > 5) prTP = g.sld_prm;
       }
-      double x0 = sld_val(g, v, av, iv, it, ip, ir);
-      // ---- r ----
-      double xr[5];  // ir-2 .. ir+2
-      xr[2] = x0;
-      for (int k = -2; k <= 2; k++) {
-        if (k == 0) continue;
-        int q = ir + k;
-        if (q >= 0 && q < nr) xr[k + 2] = sld_val(g, v, av, iv, it, ip, q);
-        else xr[k + 2] = 0.0;
+      __syncthreads();
+      // plane tile with halo 2 (theta ghosts filled below, phi periodic)
+      for (int k = threadIdx.x; k < (SLD_TP + 4) * (SLD_TT + 4); k += blockDim.x) {
+        int a = k % (SLD_TT + 4), b = k / (SLD_TT + 4);
+        int gt = t0 + a - 2, gp = (p0 + b - 2 + nphi) % nphi;
+        X[b][a] = (gt >= 0 && gt < nth) ? sld_val(g, v, av, iv, gt, gp, ir) : 0.0;
       }
-      // ghost next to a physical radial face (diffusion.f90:582-728)
-      if (ir <= 1) {
-        double t1 = sld_val(g, v, av, iv, it, ip, 0), gl;
-        switch (iv1) {
-          case 1: gl = 0.0; break;
-          case 2: case 3:
-            gl = -10.0 * (1.0 / 3.0) * t1 / r[0] + 6.0 * sld_val(g, v, av, iv, it, ip, 1) / r[1] -
-                 2.0 * sld_val(g, v, av, iv, it, ip, 2) / r[2] + (1.0 / 3.0) * sld_val(g, v, av, iv, it, ip, 3) / r[3];
-            break;
-          case 5:
-            if (!g.bottom_constant_temp && g.slaplacian)
-              gl = t1 + dr[0] * (g.lumr1 * ONE_OVER_4PI / (g.r1 * g.r1 * g.ks[0] * g.dxdr[0]));
-            else gl = 0.0;
-            break;
-          case 6: case 7: gl = g.bottom_perfect_cond ? 0.0 : t1; break;
-          default: gl = t1; break;
+      __syncthreads();
+      if (t0 == 0 && threadIdx.x < SLD_TP + 4) {  // x(-1) next to the low wall
+        int b = threadIdx.x;
+        X[b][1] = sld_ghost_t(g, iv, X[b][2], X[b][3], X[b][4], X[b][5], 1);
+      }
+      if (t0 + SLD_TT >= nth && threadIdx.x >= 32 && threadIdx.x < 32 + SLD_TP + 4) {  // x(nth)
+        int b = threadIdx.x - 32, a = nth - t0 + 2;
+        X[b][a] = sld_ghost_t(g, iv, X[b][a - 1], X[b][a - 2], X[b][a - 3], X[b][a - 4], 0);
+      }
+      __syncthreads();
+      // theta faces: face a sits between tile columns a-1 and a (a = 0..32)
+      for (int k = threadIdx.x; k < SLD_TP * (SLD_TT + 1); k += blockDim.x) {
+        int a = k % (SLD_TT + 1), b = k / (SLD_TT + 1);
+        int gt = t0 + a;  // the face below global theta gt
+        double d = 0.0;
+        if (gt > 0 && gt < nth) {
+          double vt = g.sld_coef * sqrt(0.5 * (V[b + 1][a + 1] + V[b + 1][a]));
+          double sp = g.sld_th[gt];  // sin of the face below theta gt
+          d = (vt * sp) * sld_face(X[b + 2][a], X[b + 2][a + 1], X[b + 2][a + 2], X[b + 2][a + 3], tiny);
         }
-        xr[ir == 0 ? 1 : 0] = gl;
+        FT[b][a] = d;
       }
-      if (ir >= nr - 2) {
-        int m = nr - 1;
-        double tm = sld_val(g, v, av, iv, it, ip, m), gh;
-        switch (iv1) {
-          case 1: gh = 0.0; break;
-          case 2: case 3:
-            gh = -10.0 * (1.0 / 3.0) * tm / r[m] + 6.0 * sld_val(g, v, av, iv, it, ip, m - 1) / r[m - 1] -
-                 2.0 * sld_val(g, v, av, iv, it, ip, m - 2) / r[m - 2] +
-                 (1.0 / 3.0) * sld_val(g, v, av, iv, it, ip, m - 3) / r[m - 3];
-            break;
-          case 5:
-            if (!g.top_constant_temp && g.slaplacian)
-              gh = tm - dr[0] * (g.lumr2 * ONE_OVER_4PI / (g.r2 * g.r2 * g.ks[nr - 1] * g.dxdr[nr - 1]));
-            else gh = 0.0;
-            break;
-          case 6: case 7: gh = g.top_perfect_cond ? 0.0 : tm; break;
-          default: gh = tm; break;
+      // phi faces: face b between tile rows b-1 and b (b = 0..8)
+      for (int k = threadIdx.x; k < (SLD_TP + 1) * SLD_TT; k += blockDim.x) {
+        int a = k % SLD_TT, b = k / SLD_TT;
+        double vt = g.sld_coef * sqrt(0.5 * (V[b][a + 1] + V[b + 1][a + 1]));
+        FP[b][a] = vt * sld_face(X[b][a + 2], X[b + 1][a + 2], X[b + 2][a + 2], X[b + 3][a + 2], tiny);
+      }
+      // r faces (the thread's own column); x(ir-1) is carried in xprev
+      const double x0 = X[ty + 2][tx + 2];
+      double xp1 = 0.0, xp2 = 0.0;
+      if (ir + 1 < nr) xp1 = sld_val(g, v, av, iv, itc, ipc, ir + 1);
+      if (ir + 2 < nr) xp2 = sld_val(g, v, av, iv, itc, ipc, ir + 2);
+      else if (ir + 2 == nr) xp2 = sld_ghost_r(g, v, av, iv, itc, ipc, 0);
+      double dlo;
+      if (ir == r0) {
+        xprev[isl] = (ir > 0) ? sld_val(g, v, av, iv, itc, ipc, ir - 1) : sld_ghost_r(g, v, av, iv, itc, ipc, 1);
+        if (ir == 0) {
+          dlo = 0.0;
+        } else {
+          double xm2 = (ir >= 2) ? sld_val(g, v, av, iv, itc, ipc, ir - 2) : sld_ghost_r(g, v, av, iv, itc, ipc, 1);
+          dlo = vr_lo * (sld_face(xm2, xprev[isl], x0, xp1, tiny) * rlo2);
         }
-        xr[ir == nr - 1 ? 3 : 4] = gh;
+      } else {
+        dlo = carry[isl];
       }
-      double dlo = (ir == 0) ? 0.0 : sld_face(xr[0], xr[1], xr[2], xr[3], tiny) * (rlo * rlo);
-      double dhi = (ir == nr - 1) ? 0.0 : sld_face(xr[1], xr[2], xr[3], xr[4], tiny) * (rhi * rhi);
-      dlo = vr_lo * dlo;
-      dhi = vr_hi * dhi;
-      double flux = t3 * (dhi - dlo);
+      double dup = (ir == nr - 1) ? 0.0 : vr_hi * (sld_face(xprev[isl], x0, xp1, xp2, tiny) * rhi2);
+      carry[isl] = dup;
+      xprev[isl] = x0;
+      double flux = t3 * (dup - dlo);
       if (prR != 1.0) flux = prR * flux;
       double acc = flux;
-      // ---- theta ----
-      double xt[5];
-      xt[2] = x0;
-      for (int k = -2; k <= 2; k++) {
-        if (k == 0) continue;
-        int q = it + k;
-        if (q >= 0 && q < nth) xt[k + 2] = sld_val(g, v, av, iv, q, ip, ir);
-        else xt[k + 2] = 0.0;
-      }
-      if (it <= 1) {
-        double t1 = sld_val(g, v, av, iv, 0, ip, ir), gl;
-        const double *sn = g.sines;
-        switch (iv1) {
-          case 2: gl = 0.0; break;
-          case 3:
-            gl = -10.0 * (1.0 / 3.0) * t1 / sn[0] + 6.0 * sld_val(g, v, av, iv, 1, ip, ir) / sn[1] -
-                 2.0 * sld_val(g, v, av, iv, 2, ip, ir) / sn[2] + (1.0 / 3.0) * sld_val(g, v, av, iv, 3, ip, ir) / sn[3];
-            break;
-          case 6: gl = g.theta_normal_field ? 0.0 : t1; break;
-          case 7: case 8: gl = g.theta_perf_conductor ? 0.0 : t1; break;
-          default: gl = t1; break;
-        }
-        xt[it == 0 ? 1 : 0] = gl;
-      }
-      if (it >= nth - 2) {
-        int m = nth - 1;
-        double tm = sld_val(g, v, av, iv, m, ip, ir), gh;
-        const double *sn = g.sines;
-        switch (iv1) {
-          case 2: gh = 0.0; break;
-          case 3:
-            gh = -10.0 * (1.0 / 3.0) * tm / sn[m] + 6.0 * sld_val(g, v, av, iv, m - 1, ip, ir) / sn[m - 1] -
-                 2.0 * sld_val(g, v, av, iv, m - 2, ip, ir) / sn[m - 2] +
-                 (1.0 / 3.0) * sld_val(g, v, av, iv, m - 3, ip, ir) / sn[m - 3];
-            break;
-          case 6: gh = g.theta_normal_field ? 0.0 : tm; break;
-          case 7: case 8: gh = g.theta_perf_conductor ? 0.0 : tm; break;
-          default: gh = tm; break;
-        }
-        xt[it == nth - 1 ? 3 : 4] = gh;
-      }
-      dlo = (it == 0) ? 0.0 : (vt_lo * sphl) * sld_face(xt[0], xt[1], xt[2], xt[3], tiny);
-      dhi = (it == nth - 1) ? 0.0 : (vt_hi * sphh) * sld_face(xt[1], xt[2], xt[3], xt[4], tiny);
-      flux = (rfac / (cphl - cphh)) * (dhi - dlo);
+      __syncthreads();
+      flux = (rfac / (cphl - cphh)) * (FT[ty][tx + 1] - FT[ty][tx]);
       if (prTP != 1.0) flux = prTP * flux;
       acc = acc + flux;
-      // ---- phi (periodic) ----
-      double xp[5];
-      for (int k = -2; k <= 2; k++) xp[k + 2] = (k == 0) ? x0 : sld_val(g, v, av, iv, it, (ip + k + nphi) % nphi, ir);
-      dlo = vp_lo * sld_face(xp[0], xp[1], xp[2], xp[3], tiny);
-      dhi = vp_hi * sld_face(xp[1], xp[2], xp[3], xp[4], tiny);
-      flux = dhi - dlo;
+      flux = FP[ty + 1][tx] - FP[ty][tx];
       if (prTP != 1.0) flux = prTP * flux;
       acc = acc + geom * flux;
-      Dv[iv] = acc;
+      Dv[isl] = acc;
     }
-    // viscous heating and mass-diffusion corrections (diffusion.f90:375-428)
-    double invrho = 1.0 / __ldg(v + id);
-    double itemp = (pow(__ldg(v + id), -g.gamm1)) * exp(-__ldg(v + 4 * n + id) * g.invcv) / g.invtconst;
+    if (!live) continue;
+    const size_t id = css_idx(g, it, ip, ir);
+    double D[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) D[k] = off ? (k >= 1 ? Dv[k - 1] : 0.0) : Dv[k];
+    double rho = __ldg(v + id);
+    double invrho = 1.0 / rho;
+    double itemp = (pow(rho, -g.gamm1)) * exp(-__ldg(v + 4 * n + id) * g.invcv) / g.invtconst;
     if (g.do_viscous_heating)
-      for (int iv = 1; iv <= 3; iv++) Dv[4] = Dv[4] - __ldg(v + iv * n + id) * Dv[iv] * itemp;
+#pragma unroll
+      for (int k = 1; k <= 3; k++) D[4] = D[4] - __ldg(v + k * n + id) * D[k] * itemp;
     if (g.mass_diffusion) {
-      for (int iv = 1; iv <= 3; iv++) Dv[iv] = Dv[iv] - invrho * __ldg(v + iv * n + id) * Dv[0];
-      Dv[4] = Dv[4] - (g.gamm1 * g.cv) * invrho * Dv[0];
+#pragma unroll
+      for (int k = 1; k <= 3; k++) D[k] = D[k] - invrho * __ldg(v + k * n + id) * D[0];
+      D[4] = D[4] - (g.gamm1 * g.cv) * invrho * D[0];
     }
-    for (int iv = 0; iv < g.nv; iv++) dout[iv * n + id] = Dv[iv];
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+      if (k < g.nv) dout[k * n + id] = D[k];
   }
 }
 
@@ -985,7 +1025,7 @@ __global__ void k_sld_ohmic(CssGeo g, const double *__restrict__ v, const double
 // ---------------------------------------------------------------------------
 // generic single-field derivative (css_deriv): one kernel per direction
 // ---------------------------------------------------------------------------
-template <int ORDER>
+template <int ORDER, int MT>
 __global__ void __launch_bounds__(128) k_deriv_theta(CssGeo g, const double *__restrict__ f, double *__restrict__ out,
                                                      const double *__restrict__ bclo, const double *__restrict__ bchi,
                                                      int bdry, int TL) {
@@ -1006,7 +1046,7 @@ __global__ void __launch_bounds__(128) k_deriv_theta(CssGeo g, const double *__r
     double hi = (D.rphys[bt] && bchi) ? bchi[ip + (size_t)g.nphi * ir] : 0.0;
     double dn = (ORDER == 1) ? D.dnum[bt] : dnum_d2_theta(g, ir);
     double sc = (ORDER == 1) ? D.dnum[bt] : D.dnum[bt] * D.dnum[bt];
-    line_solve<ORDER>(H + (size_t)l * SR + 4, 1, m, dtype_of(D, bt), bdry, lo, hi, tabp(g, 1, bt, ORDER, bdry),
+    solve<ORDER, MT>(H + (size_t)l * SR + 4, 1, m, dtype_of(D, bt), bdry, lo, hi, tabp(g, 1, bt, ORDER, bdry),
                       g.tstride, dn, sc, 0, O + (size_t)l * SO, 1);
   }
   __syncthreads();
@@ -1017,7 +1057,7 @@ __global__ void __launch_bounds__(128) k_deriv_theta(CssGeo g, const double *__r
   }
 }
 
-template <int ORDER>
+template <int ORDER, int MT>
 __global__ void __launch_bounds__(128) k_deriv_phi(CssGeo g, const double *__restrict__ f, double *__restrict__ out,
                                                    int TL) {
   extern __shared__ double sm[];
@@ -1033,7 +1073,7 @@ __global__ void __launch_bounds__(128) k_deriv_phi(CssGeo g, const double *__res
   for (int l = threadIdx.x; l < TL; l += blockDim.x) {
     if (tb + l >= g.nth) continue;
     double sc = (ORDER == 1) ? D.dnum[bp] : D.dnum[bp] * D.dnum[bp];
-    line_solve<ORDER>(H + 4 * SR + l, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, ORDER, 0), g.tstride, D.dnum[bp], sc, 1,
+    solve<ORDER, MT>(H + 4 * SR + l, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, ORDER, 0), g.tstride, D.dnum[bp], sc, 1,
                       O + l, SR);
   }
   __syncthreads();
@@ -1044,7 +1084,7 @@ __global__ void __launch_bounds__(128) k_deriv_phi(CssGeo g, const double *__res
   }
 }
 
-template <int ORDER>
+template <int ORDER, int MT>
 __global__ void __launch_bounds__(128) k_deriv_r(CssGeo g, const double *__restrict__ f, double *__restrict__ out,
                                                  const double *__restrict__ bclo, const double *__restrict__ bchi,
                                                  int bdry, int TL) {
@@ -1064,7 +1104,7 @@ __global__ void __launch_bounds__(128) k_deriv_r(CssGeo g, const double *__restr
     double lo = (D.lphys[br] && bclo) ? bclo[it + (size_t)g.nth * ip] : 0.0;
     double hi = (D.rphys[br] && bchi) ? bchi[it + (size_t)g.nth * ip] : 0.0;
     double sc = (ORDER == 1) ? D.dnum[br] : D.dnum[br] * D.dnum[br];
-    line_solve<ORDER>(H + 4 * SR + l, SR, m, dtype_of(D, br), bdry, lo, hi, tabp(g, 0, br, ORDER, bdry), g.tstride,
+    solve<ORDER, MT>(H + 4 * SR + l, SR, m, dtype_of(D, br), bdry, lo, hi, tabp(g, 0, br, ORDER, bdry), g.tstride,
                       D.dnum[br], sc, 0, O + l, SR);
   }
   __syncthreads();
