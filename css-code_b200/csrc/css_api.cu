@@ -49,7 +49,7 @@ struct css_ctx {
   size_t ncell;
   cudaStream_t stream;
   // device buffers
-  double *tab, *prof, *theta_prof, *sld_geo;
+  double *tab, *prof, *theta_prof, *sld_geo, *resp;
   int *rblk;
   double *v0, *vA, *vB, *dv, *vs;  // state, stage ping-pong, tendency, RK accumulator
   double *bf;                       // B = curl A (MHD)
@@ -198,6 +198,20 @@ static int partition(int n, int nn, int *start, int *size) {
 }
 
 static size_t smem_theta(int nh, int nd, int m, int TL) { return 8 * ((size_t)nh * TL * (m + 9) + (size_t)nd * TL * (m + 1)); }
+// shared memory of the RHS kernels: tiles + derivative buffers + staged LU tables
+static size_t smem_theta_terms(int mag, int m, int TL) {
+  int nh = mag ? 6 : 4, nd = mag ? 7 : 5;
+  return 8 * ((size_t)nh * TL * (m + 9) + (size_t)nd * TL * (m + 1) + (size_t)nd * 3 * (m + 2));
+}
+static size_t smem_phi_terms(int mag, int m, int TL) {
+  int nh = mag ? 7 : 5, nd = mag ? 8 : 6;
+  return 8 * ((size_t)nh * (m + 8) * (TL + 1) + (size_t)nd * m * (TL + 1) + (size_t)2 * 3 * (m + 2));
+}
+static size_t smem_radial_terms(int mag, int m, int TL) {
+  int nh = mag ? 7 : 5, nd = mag ? 8 : 6;
+  return 8 * ((size_t)nh * (m + 8) * (TL + 1) + (size_t)nd * m * (TL + 1) + (size_t)nd * 3 * (m + 2) + TL);
+}
+static size_t smem_rhot(int m, int TL) { return 8 * ((size_t)TL * (m + 9) + (size_t)TL * (m + 1) + 3 * (m + 2)); }
 static size_t smem_line(int nh, int nd, int na, int m, int TL) {
   return 8 * ((size_t)nh * (m + 8) * (TL + 1) + (size_t)(nd + na) * m * (TL + 1));
 }
@@ -213,7 +227,7 @@ static int pick_tl(int kind, int nh, int nd, int na, int m) {
 
 extern "C" void css_destroy(css_ctx *c) {
   if (!c) return;
-  cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo);
+  cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo); cudaFree(c->resp);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
   cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf);
   for (auto e : c->ev) cudaEventDestroy(e);
@@ -221,31 +235,32 @@ extern "C" void css_destroy(css_ctx *c) {
   delete c;
 }
 
-template <int MT>
+template <int MT, int TLC>
 static int setup_mt() {
   int mx = 200 * 1024;
-  CUDA_TRY(cudaFuncSetAttribute(k_theta_terms<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_phi_terms<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_radial_terms<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_rhot_update<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_theta<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_phi<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_r<MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<1, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<2, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<1, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<2, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<1, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<2, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_theta_terms<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_phi_terms<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_radial_terms<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_rhot_update<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_theta<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_phi<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_r<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   return CSS_OK;
 }
 
 static int setup_kernels() {
   static bool done = false;
   if (done) return CSS_OK;
-  if (int rc = setup_mt<0>()) return rc;
-  if (int rc = setup_mt<16>()) return rc;
-  if (int rc = setup_mt<32>()) return rc;
+  if (int rc = setup_mt<0, 0>()) return rc;
+  if (int rc = setup_mt<16, 16>()) return rc;
+  if (int rc = setup_mt<32, 16>()) return rc;
+  int mx = 200 * 1024;
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+  CUDA_TRY(cudaFuncSetAttribute(k_deriv_r<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   done = true;
   return CSS_OK;
 }
@@ -254,9 +269,9 @@ static int setup_kernels() {
 #define LAUNCH_MT(DIR, KERNEL, GRID, SMEM, ...)                                          \
   do {                                                                                    \
     switch (c->mt[DIR]) {                                                                 \
-      case 16: KERNEL<16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;           \
-      case 32: KERNEL<32><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;           \
-      default: KERNEL<0><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;            \
+      case 16: KERNEL<16, 16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;       \
+      case 32: KERNEL<32, 16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;       \
+      default: KERNEL<0, 0><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;         \
     }                                                                                     \
   } while (0)
 
@@ -365,6 +380,34 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
           else tab_d2(m, D.lphys[b], D.rphys[b], iv, g1, g2, g3);
         }
         (order == 1 ? D.tab1 : D.tab2)[b] = off;
+      }
+    }
+  }
+  // unit responses of the first-derivative system of rho (bdry ibcr(1)) to
+  // its face datum on the radial blocks with a physical face: resp = A^-1 e_1
+  // (bottom) / A^-1 e_m (top), by the same sweeps the kernels run
+  std::vector<double> RESP((size_t)2 * g.d[0].nb * ts, 0.0);
+  {
+    int bdry = 4;  // lbcr_rho (Read_Input, mhdsph_mpi.f90:1362)
+    for (int b = 0; b < g.d[0].nb; b++) {
+      CssDir &D = g.d[0];
+      int m = D.size[b];
+      const double *g1 = &T[D.tab1[b] + (size_t)bdry * 3 * ts], *g2 = g1 + ts, *g3 = g2 + ts;
+      for (int side = 0; side < 2; side++) {
+        bool on = side == 0 ? (D.lphys[b] && (bdry == 2 || bdry == 4)) : (D.rphys[b] && (bdry == 3 || bdry == 4));
+        if (!on) continue;
+        std::vector<double> d(m + 2, 0.0), t(m + 2, 0.0), x(m + 2, 0.0);
+        d[side == 0 ? 1 : m] = 1.0;
+        const double a1 = -1.0 / 3.0;
+        t[1] = g2[1] * d[1];
+        t[2] = g2[2] * d[2] + g3[2] * t[1];
+        for (int j = 3; j <= m - 2; j++) t[j] = g2[j] * (d[j] + a1 * t[j - 1]);
+        t[m - 1] = g2[m - 1] * d[m - 1] + g3[m - 1] * t[m - 2];
+        t[m] = g2[m] * d[m] + g3[m] * t[m - 1];
+        x[m] = t[m];
+        for (int j = m - 1; j >= 1; j--) x[j] = t[j] + g1[j + 1] * x[j + 1];
+        double *dst = &RESP[(size_t)(2 * b + side) * ts];
+        for (int j = 1; j <= m; j++) dst[j] = x[j];
       }
     }
   }
@@ -505,6 +548,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   ALLOC(c->prof, R.size() * 8);
   ALLOC(c->theta_prof, TH.size() * 8);
   ALLOC(c->sld_geo, SG.size() * 8);
+  ALLOC(c->resp, RESP.size() * 8);
   ALLOC(c->rblk, nr * sizeof(int));
   size_t sb = c->ncell * c->nv * sizeof(double);
   ALLOC(c->v0, sb); ALLOC(c->vA, sb); ALLOC(c->vB, sb); ALLOC(c->dv, sb); ALLOC(c->vs, sb);
@@ -516,10 +560,11 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   cudaMemcpy(c->prof, R.data(), R.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->theta_prof, TH.data(), TH.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->sld_geo, SG.data(), SG.size() * 8, cudaMemcpyHostToDevice);
+  cudaMemcpy(c->resp, RESP.data(), RESP.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->rblk, rblk.data(), nr * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemset(c->flag, 0, sizeof(int));
   cudaMemset(c->vs, 0, sb);
-  g.tab = c->tab; g.rblk = c->rblk;
+  g.tab = c->tab; g.rblk = c->rblk; g.resp_r = c->resp;
   g.r_ind = c->prof; g.r_inv = c->prof + nr; g.dr_ind = c->prof + 2 * nr; g.dxdr = c->prof + 3 * nr;
   g.d2xdr2 = c->prof + 4 * nr; g.rhor = c->prof + 5 * nr; g.sr = c->prof + 6 * nr; g.grav = c->prof + 7 * nr;
   g.ks = c->prof + 8 * nr; g.dlnks = c->prof + 9 * nr; g.eps = c->prof + 10 * nr; g.dspeed = c->prof + 11 * nr;
@@ -532,14 +577,20 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     return CSS_ERR_CUDA;
   }
   int mag = p.magnetic;
-  c->tl_theta = pick_tl(0, mag ? 6 : 4, mag ? 7 : 5, 0, g.d[1].maxm);
-  c->tl_phi = pick_tl(1, mag ? 7 : 5, mag ? 8 : 6, 0, g.d[2].maxm);
-  c->tl_r = pick_tl(1, mag ? 7 : 5, mag ? 7 : 5, 5, g.d[0].maxm);
   for (int d = 0; d < 3; d++) {
     int m0 = g.d[d].size[0], same = 1;
     for (int b = 1; b < g.d[d].nb; b++) same &= (g.d[d].size[b] == m0);
     c->mt[d] = (same && (m0 == 16 || m0 == 32)) ? m0 : 0;
   }
+  auto pick = [](int mt, size_t (*f)(int, int, int), int mag, int m) {
+    if (mt) return 16;
+    for (int tl = 16; tl >= 1; tl /= 2)
+      if (f(mag, m, tl) <= kSmemCap) return tl;
+    return 1;
+  };
+  c->tl_theta = pick(c->mt[1], smem_theta_terms, mag, g.d[1].maxm);
+  c->tl_phi = pick(c->mt[2], smem_phi_terms, mag, g.d[2].maxm);
+  c->tl_r = pick(c->mt[0], smem_radial_terms, mag, g.d[0].maxm);
   *out = c;
   return CSS_OK;
 }
@@ -590,29 +641,26 @@ static int launch_rhs(css_ctx *c, const double *cur, double *nx, int stage, doub
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_THETA);
-  LAUNCH_MT(1, k_theta_terms, gt, smem_theta(mag ? 6 : 4, mag ? 7 : 5, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
-            TL);
+  LAUNCH_MT(1, k_theta_terms, gt, smem_theta_terms(mag, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
   prof_begin(c, KI_PHI);
-  LAUNCH_MT(2, k_phi_terms, gp, smem_line(mag ? 7 : 5, mag ? 8 : 6, 0, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
-            TL);
+  LAUNCH_MT(2, k_phi_terms, gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_RADIAL);
-  LAUNCH_MT(0, k_radial_terms, gr, smem_line(mag ? 7 : 5, mag ? 7 : 5, 5, g.d[0].maxm, TL), g, cur, c->bf, c->dv,
-            c->tbuf, TL);
+  LAUNCH_MT(0, k_radial_terms, gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_RHOT_UPDATE);
-  LAUNCH_MT(1, k_rhot_update, gu, smem_theta(1, 1, g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf,
-            stage, dtcur, TL, c->flag);
+  LAUNCH_MT(1, k_rhot_update, gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            TL, c->flag);
   prof_end(c);
   return check_launch(c);
 }

@@ -27,6 +27,7 @@ struct CssGeo {
   int tstride;              // length of one 1-based table array (maxm + 2)
   const double *tab;        // [.. bdry][g1|g2|g3][tstride]
   const int *rblk;          // radial block index of each global ir
+  const double *resp_r;     // [r block][lo|hi][tstride]: unit response of d/dr to the face datum of rho
   // radial profiles (length nr)
   const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
   // theta profiles (length nth)

@@ -89,33 +89,96 @@ __device__ __forceinline__ void load_r_tile(const CssGeo &g, const double *__res
   }
 }
 
+// copies the LU tables (g1|g2|g3, 1-based, m+2 each) of one block into dst
+__device__ __forceinline__ void stage_table(const CssGeo &g, int dir, int blk, int order, int bdry, int m,
+                                            double *dst) {
+  const double *src = tabp(g, dir, blk, order, bdry);
+  const int ts = m + 2;
+  for (int k = threadIdx.x; k < 3 * ts; k += blockDim.x) {
+    int a = k / ts, j = k - a * ts;
+    dst[k] = src[(size_t)a * g.tstride + j];
+  }
+}
+
+// plane offset of radius ir, line offset of (ip) inside a plane
+__device__ __forceinline__ size_t plane(const CssGeo &g, int ir) { return (size_t)ir * g.nth * g.nphi; }
+
+// theta tile: S[l*SR + j+4], lines = phi indices pb..pb+TL-1 of radius ir
+template <int MT, int TLC>
+__device__ __forceinline__ void tile_theta(const CssGeo &g, const double *__restrict__ f, double *S, int SR, int t0,
+                                           int m_, int pb, int TL_, int ir) {
+  const int m = MT ? MT : m_, TL = TLC ? TLC : TL_, w = m + 8;
+  const double *fp = f + plane(g, ir);
+  for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
+    int l = idx / w, jj = idx - l * w;
+    int gt = t0 + jj - 4, gp = pb + l;
+    if (gt < 0 || gt >= g.nth || gp >= g.nphi) continue;
+    S[l * SR + jj] = __ldg(fp + (size_t)gp * g.nth + gt);
+  }
+}
+
+// phi tile: S[(j+4)*SR + l], lines = theta indices tb..tb+TL-1, periodic phi
+template <int MT, int TLC>
+__device__ __forceinline__ void tile_phi(const CssGeo &g, const double *__restrict__ f, double *S, int SR, int p0,
+                                         int m_, int tb, int TL_, int ir) {
+  const int m = MT ? MT : m_, TL = TLC ? TLC : TL_, w = m + 8;
+  const double *fp = f + plane(g, ir);
+  for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
+    int jj = idx / TL, l = idx - jj * TL;
+    int gp = p0 + jj - 4, gt = tb + l;
+    if (gp < 0) gp += g.nphi;
+    else if (gp >= g.nphi) gp -= g.nphi;
+    if (gt >= g.nth) continue;
+    S[jj * SR + l] = __ldg(fp + (size_t)gp * g.nth + gt);
+  }
+}
+
+// r tile: S[(j+4)*SR + l], lines = theta indices tb..tb+TL-1 at phi ip
+template <int MT, int TLC>
+__device__ __forceinline__ void tile_r(const CssGeo &g, const double *__restrict__ f, double *S, int SR, int r0,
+                                       int m_, int tb, int TL_, int ip) {
+  const int m = MT ? MT : m_, TL = TLC ? TLC : TL_, w = m + 8;
+  const size_t ps = (size_t)g.nth * g.nphi;
+  const double *fp = f + (size_t)ip * g.nth + tb;
+  for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
+    int jj = idx / TL, l = idx - jj * TL;
+    int gr = r0 + jj - 4;
+    if (gr < 0 || gr >= g.nr || tb + l >= g.nth) continue;
+    S[jj * SR + l] = __ldg(fp + (size_t)gr * ps + l);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Source_Theta_Terms (rhs_mpi.f90:786-1029) + Induction_Terms (:2340-2346)
 // grid: x = theta block * nchunk + phi chunk, y = r.  cur = stage input
-// (vars1), B = curl A (MHD) in bf, dv = dvars1 (written, not read).
+// (vars1), B = curl A (MHD) in bf, dv = dvars1 (written, not read), tbuf =
+// the stage temperature (written here, read by the later kernels).
 // ---------------------------------------------------------------------------
-template <int MT>
+template <int MT, int TLC>
 __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__restrict__ cur,
                                                      const double *__restrict__ bf, double *__restrict__ dv,
-                                                     double *__restrict__ tbuf, int TL) {
+                                                     double *__restrict__ tbuf, int TLrt) {
   extern __shared__ double sm[];
+  const int TL = TLC ? TLC : TLrt;
   const int nchunk = (g.nphi + TL - 1) / TL;
   const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
   const int ir = blockIdx.y;
   const CssDir &D = g.d[1];
-  const int t0 = D.start[bt], m = D.size[bt];
+  const int t0 = D.start[bt], m = MT ? MT : D.size[bt];
   const int dtype = dtype_of(D, bt);
   const int mag = g.magnetic;
-  const int SR = m + 9, SO = m + 1;
+  const int SR = m + 9, SO = m + 1, TS = 3 * (m + 2);
   const size_t n = (size_t)g.ncell;
   const int nh = mag ? 6 : 4;   // w v u s [bp br]
-  double *H = sm;                       // nh * TL * SR
-  double *O = H + (size_t)nh * TL * SR;  // nd * TL * SO
+  const int nd = mag ? 7 : 5;   // dw dv du ds d2s [dbp dbr]
+  double *H = sm;
+  double *O = H + (size_t)nh * TL * SR;
+  double *Tb = O + (size_t)nd * TL * SO;
   const double *fld[6] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, bf + n, bf + 2 * n};
-  for (int k = 0; k < nh; k++) load_theta_tile(g, fld[k], H + (size_t)k * TL * SR, SR, t0, m, pb, TL, ir, true);
+  for (int k = 0; k < nh; k++) tile_theta<MT, TLC>(g, fld[k], H + (size_t)k * TL * SR, SR, t0, m, pb, TL, ir);
+  const int var[7] = {2, 3, 4, 5, 5, 8, 9};
+  for (int k = 0; k < nd; k++) stage_table(g, 1, bt, k == 4 ? 2 : 1, g.ibct[var[k]], m, Tb + k * TS);
   __syncthreads();
-  // solves: 0 dw, 1 dv, 2 du, 3 ds, 4 d2s, 5 dbp, 6 dbr
-  const int nd = mag ? 7 : 5;
   const double ri = g.r_inv[ir];
   for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
     int k = task / TL, l = task - k * TL;
@@ -124,8 +187,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
     int hk = (k <= 3) ? k : (k == 4 ? 3 : k - 1);
     const double *x = H + ((size_t)hk * TL + l) * SR + 4;
     double *o = O + ((size_t)k * TL + l) * SO;
-    int var = (k == 0) ? 2 : (k == 1) ? 3 : (k == 2) ? 4 : (k <= 4) ? 5 : (k == 5) ? 8 : 9;
-    int bdry = g.ibct[var];
+    int bdry = g.ibct[var[k]];
     double lo = 0.0, hi = 0.0;
     if (k == 1) {  // stress-free datum cot(theta)*v on the walls (rhs_mpi.f90:414, :444)
       if (D.lphys[bt]) lo = (g.cosines[0] / g.sines[0]) * x[0];
@@ -136,19 +198,20 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
       if (D.rphys[bt]) hi = -(g.cosines[g.nth - 1] / g.sines[g.nth - 1]) * x[m - 1];
     }
     if (k == 4)
-      solve<2, MT>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 2, bdry), g.tstride, dnum_d2_theta(g, ir),
-                    D.dnum[bt] * D.dnum[bt], 0, o, 1);
+      solve<2, MT>(x, 1, m, dtype, bdry, lo, hi, Tb + k * TS, m + 2, dnum_d2_theta(g, ir), D.dnum[bt] * D.dnum[bt],
+                   0, o, 1);
     else
-      solve<1, MT>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, D.dnum[bt], D.dnum[bt], 0, o, 1);
+      solve<1, MT>(x, 1, m, dtype, bdry, lo, hi, Tb + k * TS, m + 2, D.dnum[bt], D.dnum[bt], 0, o, 1);
   }
   __syncthreads();
   const double rv = g.r_ind[ir], epsr = g.eps[ir];
   const double omsq = rv * g.omega0 * g.omega0, om2 = 2.0 * g.omega0;
+  const size_t pl = plane(g, ir);
   for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
     int l = pt / m, j = pt - l * m;
     int it = t0 + j, ip = pb + l;
     if (ip >= g.nphi) continue;
-    size_t id = css_idx(g, it, ip, ir);
+    size_t id = pl + (size_t)ip * g.nth + it;
     double sn = g.sines[it], cs = g.cosines[it], ct = cs / sn;
     double rho = __ldg(cur + id);
     const double *hl = H + (size_t)l * SR + 4 + j;
@@ -173,7 +236,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
     w1 = ol[(size_t)2 * TL * SO] * ri;
     du = du - w * w1;
     double t = temp_of(g, rho, s);
-    tbuf[id] = t;  // the stage's temperature, read by the later kernels
+    tbuf[id] = t;
     double invrho = 1.0 / rho;
     double ds;
     if (fabs(epsr) > 0.0) ds = epsr * invrho / t;
@@ -222,52 +285,54 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
 // Phi_Terms (rhs_mpi.f90:1032-1261).  grid: x = phi block * nchunk + theta
 // chunk, y = r.
 // ---------------------------------------------------------------------------
-template <int MT>
+template <int MT, int TLC>
 __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__restrict__ cur,
                                                    const double *__restrict__ bf, double *__restrict__ dv,
-                                                   const double *__restrict__ tbuf, int TL) {
+                                                   const double *__restrict__ tbuf, int TLrt) {
   extern __shared__ double sm[];
+  const int TL = TLC ? TLC : TLrt;
   const int nchunk = (g.nth + TL - 1) / TL;
   const int bp = blockIdx.x / nchunk, tb = (blockIdx.x - bp * nchunk) * TL;
   const int ir = blockIdx.y;
   const CssDir &D = g.d[2];
-  const int p0 = D.start[bp], m = D.size[bp];
+  const int p0 = D.start[bp], m = MT ? MT : D.size[bp];
   const int mag = g.magnetic;
-  const int SR = TL + 1;
+  const int SR = TL + 1, TS = 3 * (m + 2);
   const size_t n = (size_t)g.ncell;
   const int nh = mag ? 7 : 5;  // rho v w u s [bt br]
+  const int nd = mag ? 8 : 6;  // drho dv dw du ds d2s [dbt dbr]
+  const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
   double *H = sm;
-  double *O = H + (size_t)nh * (m + 8) * SR;
+  double *O = H + nh * HS;
+  double *Tb = O + nd * OS;
   const double *fld[7] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n, bf, bf + 2 * n};
-  for (int k = 0; k < nh; k++) load_phi_tile(g, fld[k], H + (size_t)k * (m + 8) * SR, SR, p0, m, tb, TL, ir, true);
+  for (int k = 0; k < nh; k++) tile_phi<MT, TLC>(g, fld[k], H + k * HS, SR, p0, m, tb, TL, ir);
+  stage_table(g, 2, bp, 1, 0, m, Tb);
+  stage_table(g, 2, bp, 2, 0, m, Tb + TS);
   __syncthreads();
-  // solves: 0 drho 1 dv 2 dw 3 du 4 ds 5 d2s 6 dbt 7 dbr
-  const int nd = mag ? 8 : 6;
   for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
     int k = task / TL, l = task - k * TL;
     if (tb + l >= g.nth) continue;
     if (k == 5 && !g.slaplacian) continue;
     int hk = (k <= 4) ? k : (k == 5 ? 4 : k - 1);
-    const double *x = H + (size_t)hk * (m + 8) * SR + 4 * SR + l;
-    double *o = O + (size_t)k * m * SR + l;
+    const double *x = H + hk * HS + 4 * SR + l;
+    double *o = O + k * OS + l;
     if (k == 5)
-      solve<2, MT>(x, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 2, 0), g.tstride, D.dnum[bp], D.dnum[bp] * D.dnum[bp], 1,
-                    o, SR);
+      solve<2, MT>(x, SR, m, 3, 0, 0.0, 0.0, Tb + TS, m + 2, D.dnum[bp], D.dnum[bp] * D.dnum[bp], 1, o, SR);
     else
-      solve<1, MT>(x, SR, m, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, D.dnum[bp], D.dnum[bp], 1, o, SR);
+      solve<1, MT>(x, SR, m, 3, 0, 0.0, 0.0, Tb, m + 2, D.dnum[bp], D.dnum[bp], 1, o, SR);
   }
   __syncthreads();
   const double ri = g.r_inv[ir];
+  const size_t pl = plane(g, ir);
   for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
     int j = pt / TL, l = pt - j * TL;
     int it = tb + l, ip = p0 + j;
     if (it >= g.nth) continue;
-    size_t id = css_idx(g, it, ip, ir);
+    size_t id = pl + (size_t)ip * g.nth + it;
     const double *hl = H + (size_t)(j + 4) * SR + l;
-    const size_t HS = (size_t)(m + 8) * SR;
     double rho = hl[0], v = hl[HS];
     const double *ol = O + (size_t)j * SR + l;
-    const size_t OS = (size_t)m * SR;
     double cscth = 1.0 / g.sines[it];
     double oors = ri * cscth;
     double t = __ldg(tbuf + id), oorho = 1.0 / rho;
@@ -311,43 +376,99 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__res
   }
 }
 
+// pointwise Radial_Terms (rhs_mpi.f90:1302-1517) for one point: updates
+// drho, dw, dv, du, ds (in: the values accumulated so far)
+struct RadIn {
+  double u, rho, t, dw_r, dv_r, du_r, ds_r, d2s_r, bt, bp, br, dbt_r, dbp_r;
+};
+__device__ __forceinline__ void radial_point(const CssGeo &g, int ir, const RadIn &q, double &drho, double &dw,
+                                             double &dvv, double &du, double &ds) {
+  const int nu = g.non_uniform;
+  const double w3 = g.dxdr[ir];
+  const double invrho = 1.0 / q.rho;
+  double w1 = q.dw_r;
+  if (nu) w1 = w1 * w3;
+  dw = dw - q.u * w1;
+  w1 = q.dv_r;
+  if (nu) w1 = w1 * w3;
+  dvv = dvv - q.u * w1;
+  w1 = q.du_r;
+  if (nu) w1 = w1 * w3;
+  du = du - q.u * w1;
+  drho = drho - q.rho * w1;
+  w1 = q.ds_r;
+  if (nu) w1 = w1 * w3;
+  du = du - g.gamm1 * q.t * w1;
+  ds = ds - q.u * w1;
+  if (g.slaplacian) {
+    double oorho = invrho / q.t;
+    double work6 = (2.0 * g.r_inv[ir] + g.dlnks[ir]) * g.ks[ir];
+    w1 = w1 * oorho;
+    ds = ds + w1 * work6;
+    if (nu) ds = ds + (g.d2xdr2[ir] / w3) * w1 * g.ks[ir];
+    double d2 = q.d2s_r;
+    if (nu) d2 = d2 * (w3 * w3);
+    ds = ds + g.ks[ir] * d2 * oorho;
+  }
+  if (g.magnetic) {
+    double oo = invrho * ONE_OVER_4PI;
+    w1 = q.dbt_r;
+    if (nu) w1 = w1 * w3;
+    w1 = w1 * oo;
+    du = du - q.bt * w1;
+    dw = dw + q.br * w1;
+    w1 = q.dbp_r;
+    if (nu) w1 = w1 * w3;
+    w1 = w1 * oo;
+    dvv = dvv + q.br * w1;
+    du = du - q.bp * w1;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Radial_Terms (rhs_mpi.f90:1264-1519) + Density_Terms_Radial (:1710-1855)
 // grid: x = r block * nchunk + theta chunk, y = phi.
+// d(rho)/dr on a block with a physical face is linear in the face datum
+// (the hydrostatic condition built from the completed du/dt on that face):
+// it is solved with a zero datum together with the other derivatives and
+// the datum times the block's unit response (resp) is added afterwards.
 // ---------------------------------------------------------------------------
-template <int MT>
+template <int MT, int TLC>
 __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__restrict__ cur,
                                                       const double *__restrict__ bf, double *__restrict__ dv,
-                                                      const double *__restrict__ tbuf, int TL) {
+                                                      const double *__restrict__ tbuf, int TLrt) {
   extern __shared__ double sm[];
+  const int TL = TLC ? TLC : TLrt;
   const int nchunk = (g.nth + TL - 1) / TL;
   const int br = blockIdx.x / nchunk, tb = (blockIdx.x - br * nchunk) * TL;
   const int ip = blockIdx.y;
   const CssDir &D = g.d[0];
-  const int r0 = D.start[br], m = D.size[br];
+  const int r0 = D.start[br], m = MT ? MT : D.size[br];
   const int dtype = dtype_of(D, br);
-  const int mag = g.magnetic, nu = g.non_uniform;
-  const int SR = TL + 1;
+  const int mag = g.magnetic;
+  const int SR = TL + 1, TS = 3 * (m + 2);
   const size_t n = (size_t)g.ncell;
   const int nh = mag ? 7 : 5;  // w v u s rho [bt bp]
+  const int nd = mag ? 8 : 6;  // dw dv du ds d2s drho0 [dbt dbp]
   const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
   double *H = sm;
-  double *O = H + nh * HS;            // nd derivative buffers
-  const int nd = mag ? 7 : 5;         // dw dv du ds d2s [dbt dbp]; slot 0 reused for drho
-  double *A = O + nd * OS;            // 5 accumulators (dvars 0..4)
+  double *O = H + nh * HS;
+  double *Tb = O + nd * OS;
+  double *datum = Tb + nd * TS;
   const double *fld[7] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, cur, bf, bf + n};
-  for (int k = 0; k < nh; k++) load_r_tile(g, fld[k], H + k * HS, SR, r0, m, tb, TL, ip, true);
+  for (int k = 0; k < nh; k++) tile_r<MT, TLC>(g, fld[k], H + k * HS, SR, r0, m, tb, TL, ip);
+  const int var[8] = {2, 3, 4, 5, 5, 1, 7, 8};
+  for (int k = 0; k < nd; k++) stage_table(g, 0, br, k == 4 ? 2 : 1, g.ibcr[var[k]], m, Tb + k * TS);
   __syncthreads();
   const int nr = g.nr;
   for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
     int k = task / TL, l = task - k * TL;
     if (tb + l >= g.nth) continue;
     if (k == 4 && !g.slaplacian) continue;
-    int hk = (k <= 3) ? k : (k == 4 ? 3 : k);  // d2s uses s; dbt -> 5, dbp -> 6
+    int hk = (k <= 3) ? k : (k == 4 ? 3 : (k == 5 ? 4 : k - 1));
     const double *x = H + hk * HS + 4 * SR + l;
     double *o = O + k * OS + l;
-    int var = (k == 0) ? 2 : (k == 1) ? 3 : (k == 2) ? 4 : (k <= 4) ? 5 : (k == 5) ? 7 : 8;
-    int bdry = g.ibcr[var];
+    int bdry = g.ibcr[var[k]];
     double lo = 0.0, hi = 0.0;
     if (k == 0 || k == 1) {  // stress-free datum w/r/dxdr (rhs_mpi.f90:578-614)
       if (D.lphys[br] && g.bottom_stress_free) lo = x[0] / g.r1 / g.dxdr[0];
@@ -361,120 +482,68 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
       hi = g.s_flux_hi;
     }
     if (k == 4)
-      solve<2, MT>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 2, bdry), g.tstride, D.dnum[br],
-                    D.dnum[br] * D.dnum[br], 0, o, SR);
+      solve<2, MT>(x, SR, m, dtype, bdry, lo, hi, Tb + k * TS, m + 2, D.dnum[br], D.dnum[br] * D.dnum[br], 0, o, SR);
     else
-      solve<1, MT>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, D.dnum[br], D.dnum[br], 0, o,
-                    SR);
+      solve<1, MT>(x, SR, m, dtype, bdry, lo, hi, Tb + k * TS, m + 2, D.dnum[br], D.dnum[br], 0, o, SR);
   }
   __syncthreads();
-  // radial terms
-  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
-    int j = pt / TL, l = pt - j * TL;
-    int it = tb + l, ir = r0 + j;
-    if (it >= g.nth) continue;
-    size_t id = css_idx(g, it, ip, ir);
+  const size_t ps = (size_t)g.nth * g.nphi;
+  const size_t base = (size_t)ip * g.nth + tb;
+  auto gather = [&](int j, int l, RadIn &q) {
     const double *hl = H + (size_t)(j + 4) * SR + l;
-    double u = hl[2 * HS], rho = hl[4 * HS];
     const double *ol = O + (size_t)j * SR + l;
-    double w3 = g.dxdr[ir];
-    double t = __ldg(tbuf + id), invrho = 1.0 / rho;
-    double w1 = ol[0];
-    if (nu) w1 = w1 * w3;
-    double dw = dv[n + id];
-    dw = dw - u * w1;
-    w1 = ol[OS];
-    if (nu) w1 = w1 * w3;
-    double dvv = dv[2 * n + id];
-    dvv = dvv - u * w1;
-    double du = dv[3 * n + id];
-    w1 = ol[2 * OS];
-    if (nu) w1 = w1 * w3;
-    du = du - u * w1;
-    double drho = dv[id];
-    drho = drho - rho * w1;
-    double ds = dv[4 * n + id];
-    w1 = ol[3 * OS];
-    if (nu) w1 = w1 * w3;
-    du = du - g.gamm1 * t * w1;
-    ds = ds - u * w1;
-    if (g.slaplacian) {
-      double oorho = invrho / t;
-      double work6 = (2.0 * g.r_inv[ir] + g.dlnks[ir]) * g.ks[ir];
-      w1 = w1 * oorho;
-      ds = ds + w1 * work6;
-      if (nu) ds = ds + (g.d2xdr2[ir] / w3) * w1 * g.ks[ir];
-      double d2 = ol[4 * OS];
-      if (nu) d2 = d2 * (w3 * w3);
-      ds = ds + g.ks[ir] * d2 * oorho;
-    }
+    size_t id = base + (size_t)(r0 + j) * ps + l;
+    q.u = hl[2 * HS];
+    q.rho = hl[4 * HS];
+    q.t = __ldg(tbuf + id);
+    q.dw_r = ol[0]; q.dv_r = ol[OS]; q.du_r = ol[2 * OS]; q.ds_r = ol[3 * OS]; q.d2s_r = ol[4 * OS];
     if (mag) {
-      double oo = invrho * ONE_OVER_4PI;
-      double bt_ = hl[5 * HS], bp_ = hl[6 * HS], br_ = __ldg(bf + 2 * n + id);
-      w1 = ol[5 * OS];
-      if (nu) w1 = w1 * w3;
-      w1 = w1 * oo;
-      du = du - bt_ * w1;
-      dw = dw + br_ * w1;
-      w1 = ol[6 * OS];
-      if (nu) w1 = w1 * w3;
-      w1 = w1 * oo;
-      dvv = dvv + br_ * w1;
-      du = du - bp_ * w1;
+      q.bt = hl[5 * HS]; q.bp = hl[6 * HS]; q.br = __ldg(bf + 2 * n + id);
+      q.dbt_r = ol[6 * OS]; q.dbp_r = ol[7 * OS];
     }
-    double *al = A + (size_t)j * SR + l;
-    al[0] = drho;
-    al[OS] = dw;
-    al[2 * OS] = dvv;
-    al[3 * OS] = du;
-    al[4 * OS] = ds;
-  }
-  __syncthreads();
-  // density radial: BC datum from the completed du on the physical face
-  for (int l = threadIdx.x; l < TL; l += blockDim.x) {
-    if (tb + l >= g.nth) continue;
-    const double *x = H + 4 * HS + 4 * SR + l;  // rho
-    double lo = 0.0, hi = 0.0;
-    if (D.lphys[br]) {
-      double rho = x[0], t = __ldg(tbuf + css_idx(g, tb + l, ip, r0));
-      double du = A[3 * OS + l];
-      if (g.lbcr_rho == 2 || g.lbcr_rho == 4) lo = du * rho * g.invpconst / t;
-      else lo = rho;
-      if (nu) lo = lo / g.dxdr[0];
-    } else if (D.rphys[br]) {
-      double rho = x[(m - 1) * SR], t = __ldg(tbuf + css_idx(g, tb + l, ip, r0 + m - 1));
-      double du = A[3 * OS + (size_t)(m - 1) * SR + l];
-      if (g.lbcr_rho == 3 || g.lbcr_rho == 4) hi = du * rho * g.invpconst / t;
-      else hi = rho;
-      if (nu) hi = hi / g.dxdr[nr - 1];
+    return id;
+  };
+  // hydrostatic datum of d(rho)/dr on a physical face (rhs_mpi.f90:1750-1768)
+  const int phys = D.lphys[br] ? 1 : (D.rphys[br] ? 2 : 0);
+  if (phys) {
+    for (int l = threadIdx.x; l < TL; l += blockDim.x) {
+      if (tb + l >= g.nth) continue;
+      int j = phys == 1 ? 0 : m - 1;
+      RadIn q;
+      size_t id = gather(j, l, q);
+      double drho = dv[id], dw = dv[n + id], dvv = dv[2 * n + id], du = dv[3 * n + id], ds = dv[4 * n + id];
+      radial_point(g, r0 + j, q, drho, dw, dvv, du, ds);
+      double d;
+      if (g.lbcr_rho == 4 || g.lbcr_rho == (phys == 1 ? 2 : 3)) d = du * q.rho * g.invpconst / q.t;
+      else d = q.rho;
+      if (g.non_uniform) d = d / g.dxdr[phys == 1 ? 0 : nr - 1];
+      datum[l] = d;
     }
-    int bdry = g.ibcr[1];
-    solve<1, MT>(x, SR, m, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, D.dnum[br], D.dnum[br], 0,
-                  O + l, SR);
+    __syncthreads();
   }
-  __syncthreads();
+  const double *resp = g.resp_r + (size_t)(2 * br + (phys == 2 ? 1 : 0)) * g.tstride;
   for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
     int j = pt / TL, l = pt - j * TL;
-    int it = tb + l, ir = r0 + j;
-    if (it >= g.nth) continue;
-    size_t id = css_idx(g, it, ip, ir);
-    const double *hl = H + (size_t)(j + 4) * SR + l;
-    double u = hl[2 * HS], rho = hl[4 * HS];
-    double t = __ldg(tbuf + id), invrho = 1.0 / rho;
-    const double *al = A + (size_t)j * SR + l;
-    double w1 = O[(size_t)j * SR + l];
-    if (nu) w1 = w1 * g.dxdr[ir];
-    double drho = al[0] - u * w1;
-    w1 = w1 * invrho;
-    double du = al[3 * OS] - g.pconst * t * w1;
-    double ds = al[4 * OS];
-    if (D.rphys[br] && j == m - 1 && !g.set_stop) {  // rhs_mpi.f90:1807-1818
-      drho = drho + rho * (g.t0 - t) / (g.damping_time * (g.gamma - 2.0) * t);
-      ds = ds - g.cv * (g.t0 - t) / (g.damping_time * (g.gamma - 2.0) * t);
+    int ir = r0 + j;
+    if (tb + l >= g.nth) continue;
+    RadIn q;
+    size_t id = gather(j, l, q);
+    double drho = dv[id], dw = dv[n + id], dvv = dv[2 * n + id], du = dv[3 * n + id], ds = dv[4 * n + id];
+    radial_point(g, ir, q, drho, dw, dvv, du, ds);
+    // Density_Terms_Radial
+    double w1 = O[5 * OS + (size_t)j * SR + l];
+    if (phys) w1 = w1 + datum[l] * resp[j + 1];
+    if (g.non_uniform) w1 = w1 * g.dxdr[ir];
+    drho = drho - q.u * w1;
+    w1 = w1 * (1.0 / q.rho);
+    du = du - g.pconst * q.t * w1;
+    if (phys == 2 && j == m - 1 && !g.set_stop) {  // rhs_mpi.f90:1807-1818
+      drho = drho + q.rho * (g.t0 - q.t) / (g.damping_time * (g.gamma - 2.0) * q.t);
+      ds = ds - g.cv * (g.t0 - q.t) / (g.damping_time * (g.gamma - 2.0) * q.t);
     }
     dv[id] = drho;
-    dv[n + id] = al[OS];
-    dv[2 * n + id] = al[2 * OS];
+    dv[n + id] = dw;
+    dv[2 * n + id] = dvv;
     dv[3 * n + id] = du;
     dv[4 * n + id] = ds;
   }
@@ -489,41 +558,42 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
 //   stage 2,3: vs = vs + dv/3;            nx = v0 + dtcur*dv
 //   stage 4: vs = vs + dv/6;              nx = v0 + dtcur*vs  (nx may be v0)
 // ---------------------------------------------------------------------------
-template <int MT>
+template <int MT, int TLC>
 __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__restrict__ cur,
                                                      double *__restrict__ dv, const double *v0, double *vs, double *nx,
-                                                     const double *__restrict__ tbuf, int stage, double dtcur, int TL,
-                                                     int *flag) {
+                                                     const double *__restrict__ tbuf, int stage, double dtcur,
+                                                     int TLrt, int *flag) {
   extern __shared__ double sm[];
+  const int TL = TLC ? TLC : TLrt;
   const int nchunk = (g.nphi + TL - 1) / TL;
   const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
   const int ir = blockIdx.y;
   const CssDir &D = g.d[1];
-  const int t0 = D.start[bt], m = D.size[bt];
+  const int t0 = D.start[bt], m = MT ? MT : D.size[bt];
   const int dtype = dtype_of(D, bt);
-  const int SR = m + 9, SO = m + 1;
+  const int SR = m + 9, SO = m + 1, TS = 3 * (m + 2);
   const size_t n = (size_t)g.ncell;
   double *H = sm;
   double *O = H + (size_t)TL * SR;
-  load_theta_tile(g, cur, H, SR, t0, m, pb, TL, ir, true);
+  double *Tb = O + (size_t)TL * SO;
+  tile_theta<MT, TLC>(g, cur, H, SR, t0, m, pb, TL, ir);
+  const int bdry = g.ibct[1];
+  stage_table(g, 1, bt, 1, bdry, m, Tb);
   __syncthreads();
   const double rvv = g.r_ind[ir] * g.invpconst, ri = g.r_inv[ir];
+  const size_t pl = plane(g, ir);
   for (int l = threadIdx.x; l < TL; l += blockDim.x) {
     if (pb + l >= g.nphi) continue;
     const double *x = H + (size_t)l * SR + 4;
     double lo = 0.0, hi = 0.0;
     if (D.lphys[bt]) {  // rhs_mpi.f90:1553-1555: make dw = 0 on the wall
-      size_t id = css_idx(g, t0, pb + l, ir);
-      double rho = x[0], t = __ldg(tbuf + id);
-      lo = rvv * dv[n + id] * rho / t;
+      size_t id = pl + (size_t)(pb + l) * g.nth + t0;
+      lo = rvv * dv[n + id] * x[0] / __ldg(tbuf + id);
     } else if (D.rphys[bt]) {
-      size_t id = css_idx(g, t0 + m - 1, pb + l, ir);
-      double rho = x[m - 1], t = __ldg(tbuf + id);
-      hi = rvv * dv[n + id] * rho / t;
+      size_t id = pl + (size_t)(pb + l) * g.nth + t0 + m - 1;
+      hi = rvv * dv[n + id] * x[m - 1] / __ldg(tbuf + id);
     }
-    int bdry = g.ibct[1];
-    solve<1, MT>(x, 1, m, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, D.dnum[bt], D.dnum[bt], 0,
-                  O + (size_t)l * SO, 1);
+    solve<1, MT>(x, 1, m, dtype, bdry, lo, hi, Tb, m + 2, D.dnum[bt], D.dnum[bt], 0, O + (size_t)l * SO, 1);
   }
   __syncthreads();
   const int nv = g.nv;
@@ -532,7 +602,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
     int l = pt / m, j = pt - l * m;
     int it = t0 + j, ip = pb + l;
     if (ip >= g.nphi) continue;
-    size_t id = css_idx(g, it, ip, ir);
+    size_t id = pl + (size_t)ip * g.nth + it;
     double rho = H[(size_t)l * SR + 4 + j];
     double w = __ldg(cur + n + id);
     double t = __ldg(tbuf + id);
@@ -546,6 +616,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
       dv[n + id] = d1;
       continue;
     }
+    const bool twall = (it == 0 || it == g.nth - 1), rlo = (ir == 0), rhi = (ir == g.nr - 1);
     for (int iv = 0; iv < nv; iv++) {
       size_t q = (size_t)iv * n + id;
       double d = (iv == 0) ? d0 : (iv == 1) ? d1 : dv[q];
@@ -563,29 +634,31 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
         o = a + dtcur * d;
       }
       // Bound (rhs_mpi.f90:2395-2491)
-      if (iv == 1 && (it == 0 || it == g.nth - 1)) o = 0.0;
-      if (iv == 3 && !g.theta_stress_free && (it == 0 || it == g.nth - 1)) o = 0.0;
-      if (ir == 0) {
-        if ((iv == 1 || iv == 2) && !g.bottom_stress_free) o = 0.0;
-        if (iv == 3) o = 0.0;
-      }
-      if (ir == g.nr - 1) {
-        if ((iv == 1 || iv == 2) && !g.top_stress_free) o = 0.0;
-        if (iv == 3) o = 0.0;
-      }
-      if (iv >= 5) {
-        if (g.theta_perf_conductor) {
-          if ((iv == 6 || iv == 7) && (it == 0 || it == g.nth - 1)) o = 0.0;
-        } else if (iv == 5 && (it == 0 || it == g.nth - 1)) {
-          o = 0.0;
+      if (twall || rlo || rhi) {
+        if (iv == 1 && twall) o = 0.0;
+        if (iv == 3 && !g.theta_stress_free && twall) o = 0.0;
+        if (rlo) {
+          if ((iv == 1 || iv == 2) && !g.bottom_stress_free) o = 0.0;
+          if (iv == 3) o = 0.0;
         }
-        if (ir == 0) {
-          if (g.bottom_radial_field) { if (iv == 7) o = 0.0; }
-          else if (g.bottom_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+        if (rhi) {
+          if ((iv == 1 || iv == 2) && !g.top_stress_free) o = 0.0;
+          if (iv == 3) o = 0.0;
         }
-        if (ir == g.nr - 1) {
-          if (g.top_radial_field) { if (iv == 7) o = 0.0; }
-          else if (g.top_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+        if (iv >= 5) {
+          if (g.theta_perf_conductor) {
+            if ((iv == 6 || iv == 7) && twall) o = 0.0;
+          } else if (iv == 5 && twall) {
+            o = 0.0;
+          }
+          if (rlo) {
+            if (g.bottom_radial_field) { if (iv == 7) o = 0.0; }
+            else if (g.bottom_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+          }
+          if (rhi) {
+            if (g.top_radial_field) { if (iv == 7) o = 0.0; }
+            else if (g.top_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+          }
         }
       }
       if (!isfinite(o)) bad = 1;
@@ -600,7 +673,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
 // (theta, phi, r).  Three kernels, one per sweep direction; the r sweep
 // optionally applies Compute_B's boundary zeroing (:1842-1883).
 // ---------------------------------------------------------------------------
-template <int MT>
+template <int MT, int TLC>
 __global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
                                                     int TL) {
   extern __shared__ double sm[];
@@ -643,7 +716,7 @@ __global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__re
   }
 }
 
-template <int MT>
+template <int MT, int TLC>
 __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
                                                   int TL) {
   extern __shared__ double sm[];
@@ -679,7 +752,7 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__rest
   }
 }
 
-template <int MT>
+template <int MT, int TLC>
 __global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
                                                 int TL, int apply_bc) {
   extern __shared__ double sm[];

@@ -175,96 +175,85 @@ __device__ __forceinline__ void line_solve(const double *__restrict__ x, int sx,
     rm1 = d2_row_hi1(x, sx, m, dtype);
     rm = d2_row_hi2(x, sx, m, dtype, bdry, bchi, dnum);
   }
-  double t = __ldg(g2 + 1) * r1;
+  double t = g2[1] * r1;
   out[0] = t;
   if (phi) {
-    t = __ldg(g2 + 2) * (r2 + a1 * t);
+    t = g2[2] * (r2 + a1 * t);
     out[so] = t;
     for (int j = 3; j <= m - 2; j++) {
       double d = (ORDER == 1) ? d1_row_int(x, sx, j) : d2_row_int(x, sx, j);
-      t = __ldg(g2 + j) * (d + a1 * t);
+      t = g2[j] * (d + a1 * t);
       out[(j - 1) * so] = t;
     }
-    t = __ldg(g2 + m - 1) * (rm1 + a1 * t);
+    t = g2[m - 1] * (rm1 + a1 * t);
     out[(m - 2) * so] = t;
-    t = __ldg(g2 + m) * (rm + a1 * t);
+    t = g2[m] * (rm + a1 * t);
   } else {
-    t = __ldg(g2 + 2) * r2 + __ldg(g3 + 2) * t;
+    t = g2[2] * r2 + g3[2] * t;
     out[so] = t;
     for (int j = 3; j <= m - 2; j++) {
       double d = (ORDER == 1) ? d1_row_int(x, sx, j) : d2_row_int(x, sx, j);
-      t = __ldg(g2 + j) * (d + a1 * t);
+      t = g2[j] * (d + a1 * t);
       out[(j - 1) * so] = t;
     }
-    t = __ldg(g2 + m - 1) * rm1 + __ldg(g3 + m - 1) * t;
+    t = g2[m - 1] * rm1 + g3[m - 1] * t;
     out[(m - 2) * so] = t;
-    t = __ldg(g2 + m) * rm + __ldg(g3 + m) * t;
+    t = g2[m] * rm + g3[m] * t;
   }
   double sol = t;
   out[(m - 1) * so] = scale * sol;
   for (int j = m - 1; j >= 1; j--) {
-    sol = out[(j - 1) * so] + __ldg(g1 + j + 1) * sol;
+    sol = out[(j - 1) * so] + g1[j + 1] * sol;
     out[(j - 1) * so] = scale * sol;
   }
 }
 
 // Same operator with the block length M known at compile time: the sweeps
-// are fully unrolled, the forward values stay in registers and every input
-// point is read from shared memory once.  Identical arithmetic to
-// line_solve (same rows, same sweep form), so the two agree bit for bit.
+// are fully unrolled (the forward values go through the output buffer, so
+// register use stays low); identical arithmetic to line_solve.
 template <int ORDER, int M>
 __device__ __forceinline__ void line_solve_u(const double *__restrict__ x, int sx, int dtype, int bdry, double bclo,
                                              double bchi, const double *__restrict__ G, int ts, double dnum,
                                              double scale, int phi, double *__restrict__ out, int so) {
   const double *g1 = G, *g2 = G + ts, *g3 = G + 2 * ts;
   const double a1 = (ORDER == 1) ? -1.0 / 3.0 : -2.0 / 11.0;
-  double xs[M + 8];
-#pragma unroll
-  for (int j = 0; j < M + 8; j++) {
-    // halo slots of a physical end are never read by the physical rows
-    bool halo = j < 4 || j >= M + 4;
-    bool need = !halo || (j < 4 ? (dtype == 1 || dtype == 3) : (dtype == 2 || dtype == 3));
-    xs[j] = need ? x[(j - 4) * sx] : 0.0;
-  }
-  const double *xr = xs + 4;  // xr[(j-1)] is point j
   double r1, r2, rm1, rm;
   if (ORDER == 1) {
-    r2 = d1_row_lo2(xr, 1, dtype);
-    r1 = d1_row_lo1(xr, 1, dtype, bdry, bclo, dnum, r2);
-    rm1 = d1_row_hi1(xr, 1, M, dtype);
-    rm = d1_row_hi2(xr, 1, M, dtype, bdry, bchi, dnum, rm1);
+    r2 = d1_row_lo2(x, sx, dtype);
+    r1 = d1_row_lo1(x, sx, dtype, bdry, bclo, dnum, r2);
+    rm1 = d1_row_hi1(x, sx, M, dtype);
+    rm = d1_row_hi2(x, sx, M, dtype, bdry, bchi, dnum, rm1);
   } else {
-    r1 = d2_row_lo1(xr, 1, dtype, bdry, bclo, dnum);
-    r2 = d2_row_lo2(xr, 1, dtype);
-    rm1 = d2_row_hi1(xr, 1, M, dtype);
-    rm = d2_row_hi2(xr, 1, M, dtype, bdry, bchi, dnum);
+    r1 = d2_row_lo1(x, sx, dtype, bdry, bclo, dnum);
+    r2 = d2_row_lo2(x, sx, dtype);
+    rm1 = d2_row_hi1(x, sx, M, dtype);
+    rm = d2_row_hi2(x, sx, M, dtype, bdry, bchi, dnum);
   }
-  double t[M];
-  t[0] = __ldg(g2 + 1) * r1;
+  double t = g2[1] * r1;
+  out[0] = t;
+  if (phi) t = g2[2] * (r2 + a1 * t);
+  else t = g2[2] * r2 + g3[2] * t;
+  out[so] = t;
+#pragma unroll
+  for (int j = 3; j <= M - 2; j++) {
+    double d = (ORDER == 1) ? d1_row_int(x, sx, j) : d2_row_int(x, sx, j);
+    t = g2[j] * (d + a1 * t);
+    out[(j - 1) * so] = t;
+  }
   if (phi) {
-    t[1] = __ldg(g2 + 2) * (r2 + a1 * t[0]);
-#pragma unroll
-    for (int j = 3; j <= M - 2; j++) {
-      double d = (ORDER == 1) ? d1_row_int(xr, 1, j) : d2_row_int(xr, 1, j);
-      t[j - 1] = __ldg(g2 + j) * (d + a1 * t[j - 2]);
-    }
-    t[M - 2] = __ldg(g2 + M - 1) * (rm1 + a1 * t[M - 3]);
-    t[M - 1] = __ldg(g2 + M) * (rm + a1 * t[M - 2]);
+    t = g2[M - 1] * (rm1 + a1 * t);
+    out[(M - 2) * so] = t;
+    t = g2[M] * (rm + a1 * t);
   } else {
-    t[1] = __ldg(g2 + 2) * r2 + __ldg(g3 + 2) * t[0];
-#pragma unroll
-    for (int j = 3; j <= M - 2; j++) {
-      double d = (ORDER == 1) ? d1_row_int(xr, 1, j) : d2_row_int(xr, 1, j);
-      t[j - 1] = __ldg(g2 + j) * (d + a1 * t[j - 2]);
-    }
-    t[M - 2] = __ldg(g2 + M - 1) * rm1 + __ldg(g3 + M - 1) * t[M - 3];
-    t[M - 1] = __ldg(g2 + M) * rm + __ldg(g3 + M) * t[M - 2];
+    t = g2[M - 1] * rm1 + g3[M - 1] * t;
+    out[(M - 2) * so] = t;
+    t = g2[M] * rm + g3[M] * t;
   }
-  double sol = t[M - 1];
+  double sol = t;
   out[(M - 1) * so] = scale * sol;
 #pragma unroll
   for (int j = M - 1; j >= 1; j--) {
-    sol = t[j - 1] + __ldg(g1 + j + 1) * sol;
+    sol = out[(j - 1) * so] + g1[j + 1] * sol;
     out[(j - 1) * so] = scale * sol;
   }
 }
