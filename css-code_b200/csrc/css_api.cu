@@ -217,14 +217,6 @@ static size_t smem_line(int nh, int nd, int na, int m, int TL) {
 }
 static const size_t kSmemCap = 100 * 1024;
 
-static int pick_tl(int kind, int nh, int nd, int na, int m) {
-  for (int tl = 16; tl >= 1; tl /= 2) {
-    size_t s = kind == 0 ? smem_theta(nh, nd, m, tl) : smem_line(nh, nd, na, m, tl);
-    if (s <= kSmemCap) return tl;
-  }
-  return 1;
-}
-
 extern "C" void css_destroy(css_ctx *c) {
   if (!c) return;
   cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo); cudaFree(c->resp);

@@ -325,53 +325,77 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__res
   __syncthreads();
   const double ri = g.r_inv[ir];
   const size_t pl = plane(g, ir);
-  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
-    int j = pt / TL, l = pt - j * TL;
-    int it = tb + l, ip = p0 + j;
-    if (it >= g.nth) continue;
-    size_t id = pl + (size_t)ip * g.nth + it;
-    const double *hl = H + (size_t)(j + 4) * SR + l;
-    double rho = hl[0], v = hl[HS];
-    const double *ol = O + (size_t)j * SR + l;
-    double cscth = 1.0 / g.sines[it];
-    double oors = ri * cscth;
-    double t = __ldg(tbuf + id), oorho = 1.0 / rho;
-    double w1 = ol[0] * oors;
-    double drho = dv[id];
-    double dvv = dv[2 * n + id];
-    drho = drho - v * w1;
-    dvv = dvv - g.pconst * w1 * t * oorho;
-    double ds = dv[4 * n + id];
-    w1 = ol[OS] * oors;
-    dvv = dvv - v * w1;
-    dv[id] = drho - rho * w1;
-    double dw = dv[n + id];
-    w1 = ol[2 * OS] * oors;
-    dw = dw - v * w1;
-    double du = dv[3 * n + id];
-    w1 = ol[3 * OS] * oors;
-    du = du - v * w1;
-    w1 = ol[4 * OS] * oors;
-    ds = ds - v * w1;
-    dvv = dvv - g.gamm1 * t * w1;
-    if (g.slaplacian) {
-      w1 = ol[5 * OS] * (oors * oors);
-      ds = ds + g.ks[ir] * w1 * (oorho / t);
+  // points per thread; the loads of all of a thread's points are issued
+  // before any store (dv is read and written, so the compiler cannot move
+  // loads across the stores by itself)
+  constexpr int PPT = (MT > 0 && TLC > 0) ? (MT * TLC + 127) / 128 : 1;
+  for (int pt0 = threadIdx.x; pt0 < TL * m; pt0 += PPT * blockDim.x) {
+    double in_[PPT][6];
+    size_t ids[PPT];
+    bool ok[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      int pt = pt0 + k * blockDim.x;
+      int j = pt / TL, l = pt - j * TL;
+      ok[k] = pt < TL * m && tb + l < g.nth;
+      ids[k] = pl + (size_t)(p0 + j) * g.nth + tb + l;
+      if (ok[k]) {
+        size_t id = ids[k];
+        in_[k][0] = dv[id]; in_[k][1] = dv[n + id]; in_[k][2] = dv[2 * n + id];
+        in_[k][3] = dv[3 * n + id]; in_[k][4] = dv[4 * n + id]; in_[k][5] = __ldg(tbuf + id);
+      }
     }
-    dv[4 * n + id] = ds;
-    if (!mag) {
-      dv[n + id] = dw;
-      dv[3 * n + id] = du;
-      dv[2 * n + id] = dvv;
-    } else {
-      double oo = ONE_OVER_4PI * oorho * oors;
-      double bt_ = hl[5 * HS], br_ = hl[6 * HS], bp_ = __ldg(bf + n + id);
-      w1 = ol[6 * OS] * oo;
-      dvv = dvv - bt_ * w1;
-      dv[n + id] = dw + bp_ * w1;
-      w1 = ol[7 * OS] * oo;
-      dv[2 * n + id] = dvv - br_ * w1;
-      dv[3 * n + id] = du + bp_ * w1;
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      if (!ok[k]) continue;
+      int pt = pt0 + k * blockDim.x;
+      int j = pt / TL, l = pt - j * TL;
+      int it = tb + l;
+      size_t id = ids[k];
+      const double *hl = H + (size_t)(j + 4) * SR + l;
+      double rho = hl[0], v = hl[HS];
+      const double *ol = O + (size_t)j * SR + l;
+      double cscth = 1.0 / g.sines[it];
+      double oors = ri * cscth;
+      double t = in_[k][5], oorho = 1.0 / rho;
+      double w1 = ol[0] * oors;
+      double drho = in_[k][0];
+      double dvv = in_[k][2];
+      drho = drho - v * w1;
+      dvv = dvv - g.pconst * w1 * t * oorho;
+      double ds = in_[k][4];
+      w1 = ol[OS] * oors;
+      dvv = dvv - v * w1;
+      double drho_out = drho - rho * w1;
+      double dw = in_[k][1];
+      w1 = ol[2 * OS] * oors;
+      dw = dw - v * w1;
+      double du = in_[k][3];
+      w1 = ol[3 * OS] * oors;
+      du = du - v * w1;
+      w1 = ol[4 * OS] * oors;
+      ds = ds - v * w1;
+      dvv = dvv - g.gamm1 * t * w1;
+      if (g.slaplacian) {
+        w1 = ol[5 * OS] * (oors * oors);
+        ds = ds + g.ks[ir] * w1 * (oorho / t);
+      }
+      dv[id] = drho_out;
+      dv[4 * n + id] = ds;
+      if (!mag) {
+        dv[n + id] = dw;
+        dv[3 * n + id] = du;
+        dv[2 * n + id] = dvv;
+      } else {
+        double oo = ONE_OVER_4PI * oorho * oors;
+        double bt_ = hl[5 * HS], br_ = hl[6 * HS], bp_ = __ldg(bf + n + id);
+        w1 = ol[6 * OS] * oo;
+        dvv = dvv - bt_ * w1;
+        dv[n + id] = dw + bp_ * w1;
+        w1 = ol[7 * OS] * oo;
+        dv[2 * n + id] = dvv - br_ * w1;
+        dv[3 * n + id] = du + bp_ * w1;
+      }
     }
   }
 }
@@ -522,30 +546,59 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
     __syncthreads();
   }
   const double *resp = g.resp_r + (size_t)(2 * br + (phys == 2 ? 1 : 0)) * g.tstride;
-  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
-    int j = pt / TL, l = pt - j * TL;
-    int ir = r0 + j;
-    if (tb + l >= g.nth) continue;
-    RadIn q;
-    size_t id = gather(j, l, q);
-    double drho = dv[id], dw = dv[n + id], dvv = dv[2 * n + id], du = dv[3 * n + id], ds = dv[4 * n + id];
-    radial_point(g, ir, q, drho, dw, dvv, du, ds);
-    // Density_Terms_Radial
-    double w1 = O[5 * OS + (size_t)j * SR + l];
-    if (phys) w1 = w1 + datum[l] * resp[j + 1];
-    if (g.non_uniform) w1 = w1 * g.dxdr[ir];
-    drho = drho - q.u * w1;
-    w1 = w1 * (1.0 / q.rho);
-    du = du - g.pconst * q.t * w1;
-    if (phys == 2 && j == m - 1 && !g.set_stop) {  // rhs_mpi.f90:1807-1818
-      drho = drho + q.rho * (g.t0 - q.t) / (g.damping_time * (g.gamma - 2.0) * q.t);
-      ds = ds - g.cv * (g.t0 - q.t) / (g.damping_time * (g.gamma - 2.0) * q.t);
+  constexpr int PPT = (MT > 0 && TLC > 0) ? (MT * TLC + 127) / 128 : 1;
+  for (int pt0 = threadIdx.x; pt0 < TL * m; pt0 += PPT * blockDim.x) {
+    double in_[PPT][7];
+    bool ok[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      int pt = pt0 + k * blockDim.x;
+      int j = pt / TL, l = pt - j * TL;
+      ok[k] = pt < TL * m && tb + l < g.nth;
+      if (ok[k]) {
+        size_t id = base + (size_t)(r0 + j) * ps + l;
+        in_[k][0] = dv[id]; in_[k][1] = dv[n + id]; in_[k][2] = dv[2 * n + id];
+        in_[k][3] = dv[3 * n + id]; in_[k][4] = dv[4 * n + id]; in_[k][5] = __ldg(tbuf + id);
+        in_[k][6] = mag ? __ldg(bf + 2 * n + id) : 0.0;
+      }
     }
-    dv[id] = drho;
-    dv[n + id] = dw;
-    dv[2 * n + id] = dvv;
-    dv[3 * n + id] = du;
-    dv[4 * n + id] = ds;
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      if (!ok[k]) continue;
+      int pt = pt0 + k * blockDim.x;
+      int j = pt / TL, l = pt - j * TL;
+      int ir = r0 + j;
+      size_t id = base + (size_t)(r0 + j) * ps + l;
+      const double *hl = H + (size_t)(j + 4) * SR + l;
+      const double *ol = O + (size_t)j * SR + l;
+      RadIn q;
+      q.u = hl[2 * HS];
+      q.rho = hl[4 * HS];
+      q.t = in_[k][5];
+      q.dw_r = ol[0]; q.dv_r = ol[OS]; q.du_r = ol[2 * OS]; q.ds_r = ol[3 * OS]; q.d2s_r = ol[4 * OS];
+      if (mag) {
+        q.bt = hl[5 * HS]; q.bp = hl[6 * HS]; q.br = in_[k][6];
+        q.dbt_r = ol[6 * OS]; q.dbp_r = ol[7 * OS];
+      }
+      double drho = in_[k][0], dw = in_[k][1], dvv = in_[k][2], du = in_[k][3], ds = in_[k][4];
+      radial_point(g, ir, q, drho, dw, dvv, du, ds);
+      // Density_Terms_Radial
+      double w1 = O[5 * OS + (size_t)j * SR + l];
+      if (phys) w1 = w1 + datum[l] * resp[j + 1];
+      if (g.non_uniform) w1 = w1 * g.dxdr[ir];
+      drho = drho - q.u * w1;
+      w1 = w1 * (1.0 / q.rho);
+      du = du - g.pconst * q.t * w1;
+      if (phys == 2 && j == m - 1 && !g.set_stop) {  // rhs_mpi.f90:1807-1818
+        drho = drho + q.rho * (g.t0 - q.t) / (g.damping_time * (g.gamma - 2.0) * q.t);
+        ds = ds - g.cv * (g.t0 - q.t) / (g.damping_time * (g.gamma - 2.0) * q.t);
+      }
+      dv[id] = drho;
+      dv[n + id] = dw;
+      dv[2 * n + id] = dvv;
+      dv[3 * n + id] = du;
+      dv[4 * n + id] = ds;
+    }
   }
 }
 
@@ -571,7 +624,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
   const CssDir &D = g.d[1];
   const int t0 = D.start[bt], m = MT ? MT : D.size[bt];
   const int dtype = dtype_of(D, bt);
-  const int SR = m + 9, SO = m + 1, TS = 3 * (m + 2);
+  const int SR = m + 9, SO = m + 1;
   const size_t n = (size_t)g.ncell;
   double *H = sm;
   double *O = H + (size_t)TL * SR;
@@ -617,19 +670,29 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
       continue;
     }
     const bool twall = (it == 0 || it == g.nth - 1), rlo = (ir == 0), rhi = (ir == g.nr - 1);
-    for (int iv = 0; iv < nv; iv++) {
+    double dd[8], aa[8], ss[8];
+#pragma unroll
+    for (int iv = 0; iv < 8; iv++) {
+      if (iv >= nv) break;
       size_t q = (size_t)iv * n + id;
-      double d = (iv == 0) ? d0 : (iv == 1) ? d1 : dv[q];
-      double a = v0[q], o;
+      dd[iv] = (iv == 0) ? d0 : (iv == 1) ? d1 : dv[q];
+      aa[iv] = v0[q];
+      ss[iv] = (stage == 1 && !g.sldiffusion) ? 0.0 : vs[q];
+    }
+#pragma unroll
+    for (int iv = 0; iv < 8; iv++) {
+      if (iv >= nv) break;
+      size_t q = (size_t)iv * n + id;
+      double d = dd[iv], a = aa[iv], o;
       if (stage == 1) {
-        double sv = g.sldiffusion ? vs[q] + d / 6.0 : d;
+        double sv = g.sldiffusion ? ss[iv] + d / 6.0 : d;
         vs[q] = sv;
         o = a + dtcur * d;
       } else if (stage == 4) {
-        double sv = vs[q] + d / 6.0;
+        double sv = ss[iv] + d / 6.0;
         o = a + dtcur * sv;
       } else {
-        double sv = vs[q] + d / 3.0;
+        double sv = ss[iv] + d / 3.0;
         vs[q] = sv;
         o = a + dtcur * d;
       }
