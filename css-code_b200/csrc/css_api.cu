@@ -244,6 +244,10 @@ static int setup_kernels() {
   static bool done = false;
   if (done) return CSS_OK;
   if (int rc = setup_mt<0, 0>()) return rc;
+  CUDA_TRY(cudaFuncSetAttribute(k_sld<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<4>)));
+  CUDA_TRY(cudaFuncSetAttribute(k_sld<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<5>)));
+  CUDA_TRY(cudaFuncSetAttribute(k_sld<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<7>)));
+  CUDA_TRY(cudaFuncSetAttribute(k_sld<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<8>)));
   if (int rc = setup_mt<16, 16>()) return rc;
   if (int rc = setup_mt<32, 16>()) return rc;
   int mx = 200 * 1024;
@@ -668,7 +672,12 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
   if (int rc = check_launch(c)) return rc;
   prof_begin(c, KI_SLD);
   dim3 gs((g.nth + SLD_TT - 1) / SLD_TT, (g.nphi + SLD_TP - 1) / SLD_TP, (g.nr + SLD_RC - 1) / SLD_RC);
-  k_sld<<<gs, SLD_TT * SLD_TP, 0, c->stream>>>(g, v, av, c->vcc, dout);
+  switch (g.nsld) {
+    case 4: k_sld<4><<<gs, SLD_TT * SLD_TP, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout); break;
+    case 5: k_sld<5><<<gs, SLD_TT * SLD_TP, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout); break;
+    case 7: k_sld<7><<<gs, SLD_TT * SLD_TP, sizeof(SldSmem<7>), c->stream>>>(g, v, av, c->vcc, dout); break;
+    default: k_sld<8><<<gs, SLD_TT * SLD_TP, sizeof(SldSmem<8>), c->stream>>>(g, v, av, c->vcc, dout); break;
+  }
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   if (g.do_ohmic_heating) {

@@ -999,20 +999,38 @@ __device__ __forceinline__ double sld_ghost_t(const CssGeo &g, int iv, double q0
 
 // Slope-limited diffusion, all three directions and all nsld fields in one
 // pass.  CTA = a 32 (theta) x 8 (phi) plane tile marching over an r chunk of
-// SLD_RC radii; each face's limited flux is computed once: theta and phi
-// faces of the plane from a shared tile with a 2-point halo, r faces carried
-// in registers from one radius to the next.  Then viscous heating and the
-// mass-diffusion corrections (diffusion.f90:375-428) per cell.
+// SLD_RC radii.  Per radius: the plane values of every field (2-point halo)
+// and the speed plane (1-point halo) go to shared memory, every theta and
+// phi face flux is computed once, the r faces come from a 4-point window
+// per field carried in registers (one new global load per field and
+// radius), then viscous heating and the mass-diffusion corrections
+// (diffusion.f90:375-428) per cell.  NF = number of diffused fields.
 #define SLD_TT 32
 #define SLD_TP 8
 #define SLD_RC 16
-__global__ void __launch_bounds__(SLD_TT * SLD_TP) k_sld(CssGeo g, const double *__restrict__ v,
-                                                         const double *__restrict__ av,
-                                                         const double *__restrict__ vcc, double *__restrict__ dout) {
-  __shared__ double X[SLD_TP + 4][SLD_TT + 5];   // field plane, halo 2
-  __shared__ double V[SLD_TP + 2][SLD_TT + 3];   // vcc plane, halo 1
-  __shared__ double FT[SLD_TP][SLD_TT + 1];      // theta faces
-  __shared__ double FP[SLD_TP + 1][SLD_TT + 1];  // phi faces
+template <int NF>
+struct SldSmem {
+  double X[NF][SLD_TP + 4][SLD_TT + 5];   // field planes, halo 2
+  double V[SLD_TP + 2][SLD_TT + 3];       // vcc plane, halo 1
+  double FT[NF][SLD_TP][SLD_TT + 1];      // theta faces
+  double FP[NF][SLD_TP + 1][SLD_TT];      // phi faces
+  double ST[SLD_TP][SLD_TT + 1];          // theta face speed * sin(face)
+  double SP[SLD_TP + 1][SLD_TT];          // phi face speed
+};
+
+template <int NF>
+__global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const double *__restrict__ v,
+                                                            const double *__restrict__ av,
+                                                            const double *__restrict__ vcc,
+                                                            double *__restrict__ dout) {
+  extern __shared__ double sm_raw[];
+  SldSmem<NF> &S = *reinterpret_cast<SldSmem<NF> *>(sm_raw);
+  auto &X = S.X;
+  auto &V = S.V;
+  auto &FT = S.FT;
+  auto &FP = S.FP;
+  auto &ST = S.ST;
+  auto &SP = S.SP;
   const size_t n = (size_t)g.ncell;
   const int nth = g.nth, nphi = g.nphi, nr = g.nr;
   const int tx = threadIdx.x % SLD_TT, ty = threadIdx.x / SLD_TT;
@@ -1021,112 +1039,134 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP) k_sld(CssGeo g, const double 
   const int it = t0 + tx, ip = p0 + ty;
   const bool live = it < nth && ip < nphi;
   const int itc = min(it, nth - 1), ipc = min(ip, nphi - 1);
-  // r-face carry per field: de of the lower r face of the current radius,
-  // and x(ir-1)
-  double carry[8], xprev[8];
+  const int off = g.varlist[0];  // the diffused fields are off, off+1, ..., contiguous
+  // per-field r window: x(ir-1), x(ir), x(ir+1), x(ir+2), and the de of the
+  // lower r face of the current radius
+  double win[NF][4], carry[NF];
+#pragma unroll
+  for (int f = 0; f < NF; f++) {
+    const int iv = f + off;
+    auto xr = [&](int q) -> double {  // x at radius q of this column (ghosts outside)
+      if (q >= 0 && q < nr) return sld_val(g, v, av, iv, itc, ipc, q);
+      if (q == -1) return sld_ghost_r(g, v, av, iv, itc, ipc, 1);
+      if (q == nr) return sld_ghost_r(g, v, av, iv, itc, ipc, 0);
+      return 0.0;
+    };
+    win[f][0] = xr(r0 - 1);
+    win[f][1] = xr(r0);
+    win[f][2] = xr(r0 + 1);
+    win[f][3] = xr(r0 + 2);
+    carry[f] = 0.0;
+    if (r0 > 0) {
+      const double vc = __ldg(vcc + css_idx(g, itc, ipc, r0)), vcm = __ldg(vcc + css_idx(g, itc, ipc, r0 - 1));
+      carry[f] = (g.sld_coef * sqrt(0.5 * (vc + vcm))) *
+                 (sld_face(xr(r0 - 2), win[f][0], win[f][1], win[f][2], g.tinyvar[iv]) * g.sld_r[2 * nr + r0]);
+    }
+  }
   for (int ir = r0; ir < r1; ir++) {
-    const double t3 = g.sld_r[ir], rfac = g.sld_r[nr + ir], rlo2 = g.sld_r[2 * nr + ir];
-    const double rhi2 = g.sld_r[3 * nr + ir];
+    const double t3 = g.sld_r[ir], rfac = g.sld_r[nr + ir], rhi2 = g.sld_r[3 * nr + ir];
     const double cphl = g.sld_th[nth + itc], cphh = g.sld_th[3 * nth + itc];
     const double geom = g.sld_th[4 * nth + itc] * (rfac / g.dphi);
-    // vcc plane with halo 1 (clamped at theta walls: those faces are zeroed)
+    const double vc = __ldg(vcc + css_idx(g, itc, ipc, ir));
+    const double vcp = ir < nr - 1 ? __ldg(vcc + css_idx(g, itc, ipc, ir + 1)) : vc;
+    const double vr_hi = g.sld_coef * sqrt(0.5 * (vcp + vc));
+    // next window value x(ir+3), issued early
+    double nxt[NF];
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const int q = ir + 3;
+      nxt[f] = (q < nr) ? sld_val(g, v, av, f + off, itc, ipc, q) : 0.0;
+    }
     __syncthreads();
     for (int k = threadIdx.x; k < (SLD_TP + 2) * (SLD_TT + 2); k += blockDim.x) {
       int a = k % (SLD_TT + 2), b = k / (SLD_TT + 2);
       int gt = min(max(t0 + a - 1, 0), nth - 1), gp = (p0 + b - 1 + nphi) % nphi;
       V[b][a] = __ldg(vcc + css_idx(g, gt, gp, ir));
     }
-    const double vc = __ldg(vcc + css_idx(g, itc, ipc, ir));
-    const double vcm = ir > 0 ? __ldg(vcc + css_idx(g, itc, ipc, ir - 1)) : vc;
-    const double vcp = ir < nr - 1 ? __ldg(vcc + css_idx(g, itc, ipc, ir + 1)) : vc;
-    const double vr_lo = g.sld_coef * sqrt(0.5 * (vc + vcm));
-    const double vr_hi = g.sld_coef * sqrt(0.5 * (vcp + vc));
-    double Dv[8];
-    const int off = g.varlist[0];  // varlist is off, off+1, ..., contiguous
+    for (int k = threadIdx.x; k < NF * (SLD_TP + 4) * (SLD_TT + 4); k += blockDim.x) {
+      int f = k / ((SLD_TP + 4) * (SLD_TT + 4)), rem = k - f * (SLD_TP + 4) * (SLD_TT + 4);
+      int a = rem % (SLD_TT + 4), b = rem / (SLD_TT + 4);
+      int gt = t0 + a - 2, gp = (p0 + b - 2 + nphi) % nphi;
+      X[f][b][a] = (gt >= 0 && gt < nth) ? sld_val(g, v, av, f + off, gt, gp, ir) : 0.0;
+    }
+    __syncthreads();
+    // theta ghosts next to the walls (diffusion.f90:1008-1118)
+    if (t0 == 0)
+      for (int k = threadIdx.x; k < NF * (SLD_TP + 4); k += blockDim.x) {
+        int f = k / (SLD_TP + 4), b = k - f * (SLD_TP + 4);
+        X[f][b][1] = sld_ghost_t(g, f + off, X[f][b][2], X[f][b][3], X[f][b][4], X[f][b][5], 1);
+      }
+    if (t0 + SLD_TT >= nth)
+      for (int k = threadIdx.x; k < NF * (SLD_TP + 4); k += blockDim.x) {
+        int f = k / (SLD_TP + 4), b = k - f * (SLD_TP + 4), a = nth - t0 + 2;
+        X[f][b][a] = sld_ghost_t(g, f + off, X[f][b][a - 1], X[f][b][a - 2], X[f][b][a - 3], X[f][b][a - 4], 0);
+      }
+    // face speeds, shared by every field
+    for (int k = threadIdx.x; k < SLD_TP * (SLD_TT + 1); k += blockDim.x) {
+      int a = k % (SLD_TT + 1), b = k / (SLD_TT + 1);
+      int gt = t0 + a;
+      ST[b][a] = (gt > 0 && gt < nth) ? (g.sld_coef * sqrt(0.5 * (V[b + 1][a + 1] + V[b + 1][a]))) * g.sld_th[gt]
+                                      : 0.0;
+    }
+    for (int k = threadIdx.x; k < (SLD_TP + 1) * SLD_TT; k += blockDim.x) {
+      int a = k % SLD_TT, b = k / SLD_TT;
+      SP[b][a] = g.sld_coef * sqrt(0.5 * (V[b][a + 1] + V[b + 1][a + 1]));
+    }
+    __syncthreads();
+    // face fluxes of every field
+    for (int k = threadIdx.x; k < NF * SLD_TP * (SLD_TT + 1); k += blockDim.x) {
+      int f = k / (SLD_TP * (SLD_TT + 1)), rem = k - f * SLD_TP * (SLD_TT + 1);
+      int a = rem % (SLD_TT + 1), b = rem / (SLD_TT + 1);
+      int gt = t0 + a;
+      double d = 0.0;
+      if (gt > 0 && gt < nth)
+        d = ST[b][a] * sld_face(X[f][b + 2][a], X[f][b + 2][a + 1], X[f][b + 2][a + 2], X[f][b + 2][a + 3],
+                                g.tinyvar[f + off]);
+      FT[f][b][a] = d;
+    }
+    for (int k = threadIdx.x; k < NF * (SLD_TP + 1) * SLD_TT; k += blockDim.x) {
+      int f = k / ((SLD_TP + 1) * SLD_TT), rem = k - f * (SLD_TP + 1) * SLD_TT;
+      int a = rem % SLD_TT, b = rem / SLD_TT;
+      FP[f][b][a] = SP[b][a] * sld_face(X[f][b][a + 2], X[f][b + 1][a + 2], X[f][b + 2][a + 2], X[f][b + 3][a + 2],
+                                        g.tinyvar[f + off]);
+    }
+    __syncthreads();
+    double Dv[NF];
 #pragma unroll
-    for (int isl = 0; isl < 8; isl++) {
-      Dv[isl] = 0.0;
-      if (isl >= g.nsld) continue;
-      const int iv = isl + off, iv1 = iv + 1;
-      const double tiny = g.tinyvar[iv];
+    for (int f = 0; f < NF; f++) {
+      const int iv = f + off, iv1 = iv + 1;
       double prR = 1.0, prTP = 1.0;
       if (g.sld_pr != 1.0 || g.sld_prm != 1.0) {
         if (iv1 <= 3) prR = g.sld_pr; else if (iv1 >= 5) prR = g.sld_prm;
         if (iv1 < 5) prTP = g.sld_pr; else if (iv1 > 5) prTP = g.sld_prm;
       }
-      __syncthreads();
-      // plane tile with halo 2 (theta ghosts filled below, phi periodic)
-      for (int k = threadIdx.x; k < (SLD_TP + 4) * (SLD_TT + 4); k += blockDim.x) {
-        int a = k % (SLD_TT + 4), b = k / (SLD_TT + 4);
-        int gt = t0 + a - 2, gp = (p0 + b - 2 + nphi) % nphi;
-        X[b][a] = (gt >= 0 && gt < nth) ? sld_val(g, v, av, iv, gt, gp, ir) : 0.0;
-      }
-      __syncthreads();
-      if (t0 == 0 && threadIdx.x < SLD_TP + 4) {  // x(-1) next to the low wall
-        int b = threadIdx.x;
-        X[b][1] = sld_ghost_t(g, iv, X[b][2], X[b][3], X[b][4], X[b][5], 1);
-      }
-      if (t0 + SLD_TT >= nth && threadIdx.x >= 32 && threadIdx.x < 32 + SLD_TP + 4) {  // x(nth)
-        int b = threadIdx.x - 32, a = nth - t0 + 2;
-        X[b][a] = sld_ghost_t(g, iv, X[b][a - 1], X[b][a - 2], X[b][a - 3], X[b][a - 4], 0);
-      }
-      __syncthreads();
-      // theta faces: face a sits between tile columns a-1 and a (a = 0..32)
-      for (int k = threadIdx.x; k < SLD_TP * (SLD_TT + 1); k += blockDim.x) {
-        int a = k % (SLD_TT + 1), b = k / (SLD_TT + 1);
-        int gt = t0 + a;  // the face below global theta gt
-        double d = 0.0;
-        if (gt > 0 && gt < nth) {
-          double vt = g.sld_coef * sqrt(0.5 * (V[b + 1][a + 1] + V[b + 1][a]));
-          double sp = g.sld_th[gt];  // sin of the face below theta gt
-          d = (vt * sp) * sld_face(X[b + 2][a], X[b + 2][a + 1], X[b + 2][a + 2], X[b + 2][a + 3], tiny);
-        }
-        FT[b][a] = d;
-      }
-      // phi faces: face b between tile rows b-1 and b (b = 0..8)
-      for (int k = threadIdx.x; k < (SLD_TP + 1) * SLD_TT; k += blockDim.x) {
-        int a = k % SLD_TT, b = k / SLD_TT;
-        double vt = g.sld_coef * sqrt(0.5 * (V[b][a + 1] + V[b + 1][a + 1]));
-        FP[b][a] = vt * sld_face(X[b][a + 2], X[b + 1][a + 2], X[b + 2][a + 2], X[b + 3][a + 2], tiny);
-      }
-      // r faces (the thread's own column); x(ir-1) is carried in xprev
-      const double x0 = X[ty + 2][tx + 2];
-      double xp1 = 0.0, xp2 = 0.0;
-      if (ir + 1 < nr) xp1 = sld_val(g, v, av, iv, itc, ipc, ir + 1);
-      if (ir + 2 < nr) xp2 = sld_val(g, v, av, iv, itc, ipc, ir + 2);
-      else if (ir + 2 == nr) xp2 = sld_ghost_r(g, v, av, iv, itc, ipc, 0);
-      double dlo;
-      if (ir == r0) {
-        xprev[isl] = (ir > 0) ? sld_val(g, v, av, iv, itc, ipc, ir - 1) : sld_ghost_r(g, v, av, iv, itc, ipc, 1);
-        if (ir == 0) {
-          dlo = 0.0;
-        } else {
-          double xm2 = (ir >= 2) ? sld_val(g, v, av, iv, itc, ipc, ir - 2) : sld_ghost_r(g, v, av, iv, itc, ipc, 1);
-          dlo = vr_lo * (sld_face(xm2, xprev[isl], x0, xp1, tiny) * rlo2);
-        }
-      } else {
-        dlo = carry[isl];
-      }
-      double dup = (ir == nr - 1) ? 0.0 : vr_hi * (sld_face(xprev[isl], x0, xp1, xp2, tiny) * rhi2);
-      carry[isl] = dup;
-      xprev[isl] = x0;
-      double flux = t3 * (dup - dlo);
+      double dup = (ir == nr - 1) ? 0.0
+                                  : vr_hi * (sld_face(win[f][0], win[f][1], win[f][2], win[f][3], g.tinyvar[iv]) * rhi2);
+      double flux = t3 * (dup - carry[f]);
       if (prR != 1.0) flux = prR * flux;
       double acc = flux;
-      __syncthreads();
-      flux = (rfac / (cphl - cphh)) * (FT[ty][tx + 1] - FT[ty][tx]);
+      carry[f] = dup;
+      flux = (rfac / (cphl - cphh)) * (FT[f][ty][tx + 1] - FT[f][ty][tx]);
       if (prTP != 1.0) flux = prTP * flux;
       acc = acc + flux;
-      flux = FP[ty + 1][tx] - FP[ty][tx];
+      flux = FP[f][ty + 1][tx] - FP[f][ty][tx];
       if (prTP != 1.0) flux = prTP * flux;
       acc = acc + geom * flux;
-      Dv[isl] = acc;
+      Dv[f] = acc;
+      // slide the window: x(ir+3) is a ghost exactly when ir+3 == nr
+      win[f][0] = win[f][1];
+      win[f][1] = win[f][2];
+      win[f][2] = win[f][3];
+      win[f][3] = (ir + 3 == nr) ? sld_ghost_r(g, v, av, iv, itc, ipc, 0) : nxt[f];
     }
     if (!live) continue;
     const size_t id = css_idx(g, it, ip, ir);
     double D[8];
 #pragma unroll
-    for (int k = 0; k < 8; k++) D[k] = off ? (k >= 1 ? Dv[k - 1] : 0.0) : Dv[k];
+    for (int k = 0; k < 8; k++) {
+      int f = k - off;
+      D[k] = (f >= 0 && f < NF) ? Dv[f >= 0 && f < NF ? f : 0] : 0.0;
+    }
     double rho = __ldg(v + id);
     double invrho = 1.0 / rho;
     double itemp = (pow(rho, -g.gamm1)) * exp(-__ldg(v + 4 * n + id) * g.invcv) / g.invtconst;
