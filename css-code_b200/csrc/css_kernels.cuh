@@ -1077,17 +1077,30 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
       const int q = ir + 3;
       nxt[f] = (q < nr) ? sld_val(g, v, av, f + off, itc, ipc, q) : 0.0;
     }
+    (void)0;
     __syncthreads();
-    for (int k = threadIdx.x; k < (SLD_TP + 2) * (SLD_TT + 2); k += blockDim.x) {
-      int a = k % (SLD_TT + 2), b = k / (SLD_TT + 2);
-      int gt = min(max(t0 + a - 1, 0), nth - 1), gp = (p0 + b - 1 + nphi) % nphi;
-      V[b][a] = __ldg(vcc + css_idx(g, gt, gp, ir));
+    {
+      const double *vp = vcc + plane(g, ir);
+      for (int k = threadIdx.x; k < (SLD_TP + 2) * (SLD_TT + 2); k += blockDim.x) {
+        int a = k % (SLD_TT + 2), bb = k / (SLD_TT + 2);
+        int gt = min(max(t0 + a - 1, 0), nth - 1), gp = p0 + bb - 1;
+        gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
+        V[bb][a] = __ldg(vp + (size_t)gp * nth + gt);
+      }
     }
-    for (int k = threadIdx.x; k < NF * (SLD_TP + 4) * (SLD_TT + 4); k += blockDim.x) {
-      int f = k / ((SLD_TP + 4) * (SLD_TT + 4)), rem = k - f * (SLD_TP + 4) * (SLD_TT + 4);
-      int a = rem % (SLD_TT + 4), b = rem / (SLD_TT + 4);
-      int gt = t0 + a - 2, gp = (p0 + b - 2 + nphi) % nphi;
-      X[f][b][a] = (gt >= 0 && gt < nth) ? sld_val(g, v, av, f + off, gt, gp, ir) : 0.0;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const int iv = f + off;
+      const double *fp = (iv >= 5 ? av + (size_t)(iv - 5) * n : v + (size_t)iv * n) + plane(g, ir);
+      const double mean = (iv == 0) ? g.rhor[ir] : (iv == 4 ? g.sr[ir] : 0.0);
+      for (int k = threadIdx.x; k < (SLD_TP + 4) * (SLD_TT + 4); k += blockDim.x) {
+        int a = k % (SLD_TT + 4), bb = k / (SLD_TT + 4);
+        int gt = t0 + a - 2, gp = p0 + bb - 2;
+        gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
+        double q = 0.0;
+        if (gt >= 0 && gt < nth) q = __ldg(fp + (size_t)gp * nth + gt) - mean;
+        X[f][bb][a] = q;
+      }
     }
     __syncthreads();
     // theta ghosts next to the walls (diffusion.f90:1008-1118)
@@ -1114,21 +1127,22 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     }
     __syncthreads();
     // face fluxes of every field
-    for (int k = threadIdx.x; k < NF * SLD_TP * (SLD_TT + 1); k += blockDim.x) {
-      int f = k / (SLD_TP * (SLD_TT + 1)), rem = k - f * SLD_TP * (SLD_TT + 1);
-      int a = rem % (SLD_TT + 1), b = rem / (SLD_TT + 1);
-      int gt = t0 + a;
-      double d = 0.0;
-      if (gt > 0 && gt < nth)
-        d = ST[b][a] * sld_face(X[f][b + 2][a], X[f][b + 2][a + 1], X[f][b + 2][a + 2], X[f][b + 2][a + 3],
-                                g.tinyvar[f + off]);
-      FT[f][b][a] = d;
-    }
-    for (int k = threadIdx.x; k < NF * (SLD_TP + 1) * SLD_TT; k += blockDim.x) {
-      int f = k / ((SLD_TP + 1) * SLD_TT), rem = k - f * (SLD_TP + 1) * SLD_TT;
-      int a = rem % SLD_TT, b = rem / SLD_TT;
-      FP[f][b][a] = SP[b][a] * sld_face(X[f][b][a + 2], X[f][b + 1][a + 2], X[f][b + 2][a + 2], X[f][b + 3][a + 2],
-                                        g.tinyvar[f + off]);
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const double tiny = g.tinyvar[f + off];
+      for (int k = threadIdx.x; k < SLD_TP * (SLD_TT + 1); k += blockDim.x) {
+        int a = k % (SLD_TT + 1), bb = k / (SLD_TT + 1);
+        int gt = t0 + a;
+        double d = 0.0;
+        if (gt > 0 && gt < nth)
+          d = ST[bb][a] * sld_face(X[f][bb + 2][a], X[f][bb + 2][a + 1], X[f][bb + 2][a + 2], X[f][bb + 2][a + 3], tiny);
+        FT[f][bb][a] = d;
+      }
+      for (int k = threadIdx.x; k < (SLD_TP + 1) * SLD_TT; k += blockDim.x) {
+        int a = k % SLD_TT, bb = k / SLD_TT;
+        FP[f][bb][a] =
+            SP[bb][a] * sld_face(X[f][bb][a + 2], X[f][bb + 1][a + 2], X[f][bb + 2][a + 2], X[f][bb + 3][a + 2], tiny);
+      }
     }
     __syncthreads();
     double Dv[NF];
