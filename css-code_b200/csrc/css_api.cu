@@ -940,3 +940,114 @@ extern "C" int css_kernel_stats(css_ctx *c, int kind, const char **name, double 
   if (launches) *launches = c->k_count[kind];
   return CSS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Allocation-free compact lines.
+//
+// Some callers cannot allocate device memory at the moment they want a
+// derivative: a code that has handed all device memory to its own pool or
+// to a framework's caching allocator at start-up (cudaMalloc then fails or
+// evicts their cache), or one that must not stall, because cudaMalloc and
+// cudaFree synchronize the whole device.  css_compact_lines_noalloc serves
+// them: the caller passes device buffers for the inputs and outputs, and
+// the LU tables and the halo-padded copies of the lines live in one
+// file-scope device array of fixed size that every GPU loading this library
+// holds until the process exits.  Nothing is allocated, on the device or
+// on the host.
+// ---------------------------------------------------------------------------
+#define CSS_NOALLOC_DOUBLES (1 << 18)  // 2 MiB of scratch per device
+static __device__ __align__(256) double g_noalloc_scratch[CSS_NOALLOC_DOUBLES];
+static double *g_noalloc_addr[64];     // device address of the array, per device
+static int g_noalloc_ready[64];
+
+// LU tables of one (n, lphys, rphys) line for bdry 0..4, written on the
+// device with the same correctly rounded steps as the host's tab_d1/tab_d2
+// (no contraction), so they equal the tables css_compact_lines uses.
+__global__ void k_noalloc_tables(double *T, int n, int lphys, int rphys, int order) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int ts = n + 2;
+  for (int k = 0; k < 15 * ts; k++) T[k] = 0.0;
+  for (int iv = 0; iv < 5; iv++) {
+    double *g1 = T + (size_t)iv * 3 * ts, *g2 = g1 + ts, *g3 = g2 + ts;
+    double alpha, a2, g2c, up1, up2;
+    if (order == 1) {
+      alpha = 1.0 / 3.0; a2 = 0.75; g2c = 0.125;
+      double cn = __ddiv_rn(1.0, __dsub_rn(a2, __dmul_rn(3.0, g2c)));
+      up1 = __dmul_rn(__dsub_rn(__dmul_rn(6.0, a2), 3.0), cn);
+      up2 = ((iv != 1) && (iv != 2)) ? 0.0 : up1;
+      if (iv % 2 == 0) up1 = 0.0;
+    } else {
+      const double U1[5] = {707.0 / 193.0, 137.0 / 13.0, 707.0 / 193.0, 137.0 / 13.0, 707.0 / 193.0};
+      const double U2[5] = {707.0 / 193.0, 137.0 / 13.0, 137.0 / 13.0, 707.0 / 193.0, 707.0 / 193.0};
+      alpha = 2.0 / 11.0; a2 = -0.35; g2c = 0.1; up1 = U1[iv]; up2 = U2[iv];
+    }
+    double c1 = 1.0, c2 = 1.0, c3;
+    g1[1] = g2[1] = g3[1] = c2;
+    if (lphys) {
+      c3 = (order == 1) ? __dmul_rn(up1, c2) : up1;
+      g1[2] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(g2c, c3))); g2[2] = c2;
+      c3 = __dmul_rn(a2, c2); g1[3] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(alpha, c3))); g2[3] = c2;
+      g3[2] = __dmul_rn(-g2c, g2[2]);
+    } else {
+      c3 = __dmul_rn(alpha, c2); g1[2] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(alpha, c3))); g2[2] = c2;
+      g3[2] = __dmul_rn(-alpha, g2[2]);
+      c3 = __dmul_rn(alpha, c2); g1[3] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(alpha, c3))); g2[3] = c2;
+    }
+    for (int i = 4; i <= n - 2; i++) {
+      c3 = __dmul_rn(alpha, c2); g1[i] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(alpha, c3))); g2[i] = c2;
+    }
+    for (int i = 3; i <= n - 2; i++) g3[i] = __dmul_rn(-alpha, g2[i]);
+    // row n-1 of a physical upper end mirrors row 2: lower coefficient a2,
+    // upper coefficient g2c (tab_d1; tab_d2 swaps its two names, same values)
+    const double rl = a2, ru = g2c;
+    if (rphys) {
+      c3 = __dmul_rn(alpha, c2); g1[n - 1] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(rl, c3))); g2[n - 1] = c2;
+      c3 = __dmul_rn(ru, c2); g1[n] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(up2, c3))); g2[n] = c2;
+      g3[n - 1] = __dmul_rn(-rl, g2[n - 1]);
+      g3[n] = __dmul_rn(-up2, g2[n]);
+    } else {
+      c3 = __dmul_rn(alpha, c2); g1[n - 1] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(alpha, c3))); g2[n - 1] = c2;
+      c3 = __dmul_rn(alpha, c2); g1[n] = c3; c2 = __ddiv_rn(c1, __dsub_rn(c1, __dmul_rn(alpha, c3))); g2[n] = c2;
+      g3[n - 1] = __dmul_rn(-alpha, g2[n - 1]);
+      g3[n] = __dmul_rn(-alpha, g2[n]);
+    }
+    for (int j = 1; j <= n; j++) g1[j] = -g1[j];
+  }
+}
+
+extern "C" int css_compact_lines_noalloc(const double *x, double *dx, int n, int nlines, int order, int lphys,
+                                         int rphys, int bdry, const double *bc_lo, const double *bc_hi,
+                                         const double *halo_lo, const double *halo_hi, double dnum, double scale,
+                                         void *stream) {
+  if (!x || !dx || n < 10 || order < 1 || order > 2 || bdry < 0 || bdry > 4 || nlines < 0 ||
+      (!lphys && !halo_lo) || (!rphys && !halo_hi)) {
+    set_err("css_compact_lines_noalloc: bad argument");
+    return CSS_ERR_ARG;
+  }
+  const size_t ts = (size_t)n + 2, need = 15 * ts + (size_t)nlines * ((size_t)n + 8);
+  if (need > (size_t)CSS_NOALLOC_DOUBLES) {
+    set_err("css_compact_lines_noalloc: %zu doubles of scratch needed, the fixed device array holds %d "
+            "(15*(n+2) + nlines*(n+8) must fit); split the lines into smaller batches",
+            need, CSS_NOALLOC_DOUBLES);
+    return CSS_ERR_ARG;
+  }
+  if (nlines == 0) return CSS_OK;
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { set_err("css_compact_lines_noalloc: device index %d out of range", dev); return CSS_ERR_ARG; }
+  if (!g_noalloc_ready[dev]) {  // once per device, with that device current
+    double *p = nullptr;
+    CUDA_TRY(cudaGetSymbolAddress((void **)&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = p;
+    g_noalloc_ready[dev] = 1;
+  }
+  double *T = g_noalloc_addr[dev], *work = T + 15 * ts;
+  cudaStream_t st = (cudaStream_t)stream;
+  k_noalloc_tables<<<1, 1, 0, st>>>(T, n, lphys, rphys, order);
+  CUDA_TRY(cudaGetLastError());
+  int dtype = lphys ? (rphys ? 0 : 2) : (rphys ? 1 : 3);
+  k_lines<<<(nlines + 127) / 128, 128, 0, st>>>(x, dx, n, nlines, order, dtype, bdry, bc_lo, bc_hi, halo_lo, halo_hi,
+                                                T, (int)ts, dnum, scale, work);
+  CUDA_TRY(cudaGetLastError());
+  return CSS_OK;
+}

@@ -45,6 +45,10 @@ def lib():
         L.css_kernel_launches.argtypes = [ctypes.c_void_p]
         L.css_kernel_launches.restype = ctypes.c_longlong
         L.css_set_stream.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.css_compact_lines_noalloc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                                ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_double, ctypes.c_double, ctypes.c_void_p]
         L.css_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.css_kernel_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
@@ -63,5 +67,5 @@ EXPORTS = [
     "css_last_error", "css_create", "css_destroy", "css_upload_state", "css_download_state", "css_step_rk4",
     "css_step_rk4_host", "css_rhs", "css_diffusion", "css_deriv", "css_deriv_dev", "css_dbyd1_dt0",
     "css_compact_lines", "css_sync", "css_state_device_ptr", "css_kernel_launches", "css_set_stream",
-    "css_profile", "css_kernel_stats",
+    "css_profile", "css_kernel_stats", "css_compact_lines_noalloc",
 ]

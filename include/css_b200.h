@@ -174,6 +174,32 @@ int css_compact_lines(const double *x, double *dx, int n, int nlines, int order,
                       const double *bc_hi, const double *halo_lo,
                       const double *halo_hi, double dnum, double scale);
 
+/* Allocation-free variant of css_compact_lines, for callers that cannot
+ * allocate device memory when they need a derivative: codes that gave all
+ * device memory to their own pool or a framework's caching allocator at
+ * start-up, and codes that must not stall on cudaMalloc/cudaFree, which
+ * synchronize the whole device.  It has no counterpart in the reference.
+ * x, dx, bc_lo, bc_hi, halo_lo, halo_hi are DEVICE pointers (same layout as
+ * css_compact_lines; the boundary and halo arrays may be NULL as there);
+ * work is enqueued on `stream` (NULL = the default stream) and the call
+ * returns without waiting.  Scratch (the LU tables and halo-padded copies
+ * of the lines) lives in one fixed 2 MiB device array per GPU, held from
+ * the library's first use until the process exits: a call needs
+ * 15*(n+2) + nlines*(n+8) doubles of it, at most 262144, and larger
+ * requests fail with CSS_ERR_ARG.  Nothing in the array needs to start at
+ * zero: each call writes every table entry and every padded line before
+ * reading it.  The array is shared by every call on a device, so calls that
+ * overlap on the GPU (other streams, other host threads) race: serialize
+ * them on one stream.  The
+ * first call on each device looks up the array's device address, so make
+ * it before any stream capture.  No memory is allocated, on the device or
+ * the host.                                                              */
+int css_compact_lines_noalloc(const double *x, double *dx, int n, int nlines,
+                              int order, int lphys, int rphys, int bdry,
+                              const double *bc_lo, const double *bc_hi,
+                              const double *halo_lo, const double *halo_hi,
+                              double dnum, double scale, void *stream);
+
 /* Block until all work on the context stream is done. */
 int css_sync(css_ctx *ctx);
 
