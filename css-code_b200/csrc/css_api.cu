@@ -14,6 +14,7 @@
 
 #include "../../include/css_b200.h"
 #include "css_kernels.cuh"
+#include "css_stats.cuh"
 
 using namespace css;
 
@@ -938,6 +939,201 @@ extern "C" int css_kernel_stats(css_ctx *c, int kind, const char **name, double 
   if (name) *name = kKernelNames[kind];
   if (total_ms) *total_ms = c->k_ms[kind];
   if (launches) *launches = c->k_count[kind];
+  return CSS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Diagnostics of the current state (vars0): Scalar_Output, Compute_Step_Size,
+// Shell_Average_Output and the (theta, phi) spectrum.  Between steps the
+// stage buffers are free, so they hold the scratch: vA = ds/dr, vB = face
+// data and spectrum tables, vs = reduction partials and per-radius results,
+// dv = spectrum line sums, bf = B.
+// ---------------------------------------------------------------------------
+__global__ void k_fill2(double *a, size_t n, double x, double y) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < 2 * n; i += (size_t)gridDim.x * blockDim.x)
+    a[i] = i < n ? x : y;
+}
+
+static int stats_chunks(const css_ctx *c) {
+  const size_t np = (size_t)c->p.nth * c->p.nphi;
+  int nchunk = (4 * 148 + c->p.nr - 1) / c->p.nr;  // about four CTAs per SM over all radii
+  nchunk = std::max(1, std::min(nchunk, 64));
+  while (nchunk > 1 && np / (size_t)nchunk < 256) nchunk--;
+  return nchunk;
+}
+
+// per-radius accumulators res[ir*SA_N + a] of the current state
+static int run_stats(css_ctx *c, int need_dsdr, std::vector<double> &res) {
+  const CssGeo &g = c->g;
+  const size_t n = c->ncell, np = (size_t)g.nth * g.nphi;
+  const int nr = g.nr, nchunk = stats_chunks(c);
+  if ((size_t)nr * nchunk * SA_NPASS1 + (size_t)nr * SA_N > (size_t)c->nv * n) {
+    set_err("diagnostics: grid too small for the reduction scratch");
+    return CSS_ERR_ARG;
+  }
+  cudaStream_t st = c->stream;
+  if (g.magnetic)
+    if (int rc = launch_curl(c, c->v0 + 5 * n, c->bf, 1)) return rc;  // Compute_B(0)
+  const double *dsdr = nullptr;
+  if (need_dsdr) {
+    // Compute_Derivatives (report_mpi.f90:288-318): d s/d r with the
+    // constant-flux datum dsdr1/dxdr(1), dsdr2/dxdr(nr) at the faces
+    k_fill2<<<256, 256, 0, st>>>(c->vB, np, g.s_flux_lo, g.s_flux_hi);
+    if (int rc = check_launch(c)) return rc;
+    if (int rc = css_deriv_dev(c, 0, 1, c->v0 + 4 * n, c->vA, c->vB, c->vB + np, g.ibcr[5], nullptr)) return rc;
+    dsdr = c->vA;
+  }
+  double *part = c->vs, *resd = c->vs + (size_t)nr * nchunk * SA_NPASS1;
+  k_stats_pass1<<<dim3(nchunk, nr), 256, 0, st>>>(g, c->v0, c->bf, dsdr, part);
+  if (int rc = check_launch(c)) return rc;
+  k_stats_combine<<<nr, 32, 0, st>>>(part, nchunk, SA_NPASS1, 0, resd);
+  if (int rc = check_launch(c)) return rc;
+  k_stats_pass2<<<dim3(nchunk, nr), 256, 0, st>>>(g, c->v0, resd, part);
+  if (int rc = check_launch(c)) return rc;
+  k_stats_combine<<<nr, 32, 0, st>>>(part, nchunk, SA_NPASS2, SA_NPASS1, resd);
+  if (int rc = check_launch(c)) return rc;
+  res.assign((size_t)nr * SA_N, 0.0);
+  CUDA_TRY(cudaMemcpyAsync(res.data(), resd, res.size() * 8, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
+  return CSS_OK;
+}
+
+extern "C" int css_scalars(css_ctx *c, double *out) {
+  if (!c || !out) { set_err("css_scalars: NULL argument"); return CSS_ERR_ARG; }
+  std::vector<double> res;
+  if (int rc = run_stats(c, 0, res)) return rc;
+  const int nr = c->p.nr;
+  const double ntot = (double)c->ncell;
+  double s[SA_N] = {0};
+  double umax = -INFINITY, bmax2 = -INFINITY;
+  for (int ir = 0; ir < nr; ir++) {
+    const double *r = &res[(size_t)ir * SA_N];
+    for (int a : {SA_RU2, SA_RW2, SA_RV2, SA_RUSQ, SA_BSQ}) s[a] += r[a];
+    umax = std::max(umax, r[SA_UMACH]);
+    bmax2 = std::max(bmax2, r[SA_BMAX2]);
+  }
+  const double cke = s[SA_RU2] / (2.0 * ntot);
+  out[0] = s[SA_RUSQ] / (2.0 * ntot);                                // kinener
+  out[1] = cke;                                                      // cke
+  out[2] = cke + s[SA_RW2] / (2.0 * ntot);                           // mcke
+  out[3] = s[SA_RV2] / (2.0 * ntot);                                 // drke
+  out[4] = sqrt(umax);                                               // umach
+  out[5] = c->p.magnetic ? s[SA_BSQ] / (8.0 * M_PI * ntot) : 0.0;    // magener
+  out[6] = c->p.magnetic ? sqrt(bmax2) * 2.0 * sqrt(2.0 * M_PI) : 0.0;  // bmax
+  return CSS_OK;
+}
+
+extern "C" int css_step_size(css_ctx *c, double cfl_safety, double *out) {
+  if (!c || !out) { set_err("css_step_size: NULL argument"); return CSS_ERR_ARG; }
+  std::vector<double> res;
+  if (int rc = run_stats(c, 0, res)) return rc;
+  double dtc = 1e4, dtb = 1e4, e = 0.0, l = 0.0, m = 0.0, mrs = 0.0;
+  for (int ir = 0; ir < c->p.nr; ir++) {
+    const double *r = &res[(size_t)ir * SA_N];
+    dtc = std::min(dtc, r[SA_DTC]);
+    if (c->p.magnetic) dtb = std::min(dtb, r[SA_DTB]);
+    e += r[SA_E];
+    l += r[SA_L];
+    m += r[SA_M];
+    mrs += r[SA_MRS];
+  }
+  const double dtd = 1e10;  // no explicit (Laplacian) viscosity limit
+  out[0] = std::min(std::min(dtb, dtc), dtd) * cfl_safety;
+  out[1] = e;
+  out[2] = l;
+  out[3] = m;
+  out[4] = mrs;
+  return CSS_OK;
+}
+
+extern "C" int css_shell_averages(css_ctx *c, const int *quantities, int nq, const double *k0, double *out) {
+  if (!c || !quantities || !out || nq < 1) { set_err("css_shell_averages: bad argument"); return CSS_ERR_ARG; }
+  int need_dsdr = 0;
+  for (int iq = 0; iq < nq; iq++) {
+    const int q = quantities[iq];
+    if (q < 1 || q > 18) {
+      set_err("css_shell_averages: quantity %d not supported (1..18; 19 needs the SLD flux output)", q);
+      return CSS_ERR_ARG;
+    }
+    if (q >= 10 && q <= 14 && !c->p.magnetic) {
+      set_err("css_shell_averages: quantity %d needs a magnetic run", q);
+      return CSS_ERR_ARG;
+    }
+    if (q == 9 || q == 15) need_dsdr = 1;
+  }
+  std::vector<double> res;
+  if (int rc = run_stats(c, need_dsdr, res)) return rc;
+  const int nr = c->p.nr;
+  const double inv = 1.0 / ((double)c->p.nth * c->p.nphi);
+  const double gamm1 = c->p.gamma - 1.0, cv = c->p.cp / c->p.gamma;
+  std::vector<double> ksh(nr);
+  CUDA_TRY(cudaMemcpy(ksh.data(), c->g.ks, nr * 8, cudaMemcpyDeviceToHost));
+  static const int kMap[19] = {-1, SA_RHO, SA_T, SA_S, SA_RHOT, SA_VR, SA_VT, SA_VP, SA_KE, SA_DSDR,
+                               SA_BR, SA_BT, SA_BP, SA_ME, SA_BPOL, SA_DSDR, SA_FEN, SA_FKE, SA_FAC};
+  for (int iq = 0; iq < nq; iq++) {
+    const int q = quantities[iq];
+    for (int ir = 0; ir < nr; ir++) {
+      const double sum = res[(size_t)ir * SA_N + kMap[q]];
+      double v;
+      if (q == 4) v = gamm1 * cv * sum * inv;
+      else if (q == 15) {  // F_ks: conduction by the SLaplacian ks plus the prescribed flux k0
+        const double k0r = k0 ? k0[ir] : 0.0;
+        v = c->p.slaplacian ? -ksh[ir] * sum * inv + k0r : k0r;
+      } else if (q == 16) v = c->p.cp * sum * inv;
+      else v = sum * inv;
+      out[(size_t)iq * nr + ir] = v;
+    }
+  }
+  return CSS_OK;
+}
+
+extern "C" int css_spectrum(css_ctx *c, int kind, double *out) {
+  if (!c || !out) { set_err("css_spectrum: NULL argument"); return CSS_ERR_ARG; }
+  const int nth = c->p.nth, nphi = c->p.nphi, nr = c->p.nr;
+  if (nth % 2 || nphi % 2 || nth < 4 || nphi < 4) {
+    set_err("css_spectrum: nth and nphi must be even");
+    return CSS_ERR_ARG;
+  }
+  if (kind < 0 || kind > 1 + c->nv || (kind == 1 && !c->p.magnetic)) {
+    set_err("css_spectrum: kind %d not available (0 KE, 1 ME (magnetic), 2+iv variable iv)", kind);
+    return CSS_ERR_ARG;
+  }
+  const size_t n = c->ncell;
+  cudaStream_t st = c->stream;
+  if (kind == 1)
+    if (int rc = launch_curl(c, c->v0 + 5 * n, c->bf, 1)) return rc;
+  // theta weights: apodisation 1 - cos(pi (theta - theta_1)/(theta_n - theta_1))^64 and
+  // W(t) = sum_{kt=1}^{nth/2-1} exp(-2 pi i kt t / nth); phi twiddles cos|sin(2 pi j / nphi)
+  std::vector<double> tab(3 * (size_t)nth + 2 * (size_t)nphi);
+  const double dth = (c->p.th2 - c->p.th1) / (double)(nth - 1);
+  const double th0 = c->p.th1, thn = dth * (double)(nth - 1) + c->p.th1;
+  for (int t = 0; t < nth; t++) {
+    const double th = dth * (double)t + c->p.th1;
+    const double apod = 1.0 - pow(cos(M_PI * (th - th0) / (thn - th0)), 64);
+    double wr = 0.0, wi = 0.0;
+    for (int kt = 1; kt < nth / 2; kt++) {
+      const double ang = 2.0 * M_PI * (double)(((long long)kt * t) % nth) / (double)nth;
+      wr += cos(ang);
+      wi -= sin(ang);
+    }
+    tab[t] = apod;
+    tab[nth + t] = apod * wr;
+    tab[2 * nth + t] = apod * wi;
+  }
+  for (int j = 0; j < nphi; j++) {
+    const double ang = 2.0 * M_PI * (double)j / (double)nphi;
+    tab[3 * nth + j] = cos(ang);
+    tab[3 * nth + nphi + j] = sin(ang);
+  }
+  CUDA_TRY(cudaMemcpyAsync(c->vB, tab.data(), tab.size() * 8, cudaMemcpyHostToDevice, st));
+  k_spec_theta<<<dim3((nphi + 7) / 8, nr), 256, 0, st>>>(c->g, c->v0, c->bf, kind, c->vB, c->dv);
+  if (int rc = check_launch(c)) return rc;
+  const size_t sm = (size_t)3 * nphi * 8;
+  if (sm > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(k_spec_phi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_spec_phi<<<nr, 256, sm, st>>>(c->dv, c->vB + 3 * nth, nth, nphi, c->vA);
+  if (int rc = check_launch(c)) return rc;
+  CUDA_TRY(cudaMemcpyAsync(out, c->vA, (size_t)nr * (nphi / 2) * 8, cudaMemcpyDeviceToHost, st));
+  CUDA_TRY(cudaStreamSynchronize(st));
   return CSS_OK;
 }
 

@@ -52,6 +52,10 @@ def lib():
         L.css_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.css_kernel_stats.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_char_p),
                                        ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_longlong)]
+        L.css_scalars.argtypes = [ctypes.c_void_p, dp]
+        L.css_step_size.argtypes = [ctypes.c_void_p, ctypes.c_double, dp]
+        L.css_shell_averages.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, dp, dp]
+        L.css_spectrum.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
         _LIB = L
     return _LIB
 
@@ -67,5 +71,6 @@ EXPORTS = [
     "css_last_error", "css_create", "css_destroy", "css_upload_state", "css_download_state", "css_step_rk4",
     "css_step_rk4_host", "css_rhs", "css_diffusion", "css_deriv", "css_deriv_dev", "css_dbyd1_dt0",
     "css_compact_lines", "css_sync", "css_state_device_ptr", "css_kernel_launches", "css_set_stream",
-    "css_profile", "css_kernel_stats", "css_compact_lines_noalloc",
+    "css_profile", "css_kernel_stats", "css_compact_lines_noalloc", "css_scalars", "css_step_size",
+    "css_shell_averages", "css_spectrum",
 ]

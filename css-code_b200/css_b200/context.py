@@ -98,6 +98,40 @@ class Simulation:
                 out[nm.value.decode()] = (ms.value, cnt.value)
         return out
 
+    # diagnostics of the current state ----------------------------------------
+    SCALAR_NAMES = ("kinener", "cke", "mcke", "drke", "umach", "magener", "bmax")
+    STEP_SIZE_NAMES = ("dtmax", "Etot", "Ltot", "mtot", "mrsint")
+
+    def scalars(self):
+        """Scalar_Output (report_mpi.f90:173-262) of the resident state, as a dict."""
+        out = np.zeros(7)
+        check(_lib.lib().css_scalars(self.h, _p(out)))
+        return dict(zip(self.SCALAR_NAMES, out.tolist()))
+
+    def step_size(self, cfl_safety):
+        """Compute_Step_Size (rhs_mpi.f90:92-275): dtmax and the conservation totals."""
+        out = np.zeros(5)
+        check(_lib.lib().css_step_size(self.h, float(cfl_safety), _p(out)))
+        return dict(zip(self.STEP_SIZE_NAMES, out.tolist()))
+
+    def shell_averages(self, quantities, k0=None):
+        """Shell_Average_Output (report_mpi.f90:783-1094): array (nq, nr) of the
+        horizontal averages of the reference's quantity codes 1..18."""
+        q = np.ascontiguousarray(quantities, dtype=np.int32)
+        out = np.zeros((len(q), self.p.nr))
+        k = None if k0 is None else np.ascontiguousarray(k0, dtype=np.float64)
+        check(_lib.lib().css_shell_averages(self.h, q.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(q), _p(k),
+                                            _p(out)))
+        return out
+
+    def spectrum(self, kind=0):
+        """(theta, phi) spectrum per radius, array (nr, nphi/2), folded as
+        CSS-IDL/spectral_analysis_new.pro:16-25 folds it (kind 0 kinetic energy
+        density, 1 magnetic energy density, 2+iv state variable iv)."""
+        out = np.zeros((self.p.nr, self.p.nphi // 2))
+        check(_lib.lib().css_spectrum(self.h, int(kind), _p(out)))
+        return out
+
     # parity entry points ----------------------------------------------------
     def rhs(self, vars1, call_num=1):
         v = np.array(vars1, dtype=np.float64, order="C", copy=True)

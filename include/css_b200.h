@@ -226,6 +226,45 @@ int css_profile(css_ctx *ctx, int enable);
 int css_kernel_stats(css_ctx *ctx, int kind, const char **name, double *total_ms,
                      long long *launches);
 
+/* ---- diagnostics of the current state (vars0), computed on the device ----
+ * Each call reads the state left by css_upload_state / css_step_rk4, uses
+ * the stage buffers as scratch (so it must not overlap a step on another
+ * stream), and returns on the host when its results are there.  For a
+ * magnetic run B = curl A with Compute_B's boundary zeroing
+ * (derivatives.f90:1830-1892) is formed first, as the reference's output
+ * routines do.                                                             */
+
+/* Scalar_Output (report_mpi.f90:173-262): out[7] = kinener, cke, mcke,
+ * drke, umach, magener, bmax (the two magnetic entries are 0 for hydro).  */
+#define CSS_NSCALARS 7
+int css_scalars(css_ctx *ctx, double *out);
+
+/* Compute_Step_Size (rhs_mpi.f90:92-275): out[5] = dtmax (the Courant limit
+ * min(dtmaxb, dtmaxc, dtmaxd) times cfl_safety), Etot, Ltot, mtot, mrsint.
+ * dtmaxd is the reference's 1e10 (no explicit Laplacian viscosity).       */
+#define CSS_NSTEPSIZE 5
+int css_step_size(css_ctx *ctx, double cfl_safety, double *out);
+
+/* Shell_Average_Output (report_mpi.f90:783-1094): horizontal averages per
+ * radius of quantities[0..nq) with the reference's codes 1..18 (1 rho,
+ * 2 T, 3 s, 4 P, 5 v_r, 6 v_theta, 7 v_phi, 8 KE, 9 ds/dr, 10 B_r,
+ * 11 B_theta, 12 B_phi, 13 ME, 14 |B_pol|, 15 F_ks, 16 F_en, 17 F_ke,
+ * 18 F_ac); out is (nr, nq) in Fortran order, out[iq*nr + ir].  k0 (nr,
+ * may be NULL = 0) is the prescribed radiative flux profile of F_ks.
+ * Code 19 (the SLD entropy flux) and magnetic codes on a hydro run return
+ * CSS_ERR_ARG.                                                             */
+int css_shell_averages(css_ctx *ctx, const int *quantities, int nq,
+                       const double *k0, double *out);
+
+/* Horizontal spectrum per radius with the folding of
+ * CSS-IDL/spectral_analysis_new.pro:16-25 (apodisation in theta, forward
+ * 2D FFT normalised by 1/(nth nphi), F[kt,kp] + F[nth-kt,nphi-kp] kept as
+ * a real number, summed over 1 <= kt < nth/2 and divided by nth/2) of one
+ * snapshot: out[ir*(nphi/2) + kp], kp = 0..nphi/2-1.  kind 0 = kinetic
+ * energy density rho|u|^2/2, 1 = magnetic energy density |B|^2/(8 pi),
+ * 2+iv = state variable iv.  nth and nphi must be even.                    */
+int css_spectrum(css_ctx *ctx, int kind, double *out);
+
 #ifdef __cplusplus
 }
 #endif

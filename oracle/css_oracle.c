@@ -1976,3 +1976,253 @@ int orc_step_rk4(orc_ctx *c, double *vars0, double dt, int nsteps) {
   free(av);
   return CSS_OK;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Diagnostics of vars0: Scalar_Output (report_mpi.f90:173-262),            */
+/* Compute_Step_Size (rhs_mpi.f90:92-275), Shell_Average_Output             */
+/* (report_mpi.f90:783-1094, with Compute_Derivatives :264-439 for ds/dr)   */
+/* and the spectrum of CSS-IDL/spectral_analysis_new.pro:16-25.  Sums run   */
+/* in the Fortran array order of one plane (theta fastest).                 */
+/* ------------------------------------------------------------------------ */
+/* B = curl A of vars0 (Compute_B(0)), or NULL for hydro; caller frees */
+static double *diag_b(orc_ctx *c, const double *vars0) {
+  if (!c->p.magnetic) return NULL;
+  double *b = dalloc(3 * (size_t)c->ncell);
+  vector_curl_a(c, vars0 + 5 * (size_t)c->ncell, b);
+  compute_b_bc(c, b);
+  return b;
+}
+
+int orc_scalars(orc_ctx *c, const double *vars0, double *out) {
+  size_t n = c->ncell;
+  const double *prho = vars0, *pw = vars0 + n, *pv = vars0 + 2 * n, *pu = vars0 + 3 * n, *ps = vars0 + 4 * n;
+  double *b = diag_b(c, vars0);
+  double nsize = (double)n;
+  double magener = 0.0, bmax = 0.0, cke = 0.0, mcke = 0.0, drke = 0.0, kinener = 0.0, umach = -1.0;
+  double sumb = 0.0, maxb = 0.0, s;
+  if (b) {
+    for (size_t i = 0; i < n; i++) {
+      double bsq = b[2 * n + i] * b[2 * n + i] + b[i] * b[i] + b[n + i] * b[n + i];
+      sumb += bsq;
+      if (i == 0 || sqrt(bsq) > maxb) maxb = sqrt(bsq);
+    }
+    magener = sumb / (8 * PI * nsize);
+  }
+  s = 0.0;
+  for (size_t i = 0; i < n; i++) s += prho[i] * (pu[i] * pu[i]);
+  cke = s / (double)(2 * n);
+  s = 0.0;
+  for (size_t i = 0; i < n; i++) s += prho[i] * (pw[i] * pw[i]);
+  mcke = cke + s / (double)(2 * n);
+  s = 0.0;
+  for (size_t i = 0; i < n; i++) s += prho[i] * (pv[i] * pv[i]);
+  drke = s / (double)(2 * n);
+  s = 0.0;
+  for (size_t i = 0; i < n; i++) {
+    double t = pow(prho[i], c->gamm1) * exp(ps[i] * c->invcv) * c->invtconst * c->gamm1 * c->p.cp;
+    double usqr = pw[i] * pw[i] + pv[i] * pv[i] + pu[i] * pu[i];
+    double q;
+    if (b) {
+      double bsq = b[2 * n + i] * b[2 * n + i] + b[i] * b[i] + b[n + i] * b[n + i];
+      q = usqr / (2.0 * bsq / prho[i] + usqr + t);
+    } else {
+      q = usqr / (usqr + t);
+    }
+    if (q > umach) umach = q;
+    s += prho[i] * usqr;
+  }
+  kinener = s / (double)(2 * n);
+  umach = sqrt(umach);
+  if (b) bmax = maxb * 2.0 * sqrt(2.0 * PI);
+  out[0] = kinener; out[1] = cke; out[2] = mcke; out[3] = drke; out[4] = umach; out[5] = magener; out[6] = bmax;
+  free(b);
+  return CSS_OK;
+}
+
+int orc_step_size(orc_ctx *c, const double *vars0, double cfl_safety, double *out) {
+  size_t n = c->ncell;
+  int nth = c->nth, nphi = c->nphi, nr = c->nr;
+  double *b = diag_b(c, vars0);
+  double dtmaxb = 1e4, dtmaxc = 1e4, etot = 0.0, ltot = 0.0, mtot = 0.0, mrsint = 0.0;
+  const double dth = c->dth, dphi = c->dphi, om = c->p.omega_0;
+  for (int ir = 0; ir < nr; ir++) {
+    double radius = c->r_ind[ir], drad = c->dr_ind[ir];
+    for (int it = 0; it < nth; it++) {
+      double sinth = c->sines[it];
+      double dxmin = fmin(drad, radius * fmin(dth, sinth * dphi));
+      double srho = 0.0, sl = 0.0, se = 0.0, vmax = INFINITY, sb = 0.0, vamax = INFINITY;
+      for (int ip = 0; ip < nphi; ip++) {
+        size_t i = IDX(c, it, ip, ir);
+        double rho = vars0[i], wt = vars0[n + i] * vars0[n + i], vt = vars0[2 * n + i], ut = vars0[3 * n + i] * vars0[3 * n + i];
+        double tt = c->invtconst * pow(rho, c->gamm1) * exp(vars0[4 * n + i] * c->invcv);
+        double q = vt + radius * sinth * om;
+        srho += rho;
+        sl += rho * sqrt(wt + sinth * sinth * (q * q));
+        vt = vt * vt;
+        se += rho * (c->cv * tt + 0.5 * (ut + wt + vt));
+        tt = c->gamm1 * c->p.cp * c->p.xi_cs * c->p.xi_cs * tt;
+        ut = ut + vt + wt + tt;
+        vmax = fmin(vmax, dxmin / sqrt(ut));
+        if (b) {
+          double btt = b[i] * b[i], bpt = b[n + i] * b[n + i], brt = b[2 * n + i] * b[2 * n + i];
+          sb += brt + btt + bpt;
+          vamax = fmin(vamax, dxmin / sqrt(ut + (brt + btt + bpt) * ONE_OVER_4PI / rho));
+        }
+      }
+      mtot += radius * radius * sinth * srho * drad * dth * dphi;
+      mrsint += radius * radius * radius * sinth * sinth * sinth * srho * drad * dth * dphi;
+      ltot += radius * radius * radius * sinth * sl * drad * dth * dphi;
+      etot += radius * radius * sinth * se * drad * dth * dphi;
+      dtmaxc = fmin(dtmaxc, vmax);
+      if (b) {
+        etot += 0.5 * radius * radius * sinth * sb * drad * dth * dphi * ONE_OVER_4PI;
+        dtmaxb = fmin(dtmaxb, vamax);
+      }
+    }
+  }
+  double dtmaxd = 1e10;
+  out[0] = fmin(fmin(dtmaxb, dtmaxc), dtmaxd) * cfl_safety;
+  out[1] = etot; out[2] = ltot; out[3] = mtot; out[4] = mrsint;
+  free(b);
+  return CSS_OK;
+}
+
+int orc_shell_averages(orc_ctx *c, const double *vars0, const int *q, int nq, const double *k0, double *out) {
+  size_t n = c->ncell;
+  int nth = c->nth, nphi = c->nphi, nr = c->nr;
+  size_t np = (size_t)nth * nphi;
+  const css_params *p = &c->p;
+  for (int iq = 0; iq < nq; iq++)
+    if (q[iq] < 1 || q[iq] > 18 || (q[iq] >= 10 && q[iq] <= 14 && !p->magnetic)) {
+      set_err("orc_shell_averages: quantity %d not available", q[iq]);
+      return CSS_ERR_ARG;
+    }
+  const double *prho = vars0, *pw = vars0 + n, *pv = vars0 + 2 * n, *pu = vars0 + 3 * n, *ps = vars0 + 4 * n;
+  double *b = diag_b(c, vars0);
+  double *temp = dalloc(n), *dsdr = dalloc(n), *flo = dalloc(np), *fhi = dalloc(np);
+  /* Compute_Derivatives: ds/dr with dsdr1/dxdr(1), dsdr2/dxdr(nr) (or the face value) at the faces */
+  double dsdr1 = 0.0, dsdr2 = 0.0; /* dsdrm of the isentropic background */
+  if (p->slaplacian) {
+    if (!p->bottom_constant_temp) dsdr1 = -p->lumr1 * ONE_OVER_4PI / (c->ks[0] * p->r1 * p->r1);
+    if (!p->top_constant_temp) dsdr2 = -p->lumr2 * ONE_OVER_4PI / (c->ks[nr - 1] * p->r2 * p->r2);
+  }
+  int lbs = c->ibcr[5];
+  for (size_t k = 0; k < np; k++) {
+    flo[k] = (lbs == 2 || lbs == 4) ? dsdr1 / c->dxdr[0] : ps[k];
+    fhi[k] = (lbs == 3 || lbs == 4) ? dsdr2 / c->dxdr[nr - 1] : ps[(size_t)(nr - 1) * np + k];
+  }
+  orc_deriv(c, 0, 1, ps, dsdr, flo, fhi, lbs);
+  if (p->non_uniform)
+    for (size_t i = 0; i < n; i++) dsdr[i] = dsdr[i] * c->dxdr[i / np];
+  for (size_t i = 0; i < n; i++) temp[i] = pow(prho[i], c->gamm1) * exp(ps[i] * c->invcv) * c->invtconst;
+  double nsize = (double)np;
+  for (int ir = 0; ir < nr; ir++) {
+    size_t o = (size_t)ir * np;
+    double avgT = 0, avgrho = 0, avgP = 0, avgvr = 0, sumrt = 0;
+    for (size_t k = 0; k < np; k++) { avgT += temp[o + k]; avgrho += prho[o + k]; sumrt += prho[o + k] * temp[o + k]; avgvr += pu[o + k]; }
+    avgP = c->gamm1 * c->cv * sumrt;
+    avgT /= nsize; avgrho /= nsize; avgP /= nsize; avgvr /= nsize;
+    for (int iq = 0; iq < nq; iq++) {
+      double s = 0.0, v;
+      for (size_t k = 0; k < np; k++) {
+        size_t i = o + k;
+        double usqr = 0.5 * prho[i] * (pu[i] * pu[i] + pv[i] * pv[i] + pw[i] * pw[i]);
+        double bt = b ? b[i] : 0, bp = b ? b[n + i] : 0, br = b ? b[2 * n + i] : 0;
+        switch (q[iq]) {
+          case 1: s += prho[i]; break;
+          case 2: s += temp[i]; break;
+          case 3: s += ps[i]; break;
+          case 4: s += prho[i] * temp[i]; break;
+          case 5: s += pu[i]; break;
+          case 6: s += pw[i]; break;
+          case 7: s += pv[i]; break;
+          case 8: s += usqr; break;
+          case 9: case 15: s += dsdr[i]; break;
+          case 10: s += br; break;
+          case 11: s += bt; break;
+          case 12: s += bp; break;
+          case 13: s += 0.125 * (br * br + bt * bt + bp * bp) / PI; break;
+          case 14: s += sqrt(br * br + bt * bt); break;
+          case 16: s += (pu[i] - avgvr) * prho[i] * (temp[i] - avgT); break;
+          case 17: s += usqr * (pu[i] - avgvr); break;
+          case 18: s += (c->gamm1 * c->cv * prho[i] * temp[i] - avgP) * (pu[i] - avgvr); break;
+        }
+      }
+      switch (q[iq]) {
+        case 4: v = c->gamm1 * c->cv * s / nsize; break;
+        case 5: v = avgvr; break;
+        case 15: v = (p->slaplacian ? -c->ks[ir] * s / nsize : 0.0) + (k0 ? k0[ir] : 0.0); break;
+        case 16: v = p->cp * s / nsize; break;
+        default: v = s / nsize;
+      }
+      out[(size_t)iq * nr + ir] = v;
+    }
+  }
+  free(b); free(temp); free(dsdr); free(flo); free(fhi);
+  return CSS_OK;
+}
+
+int orc_spectrum(orc_ctx *c, const double *vars0, int kind, double *out) {
+  size_t n = c->ncell;
+  int nth = c->nth, nphi = c->nphi, nr = c->nr;
+  if (nth % 2 || nphi % 2 || kind < 0 || kind > 1 + c->nv || (kind == 1 && !c->p.magnetic)) {
+    set_err("orc_spectrum: bad kind or odd grid");
+    return CSS_ERR_ARG;
+  }
+  double *b = kind == 1 ? diag_b(c, vars0) : NULL;
+  double *apod = dalloc(nth), *a = dalloc((size_t)nth * nphi);
+  double *xr = dalloc((size_t)nth * nphi), *xi = dalloc((size_t)nth * nphi);
+  double *tr = dalloc((size_t)nth * nphi), *ti = dalloc((size_t)nth * nphi);
+  double th0 = c->theta[0], thn = c->theta[nth - 1];
+  for (int t = 0; t < nth; t++) apod[t] = 1.0 - pow(cos(PI * (c->theta[t] - th0) / (thn - th0)), 64);
+  double nn = (double)nth * (double)nphi;
+  double *cp_ = dalloc(nphi), *sp_ = dalloc(nphi), *ct_ = dalloc(nth), *st_ = dalloc(nth);
+  for (int j = 0; j < nphi; j++) { cp_[j] = cos(2.0 * PI * (double)j / (double)nphi); sp_[j] = sin(2.0 * PI * (double)j / (double)nphi); }
+  for (int j = 0; j < nth; j++) { ct_[j] = cos(2.0 * PI * (double)j / (double)nth); st_[j] = sin(2.0 * PI * (double)j / (double)nth); }
+  for (int ir = 0; ir < nr; ir++) {
+    for (int ip = 0; ip < nphi; ip++)
+      for (int t = 0; t < nth; t++) {
+        size_t i = IDX(c, t, ip, ir);
+        double f;
+        if (kind == 0) f = 0.5 * vars0[i] * (vars0[3 * n + i] * vars0[3 * n + i] + vars0[2 * n + i] * vars0[2 * n + i] + vars0[n + i] * vars0[n + i]);
+        else if (kind == 1) f = 0.125 * (b[2 * n + i] * b[2 * n + i] + b[i] * b[i] + b[n + i] * b[n + i]) / PI;
+        else f = vars0[(size_t)(kind - 2) * n + i];
+        a[t + (size_t)nth * ip] = f * apod[t];
+      }
+    /* forward 2D DFT (IDL fft(.,-1) divides by the number of points): phi then theta */
+    for (int t = 0; t < nth; t++)
+      for (int kp = 0; kp < nphi; kp++) {
+        double sr = 0, si = 0;
+        for (int ip = 0; ip < nphi; ip++) {
+          int j = (int)(((long long)kp * ip) % nphi);
+          sr += a[t + (size_t)nth * ip] * cp_[j];
+          si -= a[t + (size_t)nth * ip] * sp_[j];
+        }
+        xr[t + (size_t)nth * kp] = sr; xi[t + (size_t)nth * kp] = si;
+      }
+    for (int kp = 0; kp < nphi; kp++)
+      for (int kt = 0; kt < nth; kt++) {
+        double sr = 0, si = 0;
+        for (int t = 0; t < nth; t++) {
+          int j = (int)(((long long)kt * t) % nth);
+          double cr = ct_[j], ci = -st_[j];
+          double yr = xr[t + (size_t)nth * kp], yi = xi[t + (size_t)nth * kp];
+          sr += yr * cr - yi * ci;
+          si += yr * ci + yi * cr;
+        }
+        tr[kt + (size_t)nth * kp] = sr / nn; ti[kt + (size_t)nth * kp] = si / nn;
+      }
+    /* fold: cube[0,0] = F[0,0]; cube[kt,kp] = F[kt,kp] + F[nth-kt,nphi-kp] for 1 <= kt < nth/2,
+       1 <= kp < nphi/2, stored into a real array (real part); total over kt / (nth/2) */
+    for (int kp = 0; kp < nphi / 2; kp++) {
+      double s = 0.0;
+      if (kp == 0) s = tr[0];
+      else
+        for (int kt = 1; kt < nth / 2; kt++) s += tr[kt + (size_t)nth * kp] + tr[(nth - kt) + (size_t)nth * (nphi - kp)];
+      out[(size_t)ir * (nphi / 2) + kp] = s / (nth / 2.0);
+    }
+  }
+  free(b); free(apod); free(a); free(xr); free(xi); free(tr); free(ti);
+  free(cp_); free(sp_); free(ct_); free(st_);
+  return CSS_OK;
+}

@@ -17,6 +17,9 @@
  *   diffusion.f90   (Initialize_Diffusion, Compute_Diffusion, Diffusion_R,
  *                    Diffusion_Th, Diffusion_Phi),
  *   step_rk4.f90    (Step_RK4),
+ *   report_mpi.f90  (Scalar_Output, Shell_Average_Output and the ds/dr of
+ *                    Compute_Derivatives), rhs_mpi.f90 Compute_Step_Size,
+ *   CSS-IDL/spectral_analysis_new.pro (the folded FFT spectrum),
  * emulating the MPI ranks serially (one virtual rank per block).
  *
  * Pinning: Dbyd1_dt0 / the whole-line closures are checked against golden
@@ -52,6 +55,12 @@ int orc_compact_lines(const double *x, double *dx, int n, int nlines, int order,
                       const double *halo_hi, double dnum, double scale);
 /* curl of A (VectorCurlA + Compute_B boundary zeroing): b = curl(a), 3 fields */
 int orc_curl_b(orc_ctx *c, const double *a, double *b);
+/* diagnostics of vars0, same outputs as css_scalars / css_step_size /
+ * css_shell_averages / css_spectrum */
+int orc_scalars(orc_ctx *c, const double *vars0, double *out);
+int orc_step_size(orc_ctx *c, const double *vars0, double cfl_safety, double *out);
+int orc_shell_averages(orc_ctx *c, const double *vars0, const int *q, int nq, const double *k0, double *out);
+int orc_spectrum(orc_ctx *c, const double *vars0, int kind, double *out);
 
 #ifdef __cplusplus
 }

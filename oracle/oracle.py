@@ -42,6 +42,10 @@ def lib():
         L.orc_compact_lines.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                         ctypes.c_int, ctypes.c_int, _dp, _dp, _dp, _dp, ctypes.c_double,
                                         ctypes.c_double]
+        L.orc_scalars.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_step_size.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, _dp]
+        L.orc_shell_averages.argtypes = [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp]
+        L.orc_spectrum.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
         _LIB = L
     return _LIB
 
@@ -124,6 +128,36 @@ class Oracle:
         b = np.zeros_like(a)
         _check(lib().orc_curl_b(self.h, _ptr(a), _ptr(b)))
         return b
+
+    SCALAR_NAMES = ("kinener", "cke", "mcke", "drke", "umach", "magener", "bmax")
+    STEP_SIZE_NAMES = ("dtmax", "Etot", "Ltot", "mtot", "mrsint")
+
+    def scalars(self, vars0):
+        v = np.ascontiguousarray(vars0, dtype=np.float64)
+        out = np.zeros(7)
+        _check(lib().orc_scalars(self.h, _ptr(v), _ptr(out)))
+        return dict(zip(self.SCALAR_NAMES, out.tolist()))
+
+    def step_size(self, vars0, cfl_safety):
+        v = np.ascontiguousarray(vars0, dtype=np.float64)
+        out = np.zeros(5)
+        _check(lib().orc_step_size(self.h, _ptr(v), float(cfl_safety), _ptr(out)))
+        return dict(zip(self.STEP_SIZE_NAMES, out.tolist()))
+
+    def shell_averages(self, vars0, quantities, k0=None):
+        v = np.ascontiguousarray(vars0, dtype=np.float64)
+        q = np.ascontiguousarray(quantities, dtype=np.int32)
+        out = np.zeros((len(q), self.p.nr))
+        k = None if k0 is None else np.ascontiguousarray(k0, dtype=np.float64)
+        _check(lib().orc_shell_averages(self.h, _ptr(v), q.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), len(q),
+                                        _ptr(k), _ptr(out)))
+        return out
+
+    def spectrum(self, vars0, kind=0):
+        v = np.ascontiguousarray(vars0, dtype=np.float64)
+        out = np.zeros((self.p.nr, self.p.nphi // 2))
+        _check(lib().orc_spectrum(self.h, _ptr(v), int(kind), _ptr(out)))
+        return out
 
     def step(self, vars0, dt, nsteps=1):
         v = np.array(vars0, dtype=np.float64, order="C", copy=True)
