@@ -148,6 +148,65 @@ __device__ __forceinline__ void tile_r(const CssGeo &g, const double *__restrict
   }
 }
 
+// threads per CTA of the line-solve kernels (every launch uses this count)
+constexpr int NT = 128;
+
+// Compile-time tiles of NF fields at once (MT, TLC > 0): every thread issues
+// all of its global loads (NF fields x ceil(TLC*(MT+8)/NT) points) before it
+// stores any of them to shared memory, so a CTA has NF times more loads in
+// flight than a field-by-field loop.  DIR 1: theta tile S[l*SR + jj] of
+// radius `fixed`, lines = phi indices lb..; DIR 2: phi tile S[jj*SR + l],
+// periodic in phi, lines = theta indices lb..; DIR 0: r tile S[jj*SR + l]
+// at phi index `fixed`, lines = theta indices lb...  a0 = first point of
+// the block along the sweep; jj = 0..MT+7 covers the 4-point halos.
+template <int NF, int MT, int TLC, int DIR>
+__device__ __forceinline__ void tiles_ct(const CssGeo &g, const double *const *f, double *S, size_t FS, int SR,
+                                         int a0, int lb, int fixed) {
+  constexpr int W = MT + 8, N = TLC * W, IT = (N + NT - 1) / NT;
+  double val[NF][IT];
+  int so[IT];
+  size_t go[IT];
+#pragma unroll
+  for (int k = 0; k < IT; k++) {
+    const int idx = threadIdx.x + k * NT;
+    int l, jj;
+    if (DIR == 1) { l = idx / W; jj = idx - l * W; }
+    else { jj = idx / TLC; l = idx - jj * TLC; }
+    bool ok = idx < N;
+    size_t off;
+    if (DIR == 1) {
+      const int gt = a0 + jj - 4, gp = lb + l;
+      ok = ok && gt >= 0 && gt < g.nth && gp < g.nphi;
+      off = plane(g, fixed) + (size_t)gp * g.nth + gt;
+      so[k] = l * SR + jj;
+    } else if (DIR == 2) {
+      int gp = a0 + jj - 4;
+      if (gp < 0) gp += g.nphi;
+      else if (gp >= g.nphi) gp -= g.nphi;
+      const int gt = lb + l;
+      ok = ok && gt < g.nth;
+      off = plane(g, fixed) + (size_t)gp * g.nth + gt;
+      so[k] = jj * SR + l;
+    } else {
+      const int gr = a0 + jj - 4, gt = lb + l;
+      ok = ok && gr >= 0 && gr < g.nr && gt < g.nth;
+      off = plane(g, gr < 0 ? 0 : gr) + (size_t)fixed * g.nth + gt;
+      so[k] = jj * SR + l;
+    }
+    if (!ok) so[k] = -1;
+    go[k] = ok ? off : 0;
+  }
+#pragma unroll
+  for (int q = 0; q < NF; q++)
+#pragma unroll
+    for (int k = 0; k < IT; k++) val[q][k] = (so[k] >= 0) ? __ldg(f[q] + go[k]) : 0.0;
+#pragma unroll
+  for (int q = 0; q < NF; q++)
+#pragma unroll
+    for (int k = 0; k < IT; k++)
+      if (so[k] >= 0) S[(size_t)q * FS + so[k]] = val[q][k];
+}
+
 // ---------------------------------------------------------------------------
 // Source_Theta_Terms (rhs_mpi.f90:786-1029) + Induction_Terms (:2340-2346)
 // grid: x = theta block * nchunk + phi chunk, y = r.  cur = stage input
@@ -175,7 +234,12 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
   double *O = H + (size_t)nh * TL * SR;
   double *Tb = O + (size_t)nd * TL * SO;
   const double *fld[6] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, bf + n, bf + 2 * n};
-  for (int k = 0; k < nh; k++) tile_theta<MT, TLC>(g, fld[k], H + (size_t)k * TL * SR, SR, t0, m, pb, TL, ir);
+  if constexpr (MT > 0 && TLC > 0) {
+    tiles_ct<4, MT, TLC, 1>(g, fld, H, (size_t)TL * SR, SR, t0, pb, ir);
+    if (mag) tiles_ct<2, MT, TLC, 1>(g, fld + 4, H + (size_t)4 * TL * SR, (size_t)TL * SR, SR, t0, pb, ir);
+  } else {
+    for (int k = 0; k < nh; k++) tile_theta<MT, TLC>(g, fld[k], H + (size_t)k * TL * SR, SR, t0, m, pb, TL, ir);
+  }
   const int var[7] = {2, 3, 4, 5, 5, 8, 9};
   for (int k = 0; k < nd; k++) stage_table(g, 1, bt, k == 4 ? 2 : 1, g.ibct[var[k]], m, Tb + k * TS);
   __syncthreads();
@@ -306,7 +370,12 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__res
   double *O = H + nh * HS;
   double *Tb = O + nd * OS;
   const double *fld[7] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n, bf, bf + 2 * n};
-  for (int k = 0; k < nh; k++) tile_phi<MT, TLC>(g, fld[k], H + k * HS, SR, p0, m, tb, TL, ir);
+  if constexpr (MT > 0 && TLC > 0) {
+    tiles_ct<5, MT, TLC, 2>(g, fld, H, HS, SR, p0, tb, ir);
+    if (mag) tiles_ct<2, MT, TLC, 2>(g, fld + 5, H + 5 * HS, HS, SR, p0, tb, ir);
+  } else {
+    for (int k = 0; k < nh; k++) tile_phi<MT, TLC>(g, fld[k], H + k * HS, SR, p0, m, tb, TL, ir);
+  }
   stage_table(g, 2, bp, 1, 0, m, Tb);
   stage_table(g, 2, bp, 2, 0, m, Tb + TS);
   __syncthreads();
@@ -480,7 +549,12 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
   double *Tb = O + nd * OS;
   double *datum = Tb + nd * TS;
   const double *fld[7] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, cur, bf, bf + n};
-  for (int k = 0; k < nh; k++) tile_r<MT, TLC>(g, fld[k], H + k * HS, SR, r0, m, tb, TL, ip);
+  if constexpr (MT > 0 && TLC > 0) {
+    tiles_ct<5, MT, TLC, 0>(g, fld, H, HS, SR, r0, tb, ip);
+    if (mag) tiles_ct<2, MT, TLC, 0>(g, fld + 5, H + 5 * HS, HS, SR, r0, tb, ip);
+  } else {
+    for (int k = 0; k < nh; k++) tile_r<MT, TLC>(g, fld[k], H + k * HS, SR, r0, m, tb, TL, ip);
+  }
   const int var[8] = {2, 3, 4, 5, 5, 1, 7, 8};
   for (int k = 0; k < nd; k++) stage_table(g, 0, br, k == 4 ? 2 : 1, g.ibcr[var[k]], m, Tb + k * TS);
   __syncthreads();
@@ -629,7 +703,12 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
   double *H = sm;
   double *O = H + (size_t)TL * SR;
   double *Tb = O + (size_t)TL * SO;
-  tile_theta<MT, TLC>(g, cur, H, SR, t0, m, pb, TL, ir);
+  if constexpr (MT > 0 && TLC > 0) {
+    const double *f1[1] = {cur};
+    tiles_ct<1, MT, TLC, 1>(g, f1, H, 0, SR, t0, pb, ir);
+  } else {
+    tile_theta<MT, TLC>(g, cur, H, SR, t0, m, pb, TL, ir);
+  }
   const int bdry = g.ibct[1];
   stage_table(g, 1, bt, 1, bdry, m, Tb);
   __syncthreads();
