@@ -531,8 +531,13 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
       R4[3 * nr + ir] = rhi * rhi;
     }
   }
-  std::vector<double> TH((size_t)3 * nth);
-  for (int i = 0; i < nth; i++) { TH[i] = sines[i]; TH[nth + i] = cosines[i]; TH[2 * nth + i] = theta[i]; }
+  // sin, cos, theta, cot = cos/sin, csc = 1/sin (correctly rounded divisions,
+  // the same values the kernels would get by dividing on the device)
+  std::vector<double> TH((size_t)5 * nth);
+  for (int i = 0; i < nth; i++) {
+    TH[i] = sines[i]; TH[nth + i] = cosines[i]; TH[2 * nth + i] = theta[i];
+    TH[3 * nth + i] = cosines[i] / sines[i]; TH[4 * nth + i] = 1.0 / sines[i];
+  }
 #define ALLOC(ptr, bytes)                                                                \
   do {                                                                                   \
     if (cudaMalloc(&(ptr), (bytes)) != cudaSuccess) {                                     \
@@ -566,6 +571,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   g.d2xdr2 = c->prof + 4 * nr; g.rhor = c->prof + 5 * nr; g.sr = c->prof + 6 * nr; g.grav = c->prof + 7 * nr;
   g.ks = c->prof + 8 * nr; g.dlnks = c->prof + 9 * nr; g.eps = c->prof + 10 * nr; g.dspeed = c->prof + 11 * nr;
   g.sines = c->theta_prof; g.cosines = c->theta_prof + nth; g.theta = c->theta_prof + 2 * nth;
+  g.cot = c->theta_prof + 3 * nth; g.csc = c->theta_prof + 4 * nth;
   g.sld_th = c->sld_geo; g.sld_r = c->sld_geo + 5 * (size_t)nth;
   cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {

@@ -31,7 +31,7 @@ struct CssGeo {
   // radial profiles (length nr)
   const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
   // theta profiles (length nth)
-  const double *sines, *cosines, *theta;
+  const double *sines, *cosines, *theta, *cot, *csc;  // cot = cos/sin, csc = 1/sin
   // SLD cell geometry (diffusion.f90:806-849, :1196-1247, :1316-1351):
   // per theta: sin/cos of the lower and upper faces and the phi geometry
   // factor; per r: 3/(r+^3 - r-^3), the volume-averaged 1/r factor, r-^2, r+^2

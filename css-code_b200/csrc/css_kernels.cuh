@@ -34,11 +34,10 @@ __device__ __forceinline__ int dtype_of(const CssDir &d, int b) {
 }
 
 // temperature (rhs_mpi.f90:376-385)
+// invtconst * rho^(gamma-1) * exp(s/Cv) as one exponential: the reference's
+// pow * exp product to within a few roundings of its exponent
 __device__ __forceinline__ double temp_of(const CssGeo &g, double rho, double s) {
-  double a = pow(rho, g.gamm1);
-  double t = g.invtconst * a;
-  double e = exp(s * g.invcv);
-  return t * e;
+  return g.invtconst * exp(fma(g.gamm1, log(rho), s * g.invcv));
 }
 
 __device__ __forceinline__ double dnum_d2_theta(const CssGeo &g, int ir) {
@@ -271,13 +270,31 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
   const double rv = g.r_ind[ir], epsr = g.eps[ir];
   const double omsq = rv * g.omega0 * g.omega0, om2 = 2.0 * g.omega0;
   const size_t pl = plane(g, ir);
-  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+  // points per thread: their global loads (rho, B_theta) go out before any store
+  constexpr int PPT = (MT > 0 && TLC > 0) ? (MT * TLC + NT - 1) / NT : 1;
+  constexpr int STRIDE = (MT > 0 && TLC > 0) ? NT : 0;
+  const int stride = STRIDE ? STRIDE : blockDim.x;
+  for (int pt0 = threadIdx.x; pt0 < TL * m; pt0 += PPT * stride) {
+  double rho_[PPT], bt_in[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; k++) {
+    const int pt = pt0 + k * stride;
+    const int l = pt / m, j = pt - l * m;
+    const bool ok = pt < TL * m && pb + l < g.nphi;
+    const size_t id = pl + (size_t)(pb + l) * g.nth + t0 + j;
+    rho_[k] = ok ? __ldg(cur + id) : 1.0;
+    bt_in[k] = (ok && mag) ? __ldg(bf + id) : 0.0;
+  }
+#pragma unroll
+  for (int k = 0; k < PPT; k++) {
+    const int pt = pt0 + k * stride;
+    if (pt >= TL * m) continue;
     int l = pt / m, j = pt - l * m;
     int it = t0 + j, ip = pb + l;
     if (ip >= g.nphi) continue;
     size_t id = pl + (size_t)ip * g.nth + it;
-    double sn = g.sines[it], cs = g.cosines[it], ct = cs / sn;
-    double rho = __ldg(cur + id);
+    double sn = g.sines[it], cs = g.cosines[it], ct = g.cot[it];
+    double rho = rho_[k];
     const double *hl = H + (size_t)l * SR + 4 + j;
     double w = hl[0], v = hl[(size_t)TL * SR], u = hl[(size_t)2 * TL * SR], s = hl[(size_t)3 * TL * SR];
     const double *ol = O + (size_t)l * SO + j;
@@ -302,15 +319,16 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
     double t = temp_of(g, rho, s);
     tbuf[id] = t;
     double invrho = 1.0 / rho;
+    const double oorho_t = invrho / t;
     double ds;
-    if (fabs(epsr) > 0.0) ds = epsr * invrho / t;
+    if (fabs(epsr) > 0.0) ds = epsr * oorho_t;
     else ds = 0.0;
     w1 = ol[(size_t)3 * TL * SO] * ri;
     double dwfin = dw - g.gamm1 * t * w1;
     ds = ds - w * w1;
     if (g.slaplacian) {
       double ddiff = ri * g.ks[ir];
-      double oorho = invrho / t;
+      double oorho = oorho_t;
       w1 = ddiff * w1 * oorho;
       ds = ds + ct * w1;
       double dd2 = ddiff * ri * ri;  // ks/r^3 as rhs_mpi.f90:972 has it
@@ -325,7 +343,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
       dw = dwfin;
       double oo = invrho;
       oo = oo * ONE_OVER_4PI * ri;
-      double bt_ = __ldg(bf + id), bp_ = hl[(size_t)4 * TL * SR], br_ = hl[(size_t)5 * TL * SR];
+      double bt_ = bt_in[k], bp_ = hl[(size_t)4 * TL * SR], br_ = hl[(size_t)5 * TL * SR];
       du = du - bt_ * bt_ * oo;
       dw = dw - bp_ * bp_ * ct * oo;
       dvv = dvv + bp_ * bt_ * ct * oo;
@@ -342,6 +360,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
       dv[6 * n + id] = u * bt_ - w * br_;
       dv[7 * n + id] = w * bp_ - v * bt_;
     }
+  }
   }
 }
 
@@ -424,7 +443,7 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__res
       const double *hl = H + (size_t)(j + 4) * SR + l;
       double rho = hl[0], v = hl[HS];
       const double *ol = O + (size_t)j * SR + l;
-      double cscth = 1.0 / g.sines[it];
+      double cscth = g.csc[it];
       double oors = ri * cscth;
       double t = in_[k][5], oorho = 1.0 / rho;
       double w1 = ol[0] * oors;
@@ -853,7 +872,7 @@ __global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__re
     int it = t0 + j, ip = pb + l;
     if (ip >= g.nphi) continue;
     size_t id = css_idx(g, it, ip, ir);
-    out[2 * n + id] = O[(size_t)l * SO + j] * (1.0 / g.sines[it]) * invr;
+    out[2 * n + id] = O[(size_t)l * SO + j] * g.csc[it] * invr;
     out[n + id] = -O[(size_t)(TL + l) * SO + j] * invr;
   }
 }
@@ -888,7 +907,7 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__rest
     int it = tb + l, ip = p0 + j;
     if (it >= g.nth) continue;
     size_t id = css_idx(g, it, ip, ir);
-    double csc = 1.0 / g.sines[it];
+    double csc = g.csc[it];
     out[id] = invr * O[(size_t)j * SR + l] * csc;
     out[2 * n + id] = out[2 * n + id] - invr * O[OS + (size_t)j * SR + l] * csc;
   }
@@ -990,9 +1009,17 @@ __global__ void k_sld_vcc(CssGeo g, const double *__restrict__ v, const double *
   }
 }
 
+// q * max(0, min(1, q*qph / max(|q|,tiny)^2)).  For |q| >= tiny the ratio is
+// qph/q, so the limited value is 0 (opposite signs), q (|qph| >= |q|) or qph:
+// a minmod, evaluated without the division (equal to the reference's
+// product to within its roundings); below tiny the formula as written.
 __device__ __forceinline__ double sld_limiter(double q, double qph, double tiny) {
-  double rtmp = fabs(q);
-  rtmp = 1.0 / fmax(rtmp, tiny);
+  const double a = fabs(q);
+  if (a >= tiny) {
+    if (!(q * qph > 0.0)) return q * 0.0;
+    return fabs(qph) >= a ? q : qph;
+  }
+  double rtmp = 1.0 / tiny;
   rtmp = q * (rtmp * rtmp);
   rtmp = rtmp * qph;
   rtmp = fmin(1.0, rtmp);
