@@ -301,6 +301,11 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     set_err("css_create: ohmic heating needs magnetic diffusion");
     return CSS_ERR_ARG;
   }
+  if (p.sldiffusion && (p.nth % 2)) {
+    // the SLD kernel streams theta pairs with 16-byte copies
+    set_err("css_create: slope-limited diffusion needs an even nth (got %d)", p.nth);
+    return CSS_ERR_ARG;
+  }
   if (p.precision != 0) {
     set_err("css_create: precision %d not available in this build", p.precision);
     return CSS_ERR_ARG;

@@ -1114,15 +1114,64 @@ __device__ __forceinline__ double sld_ghost_t(const CssGeo &g, int iv, double q0
 #define SLD_TT 32
 #define SLD_TP 8
 #define SLD_RC 16
+#define SLD_XW (SLD_TT + 4)  // plane row: 36 doubles = 288 B, so 16-byte copies stay aligned
 template <int NF>
 struct SldSmem {
-  double X[NF][SLD_TP + 4][SLD_TT + 5];   // field planes, halo 2
-  double V[SLD_TP + 2][SLD_TT + 3];       // vcc plane, halo 1
+  double X[2][NF][SLD_TP + 4][SLD_XW];    // field planes (halo 2) of radii ir and ir+1
+  double V[2][SLD_TP + 2][SLD_TT + 3];    // vcc planes (halo 1)
   double FT[NF][SLD_TP][SLD_TT + 1];      // theta faces
   double FP[NF][SLD_TP + 1][SLD_TT];      // phi faces
   double ST[SLD_TP][SLD_TT + 1];          // theta face speed * sin(face)
   double SP[SLD_TP + 1][SLD_TT];          // phi face speed
 };
+
+// asynchronous global -> shared copies (completion tracked per commit group)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Starts the copies of radius ir's planes (every diffused field with a
+// 2-point halo, raw values; the speed plane with a 1-point halo, theta
+// clamped) into buffer `buf`: 16-byte copies of theta pairs (the tile's
+// first theta is even, and so is nth on this path), zero fill outside
+// 0 <= theta < nth, periodic phi.
+template <int NF>
+__device__ __forceinline__ void sld_issue_plane(const CssGeo &g, const double *__restrict__ v,
+                                                const double *__restrict__ av, const double *__restrict__ vcc,
+                                                SldSmem<NF> &S, int buf, int ir, int t0, int p0, int off) {
+  const size_t n = (size_t)g.ncell, pl = plane(g, ir);
+  const int nth = g.nth, nphi = g.nphi;
+  constexpr int PAIRS = SLD_XW / 2, ROWS = SLD_TP + 4, NX = NF * ROWS * PAIRS;
+  for (int k = threadIdx.x; k < NX; k += SLD_TT * SLD_TP) {
+    const int f = k / (ROWS * PAIRS), rem = k - f * (ROWS * PAIRS);
+    const int bb = rem / PAIRS, a2 = rem - bb * PAIRS;
+    const int gt = t0 - 2 + 2 * a2;
+    int gp = p0 + bb - 2;
+    gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
+    const int iv = f + off;
+    const double *fp = (iv >= 5 ? av + (size_t)(iv - 5) * n : v + (size_t)iv * n) + pl;
+    const bool in = gt >= 0 && gt < nth;
+    cp_async16(&S.X[buf][f][bb][2 * a2], in ? fp + (size_t)gp * nth + gt : fp, in ? 16 : 0);
+  }
+  constexpr int NVV = (SLD_TP + 2) * (SLD_TT + 2);
+  const double *vp = vcc + pl;
+  for (int k = threadIdx.x; k < NVV; k += SLD_TT * SLD_TP) {
+    const int a = k % (SLD_TT + 2), bb = k / (SLD_TT + 2);
+    const int gt = min(max(t0 + a - 1, 0), nth - 1);
+    int gp = p0 + bb - 1;
+    gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
+    cp_async8(&S.V[buf][bb][a], vp + (size_t)gp * nth + gt, 8);
+  }
+  cp_async_commit();
+}
 
 template <int NF>
 __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const double *__restrict__ v,
@@ -1131,8 +1180,6 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
                                                             double *__restrict__ dout) {
   extern __shared__ double sm_raw[];
   SldSmem<NF> &S = *reinterpret_cast<SldSmem<NF> *>(sm_raw);
-  auto &X = S.X;
-  auto &V = S.V;
   auto &FT = S.FT;
   auto &FP = S.FP;
   auto &ST = S.ST;
@@ -1169,7 +1216,11 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
                  (sld_face(xr(r0 - 2), win[f][0], win[f][1], win[f][2], g.tinyvar[iv]) * g.sld_r[2 * nr + r0]);
     }
   }
+  sld_issue_plane<NF>(g, v, av, vcc, S, 0, r0, t0, p0, off);
   for (int ir = r0; ir < r1; ir++) {
+    const int cb = (ir - r0) & 1;
+    auto &X = S.X[cb];
+    auto &V = S.V[cb];
     const double t3 = g.sld_r[ir], rfac = g.sld_r[nr + ir], rhi2 = g.sld_r[3 * nr + ir];
     const double cphl = g.sld_th[nth + itc], cphh = g.sld_th[3 * nth + itc];
     const double geom = g.sld_th[4 * nth + itc] * (rfac / g.dphi);
@@ -1183,29 +1234,26 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
       const int q = ir + 3;
       nxt[f] = (q < nr) ? sld_val(g, v, av, f + off, itc, ipc, q) : 0.0;
     }
-    (void)0;
-    __syncthreads();
-    {
-      const double *vp = vcc + plane(g, ir);
-      for (int k = threadIdx.x; k < (SLD_TP + 2) * (SLD_TT + 2); k += blockDim.x) {
-        int a = k % (SLD_TT + 2), bb = k / (SLD_TT + 2);
-        int gt = min(max(t0 + a - 1, 0), nth - 1), gp = p0 + bb - 1;
-        gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
-        V[bb][a] = __ldg(vp + (size_t)gp * nth + gt);
-      }
+    // radius ir+1 streams into the other buffer while this radius is computed
+    // (that buffer's last readers finished before the previous radius's
+    // last barrier)
+    if (ir + 1 < r1) {
+      sld_issue_plane<NF>(g, v, av, vcc, S, cb ^ 1, ir + 1, t0, p0, off);
+      cp_async_wait<1>();
+    } else {
+      cp_async_wait<0>();
     }
+    __syncthreads();
+    // the diffused rho and s are the deviations from the mean state
 #pragma unroll
     for (int f = 0; f < NF; f++) {
       const int iv = f + off;
-      const double *fp = (iv >= 5 ? av + (size_t)(iv - 5) * n : v + (size_t)iv * n) + plane(g, ir);
-      const double mean = (iv == 0) ? g.rhor[ir] : (iv == 4 ? g.sr[ir] : 0.0);
-      for (int k = threadIdx.x; k < (SLD_TP + 4) * (SLD_TT + 4); k += blockDim.x) {
-        int a = k % (SLD_TT + 4), bb = k / (SLD_TT + 4);
-        int gt = t0 + a - 2, gp = p0 + bb - 2;
-        gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
-        double q = 0.0;
-        if (gt >= 0 && gt < nth) q = __ldg(fp + (size_t)gp * nth + gt) - mean;
-        X[f][bb][a] = q;
+      if (iv != 0 && iv != 4) continue;
+      const double mean = (iv == 0) ? g.rhor[ir] : g.sr[ir];
+      for (int k = threadIdx.x; k < (SLD_TP + 4) * SLD_XW; k += SLD_TT * SLD_TP) {
+        const int a = k % SLD_XW, bb = k / SLD_XW;
+        const int gt = t0 + a - 2;
+        if (gt >= 0 && gt < nth) X[f][bb][a] -= mean;
       }
     }
     __syncthreads();
