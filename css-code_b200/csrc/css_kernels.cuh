@@ -1280,23 +1280,35 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
       SP[b][a] = g.sld_coef * sqrt(0.5 * (V[b][a + 1] + V[b + 1][a + 1]));
     }
     __syncthreads();
-    // face fluxes of every field
+    // face fluxes of every field: each thread takes the upper theta face and
+    // the upper phi face of its cell; the first column / row of the tile
+    // also take the lower face
 #pragma unroll
     for (int f = 0; f < NF; f++) {
       const double tiny = g.tinyvar[f + off];
-      for (int k = threadIdx.x; k < SLD_TP * (SLD_TT + 1); k += blockDim.x) {
-        int a = k % (SLD_TT + 1), bb = k / (SLD_TT + 1);
-        int gt = t0 + a;
+      auto tface = [&](int bb, int a) {
+        const int gt = t0 + a;
         double d = 0.0;
         if (gt > 0 && gt < nth)
           d = ST[bb][a] * sld_face(X[f][bb + 2][a], X[f][bb + 2][a + 1], X[f][bb + 2][a + 2], X[f][bb + 2][a + 3], tiny);
         FT[f][bb][a] = d;
-      }
-      for (int k = threadIdx.x; k < (SLD_TP + 1) * SLD_TT; k += blockDim.x) {
-        int a = k % SLD_TT, bb = k / SLD_TT;
+      };
+      auto pface = [&](int bb, int a) {
         FP[f][bb][a] =
             SP[bb][a] * sld_face(X[f][bb][a + 2], X[f][bb + 1][a + 2], X[f][bb + 2][a + 2], X[f][bb + 3][a + 2], tiny);
-      }
+      };
+      tface(ty, tx + 1);
+      pface(ty + 1, tx);
+      if (tx == 0) tface(ty, 0);
+      if (ty == 0) pface(0, tx);
+    }
+    // the velocities of this cell, taken from the tile when they are diffused
+    // fields (before the barrier: the next radius's copies reuse the buffer)
+    double uu[4];
+#pragma unroll
+    for (int k = 1; k <= 3; k++) {
+      const int f = k - off;
+      uu[k] = (f >= 0 && f < NF) ? X[f >= 0 && f < NF ? f : 0][ty + 2][tx + 2] : __ldg(v + k * n + css_idx(g, itc, ipc, ir));
     }
     __syncthreads();
     double Dv[NF];
@@ -1337,13 +1349,14 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     }
     double rho = __ldg(v + id);
     double invrho = 1.0 / rho;
-    double itemp = (pow(rho, -g.gamm1)) * exp(-__ldg(v + 4 * n + id) * g.invcv) / g.invtconst;
+    // 1/T = rho^(1-gamma) exp(-s/Cv) / invtconst, as one exponential
+    double itemp = exp(-fma(g.gamm1, log(rho), __ldg(v + 4 * n + id) * g.invcv)) / g.invtconst;
     if (g.do_viscous_heating)
 #pragma unroll
-      for (int k = 1; k <= 3; k++) D[4] = D[4] - __ldg(v + k * n + id) * D[k] * itemp;
+      for (int k = 1; k <= 3; k++) D[4] = D[4] - uu[k] * D[k] * itemp;
     if (g.mass_diffusion) {
 #pragma unroll
-      for (int k = 1; k <= 3; k++) D[k] = D[k] - invrho * __ldg(v + k * n + id) * D[0];
+      for (int k = 1; k <= 3; k++) D[k] = D[k] - invrho * uu[k] * D[0];
       D[4] = D[4] - (g.gamm1 * g.cv) * invrho * D[0];
     }
 #pragma unroll
