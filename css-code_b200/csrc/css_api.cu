@@ -251,6 +251,8 @@ static int setup_kernels() {
   CUDA_TRY(cudaFuncSetAttribute(k_sld<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<8>)));
   if (int rc = setup_mt<16, 16>()) return rc;
   if (int rc = setup_mt<32, 16>()) return rc;
+  if (int rc = setup_mt<16, 8>()) return rc;
+  if (int rc = setup_mt<32, 8>()) return rc;
   int mx = 200 * 1024;
   CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
@@ -263,11 +265,14 @@ static int setup_kernels() {
 }
 
 // launch KERNEL<MT> with MT = c->mt[DIR] chosen at run time
-#define LAUNCH_MT(DIR, KERNEL, GRID, SMEM, ...)                                          \
+// and the compile-time tile of TLV lines (8 or 16) when MT > 0
+#define LAUNCH_MT(DIR, TLV, KERNEL, GRID, SMEM, ...)                                     \
   do {                                                                                    \
-    switch (c->mt[DIR]) {                                                                 \
-      case 16: KERNEL<16, 16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;       \
-      case 32: KERNEL<32, 16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;       \
+    switch (c->mt[DIR] * 100 + (TLV)) {                                                   \
+      case 1616: KERNEL<16, 16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;     \
+      case 3216: KERNEL<32, 16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;     \
+      case 1608: KERNEL<16, 8><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;      \
+      case 3208: KERNEL<32, 8><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;      \
       default: KERNEL<0, 0><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;         \
     }                                                                                     \
   } while (0)
@@ -622,19 +627,19 @@ static int launch_curl(css_ctx *c, const double *a, double *out, int apply_bc) {
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_CURL_THETA);
-  LAUNCH_MT(1, k_curl_theta, gt, smem_theta(2, 2, mt, TL), g, a, out, TL);
+  LAUNCH_MT(1, TL, k_curl_theta, gt, smem_theta(2, 2, mt, TL), g, a, out, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
   prof_begin(c, KI_CURL_PHI);
-  LAUNCH_MT(2, k_curl_phi, gp, smem_line(2, 2, 0, mp, TL), g, a, out, TL);
+  LAUNCH_MT(2, TL, k_curl_phi, gp, smem_line(2, 2, 0, mp, TL), g, a, out, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_CURL_R);
-  LAUNCH_MT(0, k_curl_r, gr, smem_line(2, 2, 0, mr, TL), g, a, out, TL, apply_bc);
+  LAUNCH_MT(0, TL, k_curl_r, gr, smem_line(2, 2, 0, mr, TL), g, a, out, TL, apply_bc);
   prof_end(c);
   return check_launch(c);
 }
@@ -649,25 +654,25 @@ static int launch_rhs(css_ctx *c, const double *cur, double *nx, int stage, doub
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_THETA);
-  LAUNCH_MT(1, k_theta_terms, gt, smem_theta_terms(mag, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  LAUNCH_MT(1, TL, k_theta_terms, gt, smem_theta_terms(mag, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
   prof_begin(c, KI_PHI);
-  LAUNCH_MT(2, k_phi_terms, gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  LAUNCH_MT(2, TL, k_phi_terms, gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_RADIAL);
-  LAUNCH_MT(0, k_radial_terms, gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  LAUNCH_MT(0, TL, k_radial_terms, gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_RHOT_UPDATE);
-  LAUNCH_MT(1, k_rhot_update, gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+  LAUNCH_MT(1, TL, k_rhot_update, gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
             TL, c->flag);
   prof_end(c);
   return check_launch(c);
@@ -952,6 +957,181 @@ extern "C" int css_kernel_stats(css_ctx *c, int kind, const char **name, double 
   if (launches) *launches = c->k_count[kind];
   return CSS_OK;
 }
+
+// ---------------------------------------------------------------------------
+// Tile autotuner: for each sweep direction, the RHS of the resident state is
+// timed with every tile height that direction's kernels have (8 or 16
+// lines for the compile-time block lengths; 16, 8, 4 lines that fit for
+// the generic kernels) and the fastest is kept.  Every line's arithmetic is
+// the same for any tile height, so the choice changes no result bit.
+// ---------------------------------------------------------------------------
+extern "C" int css_autotune(css_ctx *c, int reps, int *chosen) {
+  if (!c || reps < 1) { set_err("css_autotune: bad argument"); return CSS_ERR_ARG; }
+  const int prof_was = c->profiling;
+  c->profiling = 0;
+  cudaEvent_t e0, e1;
+  CUDA_TRY(cudaEventCreate(&e0));
+  CUDA_TRY(cudaEventCreate(&e1));
+  int *tl[3] = {&c->tl_r, &c->tl_theta, &c->tl_phi};
+  const int dirs[3] = {1, 2, 0};  // theta (theta terms, rhot, curl), phi, r
+  int rc = CSS_OK;
+  for (int di = 0; di < 3 && rc == CSS_OK; di++) {
+    const int d = dirs[di];
+    const int mag = c->g.magnetic, m = c->g.d[d].maxm;
+    std::vector<int> cand;
+    if (c->mt[d]) cand = {16, 8};
+    else
+      for (int t : {16, 8, 4}) {
+        size_t need = d == 1 ? std::max(smem_theta_terms(mag, m, t), smem_rhot(m, t))
+                             : (d == 2 ? smem_phi_terms(mag, m, t) : smem_radial_terms(mag, m, t));
+        if (need <= kSmemCap) cand.push_back(t);
+      }
+    int best = *tl[d];
+    float best_ms = 1e30f;
+    for (int t : cand) {
+      *tl[d] = t;
+      if ((rc = launch_rhs(c, c->v0, nullptr, 0, 0.0))) break;  // warm
+      cudaEventRecord(e0, c->stream);
+      for (int k = 0; k < reps && rc == CSS_OK; k++) rc = launch_rhs(c, c->v0, nullptr, 0, 0.0);
+      cudaEventRecord(e1, c->stream);
+      if (rc) break;
+      if (cudaEventSynchronize(e1) != cudaSuccess) { set_err("css_autotune: timing failed"); rc = CSS_ERR_CUDA; break; }
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best_ms) { best_ms = ms; best = t; }
+    }
+    *tl[d] = best;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  c->profiling = prof_was;
+  if (chosen) { chosen[0] = c->tl_r; chosen[1] = c->tl_theta; chosen[2] = c->tl_phi; }
+  return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Batched ensemble: one RK4 step of every member is captured once into a
+// CUDA graph (each member's kernels on a stream of its own, forked from and
+// joined to the ensemble's root stream, so small members run side by side)
+// and the graph is replayed for every step.  Members keep their own state,
+// parameters and tables; the graph is captured again when a time step
+// changes.
+// ---------------------------------------------------------------------------
+struct css_ensemble {
+  std::vector<css_ctx *> m;
+  std::vector<cudaStream_t> ms;
+  std::vector<cudaEvent_t> join;
+  std::vector<double> dt;
+  cudaStream_t root = nullptr;
+  cudaEvent_t fork = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long long launches_per_step = 0, launches = 0;
+};
+
+extern "C" void css_ensemble_destroy(css_ensemble *e) {
+  if (!e) return;
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  for (auto s : e->ms) cudaStreamDestroy(s);
+  for (auto v : e->join) cudaEventDestroy(v);
+  if (e->fork) cudaEventDestroy(e->fork);
+  if (e->root) cudaStreamDestroy(e->root);
+  delete e;
+}
+
+extern "C" int css_ensemble_create(int nmem, css_ctx *const *members, css_ensemble **out) {
+  if (!out || nmem < 1 || !members) { set_err("css_ensemble_create: bad argument"); return CSS_ERR_ARG; }
+  *out = nullptr;
+  for (int i = 0; i < nmem; i++)
+    if (!members[i]) { set_err("css_ensemble_create: member %d is NULL", i); return CSS_ERR_ARG; }
+  css_ensemble *e = new css_ensemble();
+  e->m.assign(members, members + nmem);
+  e->ms.resize(nmem);
+  e->join.resize(nmem);
+  cudaError_t err = cudaStreamCreateWithFlags(&e->root, cudaStreamNonBlocking);
+  if (!err) err = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+  for (int i = 0; i < nmem && !err; i++) {
+    err = cudaStreamCreateWithFlags(&e->ms[i], cudaStreamNonBlocking);
+    if (!err) err = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
+  }
+  if (err) {
+    set_err("css_ensemble_create: %s", cudaGetErrorString(err));
+    css_ensemble_destroy(e);
+    return CSS_ERR_CUDA;
+  }
+  *out = e;
+  return CSS_OK;
+}
+
+static int ensemble_capture(css_ensemble *e, const double *dt) {
+  if (e->exec) { cudaGraphExecDestroy(e->exec); e->exec = nullptr; }
+  if (e->graph) { cudaGraphDestroy(e->graph); e->graph = nullptr; }
+  const int nm = (int)e->m.size();
+  CUDA_TRY(cudaStreamBeginCapture(e->root, cudaStreamCaptureModeThreadLocal));
+  int rc = CSS_OK;
+  long long l0 = 0, l1 = 0;
+  cudaError_t err = cudaEventRecord(e->fork, e->root);
+  for (int i = 0; i < nm && !rc && !err; i++) {
+    css_ctx *c = e->m[i];
+    err = cudaStreamWaitEvent(e->ms[i], e->fork, 0);
+    if (err) break;
+    cudaStream_t keep = c->stream;
+    const int prof = c->profiling;
+    c->stream = e->ms[i];
+    c->profiling = 0;
+    l0 = c->launches;
+    rc = step_once(c, dt[i]);
+    l1 += c->launches - l0;
+    c->stream = keep;
+    c->profiling = prof;
+    if (!rc) err = cudaEventRecord(e->join[i], e->ms[i]);
+    if (!rc && !err) err = cudaStreamWaitEvent(e->root, e->join[i], 0);
+  }
+  cudaGraph_t g = nullptr;
+  cudaError_t end = cudaStreamEndCapture(e->root, &g);
+  if (rc || err || end) {
+    if (g) cudaGraphDestroy(g);
+    if (!rc) {
+      set_err("css_ensemble_step: capture failed: %s", cudaGetErrorString(err ? err : end));
+      rc = CSS_ERR_CUDA;
+    }
+    return rc;
+  }
+  e->graph = g;
+  CUDA_TRY(cudaGraphInstantiate(&e->exec, e->graph, 0));
+  e->dt.assign(dt, dt + nm);
+  e->launches_per_step = l1;
+  return CSS_OK;
+}
+
+extern "C" int css_ensemble_step(css_ensemble *e, const double *dt, int nsteps) {
+  if (!e || !dt || nsteps < 0) { set_err("css_ensemble_step: bad argument"); return CSS_ERR_ARG; }
+  const int nm = (int)e->m.size();
+  for (int i = 0; i < nm; i++)
+    if (!(dt[i] > 0.0)) { set_err("css_ensemble_step: dt[%d] must be positive", i); return CSS_ERR_ARG; }
+  bool same = e->exec != nullptr;
+  for (int i = 0; i < nm && same; i++) same = (e->dt[i] == dt[i]);
+  // order after whatever each member's own stream has queued (uploads)
+  for (int i = 0; i < nm; i++) {
+    CUDA_TRY(cudaEventRecord(e->join[i], e->m[i]->stream));
+    CUDA_TRY(cudaStreamWaitEvent(e->root, e->join[i], 0));
+  }
+  if (!same)
+    if (int rc = ensemble_capture(e, dt)) return rc;
+  for (int i = 0; i < nm; i++) CUDA_TRY(cudaMemsetAsync(e->m[i]->flag, 0, sizeof(int), e->root));
+  for (int s = 0; s < nsteps; s++) CUDA_TRY(cudaGraphLaunch(e->exec, e->root));
+  e->launches += e->launches_per_step * nsteps;
+  std::vector<int> h(nm, 0);
+  for (int i = 0; i < nm; i++)
+    CUDA_TRY(cudaMemcpyAsync(&h[i], e->m[i]->flag, sizeof(int), cudaMemcpyDeviceToHost, e->root));
+  CUDA_TRY(cudaStreamSynchronize(e->root));
+  for (int i = 0; i < nm; i++)
+    if (h[i]) { set_err("css_ensemble_step: non-finite value in member %d", i); return CSS_ERR_NAN; }
+  return CSS_OK;
+}
+
+extern "C" long long css_ensemble_launches(css_ensemble *e) { return e ? e->launches : -1; }
 
 // ---------------------------------------------------------------------------
 // Diagnostics of the current state (vars0): Scalar_Output, Compute_Step_Size,

@@ -56,6 +56,14 @@ def lib():
         L.css_step_size.argtypes = [ctypes.c_void_p, ctypes.c_double, dp]
         L.css_shell_averages.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, dp, dp]
         L.css_spectrum.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
+        L.css_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.css_ensemble_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
+                                          ctypes.POINTER(ctypes.c_void_p)]
+        L.css_ensemble_step.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
+        L.css_ensemble_launches.argtypes = [ctypes.c_void_p]
+        L.css_ensemble_launches.restype = ctypes.c_longlong
+        L.css_ensemble_destroy.argtypes = [ctypes.c_void_p]
+        L.css_ensemble_destroy.restype = None
         _LIB = L
     return _LIB
 
@@ -72,5 +80,6 @@ EXPORTS = [
     "css_step_rk4_host", "css_rhs", "css_diffusion", "css_deriv", "css_deriv_dev", "css_dbyd1_dt0",
     "css_compact_lines", "css_sync", "css_state_device_ptr", "css_kernel_launches", "css_set_stream",
     "css_profile", "css_kernel_stats", "css_compact_lines_noalloc", "css_scalars", "css_step_size",
-    "css_shell_averages", "css_spectrum",
+    "css_shell_averages", "css_spectrum", "css_autotune", "css_ensemble_create", "css_ensemble_step",
+    "css_ensemble_launches", "css_ensemble_destroy",
 ]

@@ -98,6 +98,14 @@ class Simulation:
                 out[nm.value.decode()] = (ms.value, cnt.value)
         return out
 
+    def autotune(self, reps=3):
+        """Time every tile height of each sweep direction on the resident state
+        and keep the fastest (css_autotune); returns (r, theta, phi) lines
+        per CTA.  Results are unchanged bit for bit."""
+        ch = (ctypes.c_int * 3)()
+        check(_lib.lib().css_autotune(self.h, int(reps), ch))
+        return tuple(ch)
+
     # diagnostics of the current state ----------------------------------------
     SCALAR_NAMES = ("kinener", "cke", "mcke", "drke", "umach", "magener", "bmax")
     STEP_SIZE_NAMES = ("dtmax", "Etot", "Ltot", "mtot", "mrsint")

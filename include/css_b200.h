@@ -226,6 +226,35 @@ int css_profile(css_ctx *ctx, int enable);
 int css_kernel_stats(css_ctx *ctx, int kind, const char **name, double *total_ms,
                      long long *launches);
 
+/* ---- tile autotuning and batched ensembles ---------------------------------
+ * css_autotune times, on the resident state and with reps RHS evaluations
+ * per candidate, every tile height (lines per CTA) that each sweep
+ * direction's kernels offer and keeps the fastest; chosen[3] (may be NULL)
+ * receives the r, theta and phi choices.  The state is not modified and no
+ * result changes: every line's arithmetic is the same for any tile height.
+ * This has no counterpart in the reference (its per-rank loops have fixed
+ * extents).                                                                */
+int css_autotune(css_ctx *ctx, int reps, int *chosen);
+
+/* A batched ensemble of independent runs (many small shells, each with its
+ * own grid, decomposition and parameters: hydro and MHD members may mix).
+ * css_ensemble_step advances every member by nsteps RK4 steps of its own
+ * dt[i]: one step of all members is captured once into a CUDA graph, each
+ * member's kernels on a stream of its own so small members share the GPU,
+ * and the graph is replayed per step (it is captured again when a dt
+ * changes).  The first call, and every call with a new dt, must not be made
+ * during another stream capture.  Member contexts stay owned by the caller
+ * and must outlive the ensemble; a member must not be stepped through
+ * css_step_rk4 while an ensemble step is running.  Returns CSS_ERR_NAN
+ * (naming the member) when a member's state went non-finite.  The ensemble
+ * has no counterpart in the reference, which runs one shell per job.       */
+typedef struct css_ensemble css_ensemble;
+int css_ensemble_create(int nmem, css_ctx *const *members, css_ensemble **out);
+int css_ensemble_step(css_ensemble *ens, const double *dt, int nsteps);
+/* kernels launched by all replays so far */
+long long css_ensemble_launches(css_ensemble *ens);
+void css_ensemble_destroy(css_ensemble *ens);
+
 /* ---- diagnostics of the current state (vars0), computed on the device ----
  * Each call reads the state left by css_upload_state / css_step_rk4, uses
  * the stage buffers as scratch (so it must not overlap a step on another
