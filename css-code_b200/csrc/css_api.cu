@@ -1026,6 +1026,8 @@ struct css_ensemble {
   cudaEvent_t fork = nullptr;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
+  cudaEvent_t t0 = nullptr, t1 = nullptr;  // around the replays of the last step call
+  double last_ms = 0.0;
   long long launches_per_step = 0, launches = 0;
 };
 
@@ -1036,6 +1038,8 @@ extern "C" void css_ensemble_destroy(css_ensemble *e) {
   for (auto s : e->ms) cudaStreamDestroy(s);
   for (auto v : e->join) cudaEventDestroy(v);
   if (e->fork) cudaEventDestroy(e->fork);
+  if (e->t0) cudaEventDestroy(e->t0);
+  if (e->t1) cudaEventDestroy(e->t1);
   if (e->root) cudaStreamDestroy(e->root);
   delete e;
 }
@@ -1051,6 +1055,8 @@ extern "C" int css_ensemble_create(int nmem, css_ctx *const *members, css_ensemb
   e->join.resize(nmem);
   cudaError_t err = cudaStreamCreateWithFlags(&e->root, cudaStreamNonBlocking);
   if (!err) err = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+  if (!err) err = cudaEventCreate(&e->t0);
+  if (!err) err = cudaEventCreate(&e->t1);
   for (int i = 0; i < nmem && !err; i++) {
     err = cudaStreamCreateWithFlags(&e->ms[i], cudaStreamNonBlocking);
     if (!err) err = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
@@ -1120,16 +1126,23 @@ extern "C" int css_ensemble_step(css_ensemble *e, const double *dt, int nsteps) 
   if (!same)
     if (int rc = ensemble_capture(e, dt)) return rc;
   for (int i = 0; i < nm; i++) CUDA_TRY(cudaMemsetAsync(e->m[i]->flag, 0, sizeof(int), e->root));
+  CUDA_TRY(cudaEventRecord(e->t0, e->root));
   for (int s = 0; s < nsteps; s++) CUDA_TRY(cudaGraphLaunch(e->exec, e->root));
+  CUDA_TRY(cudaEventRecord(e->t1, e->root));
   e->launches += e->launches_per_step * nsteps;
   std::vector<int> h(nm, 0);
   for (int i = 0; i < nm; i++)
     CUDA_TRY(cudaMemcpyAsync(&h[i], e->m[i]->flag, sizeof(int), cudaMemcpyDeviceToHost, e->root));
   CUDA_TRY(cudaStreamSynchronize(e->root));
+  float ms = 0.f;
+  CUDA_TRY(cudaEventElapsedTime(&ms, e->t0, e->t1));
+  e->last_ms = ms;
   for (int i = 0; i < nm; i++)
     if (h[i]) { set_err("css_ensemble_step: non-finite value in member %d", i); return CSS_ERR_NAN; }
   return CSS_OK;
 }
+
+extern "C" double css_ensemble_last_ms(css_ensemble *e) { return e ? e->last_ms : -1.0; }
 
 extern "C" long long css_ensemble_launches(css_ensemble *e) { return e ? e->launches : -1; }
 

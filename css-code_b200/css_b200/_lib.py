@@ -62,6 +62,8 @@ def lib():
         L.css_ensemble_step.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
         L.css_ensemble_launches.argtypes = [ctypes.c_void_p]
         L.css_ensemble_launches.restype = ctypes.c_longlong
+        L.css_ensemble_last_ms.argtypes = [ctypes.c_void_p]
+        L.css_ensemble_last_ms.restype = ctypes.c_double
         L.css_ensemble_destroy.argtypes = [ctypes.c_void_p]
         L.css_ensemble_destroy.restype = None
         _LIB = L
@@ -81,5 +83,5 @@ EXPORTS = [
     "css_compact_lines", "css_sync", "css_state_device_ptr", "css_kernel_launches", "css_set_stream",
     "css_profile", "css_kernel_stats", "css_compact_lines_noalloc", "css_scalars", "css_step_size",
     "css_shell_averages", "css_spectrum", "css_autotune", "css_ensemble_create", "css_ensemble_step",
-    "css_ensemble_launches", "css_ensemble_destroy",
+    "css_ensemble_launches", "css_ensemble_last_ms", "css_ensemble_destroy",
 ]

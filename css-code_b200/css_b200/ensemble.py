@@ -119,6 +119,10 @@ class Ensemble:
     def launches(self):
         return _lib.lib().css_ensemble_launches(self.h)
 
+    def last_ms(self):
+        """Device time of the replays of the last step() call (CUDA events)."""
+        return _lib.lib().css_ensemble_last_ms(self.h)
+
     def close(self):
         if getattr(self, "h", None):
             _lib.lib().css_ensemble_destroy(self.h)

@@ -253,6 +253,9 @@ int css_ensemble_create(int nmem, css_ctx *const *members, css_ensemble **out);
 int css_ensemble_step(css_ensemble *ens, const double *dt, int nsteps);
 /* kernels launched by all replays so far */
 long long css_ensemble_launches(css_ensemble *ens);
+/* device time (CUDA events on the ensemble stream) of the replays of the
+ * last css_ensemble_step call, in milliseconds                             */
+double css_ensemble_last_ms(css_ensemble *ens);
 void css_ensemble_destroy(css_ensemble *ens);
 
 /* ---- diagnostics of the current state (vars0), computed on the device ----
