@@ -231,13 +231,24 @@ extern "C" void css_destroy(css_ctx *c) {
 template <int MT, int TLC>
 static int setup_mt() {
   int mx = 200 * 1024;
-  CUDA_TRY(cudaFuncSetAttribute(k_theta_terms<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_phi_terms<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_radial_terms<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_rhot_update<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_theta<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_phi<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  CUDA_TRY(cudaFuncSetAttribute(k_curl_r<MT, TLC>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
+#define CSS_SMEM_ATTR(...) CUDA_TRY(cudaFuncSetAttribute(__VA_ARGS__, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
+  CSS_SMEM_ATTR(k_theta_terms<MT, TLC, double>);
+  CSS_SMEM_ATTR(k_theta_terms<MT, TLC, float>);
+  CSS_SMEM_ATTR(k_phi_terms<MT, TLC, double>);
+  CSS_SMEM_ATTR(k_phi_terms<MT, TLC, float>);
+  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, double>);
+  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, float>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, float>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, float>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, double>);
+  CSS_SMEM_ATTR(k_curl_theta<MT, TLC, double>);
+  CSS_SMEM_ATTR(k_curl_theta<MT, TLC, float>);
+  CSS_SMEM_ATTR(k_curl_phi<MT, TLC, double>);
+  CSS_SMEM_ATTR(k_curl_phi<MT, TLC, float>);
+  CSS_SMEM_ATTR(k_curl_r<MT, TLC, double>);
+  CSS_SMEM_ATTR(k_curl_r<MT, TLC, float>);
+#undef CSS_SMEM_ATTR
   return CSS_OK;
 }
 
@@ -265,15 +276,17 @@ static int setup_kernels() {
 }
 
 // launch KERNEL<MT> with MT = c->mt[DIR] chosen at run time
-// and the compile-time tile of TLV lines (8 or 16) when MT > 0
-#define LAUNCH_MT(DIR, TLV, KERNEL, GRID, SMEM, ...)                                     \
+// and the compile-time tile of TLV lines (8 or 16) when MT > 0; XT is the
+// parenthesised list of the kernel's storage-type template arguments
+#define CSS_STRIP(...) __VA_ARGS__
+#define LAUNCH_MT(DIR, TLV, KERNEL, XT, GRID, SMEM, ...)                                 \
   do {                                                                                    \
     switch (c->mt[DIR] * 100 + (TLV)) {                                                   \
-      case 1616: KERNEL<16, 16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;     \
-      case 3216: KERNEL<32, 16><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;     \
-      case 1608: KERNEL<16, 8><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;      \
-      case 3208: KERNEL<32, 8><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;      \
-      default: KERNEL<0, 0><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;         \
+      case 1616: KERNEL<16, 16, CSS_STRIP XT><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break; \
+      case 3216: KERNEL<32, 16, CSS_STRIP XT><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break; \
+      case 1608: KERNEL<16, 8, CSS_STRIP XT><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;  \
+      case 3208: KERNEL<32, 8, CSS_STRIP XT><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;  \
+      default: KERNEL<0, 0, CSS_STRIP XT><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;     \
     }                                                                                     \
   } while (0)
 
@@ -311,8 +324,8 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     set_err("css_create: slope-limited diffusion needs an even nth (got %d)", p.nth);
     return CSS_ERR_ARG;
   }
-  if (p.precision != 0) {
-    set_err("css_create: precision %d not available in this build", p.precision);
+  if (p.precision != 0 && p.precision != 1) {
+    set_err("css_create: precision %d unknown (0 FP64, 1 mixed: FP32 stage states)", p.precision);
     return CSS_ERR_ARG;
   }
   css_ctx *c = new css_ctx();
@@ -621,31 +634,34 @@ static int check_launch(css_ctx *c) {
   return CSS_OK;
 }
 
-static int launch_curl(css_ctx *c, const double *a, double *out, int apply_bc) {
+template <typename TS>
+static int launch_curl(css_ctx *c, const TS *a, double *out, int apply_bc) {
   const CssGeo &g = c->g;
   int mt = g.d[1].maxm, mp = g.d[2].maxm, mr = g.d[0].maxm;
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_CURL_THETA);
-  LAUNCH_MT(1, TL, k_curl_theta, gt, smem_theta(2, 2, mt, TL), g, a, out, TL);
+  LAUNCH_MT(1, TL, k_curl_theta, (TS), gt, smem_theta(2, 2, mt, TL), g, a, out, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
   prof_begin(c, KI_CURL_PHI);
-  LAUNCH_MT(2, TL, k_curl_phi, gp, smem_line(2, 2, 0, mp, TL), g, a, out, TL);
+  LAUNCH_MT(2, TL, k_curl_phi, (TS), gp, smem_line(2, 2, 0, mp, TL), g, a, out, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_CURL_R);
-  LAUNCH_MT(0, TL, k_curl_r, gr, smem_line(2, 2, 0, mr, TL), g, a, out, TL, apply_bc);
+  LAUNCH_MT(0, TL, k_curl_r, (TS), gr, smem_line(2, 2, 0, mr, TL), g, a, out, TL, apply_bc);
   prof_end(c);
   return check_launch(c);
 }
 
 // RHS of one stage on `cur`; if stage > 0 also the stage update into `nx`
-static int launch_rhs(css_ctx *c, const double *cur, double *nx, int stage, double dtcur) {
+// stage input of storage type TS, next stage state of storage type TO
+template <typename TS, typename TO>
+static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur) {
   const CssGeo &g = c->g;
   const int mag = g.magnetic;
   if (mag) {
@@ -654,25 +670,25 @@ static int launch_rhs(css_ctx *c, const double *cur, double *nx, int stage, doub
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_THETA);
-  LAUNCH_MT(1, TL, k_theta_terms, gt, smem_theta_terms(mag, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  LAUNCH_MT(1, TL, k_theta_terms, (TS), gt, smem_theta_terms(mag, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
   prof_begin(c, KI_PHI);
-  LAUNCH_MT(2, TL, k_phi_terms, gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  LAUNCH_MT(2, TL, k_phi_terms, (TS), gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_RADIAL);
-  LAUNCH_MT(0, TL, k_radial_terms, gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  LAUNCH_MT(0, TL, k_radial_terms, (TS), gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_RHOT_UPDATE);
-  LAUNCH_MT(1, TL, k_rhot_update, gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+  LAUNCH_MT(1, TL, k_rhot_update, (TS, TO), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
             TL, c->flag);
   prof_end(c);
   return check_launch(c);
@@ -698,7 +714,7 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   if (g.do_ohmic_heating) {
-    if (int rc = launch_curl(c, dout + 5 * c->ncell, c->cda, 0)) return rc;
+    if (int rc = launch_curl(c, (const double *)(dout + 5 * c->ncell), c->cda, 0)) return rc;
     prof_begin(c, KI_SLD_OHMIC);
     k_sld_ohmic<<<nb, 256, 0, c->stream>>>(g, v, c->bf, c->cda, dout);
     prof_end(c);
@@ -712,14 +728,24 @@ static int step_once(css_ctx *c, double dt) {
   (void)N;
   if (c->p.sldiffusion) {
     if (c->g.magnetic) {
-      if (int rc = launch_curl(c, c->v0 + 5 * c->ncell, c->bf, 1)) return rc;
+      if (int rc = launch_curl(c, (const double *)(c->v0 + 5 * c->ncell), c->bf, 1)) return rc;
     }
     if (int rc = launch_sld(c, c->v0, c->v0 + 5 * c->ncell, c->vs)) return rc;
   }
-  if (int rc = launch_rhs(c, c->v0, c->vA, 1, dt / 2.0)) return rc;
-  if (int rc = launch_rhs(c, c->vA, c->vB, 2, dt / 2.0)) return rc;
-  if (int rc = launch_rhs(c, c->vB, c->vA, 3, dt)) return rc;
-  if (int rc = launch_rhs(c, c->vA, c->v0, 4, dt)) return rc;
+  if (c->p.precision == 1) {
+    // mixed: the stage states U1..U3 are FP32 (rho, s as perturbations about
+    // the background); vars0, the accumulator and the tendency stay FP64
+    float *fA = reinterpret_cast<float *>(c->vA), *fB = reinterpret_cast<float *>(c->vB);
+    if (int rc = launch_rhs(c, (const double *)c->v0, fA, 1, dt / 2.0)) return rc;
+    if (int rc = launch_rhs(c, (const float *)fA, fB, 2, dt / 2.0)) return rc;
+    if (int rc = launch_rhs(c, (const float *)fB, fA, 3, dt)) return rc;
+    if (int rc = launch_rhs(c, (const float *)fA, c->v0, 4, dt)) return rc;
+    return CSS_OK;
+  }
+  if (int rc = launch_rhs(c, (const double *)c->v0, c->vA, 1, dt / 2.0)) return rc;
+  if (int rc = launch_rhs(c, (const double *)c->vA, c->vB, 2, dt / 2.0)) return rc;
+  if (int rc = launch_rhs(c, (const double *)c->vB, c->vA, 3, dt)) return rc;
+  if (int rc = launch_rhs(c, (const double *)c->vA, c->v0, 4, dt)) return rc;
   return CSS_OK;
 }
 
@@ -764,7 +790,7 @@ extern "C" int css_rhs(css_ctx *c, double *vars1, double *dvars1, int call_num) 
   if (!c || !vars1 || !dvars1) { set_err("css_rhs: NULL"); return CSS_ERR_ARG; }
   size_t sb = c->ncell * c->nv * 8;
   CUDA_TRY(cudaMemcpyAsync(c->vA, vars1, sb, cudaMemcpyHostToDevice, c->stream));
-  if (int rc = launch_rhs(c, c->vA, nullptr, 0, 0.0)) return rc;
+  if (int rc = launch_rhs(c, (const double *)c->vA, (double *)nullptr, 0, 0.0)) return rc;
   CUDA_TRY(cudaMemcpyAsync(dvars1, c->dv, sb, cudaMemcpyDeviceToHost, c->stream));
   if (c->g.magnetic && call_num == 1)
     CUDA_TRY(cudaMemcpyAsync(vars1 + 5 * c->ncell, c->bf, 3 * c->ncell * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -990,9 +1016,9 @@ extern "C" int css_autotune(css_ctx *c, int reps, int *chosen) {
     float best_ms = 1e30f;
     for (int t : cand) {
       *tl[d] = t;
-      if ((rc = launch_rhs(c, c->v0, nullptr, 0, 0.0))) break;  // warm
+      if ((rc = launch_rhs(c, (const double *)c->v0, (double *)nullptr, 0, 0.0))) break;  // warm
       cudaEventRecord(e0, c->stream);
-      for (int k = 0; k < reps && rc == CSS_OK; k++) rc = launch_rhs(c, c->v0, nullptr, 0, 0.0);
+      for (int k = 0; k < reps && rc == CSS_OK; k++) rc = launch_rhs(c, (const double *)c->v0, (double *)nullptr, 0, 0.0);
       cudaEventRecord(e1, c->stream);
       if (rc) break;
       if (cudaEventSynchronize(e1) != cudaSuccess) { set_err("css_autotune: timing failed"); rc = CSS_ERR_CUDA; break; }
@@ -1177,7 +1203,7 @@ static int run_stats(css_ctx *c, int need_dsdr, std::vector<double> &res) {
   }
   cudaStream_t st = c->stream;
   if (g.magnetic)
-    if (int rc = launch_curl(c, c->v0 + 5 * n, c->bf, 1)) return rc;  // Compute_B(0)
+    if (int rc = launch_curl(c, (const double *)(c->v0 + 5 * n), c->bf, 1)) return rc;  // Compute_B(0)
   const double *dsdr = nullptr;
   if (need_dsdr) {
     // Compute_Derivatives (report_mpi.f90:288-318): d s/d r with the
@@ -1305,7 +1331,7 @@ extern "C" int css_spectrum(css_ctx *c, int kind, double *out) {
   const size_t n = c->ncell;
   cudaStream_t st = c->stream;
   if (kind == 1)
-    if (int rc = launch_curl(c, c->v0 + 5 * n, c->bf, 1)) return rc;
+    if (int rc = launch_curl(c, (const double *)(c->v0 + 5 * n), c->bf, 1)) return rc;
   // theta weights: apodisation 1 - cos(pi (theta - theta_1)/(theta_n - theta_1))^64 and
   // W(t) = sum_{kt=1}^{nth/2-1} exp(-2 pi i kt t / nth); phi twiddles cos|sin(2 pi j / nphi)
   std::vector<double> tab(3 * (size_t)nth + 2 * (size_t)nphi);

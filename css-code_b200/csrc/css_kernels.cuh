@@ -46,23 +46,46 @@ __device__ __forceinline__ double dnum_d2_theta(const CssGeo &g, int ir) {
   return g.d[0].dnum[__ldg(g.rblk + ir)];
 }
 
+// A stage state is stored either as FP64 values (the FP64 path, and vars0)
+// or as FP32 perturbations of rho and s about the background rhor(r), sr(r)
+// (the mixed path; the other fields are plain FP32).  st_val returns the
+// FP64 value: the stored number, plus the background when it is FP32 and a
+// background profile is given.
+template <typename TS>
+__device__ __forceinline__ double st_val(const TS *p, size_t off, const double *mean, int r) {
+  double x = (double)__ldg(p + off);
+  if constexpr (sizeof(TS) == 4) {
+    if (mean) x += mean[r];
+  }
+  return x;
+}
+
+// the stored form of a new stage value (inverse of st_val)
+template <typename TO>
+__device__ __forceinline__ TO st_store(double x, double mean) {
+  if constexpr (sizeof(TO) == 4) return (TO)(x - mean);
+  else return x;
+}
+
 // ---------------------------------------------------------------------------
 // tile loaders
 // ---------------------------------------------------------------------------
 // theta tile: S[l*SR + j+4], j in [-4, m+4), lines = phi indices pb..pb+TL-1
-__device__ __forceinline__ void load_theta_tile(const CssGeo &g, const double *__restrict__ f, double *S, int SR,
+template <typename TS>
+__device__ __forceinline__ void load_theta_tile(const CssGeo &g, const TS *__restrict__ f, double *S, int SR,
                                                 int t0, int m, int pb, int TL, int ir, bool halo) {
   int w = m + 8;
   for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
     int l = idx / w, jj = idx - l * w;
     int gt = t0 + jj - 4, gp = pb + l;
     if ((!halo && (jj < 4 || jj >= m + 4)) || gt < 0 || gt >= g.nth || gp >= g.nphi) continue;
-    S[l * SR + jj] = __ldg(f + css_idx(g, gt, gp, ir));
+    S[l * SR + jj] = (double)__ldg(f + css_idx(g, gt, gp, ir));
   }
 }
 
 // phi tile: S[(j+4)*SR + l], lines = theta indices tb..tb+TL-1, periodic in phi
-__device__ __forceinline__ void load_phi_tile(const CssGeo &g, const double *__restrict__ f, double *S, int SR,
+template <typename TS>
+__device__ __forceinline__ void load_phi_tile(const CssGeo &g, const TS *__restrict__ f, double *S, int SR,
                                               int p0, int m, int tb, int TL, int ir, bool halo) {
   int w = m + 8;
   for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
@@ -72,19 +95,20 @@ __device__ __forceinline__ void load_phi_tile(const CssGeo &g, const double *__r
     gp = (gp + g.nphi) % g.nphi;
     int gt = tb + l;
     if (gt >= g.nth) continue;
-    S[jj * SR + l] = __ldg(f + css_idx(g, gt, gp, ir));
+    S[jj * SR + l] = (double)__ldg(f + css_idx(g, gt, gp, ir));
   }
 }
 
 // r tile: S[(j+4)*SR + l], lines = theta indices tb..tb+TL-1 at fixed phi
-__device__ __forceinline__ void load_r_tile(const CssGeo &g, const double *__restrict__ f, double *S, int SR, int r0,
+template <typename TS>
+__device__ __forceinline__ void load_r_tile(const CssGeo &g, const TS *__restrict__ f, double *S, int SR, int r0,
                                             int m, int tb, int TL, int ip, bool halo) {
   int w = m + 8;
   for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
     int jj = idx / TL, l = idx - jj * TL;
     int gr = r0 + jj - 4, gt = tb + l;
     if ((!halo && (jj < 4 || jj >= m + 4)) || gr < 0 || gr >= g.nr || gt >= g.nth) continue;
-    S[jj * SR + l] = __ldg(f + css_idx(g, gt, ip, gr));
+    S[jj * SR + l] = (double)__ldg(f + css_idx(g, gt, ip, gr));
   }
 }
 
@@ -103,47 +127,47 @@ __device__ __forceinline__ void stage_table(const CssGeo &g, int dir, int blk, i
 __device__ __forceinline__ size_t plane(const CssGeo &g, int ir) { return (size_t)ir * g.nth * g.nphi; }
 
 // theta tile: S[l*SR + j+4], lines = phi indices pb..pb+TL-1 of radius ir
-template <int MT, int TLC>
-__device__ __forceinline__ void tile_theta(const CssGeo &g, const double *__restrict__ f, double *S, int SR, int t0,
-                                           int m_, int pb, int TL_, int ir) {
+template <int MT, int TLC, typename TS>
+__device__ __forceinline__ void tile_theta(const CssGeo &g, const TS *__restrict__ f, double *S, int SR, int t0,
+                                           int m_, int pb, int TL_, int ir, const double *mean = nullptr) {
   const int m = MT ? MT : m_, TL = TLC ? TLC : TL_, w = m + 8;
-  const double *fp = f + plane(g, ir);
+  const TS *fp = f + plane(g, ir);
   for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
     int l = idx / w, jj = idx - l * w;
     int gt = t0 + jj - 4, gp = pb + l;
     if (gt < 0 || gt >= g.nth || gp >= g.nphi) continue;
-    S[l * SR + jj] = __ldg(fp + (size_t)gp * g.nth + gt);
+    S[l * SR + jj] = st_val(fp, (size_t)gp * g.nth + gt, mean, ir);
   }
 }
 
 // phi tile: S[(j+4)*SR + l], lines = theta indices tb..tb+TL-1, periodic phi
-template <int MT, int TLC>
-__device__ __forceinline__ void tile_phi(const CssGeo &g, const double *__restrict__ f, double *S, int SR, int p0,
-                                         int m_, int tb, int TL_, int ir) {
+template <int MT, int TLC, typename TS>
+__device__ __forceinline__ void tile_phi(const CssGeo &g, const TS *__restrict__ f, double *S, int SR, int p0,
+                                         int m_, int tb, int TL_, int ir, const double *mean = nullptr) {
   const int m = MT ? MT : m_, TL = TLC ? TLC : TL_, w = m + 8;
-  const double *fp = f + plane(g, ir);
+  const TS *fp = f + plane(g, ir);
   for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
     int jj = idx / TL, l = idx - jj * TL;
     int gp = p0 + jj - 4, gt = tb + l;
     if (gp < 0) gp += g.nphi;
     else if (gp >= g.nphi) gp -= g.nphi;
     if (gt >= g.nth) continue;
-    S[jj * SR + l] = __ldg(fp + (size_t)gp * g.nth + gt);
+    S[jj * SR + l] = st_val(fp, (size_t)gp * g.nth + gt, mean, ir);
   }
 }
 
 // r tile: S[(j+4)*SR + l], lines = theta indices tb..tb+TL-1 at phi ip
-template <int MT, int TLC>
-__device__ __forceinline__ void tile_r(const CssGeo &g, const double *__restrict__ f, double *S, int SR, int r0,
-                                       int m_, int tb, int TL_, int ip) {
+template <int MT, int TLC, typename TS>
+__device__ __forceinline__ void tile_r(const CssGeo &g, const TS *__restrict__ f, double *S, int SR, int r0,
+                                       int m_, int tb, int TL_, int ip, const double *mean = nullptr) {
   const int m = MT ? MT : m_, TL = TLC ? TLC : TL_, w = m + 8;
   const size_t ps = (size_t)g.nth * g.nphi;
-  const double *fp = f + (size_t)ip * g.nth + tb;
+  const TS *fp = f + (size_t)ip * g.nth + tb;
   for (int idx = threadIdx.x; idx < TL * w; idx += blockDim.x) {
     int jj = idx / TL, l = idx - jj * TL;
     int gr = r0 + jj - 4;
     if (gr < 0 || gr >= g.nr || tb + l >= g.nth) continue;
-    S[jj * SR + l] = __ldg(fp + (size_t)gr * ps + l);
+    S[jj * SR + l] = st_val(fp, (size_t)gr * ps + l, mean, gr);
   }
 }
 
@@ -158,12 +182,12 @@ constexpr int NT = 128;
 // periodic in phi, lines = theta indices lb..; DIR 0: r tile S[jj*SR + l]
 // at phi index `fixed`, lines = theta indices lb...  a0 = first point of
 // the block along the sweep; jj = 0..MT+7 covers the 4-point halos.
-template <int NF, int MT, int TLC, int DIR>
-__device__ __forceinline__ void tiles_ct(const CssGeo &g, const double *const *f, double *S, size_t FS, int SR,
-                                         int a0, int lb, int fixed) {
+template <int NF, int MT, int TLC, int DIR, typename TS>
+__device__ __forceinline__ void tiles_ct(const CssGeo &g, const TS *const *f, double *S, size_t FS, int SR,
+                                         int a0, int lb, int fixed, const double *const *mp = nullptr) {
   constexpr int W = MT + 8, N = TLC * W, IT = (N + NT - 1) / NT;
   double val[NF][IT];
-  int so[IT];
+  int so[IT], rr[IT];
   size_t go[IT];
 #pragma unroll
   for (int k = 0; k < IT; k++) {
@@ -192,13 +216,14 @@ __device__ __forceinline__ void tiles_ct(const CssGeo &g, const double *const *f
       off = plane(g, gr < 0 ? 0 : gr) + (size_t)fixed * g.nth + gt;
       so[k] = jj * SR + l;
     }
+    rr[k] = DIR == 0 ? (ok ? a0 + jj - 4 : 0) : fixed;
     if (!ok) so[k] = -1;
     go[k] = ok ? off : 0;
   }
 #pragma unroll
   for (int q = 0; q < NF; q++)
 #pragma unroll
-    for (int k = 0; k < IT; k++) val[q][k] = (so[k] >= 0) ? __ldg(f[q] + go[k]) : 0.0;
+    for (int k = 0; k < IT; k++) val[q][k] = (so[k] >= 0) ? st_val(f[q], go[k], mp ? mp[q] : nullptr, rr[k]) : 0.0;
 #pragma unroll
   for (int q = 0; q < NF; q++)
 #pragma unroll
@@ -212,8 +237,8 @@ __device__ __forceinline__ void tiles_ct(const CssGeo &g, const double *const *f
 // (vars1), B = curl A (MHD) in bf, dv = dvars1 (written, not read), tbuf =
 // the stage temperature (written here, read by the later kernels).
 // ---------------------------------------------------------------------------
-template <int MT, int TLC>
-__global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__restrict__ cur,
+template <int MT, int TLC, typename TV>
+__global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const TV *__restrict__ cur,
                                                      const double *__restrict__ bf, double *__restrict__ dv,
                                                      double *__restrict__ tbuf, int TLrt) {
   extern __shared__ double sm[];
@@ -232,12 +257,15 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
   double *H = sm;
   double *O = H + (size_t)nh * TL * SR;
   double *Tb = O + (size_t)nd * TL * SO;
-  const double *fld[6] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, bf + n, bf + 2 * n};
+  const TV *fs[4] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n};
+  const double *ms[4] = {nullptr, nullptr, nullptr, g.sr};
+  const double *fb[2] = {bf + n, bf + 2 * n};
   if constexpr (MT > 0 && TLC > 0) {
-    tiles_ct<4, MT, TLC, 1>(g, fld, H, (size_t)TL * SR, SR, t0, pb, ir);
-    if (mag) tiles_ct<2, MT, TLC, 1>(g, fld + 4, H + (size_t)4 * TL * SR, (size_t)TL * SR, SR, t0, pb, ir);
+    tiles_ct<4, MT, TLC, 1>(g, fs, H, (size_t)TL * SR, SR, t0, pb, ir, ms);
+    if (mag) tiles_ct<2, MT, TLC, 1>(g, fb, H + (size_t)4 * TL * SR, (size_t)TL * SR, SR, t0, pb, ir);
   } else {
-    for (int k = 0; k < nh; k++) tile_theta<MT, TLC>(g, fld[k], H + (size_t)k * TL * SR, SR, t0, m, pb, TL, ir);
+    for (int k = 0; k < 4; k++) tile_theta<MT, TLC>(g, fs[k], H + (size_t)k * TL * SR, SR, t0, m, pb, TL, ir, ms[k]);
+    for (int k = 4; k < nh; k++) tile_theta<MT, TLC>(g, fb[k - 4], H + (size_t)k * TL * SR, SR, t0, m, pb, TL, ir);
   }
   const int var[7] = {2, 3, 4, 5, 5, 8, 9};
   for (int k = 0; k < nd; k++) stage_table(g, 1, bt, k == 4 ? 2 : 1, g.ibct[var[k]], m, Tb + k * TS);
@@ -282,7 +310,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
     const int l = pt / m, j = pt - l * m;
     const bool ok = pt < TL * m && pb + l < g.nphi;
     const size_t id = pl + (size_t)(pb + l) * g.nth + t0 + j;
-    rho_[k] = ok ? __ldg(cur + id) : 1.0;
+    rho_[k] = ok ? st_val(cur, id, g.rhor, ir) : 1.0;
     bt_in[k] = (ok && mag) ? __ldg(bf + id) : 0.0;
   }
 #pragma unroll
@@ -368,8 +396,8 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const double *__r
 // Phi_Terms (rhs_mpi.f90:1032-1261).  grid: x = phi block * nchunk + theta
 // chunk, y = r.
 // ---------------------------------------------------------------------------
-template <int MT, int TLC>
-__global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__restrict__ cur,
+template <int MT, int TLC, typename TV>
+__global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restrict__ cur,
                                                    const double *__restrict__ bf, double *__restrict__ dv,
                                                    const double *__restrict__ tbuf, int TLrt) {
   extern __shared__ double sm[];
@@ -388,12 +416,15 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const double *__res
   double *H = sm;
   double *O = H + nh * HS;
   double *Tb = O + nd * OS;
-  const double *fld[7] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n, bf, bf + 2 * n};
+  const TV *fs[5] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n};
+  const double *ms[5] = {g.rhor, nullptr, nullptr, nullptr, g.sr};
+  const double *fb[2] = {bf, bf + 2 * n};
   if constexpr (MT > 0 && TLC > 0) {
-    tiles_ct<5, MT, TLC, 2>(g, fld, H, HS, SR, p0, tb, ir);
-    if (mag) tiles_ct<2, MT, TLC, 2>(g, fld + 5, H + 5 * HS, HS, SR, p0, tb, ir);
+    tiles_ct<5, MT, TLC, 2>(g, fs, H, HS, SR, p0, tb, ir, ms);
+    if (mag) tiles_ct<2, MT, TLC, 2>(g, fb, H + 5 * HS, HS, SR, p0, tb, ir);
   } else {
-    for (int k = 0; k < nh; k++) tile_phi<MT, TLC>(g, fld[k], H + k * HS, SR, p0, m, tb, TL, ir);
+    for (int k = 0; k < 5; k++) tile_phi<MT, TLC>(g, fs[k], H + k * HS, SR, p0, m, tb, TL, ir, ms[k]);
+    for (int k = 5; k < nh; k++) tile_phi<MT, TLC>(g, fb[k - 5], H + k * HS, SR, p0, m, tb, TL, ir);
   }
   stage_table(g, 2, bp, 1, 0, m, Tb);
   stage_table(g, 2, bp, 2, 0, m, Tb + TS);
@@ -545,8 +576,8 @@ __device__ __forceinline__ void radial_point(const CssGeo &g, int ir, const RadI
 // it is solved with a zero datum together with the other derivatives and
 // the datum times the block's unit response (resp) is added afterwards.
 // ---------------------------------------------------------------------------
-template <int MT, int TLC>
-__global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__restrict__ cur,
+template <int MT, int TLC, typename TV>
+__global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const TV *__restrict__ cur,
                                                       const double *__restrict__ bf, double *__restrict__ dv,
                                                       const double *__restrict__ tbuf, int TLrt) {
   extern __shared__ double sm[];
@@ -567,12 +598,15 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
   double *O = H + nh * HS;
   double *Tb = O + nd * OS;
   double *datum = Tb + nd * TS;
-  const double *fld[7] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, cur, bf, bf + n};
+  const TV *fs[5] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, cur};
+  const double *ms[5] = {nullptr, nullptr, nullptr, g.sr, g.rhor};
+  const double *fb[2] = {bf, bf + n};
   if constexpr (MT > 0 && TLC > 0) {
-    tiles_ct<5, MT, TLC, 0>(g, fld, H, HS, SR, r0, tb, ip);
-    if (mag) tiles_ct<2, MT, TLC, 0>(g, fld + 5, H + 5 * HS, HS, SR, r0, tb, ip);
+    tiles_ct<5, MT, TLC, 0>(g, fs, H, HS, SR, r0, tb, ip, ms);
+    if (mag) tiles_ct<2, MT, TLC, 0>(g, fb, H + 5 * HS, HS, SR, r0, tb, ip);
   } else {
-    for (int k = 0; k < nh; k++) tile_r<MT, TLC>(g, fld[k], H + k * HS, SR, r0, m, tb, TL, ip);
+    for (int k = 0; k < 5; k++) tile_r<MT, TLC>(g, fs[k], H + k * HS, SR, r0, m, tb, TL, ip, ms[k]);
+    for (int k = 5; k < nh; k++) tile_r<MT, TLC>(g, fb[k - 5], H + k * HS, SR, r0, m, tb, TL, ip);
   }
   const int var[8] = {2, 3, 4, 5, 5, 1, 7, 8};
   for (int k = 0; k < nd; k++) stage_table(g, 0, br, k == 4 ? 2 : 1, g.ibcr[var[k]], m, Tb + k * TS);
@@ -704,9 +738,9 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const double *__
 //   stage 2,3: vs = vs + dv/3;            nx = v0 + dtcur*dv
 //   stage 4: vs = vs + dv/6;              nx = v0 + dtcur*vs  (nx may be v0)
 // ---------------------------------------------------------------------------
-template <int MT, int TLC>
-__global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__restrict__ cur,
-                                                     double *__restrict__ dv, const double *v0, double *vs, double *nx,
+template <int MT, int TLC, typename TS, typename TO>
+__global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restrict__ cur,
+                                                     double *__restrict__ dv, const double *v0, double *vs, TO *nx,
                                                      const double *__restrict__ tbuf, int stage, double dtcur,
                                                      int TLrt, int *flag) {
   extern __shared__ double sm[];
@@ -723,10 +757,11 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
   double *O = H + (size_t)TL * SR;
   double *Tb = O + (size_t)TL * SO;
   if constexpr (MT > 0 && TLC > 0) {
-    const double *f1[1] = {cur};
-    tiles_ct<1, MT, TLC, 1>(g, f1, H, 0, SR, t0, pb, ir);
+    const TS *f1[1] = {cur};
+    const double *m1[1] = {g.rhor};
+    tiles_ct<1, MT, TLC, 1>(g, f1, H, 0, SR, t0, pb, ir, m1);
   } else {
-    tile_theta<MT, TLC>(g, cur, H, SR, t0, m, pb, TL, ir);
+    tile_theta<MT, TLC>(g, cur, H, SR, t0, m, pb, TL, ir, g.rhor);
   }
   const int bdry = g.ibct[1];
   stage_table(g, 1, bt, 1, bdry, m, Tb);
@@ -755,7 +790,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
     if (ip >= g.nphi) continue;
     size_t id = pl + (size_t)ip * g.nth + it;
     double rho = H[(size_t)l * SR + 4 + j];
-    double w = __ldg(cur + n + id);
+    double w = st_val(cur + n, id, nullptr, ir);
     double t = __ldg(tbuf + id);
     double w1 = ri * O[(size_t)l * SO + j];
     double d0 = dv[id] - w * w1;
@@ -823,7 +858,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
         }
       }
       if (!isfinite(o)) bad = 1;
-      nx[q] = o;
+      nx[q] = st_store<TO>(o, iv == 0 ? g.rhor[ir] : (iv == 4 ? g.sr[ir] : 0.0));
     }
   }
   if (bad && flag) atomicOr(flag, 1);
@@ -834,8 +869,8 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const double *__r
 // (theta, phi, r).  Three kernels, one per sweep direction; the r sweep
 // optionally applies Compute_B's boundary zeroing (:1842-1883).
 // ---------------------------------------------------------------------------
-template <int MT, int TLC>
-__global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
+template <int MT, int TLC, typename TS>
+__global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const TS *__restrict__ a, double *__restrict__ out,
                                                     int TL) {
   extern __shared__ double sm[];
   const int nchunk = (g.nphi + TL - 1) / TL;
@@ -877,8 +912,8 @@ __global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const double *__re
   }
 }
 
-template <int MT, int TLC>
-__global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
+template <int MT, int TLC, typename TS>
+__global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const TS *__restrict__ a, double *__restrict__ out,
                                                   int TL) {
   extern __shared__ double sm[];
   const int nchunk = (g.nth + TL - 1) / TL;
@@ -913,8 +948,8 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const double *__rest
   }
 }
 
-template <int MT, int TLC>
-__global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const double *__restrict__ a, double *__restrict__ out,
+template <int MT, int TLC, typename TS>
+__global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const TS *__restrict__ a, double *__restrict__ out,
                                                 int TL, int apply_bc) {
   extern __shared__ double sm[];
   const int nchunk = (g.nth + TL - 1) / TL;
