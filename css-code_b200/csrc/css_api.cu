@@ -1,6 +1,7 @@
 // css_api.cu -- C ABI of the CSS B200 library (include/css_b200.h): context
 // set-up (virtual decomposition, LU tables, profiles), device buffers, the
 // RK4 step loop and the parity entry points.
+#include <cublasLt.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -15,6 +16,7 @@
 #include "../../include/css_b200.h"
 #include "css_kernels.cuh"
 #include "css_stats.cuh"
+#include "css_closure.cuh"
 
 using namespace css;
 
@@ -1364,6 +1366,330 @@ extern "C" int css_spectrum(css_ctx *c, int kind, double *out) {
   if (int rc = check_launch(c)) return rc;
   CUDA_TRY(cudaMemcpyAsync(out, c->vA, (size_t)nr * (nphi / 2) * 8, cudaMemcpyDeviceToHost, st));
   CUDA_TRY(cudaStreamSynchronize(st));
+  return CSS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Learned subgrid closure.  A fine state is box-filtered into coarse fields
+// and the twelve subgrid targets; 3x3x3 stencil features of the coarse
+// fields feed an MLP (in 135 -> 128 -> 128 -> 128 -> 12, GELU, BF16 weights
+// and activations, FP32 accumulation) whose matrix products run on the
+// tensor cores through cuBLASLt; its predicted subgrid velocity variance
+// becomes the per-cell SLD speed^2 of a coarse run, in place of the
+// prescribed radial profile (diffusion.f90:19-63).
+// ---------------------------------------------------------------------------
+extern "C" int css_set_sld_speed2(css_ctx *c, const double *speed2) {
+  if (!c) { set_err("css_set_sld_speed2: NULL context"); return CSS_ERR_ARG; }
+  c->g.speed2 = speed2;
+  return CSS_OK;
+}
+
+extern "C" int css_box_filter(css_ctx *c, int f, double *fields, double *targets) {
+  if (!c || !fields || !targets || f < 1 || c->p.nr % f || c->p.nth % f || c->p.nphi % f) {
+    set_err("css_box_filter: bad argument (the factor must divide nr, nth and nphi)");
+    return CSS_ERR_ARG;
+  }
+  const size_t n = c->ncell;
+  if (c->g.magnetic)
+    if (int rc = launch_curl(c, (const double *)(c->v0 + 5 * n), c->bf, 1)) return rc;
+  k_box_filter<<<148 * 8, 256, 0, c->stream>>>(c->g, c->v0, c->g.magnetic ? c->bf : nullptr, f, c->p.nth / f,
+                                                c->p.nphi / f, c->p.nr / f, fields, targets);
+  if (int rc = check_launch(c)) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+extern "C" int css_closure_scales(int nct, int ncp, int ncr, const double *fields, const double *targets,
+                                  float *scales) {
+  if (!fields || !scales || nct < 1 || ncp < 1 || ncr < 1) { set_err("css_closure_scales: bad argument"); return CSS_ERR_ARG; }
+  const int nb = 148 * 2, nk = CL_NQ + CL_NTARGET;
+  double *part = nullptr;
+  CUDA_TRY(cudaMalloc(&part, (size_t)nb * nk * 8));
+  k_closure_sumsq<<<nb, 256>>>(fields, targets, nct, ncp, ncr, part);
+  std::vector<double> h((size_t)nb * nk);
+  cudaError_t e = cudaGetLastError();
+  if (!e) e = cudaMemcpy(h.data(), part, h.size() * 8, cudaMemcpyDeviceToHost);
+  cudaFree(part);
+  if (e) { set_err("css_closure_scales: %s", cudaGetErrorString(e)); return CSS_ERR_CUDA; }
+  const double nc = (double)nct * ncp * ncr;
+  for (int k = 0; k < nk; k++) {
+    double s = 0.0;
+    for (int b = 0; b < nb; b++) s += h[(size_t)b * nk + k];
+    const double rms = sqrt(s / nc);
+    scales[k] = (float)(rms > 0.0 ? rms : 1.0);
+  }
+  return CSS_OK;
+}
+
+extern "C" int css_closure_features(int nct, int ncp, int ncr, const double *fields, const float *scale, void *x) {
+  if (!fields || !scale || !x || nct < 1 || ncp < 1 || ncr < 1) { set_err("css_closure_features: bad argument"); return CSS_ERR_ARG; }
+  k_closure_features<<<148 * 8, 128>>>(fields, nct, ncp, ncr, scale, (__nv_bfloat16 *)x);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaDeviceSynchronize());
+  return CSS_OK;
+}
+
+extern "C" int css_closure_targets(long long nc, const double *targets, const float *tscale, float *tn) {
+  if (!targets || !tscale || !tn || nc < 1) { set_err("css_closure_targets: bad argument"); return CSS_ERR_ARG; }
+  k_closure_targets<<<148 * 8, 256>>>(targets, (size_t)nc, tscale, tn);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaDeviceSynchronize());
+  return CSS_OK;
+}
+
+extern "C" int css_closure_speed2(long long nc, const float *y, const float *tscale, double *speed2) {
+  if (!y || !tscale || !speed2 || nc < 1) { set_err("css_closure_speed2: bad argument"); return CSS_ERR_ARG; }
+  k_closure_speed2<<<148 * 8, 256>>>(y, (size_t)nc, tscale, speed2);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaDeviceSynchronize());
+  return CSS_OK;
+}
+
+struct css_mlp {
+  int dims[5];          // padded widths: input, hidden x3, output
+  int nreal_in, nreal_out;
+  size_t cap;           // rows per pass
+  float *W[4] = {}, *B[4] = {}, *gW[4] = {}, *gB[4] = {}, *mW[4] = {}, *vW[4] = {}, *mB[4] = {}, *vB[4] = {};
+  __nv_bfloat16 *Wb[4] = {};
+  float *Z[4] = {};             // pre-activations; Z[3] is the output
+  __nv_bfloat16 *H[4] = {};     // H[1..3] activations; H[0] is the caller's input
+  float *dH = nullptr;          // FP32 gradient scratch
+  __nv_bfloat16 *dZb = nullptr; // BF16 gradient
+  double *part = nullptr;
+  int adam_t = 0;
+  cublasLtHandle_t lt = nullptr;
+  void *ws = nullptr;
+  size_t wsz = 32u << 20;
+  cudaStream_t st = nullptr;
+};
+
+static int lt_gemm(css_mlp *m, bool ta, bool tb, int M, int N, int K, const __nv_bfloat16 *A, int lda,
+                   const __nv_bfloat16 *Bm, int ldb, float *C, int ldc) {
+  cublasLtMatmulDesc_t op = nullptr;
+  cublasLtMatrixLayout_t la = nullptr, lb = nullptr, lc = nullptr;
+  cublasLtMatmulPreference_t pref = nullptr;
+  cublasLtMatmulHeuristicResult_t heur;
+  int nres = 0;
+  const cublasOperation_t oa = ta ? CUBLAS_OP_T : CUBLAS_OP_N, ob = tb ? CUBLAS_OP_T : CUBLAS_OP_N;
+  const float alpha = 1.0f, beta = 0.0f;
+  cublasStatus_t s = cublasLtMatmulDescCreate(&op, CUBLAS_COMPUTE_32F, CUDA_R_32F);
+  if (!s) s = cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSA, &oa, sizeof(oa));
+  if (!s) s = cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSB, &ob, sizeof(ob));
+  if (!s) s = cublasLtMatrixLayoutCreate(&la, CUDA_R_16BF, ta ? K : M, ta ? M : K, lda);
+  if (!s) s = cublasLtMatrixLayoutCreate(&lb, CUDA_R_16BF, tb ? N : K, tb ? K : N, ldb);
+  if (!s) s = cublasLtMatrixLayoutCreate(&lc, CUDA_R_32F, M, N, ldc);
+  if (!s) s = cublasLtMatmulPreferenceCreate(&pref);
+  if (!s) s = cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &m->wsz, sizeof(m->wsz));
+  if (!s) s = cublasLtMatmulAlgoGetHeuristic(m->lt, op, la, lb, lc, lc, pref, 1, &heur, &nres);
+  if (!s && nres == 0) s = CUBLAS_STATUS_NOT_SUPPORTED;
+  if (!s) s = cublasLtMatmul(m->lt, op, &alpha, A, la, Bm, lb, &beta, C, lc, C, lc, &heur.algo, m->ws, m->wsz, m->st);
+  if (pref) cublasLtMatmulPreferenceDestroy(pref);
+  if (lc) cublasLtMatrixLayoutDestroy(lc);
+  if (lb) cublasLtMatrixLayoutDestroy(lb);
+  if (la) cublasLtMatrixLayoutDestroy(la);
+  if (op) cublasLtMatmulDescDestroy(op);
+  if (s) {
+    set_err("cuBLASLt matmul %dx%dx%d: status %d", M, N, K, (int)s);
+    return CSS_ERR_CUDA;
+  }
+  return CSS_OK;
+}
+
+__global__ void k_to_bf16(const float *__restrict__ a, __nv_bfloat16 *__restrict__ b, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    b[i] = __float2bfloat16_rn(a[i]);
+}
+
+extern "C" void css_mlp_destroy(css_mlp *m) {
+  if (!m) return;
+  for (int l = 0; l < 4; l++) {
+    cudaFree(m->W[l]); cudaFree(m->B[l]); cudaFree(m->gW[l]); cudaFree(m->gB[l]);
+    cudaFree(m->mW[l]); cudaFree(m->vW[l]); cudaFree(m->mB[l]); cudaFree(m->vB[l]); cudaFree(m->Wb[l]);
+    cudaFree(m->Z[l]); cudaFree(m->H[l]);
+  }
+  cudaFree(m->dH); cudaFree(m->dZb); cudaFree(m->part); cudaFree(m->ws);
+  if (m->lt) cublasLtDestroy(m->lt);
+  if (m->st) cudaStreamDestroy(m->st);
+  delete m;
+}
+
+extern "C" int css_mlp_create(int n_in, int width, int n_out, int max_rows, unsigned long long seed, css_mlp **out) {
+  if (!out || n_in < 1 || width < 16 || width % 16 || n_out < 1 || max_rows < 1) {
+    set_err("css_mlp_create: bad argument (width a multiple of 16)");
+    return CSS_ERR_ARG;
+  }
+  *out = nullptr;
+  css_mlp *m = new css_mlp();
+  auto pad16 = [](int x) { return (x + 15) / 16 * 16; };
+  m->nreal_in = n_in;
+  m->nreal_out = n_out;
+  m->dims[0] = pad16(n_in);
+  m->dims[1] = m->dims[2] = m->dims[3] = width;
+  m->dims[4] = pad16(n_out);
+  m->cap = (size_t)max_rows;
+  cudaError_t e = cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking);
+  if (!e && cublasLtCreate(&m->lt) != CUBLAS_STATUS_SUCCESS) e = cudaErrorUnknown;
+  if (!e) e = cudaMalloc(&m->ws, m->wsz);
+  const int wmax = std::max(std::max(m->dims[0], width), m->dims[4]);
+  for (int l = 0; l < 4 && !e; l++) {
+    const size_t K = m->dims[l], M = m->dims[l + 1];
+    float **f4[] = {&m->W[l], &m->gW[l], &m->mW[l], &m->vW[l]};
+    for (auto pp : f4)
+      if (!e) e = cudaMalloc(pp, K * M * 4);
+    float **b4[] = {&m->B[l], &m->gB[l], &m->mB[l], &m->vB[l]};
+    for (auto pp : b4)
+      if (!e) e = cudaMalloc(pp, M * 4);
+    if (!e) e = cudaMalloc(&m->Wb[l], K * M * 2);
+    if (!e) e = cudaMalloc(&m->Z[l], m->cap * M * 4);
+    if (!e && l > 0) e = cudaMalloc(&m->H[l], m->cap * K * 2);
+  }
+  if (!e) e = cudaMalloc(&m->dH, m->cap * wmax * 4);
+  if (!e) e = cudaMalloc(&m->dZb, m->cap * wmax * 2);
+  if (!e) e = cudaMalloc(&m->part, 1024 * 8);
+  if (e) {
+    set_err("css_mlp_create: %s", cudaGetErrorString(e));
+    css_mlp_destroy(m);
+    return e == cudaErrorMemoryAllocation ? CSS_ERR_NOMEM : CSS_ERR_CUDA;
+  }
+  // Glorot-uniform weights from a SplitMix64 stream, zero biases; the rows
+  // of padded inputs and the columns of padded outputs are zero
+  unsigned long long x = seed;
+  auto next = [&x]() {
+    unsigned long long z = (x += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    return (double)(z >> 11) * (1.0 / 9007199254740992.0);
+  };
+  for (int l = 0; l < 4 && !e; l++) {
+    const int K = m->dims[l], M = m->dims[l + 1];
+    const int kr = l == 0 ? n_in : K, mr = l == 3 ? n_out : M;
+    const double a = sqrt(6.0 / (double)(kr + mr));
+    std::vector<float> w((size_t)K * M, 0.0f), z((size_t)K * M, 0.0f), zb(M, 0.0f);
+    for (int k = 0; k < K; k++)
+      for (int j = 0; j < M; j++) {
+        const double u = next();
+        if (k < kr && j < mr) w[(size_t)k * M + j] = (float)(a * (2.0 * u - 1.0));
+      }
+    if (!e) e = cudaMemcpy(m->W[l], w.data(), w.size() * 4, cudaMemcpyHostToDevice);
+    for (float *p : {m->mW[l], m->vW[l]})
+      if (!e) e = cudaMemcpy(p, z.data(), z.size() * 4, cudaMemcpyHostToDevice);
+    for (float *p : {m->B[l], m->mB[l], m->vB[l]})
+      if (!e) e = cudaMemcpy(p, zb.data(), zb.size() * 4, cudaMemcpyHostToDevice);
+    if (!e) {
+      k_to_bf16<<<64, 256, 0, m->st>>>(m->W[l], m->Wb[l], (size_t)K * M);
+      e = cudaGetLastError();
+    }
+  }
+  if (!e) e = cudaStreamSynchronize(m->st);
+  if (e) {
+    set_err("css_mlp_create: %s", cudaGetErrorString(e));
+    css_mlp_destroy(m);
+    return CSS_ERR_CUDA;
+  }
+  *out = m;
+  return CSS_OK;
+}
+
+extern "C" int css_mlp_dims(css_mlp *m, int *dims) {
+  if (!m || !dims) return CSS_ERR_ARG;
+  for (int k = 0; k < 5; k++) dims[k] = m->dims[k];
+  return CSS_OK;
+}
+
+// forward pass of n <= cap rows: Z[3] holds the outputs (row-major n x dims[4])
+static int mlp_forward_rows(css_mlp *m, const __nv_bfloat16 *x, size_t n) {
+  const __nv_bfloat16 *in = x;
+  for (int l = 0; l < 4; l++) {
+    const int K = m->dims[l], M = m->dims[l + 1];
+    if (int rc = lt_gemm(m, false, false, M, (int)n, K, m->Wb[l], M, in, K, m->Z[l], M)) return rc;
+    __nv_bfloat16 *next = l < 3 ? m->H[l + 1] : nullptr;
+    k_bias_gelu<<<148 * 4, 256, 0, m->st>>>(m->Z[l], m->B[l], next, M, n);
+    CUDA_TRY(cudaGetLastError());
+    in = next;
+  }
+  return CSS_OK;
+}
+
+extern "C" int css_mlp_forward(css_mlp *m, const void *x, long long n, float *y) {
+  if (!m || !x || !y || n < 1) { set_err("css_mlp_forward: bad argument"); return CSS_ERR_ARG; }
+  const int K0 = m->dims[0], MO = m->dims[4];
+  for (long long r0 = 0; r0 < n; r0 += (long long)m->cap) {
+    const size_t rows = (size_t)std::min<long long>((long long)m->cap, n - r0);
+    if (int rc = mlp_forward_rows(m, (const __nv_bfloat16 *)x + (size_t)r0 * K0, rows)) return rc;
+    CUDA_TRY(cudaMemcpyAsync(y + (size_t)r0 * MO, m->Z[3], rows * MO * 4, cudaMemcpyDeviceToDevice, m->st));
+  }
+  CUDA_TRY(cudaStreamSynchronize(m->st));
+  return CSS_OK;
+}
+
+extern "C" int css_mlp_train_step(css_mlp *m, const void *x, const float *t, long long n, float lr, float *loss) {
+  if (!m || !x || !t || n < 1 || (size_t)n > m->cap) {
+    set_err("css_mlp_train_step: bad argument (at most %zu rows per step)", m ? m->cap : (size_t)0);
+    return CSS_ERR_ARG;
+  }
+  const size_t rows = (size_t)n;
+  const __nv_bfloat16 *xb = (const __nv_bfloat16 *)x;
+  if (int rc = mlp_forward_rows(m, xb, rows)) return rc;
+  const int nb = 256;
+  k_mse<<<nb, 256, 0, m->st>>>(m->Z[3], t, rows, m->nreal_out, m->dH, m->dZb, m->part);
+  CUDA_TRY(cudaGetLastError());
+  for (int l = 3; l >= 0; l--) {
+    const int K = m->dims[l], M = m->dims[l + 1];
+    const __nv_bfloat16 *in = l == 0 ? xb : m->H[l];
+    // dW = dZ^T-contracted input, db = column sums of dZ
+    if (int rc = lt_gemm(m, false, true, M, K, (int)rows, m->dZb, M, in, K, m->gW[l], M)) return rc;
+    k_colsum<<<M, 256, 0, m->st>>>(m->dH, M, rows, m->gB[l]);
+    CUDA_TRY(cudaGetLastError());
+    if (l > 0) {
+      if (int rc = lt_gemm(m, true, false, K, (int)rows, M, m->Wb[l], M, m->dZb, M, m->dH, K)) return rc;
+      k_gelu_back<<<148 * 4, 256, 0, m->st>>>(m->dH, m->Z[l - 1], m->dZb, (size_t)K * rows);
+      CUDA_TRY(cudaGetLastError());
+    }
+  }
+  m->adam_t++;
+  const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+  const float c1 = 1.0f - powf(b1, (float)m->adam_t), c2 = 1.0f - powf(b2, (float)m->adam_t);
+  for (int l = 0; l < 4; l++) {
+    const size_t K = m->dims[l], M = m->dims[l + 1];
+    k_adam<<<148, 256, 0, m->st>>>(m->W[l], m->gW[l], m->mW[l], m->vW[l], m->Wb[l], K * M, lr, b1, b2, eps, c1, c2);
+    k_adam<<<4, 256, 0, m->st>>>(m->B[l], m->gB[l], m->mB[l], m->vB[l], nullptr, M, lr, b1, b2, eps, c1, c2);
+  }
+  CUDA_TRY(cudaGetLastError());
+  std::vector<double> h(nb);
+  CUDA_TRY(cudaMemcpyAsync(h.data(), m->part, nb * 8, cudaMemcpyDeviceToHost, m->st));
+  CUDA_TRY(cudaStreamSynchronize(m->st));
+  double s = 0.0;
+  for (double v : h) s += v;
+  if (loss) *loss = (float)(s / ((double)rows * m->nreal_out));
+  return CSS_OK;
+}
+
+// host copies of layer l's FP32 weights (row-major dims[l] x dims[l+1]) and
+// biases; set = 1 writes them (and refreshes the BF16 copy)
+extern "C" int css_mlp_params(css_mlp *m, int l, float *w, float *b, int set) {
+  if (!m || l < 0 || l > 3) { set_err("css_mlp_params: bad argument"); return CSS_ERR_ARG; }
+  const size_t K = m->dims[l], M = m->dims[l + 1];
+  if (set) {
+    if (w) CUDA_TRY(cudaMemcpy(m->W[l], w, K * M * 4, cudaMemcpyHostToDevice));
+    if (b) CUDA_TRY(cudaMemcpy(m->B[l], b, M * 4, cudaMemcpyHostToDevice));
+    k_to_bf16<<<64, 256, 0, m->st>>>(m->W[l], m->Wb[l], K * M);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(m->st));
+  } else {
+    if (w) CUDA_TRY(cudaMemcpy(w, m->W[l], K * M * 4, cudaMemcpyDeviceToHost));
+    if (b) CUDA_TRY(cudaMemcpy(b, m->B[l], M * 4, cudaMemcpyDeviceToHost));
+  }
+  return CSS_OK;
+}
+
+// the last train step's gradients of layer l (host, same layout)
+extern "C" int css_mlp_grads(css_mlp *m, int l, float *gw, float *gb) {
+  if (!m || l < 0 || l > 3) { set_err("css_mlp_grads: bad argument"); return CSS_ERR_ARG; }
+  const size_t K = m->dims[l], M = m->dims[l + 1];
+  CUDA_TRY(cudaStreamSynchronize(m->st));
+  if (gw) CUDA_TRY(cudaMemcpy(gw, m->gW[l], K * M * 4, cudaMemcpyDeviceToHost));
+  if (gb) CUDA_TRY(cudaMemcpy(gb, m->gB[l], M * 4, cudaMemcpyDeviceToHost));
   return CSS_OK;
 }
 

@@ -1,0 +1,248 @@
+// css_closure.cuh -- the learned subgrid closure: box filtering of a fine
+// state into coarse fields and subgrid targets, the 3x3x3 stencil features,
+// and the elementwise parts of the MLP (bias + GELU and its derivative,
+// loss, bias gradients, Adam).  The MLP's matrix products are BF16 GEMMs
+// with FP32 accumulation on the tensor cores (cuBLASLt), issued from
+// css_api.cu.
+#pragma once
+#include <cuda_bf16.h>
+
+#include "css_geo.cuh"
+
+namespace css {
+
+#define CL_NFIELD 7    // coarse fields: u_theta, u_phi, u_r, s', B_theta, B_phi, B_r
+#define CL_NTARGET 12  // tau_tt tau_tp tau_tr tau_pp tau_pr tau_rr, q_t q_p q_r, emf_t emf_p emf_r
+#define CL_NQ 5        // stencil quantities: u_theta, u_phi, u_r, |B|, ds'/dr
+#define CL_NFEAT 135   // 27 stencil points x 5 quantities
+#define CL_XPAD 144    // feature row length (zero padded to a multiple of 16)
+#define CL_YPAD 16     // output row length (12 targets, zero padded)
+
+// Box filter by the factor f in every direction: coarse cell (it, ip, ir)
+// averages the f^3 fine cells f*it.., f*ip.., f*ir...  fields[k*nc + c],
+// targets[k*nc + c]; c = it + nct*(ip + ncp*ir).  s' = s - sr(r); B from bf
+// (NULL for hydro: B and the EMF are zero).
+__global__ void k_box_filter(CssGeo g, const double *__restrict__ v, const double *__restrict__ bf, int f, int nct,
+                             int ncp, int ncr, double *__restrict__ fields, double *__restrict__ targets) {
+  const size_t nc = (size_t)nct * ncp * ncr, n = (size_t)g.ncell;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+    const int it = (int)(c % nct), ip = (int)((c / nct) % ncp), ir = (int)(c / ((size_t)nct * ncp));
+    double m[19];
+#pragma unroll
+    for (int k = 0; k < 19; k++) m[k] = 0.0;
+    for (int dr = 0; dr < f; dr++) {
+      const int fr = f * ir + dr;
+      const double sbar = g.sr[fr];
+      for (int dp = 0; dp < f; dp++)
+        for (int dt = 0; dt < f; dt++) {
+          const size_t id = css_idx(g, f * it + dt, f * ip + dp, fr);
+          const double ut = v[n + id], up = v[2 * n + id], ur = v[3 * n + id], sp = v[4 * n + id] - sbar;
+          double bt = 0.0, bp = 0.0, br = 0.0;
+          if (bf) { bt = bf[id]; bp = bf[n + id]; br = bf[2 * n + id]; }
+          m[0] += ut; m[1] += up; m[2] += ur; m[3] += sp; m[4] += bt; m[5] += bp; m[6] += br;
+          m[7] += ut * ut; m[8] += ut * up; m[9] += ut * ur; m[10] += up * up; m[11] += up * ur; m[12] += ur * ur;
+          m[13] += ut * sp; m[14] += up * sp; m[15] += ur * sp;
+          m[16] += up * br - ur * bp; m[17] += ur * bt - ut * br; m[18] += ut * bp - up * bt;
+        }
+    }
+    const double w = 1.0 / ((double)f * f * f);
+#pragma unroll
+    for (int k = 0; k < 19; k++) m[k] *= w;
+    const double ut = m[0], up = m[1], ur = m[2], sp = m[3], bt = m[4], bp = m[5], br = m[6];
+#pragma unroll
+    for (int k = 0; k < CL_NFIELD; k++) fields[k * nc + c] = m[k];
+    targets[0 * nc + c] = m[7] - ut * ut;
+    targets[1 * nc + c] = m[8] - ut * up;
+    targets[2 * nc + c] = m[9] - ut * ur;
+    targets[3 * nc + c] = m[10] - up * up;
+    targets[4 * nc + c] = m[11] - up * ur;
+    targets[5 * nc + c] = m[12] - ur * ur;
+    targets[6 * nc + c] = m[13] - ut * sp;
+    targets[7 * nc + c] = m[14] - up * sp;
+    targets[8 * nc + c] = m[15] - ur * sp;
+    targets[9 * nc + c] = m[16] - (up * br - ur * bp);
+    targets[10 * nc + c] = m[17] - (ur * bt - ut * br);
+    targets[11 * nc + c] = m[18] - (ut * bp - up * bt);
+  }
+}
+
+// the five stencil quantities of coarse cell (it, ip, ir)
+__device__ __forceinline__ void cl_quantities(const double *__restrict__ F, int nct, int ncp, int ncr, int it, int ip,
+                                              int ir, double q[CL_NQ]) {
+  const size_t nc = (size_t)nct * ncp * ncr;
+  const size_t c = it + (size_t)nct * (ip + (size_t)ncp * ir);
+  q[0] = F[c];
+  q[1] = F[nc + c];
+  q[2] = F[2 * nc + c];
+  const double bt = F[4 * nc + c], bp = F[5 * nc + c], br = F[6 * nc + c];
+  q[3] = sqrt(bt * bt + bp * bp + br * br);
+  // ds'/dr in coarse index units: central inside, one-sided at the ends
+  const int lo = ir > 0 ? ir - 1 : ir, hi = ir < ncr - 1 ? ir + 1 : ir;
+  const size_t cl = it + (size_t)nct * (ip + (size_t)ncp * lo), ch = it + (size_t)nct * (ip + (size_t)ncp * hi);
+  q[4] = (F[3 * nc + ch] - F[3 * nc + cl]) / (double)(hi - lo);
+}
+
+// features: row c of X (CL_XPAD bf16) = the 27 neighbours (r, theta clamped
+// at the ends, phi periodic; order (dr, dt, dp) with dp fastest) x the five
+// quantities divided by scale[q], then zeros
+__global__ void k_closure_features(const double *__restrict__ F, int nct, int ncp, int ncr,
+                                   const float *__restrict__ scale, __nv_bfloat16 *__restrict__ X) {
+  const size_t nc = (size_t)nct * ncp * ncr;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+    const int it = (int)(c % nct), ip = (int)((c / nct) % ncp), ir = (int)(c / ((size_t)nct * ncp));
+    __nv_bfloat16 *row = X + c * CL_XPAD;
+    int col = 0;
+    for (int dr = -1; dr <= 1; dr++)
+      for (int dt = -1; dt <= 1; dt++)
+        for (int dp = -1; dp <= 1; dp++) {
+          const int jr = min(max(ir + dr, 0), ncr - 1), jt = min(max(it + dt, 0), nct - 1);
+          const int jp = (ip + dp + ncp) % ncp;
+          double q[CL_NQ];
+          cl_quantities(F, nct, ncp, ncr, jt, jp, jr, q);
+#pragma unroll
+          for (int k = 0; k < CL_NQ; k++) row[col++] = __float2bfloat16_rn((float)(q[k] / (double)scale[k]));
+        }
+    for (; col < CL_XPAD; col++) row[col] = __float2bfloat16_rn(0.0f);
+  }
+}
+
+// root mean square of the five stencil quantities and of the twelve targets:
+// part[(blk)*17 + k] partial sums of squares (grid-stride, one block row each)
+__global__ void k_closure_sumsq(const double *__restrict__ F, const double *__restrict__ T, int nct, int ncp, int ncr,
+                                double *__restrict__ part) {
+  __shared__ double red[256];
+  const size_t nc = (size_t)nct * ncp * ncr;
+  double acc[CL_NQ + CL_NTARGET];
+#pragma unroll
+  for (int k = 0; k < CL_NQ + CL_NTARGET; k++) acc[k] = 0.0;
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+    const int it = (int)(c % nct), ip = (int)((c / nct) % ncp), ir = (int)(c / ((size_t)nct * ncp));
+    double q[CL_NQ];
+    cl_quantities(F, nct, ncp, ncr, it, ip, ir, q);
+#pragma unroll
+    for (int k = 0; k < CL_NQ; k++) acc[k] += q[k] * q[k];
+    if (T)
+#pragma unroll
+      for (int k = 0; k < CL_NTARGET; k++) acc[CL_NQ + k] += T[k * nc + c] * T[k * nc + c];
+  }
+  for (int k = 0; k < CL_NQ + CL_NTARGET; k++) {
+    red[threadIdx.x] = acc[k];
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+      if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) part[(size_t)blockIdx.x * (CL_NQ + CL_NTARGET) + k] = red[0];
+    __syncthreads();
+  }
+}
+
+// training targets: Tn[c*CL_YPAD + k] = T[k*nc + c] / tscale[k] (FP32), pad zero
+__global__ void k_closure_targets(const double *__restrict__ T, size_t nc, const float *__restrict__ tscale,
+                                  float *__restrict__ Tn) {
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x)
+    for (int k = 0; k < CL_YPAD; k++)
+      Tn[c * CL_YPAD + k] = k < CL_NTARGET ? (float)(T[k * nc + c] / (double)tscale[k]) : 0.0f;
+}
+
+// exact GELU and its derivative: x Phi(x), Phi(x) + x phi(x)
+__device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+__device__ __forceinline__ float gelu_df(float x) {
+  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+}
+
+// Z (col-major M x n: Z[r*M + j]) += b[j]; H = bf16(GELU(Z)) when H != NULL
+__global__ void k_bias_gelu(float *__restrict__ Z, const float *__restrict__ b, __nv_bfloat16 *__restrict__ H,
+                            int M, size_t n) {
+  const size_t tot = (size_t)M * n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    const float z = Z[i] + b[i % M];
+    Z[i] = z;
+    if (H) H[i] = __float2bfloat16_rn(gelu_f(z));
+  }
+}
+
+// loss and output gradient: D = Y - T over the first nreal of CL_YPAD
+// columns; dY = 2 D / (n nreal) (FP32 and BF16), pad columns zero;
+// part[block] = partial sum of D^2
+__global__ void k_mse(const float *__restrict__ Y, const float *__restrict__ T, size_t n, int nreal,
+                      float *__restrict__ dY, __nv_bfloat16 *__restrict__ dYb, double *__restrict__ part) {
+  __shared__ double red[256];
+  const size_t tot = n * CL_YPAD;
+  const float sc = 2.0f / ((float)n * (float)nreal);
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(i % CL_YPAD);
+    float d = 0.0f;
+    if (k < nreal) {
+      d = Y[i] - T[i];
+      acc += (double)d * d;
+    }
+    dY[i] = sc * d;
+    dYb[i] = __float2bfloat16_rn(sc * d);
+  }
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// back through GELU: dZ = dH * GELU'(Z) (FP32 in place of dH, and BF16)
+__global__ void k_gelu_back(float *__restrict__ dH, const float *__restrict__ Z, __nv_bfloat16 *__restrict__ dZb,
+                            size_t tot) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < tot; i += (size_t)gridDim.x * blockDim.x) {
+    const float d = dH[i] * gelu_df(Z[i]);
+    dH[i] = d;
+    dZb[i] = __float2bfloat16_rn(d);
+  }
+}
+
+// bias gradient: db[j] = sum over the n rows of dZ[r*M + j]; grid = M
+// blocks, each sums its column in a fixed order (deterministic)
+__global__ void k_colsum(const float *__restrict__ dZ, int M, size_t n, float *__restrict__ db) {
+  __shared__ double red[256];
+  const int j = blockIdx.x;
+  double acc = 0.0;
+  for (size_t r = threadIdx.x; r < n; r += blockDim.x) acc += dZ[r * M + j];
+  red[threadIdx.x] = acc;
+  __syncthreads();
+  for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) red[threadIdx.x] += red[threadIdx.x + s];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) db[j] = (float)red[0];
+}
+
+// Adam (bias-corrected) on FP32 master parameters, refreshing the BF16 copy
+__global__ void k_adam(float *__restrict__ w, const float *__restrict__ gr, float *__restrict__ m,
+                       float *__restrict__ v2, __nv_bfloat16 *__restrict__ wb, size_t cnt, float lr, float b1,
+                       float b2, float eps, float c1, float c2) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
+    const float gi = gr[i];
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v2[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v2[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (wb) wb[i] = __float2bfloat16_rn(wi);
+  }
+}
+
+// closure -> SLD speed^2 of each coarse cell: the subgrid velocity variance
+// tau_tt + tau_pp + tau_rr (network outputs times their target scales),
+// floored at zero; -1 (the prescribed profile is used) where the output is
+// not finite
+__global__ void k_closure_speed2(const float *__restrict__ Y, size_t nc, const float *__restrict__ tscale,
+                                 double *__restrict__ speed2) {
+  for (size_t c = blockIdx.x * (size_t)blockDim.x + threadIdx.x; c < nc; c += (size_t)gridDim.x * blockDim.x) {
+    const float *y = Y + c * CL_YPAD;
+    const double tr = (double)y[0] * tscale[0] + (double)y[3] * tscale[3] + (double)y[5] * tscale[5];
+    speed2[c] = isfinite(tr) ? fmax(tr, 0.0) : -1.0;
+  }
+}
+
+}  // namespace css

@@ -30,6 +30,9 @@ struct CssGeo {
   const double *resp_r;     // [r block][lo|hi][tstride]: unit response of d/dr to the face datum of rho
   // radial profiles (length nr)
   const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
+  // per-cell SLD speed^2 replacing dspeed (a learned closure's output);
+  // NULL, or a negative entry, means the prescribed radial profile
+  const double *speed2;
   // theta profiles (length nth)
   const double *sines, *cosines, *theta, *cot, *csc;  // cot = cos/sin, csc = 1/sin
   // SLD cell geometry (diffusion.f90:806-849, :1196-1247, :1316-1351):

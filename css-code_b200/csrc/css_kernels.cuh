@@ -1027,6 +1027,10 @@ __global__ void k_sld_vcc(CssGeo g, const double *__restrict__ v, const double *
   for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x) {
     int ir = (int)(id / ((size_t)g.nth * g.nphi));
     double c = g.dspeed[ir];
+    if (g.speed2) {
+      const double s2 = g.speed2[id];
+      if (s2 >= 0.0) c = s2;
+    }
     if (g.dstype == 1) {
       for (int iv = 1; iv <= 3; iv++) {
         double q = __ldg(v + iv * n + id);

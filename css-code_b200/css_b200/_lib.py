@@ -66,6 +66,22 @@ def lib():
         L.css_ensemble_last_ms.restype = ctypes.c_double
         L.css_ensemble_destroy.argtypes = [ctypes.c_void_p]
         L.css_ensemble_destroy.restype = None
+        vp, ll, fp = ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_float)
+        L.css_set_sld_speed2.argtypes = [vp, vp]
+        L.css_box_filter.argtypes = [vp, ctypes.c_int, vp, vp]
+        L.css_closure_scales.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, fp]
+        L.css_closure_features.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
+        L.css_closure_targets.argtypes = [ll, vp, vp, vp]
+        L.css_closure_speed2.argtypes = [ll, vp, vp, vp]
+        L.css_mlp_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
+                                     ctypes.POINTER(vp)]
+        L.css_mlp_destroy.argtypes = [vp]
+        L.css_mlp_destroy.restype = None
+        L.css_mlp_dims.argtypes = [vp, ctypes.POINTER(ctypes.c_int)]
+        L.css_mlp_forward.argtypes = [vp, vp, ll, vp]
+        L.css_mlp_train_step.argtypes = [vp, vp, vp, ll, ctypes.c_float, fp]
+        L.css_mlp_params.argtypes = [vp, ctypes.c_int, fp, fp, ctypes.c_int]
+        L.css_mlp_grads.argtypes = [vp, ctypes.c_int, fp, fp]
         _LIB = L
     return _LIB
 
@@ -83,5 +99,7 @@ EXPORTS = [
     "css_compact_lines", "css_sync", "css_state_device_ptr", "css_kernel_launches", "css_set_stream",
     "css_profile", "css_kernel_stats", "css_compact_lines_noalloc", "css_scalars", "css_step_size",
     "css_shell_averages", "css_spectrum", "css_autotune", "css_ensemble_create", "css_ensemble_step",
-    "css_ensemble_launches", "css_ensemble_last_ms", "css_ensemble_destroy",
+    "css_ensemble_launches", "css_ensemble_last_ms", "css_ensemble_destroy", "css_set_sld_speed2", "css_box_filter",
+    "css_closure_scales", "css_closure_features", "css_closure_targets", "css_closure_speed2", "css_mlp_create",
+    "css_mlp_destroy", "css_mlp_dims", "css_mlp_forward", "css_mlp_train_step", "css_mlp_params", "css_mlp_grads",
 ]

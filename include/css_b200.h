@@ -258,6 +258,63 @@ long long css_ensemble_launches(css_ensemble *ens);
 double css_ensemble_last_ms(css_ensemble *ens);
 void css_ensemble_destroy(css_ensemble *ens);
 
+/* ---- learned subgrid closure ------------------------------------------------
+ * New: the reference prescribes the SLD speed profile (Initialize_Diffusion,
+ * diffusion.f90:19-63); these entry points learn it per cell from a fine
+ * run instead.  All array arguments are DEVICE pointers; the functions
+ * without a context run on the default stream and return when done.
+ *
+ * css_set_sld_speed2: use speed2[ncell] (or NULL to return to the prescribed
+ * profile) as the per-cell SLD speed^2 of ctx; a negative entry falls back
+ * to the prescribed value of that radius.  The array must stay valid while
+ * ctx steps.
+ * css_box_filter: average the resident state over f x f x f cells (f
+ * divides nr, nth, nphi) into fields[7*nc] (u_theta, u_phi, u_r, s - sr,
+ * B_theta, B_phi, B_r; B = 0 for hydro) and targets[12*nc] (tau_tt tp tr pp
+ * pr rr, q_t q_p q_r, emf_t emf_p emf_r: filtered products minus products
+ * of filtered fields), coarse index it + nct*(ip + ncp*ir).
+ * css_closure_scales: RMS of the five stencil quantities (u_theta, u_phi,
+ * u_r, |B|, ds'/dr in coarse index units) and of the twelve targets
+ * (targets may be NULL) -> scales[17] on the host.
+ * css_closure_features: x[nc*144] BF16, the 3x3x3 neighbourhood (r, theta
+ * clamped, phi periodic) of the five quantities divided by scale[5]: 135
+ * features and 9 zeros per row.
+ * css_closure_targets: tn[nc*16] FP32 = targets / tscale[12], zero padded.
+ * css_closure_speed2: speed2[nc] = max(0, tau_tt + tau_pp + tau_rr) from
+ * network outputs y[nc*16] times tscale, or -1 where not finite.          */
+int css_set_sld_speed2(css_ctx *ctx, const double *speed2);
+int css_box_filter(css_ctx *ctx, int f, double *fields, double *targets);
+int css_closure_scales(int nct, int ncp, int ncr, const double *fields,
+                       const double *targets, float *scales);
+int css_closure_features(int nct, int ncp, int ncr, const double *fields,
+                         const float *scale, void *x_bf16);
+int css_closure_targets(long long nc, const double *targets,
+                        const float *tscale, float *tn);
+int css_closure_speed2(long long nc, const float *y, const float *tscale,
+                       double *speed2);
+
+/* The closure network: n_in -> width -> width -> width -> n_out, exact
+ * GELU after the hidden layers, BF16 weights and activations, FP32
+ * accumulation (the products are tensor-core GEMMs), FP32 master weights
+ * and Adam moments.  Rows are padded to multiples of 16 (dims[5] returns
+ * the padded widths: the input rows of css_mlp_forward /
+ * css_mlp_train_step have dims[0] BF16 values, their outputs and targets
+ * dims[4] FP32 values, row-major).  css_mlp_train_step does one Adam step
+ * on the mean squared error over the n_out real outputs of n <= max_rows
+ * rows and returns the loss before the step.  css_mlp_params gets (set=0)
+ * or sets (set=1) layer l's FP32 weights (row-major dims[l] x dims[l+1])
+ * and biases on the host; css_mlp_grads returns the last step's gradients. */
+typedef struct css_mlp css_mlp;
+int css_mlp_create(int n_in, int width, int n_out, int max_rows,
+                   unsigned long long seed, css_mlp **out);
+void css_mlp_destroy(css_mlp *mlp);
+int css_mlp_dims(css_mlp *mlp, int *dims);
+int css_mlp_forward(css_mlp *mlp, const void *x_bf16, long long n, float *y);
+int css_mlp_train_step(css_mlp *mlp, const void *x_bf16, const float *t,
+                       long long n, float lr, float *loss);
+int css_mlp_params(css_mlp *mlp, int layer, float *w, float *b, int set);
+int css_mlp_grads(css_mlp *mlp, int layer, float *gw, float *gb);
+
 /* ---- diagnostics of the current state (vars0), computed on the device ----
  * Each call reads the state left by css_upload_state / css_step_rk4, uses
  * the stage buffers as scratch (so it must not overlap a step on another
