@@ -188,6 +188,10 @@ def run_reference(args):
         return 0
     if args.workload.startswith("ensemble-"):
         return run_reference_ensemble(args, world)
+    if args.workload.startswith("closure-"):
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned closure: its SLD "
+                          "speed is a prescribed radial profile (diffusion.f90:19-63)"}))
+        return 0
     p, prof, v0, dt, _ = problem.build(args.workload)
     from oracle import oracle as O
     threads = os.cpu_count() or 1
@@ -478,6 +482,98 @@ def run_ensemble(args):
     return 0
 
 
+def run_closure(args):
+    """The closure network (closure-<nr>x<nth>x<nphi>: one row per coarse
+    cell): inference over the whole coarse grid and Adam steps of 65536
+    rows, both timed with CUDA events on the network's stream.  The bound
+    is the tensor cores: achieved FLOP/s of the products against the
+    measured BF16 GEMM peak."""
+    import numpy as np
+    import torch
+    from css_b200 import closure as C
+    rank, world, local = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    nr, nth, nphi = (int(x) for x in args.workload.split("-")[1].split("x"))
+    nc = nr * nth * nphi
+    batch = 65536
+    g = torch.Generator(device="cpu").manual_seed(11)
+    xh = torch.zeros(nc, C.XPAD, dtype=torch.bfloat16)
+    xh[:, :135] = torch.randn(nc, 135, generator=g).to(torch.bfloat16)
+    x = xh.to(dev)
+    t = torch.zeros(batch, C.YPAD, dtype=torch.float32)
+    t[:, :12] = torch.randn(batch, 12, generator=g)
+    t = t.to(dev)
+    net = C.Mlp(135, 128, 12, max_rows=batch, seed=1)
+    stream = torch.cuda.current_stream(dev)
+    net.set_stream(stream.cuda_stream)
+    d = net.dims
+    fwd_flop_row = 2.0 * sum(d[l] * d[l + 1] for l in range(4))
+    # backward: weight gradients of every layer, input gradients of layers 1-3
+    bwd_flop_row = 2.0 * sum(d[l] * d[l + 1] for l in range(4)) + 2.0 * sum(d[l] * d[l + 1] for l in range(1, 4))
+    for _ in range(args.warmup):
+        net.forward(x, nc)
+        net.train_step(x[:batch], t, batch, 1e-4)
+    clocks = ClockSampler(local)
+    if rank == 0:
+        clocks.start()
+        time.sleep(0.3)
+    barrier(world)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    for _ in range(args.steps):
+        net.forward(x, nc)
+    e1.record(stream)
+    for _ in range(args.steps):
+        net.train_step(x[:batch], t, batch, 1e-4)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    barrier(world)
+    clk = clocks.stop() if rank == 0 else None
+    inf_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
+    tr_ms = max_over_ranks(e1.elapsed_time(e2) / args.steps, world)
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        pass
+    peak = peaks.get("bf16_tflops", 1590.0)
+    inf_tf = fwd_flop_row * nc / (inf_ms / 1e3) / 1e12
+    tr_tf = (fwd_flop_row + bwd_flop_row) * batch / (tr_ms / 1e3) / 1e12
+    # e2e: features from pinned host memory, inference, predictions back
+    xp = xh.pin_memory()
+    yp = torch.empty(nc * C.YPAD, dtype=torch.float32).pin_memory()
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    h0.record(stream)
+    xd = xp.to(dev, non_blocking=True)
+    y = net.forward(xd, nc)
+    yp.copy_(y, non_blocking=True)
+    h1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(h0.elapsed_time(h1), world)
+    out = {"metric": "closure inference rows/s (one row per coarse cell)", "value": nc * world / (inf_ms / 1e3),
+           "unit": "rows/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": inf_ms,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "bf16 (fp32 accumulate)",
+           "data": "synthetic",
+           "config": {"workload": args.workload, "rows": nc, "layers": list(d), "train_batch": batch,
+                      "l2": "features (%.0f MB) larger than L2" % (nc * C.XPAD * 2 / 1e6)},
+           "training": {"rows_per_s": batch * world / (tr_ms / 1e3), "ms_per_step": tr_ms, "tflops": tr_tf},
+           "roofline": {"bound": "tensor", "achieved": inf_tf, "peak": peak, "unit": "TFLOP/s",
+                        "frac": inf_tf / peak, "traffic": None, "peak_source": "measured" if peaks else "fallback",
+                        "flop_per_row": fwd_flop_row},
+           "e2e": {"value": nc * world / (e2e_ms / 1e3), "unit": "rows/s", "h2d_bytes_per_step": nc * C.XPAD * 2,
+                   "d2h_bytes_per_step": nc * C.YPAD * 4},
+           # own kernels in the timed region: 4 bias/GELU per forward batch; per training
+           # step 4 bias/GELU, loss, 4 column sums, 3 GELU backward, 8 Adam (GEMMs are cuBLASLt)
+           "gpu_launches": args.steps * (4 * ((nc + batch - 1) // batch) + 20)}
+    if clk:
+        out["clocks"] = clk
+    net.close()
+    if rank == 0:
+        print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -497,6 +593,8 @@ def main():
         return run_reference(args)
     if args.workload.startswith("ensemble-"):
         return run_ensemble(args)
+    if args.workload.startswith("closure-"):
+        return run_closure(args)
     return run_ours(args)
 
 

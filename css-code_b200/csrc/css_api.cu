@@ -1460,7 +1460,7 @@ struct css_mlp {
   cublasLtHandle_t lt = nullptr;
   void *ws = nullptr;
   size_t wsz = 32u << 20;
-  cudaStream_t st = nullptr;
+  cudaStream_t st = nullptr, own_st = nullptr;
 };
 
 static int lt_gemm(css_mlp *m, bool ta, bool tb, int M, int N, int K, const __nv_bfloat16 *A, int lda,
@@ -1509,7 +1509,8 @@ extern "C" void css_mlp_destroy(css_mlp *m) {
   }
   cudaFree(m->dH); cudaFree(m->dZb); cudaFree(m->part); cudaFree(m->ws);
   if (m->lt) cublasLtDestroy(m->lt);
-  if (m->st) cudaStreamDestroy(m->st);
+  if (m->own_st) cudaStreamDestroy(m->own_st);
+  else if (m->st) cudaStreamDestroy(m->st);
   delete m;
 }
 
@@ -1662,6 +1663,14 @@ extern "C" int css_mlp_train_step(css_mlp *m, const void *x, const float *t, lon
   double s = 0.0;
   for (double v : h) s += v;
   if (loss) *loss = (float)(s / ((double)rows * m->nreal_out));
+  return CSS_OK;
+}
+
+// run the network's work on the caller's stream (NULL: its own)
+extern "C" int css_mlp_set_stream(css_mlp *m, void *stream) {
+  if (!m) { set_err("css_mlp_set_stream: NULL"); return CSS_ERR_ARG; }
+  if (!m->own_st) m->own_st = m->st;
+  m->st = stream ? (cudaStream_t)stream : m->own_st;
   return CSS_OK;
 }
 

@@ -92,6 +92,9 @@ class Mlp:
         check(_lib.lib().css_mlp_train_step(self.h, _ptr(x), _ptr(t), n, float(lr), ctypes.byref(loss)))
         return loss.value
 
+    def set_stream(self, stream_handle):
+        check(_lib.lib().css_mlp_set_stream(self.h, stream_handle))
+
     def params(self, layer):
         k, m = self.dims[layer], self.dims[layer + 1]
         w = np.zeros((k, m), dtype=np.float32)

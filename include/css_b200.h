@@ -314,6 +314,8 @@ int css_mlp_train_step(css_mlp *mlp, const void *x_bf16, const float *t,
                        long long n, float lr, float *loss);
 int css_mlp_params(css_mlp *mlp, int layer, float *w, float *b, int set);
 int css_mlp_grads(css_mlp *mlp, int layer, float *gw, float *gb);
+/* run the network's work on the caller's cudaStream_t (NULL: its own) */
+int css_mlp_set_stream(css_mlp *mlp, void *stream);
 
 /* ---- diagnostics of the current state (vars0), computed on the device ----
  * Each call reads the state left by css_upload_state / css_step_rk4, uses
