@@ -1461,6 +1461,8 @@ struct css_mlp {
   void *ws = nullptr;
   size_t wsz = 32u << 20;
   cudaStream_t st = nullptr, own_st = nullptr;
+  unsigned char *packed = nullptr;  // weights for the fused forward kernel
+  bool packed_ok = false, fused = true;
 };
 
 static int lt_gemm(css_mlp *m, bool ta, bool tb, int M, int N, int K, const __nv_bfloat16 *A, int lda,
@@ -1507,7 +1509,7 @@ extern "C" void css_mlp_destroy(css_mlp *m) {
     cudaFree(m->mW[l]); cudaFree(m->vW[l]); cudaFree(m->mB[l]); cudaFree(m->vB[l]); cudaFree(m->Wb[l]);
     cudaFree(m->Z[l]); cudaFree(m->H[l]);
   }
-  cudaFree(m->dH); cudaFree(m->dZb); cudaFree(m->part); cudaFree(m->ws);
+  cudaFree(m->dH); cudaFree(m->dZb); cudaFree(m->part); cudaFree(m->ws); cudaFree(m->packed);
   if (m->lt) cublasLtDestroy(m->lt);
   if (m->own_st) cudaStreamDestroy(m->own_st);
   else if (m->st) cudaStreamDestroy(m->st);
@@ -1547,6 +1549,7 @@ extern "C" int css_mlp_create(int n_in, int width, int n_out, int max_rows, unsi
   if (!e) e = cudaMalloc(&m->dH, m->cap * wmax * 4);
   if (!e) e = cudaMalloc(&m->dZb, m->cap * wmax * 2);
   if (!e) e = cudaMalloc(&m->part, 1024 * 8);
+  if (!e) e = cudaMalloc(&m->packed, FM_PARAM_BYTES);
   if (e) {
     set_err("css_mlp_create: %s", cudaGetErrorString(e));
     css_mlp_destroy(m);
@@ -1612,9 +1615,52 @@ static int mlp_forward_rows(css_mlp *m, const __nv_bfloat16 *x, size_t n) {
   return CSS_OK;
 }
 
+static bool mlp_fusable(const css_mlp *m) {
+  return m->dims[0] == FM_IN && m->dims[1] == FM_W && m->dims[2] == FM_W && m->dims[3] == FM_W &&
+         m->dims[4] == FM_OUT;
+}
+
+// transposed, padded BF16 weights and FP32 biases in one block for k_mlp_fused
+static int mlp_pack(css_mlp *m) {
+  const int kp[4] = {FM_KP0, FM_KP, FM_KP, FM_KP};
+  const size_t off[4] = {0, FM_OFF_W1, FM_OFF_W2, FM_OFF_W3};
+  for (int l = 0; l < 4; l++) {
+    k_pack_wt<<<64, 256, 0, m->st>>>(m->Wb[l], m->dims[l], m->dims[l + 1], kp[l],
+                                      reinterpret_cast<__nv_bfloat16 *>(m->packed + off[l]));
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(m->packed + FM_OFF_B + (size_t)l * FM_W * 4, m->B[l], (size_t)m->dims[l + 1] * 4,
+                             cudaMemcpyDeviceToDevice, m->st));
+  }
+  m->packed_ok = true;
+  return CSS_OK;
+}
+
+// 1: forward passes use the fused kernel (the default when the widths are
+// 144/128/128/128/16); 0: the per-layer GEMM path
+extern "C" int css_mlp_set_fused(css_mlp *m, int on) {
+  if (!m) { set_err("css_mlp_set_fused: NULL"); return CSS_ERR_ARG; }
+  m->fused = on != 0;
+  return CSS_OK;
+}
+
 extern "C" int css_mlp_forward(css_mlp *m, const void *x, long long n, float *y) {
   if (!m || !x || !y || n < 1) { set_err("css_mlp_forward: bad argument"); return CSS_ERR_ARG; }
   const int K0 = m->dims[0], MO = m->dims[4];
+  if (m->fused && mlp_fusable(m)) {
+    static bool attr_done = false;
+    if (!attr_done) {
+      CUDA_TRY(cudaFuncSetAttribute(k_mlp_fused, cudaFuncAttributeMaxDynamicSharedMemorySize, FM_SMEM_BYTES));
+      attr_done = true;
+    }
+    if (!m->packed_ok)
+      if (int rc = mlp_pack(m)) return rc;
+    const long long ntiles = (n + 15) / 16;
+    const int grid = (int)std::min<long long>(148, (ntiles + FM_WARPS - 1) / FM_WARPS);
+    k_mlp_fused<<<grid, FM_WARPS * 32, FM_SMEM_BYTES, m->st>>>((const __nv_bfloat16 *)x, n, m->packed, y);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(m->st));
+    return CSS_OK;
+  }
   for (long long r0 = 0; r0 < n; r0 += (long long)m->cap) {
     const size_t rows = (size_t)std::min<long long>((long long)m->cap, n - r0);
     if (int rc = mlp_forward_rows(m, (const __nv_bfloat16 *)x + (size_t)r0 * K0, rows)) return rc;
@@ -1649,6 +1695,7 @@ extern "C" int css_mlp_train_step(css_mlp *m, const void *x, const float *t, lon
     }
   }
   m->adam_t++;
+  m->packed_ok = false;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   const float c1 = 1.0f - powf(b1, (float)m->adam_t), c2 = 1.0f - powf(b2, (float)m->adam_t);
   for (int l = 0; l < 4; l++) {
@@ -1685,6 +1732,7 @@ extern "C" int css_mlp_params(css_mlp *m, int l, float *w, float *b, int set) {
     k_to_bf16<<<64, 256, 0, m->st>>>(m->W[l], m->Wb[l], K * M);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(m->st));
+    m->packed_ok = false;
   } else {
     if (w) CUDA_TRY(cudaMemcpy(w, m->W[l], K * M * 4, cudaMemcpyDeviceToHost));
     if (b) CUDA_TRY(cudaMemcpy(b, m->B[l], M * 4, cudaMemcpyDeviceToHost));

@@ -246,3 +246,158 @@ __global__ void k_closure_speed2(const float *__restrict__ Y, size_t nc, const f
 }
 
 }  // namespace css
+
+namespace css {
+
+// ---------------------------------------------------------------------------
+// Fused forward pass of the closure network (in 144 -> 128 -> 128 -> 128 ->
+// 16, GELU after the hidden layers).  A persistent CTA of 8 warps copies the
+// BF16 weights (stored transposed, n-major with k contiguous and rows padded
+// by 8 so fragment loads hit distinct banks) and the FP32 biases into shared
+// memory once; each warp then takes 16 rows at a time: the feature rows are
+// staged in shared memory by asynchronous 16-byte copies, the four layers
+// run as BF16 tensor-core MMAs (m16n8k16, FP32 accumulate), and each
+// layer's accumulator fragments, after bias and GELU, are rounded to BF16
+// and reused in registers as the next layer's A fragments.  Only the
+// features are read and only the outputs written.
+// ---------------------------------------------------------------------------
+#define FM_IN 144
+#define FM_W 128
+#define FM_OUT 16
+#define FM_KP0 (FM_IN + 8)   // padded row of the first layer's transposed weights
+#define FM_KP (FM_W + 8)     // padded row of the other layers
+#define FM_XS (FM_IN + 8)    // padded feature row in shared memory
+#define FM_WARPS 8
+// packed parameter block (bytes): W0t | W1t | W2t | W3t | b0 b1 b2 b3 (FP32)
+#define FM_OFF_W1 (FM_W * FM_KP0 * 2)
+#define FM_OFF_W2 (FM_OFF_W1 + FM_W * FM_KP * 2)
+#define FM_OFF_W3 (FM_OFF_W2 + FM_W * FM_KP * 2)
+#define FM_OFF_B (FM_OFF_W3 + FM_OUT * FM_KP * 2)
+#define FM_PARAM_BYTES (FM_OFF_B + (3 * FM_W + FM_OUT) * 4)
+#define FM_SMEM_BYTES (FM_PARAM_BYTES + FM_WARPS * 16 * FM_XS * 2)
+
+// dst[n*KP + k] = W[k*M + n] (k < K), zero in the padding
+__global__ void k_pack_wt(const __nv_bfloat16 *__restrict__ W, int K, int M, int KP, __nv_bfloat16 *__restrict__ dst) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < M * KP; i += gridDim.x * blockDim.x) {
+    const int nn = i / KP, k = i - nn * KP;
+    dst[i] = k < K ? W[(size_t)k * M + nn] : __float2bfloat16_rn(0.0f);
+  }
+}
+
+__device__ __forceinline__ void mma_bf16_16816(float (&d)[4], const unsigned (&a)[4], unsigned b0, unsigned b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};\n"
+      : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+__device__ __forceinline__ unsigned pack_bf16x2(float lo, float hi) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<unsigned *>(&h);
+}
+
+// one hidden layer: acc (16 n-tiles of 8 columns) = A (KSTEPS k-steps) x Wt
+template <int KSTEPS, int KPAD>
+__device__ __forceinline__ void fm_layer(const unsigned (&a)[KSTEPS][4], const __nv_bfloat16 *__restrict__ Wt,
+                                         int g, int t, float (&acc)[16][4]) {
+#pragma unroll
+  for (int nt = 0; nt < 16; nt++)
+#pragma unroll
+    for (int q = 0; q < 4; q++) acc[nt][q] = 0.0f;
+#pragma unroll
+  for (int j = 0; j < KSTEPS; j++)
+#pragma unroll
+    for (int nt = 0; nt < 16; nt++) {
+      const __nv_bfloat16 *wr = Wt + (size_t)(nt * 8 + g) * KPAD + 16 * j + 2 * t;
+      const unsigned b0 = *reinterpret_cast<const unsigned *>(wr);
+      const unsigned b1 = *reinterpret_cast<const unsigned *>(wr + 8);
+      mma_bf16_16816(acc[nt], a[j], b0, b1);
+    }
+}
+
+// bias + GELU on the accumulators, rounded to BF16 A fragments of the next layer
+__device__ __forceinline__ void fm_activate(const float (&acc)[16][4], const float *__restrict__ b, int t,
+                                            unsigned (&a)[8][4]) {
+#pragma unroll
+  for (int j = 0; j < 8; j++) {
+    const int c0 = 16 * j + 2 * t, c1 = c0 + 8;
+    const float *lo = acc[2 * j], *hi = acc[2 * j + 1];
+    a[j][0] = pack_bf16x2(gelu_f(lo[0] + b[c0]), gelu_f(lo[1] + b[c0 + 1]));
+    a[j][1] = pack_bf16x2(gelu_f(lo[2] + b[c0]), gelu_f(lo[3] + b[c0 + 1]));
+    a[j][2] = pack_bf16x2(gelu_f(hi[0] + b[c1]), gelu_f(hi[1] + b[c1 + 1]));
+    a[j][3] = pack_bf16x2(gelu_f(hi[2] + b[c1]), gelu_f(hi[3] + b[c1 + 1]));
+  }
+}
+
+__global__ void __launch_bounds__(FM_WARPS * 32, 1) k_mlp_fused(const __nv_bfloat16 *__restrict__ X, long long n,
+                                                               const unsigned char *__restrict__ params,
+                                                               float *__restrict__ Y) {
+  extern __shared__ __align__(16) unsigned char fm_sm[];
+  // parameters -> shared memory (16-byte words; FM_PARAM_BYTES is a multiple of 16)
+  for (int i = threadIdx.x; i < FM_PARAM_BYTES / 16; i += blockDim.x)
+    reinterpret_cast<uint4 *>(fm_sm)[i] = reinterpret_cast<const uint4 *>(params)[i];
+  __syncthreads();
+  const __nv_bfloat16 *W0 = reinterpret_cast<const __nv_bfloat16 *>(fm_sm);
+  const __nv_bfloat16 *W1 = reinterpret_cast<const __nv_bfloat16 *>(fm_sm + FM_OFF_W1);
+  const __nv_bfloat16 *W2 = reinterpret_cast<const __nv_bfloat16 *>(fm_sm + FM_OFF_W2);
+  const __nv_bfloat16 *W3 = reinterpret_cast<const __nv_bfloat16 *>(fm_sm + FM_OFF_W3);
+  const float *bias = reinterpret_cast<const float *>(fm_sm + FM_OFF_B);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  __nv_bfloat16 *Xs = reinterpret_cast<__nv_bfloat16 *>(fm_sm + FM_PARAM_BYTES) + (size_t)warp * 16 * FM_XS;
+  const long long ntiles = (n + 15) / 16;
+  for (long long tile = (long long)blockIdx.x * FM_WARPS + warp; tile < ntiles;
+       tile += (long long)gridDim.x * FM_WARPS) {
+    const long long r0 = tile * 16;
+    // stage 16 feature rows (18 x 16 bytes each); rows past n are zero
+    for (int k = lane; k < 16 * (FM_IN / 8); k += 32) {
+      const int row = k / (FM_IN / 8), ch = k - row * (FM_IN / 8);
+      const bool in = r0 + row < n;
+      const __nv_bfloat16 *src = in ? X + (size_t)(r0 + row) * FM_IN + ch * 8 : X;
+      cp_async16(Xs + row * FM_XS + ch * 8, src, in ? 16 : 0);
+    }
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncwarp();
+    unsigned a0[FM_IN / 16][4];
+#pragma unroll
+    for (int j = 0; j < FM_IN / 16; j++) {
+      a0[j][0] = *reinterpret_cast<const unsigned *>(Xs + g * FM_XS + 16 * j + 2 * t);
+      a0[j][1] = *reinterpret_cast<const unsigned *>(Xs + (g + 8) * FM_XS + 16 * j + 2 * t);
+      a0[j][2] = *reinterpret_cast<const unsigned *>(Xs + g * FM_XS + 16 * j + 8 + 2 * t);
+      a0[j][3] = *reinterpret_cast<const unsigned *>(Xs + (g + 8) * FM_XS + 16 * j + 8 + 2 * t);
+    }
+    __syncwarp();  // the staging buffer is free for the next tile
+    float acc[16][4];
+    unsigned a[8][4];
+    fm_layer<FM_IN / 16, FM_KP0>(a0, W0, g, t, acc);
+    fm_activate(acc, bias, t, a);
+    fm_layer<8, FM_KP>(a, W1, g, t, acc);
+    fm_activate(acc, bias + FM_W, t, a);
+    fm_layer<8, FM_KP>(a, W2, g, t, acc);
+    fm_activate(acc, bias + 2 * FM_W, t, a);
+    // output layer: 2 n-tiles
+    float out[2][4] = {{0.f, 0.f, 0.f, 0.f}, {0.f, 0.f, 0.f, 0.f}};
+#pragma unroll
+    for (int j = 0; j < 8; j++)
+#pragma unroll
+      for (int nt = 0; nt < 2; nt++) {
+        const __nv_bfloat16 *wr = W3 + (size_t)(nt * 8 + g) * FM_KP + 16 * j + 2 * t;
+        mma_bf16_16816(out[nt], a[j], *reinterpret_cast<const unsigned *>(wr),
+                       *reinterpret_cast<const unsigned *>(wr + 8));
+      }
+    const float *b3 = bias + 3 * FM_W;
+#pragma unroll
+    for (int nt = 0; nt < 2; nt++) {
+      const int c = nt * 8 + 2 * t;
+      if (r0 + g < n)
+        *reinterpret_cast<float2 *>(Y + (size_t)(r0 + g) * FM_OUT + c) =
+            make_float2(out[nt][0] + b3[c], out[nt][1] + b3[c + 1]);
+      if (r0 + g + 8 < n)
+        *reinterpret_cast<float2 *>(Y + (size_t)(r0 + g + 8) * FM_OUT + c) =
+            make_float2(out[nt][2] + b3[c], out[nt][3] + b3[c + 1]);
+    }
+  }
+}
+
+}  // namespace css

@@ -83,6 +83,7 @@ def lib():
         L.css_mlp_params.argtypes = [vp, ctypes.c_int, fp, fp, ctypes.c_int]
         L.css_mlp_grads.argtypes = [vp, ctypes.c_int, fp, fp]
         L.css_mlp_set_stream.argtypes = [vp, vp]
+        L.css_mlp_set_fused.argtypes = [vp, ctypes.c_int]
         _LIB = L
     return _LIB
 
@@ -103,5 +104,5 @@ EXPORTS = [
     "css_ensemble_launches", "css_ensemble_last_ms", "css_ensemble_destroy", "css_set_sld_speed2", "css_box_filter",
     "css_closure_scales", "css_closure_features", "css_closure_targets", "css_closure_speed2", "css_mlp_create",
     "css_mlp_destroy", "css_mlp_dims", "css_mlp_forward", "css_mlp_train_step", "css_mlp_params", "css_mlp_grads",
-    "css_mlp_set_stream",
+    "css_mlp_set_stream", "css_mlp_set_fused",
 ]

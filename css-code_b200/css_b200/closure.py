@@ -92,6 +92,10 @@ class Mlp:
         check(_lib.lib().css_mlp_train_step(self.h, _ptr(x), _ptr(t), n, float(lr), ctypes.byref(loss)))
         return loss.value
 
+    def set_fused(self, on=True):
+        """Fused one-kernel forward (default) or the per-layer GEMM path."""
+        check(_lib.lib().css_mlp_set_fused(self.h, 1 if on else 0))
+
     def set_stream(self, stream_handle):
         check(_lib.lib().css_mlp_set_stream(self.h, stream_handle))
 

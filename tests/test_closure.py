@@ -149,10 +149,17 @@ def test_mlp_forward_and_gradients_match_numpy(gpu_available):
     t[:, :12] = rng.standard_normal((n, 12))
     xd = torch.from_numpy(x).to(torch.bfloat16).cuda()
     td = torch.from_numpy(t).cuda()
-    y = net.forward(xd, n).cpu().numpy().reshape(n, 16)
+    y = net.forward(xd, n).cpu().numpy().reshape(n, 16)  # fused kernel
+    net.set_fused(False)
+    yg = net.forward(xd, n).cpu().numpy().reshape(n, 16)  # per-layer GEMMs
+    net.set_fused(True)
     yr, grads, loss = numpy_net(net, x, t, 12)
-    assert np.abs(y - yr).max() <= 2e-2 * np.abs(yr).max()
-    assert np.abs(y[:, 12:]).max() == 0.0
+    for out in (y, yg):
+        assert np.abs(out - yr).max() <= 2e-2 * np.abs(yr).max()
+        assert np.abs(out[:, 12:]).max() == 0.0
+    # a ragged row count takes the partial last tile of the fused kernel
+    y7 = net.forward(xd[:4093].contiguous(), 4093).cpu().numpy().reshape(4093, 16)
+    assert np.abs(y7 - y[:4093]).max() <= 1e-6 * np.abs(y).max()
     gloss = net.train_step(xd, td, n, 0.0)  # lr 0: gradients only
     assert abs(gloss - loss) <= 2e-2 * loss
     for l in range(4):
