@@ -212,7 +212,7 @@ static size_t smem_phi_terms(int mag, int m, int TL) {
 }
 static size_t smem_radial_terms(int mag, int m, int TL) {
   int nh = mag ? 7 : 5, nd = mag ? 8 : 6;
-  return 8 * ((size_t)nh * (m + 8) * (TL + 1) + (size_t)nd * m * (TL + 1) + (size_t)nd * 3 * (m + 2) + TL);
+  return 8 * ((size_t)nh * (m + 8) * TL + (size_t)nd * m * TL + (size_t)nd * 3 * (m + 2) + TL);
 }
 static size_t smem_rhot(int m, int TL) { return 8 * ((size_t)TL * (m + 9) + (size_t)TL * (m + 1) + 3 * (m + 2)); }
 static size_t smem_line(int nh, int nd, int na, int m, int TL) {

@@ -577,7 +577,7 @@ __device__ __forceinline__ void radial_point(const CssGeo &g, int ir, const RadI
 // the datum times the block's unit response (resp) is added afterwards.
 // ---------------------------------------------------------------------------
 template <int MT, int TLC, typename TV>
-__global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const TV *__restrict__ cur,
+__global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__restrict__ cur,
                                                       const double *__restrict__ bf, double *__restrict__ dv,
                                                       const double *__restrict__ tbuf, int TLrt) {
   extern __shared__ double sm[];
@@ -589,7 +589,7 @@ __global__ void __launch_bounds__(128) k_radial_terms(CssGeo g, const TV *__rest
   const int r0 = D.start[br], m = MT ? MT : D.size[br];
   const int dtype = dtype_of(D, br);
   const int mag = g.magnetic;
-  const int SR = TL + 1, TS = 3 * (m + 2);
+  const int SR = TL, TS = 3 * (m + 2);  // lines contiguous, unpadded (4 CTAs per SM)
   const size_t n = (size_t)g.ncell;
   const int nh = mag ? 7 : 5;  // w v u s rho [bt bp]
   const int nd = mag ? 8 : 6;  // dw dv du ds d2s drho0 [dbt dbp]
@@ -784,81 +784,115 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
   __syncthreads();
   const int nv = g.nv;
   int bad = 0;
-  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
-    int l = pt / m, j = pt - l * m;
-    int it = t0 + j, ip = pb + l;
-    if (ip >= g.nphi) continue;
-    size_t id = pl + (size_t)ip * g.nth + it;
-    double rho = H[(size_t)l * SR + 4 + j];
-    double w = st_val(cur + n, id, nullptr, ir);
-    double t = __ldg(tbuf + id);
-    double w1 = ri * O[(size_t)l * SO + j];
-    double d0 = dv[id] - w * w1;
-    w1 = w1 * (1.0 / rho);
-    double d1 = dv[n + id] - g.pconst * w1 * t;
-    if (g.xi_cs < 1.0) d0 = (g.xi_cs * g.xi_cs) * d0;
+  // each thread's points: the density term with all points' loads issued
+  // first, then the stage combination field by field, again loading every
+  // point of a field before storing any (nx may be v0, so the compiler
+  // could not reorder these itself)
+  constexpr int PPT = (MT > 0 && TLC > 0) ? (MT * TLC + NT - 1) / NT : 1;
+  const int stride = (MT > 0 && TLC > 0) ? NT : (int)blockDim.x;
+  for (int pt0 = threadIdx.x; pt0 < TL * m; pt0 += PPT * stride) {
+    size_t idk[PPT];
+    bool okk[PPT];
+    int itk[PPT];
+    double d0k[PPT], d1k[PPT], wk[PPT], tk[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      const int pt = pt0 + k * stride;
+      const int l = pt / m, j = pt - l * m;
+      okk[k] = pt < TL * m && pb + l < g.nphi;
+      itk[k] = t0 + j;
+      idk[k] = pl + (size_t)(pb + l) * g.nth + t0 + j;
+      if (okk[k]) {
+        wk[k] = st_val(cur + n, idk[k], nullptr, ir);
+        tk[k] = __ldg(tbuf + idk[k]);
+        d0k[k] = dv[idk[k]];
+        d1k[k] = dv[n + idk[k]];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      if (!okk[k]) continue;
+      const int pt = pt0 + k * stride;
+      const int l = pt / m, j = pt - l * m;
+      const double rho = H[(size_t)l * SR + 4 + j];
+      double w1 = ri * O[(size_t)l * SO + j];
+      double d0 = d0k[k] - wk[k] * w1;
+      w1 = w1 * (1.0 / rho);
+      const double d1 = d1k[k] - g.pconst * w1 * tk[k];
+      if (g.xi_cs < 1.0) d0 = (g.xi_cs * g.xi_cs) * d0;
+      d0k[k] = d0;
+      d1k[k] = d1;
+    }
     if (stage == 0) {
-      dv[id] = d0;
-      dv[n + id] = d1;
+#pragma unroll
+      for (int k = 0; k < PPT; k++)
+        if (okk[k]) {
+          dv[idk[k]] = d0k[k];
+          dv[n + idk[k]] = d1k[k];
+        }
       continue;
     }
-    const bool twall = (it == 0 || it == g.nth - 1), rlo = (ir == 0), rhi = (ir == g.nr - 1);
-    double dd[8], aa[8], ss[8];
+    const bool rlo = (ir == 0), rhi = (ir == g.nr - 1);
+    for (int iv = 0; iv < nv; iv++) {
+      double dd[PPT], aa[PPT], ss[PPT];
 #pragma unroll
-    for (int iv = 0; iv < 8; iv++) {
-      if (iv >= nv) break;
-      size_t q = (size_t)iv * n + id;
-      dd[iv] = (iv == 0) ? d0 : (iv == 1) ? d1 : dv[q];
-      aa[iv] = v0[q];
-      ss[iv] = (stage == 1 && !g.sldiffusion) ? 0.0 : vs[q];
-    }
-#pragma unroll
-    for (int iv = 0; iv < 8; iv++) {
-      if (iv >= nv) break;
-      size_t q = (size_t)iv * n + id;
-      double d = dd[iv], a = aa[iv], o;
-      if (stage == 1) {
-        double sv = g.sldiffusion ? ss[iv] + d / 6.0 : d;
-        vs[q] = sv;
-        o = a + dtcur * d;
-      } else if (stage == 4) {
-        double sv = ss[iv] + d / 6.0;
-        o = a + dtcur * sv;
-      } else {
-        double sv = ss[iv] + d / 3.0;
-        vs[q] = sv;
-        o = a + dtcur * d;
+      for (int k = 0; k < PPT; k++) {
+        if (!okk[k]) continue;
+        const size_t q = (size_t)iv * n + idk[k];
+        dd[k] = (iv == 0) ? d0k[k] : (iv == 1) ? d1k[k] : dv[q];
+        aa[k] = v0[q];
+        ss[k] = (stage == 1 && !g.sldiffusion) ? 0.0 : vs[q];
       }
-      // Bound (rhs_mpi.f90:2395-2491)
-      if (twall || rlo || rhi) {
-        if (iv == 1 && twall) o = 0.0;
-        if (iv == 3 && !g.theta_stress_free && twall) o = 0.0;
-        if (rlo) {
-          if ((iv == 1 || iv == 2) && !g.bottom_stress_free) o = 0.0;
-          if (iv == 3) o = 0.0;
+#pragma unroll
+      for (int k = 0; k < PPT; k++) {
+        if (!okk[k]) continue;
+        const size_t q = (size_t)iv * n + idk[k];
+        const double d = dd[k], a = aa[k];
+        double o;
+        if (stage == 1) {
+          double sv = g.sldiffusion ? ss[k] + d / 6.0 : d;
+          vs[q] = sv;
+          o = a + dtcur * d;
+        } else if (stage == 4) {
+          double sv = ss[k] + d / 6.0;
+          o = a + dtcur * sv;
+        } else {
+          double sv = ss[k] + d / 3.0;
+          vs[q] = sv;
+          o = a + dtcur * d;
         }
-        if (rhi) {
-          if ((iv == 1 || iv == 2) && !g.top_stress_free) o = 0.0;
-          if (iv == 3) o = 0.0;
-        }
-        if (iv >= 5) {
-          if (g.theta_perf_conductor) {
-            if ((iv == 6 || iv == 7) && twall) o = 0.0;
-          } else if (iv == 5 && twall) {
-            o = 0.0;
-          }
+        const bool twall = (itk[k] == 0 || itk[k] == g.nth - 1);
+        // Bound (rhs_mpi.f90:2395-2491)
+        if (twall || rlo || rhi) {
+          if (iv == 1 && twall) o = 0.0;
+          if (iv == 3 && !g.theta_stress_free && twall) o = 0.0;
           if (rlo) {
-            if (g.bottom_radial_field) { if (iv == 7) o = 0.0; }
-            else if (g.bottom_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+            if ((iv == 1 || iv == 2) && !g.bottom_stress_free) o = 0.0;
+            if (iv == 3) o = 0.0;
           }
           if (rhi) {
-            if (g.top_radial_field) { if (iv == 7) o = 0.0; }
-            else if (g.top_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+            if ((iv == 1 || iv == 2) && !g.top_stress_free) o = 0.0;
+            if (iv == 3) o = 0.0;
+          }
+          if (iv >= 5) {
+            if (g.theta_perf_conductor) {
+              if ((iv == 6 || iv == 7) && twall) o = 0.0;
+            } else if (iv == 5 && twall) {
+              o = 0.0;
+            }
+            if (rlo) {
+              if (g.bottom_radial_field) { if (iv == 7) o = 0.0; }
+              else if (g.bottom_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+            }
+            if (rhi) {
+              if (g.top_radial_field) { if (iv == 7) o = 0.0; }
+              else if (g.top_perfect_cond) { if (iv == 5 || iv == 6) o = 0.0; }
+            }
           }
         }
+        if (!isfinite(o)) bad = 1;
+        nx[q] = st_store<TO>(o, iv == 0 ? g.rhor[ir] : (iv == 4 ? g.sr[ir] : 0.0));
       }
-      if (!isfinite(o)) bad = 1;
-      nx[q] = st_store<TO>(o, iv == 0 ? g.rhor[ir] : (iv == 4 ? g.sr[ir] : 0.0));
     }
   }
   if (bad && flag) atomicOr(flag, 1);
