@@ -280,6 +280,7 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     sim.set_stream(stream.cuda_stream)
     sim.upload(v0)
+    tiles = sim.autotune(reps=3)  # lines per CTA for r, theta, phi (no result changes)
     for _ in range(args.warmup):
         sim.step_rk4(dt, 1)
     torch.cuda.synchronize()
@@ -357,7 +358,7 @@ def run_ours(args):
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64" if args.precision == "fp64" else "f32-storage/f64", "data": "synthetic",
         "config": {"workload": args.workload, "grid": [p.nr, p.nth, p.nphi], "decomposition": [p.nnr, p.nnt, p.nnp],
-                   "precision": args.precision,
+                   "precision": args.precision, "tile_lines_r_theta_phi": list(tiles),
                    "fields": nv, "dt": dt, "l2": "state (%.0f MB per buffer) larger than L2, no flush" % (state_bytes / 1e6),
                    "parallelism": "replicas" if world > 1 else "single-gpu"},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
