@@ -911,14 +911,19 @@ __global__ void __launch_bounds__(128) k_curl_theta(CssGeo g, const TS *__restri
   const int bt = blockIdx.x / nchunk, pb = (blockIdx.x - bt * nchunk) * TL;
   const int ir = blockIdx.y;
   const CssDir &D = g.d[1];
-  const int t0 = D.start[bt], m = D.size[bt];
+  const int t0 = D.start[bt], m = MT ? MT : D.size[bt];
   const int dtype = dtype_of(D, bt);
   const int SR = m + 9, SO = m + 1;
   const size_t n = (size_t)g.ncell;
   double *H = sm;                      // 0: sin*A_phi, 1: A_r
   double *O = H + (size_t)2 * TL * SR;
-  load_theta_tile(g, a + n, H, SR, t0, m, pb, TL, ir, true);
-  load_theta_tile(g, a + 2 * n, H + (size_t)TL * SR, SR, t0, m, pb, TL, ir, true);
+  if constexpr (MT > 0 && TLC > 0) {
+    const TS *fs[2] = {a + n, a + 2 * n};
+    tiles_ct<2, MT, TLC, 1>(g, fs, H, (size_t)TL * SR, SR, t0, pb, ir);
+  } else {
+    load_theta_tile(g, a + n, H, SR, t0, m, pb, TL, ir, true);
+    load_theta_tile(g, a + 2 * n, H + (size_t)TL * SR, SR, t0, m, pb, TL, ir, true);
+  }
   __syncthreads();
   for (int idx = threadIdx.x; idx < TL * (m + 8); idx += blockDim.x) {
     int l = idx / (m + 8), jj = idx - l * (m + 8);
@@ -954,14 +959,19 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const TS *__restrict
   const int bp = blockIdx.x / nchunk, tb = (blockIdx.x - bp * nchunk) * TL;
   const int ir = blockIdx.y;
   const CssDir &D = g.d[2];
-  const int p0 = D.start[bp], m = D.size[bp];
+  const int p0 = D.start[bp], m = MT ? MT : D.size[bp];
   const int SR = TL + 1;
   const size_t n = (size_t)g.ncell;
   const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
   double *H = sm;  // 0: A_r, 1: A_theta
   double *O = H + 2 * HS;
-  load_phi_tile(g, a + 2 * n, H, SR, p0, m, tb, TL, ir, true);
-  load_phi_tile(g, a, H + HS, SR, p0, m, tb, TL, ir, true);
+  if constexpr (MT > 0 && TLC > 0) {
+    const TS *fs[2] = {a + 2 * n, a};
+    tiles_ct<2, MT, TLC, 2>(g, fs, H, HS, SR, p0, tb, ir);
+  } else {
+    load_phi_tile(g, a + 2 * n, H, SR, p0, m, tb, TL, ir, true);
+    load_phi_tile(g, a, H + HS, SR, p0, m, tb, TL, ir, true);
+  }
   __syncthreads();
   for (int task = threadIdx.x; task < 2 * TL; task += blockDim.x) {
     int k = task / TL, l = task - k * TL;
@@ -971,14 +981,26 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const TS *__restrict
   }
   __syncthreads();
   const double invr = g.r_inv[ir];
-  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
-    int j = pt / TL, l = pt - j * TL;
-    int it = tb + l, ip = p0 + j;
-    if (it >= g.nth) continue;
-    size_t id = css_idx(g, it, ip, ir);
-    double csc = g.csc[it];
-    out[id] = invr * O[(size_t)j * SR + l] * csc;
-    out[2 * n + id] = out[2 * n + id] - invr * O[OS + (size_t)j * SR + l] * csc;
+  // all of a thread's read-modify-write loads before its stores
+  constexpr int PPT = (MT > 0 && TLC > 0) ? (MT * TLC + NT - 1) / NT : 1;
+  const int stride = (MT > 0 && TLC > 0) ? NT : (int)blockDim.x;
+  for (int pt0 = threadIdx.x; pt0 < TL * m; pt0 += PPT * stride) {
+    double prev[PPT];
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      const int pt = pt0 + k * stride, j = pt / TL, l = pt - j * TL;
+      if (pt < TL * m && tb + l < g.nth) prev[k] = out[2 * n + css_idx(g, tb + l, p0 + j, ir)];
+    }
+#pragma unroll
+    for (int k = 0; k < PPT; k++) {
+      const int pt = pt0 + k * stride, j = pt / TL, l = pt - j * TL;
+      const int it = tb + l, ip = p0 + j;
+      if (pt >= TL * m || it >= g.nth) continue;
+      const size_t id = css_idx(g, it, ip, ir);
+      const double csc = g.csc[it];
+      out[id] = invr * O[(size_t)j * SR + l] * csc;
+      out[2 * n + id] = prev[k] - invr * O[OS + (size_t)j * SR + l] * csc;
+    }
   }
 }
 
@@ -990,15 +1012,20 @@ __global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const TS *__restrict__
   const int br = blockIdx.x / nchunk, tb = (blockIdx.x - br * nchunk) * TL;
   const int ip = blockIdx.y;
   const CssDir &D = g.d[0];
-  const int r0 = D.start[br], m = D.size[br];
+  const int r0 = D.start[br], m = MT ? MT : D.size[br];
   const int dtype = dtype_of(D, br);
   const int SR = TL + 1;
   const size_t n = (size_t)g.ncell;
   const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
   double *H = sm;  // 0: r*A_theta, 1: r*A_phi
   double *O = H + 2 * HS;
-  load_r_tile(g, a, H, SR, r0, m, tb, TL, ip, true);
-  load_r_tile(g, a + n, H + HS, SR, r0, m, tb, TL, ip, true);
+  if constexpr (MT > 0 && TLC > 0) {
+    const TS *fs[2] = {a, a + n};
+    tiles_ct<2, MT, TLC, 0>(g, fs, H, HS, SR, r0, tb, ip);
+  } else {
+    load_r_tile(g, a, H, SR, r0, m, tb, TL, ip, true);
+    load_r_tile(g, a + n, H + HS, SR, r0, m, tb, TL, ip, true);
+  }
   __syncthreads();
   for (int idx = threadIdx.x; idx < TL * (m + 8); idx += blockDim.x) {
     int jj = idx / TL, l = idx - jj * TL;
@@ -1016,18 +1043,34 @@ __global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const TS *__restrict__
                   D.dnum[br], D.dnum[br], 0, O + k * OS + l, SR);
   }
   __syncthreads();
-  for (int pt = threadIdx.x; pt < TL * m; pt += blockDim.x) {
+  constexpr int PPT = (MT > 0 && TLC > 0) ? (MT * TLC + NT - 1) / NT : 1;
+  const int stride = (MT > 0 && TLC > 0) ? NT : (int)blockDim.x;
+  for (int pt0 = threadIdx.x; pt0 < TL * m; pt0 += PPT * stride) {
+  double in_t[PPT], in_p[PPT], in_r[PPT];
+#pragma unroll
+  for (int k = 0; k < PPT; k++) {
+    const int pt = pt0 + k * stride, j = pt / TL, l = pt - j * TL;
+    if (pt < TL * m && tb + l < g.nth) {
+      const size_t id = css_idx(g, tb + l, ip, r0 + j);
+      in_t[k] = out[id];
+      in_p[k] = out[n + id];
+      in_r[k] = out[2 * n + id];
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < PPT; k++) {
+    const int pt = pt0 + k * stride;
     int j = pt / TL, l = pt - j * TL;
     int it = tb + l, ir = r0 + j;
-    if (it >= g.nth) continue;
+    if (pt >= TL * m || it >= g.nth) continue;
     size_t id = css_idx(g, it, ip, ir);
     double d = O[(size_t)j * SR + l];
     if (g.non_uniform) d = d * g.dxdr[ir];
-    double bp_ = out[n + id] + d * g.r_inv[ir];
+    double bp_ = in_p[k] + d * g.r_inv[ir];
     d = O[OS + (size_t)j * SR + l];
     if (g.non_uniform) d = d * g.dxdr[ir];
-    double bt_ = out[id] - d * g.r_inv[ir];
-    double br_ = out[2 * n + id];
+    double bt_ = in_t[k] - d * g.r_inv[ir];
+    double br_ = in_r[k];
     if (apply_bc) {
       if (it == 0 || it == g.nth - 1) {
         if (g.theta_perf_conductor) bt_ = 0.0;
@@ -1045,6 +1088,7 @@ __global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const TS *__restrict__
     }
     out[id] = bt_;
     out[n + id] = bp_;
+  }
   }
 }
 
