@@ -260,8 +260,7 @@ static int setup_kernels() {
   if (int rc = setup_mt<0, 0>()) return rc;
   CUDA_TRY(cudaFuncSetAttribute(k_sld<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<4>)));
   CUDA_TRY(cudaFuncSetAttribute(k_sld<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<5>)));
-  CUDA_TRY(cudaFuncSetAttribute(k_sld<7>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<7>)));
-  CUDA_TRY(cudaFuncSetAttribute(k_sld<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<8>)));
+  CUDA_TRY(cudaFuncSetAttribute(k_sld<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<3>)));
   if (int rc = setup_mt<16, 16>()) return rc;
   if (int rc = setup_mt<32, 16>()) return rc;
   if (int rc = setup_mt<16, 8>()) return rc;
@@ -707,11 +706,25 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
   if (int rc = check_launch(c)) return rc;
   prof_begin(c, KI_SLD);
   dim3 gs((g.nth + SLD_TT - 1) / SLD_TT, (g.nphi + SLD_TP - 1) / SLD_TP, (g.nr + SLD_RC - 1) / SLD_RC);
+  // the diffused fields are contiguous from varlist[0]; MHD runs them in two
+  // launches (the hydro fields, then A) so each carries a register window
+  // of at most five fields
+  const int off = g.varlist[0];
+  const unsigned all = (1u << g.nv) - 1u;
+  const int th = SLD_TT * SLD_TP;
   switch (g.nsld) {
-    case 4: k_sld<4><<<gs, SLD_TT * SLD_TP, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout); break;
-    case 5: k_sld<5><<<gs, SLD_TT * SLD_TP, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout); break;
-    case 7: k_sld<7><<<gs, SLD_TT * SLD_TP, sizeof(SldSmem<7>), c->stream>>>(g, v, av, c->vcc, dout); break;
-    default: k_sld<8><<<gs, SLD_TT * SLD_TP, sizeof(SldSmem<8>), c->stream>>>(g, v, av, c->vcc, dout); break;
+    case 4: k_sld<4><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, off, all); break;
+    case 5: k_sld<5><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, off, all); break;
+    case 7:  // fields 1..7: rho is not diffused (its tendency is zero)
+      k_sld<4><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, 1, 0x1Fu);
+      if (int rc = check_launch(c)) return rc;
+      k_sld<3><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 5, 0xE0u);
+      break;
+    default:  // fields 0..7
+      k_sld<5><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, 0, 0x1Fu);
+      if (int rc = check_launch(c)) return rc;
+      k_sld<3><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 5, 0xE0u);
+      break;
   }
   prof_end(c);
   if (int rc = check_launch(c)) return rc;

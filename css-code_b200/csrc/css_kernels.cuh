@@ -1294,7 +1294,7 @@ template <int NF>
 __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const double *__restrict__ v,
                                                             const double *__restrict__ av,
                                                             const double *__restrict__ vcc,
-                                                            double *__restrict__ dout) {
+                                                            double *__restrict__ dout, int off, unsigned wmask) {
   extern __shared__ double sm_raw[];
   SldSmem<NF> &S = *reinterpret_cast<SldSmem<NF> *>(sm_raw);
   auto &FT = S.FT;
@@ -1309,7 +1309,9 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
   const int it = t0 + tx, ip = p0 + ty;
   const bool live = it < nth && ip < nphi;
   const int itc = min(it, nth - 1), ipc = min(ip, nphi - 1);
-  const int off = g.varlist[0];  // the diffused fields are off, off+1, ..., contiguous
+  // this launch diffuses fields off .. off+NF-1 and writes the fields of
+  // wmask (a field it writes but does not diffuse gets zero)
+  const bool hydro_part = (wmask & 0x1Fu) != 0;  // the fields the corrections act on
   // per-field r window: x(ir-1), x(ir), x(ir+1), x(ir+2), and the de of the
   // lower r face of the current radius
   double win[NF][4], carry[NF];
@@ -1421,12 +1423,14 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     }
     // the velocities of this cell, taken from the tile when they are diffused
     // fields (before the barrier: the next radius's copies reuse the buffer)
-    double uu[4];
+    double uu[4] = {0.0, 0.0, 0.0, 0.0};
+    if (hydro_part)
 #pragma unroll
-    for (int k = 1; k <= 3; k++) {
-      const int f = k - off;
-      uu[k] = (f >= 0 && f < NF) ? X[f >= 0 && f < NF ? f : 0][ty + 2][tx + 2] : __ldg(v + k * n + css_idx(g, itc, ipc, ir));
-    }
+      for (int k = 1; k <= 3; k++) {
+        const int f = k - off;
+        uu[k] = (f >= 0 && f < NF) ? X[f >= 0 && f < NF ? f : 0][ty + 2][tx + 2]
+                                   : __ldg(v + k * n + css_idx(g, itc, ipc, ir));
+      }
     __syncthreads();
     double Dv[NF];
 #pragma unroll
@@ -1464,21 +1468,23 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
       int f = k - off;
       D[k] = (f >= 0 && f < NF) ? Dv[f >= 0 && f < NF ? f : 0] : 0.0;
     }
-    double rho = __ldg(v + id);
-    double invrho = 1.0 / rho;
-    // 1/T = rho^(1-gamma) exp(-s/Cv) / invtconst, as one exponential
-    double itemp = exp(-fma(g.gamm1, log(rho), __ldg(v + 4 * n + id) * g.invcv)) / g.invtconst;
-    if (g.do_viscous_heating)
+    if (hydro_part) {
+      double rho = __ldg(v + id);
+      double invrho = 1.0 / rho;
+      // 1/T = rho^(1-gamma) exp(-s/Cv) / invtconst, as one exponential
+      double itemp = exp(-fma(g.gamm1, log(rho), __ldg(v + 4 * n + id) * g.invcv)) / g.invtconst;
+      if (g.do_viscous_heating)
 #pragma unroll
-      for (int k = 1; k <= 3; k++) D[4] = D[4] - uu[k] * D[k] * itemp;
-    if (g.mass_diffusion) {
+        for (int k = 1; k <= 3; k++) D[4] = D[4] - uu[k] * D[k] * itemp;
+      if (g.mass_diffusion) {
 #pragma unroll
-      for (int k = 1; k <= 3; k++) D[k] = D[k] - invrho * uu[k] * D[0];
-      D[4] = D[4] - (g.gamm1 * g.cv) * invrho * D[0];
+        for (int k = 1; k <= 3; k++) D[k] = D[k] - invrho * uu[k] * D[0];
+        D[4] = D[4] - (g.gamm1 * g.cv) * invrho * D[0];
+      }
     }
 #pragma unroll
     for (int k = 0; k < 8; k++)
-      if (k < g.nv) dout[k * n + id] = D[k];
+      if (k < g.nv && ((wmask >> k) & 1u)) dout[k * n + id] = D[k];
   }
 }
 
