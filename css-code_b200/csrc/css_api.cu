@@ -63,6 +63,8 @@ struct css_ctx {
   int *flag;
   long long launches;
   int tl_theta, tl_phi, tl_r;
+  int phi_pers = 0;                 // 1: persistent double-buffered phi kernel (autotuned)
+  int nsm = 148;                    // SMs of the device
   cudaStream_t own_stream;
   // per-kernel event timing (css_profile)
   int profiling;
@@ -250,6 +252,7 @@ static int setup_mt() {
   CSS_SMEM_ATTR(k_curl_phi<MT, TLC, float>);
   CSS_SMEM_ATTR(k_curl_r<MT, TLC, double>);
   CSS_SMEM_ATTR(k_curl_r<MT, TLC, float>);
+  if constexpr (MT > 0 && TLC > 0) CSS_SMEM_ATTR(k_phi_terms_p<MT, TLC>);
 #undef CSS_SMEM_ATTR
   return CSS_OK;
 }
@@ -603,6 +606,12 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     css_destroy(c);
     return CSS_ERR_CUDA;
   }
+  {
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && nsm > 0)
+      c->nsm = nsm;
+  }
   int mag = p.magnetic;
   for (int d = 0; d < 3; d++) {
     int m0 = g.d[d].size[0], same = 1;
@@ -660,6 +669,20 @@ static int launch_curl(css_ctx *c, const TS *a, double *out, int apply_bc) {
 }
 
 // RHS of one stage on `cur`; if stage > 0 also the stage update into `nx`
+// the persistent phi kernel: as many CTAs as fit on the device at once
+template <int MT, int TLC>
+static void launch_phi_p(css_ctx *c, const double *cur) {
+  const CssGeo &g = c->g;
+  const int mag = g.magnetic, nh = mag ? 7 : 5, nd = mag ? 8 : 6, SR = TLC + 1;
+  const size_t HS = (size_t)(MT + 8) * SR, OS = (size_t)MT * SR;
+  const size_t smem = 8 * (2 * (size_t)nh * HS + (size_t)nd * OS + 2 * 3 * (MT + 2));
+  int per_sm = 1;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_phi_terms_p<MT, TLC>, 128, smem);
+  const long long ntile = (long long)g.d[2].nb * ((g.nth + TLC - 1) / TLC) * g.nr;
+  const int grid = (int)std::min<long long>(ntile, (long long)std::max(per_sm, 1) * c->nsm);
+  k_phi_terms_p<MT, TLC><<<grid, 128, smem, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf);
+}
+
 // stage input of storage type TS, next stage state of storage type TO
 template <typename TS, typename TO>
 static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur) {
@@ -677,7 +700,21 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   TL = c->tl_phi;
   dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
   prof_begin(c, KI_PHI);
-  LAUNCH_MT(2, TL, k_phi_terms, (TS), gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  bool pers = false;
+  if constexpr (sizeof(TS) == 8) {
+    if (c->phi_pers) {
+      pers = true;
+      switch (c->mt[2] * 100 + TL) {
+        case 1616: launch_phi_p<16, 16>(c, cur); break;
+        case 3216: launch_phi_p<32, 16>(c, cur); break;
+        case 1608: launch_phi_p<16, 8>(c, cur); break;
+        case 3208: launch_phi_p<32, 8>(c, cur); break;
+        default: pers = false;
+      }
+    }
+  }
+  if (!pers)
+    LAUNCH_MT(2, TL, k_phi_terms, (TS), gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_r;
@@ -1027,10 +1064,17 @@ extern "C" int css_autotune(css_ctx *c, int reps, int *chosen) {
                              : (d == 2 ? smem_phi_terms(mag, m, t) : smem_radial_terms(mag, m, t));
         if (need <= kSmemCap) cand.push_back(t);
       }
-    int best = *tl[d];
+    int best = *tl[d], best_pers = c->phi_pers;
     float best_ms = 1e30f;
+    std::vector<std::pair<int, int>> variants;  // (tile height, persistent phi kernel)
     for (int t : cand) {
+      variants.push_back({t, 0});
+      if (d == 2 && c->mt[d]) variants.push_back({t, 1});
+    }
+    for (auto tv : variants) {
+      const int t = tv.first;
       *tl[d] = t;
+      if (d == 2) c->phi_pers = tv.second;
       if ((rc = launch_rhs(c, (const double *)c->v0, (double *)nullptr, 0, 0.0))) break;  // warm
       cudaEventRecord(e0, c->stream);
       for (int k = 0; k < reps && rc == CSS_OK; k++) rc = launch_rhs(c, (const double *)c->v0, (double *)nullptr, 0, 0.0);
@@ -1039,15 +1083,38 @@ extern "C" int css_autotune(css_ctx *c, int reps, int *chosen) {
       if (cudaEventSynchronize(e1) != cudaSuccess) { set_err("css_autotune: timing failed"); rc = CSS_ERR_CUDA; break; }
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best_ms) { best_ms = ms; best = t; }
+      if (ms < best_ms) { best_ms = ms; best = t; best_pers = c->phi_pers; }
     }
     *tl[d] = best;
+    if (d == 2) c->phi_pers = best_pers;
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
   c->profiling = prof_was;
   if (chosen) { chosen[0] = c->tl_r; chosen[1] = c->tl_theta; chosen[2] = c->tl_phi; }
   return rc;
+}
+
+// the autotuner's choices set by hand: tile heights (lines per CTA) of the
+// r, theta and phi kernels and the persistent phi kernel (0/1); a height a
+// direction does not offer is refused
+extern "C" int css_set_tiles(css_ctx *c, int tl_r, int tl_theta, int tl_phi, int phi_persistent) {
+  if (!c) { set_err("css_set_tiles: NULL"); return CSS_ERR_ARG; }
+  const int tl[3] = {tl_r, tl_theta, tl_phi};
+  const int mag = c->g.magnetic;
+  for (int d = 0; d < 3; d++) {
+    const int t = tl[d], m = c->g.d[d].maxm;
+    bool ok = c->mt[d] ? (t == 8 || t == 16) : (t == 4 || t == 8 || t == 16);
+    if (ok && !c->mt[d]) {
+      size_t need = d == 1 ? std::max(smem_theta_terms(mag, m, t), smem_rhot(m, t))
+                           : (d == 2 ? smem_phi_terms(mag, m, t) : smem_radial_terms(mag, m, t));
+      ok = need <= kSmemCap;
+    }
+    if (!ok) { set_err("css_set_tiles: %d lines per CTA not available in direction %d", t, d); return CSS_ERR_ARG; }
+  }
+  if (phi_persistent && !c->mt[2]) { set_err("css_set_tiles: the persistent phi kernel needs 16- or 32-point blocks"); return CSS_ERR_ARG; }
+  c->tl_r = tl_r; c->tl_theta = tl_theta; c->tl_phi = tl_phi; c->phi_pers = phi_persistent ? 1 : 0;
+  return CSS_OK;
 }
 
 // ---------------------------------------------------------------------------

@@ -67,6 +67,19 @@ __device__ __forceinline__ TO st_store(double x, double mean) {
   else return x;
 }
 
+// asynchronous global -> shared copies (completion tracked per commit group)
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
 // ---------------------------------------------------------------------------
 // tile loaders
 // ---------------------------------------------------------------------------
@@ -396,36 +409,19 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const TV *__restr
 // Phi_Terms (rhs_mpi.f90:1032-1261).  grid: x = phi block * nchunk + theta
 // chunk, y = r.
 // ---------------------------------------------------------------------------
-template <int MT, int TLC, typename TV>
-__global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restrict__ cur,
-                                                   const double *__restrict__ bf, double *__restrict__ dv,
-                                                   const double *__restrict__ tbuf, int TLrt) {
-  extern __shared__ double sm[];
-  const int TL = TLC ? TLC : TLrt;
-  const int nchunk = (g.nth + TL - 1) / TL;
-  const int bp = blockIdx.x / nchunk, tb = (blockIdx.x - bp * nchunk) * TL;
-  const int ir = blockIdx.y;
+// tables, line solves and pointwise physics of one phi tile whose fields are
+// in H (shared by the one-tile-per-CTA kernel and the persistent one)
+template <int MT, int TLC>
+__device__ __forceinline__ void phi_tile_compute(const CssGeo &g, const double *__restrict__ bf,
+                                                 double *__restrict__ dv, const double *__restrict__ tbuf, int TL,
+                                                 int bp, int tb, int ir, double *H, double *O, double *Tb) {
   const CssDir &D = g.d[2];
   const int p0 = D.start[bp], m = MT ? MT : D.size[bp];
   const int mag = g.magnetic;
   const int SR = TL + 1, TS = 3 * (m + 2);
   const size_t n = (size_t)g.ncell;
-  const int nh = mag ? 7 : 5;  // rho v w u s [bt br]
-  const int nd = mag ? 8 : 6;  // drho dv dw du ds d2s [dbt dbr]
+  const int nd = mag ? 8 : 6;
   const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
-  double *H = sm;
-  double *O = H + nh * HS;
-  double *Tb = O + nd * OS;
-  const TV *fs[5] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n};
-  const double *ms[5] = {g.rhor, nullptr, nullptr, nullptr, g.sr};
-  const double *fb[2] = {bf, bf + 2 * n};
-  if constexpr (MT > 0 && TLC > 0) {
-    tiles_ct<5, MT, TLC, 2>(g, fs, H, HS, SR, p0, tb, ir, ms);
-    if (mag) tiles_ct<2, MT, TLC, 2>(g, fb, H + 5 * HS, HS, SR, p0, tb, ir);
-  } else {
-    for (int k = 0; k < 5; k++) tile_phi<MT, TLC>(g, fs[k], H + k * HS, SR, p0, m, tb, TL, ir, ms[k]);
-    for (int k = 5; k < nh; k++) tile_phi<MT, TLC>(g, fb[k - 5], H + k * HS, SR, p0, m, tb, TL, ir);
-  }
   stage_table(g, 2, bp, 1, 0, m, Tb);
   stage_table(g, 2, bp, 2, 0, m, Tb + TS);
   __syncthreads();
@@ -517,6 +513,103 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restric
       }
     }
   }
+}
+
+template <int MT, int TLC, typename TV>
+__global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restrict__ cur,
+                                                   const double *__restrict__ bf, double *__restrict__ dv,
+                                                   const double *__restrict__ tbuf, int TLrt) {
+  extern __shared__ double sm[];
+  const int TL = TLC ? TLC : TLrt;
+  const int nchunk = (g.nth + TL - 1) / TL;
+  const int bp = blockIdx.x / nchunk, tb = (blockIdx.x - bp * nchunk) * TL;
+  const int ir = blockIdx.y;
+  const CssDir &D = g.d[2];
+  const int p0 = D.start[bp], m = MT ? MT : D.size[bp];
+  const int mag = g.magnetic;
+  const int SR = TL + 1;
+  const size_t n = (size_t)g.ncell;
+  const int nh = mag ? 7 : 5;  // rho v w u s [bt br]
+  const int nd = mag ? 8 : 6;  // drho dv dw du ds d2s [dbt dbr]
+  const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
+  double *H = sm;
+  double *O = H + nh * HS;
+  double *Tb = O + nd * OS;
+  const TV *fs[5] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n};
+  const double *ms[5] = {g.rhor, nullptr, nullptr, nullptr, g.sr};
+  const double *fb[2] = {bf, bf + 2 * n};
+  if constexpr (MT > 0 && TLC > 0) {
+    tiles_ct<5, MT, TLC, 2>(g, fs, H, HS, SR, p0, tb, ir, ms);
+    if (mag) tiles_ct<2, MT, TLC, 2>(g, fb, H + 5 * HS, HS, SR, p0, tb, ir);
+  } else {
+    for (int k = 0; k < 5; k++) tile_phi<MT, TLC>(g, fs[k], H + k * HS, SR, p0, m, tb, TL, ir, ms[k]);
+    for (int k = 5; k < nh; k++) tile_phi<MT, TLC>(g, fb[k - 5], H + k * HS, SR, p0, m, tb, TL, ir);
+  }
+  phi_tile_compute<MT, TLC>(g, bf, dv, tbuf, TL, bp, tb, ir, H, O, Tb);
+}
+
+// Phi_Terms as a persistent kernel (FP64 stage input, compile-time block
+// length and tile height): each CTA walks tiles t = blockIdx.x,
+// blockIdx.x + gridDim.x, ... in the (r, phi block, theta chunk) order of
+// k_phi_terms; the next tile's fields stream into the second of two
+// shared-memory buffers with asynchronous 8-byte copies (zero fill past
+// nth, periodic phi) while the current tile is solved and its physics done.
+template <int NF, int MT, int TLC>
+__device__ __forceinline__ void phi_tile_issue(const CssGeo &g, const double *const *f, double *S, size_t FS,
+                                               int SR, int p0, int tb, int ir) {
+  constexpr int W = MT + 8, N = TLC * W;
+  const size_t pl = plane(g, ir);
+  for (int idx = threadIdx.x; idx < N; idx += NT) {
+    const int jj = idx / TLC, l = idx - jj * TLC;
+    int gp = p0 + jj - 4;
+    if (gp < 0) gp += g.nphi;
+    else if (gp >= g.nphi) gp -= g.nphi;
+    const int gt = tb + l;
+    const bool in = gt < g.nth;
+    const size_t off = pl + (size_t)gp * g.nth + (in ? gt : 0);
+#pragma unroll
+    for (int q = 0; q < NF; q++) cp_async8(S + q * FS + (size_t)jj * SR + l, f[q] + off, in ? 8 : 0);
+  }
+}
+
+template <int MT, int TLC>
+__global__ void __launch_bounds__(128) k_phi_terms_p(CssGeo g, const double *__restrict__ cur,
+                                                     const double *__restrict__ bf, double *__restrict__ dv,
+                                                     const double *__restrict__ tbuf) {
+  static_assert(MT > 0 && TLC > 0, "persistent phi kernel needs compile-time sizes");
+  extern __shared__ double sm[];
+  constexpr int TL = TLC, m = MT, SR = TLC + 1;
+  const int nchunk = (g.nth + TL - 1) / TL, nbp = g.d[2].nb;
+  const long long per_r = (long long)nbp * nchunk, ntile = per_r * g.nr;
+  const int mag = g.magnetic;
+  const int nh = mag ? 7 : 5, nd = mag ? 8 : 6;
+  const size_t n = (size_t)g.ncell;
+  const size_t HS = (size_t)(m + 8) * SR, OS = (size_t)m * SR;
+  double *Hb[2] = {sm, sm + (size_t)nh * HS};
+  double *O = sm + (size_t)2 * nh * HS;
+  double *Tb = O + (size_t)nd * OS;
+  const double *fs[5] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n};
+  const double *fb[2] = {bf, bf + 2 * n};
+  auto issue = [&](long long t, double *H) {
+    const int ir = (int)(t / per_r), x = (int)(t - (long long)ir * per_r);
+    const int bp = x / nchunk, tb = (x - bp * nchunk) * TL;
+    const int p0 = g.d[2].start[bp];
+    phi_tile_issue<5, MT, TLC>(g, fs, H, HS, SR, p0, tb, ir);
+    if (mag) phi_tile_issue<2, MT, TLC>(g, fb, H + 5 * HS, HS, SR, p0, tb, ir);
+    cp_async_commit();
+  };
+  long long t = blockIdx.x;
+  if (t < ntile) issue(t, Hb[0]);
+  for (int it = 0; t < ntile; it++, t += gridDim.x) {
+    double *H = Hb[it & 1];
+    cp_async_wait<0>();
+    __syncthreads();  // tile t is in H; the previous tile's readers are done
+    if (t + gridDim.x < ntile) issue(t + gridDim.x, Hb[(it + 1) & 1]);
+    const int ir = (int)(t / per_r), x = (int)(t - (long long)ir * per_r);
+    const int bp = x / nchunk, tb = (x - bp * nchunk) * TL;
+    phi_tile_compute<MT, TLC>(g, bf, dv, tbuf, TL, bp, tb, ir, H, O, Tb);
+  }
+  cp_async_wait<0>();
 }
 
 // pointwise Radial_Terms (rhs_mpi.f90:1302-1517) for one point: updates
@@ -1242,18 +1335,6 @@ struct SldSmem {
   double SP[SLD_TP + 1][SLD_TT];          // phi face speed
 };
 
-// asynchronous global -> shared copies (completion tracked per commit group)
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem, int src_bytes) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_bytes) {
-  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // Starts the copies of radius ir's planes (every diffused field with a
 // 2-point halo, raw values; the speed plane with a 1-point halo, theta

@@ -106,6 +106,10 @@ class Simulation:
         check(_lib.lib().css_autotune(self.h, int(reps), ch))
         return tuple(ch)
 
+    def set_tiles(self, tl_r, tl_theta, tl_phi, phi_persistent=False):
+        """The autotuner's choices by hand (css_set_tiles)."""
+        check(_lib.lib().css_set_tiles(self.h, int(tl_r), int(tl_theta), int(tl_phi), 1 if phi_persistent else 0))
+
     # diagnostics of the current state ----------------------------------------
     SCALAR_NAMES = ("kinener", "cke", "mcke", "drke", "umach", "magener", "bmax")
     STEP_SIZE_NAMES = ("dtmax", "Etot", "Ltot", "mtot", "mrsint")

@@ -235,6 +235,11 @@ int css_kernel_stats(css_ctx *ctx, int kind, const char **name, double *total_ms
  * This has no counterpart in the reference (its per-rank loops have fixed
  * extents).                                                                */
 int css_autotune(css_ctx *ctx, int reps, int *chosen);
+/* The same choices made by hand: lines per CTA of the r, theta and phi
+ * kernels (8 or 16 for 16/32-point blocks; 4, 8 or 16 otherwise) and 1 to
+ * run Phi_Terms as a persistent kernel that streams the next tile into
+ * shared memory while the current one is computed.                         */
+int css_set_tiles(css_ctx *ctx, int tl_r, int tl_theta, int tl_phi, int phi_persistent);
 
 /* A batched ensemble of independent runs (many small shells, each with its
  * own grid, decomposition and parameters: hydro and MHD members may mix).

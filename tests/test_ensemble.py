@@ -157,3 +157,23 @@ def test_autotune_changes_no_result_bit(gpu_available, spec):
     assert np.array_equal(b.download(), v0)  # autotuning leaves the state alone
     b.step_rk4(dt, 2)
     assert np.array_equal(a.download(), b.download())
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("spec", [SMALL[1], SMALL[2]])
+def test_every_tile_variant_gives_the_same_bits(gpu_available, spec):
+    from css_b200.context import Simulation
+    p, prof, v0, dt = E.build_member(spec, seed=13)
+    ref = Simulation(p, prof)
+    ref.upload(v0)
+    ref.step_rk4(dt, 2)
+    want = ref.download()
+    mt_phi = spec["nphi"] // spec["decomp"][2] in (16, 32)
+    for tl in (8, 16):
+        for pers in ((False, True) if mt_phi else (False,)):
+            sim = Simulation(p, prof)
+            sim.set_tiles(tl, tl, tl, pers)
+            sim.upload(v0)
+            sim.step_rk4(dt, 2)
+            assert np.array_equal(sim.download(), want), (tl, pers)
+            sim.close()
