@@ -12,6 +12,7 @@
 #include <cstring>
 #include <string>
 #include <vector>
+#include <sys/stat.h>
 
 #include "../../include/css_b200.h"
 #include "css_kernels.cuh"
@@ -1827,6 +1828,101 @@ extern "C" int css_mlp_grads(css_mlp *m, int l, float *gw, float *gb) {
   CUDA_TRY(cudaStreamSynchronize(m->st));
   if (gw) CUDA_TRY(cudaMemcpy(gw, m->gW[l], K * M * 4, cudaMemcpyDeviceToHost));
   if (gb) CUDA_TRY(cudaMemcpy(gb, m->gB[l], M * 4, cudaMemcpyDeviceToHost));
+  return CSS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Checkpoints in the reference's layout (Checkpoint_Output / Checkpoint_Input,
+// checkpoint.f90:146-423): a directory holding a text `header` -- line 1
+// nr, nth, nphi, nv, istep as (5i9), line 2 deltat, sim_time, r1, r2, th1,
+// th2, phi1, phi2 as (8e14.7) -- and one file `checkpoint.<name>` per field
+// (rho w v u s bt bp br; for MHD the last three hold the vector potential,
+// as vars0 does) with the raw FP64 array (nth, nphi, nr) in Fortran order,
+// which is the library's own layout of a field.
+// ---------------------------------------------------------------------------
+static const char *kCkptNames[8] = {"rho", "w", "v", "u", "s", "bt", "bp", "br"};
+
+// Fortran E14.7: [-]0.dddddddE+xx right-justified in 14 columns
+static void fortran_e14_7(double x, char *out) {
+  char m[64];
+  if (x == 0.0 || !std::isfinite(x)) {
+    if (x == 0.0) snprintf(out, 15, "%14s", std::signbit(x) ? "-0.0000000E+00" : "0.0000000E+00");
+    else snprintf(out, 15, "%14s", std::isnan(x) ? "NaN" : (x > 0 ? "Infinity" : "-Infinity"));
+    return;
+  }
+  snprintf(m, sizeof m, "%.6E", fabs(x));  // d.ddddddE+xx: the 7 significant digits
+  const int e10 = atoi(m + 9) + 1;           // exponent of the 0.d form
+  char digits[8] = {m[0], m[2], m[3], m[4], m[5], m[6], m[7], 0};
+  char buf[32];
+  if (e10 > 99 || e10 < -99) snprintf(buf, sizeof buf, "%s0.%s%+04d", x < 0 ? "-" : "", digits, e10);
+  else snprintf(buf, sizeof buf, "%s0.%sE%+03d", x < 0 ? "-" : "", digits, e10);
+  size_t len = strlen(buf);  // at most 14: -0.dddddddE+xx or -0.ddddddd+xxx
+  if (len > 14) len = 14;
+  memset(out, ' ', 14 - len);
+  memcpy(out + 14 - len, buf, len);
+  out[14] = 0;
+}
+
+extern "C" int css_checkpoint_write(css_ctx *c, const char *dir, int istep, double deltat, double sim_time) {
+  if (!c || !dir) { set_err("css_checkpoint_write: NULL argument"); return CSS_ERR_ARG; }
+  mkdir(dir, 0755);  // as Make_Checkpoint_Filename; an existing directory is fine
+  std::string d(dir);
+  if (d.empty() || d.back() != '/') d += '/';
+  const css_params &p = c->p;
+  FILE *f = fopen((d + "header").c_str(), "w");
+  if (!f) { set_err("css_checkpoint_write: cannot create %sheader", d.c_str()); return CSS_ERR_ARG; }
+  fprintf(f, "%9d%9d%9d%9d%9d\n", p.nr, p.nth, p.nphi, c->nv, istep);
+  const double h2[8] = {deltat, sim_time, p.r1, p.r2, p.th1, p.th2, p.phi1, p.phi2};
+  for (int k = 0; k < 8; k++) {
+    char e[16];
+    fortran_e14_7(h2[k], e);
+    fputs(e, f);
+  }
+  fputs("\n", f);
+  fclose(f);
+  std::vector<double> h((size_t)c->nv * c->ncell);
+  if (int rc = css_download_state(c, h.data())) return rc;
+  for (int iv = 0; iv < c->nv; iv++) {
+    FILE *g = fopen((d + "checkpoint." + kCkptNames[iv]).c_str(), "wb");
+    if (!g) { set_err("css_checkpoint_write: cannot create %scheckpoint.%s", d.c_str(), kCkptNames[iv]); return CSS_ERR_ARG; }
+    const size_t w = fwrite(h.data() + (size_t)iv * c->ncell, 8, c->ncell, g);
+    fclose(g);
+    if (w != c->ncell) { set_err("css_checkpoint_write: short write of checkpoint.%s", kCkptNames[iv]); return CSS_ERR_ARG; }
+  }
+  return CSS_OK;
+}
+
+extern "C" int css_checkpoint_read(css_ctx *c, const char *dir, int *istep, double *deltat, double *sim_time) {
+  if (!c || !dir) { set_err("css_checkpoint_read: NULL argument"); return CSS_ERR_ARG; }
+  std::string d(dir);
+  if (d.empty() || d.back() != '/') d += '/';
+  FILE *f = fopen((d + "header").c_str(), "r");
+  if (!f) { set_err("css_checkpoint_read: cannot open %sheader", d.c_str()); return CSS_ERR_ARG; }
+  int nr = 0, nth = 0, nphi = 0, nv = 0, step = 0;
+  double h2[8] = {0};
+  int got = fscanf(f, "%d %d %d %d %d", &nr, &nth, &nphi, &nv, &step);
+  for (int k = 0; k < 8 && got == 5 + k; k++) got += fscanf(f, "%lf", &h2[k]);
+  fclose(f);
+  if (got != 13) { set_err("css_checkpoint_read: malformed header in %s", d.c_str()); return CSS_ERR_ARG; }
+  if (nr != c->p.nr || nth != c->p.nth || nphi != c->p.nphi) {
+    // the reference interpolates horizontally (Checkpoint_Interpolate); not here
+    set_err("css_checkpoint_read: checkpoint is %dx%dx%d, the run %dx%dx%d", nr, nth, nphi, c->p.nr, c->p.nth,
+            c->p.nphi);
+    return CSS_ERR_ARG;
+  }
+  std::vector<double> h((size_t)c->nv * c->ncell);
+  if (int rc = css_download_state(c, h.data())) return rc;  // fields the file lacks keep their values
+  for (int iv = 0; iv < std::min(c->nv, nv); iv++) {
+    FILE *g = fopen((d + "checkpoint." + kCkptNames[iv]).c_str(), "rb");
+    if (!g) { set_err("css_checkpoint_read: cannot open %scheckpoint.%s", d.c_str(), kCkptNames[iv]); return CSS_ERR_ARG; }
+    const size_t r = fread(h.data() + (size_t)iv * c->ncell, 8, c->ncell, g);
+    fclose(g);
+    if (r != c->ncell) { set_err("css_checkpoint_read: checkpoint.%s is short", kCkptNames[iv]); return CSS_ERR_ARG; }
+  }
+  if (int rc = css_upload_state(c, h.data())) return rc;
+  if (istep) *istep = step;
+  if (deltat) *deltat = h2[0];
+  if (sim_time) *sim_time = h2[1];
   return CSS_OK;
 }
 

@@ -57,6 +57,10 @@ def lib():
         L.css_shell_averages.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.c_int, dp, dp]
         L.css_spectrum.argtypes = [ctypes.c_void_p, ctypes.c_int, dp]
         L.css_autotune.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.css_checkpoint_write.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_int, ctypes.c_double,
+                                           ctypes.c_double]
+        L.css_checkpoint_read.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.POINTER(ctypes.c_int),
+                                          ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.css_set_tiles.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.css_ensemble_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.POINTER(ctypes.c_void_p)]
@@ -99,7 +103,7 @@ def check(rc):
 EXPORTS = [
     "css_last_error", "css_create", "css_destroy", "css_upload_state", "css_download_state", "css_step_rk4",
     "css_step_rk4_host", "css_rhs", "css_diffusion", "css_deriv", "css_deriv_dev", "css_dbyd1_dt0",
-    "css_compact_lines", "css_sync", "css_state_device_ptr", "css_kernel_launches", "css_set_stream",
+    "css_compact_lines", "css_checkpoint_write", "css_checkpoint_read", "css_sync", "css_state_device_ptr", "css_kernel_launches", "css_set_stream",
     "css_profile", "css_kernel_stats", "css_compact_lines_noalloc", "css_scalars", "css_step_size",
     "css_shell_averages", "css_spectrum", "css_autotune", "css_set_tiles", "css_ensemble_create", "css_ensemble_step",
     "css_ensemble_launches", "css_ensemble_last_ms", "css_ensemble_destroy", "css_set_sld_speed2", "css_box_filter",

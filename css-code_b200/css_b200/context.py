@@ -65,6 +65,19 @@ class Simulation:
         check(_lib.lib().css_step_rk4_host(self.h, _p(v), float(dt), int(nsteps)))
         return v
 
+    def checkpoint_write(self, directory, istep, deltat, sim_time):
+        """Write the resident state as a reference-layout checkpoint."""
+        check(_lib.lib().css_checkpoint_write(self.h, str(directory).encode(), int(istep), float(deltat),
+                                              float(sim_time)))
+
+    def checkpoint_read(self, directory):
+        """Replace the state from a reference-layout checkpoint; returns
+        (istep, deltat, sim_time)."""
+        st, dt, t = ctypes.c_int(), ctypes.c_double(), ctypes.c_double()
+        check(_lib.lib().css_checkpoint_read(self.h, str(directory).encode(), ctypes.byref(st), ctypes.byref(dt),
+                                             ctypes.byref(t)))
+        return st.value, dt.value, t.value
+
     def sync(self):
         check(_lib.lib().css_sync(self.h))
 

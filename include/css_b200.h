@@ -200,6 +200,21 @@ int css_compact_lines_noalloc(const double *x, double *dx, int n, int nlines,
                               const double *halo_lo, const double *halo_hi,
                               double dnum, double scale, void *stream);
 
+/* Checkpoints in the reference's layout (Checkpoint_Output / Checkpoint_Input,
+ * checkpoint.f90:146-423): directory `dir` (created if missing) holds a
+ * text `header` -- nr nth nphi nv istep as (5i9), then deltat sim_time r1
+ * r2 th1 th2 phi1 phi2 as (8e14.7), so deltat is kept to 7 significant
+ * digits as the reference keeps it -- and `checkpoint.rho`, `.w`, `.v`,
+ * `.u`, `.s` (+ `.bt`, `.bp`, `.br`: the vector potential of an MHD run)
+ * with the raw FP64 field in Fortran (nth, nphi, nr) order.  Reading needs
+ * the same grid (the reference's horizontal interpolation is not
+ * provided: CSS_ERR_ARG) and reads min(nv, nv of the file) fields, as the
+ * reference does; the state of the context is replaced.                   */
+int css_checkpoint_write(css_ctx *ctx, const char *dir, int istep,
+                         double deltat, double sim_time);
+int css_checkpoint_read(css_ctx *ctx, const char *dir, int *istep,
+                        double *deltat, double *sim_time);
+
 /* Block until all work on the context stream is done. */
 int css_sync(css_ctx *ctx);
 
