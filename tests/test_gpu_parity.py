@@ -178,3 +178,30 @@ def test_nan_is_reported(cfg1, sims):
     with pytest.raises(CssError) as e:
         sim.step_host(v, dt, 1)
     assert e.value.code == 4
+
+
+@pytest.mark.parametrize("dims,decomp", [((24, 512, 48), (2, 2, 4)), ((24, 32, 768), (2, 2, 3))])
+def test_maximum_block_length_parity(dims, decomp, gpu_available):
+    """256-point blocks (the reference's LOOP COUNT MAX of the line loops,
+    the largest block the library accepts) in theta and in phi: the generic
+    (run-time length) kernels, against the oracle."""
+    p, prof, v0, dt, _ = problem.build(dims, decomp=decomp)
+    sim, orc = Simulation(p, prof), O.Oracle(p, prof)
+    rng = np.random.default_rng(21)
+    v = v0.copy()
+    v[1:4] = 1e-2 * rng.standard_normal(v[1:4].shape)
+    _, dg = sim.rhs(v, 1)
+    _, do = orc.rhs(v, 1)
+    assert max(fieldwise(dg, do)) < 1e-12, fieldwise(dg, do)
+    _, dg = sim.diffusion(v)
+    _, do = orc.diffusion(v)
+    assert max(fieldwise(dg, do)) < 1e-12, fieldwise(dg, do)
+    g = sim.step_host(v, dt, 2)
+    o = orc.step(v, dt, 2)
+    assert max(fieldwise(g, o)) < 1e-11, fieldwise(g, o)
+
+
+def test_empty_line_batches(gpu_available):
+    x = np.zeros((0, 40))
+    assert compact_lines(x, 1, True, True, 1).shape == (0, 40)
+    assert dbyd1_dt0(x, np.zeros(0), np.zeros(0), 1).shape == (0, 40)
