@@ -1323,7 +1323,7 @@ __device__ __forceinline__ double sld_ghost_t(const CssGeo &g, int iv, double q0
 // (diffusion.f90:375-428) per cell.  NF = number of diffused fields.
 #define SLD_TT 32
 #define SLD_TP 8
-#define SLD_RC 16
+#define SLD_RC 32
 #define SLD_XW (SLD_TT + 4)  // plane row: 36 doubles = 288 B, so 16-byte copies stay aligned
 template <int NF>
 struct SldSmem {
