@@ -1453,7 +1453,7 @@ extern "C" int css_spectrum(css_ctx *c, int kind, double *out) {
 // ---------------------------------------------------------------------------
 // Learned subgrid closure.  A fine state is box-filtered into coarse fields
 // and the twelve subgrid targets; 3x3x3 stencil features of the coarse
-// fields feed an MLP (in 135 -> 128 -> 128 -> 128 -> 12, GELU, BF16 weights
+// fields feed an MLP (in 135 -> 128 -> 128 -> 128 -> 12, GELU (tanh form), BF16 weights
 // and activations, FP32 accumulation) whose matrix products run on the
 // tensor cores through cuBLASLt; its predicted subgrid velocity variance
 // becomes the per-cell SLD speed^2 of a coarse run, in place of the

@@ -145,10 +145,24 @@ __global__ void k_closure_targets(const double *__restrict__ T, size_t nc, const
       Tn[c * CL_YPAD + k] = k < CL_NTARGET ? (float)(T[k * nc + c] / (double)tscale[k]) : 0.0f;
 }
 
-// exact GELU and its derivative: x Phi(x), Phi(x) + x phi(x)
-__device__ __forceinline__ float gelu_f(float x) { return 0.5f * x * (1.0f + erff(x * 0.70710678118654752f)); }
+// GELU in its tanh form (Hendrycks & Gimpel): 0.5 x (1 + tanh(u)),
+// u = sqrt(2/pi) (x + 0.044715 x^3), with the hardware tanh approximation
+// (relative error about 2^-11, below the BF16 rounding of the activations);
+// the derivative is 0.5 (1 + t) + 0.5 x (1 - t^2) du/dx
+__device__ __forceinline__ float tanh_hw(float x) {
+  float y;
+  asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+__device__ __forceinline__ float gelu_f(float x) {
+  const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+  return 0.5f * x * (1.0f + tanh_hw(u));
+}
 __device__ __forceinline__ float gelu_df(float x) {
-  return 0.5f * (1.0f + erff(x * 0.70710678118654752f)) + x * 0.39894228040143268f * expf(-0.5f * x * x);
+  const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
+  const float t = tanh_hw(u);
+  const float du = 0.7978845608028654f * fmaf(3.0f * 0.044715f, x * x, 1.0f);
+  return 0.5f * (1.0f + t) + 0.5f * x * (1.0f - t * t) * du;
 }
 
 // Z (col-major M x n: Z[r*M + j]) += b[j]; H = bf16(GELU(Z)) when H != NULL

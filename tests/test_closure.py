@@ -27,14 +27,17 @@ def to_bf16(a):
     return ((u + r) & 0xFFFF0000).astype(np.uint32).view(np.float32)
 
 
+C_GELU = math.sqrt(2.0 / math.pi)
+
+
 def gelu(x):
-    from scipy.special import erf
-    return 0.5 * x * (1.0 + erf(x / math.sqrt(2.0)))
+    """GELU in its tanh form (Hendrycks & Gimpel), as the network uses it."""
+    return 0.5 * x * (1.0 + np.tanh(C_GELU * (x + 0.044715 * x ** 3)))
 
 
 def dgelu(x):
-    from scipy.special import erf
-    return 0.5 * (1.0 + erf(x / math.sqrt(2.0))) + x * np.exp(-0.5 * x * x) / math.sqrt(2.0 * math.pi)
+    t = np.tanh(C_GELU * (x + 0.044715 * x ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * x * (1.0 - t * t) * C_GELU * (1.0 + 3.0 * 0.044715 * x * x)
 
 
 def stirred(dims, magnetic, decomp):
