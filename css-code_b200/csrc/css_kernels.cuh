@@ -77,6 +77,8 @@ __device__ __forceinline__ void cp_async8(void *smem, const void *gmem, int src_
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gmem), "r"(src_bytes) : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+// bring a 128-byte line into L2 ahead of its use (no register, no wait)
+__device__ __forceinline__ void prefetch_l2(const void *p) { asm volatile("prefetch.global.L2 [%0];\n" ::"l"(p)); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
@@ -535,6 +537,16 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restric
   double *H = sm;
   double *O = H + nh * HS;
   double *Tb = O + nd * OS;
+  // the pointwise phase reads dv (5 fields), T [and B_phi] at every point of
+  // the tile: start those lines toward L2 now, they are needed after the solves
+  for (int k = threadIdx.x; k < m; k += blockDim.x) {
+    const size_t id = plane(g, ir) + (size_t)(p0 + k) * g.nth + tb;
+    if (tb < g.nth) {
+      for (int f = 0; f < 5; f++) prefetch_l2(dv + f * n + id);
+      prefetch_l2(tbuf + id);
+      if (mag) prefetch_l2(bf + n + id);
+    }
+  }
   const TV *fs[5] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n};
   const double *ms[5] = {g.rhor, nullptr, nullptr, nullptr, g.sr};
   const double *fb[2] = {bf, bf + 2 * n};
@@ -691,6 +703,15 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
   double *O = H + nh * HS;
   double *Tb = O + nd * OS;
   double *datum = Tb + nd * TS;
+  // lines of dv (5 fields), T [and B_r] the pointwise phase will read
+  for (int k = threadIdx.x; k < m; k += blockDim.x) {
+    const size_t id = (size_t)ip * g.nth + tb + (size_t)(r0 + k) * g.nth * g.nphi;
+    if (tb < g.nth) {
+      for (int f = 0; f < 5; f++) prefetch_l2(dv + f * n + id);
+      prefetch_l2(tbuf + id);
+      if (mag) prefetch_l2(bf + 2 * n + id);
+    }
+  }
   const TV *fs[5] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, cur};
   const double *ms[5] = {nullptr, nullptr, nullptr, g.sr, g.rhor};
   const double *fb[2] = {bf, bf + n};
@@ -849,6 +870,25 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
   double *H = sm;
   double *O = H + (size_t)TL * SR;
   double *Tb = O + (size_t)TL * SO;
+  // lines the stage combination reads at every point of the tile: dv, vars0
+  // and the accumulator of every field, T and u_theta (128-byte steps along
+  // the tile's theta segment of each line)
+  {
+    const int seg = (m * 8 + 127) / 128, nl = TL * seg;
+    const size_t pl0 = plane(g, ir);
+    for (int k = threadIdx.x; k < nl; k += blockDim.x) {
+      const int l = k / seg, q = k - l * seg;
+      if (pb + l >= g.nphi) continue;
+      const size_t id = pl0 + (size_t)(pb + l) * g.nth + t0 + q * 16;
+      prefetch_l2(tbuf + id);
+      prefetch_l2(cur + n + id);
+      for (int f = 0; f < g.nv; f++) {
+        prefetch_l2(dv + f * n + id);
+        if (stage > 0) prefetch_l2(v0 + f * n + id);
+        if (stage > 1 || (stage == 1 && g.sldiffusion)) prefetch_l2(vs + f * n + id);
+      }
+    }
+  }
   if constexpr (MT > 0 && TLC > 0) {
     const TS *f1[1] = {cur};
     const double *m1[1] = {g.rhor};
