@@ -493,6 +493,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   const double *rhor = &P[CSS_PROF_RHO * nr];
   double tv[8] = {1e-8 * rhor[nr - 1], 1e-8, 1e-8, 1e-8, 1e-8 * 1e5, 1e-8 * 1e8, 1e-8 * 1e8, 1e-8 * 1e8};
   memcpy(g.tinyvar, tv, sizeof tv);
+  for (int k = 0; k < 8; k++) g.inv_tinyvar[k] = 1.0 / tv[k];  // correctly rounded, as a device division
   g.nsld = 0;
   if (p.mass_diffusion) g.varlist[g.nsld++] = 0;
   for (int i = 1; i <= 4; i++) g.varlist[g.nsld++] = i;

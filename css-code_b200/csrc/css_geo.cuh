@@ -52,7 +52,7 @@ struct CssGeo {
   double s_flux_lo, s_flux_hi;  // entropy-gradient datum at constant-flux faces
   // slope-limited diffusion
   double sld_coef, sld_pr, sld_prm;
-  double tinyvar[8];
+  double tinyvar[8], inv_tinyvar[8];  // floors of the SLD limiter and their reciprocals
   int nsld, varlist[8];
   int dstype, mass_diffusion, do_viscous_heating, do_ohmic_heating;
 };

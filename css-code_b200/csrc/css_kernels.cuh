@@ -1263,13 +1263,13 @@ __global__ void k_sld_vcc(CssGeo g, const double *__restrict__ v, const double *
 // qph/q, so the limited value is 0 (opposite signs), q (|qph| >= |q|) or qph:
 // a minmod, evaluated without the division (equal to the reference's
 // product to within its roundings); below tiny the formula as written.
-__device__ __forceinline__ double sld_limiter(double q, double qph, double tiny) {
+__device__ __forceinline__ double sld_limiter(double q, double qph, double tiny, double inv_tiny) {
   const double a = fabs(q);
   if (a >= tiny) {
     if (!(q * qph > 0.0)) return q * 0.0;
     return fabs(qph) >= a ? q : qph;
   }
-  double rtmp = 1.0 / tiny;
+  double rtmp = inv_tiny;  // 1/tiny, the same correctly rounded quotient
   rtmp = q * (rtmp * rtmp);
   rtmp = rtmp * qph;
   rtmp = fmin(1.0, rtmp);
@@ -1278,9 +1278,10 @@ __device__ __forceinline__ double sld_limiter(double q, double qph, double tiny)
 
 // limited face difference delta at the face whose neighbours are
 // x(-2..+1) around it: qmh = x_{-1}-x_{-2}, qph = x_0-x_{-1}, qp3h = x_1-x_0
-__device__ __forceinline__ double sld_face(double xm2, double xm1, double x0, double x1, double tiny) {
+__device__ __forceinline__ double sld_face(double xm2, double xm1, double x0, double x1, double tiny,
+                                         double inv_tiny) {
   double qmh = xm1 - xm2, qph = x0 - xm1, qp3h = x1 - x0;
-  double pl = sld_limiter(qmh, qph, tiny), pr = sld_limiter(qp3h, qph, tiny);
+  double pl = sld_limiter(qmh, qph, tiny, inv_tiny), pr = sld_limiter(qp3h, qph, tiny, inv_tiny);
   return qph - 0.5 * (pr + pl);
 }
 
@@ -1453,7 +1454,7 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     if (r0 > 0) {
       const double vc = __ldg(vcc + css_idx(g, itc, ipc, r0)), vcm = __ldg(vcc + css_idx(g, itc, ipc, r0 - 1));
       carry[f] = (g.sld_coef * sqrt(0.5 * (vc + vcm))) *
-                 (sld_face(xr(r0 - 2), win[f][0], win[f][1], win[f][2], g.tinyvar[iv]) * g.sld_r[2 * nr + r0]);
+                 (sld_face(xr(r0 - 2), win[f][0], win[f][1], win[f][2], g.tinyvar[iv], g.inv_tinyvar[iv]) * g.sld_r[2 * nr + r0]);
     }
   }
   sld_issue_plane<NF>(g, v, av, vcc, S, 0, r0, t0, p0, off);
@@ -1525,22 +1526,26 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     // also take the lower face
 #pragma unroll
     for (int f = 0; f < NF; f++) {
-      const double tiny = g.tinyvar[f + off];
+      const double tiny = g.tinyvar[f + off], itiny = g.inv_tinyvar[f + off];
       auto tface = [&](int bb, int a) {
         const int gt = t0 + a;
         double d = 0.0;
         if (gt > 0 && gt < nth)
-          d = ST[bb][a] * sld_face(X[f][bb + 2][a], X[f][bb + 2][a + 1], X[f][bb + 2][a + 2], X[f][bb + 2][a + 3], tiny);
+          d = ST[bb][a] * sld_face(X[f][bb + 2][a], X[f][bb + 2][a + 1], X[f][bb + 2][a + 2], X[f][bb + 2][a + 3], tiny,
+                                   itiny);
         FT[f][bb][a] = d;
       };
       auto pface = [&](int bb, int a) {
         FP[f][bb][a] =
-            SP[bb][a] * sld_face(X[f][bb][a + 2], X[f][bb + 1][a + 2], X[f][bb + 2][a + 2], X[f][bb + 3][a + 2], tiny);
+            SP[bb][a] * sld_face(X[f][bb][a + 2], X[f][bb + 1][a + 2], X[f][bb + 2][a + 2], X[f][bb + 3][a + 2], tiny,
+                                 itiny);
       };
       tface(ty, tx + 1);
       pface(ty + 1, tx);
-      if (tx == 0) tface(ty, 0);
+      // the tile's lower faces: warp 0 the phi faces of row 0, warp 1 the
+      // theta faces of column 0 (each warp is one theta row of the tile)
       if (ty == 0) pface(0, tx);
+      else if (ty == 1 && tx < SLD_TP) tface(tx, 0);
     }
     // the velocities of this cell, taken from the tile when they are diffused
     // fields (before the barrier: the next radius's copies reuse the buffer)
@@ -1563,7 +1568,8 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
         if (iv1 < 5) prTP = g.sld_pr; else if (iv1 > 5) prTP = g.sld_prm;
       }
       double dup = (ir == nr - 1) ? 0.0
-                                  : vr_hi * (sld_face(win[f][0], win[f][1], win[f][2], win[f][3], g.tinyvar[iv]) * rhi2);
+                                  : vr_hi * (sld_face(win[f][0], win[f][1], win[f][2], win[f][3], g.tinyvar[iv],
+                                                      g.inv_tinyvar[iv]) * rhi2);
       double flux = t3 * (dup - carry[f]);
       if (prR != 1.0) flux = prR * flux;
       double acc = flux;
