@@ -246,6 +246,23 @@ __device__ __forceinline__ void tiles_ct(const CssGeo &g, const TS *const *f, do
       if (so[k] >= 0) S[(size_t)q * FS + so[k]] = val[q][k];
 }
 
+// Line-solve phase, field of a slot.  With 16-line tiles and 128 threads,
+// slot = task / 16 and a warp holds two slots.  When the fields leave room
+// (nd <= 7) the second-derivative field k2 gets slot 6 with slot 7 idle, and
+// the others fill slots 0.. in order, so no warp runs both line operators
+// one after the other.  -1: an idle slot.
+template <int TLC>
+__device__ __forceinline__ int solve_field(int slot, int nd, int k2) {
+  if (TLC != 16 || nd > 7) return slot < nd ? slot : -1;
+  if (slot == 6) return k2;
+  if (slot >= 7 || slot >= nd - 1) return -1;
+  return slot < k2 ? slot : slot + 1;
+}
+template <int TLC>
+__device__ __forceinline__ int solve_tasks(int nd, int TL) {
+  return (TLC == 16 && nd <= 7) ? 8 * TL : nd * TL;
+}
+
 // ---------------------------------------------------------------------------
 // Source_Theta_Terms (rhs_mpi.f90:786-1029) + Induction_Terms (:2340-2346)
 // grid: x = theta block * nchunk + phi chunk, y = r.  cur = stage input
@@ -286,9 +303,10 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const TV *__restr
   for (int k = 0; k < nd; k++) stage_table(g, 1, bt, k == 4 ? 2 : 1, g.ibct[var[k]], m, Tb + k * TS);
   __syncthreads();
   const double ri = g.r_inv[ir];
-  for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
-    int k = task / TL, l = task - k * TL;
-    if (pb + l >= g.nphi) continue;
+  for (int task = threadIdx.x; task < solve_tasks<TLC>(nd, TL); task += blockDim.x) {
+    const int slot = task / TL, l = task - slot * TL;
+    const int k = solve_field<TLC>(slot, nd, 4);
+    if (k < 0 || pb + l >= g.nphi) continue;
     if (k == 4 && !g.slaplacian) continue;
     int hk = (k <= 3) ? k : (k == 4 ? 3 : k - 1);
     const double *x = H + ((size_t)hk * TL + l) * SR + 4;
@@ -427,9 +445,10 @@ __device__ __forceinline__ void phi_tile_compute(const CssGeo &g, const double *
   stage_table(g, 2, bp, 1, 0, m, Tb);
   stage_table(g, 2, bp, 2, 0, m, Tb + TS);
   __syncthreads();
-  for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
-    int k = task / TL, l = task - k * TL;
-    if (tb + l >= g.nth) continue;
+  for (int task = threadIdx.x; task < solve_tasks<TLC>(nd, TL); task += blockDim.x) {
+    const int slot = task / TL, l = task - slot * TL;
+    const int k = solve_field<TLC>(slot, nd, 5);
+    if (k < 0 || tb + l >= g.nth) continue;
     if (k == 5 && !g.slaplacian) continue;
     int hk = (k <= 4) ? k : (k == 5 ? 4 : k - 1);
     const double *x = H + hk * HS + 4 * SR + l;
@@ -726,9 +745,10 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
   for (int k = 0; k < nd; k++) stage_table(g, 0, br, k == 4 ? 2 : 1, g.ibcr[var[k]], m, Tb + k * TS);
   __syncthreads();
   const int nr = g.nr;
-  for (int task = threadIdx.x; task < nd * TL; task += blockDim.x) {
-    int k = task / TL, l = task - k * TL;
-    if (tb + l >= g.nth) continue;
+  for (int task = threadIdx.x; task < solve_tasks<TLC>(nd, TL); task += blockDim.x) {
+    const int slot = task / TL, l = task - slot * TL;
+    const int k = solve_field<TLC>(slot, nd, 4);
+    if (k < 0 || tb + l >= g.nth) continue;
     if (k == 4 && !g.slaplacian) continue;
     int hk = (k <= 3) ? k : (k == 4 ? 3 : (k == 5 ? 4 : k - 1));
     const double *x = H + hk * HS + 4 * SR + l;
