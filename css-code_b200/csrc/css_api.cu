@@ -324,6 +324,10 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     set_err("css_create: ohmic heating needs magnetic diffusion");
     return CSS_ERR_ARG;
   }
+  if (p.time_stepper != 0 && p.time_stepper != 2 && p.time_stepper != 3 && p.time_stepper != 4) {
+    set_err("css_create: time_stepper %d unknown (4 RK4, 2 RK2-TVD, 3 RK3-TVD)", p.time_stepper);
+    return CSS_ERR_ARG;
+  }
   if (p.sldiffusion && (p.nth % 2)) {
     // the SLD kernel streams theta pairs with 16-byte copies
     set_err("css_create: slope-limited diffusion needs an even nth (got %d)", p.nth);
@@ -687,7 +691,8 @@ static void launch_phi_p(css_ctx *c, const double *cur) {
 
 // stage input of storage type TS, next stage state of storage type TO
 template <typename TS, typename TO>
-static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur) {
+static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur, double ca = 0.0, double cb = 0.0,
+                      double dsld = 0.0) {
   const CssGeo &g = c->g;
   const int mag = g.magnetic;
   if (mag) {
@@ -729,7 +734,7 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_RHOT_UPDATE);
   LAUNCH_MT(1, TL, k_rhot_update, (TS, TO), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
-            TL, c->flag);
+            ca, cb, dsld, TL, c->flag);
   prof_end(c);
   return check_launch(c);
 }
@@ -785,6 +790,26 @@ static int step_once(css_ctx *c, double dt) {
       if (int rc = launch_curl(c, (const double *)(c->v0 + 5 * c->ncell), c->bf, 1)) return rc;
     }
     if (int rc = launch_sld(c, c->v0, c->v0 + 5 * c->ncell, c->vs)) return rc;
+  }
+  const int ts = c->p.time_stepper;
+  if (ts == 2 || ts == 3) {
+    // Step_RK2_TVD / Step_RK3_TVD (step_rk4.f90:31-335): vs holds the SLD
+    // tendency of the step's start, added once in the last stage
+    const double dsld = c->p.sldiffusion ? dt : 0.0;
+    float *fA = reinterpret_cast<float *>(c->vA), *fB = reinterpret_cast<float *>(c->vB);
+    const bool mixed = c->p.precision == 1;
+    int rc = mixed ? launch_rhs(c, (const double *)c->v0, fA, 5, dt, 1.0, 0.0)
+                   : launch_rhs(c, (const double *)c->v0, c->vA, 5, dt, 1.0, 0.0);
+    if (rc) return rc;
+    if (ts == 2)
+      return mixed ? launch_rhs(c, (const float *)fA, c->v0, 6, 0.5 * dt, 0.5, 0.5, dsld)
+                   : launch_rhs(c, (const double *)c->vA, c->v0, 6, 0.5 * dt, 0.5, 0.5, dsld);
+    rc = mixed ? launch_rhs(c, (const float *)fA, fB, 5, dt / 4.0, 0.75, 0.25)
+               : launch_rhs(c, (const double *)c->vA, c->vB, 5, dt / 4.0, 0.75, 0.25);
+    if (rc) return rc;
+    const double onethird = 1.0 / 3.0, twothirds = 2.0 / 3.0;
+    return mixed ? launch_rhs(c, (const float *)fB, c->v0, 6, 2.0 * dt / 3.0, onethird, twothirds, dsld)
+                 : launch_rhs(c, (const double *)c->vB, c->v0, 6, 2.0 * dt / 3.0, onethird, twothirds, dsld);
   }
   if (c->p.precision == 1) {
     // mixed: the stage states U1..U3 are FP32 (rho, s as perturbations about

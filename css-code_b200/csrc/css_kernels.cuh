@@ -871,12 +871,16 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
 //   stage 1: vs = (sld ? vs + dv/6 : dv); nx = v0 + dtcur*dv
 //   stage 2,3: vs = vs + dv/3;            nx = v0 + dtcur*dv
 //   stage 4: vs = vs + dv/6;              nx = v0 + dtcur*vs  (nx may be v0)
+// and the TVD schemes (Step_RK2_TVD / Step_RK3_TVD, step_rk4.f90:31-335),
+// where vs holds the step's SLD tendency:
+//   stage 5: nx = ca*v0 + cb*cur + dtcur*dv
+//   stage 6: nx = (ca*v0 + cb*cur + dtcur*dv) + dsld*vs  (nx may be v0)
 // ---------------------------------------------------------------------------
 template <int MT, int TLC, typename TS, typename TO>
 __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restrict__ cur,
                                                      double *__restrict__ dv, const double *v0, double *vs, TO *nx,
                                                      const double *__restrict__ tbuf, int stage, double dtcur,
-                                                     int TLrt, int *flag) {
+                                                     double ca, double cb, double dsld, int TLrt, int *flag) {
   extern __shared__ double sm[];
   const int TL = TLC ? TLC : TLrt;
   const int nchunk = (g.nphi + TL - 1) / TL;
@@ -905,7 +909,9 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
       for (int f = 0; f < g.nv; f++) {
         prefetch_l2(dv + f * n + id);
         if (stage > 0) prefetch_l2(v0 + f * n + id);
-        if (stage > 1 || (stage == 1 && g.sldiffusion)) prefetch_l2(vs + f * n + id);
+        if ((stage > 1 && stage <= 4) || (stage == 1 && g.sldiffusion) || (stage == 6 && dsld != 0.0))
+          prefetch_l2(vs + f * n + id);
+        if (stage >= 5 && cb != 0.0) prefetch_l2(cur + f * n + id);
       }
     }
   }
@@ -987,14 +993,18 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
     }
     const bool rlo = (ir == 0), rhi = (ir == g.nr - 1);
     for (int iv = 0; iv < nv; iv++) {
-      double dd[PPT], aa[PPT], ss[PPT];
+      double dd[PPT], aa[PPT], ss[PPT], cc[PPT];
+      const bool need_s = stage <= 4 ? !(stage == 1 && !g.sldiffusion) : (stage == 6 && dsld != 0.0);
+      const bool need_c = stage >= 5 && cb != 0.0;
+      const double *bg = iv == 0 ? g.rhor : (iv == 4 ? g.sr : nullptr);  // background of an FP32 stage state
 #pragma unroll
       for (int k = 0; k < PPT; k++) {
         if (!okk[k]) continue;
         const size_t q = (size_t)iv * n + idk[k];
         dd[k] = (iv == 0) ? d0k[k] : (iv == 1) ? d1k[k] : dv[q];
         aa[k] = v0[q];
-        ss[k] = (stage == 1 && !g.sldiffusion) ? 0.0 : vs[q];
+        ss[k] = need_s ? vs[q] : 0.0;
+        cc[k] = need_c ? st_val(cur + (size_t)iv * n, idk[k], bg, ir) : 0.0;
       }
 #pragma unroll
       for (int k = 0; k < PPT; k++) {
@@ -1009,10 +1019,13 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
         } else if (stage == 4) {
           double sv = ss[k] + d / 6.0;
           o = a + dtcur * sv;
-        } else {
+        } else if (stage <= 3) {
           double sv = ss[k] + d / 3.0;
           vs[q] = sv;
           o = a + dtcur * d;
+        } else {
+          o = ca * a + cb * cc[k] + dtcur * d;
+          if (stage == 6 && dsld != 0.0) o = o + dsld * ss[k];
         }
         const bool twall = (itk[k] == 0 || itk[k] == g.nth - 1);
         // Bound (rhs_mpi.f90:2395-2491)

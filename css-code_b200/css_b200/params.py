@@ -31,6 +31,7 @@ _FIELDS = [
     ("do_viscous_heating", ctypes.c_int), ("do_ohmic_heating", ctypes.c_int),
     ("flux_limiter", ctypes.c_int), ("ent_flux_limiter", ctypes.c_int), ("mag_flux_limiter", ctypes.c_int),
     ("precision", ctypes.c_int),
+    ("time_stepper", ctypes.c_int),
 ]
 
 
@@ -97,4 +98,5 @@ def default_params(nr, nth, nphi, decomp, magnetic=False):
     p.do_ohmic_heating = 1 if magnetic else 0
     p.flux_limiter = p.ent_flux_limiter = p.mag_flux_limiter = -1
     p.precision = 0
+    p.time_stepper = 4
     return p

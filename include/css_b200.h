@@ -92,6 +92,9 @@ typedef struct css_params {
   int do_viscous_heating, do_ohmic_heating;
   int flux_limiter, ent_flux_limiter, mag_flux_limiter;  /* <= 0: off         */
   int precision;              /* 0: FP64 (drop-in), 1: FP32 perturbation form  */
+  int time_stepper;           /* 4: Step_RK4 (default), 2: Step_RK2_TVD, 3:
+                                 Step_RK3_TVD (step_rk4.f90:31-335; the
+                                 RK2TVD / RK3TVD namelist switches)         */
 } css_params;
 
 typedef struct css_ctx css_ctx;

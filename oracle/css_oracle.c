@@ -1930,12 +1930,63 @@ static void bound(orc_ctx *c, double *v1) {
   }
 }
 
+/* Step_RK2_TVD / Step_RK3_TVD (step_rk4.f90:31-335): the SLD tendency of
+   the step's start (forward Euler) is added once, after the last stage's
+   combination and before its Bound */
+static void step_tvd(orc_ctx *c, double *vars0, double dt, int order, double *av) {
+  const css_params *p = &c->p;
+  size_t N = (size_t)c->ncell * c->nv;
+  double *v1 = c->vars1, *dv = c->dvars1, *v2 = c->vars2, *vs = c->vars_save;
+  const double onethird = 1.0 / 3.0, twothirds = 2.0 / 3.0;
+  double dtcur = dt;
+  memcpy(v1, vars0, sizeof(double) * N);
+  orc_rhs(c, v1, dv, 1);
+  if (p->sldiffusion) {
+    memcpy(v2, dv, sizeof(double) * N);
+    if (p->magnetic) memcpy(av, c->maga, sizeof(double) * 3 * c->ncell);
+    orc_diffusion(c, v1, av, dv);
+    memcpy(vs, dv, sizeof(double) * N);
+    memcpy(dv, v2, sizeof(double) * N);
+  }
+#pragma omp parallel for schedule(static)
+  for (size_t i = 0; i < N; i++) v1[i] = vars0[i] + dtcur * dv[i];
+  bound(c, v1);
+  if (order == 2) {
+    dtcur = 0.5 * dt;
+    orc_rhs(c, v1, dv, 2);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < N; i++) v1[i] = 0.5 * vars0[i] + 0.5 * v1[i] + dtcur * dv[i];
+  } else {
+    dtcur = dt / 4.0;
+    orc_rhs(c, v1, dv, 2);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < N; i++) v1[i] = 0.75 * vars0[i] + 0.25 * v1[i] + dtcur * dv[i];
+    bound(c, v1);
+    dtcur = 2.0 * dt / 3.0;
+    orc_rhs(c, v1, dv, 3);
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < N; i++) v1[i] = onethird * vars0[i] + twothirds * v1[i] + dtcur * dv[i];
+  }
+  if (p->sldiffusion) {
+    dtcur = dt;
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < N; i++) v1[i] = v1[i] + dtcur * vs[i];
+  }
+  bound(c, v1);
+  memcpy(vars0, v1, sizeof(double) * N);
+}
+
 int orc_step_rk4(orc_ctx *c, double *vars0, double dt, int nsteps) {
   const css_params *p = &c->p;
   size_t N = (size_t)c->ncell * c->nv;
   double *v1 = c->vars1, *dv = c->dvars1, *v2 = c->vars2, *vs = c->vars_save;
   double *av = NULL;
   if (p->magnetic) av = (double *)malloc(sizeof(double) * 3 * c->ncell);
+  if (p->time_stepper == 2 || p->time_stepper == 3) {
+    for (int step = 0; step < nsteps; step++) step_tvd(c, vars0, dt, p->time_stepper, av);
+    free(av);
+    return CSS_OK;
+  }
   for (int step = 0; step < nsteps; step++) {
     double dtcur = dt / 2.0;
     memcpy(v1, vars0, sizeof(double) * N);

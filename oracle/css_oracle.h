@@ -16,7 +16,7 @@
  *                    Density_Terms_Theta/_Radial, Induction_Terms, Bound),
  *   diffusion.f90   (Initialize_Diffusion, Compute_Diffusion, Diffusion_R,
  *                    Diffusion_Th, Diffusion_Phi),
- *   step_rk4.f90    (Step_RK4),
+ *   step_rk4.f90    (Step_RK4, Step_RK2_TVD, Step_RK3_TVD),
  *   report_mpi.f90  (Scalar_Output, Shell_Average_Output and the ds/dr of
  *                    Compute_Derivatives), rhs_mpi.f90 Compute_Step_Size,
  *   CSS-IDL/spectral_analysis_new.pro (the folded FFT spectrum),
