@@ -18,6 +18,7 @@
 #include "css_kernels.cuh"
 #include "css_stats.cuh"
 #include "css_closure.cuh"
+#include "css_lap.cuh"
 
 using namespace css;
 
@@ -60,6 +61,10 @@ struct css_ctx {
   double *vcc;                      // SLD speed^2
   double *cda;                      // curl of the A-tendency (MHD ohmic heating)
   double *tbuf;                     // temperature of the current stage input
+  double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
+  double *lapface = nullptr;        // explicit viscosity: face data, 6 x max face size
+  double dtd = 1e10;                // viscous time-step limit of Compute_Step_Size
+  double rep_flux_lo = 0.0, rep_flux_hi = 0.0;  // dsdr1/dxdr(1), dsdr2/dxdr(nr) of the reports
   int mt[3];                        // compile-time block length per direction (0 = generic)
   int *flag;
   long long launches;
@@ -228,6 +233,7 @@ extern "C" void css_destroy(css_ctx *c) {
   cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo); cudaFree(c->resp);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
   cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf);
+  cudaFree(c->lapbuf); cudaFree(c->lapface);
   for (auto e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -335,6 +341,11 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   }
   if (p.precision != 0 && p.precision != 1) {
     set_err("css_create: precision %d unknown (0 FP64, 1 mixed: FP32 stage states)", p.precision);
+    return CSS_ERR_ARG;
+  }
+  if (p.laplacian && (p.magnetic || p.precision != 0)) {
+    set_err("css_create: explicit viscosity runs hydro in FP64 only (the resistive induction terms and the FP32 "
+            "stage states are not built for it)");
     return CSS_ERR_ARG;
   }
   css_ctx *c = new css_ctx();
@@ -452,7 +463,9 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   g.invtconst = g.invcv / g.gamm1;
   g.omega0 = p.omega_0; g.t0 = p.t0; g.damping_time = p.damping_time; g.lumr1 = p.lumr1; g.lumr2 = p.lumr2;
   g.r1 = p.r1; g.r2 = p.r2; g.dth = dth; g.dphi = dphi; g.xi_cs = p.xi_cs;
-  g.slaplacian = p.slaplacian; g.sldiffusion = p.sldiffusion; g.set_stop = p.set_stop;
+  // entropy conduction is on under Laplacian .or. SLaplacian (rhs_mpi.f90:959,
+  // :1221, :1286, :1456, :586, :618; diffusion.f90:614, :688)
+  g.slaplacian = p.slaplacian || p.laplacian; g.sldiffusion = p.sldiffusion; g.set_stop = p.set_stop;
   g.top_stress_free = p.top_stress_free; g.bottom_stress_free = p.bottom_stress_free;
   g.top_constant_temp = p.top_constant_temp; g.bottom_constant_temp = p.bottom_constant_temp;
   g.theta_stress_free = p.theta_stress_free; g.theta_normal_field = p.theta_normal_field;
@@ -489,9 +502,14 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   const double *ks = &P[CSS_PROF_KS * nr];
   g.s_flux_lo = g.s_flux_hi = 0.0;
   if (!p.bottom_constant_temp)
-    g.s_flux_lo = p.slaplacian ? -p.lumr1 * one_over_4pi / (p.r1 * p.r1 * ks[0] * dxdr[0]) : 0.0 / dxdr[0];
+    g.s_flux_lo = g.slaplacian ? -p.lumr1 * one_over_4pi / (p.r1 * p.r1 * ks[0] * dxdr[0]) : 0.0 / dxdr[0];
   if (!p.top_constant_temp)
-    g.s_flux_hi = p.slaplacian ? -p.lumr2 * one_over_4pi / (p.r2 * p.r2 * ks[nr - 1] * dxdr[nr - 1]) : 0.0 / dxdr[nr - 1];
+    g.s_flux_hi = g.slaplacian ? -p.lumr2 * one_over_4pi / (p.r2 * p.r2 * ks[nr - 1] * dxdr[nr - 1]) : 0.0 / dxdr[nr - 1];
+  // the reports' dsdr1/dsdr2 follow SLaplacian alone (mhdsph_mpi.f90:576-584)
+  c->rep_flux_lo = c->rep_flux_hi = 0.0;
+  if (!p.bottom_constant_temp && p.slaplacian) c->rep_flux_lo = -p.lumr1 * one_over_4pi / (p.r1 * p.r1 * ks[0] * dxdr[0]);
+  if (!p.top_constant_temp && p.slaplacian)
+    c->rep_flux_hi = -p.lumr2 * one_over_4pi / (p.r2 * p.r2 * ks[nr - 1] * dxdr[nr - 1]);
   // SLD (diffusion.f90:76-114, :51-61)
   g.sld_coef = p.sld_coef; g.sld_pr = p.sld_pr; g.sld_prm = p.sld_prm;
   const double *rhor = &P[CSS_PROF_RHO * nr];
@@ -519,8 +537,8 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     return CSS_ERR_CUDA;
   }
   c->stream = c->own_stream;
-  // radial profile block: r_ind r_inv dr_ind dxdr d2xdr2 rhor sr grav ks dlnks eps dspeed
-  std::vector<double> R((size_t)12 * nr);
+  // radial profile block: r_ind r_inv dr_ind dxdr d2xdr2 rhor sr grav ks dlnks eps dspeed mur dlnmu
+  std::vector<double> R((size_t)14 * nr);
   for (int i = 0; i < nr; i++) {
     R[0 * nr + i] = r_ind[i];
     R[1 * nr + i] = 1.0 / r_ind[i];
@@ -534,6 +552,20 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     R[9 * nr + i] = P[CSS_PROF_DLNKS * nr + i];
     R[10 * nr + i] = P[CSS_PROF_EPS * nr + i];
     R[11 * nr + i] = dspeed[i];
+    R[12 * nr + i] = P[CSS_PROF_MUR * nr + i];
+    R[13 * nr + i] = P[CSS_PROF_DLNMU * nr + i];
+  }
+  if (p.laplacian) {
+    // dtmaxd of Compute_Step_Size (rhs_mpi.f90:194-198; etar = ks there)
+    const double *dr = &P[CSS_PROF_DR * nr], *mu = &P[CSS_PROF_MUR * nr];
+    double drmin = dr[0], ksmax = ks[0], mumax = mu[0] / rhor[0];
+    for (int i = 1; i < nr; i++) {
+      drmin = std::min(drmin, dr[i]);
+      ksmax = std::max(ksmax, ks[i]);
+      mumax = std::max(mumax, mu[i] / rhor[i]);
+    }
+    double h = std::min(drmin, p.r1 * std::min(std::min(sines[0], sines[nth - 1]) * dphi, dth));
+    c->dtd = h * h / std::max(std::max(ksmax, mumax), ksmax);
   }
   // SLD geometry tables (diffusion.f90:806-849, :1196-1247, :1316-1351),
   // the same expressions as the reference evaluates per rank
@@ -591,6 +623,11 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   ALLOC(c->tbuf, c->ncell * sizeof(double));
   if (p.magnetic) { ALLOC(c->bf, 3 * c->ncell * sizeof(double)); ALLOC(c->cda, 3 * c->ncell * sizeof(double)); }
   ALLOC(c->flag, sizeof(int));
+  if (p.laplacian) {
+    size_t nf = std::max((size_t)nth * nphi, (size_t)nphi * nr);
+    ALLOC(c->lapbuf, 12 * c->ncell * sizeof(double));
+    ALLOC(c->lapface, 6 * nf * sizeof(double));
+  }
   cudaMemcpy(c->tab, T.data(), T.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->prof, R.data(), R.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->theta_prof, TH.data(), TH.size() * 8, cudaMemcpyHostToDevice);
@@ -603,6 +640,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   g.r_ind = c->prof; g.r_inv = c->prof + nr; g.dr_ind = c->prof + 2 * nr; g.dxdr = c->prof + 3 * nr;
   g.d2xdr2 = c->prof + 4 * nr; g.rhor = c->prof + 5 * nr; g.sr = c->prof + 6 * nr; g.grav = c->prof + 7 * nr;
   g.ks = c->prof + 8 * nr; g.dlnks = c->prof + 9 * nr; g.eps = c->prof + 10 * nr; g.dspeed = c->prof + 11 * nr;
+  g.mur = c->prof + 12 * nr; g.dlnmu = c->prof + 13 * nr;
   g.sines = c->theta_prof; g.cosines = c->theta_prof + nth; g.theta = c->theta_prof + 2 * nth;
   g.cot = c->theta_prof + 3 * nth; g.csc = c->theta_prof + 4 * nth;
   g.sld_th = c->sld_geo; g.sld_r = c->sld_geo + 5 * (size_t)nth;
@@ -690,6 +728,65 @@ static void launch_phi_p(css_ctx *c, const double *cur) {
 }
 
 // stage input of storage type TS, next stage state of storage type TO
+// explicit viscosity (Laplacian): the viscous terms of the three sweeps and
+// the cross terms, added into c->dv after the phi sweep; FP64 states only
+static int launch_lap(css_ctx *c, const double *cur) {
+  const CssGeo &g = c->g;
+  const size_t n = c->ncell;
+  const size_t nf = std::max((size_t)g.nth * g.nphi, (size_t)g.nphi * g.nr);
+  double *S = c->lapbuf, *L = c->lapbuf + 6 * n, *F = c->lapface;
+  const double *w = cur + n, *v = cur + 2 * n, *u = cur + 3 * n;
+  const int nbp = (int)std::min<size_t>((n + 255) / 256, (size_t)c->nsm * 8);
+  const int nbf = (int)std::min<size_t>((nf + 255) / 256, (size_t)c->nsm * 8);
+  cudaStream_t st = c->stream;
+#define LAP_D(dir, ord, x, out, lo, hi, bdry) \
+  if (int rc = css_deriv_dev(c, dir, ord, x, out, lo, hi, bdry, nullptr)) return rc
+  // theta sweep: d/dth and d2/dth2 of w, v (wall datum cot v), u
+  k_lap_bc_theta<<<nbf, 256, 0, st>>>(g, cur, F, F + nf);
+  if (int rc = check_launch(c)) return rc;
+  LAP_D(1, 1, w, S, nullptr, nullptr, g.ibct[2]);
+  LAP_D(1, 1, v, S + n, F, F + nf, g.ibct[3]);
+  LAP_D(1, 1, u, S + 2 * n, nullptr, nullptr, g.ibct[4]);
+  LAP_D(1, 2, w, S + 3 * n, nullptr, nullptr, g.ibct[2]);
+  LAP_D(1, 2, v, S + 4 * n, F, F + nf, g.ibct[3]);
+  LAP_D(1, 2, u, S + 5 * n, nullptr, nullptr, g.ibct[4]);
+  k_lap_theta<<<nbp, 256, 0, st>>>(g, cur, S, L, c->dv);
+  if (int rc = check_launch(c)) return rc;
+  // phi sweep: v, w, u
+  LAP_D(2, 1, v, S, nullptr, nullptr, 0);
+  LAP_D(2, 1, w, S + n, nullptr, nullptr, 0);
+  LAP_D(2, 1, u, S + 2 * n, nullptr, nullptr, 0);
+  LAP_D(2, 2, v, S + 3 * n, nullptr, nullptr, 0);
+  LAP_D(2, 2, w, S + 4 * n, nullptr, nullptr, 0);
+  LAP_D(2, 2, u, S + 5 * n, nullptr, nullptr, 0);
+  k_lap_phi<<<nbp, 256, 0, st>>>(g, cur, c->tbuf, S, L, c->dv);
+  if (int rc = check_launch(c)) return rc;
+  // radial sweep: w, v with the stress-free data, u
+  k_lap_bc_r<<<nbf, 256, 0, st>>>(g, cur, F, F + nf, F + 2 * nf, F + 3 * nf);
+  if (int rc = check_launch(c)) return rc;
+  LAP_D(0, 1, w, S, F, F + nf, g.ibcr[2]);
+  LAP_D(0, 1, v, S + n, F + 2 * nf, F + 3 * nf, g.ibcr[3]);
+  LAP_D(0, 1, u, S + 2 * n, nullptr, nullptr, g.ibcr[4]);
+  LAP_D(0, 2, w, S + 3 * n, F, F + nf, g.ibcr[2]);
+  LAP_D(0, 2, v, S + 4 * n, F + 2 * nf, F + 3 * nf, g.ibcr[3]);
+  LAP_D(0, 2, u, S + 5 * n, nullptr, nullptr, g.ibcr[4]);
+  k_lap_r<<<nbp, 256, 0, st>>>(g, cur, c->tbuf, S, L, c->dv);
+  if (int rc = check_launch(c)) return rc;
+  // cross terms: r derivatives of r L0 (var 2), r L5 (var 4), r L2 (var 4),
+  // r L3 (var 3); theta derivatives of sin L3 (var 3), sin L4 (var 2)
+  k_lap_bc_cross<<<nbf, 256, 0, st>>>(g, L, F, F + nf, F + 2 * nf, F + 3 * nf);
+  if (int rc = check_launch(c)) return rc;
+  LAP_D(0, 1, S, L, F, nullptr, g.ibcr[2]);
+  LAP_D(0, 1, S + n, L + n, nullptr, nullptr, g.ibcr[4]);
+  LAP_D(0, 1, S + 2 * n, L + 2 * n, nullptr, nullptr, g.ibcr[4]);
+  LAP_D(0, 1, S + 3 * n, L + 3 * n, nullptr, F + nf, g.ibcr[3]);
+  LAP_D(1, 1, S + 4 * n, L + 4 * n, F + 2 * nf, F + 3 * nf, g.ibct[3]);
+  LAP_D(1, 1, S + 5 * n, L + 5 * n, nullptr, nullptr, g.ibct[2]);
+#undef LAP_D
+  k_lap_cross<<<nbp, 256, 0, st>>>(g, cur, L, c->dv);
+  return check_launch(c);
+}
+
 template <typename TS, typename TO>
 static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur, double ca = 0.0, double cb = 0.0,
                       double dsld = 0.0) {
@@ -724,6 +821,10 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
     LAUNCH_MT(2, TL, k_phi_terms, (TS), gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
+  if constexpr (sizeof(TS) == 8) {
+    if (c->p.laplacian)
+      if (int rc = launch_lap(c, (const double *)cur)) return rc;
+  }
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_RADIAL);
@@ -1317,7 +1418,7 @@ static int run_stats(css_ctx *c, int need_dsdr, std::vector<double> &res) {
   if (need_dsdr) {
     // Compute_Derivatives (report_mpi.f90:288-318): d s/d r with the
     // constant-flux datum dsdr1/dxdr(1), dsdr2/dxdr(nr) at the faces
-    k_fill2<<<256, 256, 0, st>>>(c->vB, np, g.s_flux_lo, g.s_flux_hi);
+    k_fill2<<<256, 256, 0, st>>>(c->vB, np, c->rep_flux_lo, c->rep_flux_hi);
     if (int rc = check_launch(c)) return rc;
     if (int rc = css_deriv_dev(c, 0, 1, c->v0 + 4 * n, c->vA, c->vB, c->vB + np, g.ibcr[5], nullptr)) return rc;
     dsdr = c->vA;
@@ -1376,7 +1477,7 @@ extern "C" int css_step_size(css_ctx *c, double cfl_safety, double *out) {
     m += r[SA_M];
     mrs += r[SA_MRS];
   }
-  const double dtd = 1e10;  // no explicit (Laplacian) viscosity limit
+  const double dtd = c->dtd;  // 1e10 unless explicit viscosity is on
   out[0] = std::min(std::min(dtb, dtc), dtd) * cfl_safety;
   out[1] = e;
   out[2] = l;
@@ -1417,7 +1518,7 @@ extern "C" int css_shell_averages(css_ctx *c, const int *quantities, int nq, con
       if (q == 4) v = gamm1 * cv * sum * inv;
       else if (q == 15) {  // F_ks: conduction by the SLaplacian ks plus the prescribed flux k0
         const double k0r = k0 ? k0[ir] : 0.0;
-        v = c->p.slaplacian ? -ksh[ir] * sum * inv + k0r : k0r;
+        v = c->g.slaplacian ? -ksh[ir] * sum * inv + k0r : k0r;
       } else if (q == 16) v = c->p.cp * sum * inv;
       else v = sum * inv;
       out[(size_t)iq * nr + ir] = v;

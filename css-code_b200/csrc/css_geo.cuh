@@ -30,6 +30,7 @@ struct CssGeo {
   const double *resp_r;     // [r block][lo|hi][tstride]: unit response of d/dr to the face datum of rho
   // radial profiles (length nr)
   const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
+  const double *mur, *dlnmu;  // viscosity and its log-derivative (explicit-viscosity path)
   // per-cell SLD speed^2 replacing dspeed (a learned closure's output);
   // NULL, or a negative entry, means the prescribed radial profile
   const double *speed2;

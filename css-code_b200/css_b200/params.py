@@ -32,6 +32,7 @@ _FIELDS = [
     ("flux_limiter", ctypes.c_int), ("ent_flux_limiter", ctypes.c_int), ("mag_flux_limiter", ctypes.c_int),
     ("precision", ctypes.c_int),
     ("time_stepper", ctypes.c_int),
+    ("laplacian", ctypes.c_int),
 ]
 
 
@@ -51,8 +52,9 @@ class CssParams(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in _FIELDS}
 
 
-NPROF = 11  # CSS_NPROF
-PROF_NAMES = ["x_ind", "r_ind", "dr_ind", "dxdr", "d2xdr2", "rhor", "sr", "gravity", "ks", "dlnks", "eps"]
+NPROF = 13  # CSS_NPROF
+PROF_NAMES = ["x_ind", "r_ind", "dr_ind", "dxdr", "d2xdr2", "rhor", "sr", "gravity", "ks", "dlnks", "eps",
+              "mur", "dlnmu"]
 
 
 def default_params(nr, nth, nphi, decomp, magnetic=False):

@@ -85,7 +85,10 @@ def polytrope(p, n_rho, stretch=1.0, kappa=None, ra=1e5, pr=1.0, g0_exp=0.0, del
     ks = kappa * rhor * tr * (rhor / rhor[-1]) ** g0_exp
     dlnks = -(gamma + g0_exp) * alp * r2 * r_inv ** 2 / base / gamm1
     eps = np.zeros(nr)
-    prof = np.stack([x, r, dr, dxdr, d2xdr2, rhor, sr, gravity, ks, dlnks, eps]).astype(np.float64)
+    # viscosity of the explicit-viscosity path (mhdsph_mpi.f90:352-354)
+    mur = p.sld_pr * kappa * rhor
+    dlnmu = -alp * r2 * r_inv ** 2 / base / gamm1
+    prof = np.stack([x, r, dr, dxdr, d2xdr2, rhor, sr, gravity, ks, dlnks, eps, mur, dlnmu]).astype(np.float64)
     assert prof.shape[0] == NPROF
     lum = delta * cp / d * 4.0 * math.pi * r1 ** 2 * ks[0]
     p.lumr1 = lum

@@ -57,6 +57,8 @@ enum {
   CSS_PROF_KS,        /* entropy conductivity ks                             */
   CSS_PROF_DLNKS,     /* d ln ks / dr                                        */
   CSS_PROF_EPS,       /* internal heating eps                                */
+  CSS_PROF_MUR,       /* dynamic viscosity mur (explicit-viscosity path)     */
+  CSS_PROF_DLNMU,     /* d ln mur / dr                                       */
   CSS_NPROF
 };
 
@@ -95,6 +97,10 @@ typedef struct css_params {
   int time_stepper;           /* 4: Step_RK4 (default), 2: Step_RK2_TVD, 3:
                                  Step_RK3_TVD (step_rk4.f90:31-335; the
                                  RK2TVD / RK3TVD namelist switches)         */
+  int laplacian;              /* 1: explicit viscosity (the Laplacian switch,
+                                 rhs_mpi.f90:844-927, :1123-1199, :1317-1435,
+                                 :2070-2296); also turns the entropy
+                                 conduction on, as SLaplacian does           */
 } css_params;
 
 typedef struct css_ctx css_ctx;

@@ -64,7 +64,7 @@ struct orc_ctx {
   css_params p;
   int nr, nth, nphi, nv, ncell;
   double *x_ind, *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks,
-      *dlnks, *eps;
+      *dlnks, *eps, *mur, *dlnmu;
   double *theta, *phi, *sines, *cosines;
   double dth, dphi;
   int ibcr[13], ibct[13]; /* 1-based as the reference's ibcr/ibct */
@@ -77,7 +77,14 @@ struct orc_ctx {
   double gamm1, cv, invcp, invcv, pconst, invpconst, invtconst;
   /* work arrays */
   double *temperature, *invrho, *maga, *vars2, *vars_save, *dvars1, *vars1, *tmpf, *tmpg, *da;
+  /* explicit viscosity: the velocity derivatives the sweeps leave for the
+   * cross terms (the reference's vars2 under Laplacian), 6 fields:
+   * LAP_W1 ri dw/dth, LAP_V1 ri dv/dth, LAP_U1 ri du/dth,
+   * LAP_PV dv/dph/(r sin), LAP_PW dw/dph/(r sin), LAP_PU du/dph/(r sin) */
+  double *lap;
+  int cond; /* entropy conduction on: Laplacian .or. SLaplacian */
 };
+enum { LAP_W1 = 0, LAP_V1, LAP_U1, LAP_PV, LAP_PW, LAP_PU, LAP_N };
 
 #define IDX(c, it, ip, ir) ((it) + (c)->nth * ((ip) + (c)->nphi * (size_t)(ir)))
 #define FLD(c, a, iv) ((a) + (size_t)(iv) * (c)->ncell)
@@ -546,6 +553,7 @@ void orc_destroy(orc_ctx *c) {
   free(c->blk); free(c->rblk_of);
   free(c->x_ind); free(c->r_ind); free(c->r_inv); free(c->dr_ind); free(c->dxdr); free(c->d2xdr2);
   free(c->rhor); free(c->sr); free(c->grav); free(c->ks); free(c->dlnks); free(c->eps);
+  free(c->mur); free(c->dlnmu); free(c->lap);
   free(c->theta); free(c->phi); free(c->sines); free(c->cosines); free(c->dspeed);
   free(c->temperature); free(c->invrho); free(c->maga); free(c->vars2); free(c->vars_save);
   free(c->dvars1); free(c->vars1); free(c->tmpf); free(c->tmpg); free(c->da);
@@ -563,6 +571,10 @@ int orc_create(const css_params *p, const double *prof, orc_ctx **out) {
     set_err("orc_create: SLD power flux limiters are not restated (all configs keep them off)");
     return CSS_ERR_ARG;
   }
+  if (p->laplacian && p->magnetic) {
+    set_err("orc_create: explicit viscosity with magnetic fields (the resistive induction terms) is not restated");
+    return CSS_ERR_ARG;
+  }
   orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
   c->p = *p;
   c->nr = p->nr; c->nth = p->nth; c->nphi = p->nphi;
@@ -570,7 +582,7 @@ int orc_create(const css_params *p, const double *prof, orc_ctx **out) {
   c->ncell = p->nr * p->nth * p->nphi;
   int nr = c->nr, nth = c->nth, nphi = c->nphi;
   double **dst[] = {&c->x_ind, &c->r_ind, &c->dr_ind, &c->dxdr, &c->d2xdr2, &c->rhor,
-                    &c->sr,    &c->grav,  &c->ks,     &c->dlnks, &c->eps};
+                    &c->sr,    &c->grav,  &c->ks,     &c->dlnks, &c->eps, &c->mur, &c->dlnmu};
   for (int k = 0; k < CSS_NPROF; k++) {
     *dst[k] = dalloc(nr);
     memcpy(*dst[k], prof + (size_t)k * nr, sizeof(double) * nr);
@@ -713,6 +725,8 @@ even:
   c->dvars1 = dalloc(n * c->nv); c->vars1 = dalloc(n * c->nv);
   c->tmpf = dalloc(n); c->tmpg = dalloc(n);
   if (p->magnetic) c->da = dalloc(3 * n);
+  if (p->laplacian) c->lap = dalloc(n * LAP_N);
+  c->cond = p->slaplacian || p->laplacian;
   *out = c;
   return CSS_OK;
 }
@@ -931,9 +945,14 @@ int orc_curl_b(orc_ctx *c, const double *a, double *b) {
 /* ------------------------------------------------------------------------ */
 /* RHS (rhs_mpi.f90:279-783)                                                */
 /* ------------------------------------------------------------------------ */
+#define ONETHIRD (1.0 / 3.0)
+#define TWOTHIRDS (2.0 / 3.0)
+#define FOURTHIRDS (4.0 / 3.0)
+#define SEVENTHIRDS (7.0 / 3.0)
+
 static void source_theta_terms(orc_ctx *c, const blk_t *B, const double *v1, double *dv1) {
   const css_params *p = &c->p;
-  int mag = p->magnetic;
+  int mag = p->magnetic, lapl = p->laplacian;
   size_t n = c->ncell;
   const double *rhoF = v1, *wF = v1 + n, *vF = v1 + 2 * n, *uF = v1 + 3 * n, *sF = v1 + 4 * n;
   double om2 = 2.0 * p->omega_0;
@@ -949,6 +968,7 @@ static void source_theta_terms(orc_ctx *c, const blk_t *B, const double *v1, dou
 #define SN(j) c->sines[t0 + (j)-1]
 #define CS(j) c->cosines[t0 + (j)-1]
 #define CT(j) (c->cosines[t0 + (j)-1] / c->sines[t0 + (j)-1])
+#define CSC2(j) (1.0 / (c->sines[t0 + (j)-1] * c->sines[t0 + (j)-1]))
       for (int j = 1; j <= m; j++) {
         double rho = PT(rhoF, j), w = PT(wF, j);
         dw[j] = omsq * SN(j) * CS(j);
@@ -960,10 +980,33 @@ static void source_theta_terms(orc_ctx *c, const blk_t *B, const double *v1, dou
       /* dw/dtheta: BC data slot of w is never set (lbct_w = 1, unused) */
       line_deriv(c, B, 1, 1, wF, ip, ir, c->ibct[2], 0.0, 0.0, w1);
       for (int j = 1; j <= m; j++) {
-        double rho = PT(rhoF, j), w = PT(wF, j), v = PT(vF, j);
+        double rho = PT(rhoF, j), w = PT(wF, j);
         w1[j] = w1[j] * ri;
         drho[j] = drho[j] - rho * w1[j];
         dw[j] = dw[j] - w * w1[j];
+      }
+      /* explicit viscosity, w terms (rhs_mpi.f90:844-862); mu6 = mur/rho */
+      double mu6[m + 2], o2[m + 2];
+      if (lapl) {
+        double dlm = c->dlnmu[ir];
+        for (int j = 1; j <= m; j++) {
+          size_t id = IDX(c, t0 + j - 1, ip, ir);
+          double w = PT(wF, j);
+          mu6[j] = c->mur[ir] * c->invrho[id];
+          double ddiff = -FOURTHIRDS * ri * ri;
+          dw[j] = dw[j] + (ddiff * CSC2(j) - ri * dlm) * mu6[j] * w;
+          c->lap[LAP_W1 * n + id] = w1[j];
+          double t1 = w1[j] * mu6[j];
+          ddiff = -ONETHIRD * (7.0 * ri + 2.0 * dlm);
+          du[j] = du[j] + ddiff * (ri * mu6[j] * CT(j) * w + t1);
+          ddiff = FOURTHIRDS * ri;
+          dw[j] = dw[j] + ddiff * CT(j) * t1;
+        }
+        line_deriv(c, B, 1, 2, wF, ip, ir, c->ibct[2], 0.0, 0.0, o2);
+        for (int j = 1; j <= m; j++) dw[j] = dw[j] + FOURTHIRDS * ri * ri * mu6[j] * o2[j];
+      }
+      for (int j = 1; j <= m; j++) {
+        double w = PT(wF, j), v = PT(vF, j);
         dw[j] = dw[j] + v * (ri * CT(j) * v + om2 * CS(j));
         dvv[j] = dvv[j] - ri * v * w * CT(j);
         du[j] = du[j] + v * (ri * v + om2 * SN(j));
@@ -973,9 +1016,23 @@ static void source_theta_terms(orc_ctx *c, const blk_t *B, const double *v1, dou
       hi = (c->cosines[nth - 1] / c->sines[nth - 1]) * vF[IDX(c, nth - 1, ip, ir)];
       line_deriv(c, B, 1, 1, vF, ip, ir, c->ibct[3], lo, hi, w1);
       for (int j = 1; j <= m; j++) {
-        double rho = PT(rhoF, j), w = PT(wF, j), v = PT(vF, j), u = PT(uF, j);
         w1[j] = w1[j] * ri;
-        dvv[j] = dvv[j] - w * w1[j];
+        dvv[j] = dvv[j] - PT(wF, j) * w1[j];
+      }
+      /* explicit viscosity, v terms (rhs_mpi.f90:883-891) */
+      if (lapl) {
+        double dlm = c->dlnmu[ir];
+        for (int j = 1; j <= m; j++) {
+          size_t id = IDX(c, t0 + j - 1, ip, ir);
+          double v = PT(vF, j);
+          dvv[j] = dvv[j] + ri * mu6[j] * (CT(j) * w1[j] - (ri * CSC2(j) + dlm) * v);
+          c->lap[LAP_V1 * n + id] = w1[j];
+        }
+        line_deriv(c, B, 1, 2, vF, ip, ir, c->ibct[3], lo, hi, o2);
+        for (int j = 1; j <= m; j++) dvv[j] = dvv[j] + ri * ri * mu6[j] * o2[j];
+      }
+      for (int j = 1; j <= m; j++) {
+        double rho = PT(rhoF, j), w = PT(wF, j), v = PT(vF, j), u = PT(uF, j);
         PT(dv1, j) = drho[j] - 2.0 * ri * rho * u; /* dvars1(:,:,ir,1) */
         dvv[j] = dvv[j] - u * (ri * v + om2 * SN(j));
         dw[j] = dw[j] - ri * u * w;
@@ -983,9 +1040,23 @@ static void source_theta_terms(orc_ctx *c, const blk_t *B, const double *v1, dou
       }
       line_deriv(c, B, 1, 1, uF, ip, ir, c->ibct[4], 0.0, 0.0, w1);
       for (int j = 1; j <= m; j++) {
-        double w = PT(wF, j);
         w1[j] = w1[j] * ri;
-        du[j] = du[j] - w * w1[j];
+        du[j] = du[j] - PT(wF, j) * w1[j];
+      }
+      /* explicit viscosity, u terms (rhs_mpi.f90:914-926) */
+      if (lapl) {
+        double ddiff = 2.0 * FOURTHIRDS * ri + c->dlnmu[ir];
+        for (int j = 1; j <= m; j++) {
+          size_t id = IDX(c, t0 + j - 1, ip, ir);
+          c->lap[LAP_U1 * n + id] = w1[j];
+          double t1 = w1[j] * mu6[j];
+          dw[j] = dw[j] + ddiff * t1;
+          du[j] = du[j] + ri * CT(j) * t1;
+        }
+        line_deriv(c, B, 1, 2, uF, ip, ir, c->ibct[4], 0.0, 0.0, o2);
+        for (int j = 1; j <= m; j++) du[j] = du[j] + ri * ri * mu6[j] * o2[j];
+      }
+      for (int j = 1; j <= m; j++) {
         if (!mag) dv1[3 * n + IDX(c, t0 + j - 1, ip, ir)] = du[j];
         double t = c->temperature[IDX(c, t0 + j - 1, ip, ir)];
         if (fabs(epsr) > 0.0) ds[j] = epsr * c->invrho[IDX(c, t0 + j - 1, ip, ir)] / t;
@@ -1000,9 +1071,8 @@ static void source_theta_terms(orc_ctx *c, const blk_t *B, const double *v1, dou
         else dv1[1 * n + id] = dw[j] - c->gamm1 * t * w1[j];
         ds[j] = ds[j] - w * w1[j];
       }
-      if (p->slaplacian) {
+      if (c->cond) {
         double ddiff = ri * c->ks[ir];
-        double o2[m + 2];
         for (int j = 1; j <= m; j++) {
           size_t id = IDX(c, t0 + j - 1, ip, ir);
           double oorho = c->invrho[id] / c->temperature[id];
@@ -1055,12 +1125,13 @@ static void source_theta_terms(orc_ctx *c, const blk_t *B, const double *v1, dou
 #undef SN
 #undef CS
 #undef CT
+#undef CSC2
     }
 }
 
 static void phi_terms(orc_ctx *c, const blk_t *B, const double *v1, double *dv1) {
   const css_params *p = &c->p;
-  int mag = p->magnetic;
+  int mag = p->magnetic, lapl = p->laplacian;
   size_t n = c->ncell;
   const double *rhoF = v1, *wF = v1 + n, *vF = v1 + 2 * n, *uF = v1 + 3 * n, *sF = v1 + 4 * n;
 #pragma omp parallel for collapse(2) schedule(static)
@@ -1090,22 +1161,73 @@ static void phi_terms(orc_ctx *c, const blk_t *B, const double *v1, double *dv1)
         dvv[j] = dvv[j] - vF[id] * w1[j];
         dv1[id] = drho[j] - rhoF[id] * w1[j];
         dw[j] = dv1[n + id];
+        du[j] = dv1[3 * n + id];
+      }
+      /* explicit viscosity (rhs_mpi.f90:1123-1199): mu2 = mur/rho; viscous
+       * heating theta-theta/phi-phi, theta-phi; cot = cos * (1/sin) here */
+      double mu2[m + 2], o2[m + 2];
+      double cot = c->cosines[it] * cscth;
+      if (lapl) {
+        for (int j = 1; j <= m; j++) {
+          size_t id = PI_(j);
+          double u = uF[id], w = wF[id], t = c->temperature[id], w1t = c->lap[LAP_W1 * n + id];
+          mu2[j] = c->invrho[id] * c->mur[ir];
+          c->lap[LAP_PV * n + id] = w1[j];
+          ds[j] = ds[j] + FOURTHIRDS * mu2[j] * (w1t + u * ri) * (w1t + 2.0 * u * ri - w1[j] - ri * cot * w) / t;
+          double t1 = w1[j] * mu2[j];
+          double ddiff = -SEVENTHIRDS * ri, ddiff2 = ddiff - TWOTHIRDS * c->dlnmu[ir];
+          dw[j] = dw[j] + ddiff * cot * t1;
+          du[j] = du[j] + ddiff2 * t1;
+        }
+        line_deriv(c, B, 2, 2, vF, it, ir, 0, 0.0, 0.0, o2);
+        for (int j = 1; j <= m; j++) {
+          o2[j] = o2[j] * (oors * oors);
+          dvv[j] = dvv[j] + FOURTHIRDS * o2[j] * mu2[j];
+        }
       }
       line_deriv(c, B, 2, 1, wF, it, ir, 0, 0.0, 0.0, w1);
       for (int j = 1; j <= m; j++) {
         size_t id = PI_(j);
         w1[j] = w1[j] * oors;
         dw[j] = dw[j] - vF[id] * w1[j];
-        du[j] = dv1[3 * n + id];
-        if (!mag) dv1[n + id] = dw[j];
       }
+      if (lapl) {
+        for (int j = 1; j <= m; j++) {
+          size_t id = PI_(j);
+          double v = vF[id], t = c->temperature[id], v1t = c->lap[LAP_V1 * n + id];
+          double q = v1t + w1[j] - ri * cot * v;
+          ds[j] = ds[j] + mu2[j] * (q * q) / t;
+          c->lap[LAP_PW * n + id] = w1[j];
+          dvv[j] = dvv[j] + SEVENTHIRDS * ri * cot * (w1[j] * mu2[j]);
+        }
+        line_deriv(c, B, 2, 2, wF, it, ir, 0, 0.0, 0.0, o2);
+        for (int j = 1; j <= m; j++) {
+          o2[j] = o2[j] * (oors * oors);
+          dw[j] = dw[j] + o2[j] * mu2[j];
+        }
+      }
+      for (int j = 1; j <= m; j++)
+        if (!mag) dv1[n + PI_(j)] = dw[j];
       line_deriv(c, B, 2, 1, uF, it, ir, 0, 0.0, 0.0, w1);
       for (int j = 1; j <= m; j++) {
         size_t id = PI_(j);
         w1[j] = w1[j] * oors;
         du[j] = du[j] - vF[id] * w1[j];
-        if (!mag) dv1[3 * n + id] = du[j];
       }
+      if (lapl) {
+        double ddiff = 2.0 * FOURTHIRDS * ri + c->dlnmu[ir];
+        for (int j = 1; j <= m; j++) {
+          c->lap[LAP_PU * n + PI_(j)] = w1[j];
+          dvv[j] = dvv[j] + ddiff * w1[j] * mu2[j];
+        }
+        line_deriv(c, B, 2, 2, uF, it, ir, 0, 0.0, 0.0, o2);
+        for (int j = 1; j <= m; j++) {
+          o2[j] = o2[j] * (oors * oors);
+          du[j] = du[j] + o2[j] * mu2[j];
+        }
+      }
+      for (int j = 1; j <= m; j++)
+        if (!mag) dv1[3 * n + PI_(j)] = du[j];
       line_deriv(c, B, 2, 1, sF, it, ir, 0, 0.0, 0.0, w1);
       for (int j = 1; j <= m; j++) {
         size_t id = PI_(j);
@@ -1115,7 +1237,7 @@ static void phi_terms(orc_ctx *c, const blk_t *B, const double *v1, double *dv1)
         dvv[j] = dvv[j] - c->gamm1 * t * w1[j];
         if (!mag) dv1[2 * n + id] = dvv[j];
       }
-      if (p->slaplacian) {
+      if (c->cond) {
         line_deriv(c, B, 2, 2, sF, it, ir, 0, 0.0, 0.0, w1);
         double ddiff = c->ks[ir];
         for (int j = 1; j <= m; j++) {
@@ -1151,7 +1273,7 @@ static void phi_terms(orc_ctx *c, const blk_t *B, const double *v1, double *dv1)
 
 static void radial_terms(orc_ctx *c, const blk_t *B, const double *v1, double *dv1) {
   const css_params *p = &c->p;
-  int mag = p->magnetic, nu = p->non_uniform;
+  int mag = p->magnetic, nu = p->non_uniform, lapl = p->laplacian;
   size_t n = c->ncell;
   const double *rhoF = v1, *wF = v1 + n, *vF = v1 + 2 * n, *uF = v1 + 3 * n, *sF = v1 + 4 * n;
 #pragma omp parallel for collapse(2) schedule(static)
@@ -1174,8 +1296,37 @@ static void radial_terms(orc_ctx *c, const blk_t *B, const double *v1, double *d
         if (nu) w1[j] = w1[j] * W3(j);
         dw[j] = dv1[n + id];
         dw[j] = dw[j] - uF[id] * w1[j];
-        if (!mag) dv1[n + id] = dw[j];
+        du[j] = dv1[3 * n + id];
+        ds[j] = dv1[4 * n + id];
       }
+      /* explicit viscosity (rhs_mpi.f90:1317-1435): mu2 = mur/rho, w5 =
+       * 2/r + dlnmu, cot = cos/sin.  The cot(theta) u_theta' / (3 r) term of
+       * du carries no mur/rho, and the r-theta heating is added once with
+       * dv/dr and once with du/dr, both as the reference writes them. */
+      double mu2[m + 2], o2[m + 2];
+      double cot = c->cosines[it] / c->sines[it];
+#define W5(j) (2.0 * c->r_inv[r0 + (j)-1] + c->dlnmu[r0 + (j)-1])
+#define RV(j) c->r_inv[r0 + (j)-1]
+      if (lapl) {
+        for (int j = 1; j <= m; j++) {
+          size_t id = RI_(j);
+          int ir = r0 + j - 1;
+          mu2[j] = c->mur[ir] * c->invrho[id];
+          du[j] = du[j] + ONETHIRD * cot * RV(j) * w1[j];
+          dw[j] = dw[j] + mu2[j] * W5(j) * w1[j];
+          double q = w1[j] + c->lap[LAP_U1 * n + id] - wF[id] * RV(j);
+          ds[j] = ds[j] + mu2[j] * (q * q) / c->temperature[id];
+        }
+        if (nu)
+          for (int j = 1; j <= m; j++) dw[j] = dw[j] + W9(j) * w1[j] * mu2[j];
+        line_deriv(c, B, 0, 2, wF, it, ip, c->ibcr[2], lo, hi, o2);
+        for (int j = 1; j <= m; j++) {
+          if (nu) o2[j] = o2[j] * (W3(j) * W3(j));
+          dw[j] = dw[j] + o2[j] * mu2[j];
+        }
+      }
+      for (int j = 1; j <= m; j++)
+        if (!mag) dv1[n + RI_(j)] = dw[j];
       lo = 0.0;
       if (p->bottom_stress_free) lo = vF[IDX(c, it, ip, 0)] / p->r1 / c->dxdr[0];
       if (p->top_stress_free) hi = vF[IDX(c, it, ip, nr - 1)] / p->r2 / c->dxdr[nr - 1];
@@ -1186,25 +1337,58 @@ static void radial_terms(orc_ctx *c, const blk_t *B, const double *v1, double *d
         if (nu) w1[j] = w1[j] * W3(j);
         dvv[j] = dv1[2 * n + id];
         dvv[j] = dvv[j] - uF[id] * w1[j];
-        if (!mag) dv1[2 * n + id] = dvv[j];
-        du[j] = dv1[3 * n + id];
       }
+      if (lapl) {
+        for (int j = 1; j <= m; j++) {
+          size_t id = RI_(j);
+          double q = w1[j] + c->lap[LAP_PU * n + id] - vF[id] * RV(j);
+          ds[j] = ds[j] + mu2[j] * (q * q) / c->temperature[id];
+          dvv[j] = dvv[j] + w1[j] * W5(j) * mu2[j];
+          if (nu) dvv[j] = dvv[j] + W9(j) * w1[j] * mu2[j];
+        }
+        line_deriv(c, B, 0, 2, vF, it, ip, c->ibcr[3], lo, hi, o2);
+        for (int j = 1; j <= m; j++) {
+          if (nu) o2[j] = o2[j] * (W3(j) * W3(j));
+          dvv[j] = dvv[j] + o2[j] * mu2[j];
+        }
+      }
+      for (int j = 1; j <= m; j++)
+        if (!mag) dv1[2 * n + RI_(j)] = dvv[j];
       line_deriv(c, B, 0, 1, uF, it, ip, c->ibcr[4], 0.0, 0.0, w1);
       for (int j = 1; j <= m; j++) {
         size_t id = RI_(j);
         if (nu) w1[j] = w1[j] * W3(j);
         du[j] = du[j] - uF[id] * w1[j];
         dv1[id] = dv1[id] - rhoF[id] * w1[j];
-        ds[j] = dv1[4 * n + id];
       }
+      if (lapl) {
+        for (int j = 1; j <= m; j++) {
+          size_t id = RI_(j);
+          double u = uF[id], v = vF[id], w = wF[id], t = c->temperature[id];
+          du[j] = du[j] + FOURTHIRDS * mu2[j] * W5(j) * (w1[j] - u * RV(j));
+          if (nu) du[j] = du[j] + FOURTHIRDS * W9(j) * w1[j] * mu2[j];
+          ds[j] = ds[j] + FOURTHIRDS * mu2[j] * w1[j] * (w1[j] - c->lap[LAP_W1 * n + id] - u * RV(j)) / t;
+          double q = w1[j] + c->lap[LAP_PU * n + id] - v * RV(j);
+          ds[j] = ds[j] + mu2[j] * (q * q) / t;
+          double a = c->lap[LAP_PV * n + id] + (cot * w + u) * RV(j);
+          ds[j] = ds[j] + FOURTHIRDS * mu2[j] * a * (a - w1[j]) / t;
+        }
+        line_deriv(c, B, 0, 2, uF, it, ip, c->ibcr[4], 0.0, 0.0, o2);
+        for (int j = 1; j <= m; j++) {
+          if (nu) o2[j] = o2[j] * (W3(j) * W3(j));
+          du[j] = du[j] + FOURTHIRDS * o2[j] * mu2[j];
+        }
+      }
+#undef W5
+#undef RV
       /* ds/dr with the constant-flux datum (rhs_mpi.f90:584-592, :616-624) */
       lo = 0.0; hi = 0.0;
       if (!p->bottom_constant_temp) {
-        if (p->slaplacian) lo = -p->lumr1 * ONE_OVER_4PI / (p->r1 * p->r1 * c->ks[0] * c->dxdr[0]);
+        if (c->cond) lo = -p->lumr1 * ONE_OVER_4PI / (p->r1 * p->r1 * c->ks[0] * c->dxdr[0]);
         else lo = 0.0 / c->dxdr[0]; /* dsdr1 = dsdrm(1) = 0 for the Isentropic model */
       }
       if (!p->top_constant_temp) {
-        if (p->slaplacian) hi = -p->lumr2 * ONE_OVER_4PI / (p->r2 * p->r2 * c->ks[nr - 1] * c->dxdr[nr - 1]);
+        if (c->cond) hi = -p->lumr2 * ONE_OVER_4PI / (p->r2 * p->r2 * c->ks[nr - 1] * c->dxdr[nr - 1]);
         else hi = 0.0 / c->dxdr[nr - 1];
       }
       line_deriv(c, B, 0, 1, sF, it, ip, c->ibcr[5], lo, hi, w1);
@@ -1215,8 +1399,7 @@ static void radial_terms(orc_ctx *c, const blk_t *B, const double *v1, double *d
         du[j] = du[j] - c->gamm1 * t * w1[j];
         ds[j] = ds[j] - uF[id] * w1[j];
       }
-      if (p->slaplacian) {
-        double o2[m + 2];
+      if (c->cond) {
         for (int j = 1; j <= m; j++) {
           size_t id = RI_(j);
           int ir = r0 + j - 1;
@@ -1340,6 +1523,94 @@ static void density_terms_radial(orc_ctx *c, const blk_t *B, const double *v1, d
     }
 }
 
+/* Laplacian_Cross_Terms_Radial (rhs_mpi.f90:2070-2205): radial derivatives
+ * of r*X for the sweeps' X = ri dw/dth, du/dph/(r sin), ri du/dth and
+ * dv/dph/(r sin), added with mur/(3 r rho) to du, dv, dw, du.  Interior block
+ * faces read the neighbours' r*X (Boundary_Exchange_Lapl(1)).  At physical
+ * faces the data are r1 (or r2) times the exchange buffer, which the
+ * reference fills only for stress-free walls: X1/r1/dxdr(1) on the bottom and
+ * X4/r2/dxdr(nr) on the top, both under Bottom_Stress_Free as written
+ * (:2112-2124); the other slots are never written for a hydro run and are
+ * taken as 0 here.  The reference scales by invrho(it+ir-1, ip, :) with it
+ * undefined (:2130); the cell's own 1/rho is used. */
+static void lap_cross_radial(orc_ctx *c, double *dv1) {
+  const css_params *p = &c->p;
+  size_t n = c->ncell, np = (size_t)c->nth * c->nphi;
+  int nr = c->nr, nu = p->non_uniform;
+  static const int src[4] = {LAP_W1, LAP_PU, LAP_U1, LAP_PV};
+  double *F = dalloc(4 * n);
+  for (int k = 0; k < 4; k++)
+    for (size_t i = 0; i < n; i++) F[k * n + i] = c->r_ind[i / np] * c->lap[src[k] * n + i];
+  const int bc[4] = {c->ibcr[2], c->ibcr[4], c->ibcr[4], c->ibcr[3]};
+  for (int kb = 0; kb < c->nblk; kb++) {
+    const blk_t *B = &c->blk[kb];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+      for (int it = B->t0; it < B->t0 + B->nt; it++) {
+        int m = B->nr, r0 = B->r0;
+        double o[4][m + 2];
+        for (int k = 0; k < 4; k++) {
+          double lo = 0.0, hi = 0.0;
+          if (k == 0 && p->bottom_stress_free)
+            lo = p->r1 * (c->lap[LAP_W1 * n + IDX(c, it, ip, 0)] / p->r1 / c->dxdr[0]);
+          if (k == 3 && p->bottom_stress_free)
+            hi = p->r2 * (c->lap[LAP_PV * n + IDX(c, it, ip, nr - 1)] / p->r2 / c->dxdr[nr - 1]);
+          line_deriv(c, B, 0, 1, F + k * n, it, ip, bc[k], lo, hi, o[k]);
+          if (nu)
+            for (int j = 1; j <= m; j++) o[k][j] = o[k][j] * c->dxdr[r0 + j - 1];
+        }
+        for (int j = 1; j <= m; j++) {
+          int ir = r0 + j - 1;
+          size_t id = IDX(c, it, ip, ir);
+          double w6 = ONETHIRD * c->mur[ir] * c->r_inv[ir] * c->invrho[id];
+          double du = dv1[3 * n + id] + w6 * o[0][j];
+          dv1[2 * n + id] = dv1[2 * n + id] + w6 * o[1][j];
+          dv1[n + id] = dv1[n + id] + w6 * o[2][j];
+          dv1[3 * n + id] = du + w6 * o[3][j];
+        }
+      }
+  }
+  free(F);
+}
+
+/* Laplacian_Cross_Terms_Theta (rhs_mpi.f90:2207-2296): theta derivatives of
+ * sin(theta) dv/dph/(r sin) and sin(theta) dw/dph/(r sin), added with
+ * mur/(3 r rho sin) to dw and dv.  Wall data of the first: sin * (X cos/sin)
+ * at the wall (:2241-2250); of the second: never written, 0. */
+static void lap_cross_theta(orc_ctx *c, double *dv1) {
+  size_t n = c->ncell;
+  int nth = c->nth;
+  double *F = dalloc(2 * n);
+  for (size_t i = 0; i < n; i++) {
+    double sn = c->sines[i % nth];
+    F[i] = sn * c->lap[LAP_PV * n + i];
+    F[n + i] = sn * c->lap[LAP_PW * n + i];
+  }
+  for (int kb = 0; kb < c->nblk; kb++) {
+    const blk_t *B = &c->blk[kb];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int ir = B->r0; ir < B->r0 + B->nr; ir++)
+      for (int ip = B->p0; ip < B->p0 + B->np; ip++) {
+        int m = B->nt, t0 = B->t0;
+        double o[2][m + 2];
+        double pv0 = c->lap[LAP_PV * n + IDX(c, 0, ip, ir)], pv1 = c->lap[LAP_PV * n + IDX(c, nth - 1, ip, ir)];
+        double lo = c->sines[0] * (pv0 * c->cosines[0] / c->sines[0]);
+        double hi = c->sines[nth - 1] * (pv1 * c->cosines[nth - 1] / c->sines[nth - 1]);
+        line_deriv(c, B, 1, 1, F, ip, ir, c->ibct[3], lo, hi, o[0]);
+        line_deriv(c, B, 1, 1, F + n, ip, ir, c->ibct[2], 0.0, 0.0, o[1]);
+        double ri = c->r_inv[ir] * c->mur[ir];
+        for (int j = 1; j <= m; j++) {
+          int it = t0 + j - 1;
+          size_t id = IDX(c, it, ip, ir);
+          double w4 = ONETHIRD * ri * c->invrho[id] / c->sines[it];
+          dv1[n + id] = dv1[n + id] + w4 * o[0][j];
+          dv1[2 * n + id] = dv1[2 * n + id] + w4 * o[1][j];
+        }
+      }
+  }
+  free(F);
+}
+
 static void thermo(orc_ctx *c, const double *v1) {
   size_t n = c->ncell;
   /* rhs_mpi.f90:376-387 */
@@ -1371,6 +1642,10 @@ int orc_rhs(orc_ctx *c, double *vars1, double *dvars1, int call_num) {
   for (int k = 0; k < c->nblk; k++) source_theta_terms(c, &c->blk[k], vars1, dvars1);
   for (int k = 0; k < c->nblk; k++) phi_terms(c, &c->blk[k], vars1, dvars1);
   for (int k = 0; k < c->nblk; k++) radial_terms(c, &c->blk[k], vars1, dvars1);
+  if (c->p.laplacian) {
+    lap_cross_radial(c, dvars1);
+    lap_cross_theta(c, dvars1);
+  }
   for (int k = 0; k < c->nblk; k++) density_terms_theta(c, &c->blk[k], vars1, dvars1);
   for (int k = 0; k < c->nblk; k++) density_terms_radial(c, &c->blk[k], vars1, dvars1);
   if (c->p.magnetic) {
@@ -1565,7 +1840,7 @@ static void diffusion_r(orc_ctx *c, const blk_t *B, const vcc_t *V, const double
             break;
           case 4: for (int k = 1; k <= 4; k++) b1[k] = tmp[1]; break;
           case 5:
-            if (!p->bottom_constant_temp && p->slaplacian) {
+            if (!p->bottom_constant_temp && c->cond) {
               double q = p->lumr1 * ONE_OVER_4PI / (p->r1 * p->r1 * c->ks[0] * c->dxdr[0]);
               b1[1] = tmp[1] + 4.0 * dri[0] * q; b1[2] = tmp[1] + 3.0 * dri[0] * q;
               b1[3] = tmp[1] + 2.0 * dri[0] * q; b1[4] = tmp[1] + dri[0] * q;
@@ -1588,7 +1863,7 @@ static void diffusion_r(orc_ctx *c, const blk_t *B, const vcc_t *V, const double
             break;
           case 4: for (int k = 1; k <= 4; k++) b2[k] = tmp[m]; break;
           case 5:
-            if (!p->top_constant_temp && p->slaplacian) {
+            if (!p->top_constant_temp && c->cond) {
               double q = p->lumr2 * ONE_OVER_4PI / (p->r2 * p->r2 * c->ks[nr - 1] * c->dxdr[nr - 1]);
               b2[1] = tmp[m] - dri[0] * q; b2[2] = tmp[m] - 2.0 * dri[0] * q;
               b2[3] = tmp[m] - 3.0 * dri[0] * q; b2[4] = tmp[m] - 4.0 * dri[0] * q;
@@ -2132,6 +2407,16 @@ int orc_step_size(orc_ctx *c, const double *vars0, double cfl_safety, double *ou
     }
   }
   double dtmaxd = 1e10;
+  if (c->p.laplacian) { /* rhs_mpi.f90:194-198 (etar = ks, mhdsph_mpi.f90:349) */
+    double drmin = c->dr_ind[0], ksmax = c->ks[0], mumax = c->mur[0] / c->rhor[0];
+    for (int ir = 1; ir < c->nr; ir++) {
+      drmin = fmin(drmin, c->dr_ind[ir]);
+      ksmax = fmax(ksmax, c->ks[ir]);
+      mumax = fmax(mumax, c->mur[ir] / c->rhor[ir]);
+    }
+    double h = fmin(drmin, c->p.r1 * fmin(fmin(c->sines[0], c->sines[c->nth - 1]) * c->dphi, c->dth));
+    dtmaxd = h * h / fmax(fmax(ksmax, mumax), ksmax);
+  }
   out[0] = fmin(fmin(dtmaxb, dtmaxc), dtmaxd) * cfl_safety;
   out[1] = etot; out[2] = ltot; out[3] = mtot; out[4] = mrsint;
   free(b);
@@ -2202,7 +2487,7 @@ int orc_shell_averages(orc_ctx *c, const double *vars0, const int *q, int nq, co
       switch (q[iq]) {
         case 4: v = c->gamm1 * c->cv * s / nsize; break;
         case 5: v = avgvr; break;
-        case 15: v = (p->slaplacian ? -c->ks[ir] * s / nsize : 0.0) + (k0 ? k0[ir] : 0.0); break;
+        case 15: v = (c->cond ? -c->ks[ir] * s / nsize : 0.0) + (k0 ? k0[ir] : 0.0); break;
         case 16: v = p->cp * s / nsize; break;
         default: v = s / nsize;
       }
