@@ -1532,7 +1532,7 @@ static void density_terms_radial(orc_ctx *c, const blk_t *B, const double *v1, d
  * X4/r2/dxdr(nr) on the top, both under Bottom_Stress_Free as written
  * (:2112-2124); the other slots are never written for a hydro run and are
  * taken as 0 here.  The reference scales by invrho(it+ir-1, ip, :) with it
- * undefined (:2130); the cell's own 1/rho is used. */
+ * undefined (:2133); the cell's own 1/rho is used. */
 static void lap_cross_radial(orc_ctx *c, double *dv1) {
   const css_params *p = &c->p;
   size_t n = c->ncell, np = (size_t)c->nth * c->nphi;
