@@ -63,6 +63,8 @@ struct css_ctx {
   double *tbuf;                     // temperature of the current stage input
   double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
   double *lapface = nullptr;        // explicit viscosity: face data, 6 x max face size
+  double *radbuf = nullptr;         // radiative diffusion: d ln(rho)/dr, ds/dr, 8 derivative fields
+  double *radface = nullptr;        // radiative diffusion: face data, 6 x max face size
   double dtd = 1e10;                // viscous time-step limit of Compute_Step_Size
   double rep_flux_lo = 0.0, rep_flux_hi = 0.0;  // dsdr1/dxdr(1), dsdr2/dxdr(nr) of the reports
   int mt[3];                        // compile-time block length per direction (0 = generic)
@@ -233,7 +235,7 @@ extern "C" void css_destroy(css_ctx *c) {
   cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo); cudaFree(c->resp);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
   cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf);
-  cudaFree(c->lapbuf); cudaFree(c->lapface);
+  cudaFree(c->lapbuf); cudaFree(c->lapface); cudaFree(c->radbuf); cudaFree(c->radface);
   for (auto e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -341,6 +343,10 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   }
   if (p.precision != 0 && p.precision != 1) {
     set_err("css_create: precision %d unknown (0 FP64, 1 mixed: FP32 stage states)", p.precision);
+    return CSS_ERR_ARG;
+  }
+  if (p.do_radheat && p.precision != 0) {
+    set_err("css_create: radiative diffusion runs in FP64 only");
     return CSS_ERR_ARG;
   }
   if (p.laplacian && (p.magnetic || p.precision != 0)) {
@@ -538,7 +544,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   }
   c->stream = c->own_stream;
   // radial profile block: r_ind r_inv dr_ind dxdr d2xdr2 rhor sr grav ks dlnks eps dspeed mur dlnmu
-  std::vector<double> R((size_t)14 * nr);
+  std::vector<double> R((size_t)16 * nr);
   for (int i = 0; i < nr; i++) {
     R[0 * nr + i] = r_ind[i];
     R[1 * nr + i] = 1.0 / r_ind[i];
@@ -554,6 +560,8 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     R[11 * nr + i] = dspeed[i];
     R[12 * nr + i] = P[CSS_PROF_MUR * nr + i];
     R[13 * nr + i] = P[CSS_PROF_DLNMU * nr + i];
+    R[14 * nr + i] = P[CSS_PROF_KR * nr + i];
+    R[15 * nr + i] = P[CSS_PROF_DLNKR * nr + i];
   }
   if (p.laplacian) {
     // dtmaxd of Compute_Step_Size (rhs_mpi.f90:194-198; etar = ks there)
@@ -628,6 +636,11 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     ALLOC(c->lapbuf, 12 * c->ncell * sizeof(double));
     ALLOC(c->lapface, 6 * nf * sizeof(double));
   }
+  if (p.do_radheat) {
+    size_t nf = std::max((size_t)nth * nphi, (size_t)nphi * nr);
+    ALLOC(c->radbuf, 10 * c->ncell * sizeof(double));
+    ALLOC(c->radface, 6 * nf * sizeof(double));
+  }
   cudaMemcpy(c->tab, T.data(), T.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->prof, R.data(), R.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->theta_prof, TH.data(), TH.size() * 8, cudaMemcpyHostToDevice);
@@ -641,6 +654,9 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   g.d2xdr2 = c->prof + 4 * nr; g.rhor = c->prof + 5 * nr; g.sr = c->prof + 6 * nr; g.grav = c->prof + 7 * nr;
   g.ks = c->prof + 8 * nr; g.dlnks = c->prof + 9 * nr; g.eps = c->prof + 10 * nr; g.dspeed = c->prof + 11 * nr;
   g.mur = c->prof + 12 * nr; g.dlnmu = c->prof + 13 * nr;
+  g.kr = c->prof + 14 * nr; g.dlnkr = c->prof + 15 * nr;
+  g.radheat = p.do_radheat;
+  if (p.do_radheat) { g.rad_lnrho_r = c->radbuf; g.rad_dsdr = c->radbuf + c->ncell; }
   g.sines = c->theta_prof; g.cosines = c->theta_prof + nth; g.theta = c->theta_prof + 2 * nth;
   g.cot = c->theta_prof + 3 * nth; g.csc = c->theta_prof + 4 * nth;
   g.sld_th = c->sld_geo; g.sld_r = c->sld_geo + 5 * (size_t)nth;
@@ -787,6 +803,34 @@ static int launch_lap(css_ctx *c, const double *cur) {
   return check_launch(c);
 }
 
+// radiative diffusion: the heating of all three directions added into ds,
+// after the radial kernel and before the density-theta / update kernel
+static int launch_rad(css_ctx *c, const double *cur) {
+  const CssGeo &g = c->g;
+  const size_t n = c->ncell;
+  const size_t nf = std::max((size_t)g.nth * g.nphi, (size_t)g.nphi * g.nr);
+  double *S = c->radbuf + 2 * n, *F = c->radface;
+  const double *rho = cur, *T = c->tbuf;
+  const int nbp = (int)std::min<size_t>((n + 255) / 256, (size_t)c->nsm * 8);
+  const int nbf = (int)std::min<size_t>((nf + 255) / 256, (size_t)c->nsm * 8);
+  cudaStream_t st = c->stream;
+  k_rad_bc<<<nbf, 256, 0, st>>>(g, cur, c->dv, T, F, F + nf, F + 2 * nf, F + 3 * nf, F + 4 * nf, F + 5 * nf);
+  if (int rc = check_launch(c)) return rc;
+#define RAD_D(dir, ord, x, out, lo, hi, bdry) \
+  if (int rc = css_deriv_dev(c, dir, ord, x, out, lo, hi, bdry, nullptr)) return rc
+  RAD_D(1, 1, rho, S, F, F + nf, g.ibct[1]);
+  RAD_D(1, 1, T, S + n, F + 2 * nf, F + 3 * nf, g.ibct[6]);
+  RAD_D(1, 2, T, S + 2 * n, F + 2 * nf, F + 3 * nf, g.ibct[6]);
+  RAD_D(2, 1, rho, S + 3 * n, nullptr, nullptr, 0);
+  RAD_D(2, 1, T, S + 4 * n, nullptr, nullptr, 0);
+  RAD_D(2, 2, T, S + 5 * n, nullptr, nullptr, 0);
+  RAD_D(0, 1, T, S + 6 * n, F + 4 * nf, F + 5 * nf, g.ibcr[6]);
+  RAD_D(0, 2, T, S + 7 * n, F + 4 * nf, F + 5 * nf, g.ibcr[6]);
+#undef RAD_D
+  k_rad_point<<<nbp, 256, 0, st>>>(g, cur, T, S, c->dv);
+  return check_launch(c);
+}
+
 template <typename TS, typename TO>
 static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur, double ca = 0.0, double cb = 0.0,
                       double dsld = 0.0) {
@@ -831,6 +875,10 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   LAUNCH_MT(0, TL, k_radial_terms, (TS), gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
+  if constexpr (sizeof(TS) == 8) {
+    if (c->p.do_radheat)
+      if (int rc = launch_rad(c, (const double *)cur)) return rc;
+  }
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_RHOT_UPDATE);
@@ -1493,6 +1541,10 @@ extern "C" int css_shell_averages(css_ctx *c, const int *quantities, int nq, con
     const int q = quantities[iq];
     if (q < 1 || q > 18) {
       set_err("css_shell_averages: quantity %d not supported (1..18; 19 needs the SLD flux output)", q);
+      return CSS_ERR_ARG;
+    }
+    if (q == 15 && c->p.do_radheat) {
+      set_err("css_shell_averages: F_ks of a radiative-diffusion run (the kr T^3 dT/dr term) is not built");
       return CSS_ERR_ARG;
     }
     if (q >= 10 && q <= 14 && !c->p.magnetic) {

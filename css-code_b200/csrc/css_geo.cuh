@@ -31,6 +31,11 @@ struct CssGeo {
   // radial profiles (length nr)
   const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
   const double *mur, *dlnmu;  // viscosity and its log-derivative (explicit-viscosity path)
+  const double *kr, *dlnkr;   // inverse opacity and the reference's dlnkr (radiative diffusion)
+  // radiative diffusion: when set, the radial kernel keeps d ln(rho)/dr (after
+  // the density datum) and ds/dr of every cell for the radiative pass
+  double *rad_lnrho_r, *rad_dsdr;
+  int radheat;
   // per-cell SLD speed^2 replacing dspeed (a learned closure's output);
   // NULL, or a negative entry, means the prescribed radial profile
   const double *speed2;

@@ -850,7 +850,11 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
       drho = drho - q.u * w1;
       w1 = w1 * (1.0 / q.rho);
       du = du - g.pconst * q.t * w1;
-      if (phys == 2 && j == m - 1 && !g.set_stop) {  // rhs_mpi.f90:1807-1818
+      if (g.rad_lnrho_r) {  // kept for the radiative pass (rhs_mpi.f90:1454, :1821)
+        g.rad_lnrho_r[id] = w1;
+        g.rad_dsdr[id] = g.non_uniform ? q.ds_r * g.dxdr[ir] : q.ds_r;
+      }
+      if (phys == 2 && j == m - 1 && !g.set_stop && !g.radheat) {  // rhs_mpi.f90:1807-1818
         drho = drho + q.rho * (g.t0 - q.t) / (g.damping_time * (g.gamma - 2.0) * q.t);
         ds = ds - g.cv * (g.t0 - q.t) / (g.damping_time * (g.gamma - 2.0) * q.t);
       }

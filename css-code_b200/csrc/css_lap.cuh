@@ -1,4 +1,6 @@
-// css_lap.cuh -- explicit viscosity (the reference's Laplacian switch).
+// css_lap.cuh -- explicit viscosity (the reference's Laplacian switch) and
+// radiative diffusion (do_radheat), the two diffusion options that run as a
+// pass of line derivatives plus pointwise kernels around the fused sweeps.
 //
 // The viscous terms of Source_Theta_Terms (rhs_mpi.f90:844-927), Phi_Terms
 // (:1123-1199) and Radial_Terms (:1317-1435), and the cross terms of
@@ -241,6 +243,83 @@ __global__ void k_lap_cross(CssGeo g, const double *__restrict__ cur, const doub
     dv[n + id] = dw;
     dv[2 * n + id] = dvv;
     dv[3 * n + id] = du;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Radiative diffusion (do_radheat): ds += coef [T''/T + T'/T (geometry +
+// 3 T'/T - rho'/rho)] per direction, coef = (4 a c kr / 3) T^3 / rho^2
+// (rhs_mpi.f90:388-392), as Phi_Terms (:1092-1106), Density_Terms_Theta
+// (:1590-1602) and Density_Terms_Radial (:1820-1853) write it.  The pass
+// runs after the radial kernel: the theta density datum reads the final dw
+// (the same value the density-theta update kernel reads next), and the
+// radial kernel has kept d ln(rho)/dr (its density datum built from du
+// before the density term changed it) and ds/dr.
+// ---------------------------------------------------------------------------
+#define RAD_AC (7.56577e-15 * 2.99792458e10)  // a_const * c_light, constants.f90:7
+
+// face data: theta [ip + nphi*ir]: the hydrostatic datum of d(rho)/dth,
+// r/(pconst) dw rho / T (rhs_mpi.f90:1553-1564), and T on the walls;
+// r [it + nth*ip]: the datum of dT/dr, T ((gamma-1) dlnrho/dr + ds/dr / Cv)
+// / dxdr on the walls (:1822-1831)
+__global__ void k_rad_bc(CssGeo g, const double *__restrict__ cur, const double *__restrict__ dv,
+                         const double *__restrict__ tb, double *__restrict__ rlo_t, double *__restrict__ rhi_t,
+                         double *__restrict__ tlo_t, double *__restrict__ thi_t, double *__restrict__ tlo_r,
+                         double *__restrict__ thi_r) {
+  const size_t n = (size_t)g.ncell, nfr = (size_t)g.nth * g.nphi, nft = (size_t)g.nphi * g.nr;
+  const size_t nf = nfr > nft ? nfr : nft;
+  const int nr = g.nr, nth = g.nth;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nf; k += (size_t)gridDim.x * blockDim.x) {
+    if (k < nft) {
+      const int ip = (int)(k % g.nphi), ir = (int)(k / g.nphi);
+      const double rv = g.r_ind[ir] * g.invpconst;
+      const size_t a = css_idx(g, 0, ip, ir), b = css_idx(g, nth - 1, ip, ir);
+      rlo_t[k] = rv * dv[n + a] * cur[a] / tb[a];
+      rhi_t[k] = rv * dv[n + b] * cur[b] / tb[b];
+      tlo_t[k] = tb[a];
+      thi_t[k] = tb[b];
+    }
+    if (k < nfr) {
+      const size_t a = k, b = (size_t)(nr - 1) * nfr + k;
+      tlo_r[k] = tb[a] * (g.gamm1 * g.rad_lnrho_r[a] + g.invcv * g.rad_dsdr[a]) / g.dxdr[0];
+      thi_r[k] = tb[b] * (g.gamm1 * g.rad_lnrho_r[b] + g.invcv * g.rad_dsdr[b]) / g.dxdr[nr - 1];
+    }
+  }
+}
+
+// S: d rho/dth, dT/dth, d2T/dth2, d rho/dph, dT/dph, d2T/dph2, dT/dx, d2T/dx2
+__global__ void k_rad_point(CssGeo g, const double *__restrict__ cur, const double *__restrict__ tb,
+                            const double *__restrict__ S, double *__restrict__ dv) {
+  const size_t n = (size_t)g.ncell;
+  const int nu = g.non_uniform;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x) {
+    int it, ip, ir;
+    lap_cell(g, id, it, ip, ir);
+    const double t = tb[id], invrho = 1.0 / cur[id], ri = g.r_inv[ir];
+    const double coef = (4.0 * RAD_AC * g.kr[ir] / 3.0) * (t * t * t) * (invrho * invrho);
+    double ds = dv[4 * n + id];
+    // phi
+    const double oors = ri * g.csc[it];
+    const double w = (S[3 * n + id] * oors) * invrho;
+    double a = S[4 * n + id] * oors / t;
+    ds = ds + coef * (3.0 * a - w) * a;
+    ds = ds + coef * (S[5 * n + id] * (oors * oors)) / t;
+    // theta
+    const double rho_t = (ri * S[id]) * invrho;
+    a = ri * S[n + id] / t;
+    ds = ds + coef * a * (3.0 * a + ri * g.cot[it] - rho_t);
+    ds = ds + (ri * ri) * coef * S[2 * n + id] / t;
+    // r
+    const double dx = g.dxdr[ir];
+    a = S[6 * n + id];
+    if (nu) a = a * dx;
+    a = a / t;
+    ds = ds + coef * a * ((2.0 * ri - g.dlnkr[ir]) + 3.0 * a - g.rad_lnrho_r[id]);
+    if (nu) ds = ds + coef * a * (g.d2xdr2[ir] / dx);
+    double d2 = S[7 * n + id];
+    if (nu) d2 = d2 * (dx * dx);
+    ds = ds + coef * d2 / t;
+    dv[4 * n + id] = ds;
   }
 }
 

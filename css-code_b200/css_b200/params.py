@@ -33,6 +33,7 @@ _FIELDS = [
     ("precision", ctypes.c_int),
     ("time_stepper", ctypes.c_int),
     ("laplacian", ctypes.c_int),
+    ("do_radheat", ctypes.c_int),
 ]
 
 
@@ -52,9 +53,9 @@ class CssParams(ctypes.Structure):
         return {k: getattr(self, k) for k, _ in _FIELDS}
 
 
-NPROF = 13  # CSS_NPROF
+NPROF = 15  # CSS_NPROF
 PROF_NAMES = ["x_ind", "r_ind", "dr_ind", "dxdr", "d2xdr2", "rhor", "sr", "gravity", "ks", "dlnks", "eps",
-              "mur", "dlnmu"]
+              "mur", "dlnmu", "kr", "dlnkr"]
 
 
 def default_params(nr, nth, nphi, decomp, magnetic=False):

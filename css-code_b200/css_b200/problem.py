@@ -24,6 +24,7 @@ import numpy as np
 from .params import NPROF
 
 GCONST = 6.67e-8  # the reference's Gconst (mhdsph_mpi.f90:318)
+A_CONST, C_LIGHT = 7.56577e-15, 2.99792458e10  # constants.f90:7
 
 
 def tanh_grid(nr, r1, r2, stretch=1.0):
@@ -88,11 +89,22 @@ def polytrope(p, n_rho, stretch=1.0, kappa=None, ra=1e5, pr=1.0, g0_exp=0.0, del
     # viscosity of the explicit-viscosity path (mhdsph_mpi.f90:352-354)
     mur = p.sld_pr * kappa * rhor
     dlnmu = -alp * r2 * r_inv ** 2 / base / gamm1
-    prof = np.stack([x, r, dr, dxdr, d2xdr2, rhor, sr, gravity, ks, dlnks, eps, mur, dlnmu]).astype(np.float64)
-    assert prof.shape[0] == NPROF
     lum = delta * cp / d * 4.0 * math.pi * r1 ** 2 * ks[0]
     p.lumr1 = lum
     p.lumr2 = lum
+    # radiative diffusion (mhdsph_mpi.f90:365-386): kr carries the luminosity
+    # on the background gradient, kr = 1 / [-16 pi a c r^2 T^3 g / (3 rho L)]
+    # with g = T (dsdr/Cp - (gamma-1) rho gravity / (gamma P)) = -G mstar /
+    # (Cp r^2) for the isentropic polytrope.  The reference differentiates
+    # ln of the bracket with Dbyd1_dt0; the polytrope's closed form is used
+    # here: d/dr ln[...] = (3 - 1/(gamma-1)) d ln(base)/dr (L constant).
+    g_bg = -GCONST * mstar / (cp * r ** 2)
+    kr_inv = -16.0 * math.pi * A_CONST * C_LIGHT * r ** 2 * tr ** 3 * g_bg / (3.0 * rhor * lum)
+    kr = 1.0 / kr_inv
+    dlnkr = (3.0 - 1.0 / gamm1) * (-alp * r2 * r_inv ** 2) / base
+    prof = np.stack([x, r, dr, dxdr, d2xdr2, rhor, sr, gravity, ks, dlnks, eps, mur, dlnmu, kr,
+                     dlnkr]).astype(np.float64)
+    assert prof.shape[0] == NPROF
     info = dict(alp=alp, mstar=mstar, kappa=kappa, rho0=rho0, tr=tr, lum=lum)
     return np.ascontiguousarray(prof.reshape(-1)), info
 

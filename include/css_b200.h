@@ -59,6 +59,8 @@ enum {
   CSS_PROF_EPS,       /* internal heating eps                                */
   CSS_PROF_MUR,       /* dynamic viscosity mur (explicit-viscosity path)     */
   CSS_PROF_DLNMU,     /* d ln mur / dr                                       */
+  CSS_PROF_KR,        /* inverse Rosseland opacity kr (radiative diffusion)  */
+  CSS_PROF_DLNKR,     /* dlnkr as the reference keeps it: d ln(1/kr) / dr    */
   CSS_NPROF
 };
 
@@ -101,6 +103,9 @@ typedef struct css_params {
                                  rhs_mpi.f90:844-927, :1123-1199, :1317-1435,
                                  :2070-2296); also turns the entropy
                                  conduction on, as SLaplacian does           */
+  int do_radheat;             /* 1: radiative diffusion of heat (rhs_mpi.f90:
+                                 388-393, :1092-1106, :1590-1602, :1820-1853);
+                                 also turns the top thermal damping off      */
 } css_params;
 
 typedef struct css_ctx css_ctx;

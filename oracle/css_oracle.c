@@ -28,6 +28,8 @@
 #define PI 3.1415926535897932384626433832795028841972
 #define ONE_OVER_4PI (1.0 / PI / 4.0)
 #define ONETHIRD (1.0 / 3.0)
+#define A_CONST 7.56577e-15    /* constants.f90:7 */
+#define C_LIGHT 2.99792458e10
 
 static __thread char g_err[512];
 static void set_err(const char *fmt, ...) {
@@ -64,7 +66,7 @@ struct orc_ctx {
   css_params p;
   int nr, nth, nphi, nv, ncell;
   double *x_ind, *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks,
-      *dlnks, *eps, *mur, *dlnmu;
+      *dlnks, *eps, *mur, *dlnmu, *kr, *dlnkr;
   double *theta, *phi, *sines, *cosines;
   double dth, dphi;
   int ibcr[13], ibct[13]; /* 1-based as the reference's ibcr/ibct */
@@ -83,6 +85,9 @@ struct orc_ctx {
    * LAP_PV dv/dph/(r sin), LAP_PW dw/dph/(r sin), LAP_PU du/dph/(r sin) */
   double *lap;
   int cond; /* entropy conduction on: Laplacian .or. SLaplacian */
+  /* radiative diffusion: rad1 = (4 a c kr / 3) T^3 / rho^2 and rad2 = ds/dr,
+   * the reference's dvars2(:,:,:,1:2) under do_radheat */
+  double *rad1, *rad2;
 };
 enum { LAP_W1 = 0, LAP_V1, LAP_U1, LAP_PV, LAP_PW, LAP_PU, LAP_N };
 
@@ -553,7 +558,7 @@ void orc_destroy(orc_ctx *c) {
   free(c->blk); free(c->rblk_of);
   free(c->x_ind); free(c->r_ind); free(c->r_inv); free(c->dr_ind); free(c->dxdr); free(c->d2xdr2);
   free(c->rhor); free(c->sr); free(c->grav); free(c->ks); free(c->dlnks); free(c->eps);
-  free(c->mur); free(c->dlnmu); free(c->lap);
+  free(c->mur); free(c->dlnmu); free(c->lap); free(c->kr); free(c->dlnkr); free(c->rad1); free(c->rad2);
   free(c->theta); free(c->phi); free(c->sines); free(c->cosines); free(c->dspeed);
   free(c->temperature); free(c->invrho); free(c->maga); free(c->vars2); free(c->vars_save);
   free(c->dvars1); free(c->vars1); free(c->tmpf); free(c->tmpg); free(c->da);
@@ -582,7 +587,8 @@ int orc_create(const css_params *p, const double *prof, orc_ctx **out) {
   c->ncell = p->nr * p->nth * p->nphi;
   int nr = c->nr, nth = c->nth, nphi = c->nphi;
   double **dst[] = {&c->x_ind, &c->r_ind, &c->dr_ind, &c->dxdr, &c->d2xdr2, &c->rhor,
-                    &c->sr,    &c->grav,  &c->ks,     &c->dlnks, &c->eps, &c->mur, &c->dlnmu};
+                    &c->sr,    &c->grav,  &c->ks,     &c->dlnks, &c->eps, &c->mur, &c->dlnmu,
+                    &c->kr,    &c->dlnkr};
   for (int k = 0; k < CSS_NPROF; k++) {
     *dst[k] = dalloc(nr);
     memcpy(*dst[k], prof + (size_t)k * nr, sizeof(double) * nr);
@@ -726,6 +732,7 @@ even:
   c->tmpf = dalloc(n); c->tmpg = dalloc(n);
   if (p->magnetic) c->da = dalloc(3 * n);
   if (p->laplacian) c->lap = dalloc(n * LAP_N);
+  if (p->do_radheat) { c->rad1 = dalloc(n); c->rad2 = dalloc(n); }
   c->cond = p->slaplacian || p->laplacian;
   *out = c;
   return CSS_OK;
@@ -945,7 +952,6 @@ int orc_curl_b(orc_ctx *c, const double *a, double *b) {
 /* ------------------------------------------------------------------------ */
 /* RHS (rhs_mpi.f90:279-783)                                                */
 /* ------------------------------------------------------------------------ */
-#define ONETHIRD (1.0 / 3.0)
 #define TWOTHIRDS (2.0 / 3.0)
 #define FOURTHIRDS (4.0 / 3.0)
 #define SEVENTHIRDS (7.0 / 3.0)
@@ -1153,6 +1159,22 @@ static void phi_terms(orc_ctx *c, const blk_t *B, const double *v1, double *dv1)
         double oorho = c->invrho[id], t = c->temperature[id];
         dvv[j] = dvv[j] - c->pconst * w1[j] * t * oorho;
         ds[j] = dv1[4 * n + id];
+      }
+      if (p->do_radheat) { /* radiative diffusion, phi (rhs_mpi.f90:1092-1106) */
+        double wr[m + 2], o[m + 2];
+        for (int j = 1; j <= m; j++) wr[j] = w1[j] * c->invrho[PI_(j)];
+        line_deriv(c, B, 2, 1, c->temperature, it, ir, 0, 0.0, 0.0, o);
+        for (int j = 1; j <= m; j++) {
+          size_t id = PI_(j);
+          o[j] = o[j] * oors / c->temperature[id];
+          ds[j] = ds[j] + c->rad1[id] * (3.0 * o[j] - wr[j]) * o[j];
+        }
+        line_deriv(c, B, 2, 2, c->temperature, it, ir, 0, 0.0, 0.0, o);
+        for (int j = 1; j <= m; j++) {
+          size_t id = PI_(j);
+          o[j] = o[j] * (oors * oors);
+          ds[j] = ds[j] + c->rad1[id] * o[j] / c->temperature[id];
+        }
       }
       line_deriv(c, B, 2, 1, vF, it, ir, 0, 0.0, 0.0, w1);
       for (int j = 1; j <= m; j++) {
@@ -1398,6 +1420,7 @@ static void radial_terms(orc_ctx *c, const blk_t *B, const double *v1, double *d
         if (nu) w1[j] = w1[j] * W3(j);
         du[j] = du[j] - c->gamm1 * t * w1[j];
         ds[j] = ds[j] - uF[id] * w1[j];
+        if (p->do_radheat) c->rad2[id] = w1[j]; /* dvars2(:,ip,:,2), rhs_mpi.f90:1454 */
       }
       if (c->cond) {
         for (int j = 1; j <= m; j++) {
@@ -1479,6 +1502,23 @@ static void density_terms_theta(orc_ctx *c, const blk_t *B, const double *v1, do
         w1[j] = w1[j] * c->invrho[id];
         dv1[n + id] = dw - c->pconst * w1[j] * t;
       }
+      if (c->p.do_radheat) { /* radiative diffusion, theta (rhs_mpi.f90:1590-1602) */
+        double o[m + 2];
+        double tlo = c->temperature[IDX(c, 0, ip, ir)], thi = c->temperature[IDX(c, c->nth - 1, ip, ir)];
+        line_deriv(c, B, 1, 1, c->temperature, ip, ir, c->ibct[6], tlo, thi, o);
+        for (int j = 1; j <= m; j++) {
+          int it = t0 + j - 1;
+          size_t id = IDX(c, it, ip, ir);
+          double t = c->temperature[id], cot = c->cosines[it] / c->sines[it];
+          o[j] = ri * o[j] / t;
+          dv1[4 * n + id] = dv1[4 * n + id] + c->rad1[id] * o[j] * (3.0 * o[j] + ri * cot - w1[j]);
+        }
+        line_deriv(c, B, 1, 2, c->temperature, ip, ir, c->ibct[6], tlo, thi, o);
+        for (int j = 1; j <= m; j++) {
+          size_t id = IDX(c, t0 + j - 1, ip, ir);
+          dv1[4 * n + id] = dv1[4 * n + id] + (ri * ri) * c->rad1[id] * o[j] / c->temperature[id];
+        }
+      }
     }
 }
 
@@ -1514,11 +1554,40 @@ static void density_terms_radial(orc_ctx *c, const blk_t *B, const double *v1, d
         dv1[3 * n + id] = du - c->pconst * t * w1[j];
       }
       /* thermal damping toward T0 on the top shell (rhs_mpi.f90:1807-1818) */
-      if (B->rhi && !p->set_stop) {
+      if (B->rhi && !p->set_stop && !p->do_radheat) {
         size_t id = IDX(c, it, ip, r0 + m - 1);
         double t = c->temperature[id], rho = rhoF[id];
         dv1[id] = dv1[id] + rho * (p->t0 - t) / (p->damping_time * (p->gamma - 2.0) * t);
         dv1[4 * n + id] = dv1[4 * n + id] - c->cv * (p->t0 - t) / (p->damping_time * (p->gamma - 2.0) * t);
+      }
+      if (p->do_radheat) { /* radiative diffusion, r (rhs_mpi.f90:1820-1853); w1 = d ln(rho)/dr */
+        double o[m + 2];
+        double tlo = 0.0, thi = 0.0;
+        if (B->rlo) {
+          size_t id = IDX(c, it, ip, r0);
+          tlo = c->temperature[id] * (c->gamm1 * w1[1] + c->invcv * c->rad2[id]) / c->dxdr[0];
+        }
+        if (B->rhi) {
+          size_t id = IDX(c, it, ip, r0 + m - 1);
+          thi = c->temperature[id] * (c->gamm1 * w1[m] + c->invcv * c->rad2[id]) / c->dxdr[c->nr - 1];
+        }
+        line_deriv(c, B, 0, 1, c->temperature, it, ip, c->ibcr[6], tlo, thi, o);
+        for (int j = 1; j <= m; j++) {
+          int ir = r0 + j - 1;
+          size_t id = IDX(c, it, ip, ir);
+          double t = c->temperature[id], w4 = 2.0 * c->r_inv[ir] - c->dlnkr[ir];
+          if (nu) o[j] = o[j] * c->dxdr[ir];
+          o[j] = o[j] / t;
+          dv1[4 * n + id] = dv1[4 * n + id] + c->rad1[id] * o[j] * (w4 + 3.0 * o[j] - w1[j]);
+          if (nu) dv1[4 * n + id] = dv1[4 * n + id] + c->rad1[id] * o[j] * (c->d2xdr2[ir] / c->dxdr[ir]);
+        }
+        line_deriv(c, B, 0, 2, c->temperature, it, ip, c->ibcr[6], tlo, thi, o);
+        for (int j = 1; j <= m; j++) {
+          int ir = r0 + j - 1;
+          size_t id = IDX(c, it, ip, ir);
+          if (nu) o[j] = o[j] * (c->dxdr[ir] * c->dxdr[ir]);
+          dv1[4 * n + id] = dv1[4 * n + id] + c->rad1[id] * o[j] / c->temperature[id];
+        }
       }
     }
 }
@@ -1623,6 +1692,14 @@ static void thermo(orc_ctx *c, const double *v1) {
     t = t * ir;
     c->temperature[i] = t;
     c->invrho[i] = 1.0 / v1[i];
+  }
+  if (c->p.do_radheat) { /* rhs_mpi.f90:388-392 */
+    size_t np = (size_t)c->nth * c->nphi;
+#pragma omp parallel for schedule(static)
+    for (size_t i = 0; i < n; i++) {
+      double t = c->temperature[i], ir = c->invrho[i];
+      c->rad1[i] = (4.0 * A_CONST * C_LIGHT * c->kr[i / np] / 3.0) * (t * t * t) * (ir * ir);
+    }
   }
 }
 
@@ -2429,7 +2506,7 @@ int orc_shell_averages(orc_ctx *c, const double *vars0, const int *q, int nq, co
   size_t np = (size_t)nth * nphi;
   const css_params *p = &c->p;
   for (int iq = 0; iq < nq; iq++)
-    if (q[iq] < 1 || q[iq] > 18 || (q[iq] >= 10 && q[iq] <= 14 && !p->magnetic)) {
+    if (q[iq] < 1 || q[iq] > 18 || (q[iq] >= 10 && q[iq] <= 14 && !p->magnetic) || (q[iq] == 15 && p->do_radheat)) {
       set_err("orc_shell_averages: quantity %d not available", q[iq]);
       return CSS_ERR_ARG;
     }
