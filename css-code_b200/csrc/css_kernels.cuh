@@ -1399,53 +1399,83 @@ __device__ __forceinline__ double sld_ghost_t(const CssGeo &g, int iv, double q0
 // per field carried in registers (one new global load per field and
 // radius), then viscous heating and the mass-diffusion corrections
 // (diffusion.f90:375-428) per cell.  NF = number of diffused fields.
+//
+// The theta and phi faces difference the values of one radius, where the
+// subtracted mean state (diffusion.f90:125-175) is a constant: (x_a - m) -
+// (x_b - m) equals x_a - x_b bit for bit whenever x lies within a factor 2
+// of m (the two inner subtractions are then exact), so the plane values are
+// differenced raw.  The r faces difference across radii and subtract the
+// mean of each radius (sld_val).
 #define SLD_TT 32
 #define SLD_TP 8
 #define SLD_RC 32
 #define SLD_XW (SLD_TT + 4)  // plane row: 36 doubles = 288 B, so 16-byte copies stay aligned
+#define SLD_VW (SLD_TT + 3)
 template <int NF>
 struct SldSmem {
   double X[2][NF][SLD_TP + 4][SLD_XW];    // field planes (halo 2) of radii ir and ir+1
-  double V[2][SLD_TP + 2][SLD_TT + 3];    // vcc planes (halo 1)
-  double FT[NF][SLD_TP][SLD_TT + 1];      // theta faces
-  double FP[NF][SLD_TP + 1][SLD_TT];      // phi faces
-  double ST[SLD_TP][SLD_TT + 1];          // theta face speed * sin(face)
-  double SP[SLD_TP + 1][SLD_TT];          // phi face speed
+  double V[2][SLD_TP + 2][SLD_VW];        // vcc planes (halo 1)
+  double FT[NF][SLD_TP][SLD_TT + 1];      // theta face fluxes
+  double FP[NF][SLD_TP + 1][SLD_TT];      // phi face fluxes
 };
 
+// This thread's share of one radius's plane copies, fixed for the CTA: one
+// 16-byte theta pair of every field (the tile's first theta is even, and
+// so is nth on this path; zero fill outside 0 <= theta < nth, periodic phi)
+// and up to two speed values (theta clamped).  Offsets are within a plane.
+struct SldCopy {
+  int xs, xg, xn;       // smem offset in a field plane, global offset, bytes (16 or 0); xs < 0: none
+  int vs0, vg0, vs1, vg1;  // speed plane: smem / global offsets; vs < 0: none
+};
 
-// Starts the copies of radius ir's planes (every diffused field with a
-// 2-point halo, raw values; the speed plane with a 1-point halo, theta
-// clamped) into buffer `buf`: 16-byte copies of theta pairs (the tile's
-// first theta is even, and so is nth on this path), zero fill outside
-// 0 <= theta < nth, periodic phi.
-template <int NF>
-__device__ __forceinline__ void sld_issue_plane(const CssGeo &g, const double *__restrict__ v,
-                                                const double *__restrict__ av, const double *__restrict__ vcc,
-                                                SldSmem<NF> &S, int buf, int ir, int t0, int p0, int off) {
-  const size_t n = (size_t)g.ncell, pl = plane(g, ir);
-  const int nth = g.nth, nphi = g.nphi;
-  constexpr int PAIRS = SLD_XW / 2, ROWS = SLD_TP + 4, NX = NF * ROWS * PAIRS;
-  for (int k = threadIdx.x; k < NX; k += SLD_TT * SLD_TP) {
-    const int f = k / (ROWS * PAIRS), rem = k - f * (ROWS * PAIRS);
-    const int bb = rem / PAIRS, a2 = rem - bb * PAIRS;
+__device__ __forceinline__ SldCopy sld_copy_plan(const CssGeo &g, int t0, int p0) {
+  constexpr int PAIRS = SLD_XW / 2, NXP = (SLD_TP + 4) * PAIRS, NVV = (SLD_TP + 2) * (SLD_TT + 2);
+  const int nth = g.nth, nphi = g.nphi, k = threadIdx.x;
+  SldCopy c;
+  c.xs = -1; c.xg = 0; c.xn = 0;
+  if (k < NXP) {
+    const int bb = k / PAIRS, a2 = k - bb * PAIRS;
     const int gt = t0 - 2 + 2 * a2;
     int gp = p0 + bb - 2;
     gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
-    const int iv = f + off;
-    const double *fp = (iv >= 5 ? av + (size_t)(iv - 5) * n : v + (size_t)iv * n) + pl;
     const bool in = gt >= 0 && gt < nth;
-    cp_async16(&S.X[buf][f][bb][2 * a2], in ? fp + (size_t)gp * nth + gt : fp, in ? 16 : 0);
+    c.xs = bb * SLD_XW + 2 * a2;
+    c.xg = in ? gp * nth + gt : 0;
+    c.xn = in ? 16 : 0;
   }
-  constexpr int NVV = (SLD_TP + 2) * (SLD_TT + 2);
+  auto vslot = [&](int kk, int &vs, int &vg) {
+    vs = -1; vg = 0;
+    if (kk < NVV) {
+      const int a = kk % (SLD_TT + 2), bb = kk / (SLD_TT + 2);
+      const int gt = min(max(t0 + a - 1, 0), nth - 1);
+      int gp = p0 + bb - 1;
+      gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
+      vs = bb * SLD_VW + a;
+      vg = gp * nth + gt;
+    }
+  };
+  vslot(k, c.vs0, c.vg0);
+  vslot(k + SLD_TT * SLD_TP, c.vs1, c.vg1);
+  return c;
+}
+
+// starts the copies of radius ir's planes into buffer `buf`
+template <int NF>
+__device__ __forceinline__ void sld_issue_plane(const CssGeo &g, const double *__restrict__ v,
+                                                const double *__restrict__ av, const double *__restrict__ vcc,
+                                                SldSmem<NF> &S, const SldCopy &c, int buf, int ir, int off) {
+  const size_t n = (size_t)g.ncell, pl = plane(g, ir);
+  if (c.xs >= 0) {
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const int iv = f + off;
+      const double *fp = (iv >= 5 ? av + (size_t)(iv - 5) * n : v + (size_t)iv * n) + pl;
+      cp_async16(&S.X[buf][f][0][0] + c.xs, fp + c.xg, c.xn);
+    }
+  }
   const double *vp = vcc + pl;
-  for (int k = threadIdx.x; k < NVV; k += SLD_TT * SLD_TP) {
-    const int a = k % (SLD_TT + 2), bb = k / (SLD_TT + 2);
-    const int gt = min(max(t0 + a - 1, 0), nth - 1);
-    int gp = p0 + bb - 1;
-    gp = gp < 0 ? gp + nphi : (gp >= nphi ? gp - nphi : gp);
-    cp_async8(&S.V[buf][bb][a], vp + (size_t)gp * nth + gt, 8);
-  }
+  if (c.vs0 >= 0) cp_async8(&S.V[buf][0][0] + c.vs0, vp + c.vg0, 8);
+  if (c.vs1 >= 0) cp_async8(&S.V[buf][0][0] + c.vs1, vp + c.vg1, 8);
   cp_async_commit();
 }
 
@@ -1458,8 +1488,6 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
   SldSmem<NF> &S = *reinterpret_cast<SldSmem<NF> *>(sm_raw);
   auto &FT = S.FT;
   auto &FP = S.FP;
-  auto &ST = S.ST;
-  auto &SP = S.SP;
   const size_t n = (size_t)g.ncell;
   const int nth = g.nth, nphi = g.nphi, nr = g.nr;
   const int tx = threadIdx.x % SLD_TT, ty = threadIdx.x / SLD_TT;
@@ -1471,6 +1499,14 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
   // this launch diffuses fields off .. off+NF-1 and writes the fields of
   // wmask (a field it writes but does not diffuse gets zero)
   const bool hydro_part = (wmask & 0x1Fu) != 0;  // the fields the corrections act on
+  const bool edge_lo = t0 == 0, edge_hi = t0 + SLD_TT >= nth;
+  // theta faces of this thread: the upper face of its cell, and for warp 1
+  // the lower face of row tx (lane < SLD_TP); their sin(face) factors
+  const int gt_hi = t0 + tx + 1;
+  const bool th_hi_in = gt_hi > 0 && gt_hi < nth;
+  const bool lo_t = ty == 1 && tx < SLD_TP, lo_p = ty == 0;
+  const bool th_lo_in = t0 > 0 && t0 < nth;
+  const SldCopy cp = sld_copy_plan(g, t0, p0);
   // per-field r window: x(ir-1), x(ir), x(ir+1), x(ir+2), and the de of the
   // lower r face of the current radius
   double win[NF][4], carry[NF];
@@ -1494,7 +1530,7 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
                  (sld_face(xr(r0 - 2), win[f][0], win[f][1], win[f][2], g.tinyvar[iv], g.inv_tinyvar[iv]) * g.sld_r[2 * nr + r0]);
     }
   }
-  sld_issue_plane<NF>(g, v, av, vcc, S, 0, r0, t0, p0, off);
+  sld_issue_plane<NF>(g, v, av, vcc, S, cp, 0, r0, off);
   for (int ir = r0; ir < r1; ir++) {
     const int cb = (ir - r0) & 1;
     auto &X = S.X[cb];
@@ -1516,73 +1552,49 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     // (that buffer's last readers finished before the previous radius's
     // last barrier)
     if (ir + 1 < r1) {
-      sld_issue_plane<NF>(g, v, av, vcc, S, cb ^ 1, ir + 1, t0, p0, off);
+      sld_issue_plane<NF>(g, v, av, vcc, S, cp, cb ^ 1, ir + 1, off);
       cp_async_wait<1>();
     } else {
       cp_async_wait<0>();
     }
     __syncthreads();
-    // the diffused rho and s are the deviations from the mean state
-#pragma unroll
-    for (int f = 0; f < NF; f++) {
-      const int iv = f + off;
-      if (iv != 0 && iv != 4) continue;
-      const double mean = (iv == 0) ? g.rhor[ir] : g.sr[ir];
-      for (int k = threadIdx.x; k < (SLD_TP + 4) * SLD_XW; k += SLD_TT * SLD_TP) {
-        const int a = k % SLD_XW, bb = k / SLD_XW;
-        const int gt = t0 + a - 2;
-        if (gt >= 0 && gt < nth) X[f][bb][a] -= mean;
-      }
-    }
-    __syncthreads();
     // theta ghosts next to the walls (diffusion.f90:1008-1118)
-    if (t0 == 0)
-      for (int k = threadIdx.x; k < NF * (SLD_TP + 4); k += blockDim.x) {
-        int f = k / (SLD_TP + 4), b = k - f * (SLD_TP + 4);
-        X[f][b][1] = sld_ghost_t(g, f + off, X[f][b][2], X[f][b][3], X[f][b][4], X[f][b][5], 1);
-      }
-    if (t0 + SLD_TT >= nth)
-      for (int k = threadIdx.x; k < NF * (SLD_TP + 4); k += blockDim.x) {
-        int f = k / (SLD_TP + 4), b = k - f * (SLD_TP + 4), a = nth - t0 + 2;
-        X[f][b][a] = sld_ghost_t(g, f + off, X[f][b][a - 1], X[f][b][a - 2], X[f][b][a - 3], X[f][b][a - 4], 0);
-      }
-    // face speeds, shared by every field
-    for (int k = threadIdx.x; k < SLD_TP * (SLD_TT + 1); k += blockDim.x) {
-      int a = k % (SLD_TT + 1), b = k / (SLD_TT + 1);
-      int gt = t0 + a;
-      ST[b][a] = (gt > 0 && gt < nth) ? (g.sld_coef * sqrt(0.5 * (V[b + 1][a + 1] + V[b + 1][a]))) * g.sld_th[gt]
-                                      : 0.0;
+    if (edge_lo || edge_hi) {
+      if (edge_lo)
+        for (int k = threadIdx.x; k < NF * (SLD_TP + 4); k += blockDim.x) {
+          int f = k / (SLD_TP + 4), b = k - f * (SLD_TP + 4);
+          X[f][b][1] = sld_ghost_t(g, f + off, X[f][b][2], X[f][b][3], X[f][b][4], X[f][b][5], 1);
+        }
+      if (edge_hi)
+        for (int k = threadIdx.x; k < NF * (SLD_TP + 4); k += blockDim.x) {
+          int f = k / (SLD_TP + 4), b = k - f * (SLD_TP + 4), a = nth - t0 + 2;
+          X[f][b][a] = sld_ghost_t(g, f + off, X[f][b][a - 1], X[f][b][a - 2], X[f][b][a - 3], X[f][b][a - 4], 0);
+        }
+      __syncthreads();
     }
-    for (int k = threadIdx.x; k < (SLD_TP + 1) * SLD_TT; k += blockDim.x) {
-      int a = k % SLD_TT, b = k / SLD_TT;
-      SP[b][a] = g.sld_coef * sqrt(0.5 * (V[b][a + 1] + V[b + 1][a + 1]));
-    }
-    __syncthreads();
+    // face speeds (shared by every field): theta faces carry sin(face)
+    const double st_hi =
+        th_hi_in ? (g.sld_coef * sqrt(0.5 * (V[ty + 1][tx + 2] + V[ty + 1][tx + 1]))) * __ldg(g.sld_th + gt_hi) : 0.0;
+    const double sp_hi = g.sld_coef * sqrt(0.5 * (V[ty + 1][tx + 1] + V[ty + 2][tx + 1]));
+    double s_lo = 0.0;
+    if (lo_p) s_lo = g.sld_coef * sqrt(0.5 * (V[0][tx + 1] + V[1][tx + 1]));
+    else if (lo_t && th_lo_in) s_lo = (g.sld_coef * sqrt(0.5 * (V[tx + 1][1] + V[tx + 1][0]))) * __ldg(g.sld_th + t0);
     // face fluxes of every field: each thread takes the upper theta face and
-    // the upper phi face of its cell; the first column / row of the tile
-    // also take the lower face
-#pragma unroll
+    // the upper phi face of its cell; warp 0 also the phi faces of row 0,
+    // warp 1 the theta faces of column 0
+#pragma unroll 1
     for (int f = 0; f < NF; f++) {
       const double tiny = g.tinyvar[f + off], itiny = g.inv_tinyvar[f + off];
-      auto tface = [&](int bb, int a) {
-        const int gt = t0 + a;
-        double d = 0.0;
-        if (gt > 0 && gt < nth)
-          d = ST[bb][a] * sld_face(X[f][bb + 2][a], X[f][bb + 2][a + 1], X[f][bb + 2][a + 2], X[f][bb + 2][a + 3], tiny,
-                                   itiny);
-        FT[f][bb][a] = d;
-      };
-      auto pface = [&](int bb, int a) {
-        FP[f][bb][a] =
-            SP[bb][a] * sld_face(X[f][bb][a + 2], X[f][bb + 1][a + 2], X[f][bb + 2][a + 2], X[f][bb + 3][a + 2], tiny,
-                                 itiny);
-      };
-      tface(ty, tx + 1);
-      pface(ty + 1, tx);
-      // the tile's lower faces: warp 0 the phi faces of row 0, warp 1 the
-      // theta faces of column 0 (each warp is one theta row of the tile)
-      if (ty == 0) pface(0, tx);
-      else if (ty == 1 && tx < SLD_TP) tface(tx, 0);
+      const double *xr = &X[f][ty + 2][tx + 1];
+      FT[f][ty][tx + 1] = th_hi_in ? st_hi * sld_face(xr[0], xr[1], xr[2], xr[3], tiny, itiny) : 0.0;
+      FP[f][ty + 1][tx] = sp_hi * sld_face(X[f][ty + 1][tx + 2], X[f][ty + 2][tx + 2], X[f][ty + 3][tx + 2],
+                                           X[f][ty + 4][tx + 2], tiny, itiny);
+      if (lo_p) {
+        FP[f][0][tx] = s_lo * sld_face(X[f][0][tx + 2], X[f][1][tx + 2], X[f][2][tx + 2], X[f][3][tx + 2], tiny, itiny);
+      } else if (lo_t) {
+        const double *xl = &X[f][tx + 2][0];
+        FT[f][tx][0] = th_lo_in ? s_lo * sld_face(xl[0], xl[1], xl[2], xl[3], tiny, itiny) : 0.0;
+      }
     }
     // the velocities of this cell, taken from the tile when they are diffused
     // fields (before the barrier: the next radius's copies reuse the buffer)
