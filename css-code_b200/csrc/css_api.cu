@@ -831,9 +831,14 @@ static int launch_rad(css_ctx *c, const double *cur) {
   return check_launch(c);
 }
 
+static int launch_sld(css_ctx *c, const double *v, const double *av, double *dout, const double *tb);
+
+// with_sld: the step's slope-limited diffusion tendency of `cur` into c->vs,
+// launched after the radial kernel (the theta kernel has left T(cur) in
+// tbuf) and before the update that reads vs
 template <typename TS, typename TO>
 static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur, double ca = 0.0, double cb = 0.0,
-                      double dsld = 0.0) {
+                      double dsld = 0.0, bool with_sld = false) {
   const CssGeo &g = c->g;
   const int mag = g.magnetic;
   if (mag) {
@@ -878,6 +883,8 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   if constexpr (sizeof(TS) == 8) {
     if (c->p.do_radheat)
       if (int rc = launch_rad(c, (const double *)cur)) return rc;
+    if (with_sld)
+      if (int rc = launch_sld(c, (const double *)cur, (const double *)cur + 5 * c->ncell, c->vs, c->tbuf)) return rc;
   }
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
@@ -890,7 +897,7 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
 
 // slope-limited diffusion tendency of `v` (A in av for MHD; B must be in
 // c->bf) into dout
-static int launch_sld(css_ctx *c, const double *v, const double *av, double *dout) {
+static int launch_sld(css_ctx *c, const double *v, const double *av, double *dout, const double *tb) {
   const CssGeo &g = c->g;
   int nb = 148 * 16;
   prof_begin(c, KI_SLD_VCC);
@@ -906,17 +913,17 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
   const unsigned all = (1u << g.nv) - 1u;
   const int th = SLD_TT * SLD_TP;
   switch (g.nsld) {
-    case 4: k_sld<4><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, off, all); break;
-    case 5: k_sld<5><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, off, all); break;
+    case 4: k_sld<4><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, off, all, tb); break;
+    case 5: k_sld<5><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, off, all, tb); break;
     case 7:  // fields 1..7: rho is not diffused (its tendency is zero)
-      k_sld<4><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, 1, 0x1Fu);
+      k_sld<4><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, 1, 0x1Fu, tb);
       if (int rc = check_launch(c)) return rc;
-      k_sld<3><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 5, 0xE0u);
+      k_sld<3><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 5, 0xE0u, tb);
       break;
     default:  // fields 0..7
-      k_sld<5><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, 0, 0x1Fu);
+      k_sld<5><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, 0, 0x1Fu, tb);
       if (int rc = check_launch(c)) return rc;
-      k_sld<3><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 5, 0xE0u);
+      k_sld<3><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 5, 0xE0u, tb);
       break;
   }
   prof_end(c);
@@ -934,12 +941,8 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
 static int step_once(css_ctx *c, double dt) {
   const size_t N = c->ncell * c->nv;
   (void)N;
-  if (c->p.sldiffusion) {
-    if (c->g.magnetic) {
-      if (int rc = launch_curl(c, (const double *)(c->v0 + 5 * c->ncell), c->bf, 1)) return rc;
-    }
-    if (int rc = launch_sld(c, c->v0, c->v0 + 5 * c->ncell, c->vs)) return rc;
-  }
+  // the SLD tendency of vars0 is launched inside the first stage (with_sld)
+  const bool sld = c->p.sldiffusion != 0;
   const int ts = c->p.time_stepper;
   if (ts == 2 || ts == 3) {
     // Step_RK2_TVD / Step_RK3_TVD (step_rk4.f90:31-335): vs holds the SLD
@@ -947,8 +950,8 @@ static int step_once(css_ctx *c, double dt) {
     const double dsld = c->p.sldiffusion ? dt : 0.0;
     float *fA = reinterpret_cast<float *>(c->vA), *fB = reinterpret_cast<float *>(c->vB);
     const bool mixed = c->p.precision == 1;
-    int rc = mixed ? launch_rhs(c, (const double *)c->v0, fA, 5, dt, 1.0, 0.0)
-                   : launch_rhs(c, (const double *)c->v0, c->vA, 5, dt, 1.0, 0.0);
+    int rc = mixed ? launch_rhs(c, (const double *)c->v0, fA, 5, dt, 1.0, 0.0, 0.0, sld)
+                   : launch_rhs(c, (const double *)c->v0, c->vA, 5, dt, 1.0, 0.0, 0.0, sld);
     if (rc) return rc;
     if (ts == 2)
       return mixed ? launch_rhs(c, (const float *)fA, c->v0, 6, 0.5 * dt, 0.5, 0.5, dsld)
@@ -964,13 +967,13 @@ static int step_once(css_ctx *c, double dt) {
     // mixed: the stage states U1..U3 are FP32 (rho, s as perturbations about
     // the background); vars0, the accumulator and the tendency stay FP64
     float *fA = reinterpret_cast<float *>(c->vA), *fB = reinterpret_cast<float *>(c->vB);
-    if (int rc = launch_rhs(c, (const double *)c->v0, fA, 1, dt / 2.0)) return rc;
+    if (int rc = launch_rhs(c, (const double *)c->v0, fA, 1, dt / 2.0, 0.0, 0.0, 0.0, sld)) return rc;
     if (int rc = launch_rhs(c, (const float *)fA, fB, 2, dt / 2.0)) return rc;
     if (int rc = launch_rhs(c, (const float *)fB, fA, 3, dt)) return rc;
     if (int rc = launch_rhs(c, (const float *)fA, c->v0, 4, dt)) return rc;
     return CSS_OK;
   }
-  if (int rc = launch_rhs(c, (const double *)c->v0, c->vA, 1, dt / 2.0)) return rc;
+  if (int rc = launch_rhs(c, (const double *)c->v0, c->vA, 1, dt / 2.0, 0.0, 0.0, 0.0, sld)) return rc;
   if (int rc = launch_rhs(c, (const double *)c->vA, c->vB, 2, dt / 2.0)) return rc;
   if (int rc = launch_rhs(c, (const double *)c->vB, c->vA, 3, dt)) return rc;
   if (int rc = launch_rhs(c, (const double *)c->vA, c->v0, 4, dt)) return rc;
@@ -1034,7 +1037,7 @@ extern "C" int css_diffusion(css_ctx *c, double *vars1, const double *avec, doub
     CUDA_TRY(cudaMemcpyAsync(c->bf, vars1 + 5 * n, 3 * n * 8, cudaMemcpyHostToDevice, c->stream));
     CUDA_TRY(cudaMemcpyAsync(c->vB, avec, 3 * n * 8, cudaMemcpyHostToDevice, c->stream));
   }
-  if (int rc = launch_sld(c, c->vA, c->vB, c->dv)) return rc;
+  if (int rc = launch_sld(c, c->vA, c->vB, c->dv, nullptr)) return rc;
   CUDA_TRY(cudaMemcpyAsync(dvars1, c->dv, sb, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   // the reference leaves rho and s with the mean state subtracted

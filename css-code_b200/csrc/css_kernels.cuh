@@ -1483,7 +1483,8 @@ template <int NF>
 __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const double *__restrict__ v,
                                                             const double *__restrict__ av,
                                                             const double *__restrict__ vcc,
-                                                            double *__restrict__ dout, int off, unsigned wmask) {
+                                                            double *__restrict__ dout, int off, unsigned wmask,
+                                                            const double *__restrict__ tb) {
   extern __shared__ double sm_raw[];
   SldSmem<NF> &S = *reinterpret_cast<SldSmem<NF> *>(sm_raw);
   auto &FT = S.FT;
@@ -1647,8 +1648,10 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     if (hydro_part) {
       double rho = __ldg(v + id);
       double invrho = 1.0 / rho;
-      // 1/T = rho^(1-gamma) exp(-s/Cv) / invtconst, as one exponential
-      double itemp = exp(-fma(g.gamm1, log(rho), __ldg(v + 4 * n + id) * g.invcv)) / g.invtconst;
+      // 1/T: from the temperature of this state when the caller has it (tb),
+      // else rho^(1-gamma) exp(-s/Cv) / invtconst as one exponential
+      double itemp = tb ? 1.0 / __ldg(tb + id)
+                        : exp(-fma(g.gamm1, log(rho), __ldg(v + 4 * n + id) * g.invcv)) / g.invtconst;
       if (g.do_viscous_heating)
 #pragma unroll
         for (int k = 1; k <= 3; k++) D[4] = D[4] - uu[k] * D[k] * itemp;
