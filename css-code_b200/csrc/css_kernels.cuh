@@ -1532,6 +1532,9 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     }
   }
   sld_issue_plane<NF>(g, v, av, vcc, S, cp, 0, r0, off);
+  // the speed of this column at radii ir and ir+1, one radius ahead
+  double vc_a = __ldg(vcc + css_idx(g, itc, ipc, r0));
+  double vc_b = r0 < nr - 1 ? __ldg(vcc + css_idx(g, itc, ipc, r0 + 1)) : vc_a;
   for (int ir = r0; ir < r1; ir++) {
     const int cb = (ir - r0) & 1;
     auto &X = S.X[cb];
@@ -1539,9 +1542,15 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     const double t3 = g.sld_r[ir], rfac = g.sld_r[nr + ir], rhi2 = g.sld_r[3 * nr + ir];
     const double cphl = g.sld_th[nth + itc], cphh = g.sld_th[3 * nth + itc];
     const double geom = g.sld_th[4 * nth + itc] * (rfac / g.dphi);
-    const double vc = __ldg(vcc + css_idx(g, itc, ipc, ir));
-    const double vcp = ir < nr - 1 ? __ldg(vcc + css_idx(g, itc, ipc, ir + 1)) : vc;
-    const double vr_hi = g.sld_coef * sqrt(0.5 * (vcp + vc));
+    const double vr_hi = g.sld_coef * sqrt(0.5 * (vc_b + vc_a));
+    const double vc_n = ir + 1 < nr - 1 ? __ldg(vcc + css_idx(g, itc, ipc, ir + 2)) : vc_b;
+    // this cell's rho and T for the corrections, issued early
+    const size_t idc = css_idx(g, itc, ipc, ir);
+    double rho_c = 1.0, t_c = 1.0;
+    if (hydro_part) {
+      rho_c = __ldg(v + idc);
+      t_c = tb ? __ldg(tb + idc) : __ldg(v + 4 * n + idc);
+    }
     // next window value x(ir+3), issued early
     double nxt[NF];
 #pragma unroll
@@ -1637,6 +1646,8 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
       win[f][2] = win[f][3];
       win[f][3] = (ir + 3 == nr) ? sld_ghost_r(g, v, av, iv, itc, ipc, 0) : nxt[f];
     }
+    vc_a = vc_b;
+    vc_b = vc_n;
     if (!live) continue;
     const size_t id = css_idx(g, it, ip, ir);
     double D[8];
@@ -1646,12 +1657,11 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
       D[k] = (f >= 0 && f < NF) ? Dv[f >= 0 && f < NF ? f : 0] : 0.0;
     }
     if (hydro_part) {
-      double rho = __ldg(v + id);
+      const double rho = rho_c;
       double invrho = 1.0 / rho;
       // 1/T: from the temperature of this state when the caller has it (tb),
-      // else rho^(1-gamma) exp(-s/Cv) / invtconst as one exponential
-      double itemp = tb ? 1.0 / __ldg(tb + id)
-                        : exp(-fma(g.gamm1, log(rho), __ldg(v + 4 * n + id) * g.invcv)) / g.invtconst;
+      // else rho^(1-gamma) exp(-s/Cv) / invtconst as one exponential (t_c = s)
+      double itemp = tb ? 1.0 / t_c : exp(-fma(g.gamm1, log(rho), t_c * g.invcv)) / g.invtconst;
       if (g.do_viscous_heating)
 #pragma unroll
         for (int k = 1; k <= 3; k++) D[4] = D[4] - uu[k] * D[k] * itemp;
