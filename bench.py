@@ -188,7 +188,7 @@ def run_reference(args):
         return 0
     if args.workload.startswith("ensemble-"):
         return run_reference_ensemble(args, world)
-    if args.workload.startswith("closure-"):
+    if args.workload.startswith("closure"):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned closure: its SLD "
                           "speed is a prescribed radial profile (diffusion.f90:19-63)"}))
         return 0
@@ -483,6 +483,33 @@ def run_ensemble(args):
     return 0
 
 
+def run_closure_study(args):
+    """The closure judged by a resolved run: hydro 96x128x256 box-filtered
+    4x in every direction onto 24x32x64 (closure.study).  Prints one JSON line
+    with the relative errors of the time-averaged kinetic-energy spectrum and
+    enthalpy-flux profile of the prescribed-profile and the learned-closure
+    coarse runs against the filtered fine run, and the wall-time ratio of the
+    fine to the closure-driven coarse window."""
+    import torch
+    from css_b200 import closure as C
+    from css_b200 import problem
+    torch.cuda.set_device(0)
+    fp, fprof, fv0, fdt, _ = problem.build((96, 128, 256), decomp=(3, 4, 8))
+    cp, cprof, cv0, cdt, _ = problem.build((24, 32, 64), decomp=(2, 2, 4))
+    r = C.study((fp, fprof, fv0, fdt), (cp, cprof, cv0, cdt), factor=4, t_spin=10.0, t_win=2.0, nsnap=20)
+    out = {"metric": "closure study: relative error of the time-averaged kinetic-energy spectrum (m >= 1) and "
+                     "enthalpy flux of the coarse run against the filtered fine run",
+           "value": r["flux_err_closure"], "unit": "relative L2 error (enthalpy flux, learned closure)",
+           "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+           "config": {"workload": "closure-study", "fine": [96, 128, 256], "coarse": [24, 32, 64], "filter": 4,
+                      "t_spin": r["t_spin"], "t_window": r["t_win"], "snapshots": r["nsnap"]},
+           "result": {k: r[k] for k in ("spectrum_err_prescribed", "spectrum_err_closure", "flux_err_prescribed",
+                                        "flux_err_closure", "fine_window_s", "coarse_window_s",
+                                        "coarse_prescribed_window_s", "wall_ratio", "loss_first", "loss_last")}}
+    print(json.dumps(out))
+    return 0
+
+
 def run_closure(args):
     """The closure network (closure-<nr>x<nth>x<nphi>: one row per coarse
     cell): inference over the whole coarse grid and Adam steps of 65536
@@ -609,6 +636,8 @@ def main():
         return run_reference(args)
     if args.workload.startswith("ensemble-"):
         return run_ensemble(args)
+    if args.workload == "closure-study":
+        return run_closure_study(args)
     if args.workload.startswith("closure-"):
         return run_closure(args)
     return run_ours(args)

@@ -176,3 +176,118 @@ class Closure:
         coarse run's SLD speed^2.  Keep speed2 alive while the run steps."""
         check(_lib.lib().css_set_sld_speed2(coarse_sim.h, None if speed2 is None else _ptr(speed2)))
         coarse_sim._speed2 = speed2
+
+
+# ---------------------------------------------------------------------------
+# Evaluation: the closure against the prescribed profile, both judged by the
+# filtered fine run
+# ---------------------------------------------------------------------------
+def coarse_statistics(u_t, u_p, u_r, s_pert, rhor, tr):
+    """Statistics a coarse run is judged by, from (nr, nphi, nth) fields:
+    the kinetic-energy spectrum in azimuthal wavenumber m summed over r and
+    theta, E(m) = sum rhor |u_hat(m)|^2 over the three components, and the
+    enthalpy-flux profile F(r) = rhor T ⟨u_r s'⟩ over theta and phi (the
+    entropy form of rho c_p ⟨u_r T'⟩ about an adiabatic background)."""
+    E = 0.0
+    for u in (u_t, u_p, u_r):
+        uh = np.fft.rfft(u, axis=1) / u.shape[1]
+        E = E + (rhor[:, None, None] * np.abs(uh) ** 2).sum(axis=(0, 2))
+    F = rhor * tr * (u_r * s_pert).mean(axis=(1, 2))
+    return E, F
+
+
+def rel_err(a, b, lo=0):
+    return float(np.linalg.norm(a[lo:] - b[lo:]) / max(np.linalg.norm(b[lo:]), 1e-300))
+
+
+def study(fine, coarse, factor=4, t_spin=10.0, t_win=2.0, nsnap=20, train_steps=400, refresh=20, seed=4):
+    """Trains a closure on a fine run and compares two coarse runs with it.
+
+    ``fine`` and ``coarse`` are (params, profiles, vars0, dt) of the two grids
+    (coarse = fine / factor in every direction).  The fine run is spun up for
+    t_spin time units, then over t_win it is box-filtered ``nsnap`` times:
+    the snapshots are the training set and their statistics (time-averaged
+    E(m) and F(r), see coarse_statistics) the reference.  Two coarse runs from
+    the coarse seeded state then cover the same physical time: one with the
+    prescribed SLD profile, one whose SLD speed^2 is the closure's prediction
+    from its own state, refreshed every ``refresh`` steps.  Returns the
+    relative errors of both against the filtered fine statistics (E over
+    m >= 1, F over r) and the wall times of the fine and coarse windows."""
+    import time
+    import torch
+    from .context import Simulation
+    from .params import PROF_NAMES
+    fp, fprof, fv0, fdt = fine
+    cp, cprof, cv0, cdt = coarse
+    cpr = np.asarray(cprof).reshape(len(PROF_NAMES), cp.nr)
+    rhor, sr = cpr[PROF_NAMES.index("rhor")], cpr[PROF_NAMES.index("sr")]
+    g, cv = cp.gamma, cp.cp / cp.gamma
+    tr = (1.0 / (cv * (g - 1.0))) * rhor ** (g - 1.0) * np.exp(sr / cv)
+    dims = (cp.nth, cp.nphi, cp.nr)
+
+    fsim = Simulation(fp, fprof)
+    fsim.upload(fv0)
+    fsim.step_rk4(fdt, int(round(t_spin / fdt)))
+    every = max(1, int(round(t_win / fdt)) // nsnap)
+    Ef, Ff, snaps = [], [], []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(nsnap):
+        fsim.step_rk4(fdt, every)
+        d = dataset(fsim, factor)
+        f = d["fields"].cpu().numpy().reshape(7, cp.nr, cp.nphi, cp.nth)
+        e, fl = coarse_statistics(f[0], f[1], f[2], f[3], rhor, tr)
+        Ef.append(e)
+        Ff.append(fl)
+        snaps.append(d)
+    torch.cuda.synchronize()
+    fine_wall = time.perf_counter() - t0
+    Ef, Ff = np.mean(Ef, axis=0), np.mean(Ff, axis=0)
+    x = torch.cat([d["x"].view(d["nc"], XPAD) for d in snaps]).contiguous()
+    t = torch.cat([d["t"].view(d["nc"], YPAD) for d in snaps]).contiguous()
+    data = dict(snaps[-1])
+    data.update({"x": x.view(-1), "t": t.view(-1), "nc": x.shape[0]})
+    clo = Closure(seed=seed)
+    losses = clo.fit(data, steps=train_steps, batch=16384, lr=2e-3, seed=seed)
+    nc = cp.nr * cp.nth * cp.nphi
+
+    def coarse_run(learned):
+        sim = Simulation(cp, cprof)
+        sim.upload(cv0)
+        fields = torch.empty(7 * nc, dtype=torch.float64, device="cuda")
+        targ = torch.empty(NTARGET * nc, dtype=torch.float64, device="cuda")
+
+        def advance(n):
+            while n > 0:
+                if learned:  # the closure's speed^2 from this run's own state
+                    check(_lib.lib().css_box_filter(sim.h, 1, _ptr(fields), _ptr(targ)))
+                    Closure.attach(sim, clo.speed2(build_inputs(fields, dims, clo.qscale)))
+                k = min(refresh, n)
+                sim.step_rk4(cdt, k)
+                n -= k
+
+        advance(int(round(t_spin / cdt)))
+        cev = max(1, int(round(t_win / cdt)) // nsnap)
+        E, F = [], []
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        for _ in range(nsnap):
+            advance(cev)
+            v = sim.download()
+            e, fl = coarse_statistics(v[1], v[2], v[3], v[4] - sr[:, None, None], rhor, tr)
+            E.append(e)
+            F.append(fl)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t1
+        sim.close()
+        return np.mean(E, axis=0), np.mean(F, axis=0), wall
+
+    E0, F0, w0 = coarse_run(False)
+    E1, F1, w1 = coarse_run(True)
+    fsim.close()
+    return {"spectrum_err_prescribed": rel_err(E0, Ef, 1), "spectrum_err_closure": rel_err(E1, Ef, 1),
+            "flux_err_prescribed": rel_err(F0, Ff), "flux_err_closure": rel_err(F1, Ff),
+            "fine_window_s": fine_wall, "coarse_window_s": w1, "coarse_prescribed_window_s": w0,
+            "wall_ratio": fine_wall / max(w1, 1e-12), "loss_first": float(np.mean(losses[:10])),
+            "loss_last": float(np.mean(losses[-10:])), "t_spin": t_spin, "t_win": t_win, "nsnap": nsnap,
+            "E_fine": Ef, "E_prescribed": E0, "E_closure": E1, "F_fine": Ff, "F_prescribed": F0, "F_closure": F1}
