@@ -349,9 +349,8 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     set_err("css_create: radiative diffusion runs in FP64 only");
     return CSS_ERR_ARG;
   }
-  if (p.laplacian && (p.magnetic || p.precision != 0)) {
-    set_err("css_create: explicit viscosity runs hydro in FP64 only (the resistive induction terms and the FP32 "
-            "stage states are not built for it)");
+  if (p.laplacian && p.precision != 0) {
+    set_err("css_create: explicit viscosity runs in FP64 only (the FP32 stage states are not built for it)");
     return CSS_ERR_ARG;
   }
   css_ctx *c = new css_ctx();
@@ -798,9 +797,25 @@ static int launch_lap(css_ctx *c, const double *cur) {
   LAP_D(0, 1, S + 3 * n, L + 3 * n, nullptr, F + nf, g.ibcr[3]);
   LAP_D(1, 1, S + 4 * n, L + 4 * n, F + 2 * nf, F + 3 * nf, g.ibct[3]);
   LAP_D(1, 1, S + 5 * n, L + 5 * n, nullptr, nullptr, g.ibct[2]);
-#undef LAP_D
   k_lap_cross<<<nbp, 256, 0, st>>>(g, cur, L, c->dv);
-  return check_launch(c);
+  if (int rc = check_launch(c)) return rc;
+  if (g.magnetic) {
+    // resistive induction: J = curl B of c->bf (B of this stage's A)
+    const int bdry_t = g.theta_normal_field ? 1 : 0;
+    const double *bf = c->bf;
+    k_mhd_curl_in<<<nbp, 256, 0, st>>>(g, bf, S);
+    if (int rc = check_launch(c)) return rc;
+    LAP_D(1, 1, S, L, nullptr, nullptr, bdry_t);
+    LAP_D(1, 1, bf + 2 * n, L + n, nullptr, nullptr, bdry_t);
+    LAP_D(2, 1, bf + 2 * n, L + 2 * n, nullptr, nullptr, 0);
+    LAP_D(2, 1, bf, L + 3 * n, nullptr, nullptr, 0);
+    LAP_D(0, 1, S + n, L + 4 * n, nullptr, nullptr, g.ibcr[7]);
+    LAP_D(0, 1, S + 2 * n, L + 5 * n, nullptr, nullptr, g.ibcr[8]);
+    k_mhd_resist<<<nbp, 256, 0, st>>>(g, cur, c->tbuf, L, L + 3 * n, c->dv);
+    if (int rc = check_launch(c)) return rc;
+  }
+#undef LAP_D
+  return CSS_OK;
 }
 
 // radiative diffusion: the heating of all three directions added into ds,

@@ -247,6 +247,49 @@ __global__ void k_lap_cross(CssGeo g, const double *__restrict__ cur, const doub
 }
 
 // ---------------------------------------------------------------------------
+// Resistive induction under the Laplacian switch (Induction_Terms,
+// rhs_mpi.f90:2303-2364): J = curl B (VectorCurl, derivatives.f90:1894-2104),
+// dA/dt += -eta J (the v x B part is already in the tendency) and ds += (4 pi
+// / c^2) eta |J|^2 / (rho T), eta = ks.  B (bf) is B_theta, B_phi, B_r.
+// ---------------------------------------------------------------------------
+__global__ void k_mhd_curl_in(CssGeo g, const double *__restrict__ bf, double *__restrict__ S) {
+  const size_t n = (size_t)g.ncell;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x) {
+    int it, ip, ir;
+    lap_cell(g, id, it, ip, ir);
+    const double bt = bf[id], bp = bf[n + id], r = g.r_ind[ir];
+    S[id] = g.sines[it] * bp;
+    S[n + id] = r * bt;
+    S[2 * n + id] = r * bp;
+  }
+}
+
+// D: d(sin B_phi)/dth, dB_r/dth, dB_r/dph, dB_theta/dph, d(r B_theta)/dx, d(r B_phi)/dx
+__global__ void k_mhd_resist(CssGeo g, const double *__restrict__ cur, const double *__restrict__ tb,
+                             const double *__restrict__ D0, const double *__restrict__ D1, double *__restrict__ dv) {
+  const size_t n = (size_t)g.ncell;
+  const double jconst = 4.0 * 3.1415926535897932384626433832795028841972 / (2.99792458e10 * 2.99792458e10);
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < n; id += (size_t)gridDim.x * blockDim.x) {
+    int it, ip, ir;
+    lap_cell(g, id, it, ip, ir);
+    const double invr = g.r_inv[ir], csc = g.csc[it];
+    double jr = D0[id] * csc * invr;
+    double jp = -D0[n + id] * invr;
+    double jt = invr * D0[2 * n + id] * csc;
+    jr = jr - invr * D1[id] * csc;
+    double a = D1[n + id], b = D1[2 * n + id];
+    if (g.non_uniform) { a = a * g.dxdr[ir]; b = b * g.dxdr[ir]; }
+    jp = jp + a * invr;
+    jt = jt - b * invr;
+    const double etar = g.ks[ir];
+    dv[4 * n + id] = dv[4 * n + id] + (jconst * etar) * (jt * jt + jp * jp + jr * jr) * (1.0 / cur[id]) / tb[id];
+    dv[5 * n + id] = dv[5 * n + id] + (-etar * jt);
+    dv[6 * n + id] = dv[6 * n + id] + (-etar * jp);
+    dv[7 * n + id] = dv[7 * n + id] + (-etar * jr);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Radiative diffusion (do_radheat): ds += coef [T''/T + T'/T (geometry +
 // 3 T'/T - rho'/rho)] per direction, coef = (4 a c kr / 3) T^3 / rho^2
 // (rhs_mpi.f90:388-392), as Phi_Terms (:1092-1106), Density_Terms_Theta

@@ -576,10 +576,6 @@ int orc_create(const css_params *p, const double *prof, orc_ctx **out) {
     set_err("orc_create: SLD power flux limiters are not restated (all configs keep them off)");
     return CSS_ERR_ARG;
   }
-  if (p->laplacian && p->magnetic) {
-    set_err("orc_create: explicit viscosity with magnetic fields (the resistive induction terms) is not restated");
-    return CSS_ERR_ARG;
-  }
   orc_ctx *c = (orc_ctx *)calloc(1, sizeof(orc_ctx));
   c->p = *p;
   c->nr = p->nr; c->nth = p->nth; c->nphi = p->nphi;
@@ -1680,6 +1676,78 @@ static void lap_cross_theta(orc_ctx *c, double *dv1) {
   free(F);
 }
 
+/* VectorCurl (derivatives.f90:1894-2104): J = curl B of b (B_theta, B_phi,
+ * B_r) into j (J_theta, J_phi, J_r).  The theta derivatives take bdry 1 under
+ * Theta_Normal_Field and 0 otherwise (var -1 / 0), the phi derivatives none,
+ * the radial ones the B BCs (var 7, 8); none of these read a wall datum. */
+static void vector_curl_b(orc_ctx *c, const double *b, double *j) {
+  size_t n = c->ncell, np = (size_t)c->nth * c->nphi;
+  int nth = c->nth, nu = c->p.non_uniform;
+  const double *bt = b, *bp = b + n, *br = b + 2 * n;
+  double *jt = j, *jp = j + n, *jr = j + 2 * n;
+  const int bdry_t = c->p.theta_normal_field ? 1 : 0;
+  double *F = dalloc(3 * n);
+  for (size_t i = 0; i < n; i++) {
+    double r = c->r_ind[i / np];
+    F[i] = c->sines[i % nth] * bp[i];
+    F[n + i] = r * bt[i];
+    F[2 * n + i] = r * bp[i];
+  }
+  for (int kb = 0; kb < c->nblk; kb++) {
+    const blk_t *B = &c->blk[kb];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int ir = B->r0; ir < B->r0 + B->nr; ir++)
+      for (int ip = B->p0; ip < B->p0 + B->np; ip++) {
+        double o[B->nt + 2], invr = c->r_inv[ir];
+        line_deriv(c, B, 1, 1, F, ip, ir, bdry_t, 0.0, 0.0, o);
+        for (int q = 1; q <= B->nt; q++) {
+          int it = B->t0 + q - 1;
+          jr[IDX(c, it, ip, ir)] = o[q] * (1.0 / c->sines[it]) * invr;
+        }
+        line_deriv(c, B, 1, 1, br, ip, ir, bdry_t, 0.0, 0.0, o);
+        for (int q = 1; q <= B->nt; q++) jp[IDX(c, B->t0 + q - 1, ip, ir)] = -o[q] * invr;
+      }
+  }
+  for (int kb = 0; kb < c->nblk; kb++) {
+    const blk_t *B = &c->blk[kb];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int ir = B->r0; ir < B->r0 + B->nr; ir++)
+      for (int it = B->t0; it < B->t0 + B->nt; it++) {
+        double o[B->np + 2], invr = c->r_inv[ir], csc = 1.0 / c->sines[it];
+        line_deriv(c, B, 2, 1, br, it, ir, 0, 0.0, 0.0, o);
+        for (int q = 1; q <= B->np; q++) jt[IDX(c, it, B->p0 + q - 1, ir)] = invr * o[q] * csc;
+        line_deriv(c, B, 2, 1, bt, it, ir, 0, 0.0, 0.0, o);
+        for (int q = 1; q <= B->np; q++) {
+          size_t id = IDX(c, it, B->p0 + q - 1, ir);
+          jr[id] = jr[id] - invr * o[q] * csc;
+        }
+      }
+  }
+  for (int kb = 0; kb < c->nblk; kb++) {
+    const blk_t *B = &c->blk[kb];
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+      for (int it = B->t0; it < B->t0 + B->nt; it++) {
+        double o[B->nr + 2];
+        line_deriv(c, B, 0, 1, F + n, it, ip, c->ibcr[7], 0.0, 0.0, o);
+        for (int q = 1; q <= B->nr; q++) {
+          int ir = B->r0 + q - 1;
+          if (nu) o[q] = o[q] * c->dxdr[ir];
+          size_t id = IDX(c, it, ip, ir);
+          jp[id] = jp[id] + o[q] * c->r_inv[ir];
+        }
+        line_deriv(c, B, 0, 1, F + 2 * n, it, ip, c->ibcr[8], 0.0, 0.0, o);
+        for (int q = 1; q <= B->nr; q++) {
+          int ir = B->r0 + q - 1;
+          if (nu) o[q] = o[q] * c->dxdr[ir];
+          size_t id = IDX(c, it, ip, ir);
+          jt[id] = jt[id] - o[q] * c->r_inv[ir];
+        }
+      }
+  }
+  free(F);
+}
+
 static void thermo(orc_ctx *c, const double *v1) {
   size_t n = c->ncell;
   /* rhs_mpi.f90:376-387 */
@@ -1726,7 +1794,26 @@ int orc_rhs(orc_ctx *c, double *vars1, double *dvars1, int call_num) {
   for (int k = 0; k < c->nblk; k++) density_terms_theta(c, &c->blk[k], vars1, dvars1);
   for (int k = 0; k < c->nblk; k++) density_terms_radial(c, &c->blk[k], vars1, dvars1);
   if (c->p.magnetic) {
-    /* Induction_Terms: dA/dt = v x B (rhs_mpi.f90:2340-2346) */
+    /* Induction_Terms: under Laplacian the resistive part first (rhs_mpi.f90:
+     * 2303-2327): J = curl B, eta J / rho / T ohmic heating with jconst =
+     * 4 pi / c^2 and etar = ks (mhdsph_mpi.f90:316, :349), -eta J kept for
+     * dA/dt; then dA/dt = v x B (:2340-2346) plus -eta J (:2347-2364) */
+    double *ej = NULL;
+    if (c->p.laplacian) {
+      size_t np = (size_t)c->nth * c->nphi;
+      double *J = dalloc(3 * n);
+      ej = dalloc(3 * n);
+      vector_curl_b(c, vars1 + 5 * n, J);
+      const double jconst = 4.0 * PI / (C_LIGHT * C_LIGHT);
+      for (size_t i = 0; i < n; i++) {
+        double etar = c->ks[i / np];
+        for (int k = 0; k < 3; k++) ej[k * n + i] = -etar * J[k * n + i];
+        dvars1[4 * n + i] = dvars1[4 * n + i] + (jconst * etar) *
+                                                    (J[i] * J[i] + J[n + i] * J[n + i] + J[2 * n + i] * J[2 * n + i]) *
+                                                    c->invrho[i] / c->temperature[i];
+      }
+      free(J);
+    }
     const double *w = vars1 + n, *v = vars1 + 2 * n, *u = vars1 + 3 * n;
     const double *bt = vars1 + 5 * n, *bp = vars1 + 6 * n, *br = vars1 + 7 * n;
 #pragma omp parallel for schedule(static)
@@ -1734,6 +1821,10 @@ int orc_rhs(orc_ctx *c, double *vars1, double *dvars1, int call_num) {
       dvars1[5 * n + i] = v[i] * br[i] - u[i] * bp[i];
       dvars1[6 * n + i] = u[i] * bt[i] - w[i] * br[i];
       dvars1[7 * n + i] = w[i] * bp[i] - v[i] * bt[i];
+    }
+    if (ej) {
+      for (size_t i = 0; i < 3 * n; i++) dvars1[5 * n + i] = dvars1[5 * n + i] + ej[i];
+      free(ej);
     }
     if (call_num > 1) memcpy(vars1 + 5 * n, c->maga, sizeof(double) * 3 * n);
   }
