@@ -954,8 +954,6 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
 }
 
 static int step_once(css_ctx *c, double dt) {
-  const size_t N = c->ncell * c->nv;
-  (void)N;
   // the SLD tendency of vars0 is launched inside the first stage (with_sld)
   const bool sld = c->p.sldiffusion != 0;
   const int ts = c->p.time_stepper;
