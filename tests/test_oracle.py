@@ -183,3 +183,21 @@ def test_step_runs_and_conserves_shape():
     # impenetrable walls (Bound): u_r = 0 on the radial faces, w = 0 on theta
     assert np.abs(v[3][0]).max() == 0.0 and np.abs(v[3][-1]).max() == 0.0
     assert np.abs(v[1][:, :, 0]).max() == 0.0
+
+
+def test_mass_is_conserved_to_the_discretisation():
+    """Total mass (Compute_Step_Size's mtot, rhs_mpi.f90:92-275) over 40 steps
+    from the seeded state with the top damping off (Set_Stop), which adds
+    mass at the top shell.  The continuity equation is in non-conservative
+    form and the SLD's density ghost at the radial walls is the mean state
+    (diffusion.f90:582-728), so mass is conserved only to the discretisation:
+    the drift falls as the grid is refined."""
+    drift = []
+    for dims, dec in (((48, 48, 96), (2, 2, 3)), ((96, 96, 192), (4, 4, 6))):
+        p, prof, v0, dt, _ = problem.build(dims, decomp=dec)
+        p.set_stop = 1
+        o = O.Oracle(p, prof)
+        m0 = o.step_size(v0, 0.4)["mtot"]
+        v1 = o.step(v0, dt, 40)
+        drift.append(abs(o.step_size(v1, 0.4)["mtot"] - m0) / m0)
+    assert drift[0] < 5e-6 and drift[1] < 0.5 * drift[0], drift
