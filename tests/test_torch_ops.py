@@ -1,0 +1,74 @@
+"""torch.ops.css.deriv, the PyTorch face of the compact derivatives.
+
+CPU: the operator is registered with a CUDA kernel only, so a CPU tensor
+raises rather than falling back.  GPU: every direction and order equals the
+host-array entry point (css_deriv) bit for bit, on PyTorch's current stream
+and on a side stream; leading dimensions are independent fields; FP32
+tensors come back as the FP64 result rounded; the boundary data reach the
+closures."""
+import numpy as np
+import pytest
+import torch
+
+from css_b200 import problem
+from css_b200 import torch_ops as T
+
+
+def test_operator_has_no_cpu_kernel():
+    x = torch.zeros(4, 4, 4, dtype=torch.float64)
+    with pytest.raises(NotImplementedError):
+        torch.ops.css.deriv(x, 0, 0, 1, None, None, 1)
+
+
+@pytest.fixture(scope="module")
+def field(gpu_available):
+    from css_b200.context import Simulation
+    p, prof, v0, dt, _ = problem.build((48, 48, 64), decomp=(2, 2, 4))
+    rng = np.random.default_rng(17)
+    f = v0[4] + 1e-3 * rng.standard_normal(v0[4].shape)
+    return p, Simulation(p, prof), f, rng
+
+
+OPS = [(0, 1, T.dbydr), (0, 2, T.d2bydr2), (1, 1, T.dbydt), (1, 2, T.d2bydt2), (2, 1, T.dbydp), (2, 2, T.d2bydp2)]
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("direction,order,op", OPS)
+def test_operator_equals_host_entry(field, direction, order, op):
+    p, sim, f, rng = field
+    lo = hi = None
+    if direction < 2:
+        shape = (p.nphi, p.nth) if direction == 0 else (p.nr, p.nphi)
+        lo, hi = rng.standard_normal(shape), rng.standard_normal(shape)
+    bdry = 4
+    want = sim.deriv(direction, order, f, None if lo is None else lo.reshape(-1), None if hi is None else hi.reshape(-1),
+                     bdry)
+    x = torch.from_numpy(f).cuda()
+    tl = None if lo is None else torch.from_numpy(lo).cuda()
+    th = None if hi is None else torch.from_numpy(hi).cuda()
+    got = op(x, sim, tl, th, bdry)
+    assert got.dtype == torch.float64 and got.shape == x.shape
+    assert np.array_equal(got.cpu().numpy(), want)
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        got2 = op(x, sim, tl, th, bdry)
+    torch.cuda.current_stream().wait_stream(side)
+    assert torch.equal(got2, got)
+
+
+@pytest.mark.gpu
+def test_leading_dims_fp32_and_wall_data(field):
+    p, sim, f, rng = field
+    x = torch.from_numpy(np.stack([f, 2.0 * f + 1.0])).cuda()
+    both = T.dbydt(x, sim, bdry=1)
+    for k in range(2):
+        assert torch.equal(both[k], T.dbydt(x[k].contiguous(), sim, bdry=1))
+    x32 = x.to(torch.float32)
+    g32 = T.dbydr(x32, sim, bdry=1)
+    assert g32.dtype == torch.float32
+    assert torch.equal(g32, T.dbydr(x32.to(torch.float64), sim, bdry=1).to(torch.float32))
+    # a Neumann datum at the theta walls changes the answer; bdry 1 ignores it
+    lo = torch.full((p.nr, p.nphi), 3.0, dtype=torch.float64, device="cuda")
+    assert torch.equal(T.dbydt(x[0], sim, lo, lo, 1), T.dbydt(x[0], sim, None, None, 1))
+    assert not torch.equal(T.dbydt(x[0], sim, lo, lo, 4), T.dbydt(x[0], sim, None, None, 4))
