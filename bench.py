@@ -596,10 +596,11 @@ def run_closure(args):
            "data": "synthetic",
            "config": {"workload": args.workload, "rows": nc, "layers": list(d), "train_batch": batch,
                       "l2": "features (%.0f MB) larger than L2" % (nc * C.XPAD * 2 / 1e6)},
-           # a training step: 4 GEMMs forward and 7 backward (cuBLASLt) around own kernels (4 bias/GELU,
-           # loss, 4 column sums, 3 GELU backward, 8 Adam)
+           # a training step: 4 weight transposes, 4 GEMMs forward and 7 backward (k_gemm_bf16; the
+           # weight gradients add a split-K partial sum each), 4 bias/GELU, loss, 4 column sums,
+           # 3 GELU backward, 8 Adam
            "training": {"rows_per_s": batch * world / (tr_ms / 1e3), "ms_per_step": tr_ms, "tflops": tr_tf,
-                        "own_kernels_per_step": 20},
+                        "own_kernels_per_step": 39},
            "inference_per_layer_gemms": {"ms": gemm_ms, "rows_per_s": nc * world / (gemm_ms / 1e3)},
            "kernel": "k_mlp_fused (one launch: weights in shared memory, BF16 mma.sync m16n8k16 chain)",
            "roofline": {"bound": "tensor", "achieved": inf_tf, "peak": peak, "unit": "TFLOP/s",

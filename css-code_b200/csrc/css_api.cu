@@ -1,7 +1,6 @@
 // css_api.cu -- C ABI of the CSS B200 library (include/css_b200.h): context
 // set-up (virtual decomposition, LU tables, profiles), device buffers, the
 // RK4 step loop and the parity entry points.
-#include <cublasLt.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -1650,7 +1649,8 @@ extern "C" int css_spectrum(css_ctx *c, int kind, double *out) {
 // and the twelve subgrid targets; 3x3x3 stencil features of the coarse
 // fields feed an MLP (in 135 -> 128 -> 128 -> 128 -> 12, GELU (tanh form), BF16 weights
 // and activations, FP32 accumulation) whose matrix products run on the
-// tensor cores through cuBLASLt; its predicted subgrid velocity variance
+// tensor cores in the fused inference kernel or, for training and the
+// per-layer path, in k_gemm_bf16; its predicted subgrid velocity variance
 // becomes the per-cell SLD speed^2 of a coarse run, in place of the
 // prescribed radial profile (diffusion.f90:19-63).
 // ---------------------------------------------------------------------------
@@ -1727,49 +1727,45 @@ struct css_mlp {
   size_t cap;           // rows per pass
   float *W[4] = {}, *B[4] = {}, *gW[4] = {}, *gB[4] = {}, *mW[4] = {}, *vW[4] = {}, *mB[4] = {}, *vB[4] = {};
   __nv_bfloat16 *Wb[4] = {};
+  __nv_bfloat16 *WbT[4] = {};   // Wb transposed (out x in), for the forward products
+  bool wt_ok = false;
   float *Z[4] = {};             // pre-activations; Z[3] is the output
   __nv_bfloat16 *H[4] = {};     // H[1..3] activations; H[0] is the caller's input
   float *dH = nullptr;          // FP32 gradient scratch
   __nv_bfloat16 *dZb = nullptr; // BF16 gradient
   double *part = nullptr;
   int adam_t = 0;
-  cublasLtHandle_t lt = nullptr;
-  void *ws = nullptr;
-  size_t wsz = 32u << 20;
+  float *gpart = nullptr;       // row-chunk partials of the weight gradients
   cudaStream_t st = nullptr, own_st = nullptr;
   unsigned char *packed = nullptr;  // weights for the fused forward kernel
   bool packed_ok = false, fused = true;
 };
 
-static int lt_gemm(css_mlp *m, bool ta, bool tb, int M, int N, int K, const __nv_bfloat16 *A, int lda,
-                   const __nv_bfloat16 *Bm, int ldb, float *C, int ldc) {
-  cublasLtMatmulDesc_t op = nullptr;
-  cublasLtMatrixLayout_t la = nullptr, lb = nullptr, lc = nullptr;
-  cublasLtMatmulPreference_t pref = nullptr;
-  cublasLtMatmulHeuristicResult_t heur;
-  int nres = 0;
-  const cublasOperation_t oa = ta ? CUBLAS_OP_T : CUBLAS_OP_N, ob = tb ? CUBLAS_OP_T : CUBLAS_OP_N;
-  const float alpha = 1.0f, beta = 0.0f;
-  cublasStatus_t s = cublasLtMatmulDescCreate(&op, CUBLAS_COMPUTE_32F, CUDA_R_32F);
-  if (!s) s = cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSA, &oa, sizeof(oa));
-  if (!s) s = cublasLtMatmulDescSetAttribute(op, CUBLASLT_MATMUL_DESC_TRANSB, &ob, sizeof(ob));
-  if (!s) s = cublasLtMatrixLayoutCreate(&la, CUDA_R_16BF, ta ? K : M, ta ? M : K, lda);
-  if (!s) s = cublasLtMatrixLayoutCreate(&lb, CUDA_R_16BF, tb ? N : K, tb ? K : N, ldb);
-  if (!s) s = cublasLtMatrixLayoutCreate(&lc, CUDA_R_32F, M, N, ldc);
-  if (!s) s = cublasLtMatmulPreferenceCreate(&pref);
-  if (!s) s = cublasLtMatmulPreferenceSetAttribute(pref, CUBLASLT_MATMUL_PREF_MAX_WORKSPACE_BYTES, &m->wsz, sizeof(m->wsz));
-  if (!s) s = cublasLtMatmulAlgoGetHeuristic(m->lt, op, la, lb, lc, lc, pref, 1, &heur, &nres);
-  if (!s && nres == 0) s = CUBLAS_STATUS_NOT_SUPPORTED;
-  if (!s) s = cublasLtMatmul(m->lt, op, &alpha, A, la, Bm, lb, &beta, C, lc, C, lc, &heur.algo, m->ws, m->wsz, m->st);
-  if (pref) cublasLtMatmulPreferenceDestroy(pref);
-  if (lc) cublasLtMatrixLayoutDestroy(lc);
-  if (lb) cublasLtMatrixLayoutDestroy(lb);
-  if (la) cublasLtMatrixLayoutDestroy(la);
-  if (op) cublasLtMatmulDescDestroy(op);
-  if (s) {
-    set_err("cuBLASLt matmul %dx%dx%d: status %d", M, N, K, (int)s);
-    return CSS_ERR_CUDA;
-  }
+// the products of a pass, on k_gemm_bf16 (row-major; see css_closure.cuh)
+#define GM_NSPLIT 64
+// Z = X W with W read as its transpose WT (out x in): the same access
+// pattern as dH = dZ W^T, so both run the row-contiguous form of the kernel
+static int gemm_fwd(css_mlp *m, const __nv_bfloat16 *X, const __nv_bfloat16 *WT, float *Z, size_t rows, int K, int M) {
+  dim3 grid((unsigned)((rows + GM_TP - 1) / GM_TP), (M + GM_TQ - 1) / GM_TQ);
+  k_gemm_bf16<GM_DIN><<<grid, 128, 0, m->st>>>(X, WT, Z, (int)rows, M, K, K, K, 0);
+  CUDA_TRY(cudaGetLastError());
+  return CSS_OK;
+}
+static int gemm_din(css_mlp *m, const __nv_bfloat16 *D, const __nv_bfloat16 *W, float *dH, size_t rows, int K, int M) {
+  dim3 grid((unsigned)((rows + GM_TP - 1) / GM_TP), (K + GM_TQ - 1) / GM_TQ);
+  k_gemm_bf16<GM_DIN><<<grid, 128, 0, m->st>>>(D, W, dH, (int)rows, K, M, M, M, 0);
+  CUDA_TRY(cudaGetLastError());
+  return CSS_OK;
+}
+static int gemm_dw(css_mlp *m, const __nv_bfloat16 *X, const __nv_bfloat16 *D, float *gW, size_t rows, int K, int M) {
+  long long chunk = ((long long)rows + GM_NSPLIT - 1) / GM_NSPLIT;
+  chunk = std::max(256LL, (chunk + 15) / 16 * 16);
+  const int nsplit = (int)(((long long)rows + chunk - 1) / chunk);
+  dim3 grid((K + GM_TP - 1) / GM_TP, (M + GM_TQ - 1) / GM_TQ, nsplit);
+  k_gemm_bf16<GM_DW><<<grid, 128, 0, m->st>>>(X, D, m->gpart, K, M, (long long)rows, K, M, chunk);
+  CUDA_TRY(cudaGetLastError());
+  k_sum_partials<<<64, 256, 0, m->st>>>(m->gpart, nsplit, K * M, gW);
+  CUDA_TRY(cudaGetLastError());
   return CSS_OK;
 }
 
@@ -1782,11 +1778,10 @@ extern "C" void css_mlp_destroy(css_mlp *m) {
   if (!m) return;
   for (int l = 0; l < 4; l++) {
     cudaFree(m->W[l]); cudaFree(m->B[l]); cudaFree(m->gW[l]); cudaFree(m->gB[l]);
-    cudaFree(m->mW[l]); cudaFree(m->vW[l]); cudaFree(m->mB[l]); cudaFree(m->vB[l]); cudaFree(m->Wb[l]);
+    cudaFree(m->mW[l]); cudaFree(m->vW[l]); cudaFree(m->mB[l]); cudaFree(m->vB[l]); cudaFree(m->Wb[l]); cudaFree(m->WbT[l]);
     cudaFree(m->Z[l]); cudaFree(m->H[l]);
   }
-  cudaFree(m->dH); cudaFree(m->dZb); cudaFree(m->part); cudaFree(m->ws); cudaFree(m->packed);
-  if (m->lt) cublasLtDestroy(m->lt);
+  cudaFree(m->dH); cudaFree(m->dZb); cudaFree(m->part); cudaFree(m->gpart); cudaFree(m->packed);
   if (m->own_st) cudaStreamDestroy(m->own_st);
   else if (m->st) cudaStreamDestroy(m->st);
   delete m;
@@ -1807,9 +1802,8 @@ extern "C" int css_mlp_create(int n_in, int width, int n_out, int max_rows, unsi
   m->dims[4] = pad16(n_out);
   m->cap = (size_t)max_rows;
   cudaError_t e = cudaStreamCreateWithFlags(&m->st, cudaStreamNonBlocking);
-  if (!e && cublasLtCreate(&m->lt) != CUBLAS_STATUS_SUCCESS) e = cudaErrorUnknown;
-  if (!e) e = cudaMalloc(&m->ws, m->wsz);
   const int wmax = std::max(std::max(m->dims[0], width), m->dims[4]);
+  if (!e) e = cudaMalloc(&m->gpart, (size_t)GM_NSPLIT * wmax * wmax * 4);
   for (int l = 0; l < 4 && !e; l++) {
     const size_t K = m->dims[l], M = m->dims[l + 1];
     float **f4[] = {&m->W[l], &m->gW[l], &m->mW[l], &m->vW[l]};
@@ -1819,6 +1813,7 @@ extern "C" int css_mlp_create(int n_in, int width, int n_out, int max_rows, unsi
     for (auto pp : b4)
       if (!e) e = cudaMalloc(pp, M * 4);
     if (!e) e = cudaMalloc(&m->Wb[l], K * M * 2);
+    if (!e) e = cudaMalloc(&m->WbT[l], K * M * 2);
     if (!e) e = cudaMalloc(&m->Z[l], m->cap * M * 4);
     if (!e && l > 0) e = cudaMalloc(&m->H[l], m->cap * K * 2);
   }
@@ -1879,10 +1874,17 @@ extern "C" int css_mlp_dims(css_mlp *m, int *dims) {
 
 // forward pass of n <= cap rows: Z[3] holds the outputs (row-major n x dims[4])
 static int mlp_forward_rows(css_mlp *m, const __nv_bfloat16 *x, size_t n) {
+  if (!m->wt_ok) {
+    for (int l = 0; l < 4; l++) {
+      k_transpose_bf16<<<64, 256, 0, m->st>>>(m->Wb[l], m->dims[l], m->dims[l + 1], m->WbT[l]);
+      CUDA_TRY(cudaGetLastError());
+    }
+    m->wt_ok = true;
+  }
   const __nv_bfloat16 *in = x;
   for (int l = 0; l < 4; l++) {
     const int K = m->dims[l], M = m->dims[l + 1];
-    if (int rc = lt_gemm(m, false, false, M, (int)n, K, m->Wb[l], M, in, K, m->Z[l], M)) return rc;
+    if (int rc = gemm_fwd(m, in, m->WbT[l], m->Z[l], n, K, M)) return rc;
     __nv_bfloat16 *next = l < 3 ? m->H[l + 1] : nullptr;
     k_bias_gelu<<<148 * 4, 256, 0, m->st>>>(m->Z[l], m->B[l], next, M, n);
     CUDA_TRY(cudaGetLastError());
@@ -1961,17 +1963,18 @@ extern "C" int css_mlp_train_step(css_mlp *m, const void *x, const float *t, lon
     const int K = m->dims[l], M = m->dims[l + 1];
     const __nv_bfloat16 *in = l == 0 ? xb : m->H[l];
     // dW = dZ^T-contracted input, db = column sums of dZ
-    if (int rc = lt_gemm(m, false, true, M, K, (int)rows, m->dZb, M, in, K, m->gW[l], M)) return rc;
+    if (int rc = gemm_dw(m, in, m->dZb, m->gW[l], rows, K, M)) return rc;
     k_colsum<<<M, 256, 0, m->st>>>(m->dH, M, rows, m->gB[l]);
     CUDA_TRY(cudaGetLastError());
     if (l > 0) {
-      if (int rc = lt_gemm(m, true, false, K, (int)rows, M, m->Wb[l], M, m->dZb, M, m->dH, K)) return rc;
+      if (int rc = gemm_din(m, m->dZb, m->Wb[l], m->dH, rows, K, M)) return rc;
       k_gelu_back<<<148 * 4, 256, 0, m->st>>>(m->dH, m->Z[l - 1], m->dZb, (size_t)K * rows);
       CUDA_TRY(cudaGetLastError());
     }
   }
   m->adam_t++;
   m->packed_ok = false;
+  m->wt_ok = false;
   const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
   const float c1 = 1.0f - powf(b1, (float)m->adam_t), c2 = 1.0f - powf(b2, (float)m->adam_t);
   for (int l = 0; l < 4; l++) {
@@ -2009,6 +2012,7 @@ extern "C" int css_mlp_params(css_mlp *m, int l, float *w, float *b, int set) {
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(m->st));
     m->packed_ok = false;
+    m->wt_ok = false;
   } else {
     if (w) CUDA_TRY(cudaMemcpy(w, m->W[l], K * M * 4, cudaMemcpyDeviceToHost));
     if (b) CUDA_TRY(cudaMemcpy(b, m->B[l], M * 4, cudaMemcpyDeviceToHost));

@@ -1,8 +1,9 @@
 // css_closure.cuh -- the learned subgrid closure: box filtering of a fine
 // state into coarse fields and subgrid targets, the 3x3x3 stencil features,
 // and the elementwise parts of the MLP (bias + GELU and its derivative,
-// loss, bias gradients, Adam).  The MLP's matrix products are BF16 GEMMs
-// with FP32 accumulation on the tensor cores (cuBLASLt), issued from
+// loss, bias gradients, Adam), and k_gemm_bf16: the MLP's matrix products
+// for training and the per-layer forward pass, BF16 operands with FP32
+// accumulation on the tensor cores (mma.sync m16n8k16), issued from
 // css_api.cu.
 #pragma once
 #include <cuda_bf16.h>
@@ -414,4 +415,139 @@ __global__ void __launch_bounds__(FM_WARPS * 32, 1) k_mlp_fused(const __nv_bfloa
   }
 }
 
+// ---------------------------------------------------------------------------
+// The products of a training step on the tensor cores: BF16 mma.sync
+// m16n8k16 with FP32 accumulation, row-major operands.
+//   GM_FWD: C[n][i] = sum_k X[n][k] W[k][i]             (Z = X W)
+//   GM_DIN: C[n][j] = sum_i D[n][i] W[j][i]             (dH = dZ W^T)
+//   GM_DW:  C[z][j][i] = sum_{n in chunk z} X[n][j] D[n][i]   (dW = X^T dZ,
+//           split over row chunks; k_sum_partials adds the chunks in order)
+// A CTA of 4 warps computes a 32 (p) x 64 (q) tile of C; the reduction runs
+// in 16-wide steps through shared memory, zero-filled outside the operands.
+// ---------------------------------------------------------------------------
+enum { GM_FWD = 0, GM_DIN = 1, GM_DW = 2 };
+#define GM_TP 32
+#define GM_TQ 64
+#define GM_KS 64              // reduction width of one shared-memory stage
+#define GM_RS (GM_KS + 8)     // shared row stride in BF16: 144 B, rows stay 16-byte aligned
+
+// 8 consecutive BF16 from p (n of them valid, the rest zero): one 16-byte
+// load when all 8 are valid (p is then 16-byte aligned: every leading
+// dimension here is a multiple of 8 elements)
+__device__ __forceinline__ uint4 gm_ld8(const __nv_bfloat16 *__restrict__ p, int n) {
+  if (n >= 8) return __ldg(reinterpret_cast<const uint4 *>(p));
+  __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+  for (int e = 0; e < 8; e++) v[e] = e < n ? p[e] : __float2bfloat16_rn(0.0f);
+  return *reinterpret_cast<uint4 *>(v);
+}
+
+// scatter 8 BF16 down a column of a [row][GM_RS] shared tile
+__device__ __forceinline__ void gm_st8_col(__nv_bfloat16 (*T)[GM_RS], int row0, int col, uint4 v) {
+  const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&v);
+#pragma unroll
+  for (int k = 0; k < 8; k++) T[row0 + k][col] = e[k];
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(128) k_gemm_bf16(const __nv_bfloat16 *__restrict__ X,
+                                                   const __nv_bfloat16 *__restrict__ Y, float *__restrict__ C,
+                                                   int P, int Q, long long R, int ldx, int ldy, long long chunk) {
+  __shared__ __align__(16) __nv_bfloat16 As[GM_TP][GM_RS];
+  __shared__ __align__(16) __nv_bfloat16 Bs[GM_TQ][GM_RS];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = lane >> 2, t = lane & 3;
+  const int p0 = blockIdx.x * GM_TP, q0 = blockIdx.y * GM_TQ;
+  long long r0 = 0, r1 = R;
+  if (MODE == GM_DW) {
+    r0 = (long long)blockIdx.z * chunk;
+    r1 = r0 + chunk < R ? r0 + chunk : R;
+    C += (size_t)blockIdx.z * P * Q;
+  }
+  const int wp = (w & 1) * 16, wq = (w >> 1) * 32;
+  float acc[4][4];
+#pragma unroll
+  for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) acc[nt][c] = 0.0f;
+  for (long long rb = r0; rb < r1; rb += GM_KS) {
+    const long long rleft = r1 - rb;
+    // A tile (32 p x 64 r): 256 vectors of 8, two per thread
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int v = tid + h * 128;
+      if (MODE == GM_DW) {  // A(p, r) = X[r * ldx + p]: vectors along p
+        const int rr = v >> 2, p8 = (v & 3) * 8;
+        const int p = p0 + p8;
+        const int n = (rr < rleft) ? (P - p < 8 ? P - p : 8) : 0;
+        gm_st8_col(As, p8, rr, gm_ld8(X + (rb + rr) * ldx + p, n));
+      } else {  // A(p, r) = X[p * ldx + r]: vectors along r
+        const int pp = v >> 3, r8 = (v & 7) * 8;
+        const int p = p0 + pp;
+        const long long rl = rleft - r8;
+        const int n = (p < P) ? (int)(rl < 8 ? (rl > 0 ? rl : 0) : 8) : 0;
+        *reinterpret_cast<uint4 *>(&As[pp][r8]) = gm_ld8(X + (long long)p * ldx + rb + r8, n);
+      }
+    }
+    // B tile (64 q x 64 r), stored [q][r]: 512 vectors of 8, four per thread
+#pragma unroll
+    for (int h = 0; h < 4; h++) {
+      const int v = tid + h * 128;
+      if (MODE == GM_DIN) {  // B(r, q) = Y[q * ldy + r]: vectors along r
+        const int qq = v >> 3, r8 = (v & 7) * 8;
+        const int q = q0 + qq;
+        const long long rl = rleft - r8;
+        const int n = (q < Q) ? (int)(rl < 8 ? (rl > 0 ? rl : 0) : 8) : 0;
+        *reinterpret_cast<uint4 *>(&Bs[qq][r8]) = gm_ld8(Y + (long long)q * ldy + rb + r8, n);
+      } else {  // B(r, q) = Y[r * ldy + q]: vectors along q
+        const int rr = v >> 3, q8 = (v & 7) * 8;
+        const int q = q0 + q8;
+        const int n = (rr < rleft) ? (Q - q < 8 ? (Q - q > 0 ? Q - q : 0) : 8) : 0;
+        gm_st8_col(Bs, q8, rr, gm_ld8(Y + (rb + rr) * ldy + (n > 0 ? q : 0), n));
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int ks = 0; ks < GM_KS; ks += 16) {
+      unsigned a[4];
+      a[0] = *reinterpret_cast<const unsigned *>(&As[wp + g][ks + 2 * t]);
+      a[1] = *reinterpret_cast<const unsigned *>(&As[wp + g + 8][ks + 2 * t]);
+      a[2] = *reinterpret_cast<const unsigned *>(&As[wp + g][ks + 2 * t + 8]);
+      a[3] = *reinterpret_cast<const unsigned *>(&As[wp + g + 8][ks + 2 * t + 8]);
+#pragma unroll
+      for (int nt = 0; nt < 4; nt++) {
+        const __nv_bfloat16 *br = &Bs[wq + nt * 8 + g][ks + 2 * t];
+        mma_bf16_16816(acc[nt], a, *reinterpret_cast<const unsigned *>(br),
+                       *reinterpret_cast<const unsigned *>(br + 8));
+      }
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int nt = 0; nt < 4; nt++)
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const int p = p0 + wp + g + (c >= 2 ? 8 : 0), q = q0 + wq + nt * 8 + 2 * t + (c & 1);
+      if (p < P && q < Q) C[(size_t)p * Q + q] = acc[nt][c];
+    }
+}
+
+// dst (M x K) = src (K x M) transposed, BF16
+__global__ void k_transpose_bf16(const __nv_bfloat16 *__restrict__ src, int K, int M, __nv_bfloat16 *__restrict__ dst) {
+  const int n = K * M;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int q = i / K, k = i - q * K;
+    dst[i] = src[(size_t)k * M + q];
+  }
+}
+
+// out[i] = sum over z in order of part[z * count + i]
+__global__ void k_sum_partials(const float *__restrict__ part, int nsplit, int count, float *__restrict__ out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    float s = 0.0f;
+    for (int z = 0; z < nsplit; z++) s += part[(size_t)z * count + i];
+    out[i] = s;
+  }
+}
+
 }  // namespace css
+
