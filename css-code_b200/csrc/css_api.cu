@@ -18,6 +18,7 @@
 #include "css_stats.cuh"
 #include "css_closure.cuh"
 #include "css_lap.cuh"
+#include "css_inout.cuh"
 
 using namespace css;
 
@@ -64,6 +65,17 @@ struct css_ctx {
   double *lapface = nullptr;        // explicit viscosity: face data, 6 x max face size
   double *radbuf = nullptr;         // radiative diffusion: d ln(rho)/dr, ds/dr, 8 derivative fields
   double *radface = nullptr;        // radiative diffusion: face data, 6 x max face size
+  // open radial boundaries: face scalars and mass totals (IO_COUNT), block
+  // parts of the face sums, rain fields (2 x nth*nphi), ASH slices (16 x
+  // nth*nphi), the interpolated bottom fields (4 x nth*nphi), squalls
+  double *io = nullptr, *io_part = nullptr, *rain = nullptr, *ash_slices = nullptr, *ashv = nullptr;
+  double *squalls = nullptr;
+  int squall_cap = 0;
+  // the run's clock: the step index the RHS sees (Program CSS2's istep),
+  // sim_time, deltat; the ASH slice times; the RHS call number in progress
+  long long istep = 0;
+  double sim_time = 0.0, deltat = 0.0, ash_times[4] = {0.0, 0.0, 0.0, 0.0};
+  int rhs_call = 0;
   double dtd = 1e10;                // viscous time-step limit of Compute_Step_Size
   double rep_flux_lo = 0.0, rep_flux_hi = 0.0;  // dsdr1/dxdr(1), dsdr2/dxdr(nr) of the reports
   int mt[3];                        // compile-time block length per direction (0 = generic)
@@ -235,6 +247,8 @@ extern "C" void css_destroy(css_ctx *c) {
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
   cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf);
   cudaFree(c->lapbuf); cudaFree(c->lapface); cudaFree(c->radbuf); cudaFree(c->radface);
+  cudaFree(c->io); cudaFree(c->io_part); cudaFree(c->rain); cudaFree(c->ash_slices); cudaFree(c->ashv);
+  cudaFree(c->squalls);
   for (auto e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -350,6 +364,17 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   }
   if (p.laplacian && p.precision != 0) {
     set_err("css_create: explicit viscosity runs in FP64 only (the FP32 stage states are not built for it)");
+    return CSS_ERR_ARG;
+  }
+  const bool open_r = p.top_inout || p.bot_inout;
+  if ((open_r || p.bottom_specified || p.do_entropy_rain) &&
+      (p.magnetic || p.laplacian || p.do_radheat || p.precision != 0)) {
+    set_err("css_create: open radial boundaries are built for hydro FP64 runs without explicit viscosity or "
+            "radiative diffusion");
+    return CSS_ERR_ARG;
+  }
+  if ((p.bottom_specified && !p.bot_inout) || (p.do_entropy_rain && !p.top_inout)) {
+    set_err("css_create: bottom_specified needs bot_inout and do_entropy_rain needs top_inout");
     return CSS_ERR_ARG;
   }
   css_ctx *c = new css_ctx();
@@ -482,7 +507,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     int lbcr_v = (tn && bn) ? 1 : (tn && !bn) ? 2 : (!tn && bn) ? 3 : 4;
     int tt = p.top_constant_temp, bt = p.bottom_constant_temp;
     int lbcr_s = (tt && bt) ? 1 : (tt && !bt) ? 2 : (!tt && bt) ? 3 : 4;
-    int lbcr_u = 1, lbcr_rho = 4, lbcr_t = 4;
+    int lbcr_u = p.top_inout ? 3 : 1, lbcr_rho = 4, lbcr_t = 4;  // mhdsph_mpi.f90:1355-1359
     int lbct_rho = 4, lbct_t = 0, lbct_w = 1, lbct_u = p.theta_stress_free ? 0 : 1, lbct_v = 4, lbct_s = 0;
     int lbcr_br = 0, lbcr_bt = 0, lbcr_bp = 0, lbcr_ar = 0, lbcr_at = 0, lbcr_ap = 0;
     int lbct_br = 0, lbct_bt = 0, lbct_bp = 0, lbct_ar = 0, lbct_at = 0, lbct_ap = 0;
@@ -639,6 +664,21 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
     ALLOC(c->radbuf, 10 * c->ncell * sizeof(double));
     ALLOC(c->radface, 6 * nf * sizeof(double));
   }
+  if (open_r) {
+    const size_t np = (size_t)nth * nphi;
+    ALLOC(c->io, IO_COUNT * sizeof(double));
+    ALLOC(c->io_part, std::max((size_t)8 * p.nnt * p.nnp, (size_t)2 * nr) * sizeof(double));
+    ALLOC(c->rain, 2 * np * sizeof(double));
+    ALLOC(c->ash_slices, 16 * np * sizeof(double));
+    ALLOC(c->ashv, 4 * np * sizeof(double));
+    cudaMemset(c->io, 0, IO_COUNT * sizeof(double));
+    cudaMemset(c->rain, 0, 2 * np * sizeof(double));
+    cudaMemset(c->ash_slices, 0, 16 * np * sizeof(double));
+    cudaMemset(c->ashv, 0, 4 * np * sizeof(double));
+    g.inout = c->io; g.dvel_rain = c->rain; g.dent_rain = c->rain + np; g.ashv = c->ashv;
+  }
+  g.top_inout = p.top_inout; g.bot_inout = p.bot_inout; g.bottom_specified = p.bottom_specified;
+  g.rain = p.do_entropy_rain; g.delta_s = p.delta_s;
   cudaMemcpy(c->tab, T.data(), T.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->prof, R.data(), R.size() * 8, cudaMemcpyHostToDevice);
   cudaMemcpy(c->theta_prof, TH.data(), TH.size() * 8, cudaMemcpyHostToDevice);
@@ -847,6 +887,24 @@ static int launch_rad(css_ctx *c, const double *cur) {
 
 static int launch_sld(css_ctx *c, const double *v, const double *av, double *dout, const double *tb);
 
+// Open radial boundaries: the face sums and scalars of this RHS, after the
+// mass total's refresh at the first call of every ufreq-th step
+// (rhs_mpi.f90:326-353)
+static int launch_inout(css_ctx *c, const double *cur) {
+  const CssGeo &g = c->g;
+  if (c->rhs_call == 1) {
+    if (c->p.ufreq > 0 && c->istep % c->p.ufreq == 0) {
+      k_plane_mass<<<g.nr, IO_NT, 0, c->stream>>>(g, cur, c->io_part);
+      k_mass_finish<<<1, 32, 0, c->stream>>>(g, c->io_part, c->io, IO_MTOT, -1);
+      if (int rc = check_launch(c)) return rc;
+    }
+    c->rhs_call = 2;  // the later stages are calls 2..4
+  }
+  k_inout_sums<<<g.d[1].nb * g.d[2].nb, IO_NT, 0, c->stream>>>(g, cur, c->io_part);
+  k_inout_scalars<<<1, 32, 0, c->stream>>>(g, c->io_part, c->io, c->deltat, c->sim_time);
+  return check_launch(c);
+}
+
 // with_sld: the step's slope-limited diffusion tendency of `cur` into c->vs,
 // launched after the radial kernel (the theta kernel has left T(cur) in
 // tbuf) and before the update that reads vs
@@ -887,6 +945,8 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   if constexpr (sizeof(TS) == 8) {
     if (c->p.laplacian)
       if (int rc = launch_lap(c, (const double *)cur)) return rc;
+    if (c->io)
+      if (int rc = launch_inout(c, (const double *)cur)) return rc;
   }
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
@@ -952,7 +1012,48 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
   return CSS_OK;
 }
 
+static int step_stages(css_ctx *c, double dt);
+
+// the prescribed bottom fields at the clock's time (Cubic_Time_Interp)
+static int ash_refresh(css_ctx *c) {
+  if (!c->p.bottom_specified || !(c->ash_times[2] > c->ash_times[1])) return CSS_OK;
+  const double mu = (c->sim_time - c->ash_times[1]) / (c->ash_times[2] - c->ash_times[1]);
+  const size_t np = (size_t)c->p.nth * c->p.nphi;
+  k_ash_interp<<<148, 256, 0, c->stream>>>(c->ash_slices, np, mu, c->ashv);
+  return check_launch(c);
+}
+
+// One step with the run's clock (Program CSS2, mhdsph_mpi.f90:28-43): the
+// step index advances before it and the time after it; a prescribed bottom
+// interpolates its fields at the start time (Read_ASH_Inflow, ash_inflow.f90:
+// 124-219) and updates the enthalpy-flux factor every ufreq steps at the end
+// (step_rk4.f90:477-482)
 static int step_once(css_ctx *c, double dt) {
+  c->istep++;
+  c->deltat = dt;
+  if (c->p.bottom_specified) {
+    if (!(c->sim_time < c->ash_times[2])) {
+      set_err("css_step_rk4: sim_time %.17g is past the third ASH slice time %.17g; shift in the next slice "
+              "first (css_set_ash_slices)", c->sim_time, c->ash_times[2]);
+      c->istep--;
+      return CSS_ERR_ARG;
+    }
+    if (int rc = ash_refresh(c)) return rc;
+  }
+  c->rhs_call = 1;
+  int rc = step_stages(c, dt);
+  c->rhs_call = 0;
+  if (rc) return rc;
+  if (c->p.bottom_specified && c->p.ufreq > 0 && c->istep % c->p.ufreq == 0) {
+    k_ash_flux<<<1, IO_NT, 0, c->stream>>>(c->g, c->v0, c->tbuf, c->io, c->sim_time,
+                                           4.0 * 3.1415926535897932384626433832795028841972);
+    if (int rc2 = check_launch(c)) return rc2;
+  }
+  c->sim_time = c->sim_time + dt;
+  return CSS_OK;
+}
+
+static int step_stages(css_ctx *c, double dt) {
   // the SLD tendency of vars0 is launched inside the first stage (with_sld)
   const bool sld = c->p.sldiffusion != 0;
   const int ts = c->p.time_stepper;
@@ -1033,7 +1134,10 @@ extern "C" int css_rhs(css_ctx *c, double *vars1, double *dvars1, int call_num) 
   if (!c || !vars1 || !dvars1) { set_err("css_rhs: NULL"); return CSS_ERR_ARG; }
   size_t sb = c->ncell * c->nv * 8;
   CUDA_TRY(cudaMemcpyAsync(c->vA, vars1, sb, cudaMemcpyHostToDevice, c->stream));
-  if (int rc = launch_rhs(c, (const double *)c->vA, (double *)nullptr, 0, 0.0)) return rc;
+  c->rhs_call = call_num;
+  int rc = launch_rhs(c, (const double *)c->vA, (double *)nullptr, 0, 0.0);
+  c->rhs_call = 0;
+  if (rc) return rc;
   CUDA_TRY(cudaMemcpyAsync(dvars1, c->dv, sb, cudaMemcpyDeviceToHost, c->stream));
   if (c->g.magnetic && call_num == 1)
     CUDA_TRY(cudaMemcpyAsync(vars1 + 5 * c->ncell, c->bf, 3 * c->ncell * 8, cudaMemcpyDeviceToHost, c->stream));
@@ -1346,8 +1450,14 @@ extern "C" void css_ensemble_destroy(css_ensemble *e) {
 extern "C" int css_ensemble_create(int nmem, css_ctx *const *members, css_ensemble **out) {
   if (!out || nmem < 1 || !members) { set_err("css_ensemble_create: bad argument"); return CSS_ERR_ARG; }
   *out = nullptr;
-  for (int i = 0; i < nmem; i++)
+  for (int i = 0; i < nmem; i++) {
     if (!members[i]) { set_err("css_ensemble_create: member %d is NULL", i); return CSS_ERR_ARG; }
+    if (members[i]->io) {
+      set_err("css_ensemble_create: member %d has an open radial boundary, whose per-step host clock a "
+              "captured step cannot carry", i);
+      return CSS_ERR_ARG;
+    }
+  }
   css_ensemble *e = new css_ensemble();
   e->m.assign(members, members + nmem);
   e->ms.resize(nmem);
@@ -2233,5 +2343,118 @@ extern "C" int css_compact_lines_noalloc(const double *x, double *dx, int n, int
   k_lines<<<(nlines + 127) / 128, 128, 0, st>>>(x, dx, n, nlines, order, dtype, bdry, bc_lo, bc_hi, halo_lo, halo_hi,
                                                 T, (int)ts, dnum, scale, work);
   CUDA_TRY(cudaGetLastError());
+  return CSS_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Open radial boundaries: clock, mass bookkeeping, rain and ASH inputs
+// ---------------------------------------------------------------------------
+extern "C" int css_set_clock(css_ctx *c, long long istep, double sim_time, double deltat) {
+  if (!c) { set_err("css_set_clock: NULL"); return CSS_ERR_ARG; }
+  c->istep = istep;
+  c->sim_time = sim_time;
+  c->deltat = deltat;
+  if (c->io) return ash_refresh(c);
+  return CSS_OK;
+}
+
+extern "C" int css_get_clock(css_ctx *c, long long *istep, double *sim_time) {
+  if (!c) { set_err("css_get_clock: NULL"); return CSS_ERR_ARG; }
+  if (istep) *istep = c->istep;
+  if (sim_time) *sim_time = c->sim_time;
+  return CSS_OK;
+}
+
+static int need_open(css_ctx *c, const char *who) {
+  if (!c) { set_err("%s: NULL", who); return CSS_ERR_ARG; }
+  if (!c->io) { set_err("%s: the run has no open radial boundary (top_inout / bot_inout)", who); return CSS_ERR_ARG; }
+  return CSS_OK;
+}
+
+// m0 and vol of the resident state (mhdsph_mpi.f90:863-947) and mtot
+// (:979-999; for a closed bottom the start-up leaves mtot = m0)
+extern "C" int css_inout_init(css_ctx *c) {
+  if (int rc = need_open(c, "css_inout_init")) return rc;
+  const CssGeo &g = c->g;
+  k_plane_mass<<<g.nr, IO_NT, 0, c->stream>>>(g, c->v0, c->io_part);
+  k_mass_finish<<<1, 32, 0, c->stream>>>(g, c->io_part, c->io, IO_M0, IO_VOL);
+  k_mass_finish<<<1, 32, 0, c->stream>>>(g, c->io_part, c->io, IO_MTOT, -1);
+  if (int rc = check_launch(c)) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+extern "C" int css_inout_state(css_ctx *c, double *out) {
+  if (int rc = need_open(c, "css_inout_state")) return rc;
+  if (!out) { set_err("css_inout_state: NULL"); return CSS_ERR_ARG; }
+  double io[IO_COUNT];
+  CUDA_TRY(cudaMemcpyAsync(io, c->io, sizeof io, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  out[0] = io[IO_M0]; out[1] = io[IO_VOL]; out[2] = io[IO_MTOT]; out[3] = io[IO_ASH_FEN_MOD];
+  return CSS_OK;
+}
+
+extern "C" int css_set_rain_fields(css_ctx *c, const double *dvel_rain, const double *dent_rain) {
+  if (int rc = need_open(c, "css_set_rain_fields")) return rc;
+  if (!dvel_rain || !dent_rain) { set_err("css_set_rain_fields: NULL"); return CSS_ERR_ARG; }
+  const size_t np = (size_t)c->p.nth * c->p.nphi;
+  CUDA_TRY(cudaMemcpyAsync(c->rain, dvel_rain, np * 8, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(c->rain + np, dent_rain, np * 8, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+extern "C" int css_get_rain_fields(css_ctx *c, double *dvel_rain, double *dent_rain) {
+  if (int rc = need_open(c, "css_get_rain_fields")) return rc;
+  if (!dvel_rain || !dent_rain) { set_err("css_get_rain_fields: NULL"); return CSS_ERR_ARG; }
+  const size_t np = (size_t)c->p.nth * c->p.nphi;
+  CUDA_TRY(cudaMemcpyAsync(dvel_rain, c->rain, np * 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(dent_rain, c->rain + np, np * 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+// squalls: 6 per squall (theta_loc, phi_loc, size, scaling, vel, dels); the
+// grid point of each centre follows Find_Position (entropy_rain.f90:817-824)
+extern "C" int css_build_gaussian_squalls(css_ctx *c, int nsq, const double *squalls) {
+  if (int rc = need_open(c, "css_build_gaussian_squalls")) return rc;
+  if (nsq < 0 || (nsq > 0 && !squalls)) { set_err("css_build_gaussian_squalls: bad argument"); return CSS_ERR_ARG; }
+  const css_params &p = c->p;
+  const double dth = (p.th2 - p.th1) / (double)(p.nth - 1), dphi = (p.phi2 - p.phi1) / (double)p.nphi;
+  std::vector<double> sq((size_t)8 * std::max(nsq, 1));
+  for (int i = 0; i < nsq; i++) {
+    const double *q = squalls + 6 * i;
+    if (!(q[2] > 0.0)) { set_err("css_build_gaussian_squalls: squall %d has size %g", i, q[2]); return CSS_ERR_ARG; }
+    for (int k = 0; k < 6; k++) sq[8 * i + k] = q[k];
+    const double ft = floor((q[0] - p.th1) / dth) + 1.0, fp = floor((q[1] - p.phi1) / dphi) + 1.0;
+    sq[8 * i + 6] = std::max(std::min(ft, (double)p.nth), 1.0);
+    sq[8 * i + 7] = std::max(std::min(fp, (double)p.nphi), 1.0);
+  }
+  if (nsq > c->squall_cap) {
+    cudaFree(c->squalls);
+    c->squalls = nullptr;
+    c->squall_cap = 0;
+    CUDA_TRY(cudaMalloc(&c->squalls, (size_t)8 * nsq * sizeof(double)));
+    c->squall_cap = nsq;
+  }
+  if (nsq > 0) CUDA_TRY(cudaMemcpyAsync(c->squalls, sq.data(), (size_t)8 * nsq * 8, cudaMemcpyHostToDevice, c->stream));
+  const size_t np = (size_t)p.nth * p.nphi;
+  k_squalls<<<(unsigned)((np + 255) / 256), 256, 0, c->stream>>>(c->g, c->squalls, nsq, p.phi1, p.phi2, c->rain,
+                                                                    c->rain + np);
+  if (int rc = check_launch(c)) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+extern "C" int css_set_ash_slices(css_ctx *c, const double *slices, const double *times, double ash_fen_mod) {
+  if (int rc = need_open(c, "css_set_ash_slices")) return rc;
+  if (!slices || !times) { set_err("css_set_ash_slices: NULL"); return CSS_ERR_ARG; }
+  if (!(times[2] > times[1])) { set_err("css_set_ash_slices: times[2] must exceed times[1]"); return CSS_ERR_ARG; }
+  const size_t np = (size_t)c->p.nth * c->p.nphi;
+  CUDA_TRY(cudaMemcpyAsync(c->ash_slices, slices, 16 * np * 8, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaMemcpyAsync(c->io + IO_ASH_FEN_MOD, &ash_fen_mod, 8, cudaMemcpyHostToDevice, c->stream));
+  for (int k = 0; k < 4; k++) c->ash_times[k] = times[k];
+  if (int rc = ash_refresh(c)) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
   return CSS_OK;
 }

@@ -61,6 +61,19 @@ struct CssGeo {
   double tinyvar[8], inv_tinyvar[8];  // floors of the SLD limiter and their reciprocals
   int nsld, varlist[8];
   int dstype, mass_diffusion, do_viscous_heating, do_ohmic_heating;
+  // open radial boundaries (Top_/Bottom_Inflow_Outflow, rhs_mpi.f90:1857-2067)
+  int top_inout, bot_inout, bottom_specified, rain;
+  double delta_s;
+  const double *inout;                  // face scalars of the current RHS (k_inout_scalars)
+  const double *dvel_rain, *dent_rain;  // rain fields (nth*nphi)
+  const double *ashv;                   // prescribed bottom fields u_r, u_theta, u_phi, s (4 x nth*nphi)
+};
+
+// slots of CssGeo::inout
+enum {
+  IO_TOP_TAU, IO_TOP_MEANU, IO_TOP_MEANS, IO_TOP_MDVEL, IO_TOP_TAUR, IO_TOP_NRAT,
+  IO_BOT_TAU, IO_BOT_MEANU, IO_BOT_MEANS, IO_BOT_NRAT, IO_BOT_TCONST, IO_BOT_FEN,
+  IO_M0, IO_VOL, IO_MTOT, IO_ASH_FEN_MOD, IO_COUNT
 };
 
 __host__ __device__ inline size_t css_idx(const CssGeo &g, int it, int ip, int ir) {

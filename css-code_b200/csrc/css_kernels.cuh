@@ -692,6 +692,45 @@ __device__ __forceinline__ void radial_point(const CssGeo &g, int ir, const RadI
   }
 }
 
+// The face-plane relaxation of an open radial boundary at one point of the
+// radial tile: hl is the point's row of the tile (w, v, u, s at 0..3 HS),
+// q its plane index.  Top: rhs_mpi.f90:2042-2066; bottom: :1913-1952.
+__device__ __forceinline__ void inout_face(const CssGeo &g, int j, int m, bool top, const double *hl, int SR,
+                                           size_t HS, size_t q, double &drho, double &dw, double &dvv, double &du,
+                                           double &ds) {
+  const double *io = g.inout;
+  if (top) {
+    if (j != m - 1) return;
+    const double ut = hl[2 * HS], st = hl[3 * HS], ub = hl[2 * HS - SR], sb = hl[3 * HS - SR];
+    if (g.rain) {
+      const double taur = io[IO_TOP_TAUR];
+      du = du + (io[IO_TOP_MDVEL] + g.dvel_rain[q] + ub - 2.0 * ut) * taur + io[IO_TOP_MEANU];
+      ds = ds + (g.sr[0] + g.delta_s + g.dent_rain[q] + sb - 2.0 * st) * taur;
+    } else {
+      const double tau = io[IO_TOP_TAU];
+      du = du + tau * (io[IO_TOP_NRAT] * ub - ut) + io[IO_TOP_MEANU];
+      ds = ds + tau * (sb - st) + io[IO_TOP_MEANS];
+    }
+    return;
+  }
+  if (j != 0) return;
+  const double u0 = hl[2 * HS], s0 = hl[3 * HS], tau = io[IO_BOT_TAU];
+  if (g.bottom_specified) {
+    const size_t np = (size_t)g.nth * g.nphi;
+    const double tc = io[IO_BOT_TCONST];
+    drho = drho + io[IO_BOT_MEANU];
+    dw = dw + tau * (tc * g.ashv[np + q] - hl[0]);
+    dvv = dvv + tau * (tc * g.ashv[2 * np + q] - hl[HS]);
+    du = du + tau * (tc * g.ashv[q] - u0);
+    ds = ds + tau * ((g.sr[0] + io[IO_BOT_FEN] * g.ashv[3 * np + q]) - s0);
+  } else {
+    const double ua = hl[2 * HS + SR], sa = hl[3 * HS + SR];
+    drho = drho + io[IO_BOT_TCONST];
+    du = du + tau * (io[IO_BOT_NRAT] * ua - u0) + io[IO_BOT_MEANU];
+    ds = ds + tau * (sa - s0 + io[IO_BOT_MEANS]);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Radial_Terms (rhs_mpi.f90:1264-1519) + Density_Terms_Radial (:1710-1855)
 // grid: x = r block * nchunk + theta chunk, y = phi.
@@ -742,7 +781,12 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
     for (int k = 5; k < nh; k++) tile_r<MT, TLC>(g, fb[k - 5], H + k * HS, SR, r0, m, tb, TL, ip);
   }
   const int var[8] = {2, 3, 4, 5, 5, 1, 7, 8};
-  for (int k = 0; k < nd; k++) stage_table(g, 0, br, k == 4 ? 2 : 1, g.ibcr[var[k]], m, Tb + k * TS);
+  // open faces (a radial block has at most one physical face): the top one
+  // takes d(rho)/dr with bdry 2 and no datum, the bottom one with the datum
+  // left in x-space (rhs_mpi.f90:2020-2023, :1895-1898)
+  const bool top_open = D.rphys[br] && g.top_inout, bot_open = D.lphys[br] && g.bot_inout;
+  auto bdry_of = [&](int k) { return (k == 5 && top_open) ? 2 : g.ibcr[var[k]]; };
+  for (int k = 0; k < nd; k++) stage_table(g, 0, br, k == 4 ? 2 : 1, bdry_of(k), m, Tb + k * TS);
   __syncthreads();
   const int nr = g.nr;
   for (int task = threadIdx.x; task < solve_tasks<TLC>(nd, TL); task += blockDim.x) {
@@ -753,7 +797,7 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
     int hk = (k <= 3) ? k : (k == 4 ? 3 : (k == 5 ? 4 : k - 1));
     const double *x = H + hk * HS + 4 * SR + l;
     double *o = O + k * OS + l;
-    int bdry = g.ibcr[var[k]];
+    int bdry = bdry_of(k);
     double lo = 0.0, hi = 0.0;
     if (k == 0 || k == 1) {  // stress-free datum w/r/dxdr (rhs_mpi.f90:578-614)
       if (D.lphys[br] && g.bottom_stress_free) lo = x[0] / g.r1 / g.dxdr[0];
@@ -766,6 +810,8 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
       lo = g.s_flux_lo;
       hi = g.s_flux_hi;
     }
+    if (bot_open) lo = 0.0;  // open faces: data of w, v, u, s zero (rhs_mpi.f90:594-596, :626-628)
+    if (top_open) hi = 0.0;
     if (k == 4)
       solve<2, MT>(x, SR, m, dtype, bdry, lo, hi, Tb + k * TS, m + 2, D.dnum[br], D.dnum[br] * D.dnum[br], 0, o, SR);
     else
@@ -789,7 +835,7 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
     return id;
   };
   // hydrostatic datum of d(rho)/dr on a physical face (rhs_mpi.f90:1750-1768)
-  const int phys = D.lphys[br] ? 1 : (D.rphys[br] ? 2 : 0);
+  const int phys = D.lphys[br] ? 1 : (D.rphys[br] && !top_open ? 2 : 0);
   if (phys) {
     for (int l = threadIdx.x; l < TL; l += blockDim.x) {
       if (tb + l >= g.nth) continue;
@@ -799,9 +845,13 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
       double drho = dv[id], dw = dv[n + id], dvv = dv[2 * n + id], du = dv[3 * n + id], ds = dv[4 * n + id];
       radial_point(g, r0 + j, q, drho, dw, dvv, du, ds);
       double d;
-      if (g.lbcr_rho == 4 || g.lbcr_rho == (phys == 1 ? 2 : 3)) d = du * q.rho * g.invpconst / q.t;
-      else d = q.rho;
-      if (g.non_uniform) d = d / g.dxdr[phys == 1 ? 0 : nr - 1];
+      if (bot_open) {
+        d = g.invpconst * q.rho * du / q.t;  // rhs_mpi.f90:1894
+      } else {
+        if (g.lbcr_rho == 4 || g.lbcr_rho == (phys == 1 ? 2 : 3)) d = du * q.rho * g.invpconst / q.t;
+        else d = q.rho;
+        if (g.non_uniform) d = d / g.dxdr[phys == 1 ? 0 : nr - 1];
+      }
       datum[l] = d;
     }
     __syncthreads();
@@ -846,10 +896,20 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
       // Density_Terms_Radial
       double w1 = O[5 * OS + (size_t)j * SR + l];
       if (phys) w1 = w1 + datum[l] * resp[j + 1];
-      if (g.non_uniform) w1 = w1 * g.dxdr[ir];
-      drho = drho - q.u * w1;
-      w1 = w1 * (1.0 / q.rho);
-      du = du - g.pconst * q.t * w1;
+      if (top_open || bot_open) {
+        // Top_/Bottom_Inflow_Outflow: no dxdr, their own product orders
+        // (rhs_mpi.f90:2032-2033, :1906-1907), then the face plane's
+        // relaxation (:2042-2066, :1913-1952)
+        drho = drho - q.u * w1;
+        if (top_open) du = du - g.pconst * q.t * (1.0 / q.rho) * w1;
+        else du = du - g.pconst * q.t * w1 * (1.0 / q.rho);
+        inout_face(g, j, m, top_open, hl, SR, HS, base + l, drho, dw, dvv, du, ds);
+      } else {
+        if (g.non_uniform) w1 = w1 * g.dxdr[ir];
+        drho = drho - q.u * w1;
+        w1 = w1 * (1.0 / q.rho);
+        du = du - g.pconst * q.t * w1;
+      }
       if (g.rad_lnrho_r) {  // kept for the radiative pass (rhs_mpi.f90:1454, :1821)
         g.rad_lnrho_r[id] = w1;
         g.rad_dsdr[id] = g.non_uniform ? q.ds_r * g.dxdr[ir] : q.ds_r;
@@ -1038,9 +1098,9 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
           if (iv == 3 && !g.theta_stress_free && twall) o = 0.0;
           if (rlo) {
             if ((iv == 1 || iv == 2) && !g.bottom_stress_free) o = 0.0;
-            if (iv == 3) o = 0.0;
+            if (iv == 3 && !g.bot_inout) o = 0.0;
           }
-          if (rhi) {
+          if (rhi && !g.top_inout) {  // an open top keeps every field (rhs_mpi.f90:2420-2432)
             if ((iv == 1 || iv == 2) && !g.top_stress_free) o = 0.0;
             if (iv == 3) o = 0.0;
           }

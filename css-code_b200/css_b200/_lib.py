@@ -89,6 +89,14 @@ def lib():
         L.css_mlp_grads.argtypes = [vp, ctypes.c_int, fp, fp]
         L.css_mlp_set_stream.argtypes = [vp, vp]
         L.css_mlp_set_fused.argtypes = [vp, ctypes.c_int]
+        L.css_set_clock.argtypes = [vp, ll, ctypes.c_double, ctypes.c_double]
+        L.css_get_clock.argtypes = [vp, ctypes.POINTER(ll), dp]
+        L.css_inout_init.argtypes = [vp]
+        L.css_inout_state.argtypes = [vp, dp]
+        L.css_set_rain_fields.argtypes = [vp, dp, dp]
+        L.css_get_rain_fields.argtypes = [vp, dp, dp]
+        L.css_build_gaussian_squalls.argtypes = [vp, ctypes.c_int, dp]
+        L.css_set_ash_slices.argtypes = [vp, dp, dp, ctypes.c_double]
         _LIB = L
     return _LIB
 
@@ -109,5 +117,7 @@ EXPORTS = [
     "css_ensemble_launches", "css_ensemble_last_ms", "css_ensemble_destroy", "css_set_sld_speed2", "css_box_filter",
     "css_closure_scales", "css_closure_features", "css_closure_targets", "css_closure_speed2", "css_mlp_create",
     "css_mlp_destroy", "css_mlp_dims", "css_mlp_forward", "css_mlp_train_step", "css_mlp_params", "css_mlp_grads",
-    "css_mlp_set_stream", "css_mlp_set_fused",
+    "css_mlp_set_stream", "css_mlp_set_fused", "css_set_clock", "css_get_clock", "css_inout_init",
+    "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_gaussian_squalls",
+    "css_set_ash_slices",
 ]

@@ -171,6 +171,46 @@ class Simulation:
         check(_lib.lib().css_diffusion(self.h, _p(v), _p(a), _p(dv)))
         return v, dv
 
+    # open radial boundaries (top_inout / bot_inout) ---------------------------
+    def set_clock(self, istep, sim_time, deltat):
+        """istep: the step index the RHS sees; deltat: the step size of the
+        mean-flow terms for ``rhs`` (the step calls set it to their dt)."""
+        check(_lib.lib().css_set_clock(self.h, int(istep), float(sim_time), float(deltat)))
+
+    def clock(self):
+        i, t = ctypes.c_longlong(), ctypes.c_double()
+        check(_lib.lib().css_get_clock(self.h, ctypes.byref(i), ctypes.byref(t)))
+        return i.value, t.value
+
+    def inout_init(self):
+        """m0, vol and mtot of the resident state, as the start-up computes them."""
+        check(_lib.lib().css_inout_init(self.h))
+
+    def inout_state(self):
+        out = np.zeros(4)
+        check(_lib.lib().css_inout_state(self.h, _p(out)))
+        return dict(zip(("m0", "vol", "mtot", "ash_fen_mod"), out.tolist()))
+
+    def set_rain_fields(self, dvel, dent):
+        check(_lib.lib().css_set_rain_fields(self.h, _p(np.ascontiguousarray(dvel, dtype=np.float64)),
+                                             _p(np.ascontiguousarray(dent, dtype=np.float64))))
+
+    def rain_fields(self):
+        dvel = np.zeros((self.p.nphi, self.p.nth))
+        dent = np.zeros_like(dvel)
+        check(_lib.lib().css_get_rain_fields(self.h, _p(dvel), _p(dent)))
+        return dvel, dent
+
+    def build_gaussian_squalls(self, squalls):
+        """squalls: (nsq, 6) theta_loc, phi_loc, size, scaling, vel, dels."""
+        sq = np.ascontiguousarray(squalls, dtype=np.float64).reshape(-1, 6)
+        check(_lib.lib().css_build_gaussian_squalls(self.h, sq.shape[0], _p(sq)))
+
+    def set_ash_slices(self, slices, times, ash_fen_mod):
+        """slices: (4 times, 4 fields u_r, u_theta, u_phi, s, nphi, nth)."""
+        check(_lib.lib().css_set_ash_slices(self.h, _p(np.ascontiguousarray(slices, dtype=np.float64)),
+                                            _p(np.ascontiguousarray(times, dtype=np.float64)), float(ash_fen_mod)))
+
     def deriv(self, direction, order, x, bc_lo=None, bc_hi=None, bdry=1):
         x = np.ascontiguousarray(x, dtype=np.float64)
         out = np.zeros_like(x)

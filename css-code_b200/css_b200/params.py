@@ -34,6 +34,10 @@ _FIELDS = [
     ("time_stepper", ctypes.c_int),
     ("laplacian", ctypes.c_int),
     ("do_radheat", ctypes.c_int),
+    ("top_inout", ctypes.c_int), ("bot_inout", ctypes.c_int),
+    ("bottom_specified", ctypes.c_int), ("do_entropy_rain", ctypes.c_int),
+    ("ufreq", ctypes.c_int),
+    ("delta_s", ctypes.c_double),
 ]
 
 
@@ -102,4 +106,5 @@ def default_params(nr, nth, nphi, decomp, magnetic=False):
     p.flux_limiter = p.ent_flux_limiter = p.mag_flux_limiter = -1
     p.precision = 0
     p.time_stepper = 4
+    p.ufreq = 100
     return p

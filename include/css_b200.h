@@ -106,6 +106,20 @@ typedef struct css_params {
   int do_radheat;             /* 1: radiative diffusion of heat (rhs_mpi.f90:
                                  388-393, :1092-1106, :1590-1602, :1820-1853);
                                  also turns the top thermal damping off      */
+  /* open radial boundaries (constants.f90:55, :69-72; hydro FP64 only) */
+  int top_inout;              /* 1: inflow/outflow top, Top_Inflow_Outflow
+                                 (rhs_mpi.f90:1955-2067): u_r free at r2,
+                                 top plane relaxed toward its neighbour     */
+  int bot_inout;              /* 1: inflow/outflow bottom, Bottom_Inflow_
+                                 Outflow (rhs_mpi.f90:1857-1953)             */
+  int bottom_specified;       /* with bot_inout: bottom plane relaxed toward
+                                 prescribed fields (the ASH inflow slices,
+                                 css_set_ash_slices)                        */
+  int do_entropy_rain;        /* with top_inout: top relaxation toward the
+                                 rain-squall fields (css_set_rain_fields)   */
+  int ufreq;                  /* step cadence of the mass-total refresh and
+                                 the ASH enthalpy-flux factor (<= 0: never) */
+  double delta_s;             /* entropy offset of the top relaxation       */
 } css_params;
 
 typedef struct css_ctx css_ctx;
@@ -393,6 +407,53 @@ int css_shell_averages(css_ctx *ctx, const int *quantities, int nq,
  * energy density rho|u|^2/2, 1 = magnetic energy density |B|^2/(8 pi),
  * 2+iv = state variable iv.  nth and nphi must be even.                    */
 int css_spectrum(css_ctx *ctx, int kind, double *out);
+
+/* ---- open radial boundaries (top_inout / bot_inout) ---------------------
+ * The reference's Top_Inflow_Outflow and Bottom_Inflow_Outflow
+ * (rhs_mpi.f90:1857-2067) read run state beyond the fields: the step index
+ * and time of Program CSS2's loop (mhdsph_mpi.f90:28-43), the step size, the
+ * mass totals m0, vol and mtot, the rain fields of the squall model and the
+ * prescribed (ASH) bottom fields.  These calls set and read that state; the
+ * step entry points advance it.  Every call returns CSS_ERR_ARG on a run
+ * without an open boundary (except the clock, which every run keeps).     */
+
+/* The clock: istep = the step index the RHS sees (the last step started),
+ * sim_time, and deltat, the step size of the mean-flow terms
+ * (rhs_mpi.f90:1882, :2012) for the RHS entry point.  Each step advances
+ * istep by one before it and sim_time by dt after it, and sets deltat = dt.
+ * Defaults 0, 0, 0.                                                        */
+int css_set_clock(css_ctx *ctx, long long istep, double sim_time, double deltat);
+int css_get_clock(css_ctx *ctx, long long *istep, double *sim_time);
+
+/* Mass bookkeeping of the start-up (mhdsph_mpi.f90:863-947, :979-999): m0,
+ * vol and mtot of the resident state.  The RHS refreshes mtot at the first
+ * call of every step whose index is a multiple of ufreq (rhs_mpi.f90:
+ * 326-353).  css_inout_state: out[0..3] = m0, vol, mtot, ash_fen_mod.     */
+int css_inout_init(css_ctx *ctx);
+int css_inout_state(css_ctx *ctx, double *out);
+
+/* Entropy rain (do_entropy_rain): the squall fields dvel_rain, dent_rain
+ * (entropy_rain.f90:40; nth*nphi each, [it + nth*ip]) the top relaxation
+ * reads, set directly or built from squalls by Build_Gaussian_Squalls
+ * (entropy_rain.f90:423-523): squalls[6*k ..] = theta_loc, phi_loc, size,
+ * scaling, vel, dels.  The squall life cycle (Update_Rain_Squalls, :171-421)
+ * is the caller's, between steps, as in the reference.  Host pointers.     */
+int css_set_rain_fields(css_ctx *ctx, const double *dvel_rain, const double *dent_rain);
+int css_get_rain_fields(css_ctx *ctx, double *dvel_rain, double *dent_rain);
+int css_build_gaussian_squalls(css_ctx *ctx, int nsq, const double *squalls);
+
+/* Prescribed bottom (bottom_specified): the four time slices of the ASH
+ * fields after the reader's spatial interpolation and wall taper
+ * (ash_inflow.f90:18-120), slices[((is*4 + iq)*nphi + ip)*nth + it] with
+ * iq = 0 u_r, 1 u_theta, 2 u_phi, 3 entropy (ashvars(:,:,1..4)); their
+ * times (ashtimes, from the data's start); and the enthalpy-flux factor
+ * ash_fen_mod.  Each step interpolates the slices at its start time
+ * (Cubic_Time_Interp, :188-219); a step that would start at sim_time >=
+ * times[2] returns CSS_ERR_ARG, as the reference would read the next slice
+ * there (Read_ASH_Inflow, :124-186): the caller shifts it in first.  Every
+ * ufreq steps ash_fen_mod is updated from the bottom enthalpy flux
+ * (ASH_Enthalpy_Flux, step_rk4.f90:495-518).  Host pointers.              */
+int css_set_ash_slices(css_ctx *ctx, const double *slices, const double *times, double ash_fen_mod);
 
 #ifdef __cplusplus
 }

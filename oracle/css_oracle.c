@@ -88,6 +88,16 @@ struct orc_ctx {
   /* radiative diffusion: rad1 = (4 a c kr / 3) T^3 / rho^2 and rad2 = ds/dr,
    * the reference's dvars2(:,:,:,1:2) under do_radheat */
   double *rad1, *rad2;
+  /* open radial boundaries (rhs_mpi.f90:1857-2067): the run's clock (the
+   * step index the RHS sees, sim_time, deltat), the mass totals m0, vol,
+   * mtot (rhs_mpi.f90:10), the rain fields dvel_rain / dent_rain
+   * (entropy_rain.f90:40), the ASH slices and times with the prescribed
+   * bottom fields interpolated from them (ashvars, ash_inflow.f90:12-13)
+   * and the enthalpy-flux factor ash_fen_mod */
+  long long istep;
+  double sim_time, deltat, m0, vol, mtot, ash_fen_mod;
+  double *dvel_rain, *dent_rain, *ash_slices, *ashv;
+  double ash_times[4];
 };
 enum { LAP_W1 = 0, LAP_V1, LAP_U1, LAP_PV, LAP_PW, LAP_PU, LAP_N };
 
@@ -562,6 +572,7 @@ void orc_destroy(orc_ctx *c) {
   free(c->theta); free(c->phi); free(c->sines); free(c->cosines); free(c->dspeed);
   free(c->temperature); free(c->invrho); free(c->maga); free(c->vars2); free(c->vars_save);
   free(c->dvars1); free(c->vars1); free(c->tmpf); free(c->tmpg); free(c->da);
+  free(c->dvel_rain); free(c->dent_rain); free(c->ash_slices); free(c->ashv);
   free(c);
 }
 
@@ -571,6 +582,17 @@ int orc_create(const css_params *p, const double *prof, orc_ctx **out) {
   if (p->nnr < 2 || p->nnt < 2 || p->nnp < 3) {
     set_err("orc_create: the reference needs nnr>=2, nnt>=2 (no dtype 0 case) and nnp>=3 (phi halos)");
     return CSS_ERR_DECOMP;
+  }
+  if (p->top_inout || p->bot_inout || p->bottom_specified || p->do_entropy_rain) {
+    if (p->magnetic || p->laplacian || p->do_radheat || p->precision) {
+      set_err("orc_create: open radial boundaries are restated for hydro FP64 runs without explicit viscosity "
+              "or radiative diffusion");
+      return CSS_ERR_ARG;
+    }
+    if ((p->bottom_specified && !p->bot_inout) || (p->do_entropy_rain && !p->top_inout)) {
+      set_err("orc_create: bottom_specified needs bot_inout and do_entropy_rain needs top_inout");
+      return CSS_ERR_ARG;
+    }
   }
   if (p->flux_limiter > 0 || p->ent_flux_limiter > 0 || p->mag_flux_limiter > 0) {
     set_err("orc_create: SLD power flux limiters are not restated (all configs keep them off)");
@@ -614,7 +636,7 @@ int orc_create(const css_params *p, const double *prof, orc_ctx **out) {
   c->invtconst = c->invcv / c->gamm1;
 
   /* BC integers (Read_Input, mhdsph_mpi.f90:1317-1461) */
-  int lbcr_v, lbcr_s, lbcr_u = 1, lbcr_rho = 4, lbcr_t = 4;
+  int lbcr_v, lbcr_s, lbcr_u = p->top_inout ? 3 : 1, lbcr_rho = 4, lbcr_t = 4; /* mhdsph_mpi.f90:1355-1359 */
   int tn = !p->top_stress_free, bn = !p->bottom_stress_free;
   if (tn && bn) lbcr_v = 1;
   else if (tn && !bn) lbcr_v = 2;
@@ -730,6 +752,11 @@ even:
   if (p->laplacian) c->lap = dalloc(n * LAP_N);
   if (p->do_radheat) { c->rad1 = dalloc(n); c->rad2 = dalloc(n); }
   c->cond = p->slaplacian || p->laplacian;
+  if (p->top_inout || p->bot_inout) {
+    size_t np = (size_t)nth * nphi;
+    c->dvel_rain = dalloc(np); c->dent_rain = dalloc(np);
+    c->ash_slices = dalloc(16 * np); c->ashv = dalloc(4 * np);
+  }
   *out = c;
   return CSS_OK;
 }
@@ -1308,6 +1335,8 @@ static void radial_terms(orc_ctx *c, const blk_t *B, const double *v1, double *d
       if (p->bottom_stress_free) lo = wF[IDX(c, it, ip, 0)] / p->r1 / c->dxdr[0];
       if (p->top_stress_free) hi = wF[IDX(c, it, ip, nr - 1)] / p->r2 / c->dxdr[nr - 1];
       else hi = wF[IDX(c, it, ip, nr - 1)];
+      if (p->bot_inout) lo = 0.0; /* open faces: data 2:5 zero (rhs_mpi.f90:594-596, :626-628) */
+      if (p->top_inout) hi = 0.0;
       line_deriv(c, B, 0, 1, wF, it, ip, c->ibcr[2], lo, hi, w1);
       for (int j = 1; j <= m; j++) {
         size_t id = RI_(j);
@@ -1349,6 +1378,8 @@ static void radial_terms(orc_ctx *c, const blk_t *B, const double *v1, double *d
       if (p->bottom_stress_free) lo = vF[IDX(c, it, ip, 0)] / p->r1 / c->dxdr[0];
       if (p->top_stress_free) hi = vF[IDX(c, it, ip, nr - 1)] / p->r2 / c->dxdr[nr - 1];
       else hi = vF[IDX(c, it, ip, nr - 1)];
+      if (p->bot_inout) lo = 0.0;
+      if (p->top_inout) hi = 0.0;
       line_deriv(c, B, 0, 1, vF, it, ip, c->ibcr[3], lo, hi, w1);
       for (int j = 1; j <= m; j++) {
         size_t id = RI_(j);
@@ -1409,6 +1440,8 @@ static void radial_terms(orc_ctx *c, const blk_t *B, const double *v1, double *d
         if (c->cond) hi = -p->lumr2 * ONE_OVER_4PI / (p->r2 * p->r2 * c->ks[nr - 1] * c->dxdr[nr - 1]);
         else hi = 0.0 / c->dxdr[nr - 1];
       }
+      if (p->bot_inout) lo = 0.0;
+      if (p->top_inout) hi = 0.0;
       line_deriv(c, B, 0, 1, sF, it, ip, c->ibcr[5], lo, hi, w1);
       for (int j = 1; j <= m; j++) {
         size_t id = RI_(j);
@@ -1586,6 +1619,173 @@ static void density_terms_radial(orc_ctx *c, const blk_t *B, const double *v1, d
         }
       }
     }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Open radial boundaries.  On the blocks of an open face Top_Inflow_Outflow */
+/* (rhs_mpi.f90:1955-2067) or Bottom_Inflow_Outflow (:1857-1953) replaces    */
+/* Density_Terms_Radial (:723-729): d(rho)/dr with the open closure, then   */
+/* the face plane relaxed toward its inner neighbour with mean-flow and     */
+/* mean-entropy corrections from sums over the whole face (the top_comm /   */
+/* bot_comm reductions).  Neither routine applies the non-uniform dxdr to   */
+/* d(rho)/dr or its datum, unlike Density_Terms_Radial; restated as written. */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  double top[4]; /* sum u rho sin, sum rho sin, sum s, sum rho sin (dvel_rain + u(nr-1)) */
+  double bot[4]; /* sum rho(mynr) sin u(1), sum rho(mynr) sin, sum s(1), max of |min u(2)| */
+} inout_sums_t;
+
+/* Tr(nr) of the Isentropic background: T0 (mhdsph_mpi.f90:343 at r = r2) */
+static double tr_top(const orc_ctx *c) { return c->p.t0; }
+
+static void inout_sums(orc_ctx *c, const double *v1, inout_sums_t *S) {
+  const css_params *p = &c->p;
+  size_t n = c->ncell;
+  int nr = c->nr;
+  memset(S, 0, sizeof *S);
+  for (int k = 0; k < c->nblk; k++) {
+    const blk_t *B = &c->blk[k];
+    if (p->top_inout && B->rhi) { /* rhs_mpi.f90:1987-1998 / :1971-1985 */
+      double a[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+        for (int it = B->t0; it < B->t0 + B->nt; it++) {
+          size_t id = IDX(c, it, ip, nr - 1);
+          double tau = v1[id] * c->sines[it];
+          a[0] = a[0] + v1[3 * n + id] * tau;
+          a[1] = a[1] + tau;
+          a[2] = a[2] + v1[4 * n + id];
+          if (p->do_entropy_rain)
+            a[3] = a[3] + tau * (c->dvel_rain[it + (size_t)c->nth * ip] + v1[3 * n + IDX(c, it, ip, nr - 2)]);
+        }
+      for (int q = 0; q < 4; q++) S->top[q] += a[q];
+    }
+    if (p->bot_inout && B->rlo && !p->bottom_specified) { /* rhs_mpi.f90:1865-1884 */
+      double a[3] = {0.0, 0.0, 0.0}, umin = 0.0;
+      int first = 1, mt = B->nr - 1; /* the block's own top radius (mynr) */
+      for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+        for (int it = B->t0; it < B->t0 + B->nt; it++) {
+          double tau = v1[IDX(c, it, ip, mt)] * c->sines[it];
+          a[0] = a[0] + tau * v1[3 * n + IDX(c, it, ip, 0)];
+          a[1] = a[1] + tau;
+          a[2] = a[2] + v1[4 * n + IDX(c, it, ip, 0)];
+          double u2 = v1[3 * n + IDX(c, it, ip, 1)];
+          if (first || u2 < umin) umin = u2;
+          first = 0;
+        }
+      for (int q = 0; q < 3; q++) S->bot[q] += a[q];
+      S->bot[3] = fmax(S->bot[3], fabs(umin)); /* 'csm': sums, then the max (mhdsph_mpi.f90:1511-1521) */
+    }
+  }
+}
+
+static void top_inflow_outflow(orc_ctx *c, const blk_t *B, const double *v1, double *dv1, const inout_sums_t *S) {
+  const css_params *p = &c->p;
+  size_t n = c->ncell;
+  int nr = c->nr;
+  const double *rhoF = v1, *uF = v1 + 3 * n, *sF = v1 + 4 * n;
+  double ntot = (double)c->nth * (double)c->nphi;
+  double meanu = -S->top[0] / S->top[1] / c->deltat;
+  double means = c->sr[0] + p->delta_s - S->top[2] / ntot;
+  double mdvel = -S->top[3] / S->top[1];
+  double tau = sqrt(c->gamm1 * p->cp * tr_top(c)) / c->dr_ind[nr - 1] / 20.0;
+  means = tau * means;
+  double nrat = c->rhor[nr - 2] / c->rhor[nr - 1];
+  double q4 = (c->r_ind[nr - 1] - c->r_ind[B->r0]) / (p->r2 - c->r_ind[B->r0]);
+  q4 = (q4 * q4) * (q4 * q4);
+  double taur = sqrt(c->gamm1 * p->cp * tr_top(c)) * q4 / c->dr_ind[nr - 1] / 2.0;
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+    for (int it = B->t0; it < B->t0 + B->nt; it++) {
+      int m = B->nr, r0 = B->r0;
+      double w1[m + 2];
+      line_deriv(c, B, 0, 1, rhoF, it, ip, 2, 0.0, 0.0, w1); /* dbydr(rho, ..., bc1, 0, -2) */
+      for (int j = 1; j <= m; j++) {
+        size_t id = IDX(c, it, ip, r0 + j - 1);
+        dv1[id] = dv1[id] - uF[id] * w1[j];
+        dv1[3 * n + id] = dv1[3 * n + id] - c->pconst * c->temperature[id] * c->invrho[id] * w1[j];
+      }
+      size_t top = IDX(c, it, ip, nr - 1), below = IDX(c, it, ip, nr - 2);
+      if (p->do_entropy_rain) { /* rhs_mpi.f90:2042-2054 */
+        size_t q = it + (size_t)c->nth * ip;
+        dv1[3 * n + top] = dv1[3 * n + top] +
+                           (mdvel + c->dvel_rain[q] + uF[below] - 2.0 * uF[top]) * taur + meanu;
+        dv1[4 * n + top] = dv1[4 * n + top] +
+                           (c->sr[0] + p->delta_s + c->dent_rain[q] + sF[below] - 2.0 * sF[top]) * taur;
+      } else { /* :2055-2066 */
+        dv1[3 * n + top] = dv1[3 * n + top] + tau * (nrat * uF[below] - uF[top]) + meanu;
+        dv1[4 * n + top] = dv1[4 * n + top] + tau * (sF[below] - sF[top]) + means;
+      }
+    }
+}
+
+static void bottom_inflow_outflow(orc_ctx *c, const blk_t *B, const double *v1, double *dv1,
+                                  const inout_sums_t *S) {
+  const css_params *p = &c->p;
+  size_t n = c->ncell;
+  const double *rhoF = v1, *wF = v1 + n, *vF = v1 + 2 * n, *uF = v1 + 3 * n, *sF = v1 + 4 * n;
+  double meanu = 0.0, means = 0.0, tau = 0.0, nrat = 0.0, tconst;
+  if (!p->bottom_specified) {
+    double ntot = (double)c->nth * (double)c->nphi;
+    meanu = -S->bot[0] / S->bot[1] / c->deltat;
+    means = c->sr[0] - S->bot[2] / ntot;
+    tau = S->bot[3] / c->dr_ind[0];
+    nrat = c->rhor[1] / c->rhor[0];
+  }
+#pragma omp parallel for collapse(2) schedule(static)
+  for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+    for (int it = B->t0; it < B->t0 + B->nt; it++) {
+      int m = B->nr, r0 = B->r0;
+      double w1[m + 2];
+      size_t i0 = IDX(c, it, ip, r0);
+      double lo = c->invpconst * rhoF[i0] * dv1[3 * n + i0] / c->temperature[i0];
+      line_deriv(c, B, 0, 1, rhoF, it, ip, 4, lo, 0.0, w1); /* dbydr(rho, ..., bc1, bc2, -4) */
+      for (int j = 1; j <= m; j++) {
+        size_t id = IDX(c, it, ip, r0 + j - 1);
+        dv1[id] = dv1[id] - uF[id] * w1[j];
+        dv1[3 * n + id] = dv1[3 * n + id] - c->pconst * c->temperature[id] * w1[j] * c->invrho[id];
+      }
+    }
+  if (p->bottom_specified) { /* rhs_mpi.f90:1913-1938 */
+    tau = sqrt(c->gamm1 * p->cp * tr_top(c)) / (20.0 * c->dr_ind[0]);
+    tconst = fmin(fabs(c->sim_time) / 1e5, 1.0);
+    meanu = tau * (c->m0 - c->mtot) / c->vol;
+    size_t np = (size_t)c->nth * c->nphi;
+    for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+      for (int it = B->t0; it < B->t0 + B->nt; it++) {
+        size_t id = IDX(c, it, ip, 0), q = it + (size_t)c->nth * ip;
+        const double *a = c->ashv;
+        dv1[id] = dv1[id] + meanu;
+        dv1[n + id] = dv1[n + id] + tau * (tconst * a[np + q] - wF[id]);
+        dv1[2 * n + id] = dv1[2 * n + id] + tau * (tconst * a[2 * np + q] - vF[id]);
+        dv1[3 * n + id] = dv1[3 * n + id] + tau * (tconst * a[q] - uF[id]);
+        dv1[4 * n + id] = dv1[4 * n + id] + tau * ((c->sr[0] + tconst * c->ash_fen_mod * a[3 * np + q]) - sF[id]);
+      }
+  } else { /* :1939-1952 */
+    tconst = tau * (c->m0 - c->mtot) / c->vol;
+    for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+      for (int it = B->t0; it < B->t0 + B->nt; it++) {
+        size_t id = IDX(c, it, ip, 0), up = IDX(c, it, ip, 1);
+        dv1[id] = dv1[id] + tconst;
+        dv1[3 * n + id] = dv1[3 * n + id] + tau * (nrat * uF[up] - uF[id]) + meanu;
+        dv1[4 * n + id] = dv1[4 * n + id] + tau * (sF[up] - sF[id] + means);
+      }
+  }
+}
+
+/* mass total as the RHS refreshes it every ufreq steps (rhs_mpi.f90:326-353)
+ * and the start-up computes it for bot_inout (mhdsph_mpi.f90:979-999):
+ * sum over r of dr r^2 sum over the plane of sin rho, times dth dphi */
+static double mass_total(const orc_ctx *c, const double *v1) {
+  double mt = 0.0;
+  for (int ir = 0; ir < c->nr; ir++) {
+    double rt = c->dr_ind[ir] * (c->r_ind[ir] * c->r_ind[ir]);
+    for (int ip = 0; ip < c->nphi; ip++) {
+      double ln = 0.0;
+      for (int it = 0; it < c->nth; it++) ln = ln + c->sines[it] * v1[IDX(c, it, ip, ir)];
+      mt = mt + ln * rt;
+    }
+  }
+  return mt * c->dth * c->dphi;
 }
 
 /* Laplacian_Cross_Terms_Radial (rhs_mpi.f90:2070-2205): radial derivatives
@@ -1784,6 +1984,8 @@ int orc_rhs(orc_ctx *c, double *vars1, double *dvars1, int call_num) {
     memset(dvars1 + 5 * n, 0, sizeof(double) * 3 * n);
   }
   thermo(c, vars1);
+  if ((c->p.top_inout || c->p.bot_inout) && call_num == 1 && c->p.ufreq > 0 && c->istep % c->p.ufreq == 0)
+    c->mtot = mass_total(c, vars1);
   for (int k = 0; k < c->nblk; k++) source_theta_terms(c, &c->blk[k], vars1, dvars1);
   for (int k = 0; k < c->nblk; k++) phi_terms(c, &c->blk[k], vars1, dvars1);
   for (int k = 0; k < c->nblk; k++) radial_terms(c, &c->blk[k], vars1, dvars1);
@@ -1792,7 +1994,18 @@ int orc_rhs(orc_ctx *c, double *vars1, double *dvars1, int call_num) {
     lap_cross_theta(c, dvars1);
   }
   for (int k = 0; k < c->nblk; k++) density_terms_theta(c, &c->blk[k], vars1, dvars1);
-  for (int k = 0; k < c->nblk; k++) density_terms_radial(c, &c->blk[k], vars1, dvars1);
+  if (c->p.top_inout || c->p.bot_inout) {
+    inout_sums_t S;
+    inout_sums(c, vars1, &S);
+    for (int k = 0; k < c->nblk; k++) {
+      const blk_t *B = &c->blk[k];
+      if (c->p.bot_inout && B->rlo) bottom_inflow_outflow(c, B, vars1, dvars1, &S);
+      else if (c->p.top_inout && B->rhi) top_inflow_outflow(c, B, vars1, dvars1, &S);
+      else density_terms_radial(c, B, vars1, dvars1);
+    }
+  } else {
+    for (int k = 0; k < c->nblk; k++) density_terms_radial(c, &c->blk[k], vars1, dvars1);
+  }
   if (c->p.magnetic) {
     /* Induction_Terms: under Laplacian the resistive part first (rhs_mpi.f90:
      * 2303-2327): J = curl B, eta J / rho / T ohmic heating with jconst =
@@ -2343,13 +2556,15 @@ static void bound(orc_ctx *c, double *v1) {
     for (int it = 0; it < nth; it++) {
       size_t lo = IDX(c, it, ip, 0), hi = IDX(c, it, ip, nr - 1);
       if (!p->bottom_stress_free) { v1[n + lo] = 0.0; v1[2 * n + lo] = 0.0; }
-      v1[3 * n + lo] = 0.0;
+      if (!p->bot_inout) v1[3 * n + lo] = 0.0;
       if (p->bottom_constant_temp) {
         /* sr1 = vars1(:,1,1,5) of the initial state; not restated: the
          * parity configs use a constant-flux bottom */
       }
-      if (!p->top_stress_free) { v1[n + hi] = 0.0; v1[2 * n + hi] = 0.0; }
-      v1[3 * n + hi] = 0.0;
+      if (!p->top_inout) { /* an open top keeps every field (rhs_mpi.f90:2420-2432) */
+        if (!p->top_stress_free) { v1[n + hi] = 0.0; v1[2 * n + hi] = 0.0; }
+        v1[3 * n + hi] = 0.0;
+      }
     }
   if (p->magnetic) {
     for (int ir = 0; ir < nr; ir++)
@@ -2371,6 +2586,192 @@ static void bound(orc_ctx *c, double *v1) {
         else if (p->top_perfect_cond) { v1[5 * n + hi] = 0.0; v1[6 * n + hi] = 0.0; }
       }
   }
+}
+
+/* The clock around one step (Program CSS2, mhdsph_mpi.f90:28-43): the step
+ * index advances before the step and the time after it; with a prescribed
+ * bottom the ASH fields are interpolated at the step's start time
+ * (Read_ASH_Inflow -> Cubic_Time_Interp, ash_inflow.f90:124-219) and every
+ * ufreq steps the enthalpy-flux factor is updated at its end
+ * (ASH_Enthalpy_Flux, step_rk4.f90:477-482, :495-518). */
+static void ash_interp(orc_ctx *c) {
+  size_t np = (size_t)c->nth * c->nphi;
+  double mu = (c->sim_time - c->ash_times[1]) / (c->ash_times[2] - c->ash_times[1]);
+  double mu2 = mu * mu, mu3 = mu * mu2;
+  for (int iq = 0; iq < 4; iq++)
+    for (size_t q = 0; q < np; q++) {
+      double t1 = c->ash_slices[(0 * 4 + iq) * np + q], a3 = c->ash_slices[(1 * 4 + iq) * np + q];
+      double t3 = c->ash_slices[(2 * 4 + iq) * np + q], t4 = c->ash_slices[(3 * 4 + iq) * np + q];
+      double a0 = -0.5 * t1 + 1.5 * a3 - 1.5 * t3 + 0.5 * t4;
+      double a1 = t1 - 2.5 * a3 + 2.0 * t3 - 0.5 * t4;
+      double a2 = -0.5 * t1 + 0.5 * t3;
+      c->ashv[iq * np + q] = a0 * mu3 + a1 * mu2 + a2 * mu + a3;
+    }
+}
+
+static void ash_refresh(orc_ctx *c) {
+  if (c->p.bottom_specified && c->ash_times[2] > c->ash_times[1]) ash_interp(c);
+}
+
+static int step_begin(orc_ctx *c, double dt) {
+  c->istep++;
+  c->deltat = dt;
+  if (c->p.bottom_specified) {
+    if (!(c->sim_time < c->ash_times[2])) {
+      set_err("step: sim_time %.17g is past the third ASH slice time %.17g; shift in the next slice first",
+              c->sim_time, c->ash_times[2]);
+      return CSS_ERR_ARG;
+    }
+    ash_refresh(c);
+  }
+  return CSS_OK;
+}
+
+static void step_end(orc_ctx *c, const double *vars0, double dt) {
+  const css_params *p = &c->p;
+  if (p->bottom_specified && p->ufreq > 0 && c->istep % p->ufreq == 0) {
+    size_t n = c->ncell;
+    double ntot = (double)c->nphi * (double)c->nth, su = 0.0, st = 0.0, len = 0.0;
+    for (int ip = 0; ip < c->nphi; ip++)
+      for (int it = 0; it < c->nth; it++) {
+        size_t id = IDX(c, it, ip, 0);
+        su = su + vars0[3 * n + id];
+        st = st + c->temperature[id]; /* the last RHS's temperature, as the module array holds it */
+      }
+    double uravg = su / ntot, t2avg = st / ntot;
+    for (int ip = 0; ip < c->nphi; ip++)
+      for (int it = 0; it < c->nth; it++) {
+        size_t id = IDX(c, it, ip, 0);
+        len = len + vars0[id] * (vars0[3 * n + id] - uravg) * (c->temperature[id] - t2avg);
+      }
+    len = p->cp * len / ntot;
+    len = 4.0 * PI * (p->r1 * p->r1) * len / p->lumr1;
+    len = 1.3 * fmin(1.0 / fmin(2.0, fmax(0.0, fabs(len))), 2.0);
+    c->ash_fen_mod = 0.5 * (len + c->ash_fen_mod);
+    if (fmin(fabs(c->sim_time) / 1e5, 1.0) < 1.0) c->ash_fen_mod = 1.0;
+  }
+  c->sim_time = c->sim_time + dt;
+}
+
+int orc_set_clock(orc_ctx *c, long long istep, double sim_time, double deltat) {
+  c->istep = istep; c->sim_time = sim_time; c->deltat = deltat;
+  if (c->ash_slices) ash_refresh(c);
+  return CSS_OK;
+}
+
+int orc_get_clock(orc_ctx *c, long long *istep, double *sim_time) {
+  if (istep) *istep = c->istep;
+  if (sim_time) *sim_time = c->sim_time;
+  return CSS_OK;
+}
+
+/* start-up mass bookkeeping (mhdsph_mpi.f90:863-947, :979-999) */
+int orc_inout_init(orc_ctx *c, const double *vars0) {
+  double m0 = 0.0, vol = 0.0;
+  for (int ir = 0; ir < c->nr; ir++) {
+    double radius = c->r_ind[ir], drad = c->dr_ind[ir];
+    for (int it = 0; it < c->nth; it++) {
+      double sinth = c->sines[it], srho = 0.0;
+      for (int ip = 0; ip < c->nphi; ip++) srho = srho + vars0[IDX(c, it, ip, ir)];
+      m0 = m0 + radius * radius * sinth * srho * drad * c->dth * c->dphi;
+      vol = vol + sinth * radius * radius * drad * c->dth * c->dphi;
+    }
+  }
+  c->m0 = m0;
+  c->vol = vol;
+  c->mtot = c->p.bot_inout ? mass_total(c, vars0) : m0;
+  return CSS_OK;
+}
+
+int orc_inout_state(orc_ctx *c, double *out) {
+  out[0] = c->m0; out[1] = c->vol; out[2] = c->mtot; out[3] = c->ash_fen_mod;
+  return CSS_OK;
+}
+
+int orc_set_rain_fields(orc_ctx *c, const double *dvel, const double *dent) {
+  if (!c->dvel_rain) { set_err("orc_set_rain_fields: the run has no open boundary"); return CSS_ERR_ARG; }
+  size_t np = (size_t)c->nth * c->nphi;
+  memcpy(c->dvel_rain, dvel, sizeof(double) * np);
+  memcpy(c->dent_rain, dent, sizeof(double) * np);
+  return CSS_OK;
+}
+
+int orc_rain_fields(orc_ctx *c, double *dvel, double *dent) {
+  if (!c->dvel_rain) { set_err("orc_rain_fields: the run has no open boundary"); return CSS_ERR_ARG; }
+  size_t np = (size_t)c->nth * c->nphi;
+  memcpy(dvel, c->dvel_rain, sizeof(double) * np);
+  memcpy(dent, c->dent_rain, sizeof(double) * np);
+  return CSS_OK;
+}
+
+int orc_set_ash_slices(orc_ctx *c, const double *slices, const double *times, double ash_fen_mod) {
+  if (!c->ash_slices) { set_err("orc_set_ash_slices: the run has no open boundary"); return CSS_ERR_ARG; }
+  memcpy(c->ash_slices, slices, sizeof(double) * 16 * (size_t)c->nth * c->nphi);
+  memcpy(c->ash_times, times, sizeof(double) * 4);
+  c->ash_fen_mod = ash_fen_mod;
+  ash_refresh(c);
+  return CSS_OK;
+}
+
+/* Build_Gaussian_Squalls (entropy_rain.f90:423-523) on the top plane: each
+ * top block evaluates the squalls whose centre (loct, locp of Find_Position,
+ * :817-824) lies within one block width of it, with the periodic images
+ * across phi1/phi2 on the first and last phi blocks; Gaussians below 1e-5
+ * (exponent -11.5) are dropped.  The squall density 1/(1 + sum) then
+ * weights each squall's velocity and entropy.  sq: 6 per squall, theta_loc,
+ * phi_loc, size, scaling, vel, dels. */
+int orc_build_gaussian_squalls(orc_ctx *c, int nsq, const double *sq) {
+  const css_params *p = &c->p;
+  if (!c->dvel_rain) { set_err("orc_build_gaussian_squalls: the run has no open boundary"); return CSS_ERR_ARG; }
+  int nth = c->nth, nphi = c->nphi;
+  size_t np = (size_t)nth * nphi;
+  double *dens = dalloc(np);
+  memset(c->dvel_rain, 0, sizeof(double) * np);
+  memset(c->dent_rain, 0, sizeof(double) * np);
+  for (int pass = 0; pass < 2; pass++) {
+    for (int k = 0; k < c->nblk; k++) {
+      const blk_t *B = &c->blk[k];
+      if (!B->rhi) continue;
+      int myth1 = B->t0 + 1, myth2 = B->t0 + B->nt, mynth = B->nt;
+      int myphi1 = B->p0 + 1, myphi2 = B->p0 + B->np, mynphi = B->np;
+      for (int is = 0; is < nsq; is++) {
+        const double *q = sq + 6 * is;
+        int lct = (int)floor((q[0] - p->th1) / c->dth) + 1, lcp = (int)floor((q[1] - p->phi1) / c->dphi) + 1;
+        lct = lct > nth ? nth : (lct < 1 ? 1 : lct);
+        lcp = lcp > nphi ? nphi : (lcp < 1 ? 1 : lcp);
+        if (!(lct + mynth >= myth1 && lct - mynth <= myth2)) continue;
+        double w2 = (p->r2 / q[2]) * (p->r2 / q[2]);
+        double shift[3];
+        int ns = 0;
+        if (lcp + mynphi >= myphi1 && lcp - mynphi <= myphi2) shift[ns++] = 0.0;
+        if (lcp + mynphi > nphi && myphi1 == 1) shift[ns++] = 1.0;
+        if (lcp - mynphi < 1 && myphi2 == nphi) shift[ns++] = -1.0;
+        for (int a = 0; a < ns; a++)
+          for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+            for (int it = B->t0; it < B->t0 + B->nt; it++) {
+              double dt_ = c->theta[it] - q[0], thtmp = dt_ * dt_;
+              double dp = c->phi[ip] - q[1];
+              if (shift[a] > 0.0) dp = dp + p->phi2 - p->phi1;
+              else if (shift[a] < 0.0) dp = dp - p->phi2 + p->phi1;
+              double e = -(thtmp + dp * dp) * w2;
+              if (!(e > -11.5)) continue;
+              size_t id = it + (size_t)nth * ip;
+              double val = q[3] * exp(e);
+              if (pass == 0) {
+                dens[id] = dens[id] + val;
+              } else {
+                val = val * dens[id];
+                c->dvel_rain[id] = c->dvel_rain[id] + q[4] * val;
+                c->dent_rain[id] = c->dent_rain[id] + q[5] * val;
+              }
+            }
+      }
+    }
+    if (pass == 0)
+      for (size_t i = 0; i < np; i++) dens[i] = 1.0 / (dens[i] + 1.0);
+  }
+  free(dens);
+  return CSS_OK;
 }
 
 /* Step_RK2_TVD / Step_RK3_TVD (step_rk4.f90:31-335): the SLD tendency of
@@ -2426,11 +2827,18 @@ int orc_step_rk4(orc_ctx *c, double *vars0, double dt, int nsteps) {
   double *av = NULL;
   if (p->magnetic) av = (double *)malloc(sizeof(double) * 3 * c->ncell);
   if (p->time_stepper == 2 || p->time_stepper == 3) {
-    for (int step = 0; step < nsteps; step++) step_tvd(c, vars0, dt, p->time_stepper, av);
+    for (int step = 0; step < nsteps; step++) {
+      int rc = step_begin(c, dt);
+      if (rc) { free(av); return rc; }
+      step_tvd(c, vars0, dt, p->time_stepper, av);
+      step_end(c, vars0, dt);
+    }
     free(av);
     return CSS_OK;
   }
   for (int step = 0; step < nsteps; step++) {
+    int rc = step_begin(c, dt);
+    if (rc) { free(av); return rc; }
     double dtcur = dt / 2.0;
     memcpy(v1, vars0, sizeof(double) * N);
     orc_rhs(c, v1, dv, 1);
@@ -2466,6 +2874,7 @@ int orc_step_rk4(orc_ctx *c, double *vars0, double dt, int nsteps) {
     for (size_t i = 0; i < N; i++) { vs[i] = vs[i] + dv[i] / 6.0; v1[i] = vars0[i] + dtcur * vs[i]; }
     bound(c, v1);
     memcpy(vars0, v1, sizeof(double) * N);
+    step_end(c, vars0, dt);
   }
   free(av);
   return CSS_OK;

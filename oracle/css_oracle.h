@@ -61,6 +61,15 @@ int orc_scalars(orc_ctx *c, const double *vars0, double *out);
 int orc_step_size(orc_ctx *c, const double *vars0, double cfl_safety, double *out);
 int orc_shell_averages(orc_ctx *c, const double *vars0, const int *q, int nq, const double *k0, double *out);
 int orc_spectrum(orc_ctx *c, const double *vars0, int kind, double *out);
+/* open radial boundaries: clock, mass bookkeeping, rain and ASH inputs */
+int orc_set_clock(orc_ctx *c, long long istep, double sim_time, double deltat);
+int orc_get_clock(orc_ctx *c, long long *istep, double *sim_time);
+int orc_inout_init(orc_ctx *c, const double *vars0);
+int orc_inout_state(orc_ctx *c, double *out);
+int orc_set_rain_fields(orc_ctx *c, const double *dvel, const double *dent);
+int orc_rain_fields(orc_ctx *c, double *dvel, double *dent);
+int orc_set_ash_slices(orc_ctx *c, const double *slices, const double *times, double ash_fen_mod);
+int orc_build_gaussian_squalls(orc_ctx *c, int nsq, const double *sq);
 
 #ifdef __cplusplus
 }

@@ -46,6 +46,14 @@ def lib():
         L.orc_step_size.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, _dp]
         L.orc_shell_averages.argtypes = [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp]
         L.orc_spectrum.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        L.orc_set_clock.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_double]
+        L.orc_get_clock.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), _dp]
+        L.orc_inout_init.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_inout_state.argtypes = [ctypes.c_void_p, _dp]
+        L.orc_set_rain_fields.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_rain_fields.argtypes = [ctypes.c_void_p, _dp, _dp]
+        L.orc_set_ash_slices.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double]
+        L.orc_build_gaussian_squalls.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
         _LIB = L
     return _LIB
 
@@ -163,6 +171,41 @@ class Oracle:
         v = np.array(vars0, dtype=np.float64, order="C", copy=True)
         _check(lib().orc_step_rk4(self.h, _ptr(v), float(dt), int(nsteps)))
         return v
+
+    # open radial boundaries (same semantics as the css_* entry points)
+    def set_clock(self, istep, sim_time, deltat):
+        _check(lib().orc_set_clock(self.h, int(istep), float(sim_time), float(deltat)))
+
+    def clock(self):
+        i, t = ctypes.c_longlong(), ctypes.c_double()
+        _check(lib().orc_get_clock(self.h, ctypes.byref(i), ctypes.byref(t)))
+        return i.value, t.value
+
+    def inout_init(self, vars0):
+        _check(lib().orc_inout_init(self.h, _ptr(np.ascontiguousarray(vars0, dtype=np.float64))))
+
+    def inout_state(self):
+        out = np.zeros(4)
+        _check(lib().orc_inout_state(self.h, _ptr(out)))
+        return dict(zip(("m0", "vol", "mtot", "ash_fen_mod"), out.tolist()))
+
+    def set_rain_fields(self, dvel, dent):
+        _check(lib().orc_set_rain_fields(self.h, _ptr(np.ascontiguousarray(dvel, dtype=np.float64)),
+                                         _ptr(np.ascontiguousarray(dent, dtype=np.float64))))
+
+    def rain_fields(self):
+        dvel = np.zeros((self.p.nphi, self.p.nth))
+        dent = np.zeros_like(dvel)
+        _check(lib().orc_rain_fields(self.h, _ptr(dvel), _ptr(dent)))
+        return dvel, dent
+
+    def set_ash_slices(self, slices, times, ash_fen_mod):
+        _check(lib().orc_set_ash_slices(self.h, _ptr(np.ascontiguousarray(slices, dtype=np.float64)),
+                                        _ptr(np.ascontiguousarray(times, dtype=np.float64)), float(ash_fen_mod)))
+
+    def build_gaussian_squalls(self, squalls):
+        sq = np.ascontiguousarray(squalls, dtype=np.float64).reshape(-1, 6)
+        _check(lib().orc_build_gaussian_squalls(self.h, sq.shape[0], _ptr(sq)))
 
 
 def compact_lines(x, order=1, lphys=True, rphys=True, bdry=1, bc_lo=None, bc_hi=None,
