@@ -719,7 +719,8 @@ __device__ __forceinline__ void inout_face(const CssGeo &g, int j, int m, bool t
     const size_t np = (size_t)g.nth * g.nphi;
     const double tc = io[IO_BOT_TCONST];
     drho = drho + io[IO_BOT_MEANU];
-    dw = dw + tau * (tc * g.ashv[np + q] - hl[0]);
+    // the u_theta term is added in k_rhot_update, after Density_Terms_Theta
+    // has read the accumulated dw for its wall datum (rhs_mpi.f90:705, :724)
     dvv = dvv + tau * (tc * g.ashv[2 * np + q] - hl[HS]);
     du = du + tau * (tc * g.ashv[q] - u0);
     ds = ds + tau * ((g.sr[0] + io[IO_BOT_FEN] * g.ashv[3 * np + q]) - s0);
@@ -1041,7 +1042,9 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
       double w1 = ri * O[(size_t)l * SO + j];
       double d0 = d0k[k] - wk[k] * w1;
       w1 = w1 * (1.0 / rho);
-      const double d1 = d1k[k] - g.pconst * w1 * tk[k];
+      double d1 = d1k[k] - g.pconst * w1 * tk[k];
+      if (ir == 0 && g.bottom_specified)  // prescribed bottom, u_theta (rhs_mpi.f90:1932)
+        d1 = d1 + g.inout[IO_BOT_TAU] * (g.inout[IO_BOT_TCONST] * g.ashv[(size_t)g.nth * g.nphi + idk[k]] - wk[k]);
       if (g.xi_cs < 1.0) d0 = (g.xi_cs * g.xi_cs) * d0;
       d0k[k] = d0;
       d1k[k] = d1;
