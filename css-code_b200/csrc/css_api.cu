@@ -1110,6 +1110,18 @@ extern "C" int css_download_state(css_ctx *c, double *vars) {
   return CSS_OK;
 }
 
+extern "C" int css_download_plane(css_ctx *c, int iv, int ir, double *plane) {
+  if (!c || !plane || iv < 0 || iv >= c->nv || ir < 0 || ir >= c->p.nr) {
+    set_err("css_download_plane: bad argument");
+    return CSS_ERR_ARG;
+  }
+  const size_t np = (size_t)c->p.nth * c->p.nphi;
+  CUDA_TRY(cudaMemcpyAsync(plane, c->v0 + (size_t)iv * c->ncell + (size_t)ir * np, np * 8, cudaMemcpyDeviceToHost,
+                           c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
 extern "C" int css_step_rk4(css_ctx *c, double dt, int nsteps) {
   if (!c || nsteps < 0 || !(dt > 0.0)) { set_err("css_step_rk4: bad argument"); return CSS_ERR_ARG; }
   CUDA_TRY(cudaMemsetAsync(c->flag, 0, sizeof(int), c->stream));

@@ -89,6 +89,7 @@ def lib():
         L.css_mlp_grads.argtypes = [vp, ctypes.c_int, fp, fp]
         L.css_mlp_set_stream.argtypes = [vp, vp]
         L.css_mlp_set_fused.argtypes = [vp, ctypes.c_int]
+        L.css_download_plane.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
         L.css_set_clock.argtypes = [vp, ll, ctypes.c_double, ctypes.c_double]
         L.css_get_clock.argtypes = [vp, ctypes.POINTER(ll), dp]
         L.css_inout_init.argtypes = [vp]
@@ -119,5 +120,5 @@ EXPORTS = [
     "css_mlp_destroy", "css_mlp_dims", "css_mlp_forward", "css_mlp_train_step", "css_mlp_params", "css_mlp_grads",
     "css_mlp_set_stream", "css_mlp_set_fused", "css_set_clock", "css_get_clock", "css_inout_init",
     "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_gaussian_squalls",
-    "css_set_ash_slices",
+    "css_set_ash_slices", "css_download_plane",
 ]

@@ -171,6 +171,12 @@ class Simulation:
         check(_lib.lib().css_diffusion(self.h, _p(v), _p(a), _p(dv)))
         return v, dv
 
+    def plane(self, iv, ir):
+        """Field iv of the resident state at radius ir, shape (nphi, nth)."""
+        out = np.zeros((self.p.nphi, self.p.nth))
+        check(_lib.lib().css_download_plane(self.h, int(iv), int(ir), _p(out)))
+        return out
+
     # open radial boundaries (top_inout / bot_inout) ---------------------------
     def set_clock(self, istep, sim_time, deltat):
         """istep: the step index the RHS sees; deltat: the step size of the

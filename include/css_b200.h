@@ -140,6 +140,11 @@ void css_destroy(css_ctx *ctx);
 int css_upload_state(css_ctx *ctx, const double *vars);
 int css_download_state(css_ctx *ctx, double *vars);
 
+/* One plane of the resident state: field iv at radius ir, nth*nphi values
+ * [it + nth*ip] into the host buffer `plane` (a face of vars0, as the rain
+ * model reads the surface velocities, entropy_rain.f90:338-343).           */
+int css_download_plane(css_ctx *ctx, int iv, int ir, double *plane);
+
 /* nsteps RK4 steps of size dt on the device-resident state.  Replaces the
  * loop body of Program CSS2 (mhdsph_mpi.f90:28-48) calling Step_RK4
  * (step_rk4.f90:339-493).  Returns CSS_ERR_NAN if the state became
