@@ -2428,15 +2428,18 @@ extern "C" int css_get_rain_fields(css_ctx *c, double *dvel_rain, double *dent_r
 
 // squalls: 6 per squall (theta_loc, phi_loc, size, scaling, vel, dels); the
 // grid point of each centre follows Find_Position (entropy_rain.f90:817-824)
-extern "C" int css_build_gaussian_squalls(css_ctx *c, int nsq, const double *squalls) {
-  if (int rc = need_open(c, "css_build_gaussian_squalls")) return rc;
-  if (nsq < 0 || (nsq > 0 && !squalls)) { set_err("css_build_gaussian_squalls: bad argument"); return CSS_ERR_ARG; }
+extern "C" int css_build_squalls(css_ctx *c, int sstruct, int nsq, const double *squalls) {
+  if (int rc = need_open(c, "css_build_squalls")) return rc;
+  if (nsq < 0 || (nsq > 0 && !squalls) || (sstruct != 0 && sstruct != 1)) {
+    set_err("css_build_squalls: bad argument");
+    return CSS_ERR_ARG;
+  }
   const css_params &p = c->p;
   const double dth = (p.th2 - p.th1) / (double)(p.nth - 1), dphi = (p.phi2 - p.phi1) / (double)p.nphi;
   std::vector<double> sq((size_t)8 * std::max(nsq, 1));
   for (int i = 0; i < nsq; i++) {
     const double *q = squalls + 6 * i;
-    if (!(q[2] > 0.0)) { set_err("css_build_gaussian_squalls: squall %d has size %g", i, q[2]); return CSS_ERR_ARG; }
+    if (!(q[2] > 0.0)) { set_err("css_build_squalls: squall %d has size %g", i, q[2]); return CSS_ERR_ARG; }
     for (int k = 0; k < 6; k++) sq[8 * i + k] = q[k];
     const double ft = floor((q[0] - p.th1) / dth) + 1.0, fp = floor((q[1] - p.phi1) / dphi) + 1.0;
     sq[8 * i + 6] = std::max(std::min(ft, (double)p.nth), 1.0);
@@ -2451,8 +2454,8 @@ extern "C" int css_build_gaussian_squalls(css_ctx *c, int nsq, const double *squ
   }
   if (nsq > 0) CUDA_TRY(cudaMemcpyAsync(c->squalls, sq.data(), (size_t)8 * nsq * 8, cudaMemcpyHostToDevice, c->stream));
   const size_t np = (size_t)p.nth * p.nphi;
-  k_squalls<<<(unsigned)((np + 255) / 256), 256, 0, c->stream>>>(c->g, c->squalls, nsq, p.phi1, p.phi2, c->rain,
-                                                                    c->rain + np);
+  k_squalls<<<(unsigned)((np + 255) / 256), 256, 0, c->stream>>>(c->g, c->squalls, nsq, sstruct == 0, p.phi1, p.phi2,
+                                                                    c->rain, c->rain + np);
   if (int rc = check_launch(c)) return rc;
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return CSS_OK;

@@ -213,13 +213,14 @@ __global__ void __launch_bounds__(IO_NT) k_ash_flux(CssGeo g, const double *__re
   }
 }
 
-// Build_Gaussian_Squalls (entropy_rain.f90:423-523), one thread per top-plane
-// cell.  sq: 8 per squall (theta_loc, phi_loc, size, scaling, vel, dels,
+// Build_Gaussian_Squalls (entropy_rain.f90:423-523) or, with poly,
+// Build_Polynomial_Squalls (:525-655, the density summing |term|), one
+// thread per top-plane cell.  sq: 8 per squall (theta_loc, phi_loc, size, scaling, vel, dels,
 // loct, locp; loct/locp 1-based as Find_Position makes them).  A cell's
 // block sees a squall whose centre lies within one block width of it, with
 // the periodic images on the first and last phi blocks; terms below 1e-5
-// are dropped.
-__global__ void k_squalls(CssGeo g, const double *__restrict__ sq, int nsq, double phi1, double phi2,
+// are dropped (polynomials: beyond the squall's size).
+__global__ void k_squalls(CssGeo g, const double *__restrict__ sq, int nsq, int poly, double phi1, double phi2,
                           double *__restrict__ dvel, double *__restrict__ dent) {
   const size_t np = (size_t)g.nth * g.nphi;
   for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < np; id += (size_t)gridDim.x * blockDim.x) {
@@ -250,13 +251,22 @@ __global__ void k_squalls(CssGeo g, const double *__restrict__ sq, int nsq, doub
             if (!(lcp - mynphi < 1 && myphi2 == g.nphi)) continue;
             dp = dp - phi2 + phi1;
           }
-          const double e = -(thtmp + dp * dp) * w2;
-          if (!(e > -11.5)) continue;
-          double val = q[3] * exp(e);
+          double val;
+          if (poly) {  // Build_Polynomial_Squalls (entropy_rain.f90:525-655)
+            const double e = (thtmp + dp * dp) * w2;
+            if (!(e <= 1.0)) continue;
+            const double tt = sqrt(e), x1 = tt * tt, x2 = x1 * tt, x3 = x2 * tt;
+            const double f = 1.0 - 18.0 * x1 + 32.0 * x2 - 15.0 * x3;
+            val = pass == 0 ? fabs(q[3] * f) : q[3] * dens * f;
+          } else {
+            const double e = -(thtmp + dp * dp) * w2;
+            if (!(e > -11.5)) continue;
+            val = q[3] * exp(e);
+            if (pass) val = val * dens;
+          }
           if (pass == 0) {
             acc[0] += val;
           } else {
-            val = val * dens;
             acc[1] += q[4] * val;
             acc[2] += q[5] * val;
           }

@@ -96,7 +96,7 @@ def lib():
         L.css_inout_state.argtypes = [vp, dp]
         L.css_set_rain_fields.argtypes = [vp, dp, dp]
         L.css_get_rain_fields.argtypes = [vp, dp, dp]
-        L.css_build_gaussian_squalls.argtypes = [vp, ctypes.c_int, dp]
+        L.css_build_squalls.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
         L.css_set_ash_slices.argtypes = [vp, dp, dp, ctypes.c_double]
         _LIB = L
     return _LIB
@@ -119,6 +119,6 @@ EXPORTS = [
     "css_closure_scales", "css_closure_features", "css_closure_targets", "css_closure_speed2", "css_mlp_create",
     "css_mlp_destroy", "css_mlp_dims", "css_mlp_forward", "css_mlp_train_step", "css_mlp_params", "css_mlp_grads",
     "css_mlp_set_stream", "css_mlp_set_fused", "css_set_clock", "css_get_clock", "css_inout_init",
-    "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_gaussian_squalls",
+    "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_squalls",
     "css_set_ash_slices", "css_download_plane",
 ]

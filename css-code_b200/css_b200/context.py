@@ -207,10 +207,11 @@ class Simulation:
         check(_lib.lib().css_get_rain_fields(self.h, _p(dvel), _p(dent)))
         return dvel, dent
 
-    def build_gaussian_squalls(self, squalls):
-        """squalls: (nsq, 6) theta_loc, phi_loc, size, scaling, vel, dels."""
+    def build_squalls(self, squalls, sstruct=1):
+        """squalls: (nsq, 6) theta_loc, phi_loc, size, scaling, vel, dels;
+        sstruct 1 Gaussian, 0 polynomial squalls."""
         sq = np.ascontiguousarray(squalls, dtype=np.float64).reshape(-1, 6)
-        check(_lib.lib().css_build_gaussian_squalls(self.h, sq.shape[0], _p(sq)))
+        check(_lib.lib().css_build_squalls(self.h, int(sstruct), sq.shape[0], _p(sq)))
 
     def set_ash_slices(self, slices, times, ash_fen_mod):
         """slices: (4 times, 4 fields u_r, u_theta, u_phi, s, nphi, nth)."""

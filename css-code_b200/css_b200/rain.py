@@ -1,12 +1,13 @@
 """Entropy rain: the rain-squall model of entropy_rain.f90 on the host,
-feeding the device's squall builder (css_build_gaussian_squalls) and the
+feeding the device's squall builder (css_build_squalls) and the
 top inflow/outflow relaxation that reads its fields.
 
 As in the reference the squall bookkeeping is host work between steps
 (Update_Rain_Squalls runs after every ufreq/10-th step on the top ranks,
 step_rk4.f90:484-486); only the fields are built on the device.  Restated:
 Initialize_Rain_Squalls for squalls (entropy_rain.f90:113-153; the Voronoi
-downflow lanes are not built), Update_Rain_Squalls (:316-419),
+downflow lanes are not built), both squall shapes (sstruct 1 Gaussian,
+0 polynomial, built on the device), Update_Rain_Squalls (:316-419),
 Temporal_Structure (:851-880), Find_Position (:817-824),
 Generate_New_Squall_Parameters (:737-814), Place_Cell (:930-945) and
 Random_Exponential (:947-962).
@@ -30,12 +31,13 @@ DELS, SIZE, DUR, THETA, PHI, VEL, DELR = range(7)
 class RainSqualls:
     """The squall population of one run.
 
-    nsqualls, meandur, meansize, rainstats, tstruct, rhotopin, stopin,
-    utopin are the reference's namelist values (mhdsph_mpi.f90:1157-1159);
+    nsqualls, meandur, meansize, rainstats, tstruct, sstruct, rhotopin,
+    stopin, utopin are the reference's namelist values (mhdsph_mpi.f90:
+    1157-1159);
     p and profiles are the run's parameters and radial profiles."""
 
     def __init__(self, p, profiles, nsqualls, meandur, meansize, rhotopin, stopin, utopin, rainstats=1,
-                 tstruct=0, seed=0, sim_time=0.0):
+                 tstruct=0, sstruct=1, seed=0, sim_time=0.0):
         pr = np.asarray(profiles, dtype=np.float64).reshape(len(PROF_NAMES), p.nr)
         self.p = p
         self.rng = np.random.default_rng(seed)
@@ -43,7 +45,7 @@ class RainSqualls:
         self.dth = (p.th2 - p.th1) / (p.nth - 1)
         self.dphi = (p.phi2 - p.phi1) / p.nphi
         self.meandur, self.meansize = float(meandur), float(meansize)
-        self.rainstats, self.tstruct = int(rainstats), int(tstruct)
+        self.rainstats, self.tstruct, self.sstruct = int(rainstats), int(tstruct), int(sstruct)
         # Initialize_Rain_Squalls (:55-58)
         self.meandrho = rhotopin * pr[PROF_NAMES.index("rhor")][-1]
         self.meands = float(stopin)
@@ -125,7 +127,7 @@ class RainSqualls:
         """Update_Rain_Squalls for squalls: age, advect by the surface flow
         (w_top, v_top: the top plane of vars0, shape (nphi, nth)), then the
         squall list the fields are built from (returned; the caller hands it
-        to build_gaussian_squalls), then replace the dead squalls."""
+        to build_squalls with self.sstruct), then replace the dead squalls."""
         p = self.p
         n = len(self.start)
         iup = np.zeros(n, dtype=bool)
@@ -172,4 +174,4 @@ def advance(sim, rain, dt, nsteps, ufreq):
         istep, t_end = sim.clock()
         if istep % every == 0:
             built = rain.update(t_end - dt, dt, sim.plane(1, nr - 1), sim.plane(2, nr - 1))
-            sim.build_gaussian_squalls(built)
+            sim.build_squalls(built, rain.sstruct)

@@ -439,13 +439,15 @@ int css_inout_state(css_ctx *ctx, double *out);
 
 /* Entropy rain (do_entropy_rain): the squall fields dvel_rain, dent_rain
  * (entropy_rain.f90:40; nth*nphi each, [it + nth*ip]) the top relaxation
- * reads, set directly or built from squalls by Build_Gaussian_Squalls
- * (entropy_rain.f90:423-523): squalls[6*k ..] = theta_loc, phi_loc, size,
- * scaling, vel, dels.  The squall life cycle (Update_Rain_Squalls, :171-421)
- * is the caller's, between steps, as in the reference.  Host pointers.     */
+ * reads, set directly or built from squalls: sstruct 1 Gaussian squalls
+ * (Build_Gaussian_Squalls, entropy_rain.f90:423-523), 0 polynomial ones
+ * (Build_Polynomial_Squalls, :525-655); squalls[6*k ..] = theta_loc,
+ * phi_loc, size, scaling, vel, dels.  The squall life cycle
+ * (Update_Rain_Squalls, :171-421) is the caller's, between steps, as in the
+ * reference.  Host pointers.                                              */
 int css_set_rain_fields(css_ctx *ctx, const double *dvel_rain, const double *dent_rain);
 int css_get_rain_fields(css_ctx *ctx, double *dvel_rain, double *dent_rain);
-int css_build_gaussian_squalls(css_ctx *ctx, int nsq, const double *squalls);
+int css_build_squalls(css_ctx *ctx, int sstruct, int nsq, const double *squalls);
 
 /* Prescribed bottom (bottom_specified): the four time slices of the ASH
  * fields after the reader's spatial interpolation and wall taper

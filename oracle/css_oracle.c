@@ -2713,16 +2713,19 @@ int orc_set_ash_slices(orc_ctx *c, const double *slices, const double *times, do
   return CSS_OK;
 }
 
-/* Build_Gaussian_Squalls (entropy_rain.f90:423-523) on the top plane: each
+/* Build_Gaussian_Squalls (entropy_rain.f90:423-523; sstruct 1) or
+ * Build_Polynomial_Squalls (:525-655; sstruct 0) on the top plane: each
  * top block evaluates the squalls whose centre (loct, locp of Find_Position,
  * :817-824) lies within one block width of it, with the periodic images
  * across phi1/phi2 on the first and last phi blocks; Gaussians below 1e-5
- * (exponent -11.5) are dropped.  The squall density 1/(1 + sum) then
+ * (exponent -11.5) are dropped, polynomials beyond the squall's size.  The
+ * squall density 1/(1 + sum) (of |term| for the polynomial) then
  * weights each squall's velocity and entropy.  sq: 6 per squall, theta_loc,
  * phi_loc, size, scaling, vel, dels. */
-int orc_build_gaussian_squalls(orc_ctx *c, int nsq, const double *sq) {
+int orc_build_squalls(orc_ctx *c, int sstruct, int nsq, const double *sq) {
   const css_params *p = &c->p;
-  if (!c->dvel_rain) { set_err("orc_build_gaussian_squalls: the run has no open boundary"); return CSS_ERR_ARG; }
+  if (!c->dvel_rain) { set_err("orc_build_squalls: the run has no open boundary"); return CSS_ERR_ARG; }
+  const int poly = sstruct == 0;
   int nth = c->nth, nphi = c->nphi;
   size_t np = (size_t)nth * nphi;
   double *dens = dalloc(np);
@@ -2753,14 +2756,23 @@ int orc_build_gaussian_squalls(orc_ctx *c, int nsq, const double *sq) {
               double dp = c->phi[ip] - q[1];
               if (shift[a] > 0.0) dp = dp + p->phi2 - p->phi1;
               else if (shift[a] < 0.0) dp = dp - p->phi2 + p->phi1;
-              double e = -(thtmp + dp * dp) * w2;
-              if (!(e > -11.5)) continue;
               size_t id = it + (size_t)nth * ip;
-              double val = q[3] * exp(e);
+              double val;
+              if (poly) { /* Build_Polynomial_Squalls (:525-655) */
+                double e = (thtmp + dp * dp) * w2;
+                if (!(e <= 1.0)) continue;
+                double tt = sqrt(e), x1 = tt * tt, x2 = x1 * tt, x3 = x2 * tt;
+                double f = 1.0 - 18.0 * x1 + 32.0 * x2 - 15.0 * x3;
+                val = pass == 0 ? fabs(q[3] * f) : q[3] * dens[id] * f;
+              } else {
+                double e = -(thtmp + dp * dp) * w2;
+                if (!(e > -11.5)) continue;
+                val = q[3] * exp(e);
+                if (pass) val = val * dens[id];
+              }
               if (pass == 0) {
                 dens[id] = dens[id] + val;
               } else {
-                val = val * dens[id];
                 c->dvel_rain[id] = c->dvel_rain[id] + q[4] * val;
                 c->dent_rain[id] = c->dent_rain[id] + q[5] * val;
               }

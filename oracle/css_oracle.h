@@ -69,7 +69,7 @@ int orc_inout_state(orc_ctx *c, double *out);
 int orc_set_rain_fields(orc_ctx *c, const double *dvel, const double *dent);
 int orc_rain_fields(orc_ctx *c, double *dvel, double *dent);
 int orc_set_ash_slices(orc_ctx *c, const double *slices, const double *times, double ash_fen_mod);
-int orc_build_gaussian_squalls(orc_ctx *c, int nsq, const double *sq);
+int orc_build_squalls(orc_ctx *c, int sstruct, int nsq, const double *sq);
 
 #ifdef __cplusplus
 }

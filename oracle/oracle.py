@@ -53,7 +53,7 @@ def lib():
         L.orc_set_rain_fields.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.orc_rain_fields.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.orc_set_ash_slices.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double]
-        L.orc_build_gaussian_squalls.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp]
+        L.orc_build_squalls.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
         _LIB = L
     return _LIB
 
@@ -203,9 +203,9 @@ class Oracle:
         _check(lib().orc_set_ash_slices(self.h, _ptr(np.ascontiguousarray(slices, dtype=np.float64)),
                                         _ptr(np.ascontiguousarray(times, dtype=np.float64)), float(ash_fen_mod)))
 
-    def build_gaussian_squalls(self, squalls):
+    def build_squalls(self, squalls, sstruct=1):
         sq = np.ascontiguousarray(squalls, dtype=np.float64).reshape(-1, 6)
-        _check(lib().orc_build_gaussian_squalls(self.h, sq.shape[0], _ptr(sq)))
+        _check(lib().orc_build_squalls(self.h, int(sstruct), sq.shape[0], _ptr(sq)))
 
 
 def compact_lines(x, order=1, lphys=True, rphys=True, bdry=1, bc_lo=None, bc_hi=None,

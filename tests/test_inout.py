@@ -159,8 +159,9 @@ def test_oracle_ash_forcing_is_a_catmull_rom_curve():
     assert np.array_equal(db[:, 1:], da[:, 1:]) and np.array_equal(db[0, 0], da[0, 0])
 
 
-def squalls_numpy(p, sq):
-    """Build_Gaussian_Squalls restated with numpy over the top blocks."""
+def squalls_numpy(p, sq, sstruct=1):
+    """Build_Gaussian_Squalls / Build_Polynomial_Squalls restated with numpy
+    over the top blocks."""
     th, ph, dth, dphi = problem.angles(p)
     nth, nphi = p.nth, p.nphi
     tb = np.array_split(np.arange(nth), p.nnt)
@@ -186,11 +187,15 @@ def squalls_numpy(p, sq):
                 if lcp - mynp < 1 and myp2 == nphi:
                     shifts.append(-(p.phi2 - p.phi1))
                 for sh in shifts:
-                    e = -((T - t0) ** 2 + (P - p0 + sh) ** 2) * (p.r2 / size) ** 2
-                    val = np.where(e > -11.5, scal * np.exp(e), 0.0)
+                    x2 = ((T - t0) ** 2 + (P - p0 + sh) ** 2) * (p.r2 / size) ** 2
+                    if sstruct == 1:
+                        val = np.where(-x2 > -11.5, scal * np.exp(-x2), 0.0)
+                    else:
+                        x = np.sqrt(np.minimum(x2, 1.0))
+                        val = np.where(x2 <= 1.0, scal * (1 - 18 * x ** 2 + 32 * x ** 3 - 15 * x ** 4), 0.0)
                     terms.append((np.ix_(p_idx, t_idx), val, vel, dels))
     for ix, val, vel, dels in terms:
-        dens[ix] += val
+        dens[ix] += np.abs(val)
     dens = 1.0 / (dens + 1.0)
     for ix, val, vel, dels in terms:
         dvel[ix] += vel * val * dens[ix]
@@ -211,16 +216,30 @@ def squall_list(p, n=12, seed=21):
     return sq
 
 
-def test_oracle_squalls_match_numpy():
+@pytest.mark.parametrize("sstruct", [1, 0])
+def test_oracle_squalls_match_numpy(sstruct):
     p, prof, v0, dt = build(top_inout=1, do_entropy_rain=1)
     o = O.Oracle(p, prof)
     sq = squall_list(p)
-    o.build_gaussian_squalls(sq)
+    o.build_squalls(sq, sstruct)
     dvel, dent = o.rain_fields()
-    wv, we = squalls_numpy(p, sq)
+    wv, we = squalls_numpy(p, sq, sstruct)
     assert np.abs(dvel - wv).max() <= 1e-14 * np.abs(wv).max()
     assert np.abs(dent - we).max() <= 1e-14 * np.abs(we).max()
     assert np.abs(wv).max() > 0 and np.abs(wv[:, :]).min() == 0.0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sstruct", [1, 0])
+def test_squall_builder_parity(sstruct, gpu_available):
+    from css_b200.context import Simulation
+    p, prof, v0, dt = build(top_inout=1, do_entropy_rain=1)
+    sim, orc = Simulation(p, prof), O.Oracle(p, prof)
+    sq = squall_list(p, n=40, seed=sstruct + 3)
+    sim.build_squalls(sq, sstruct)
+    orc.build_squalls(sq, sstruct)
+    for a, b in zip(sim.rain_fields(), orc.rain_fields()):
+        assert np.abs(a - b).max() <= 1e-13 * np.abs(b).max()
 
 
 def test_oracle_clock_and_mass_total():
@@ -276,7 +295,7 @@ def setup_pair(name):
     for o in (sim, orc):
         o.set_clock(1, t0, dt)
         if p.do_entropy_rain:
-            o.build_gaussian_squalls(squall_list(p))
+            o.build_squalls(squall_list(p))
         if p.bottom_specified:
             slices, times = ash_case(p)
             o.set_ash_slices(slices, times, 1.3)

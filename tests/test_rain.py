@@ -101,8 +101,8 @@ def test_rain_run_parity(gpu_available):
         if step % every == 0:
             _, t_end = orc.clock()
             built = r.update(t_end - dt, dt, o_state[1, -1], o_state[2, -1])
-            sim.build_gaussian_squalls(built)
-            orc.build_gaussian_squalls(built)
+            sim.build_squalls(built)
+            orc.build_squalls(built)
             for a, b in zip(sim.rain_fields(), orc.rain_fields()):
                 assert np.abs(a - b).max() <= 1e-13 * max(np.abs(b).max(), 1e-300)
     assert np.abs(orc.rain_fields()[0]).max() > 0.0
