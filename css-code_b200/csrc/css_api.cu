@@ -262,8 +262,10 @@ static int setup_mt() {
   CSS_SMEM_ATTR(k_theta_terms<MT, TLC, float>);
   CSS_SMEM_ATTR(k_phi_terms<MT, TLC, double>);
   CSS_SMEM_ATTR(k_phi_terms<MT, TLC, float>);
-  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, double>);
-  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, float>);
+  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, double, 0>);
+  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, float, 0>);
+  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, double, 1>);
+  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, float, 1>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, float>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, float>);
@@ -949,9 +951,14 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
       if (int rc = launch_inout(c, (const double *)cur)) return rc;
   }
   TL = c->tl_r;
-  dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
+  const dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_RADIAL);
-  LAUNCH_MT(0, TL, k_radial_terms, (TS), gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  if (c->io)
+    LAUNCH_MT(0, TL, k_radial_terms, (TS, 1), gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+              TL);
+  else
+    LAUNCH_MT(0, TL, k_radial_terms, (TS, 0), gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+              TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   if constexpr (sizeof(TS) == 8) {
@@ -1390,7 +1397,7 @@ extern "C" int css_autotune(css_ctx *c, int reps, int *chosen) {
       if (cudaEventSynchronize(e1) != cudaSuccess) { set_err("css_autotune: timing failed"); rc = CSS_ERR_CUDA; break; }
       float ms = 0.f;
       cudaEventElapsedTime(&ms, e0, e1);
-      if (ms < best_ms) { best_ms = ms; best = t; best_pers = c->phi_pers; }
+      if (ms < best_ms) { best_ms = ms; best = t; best_pers = tv.second; }
     }
     *tl[d] = best;
     if (d == 2) c->phi_pers = best_pers;

@@ -740,15 +740,14 @@ __device__ __forceinline__ void inout_face(const CssGeo &g, int j, int m, bool t
 // it is solved with a zero datum together with the other derivatives and
 // the datum times the block's unit response (resp) is added afterwards.
 // ---------------------------------------------------------------------------
-template <int MT, int TLC, typename TV>
-__global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__restrict__ cur,
-                                                      const double *__restrict__ bf, double *__restrict__ dv,
-                                                      const double *__restrict__ tbuf, int TLrt) {
-  extern __shared__ double sm[];
-  const int TL = TLC ? TLC : TLrt;
-  const int nchunk = (g.nth + TL - 1) / TL;
-  const int br = blockIdx.x / nchunk, tb = (blockIdx.x - br * nchunk) * TL;
-  const int ip = blockIdx.y;
+// One tile of Radial_Terms + Density_Terms_Radial: r block br, theta lines
+// tb .. tb+TL-1, phi ip; sm is the CTA's shared buffer.  OPEN = 1 compiles
+// the open radial boundaries in (a run with top_inout or bot_inout); the
+// closed instance carries none of their code.
+template <int MT, int TLC, typename TV, int OPEN>
+__device__ __forceinline__ void radial_tile(const CssGeo &g, const TV *__restrict__ cur, const double *__restrict__ bf,
+                                            double *__restrict__ dv, const double *__restrict__ tbuf, int TL, int br,
+                                            int tb, int ip, double *sm) {
   const CssDir &D = g.d[0];
   const int r0 = D.start[br], m = MT ? MT : D.size[br];
   const int dtype = dtype_of(D, br);
@@ -785,7 +784,7 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
   // open faces (a radial block has at most one physical face): the top one
   // takes d(rho)/dr with bdry 2 and no datum, the bottom one with the datum
   // left in x-space (rhs_mpi.f90:2020-2023, :1895-1898)
-  const bool top_open = D.rphys[br] && g.top_inout, bot_open = D.lphys[br] && g.bot_inout;
+  const bool top_open = OPEN && D.rphys[br] && g.top_inout, bot_open = OPEN && D.lphys[br] && g.bot_inout;
   auto bdry_of = [&](int k) { return (k == 5 && top_open) ? 2 : g.ibcr[var[k]]; };
   for (int k = 0; k < nd; k++) stage_table(g, 0, br, k == 4 ? 2 : 1, bdry_of(k), m, Tb + k * TS);
   __syncthreads();
@@ -926,6 +925,18 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
       dv[4 * n + id] = ds;
     }
   }
+}
+
+// grid: x = r block * nchunk + theta chunk, y = phi; one tile per CTA
+template <int MT, int TLC, typename TV, int OPEN>
+__global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__restrict__ cur,
+                                                      const double *__restrict__ bf, double *__restrict__ dv,
+                                                      const double *__restrict__ tbuf, int TLrt) {
+  extern __shared__ double sm[];
+  const int TL = TLC ? TLC : TLrt;
+  const int nchunk = (g.nth + TL - 1) / TL;
+  const int br = blockIdx.x / nchunk;
+  radial_tile<MT, TLC, TV, OPEN>(g, cur, bf, dv, tbuf, TL, br, (blockIdx.x - br * nchunk) * TL, blockIdx.y, sm);
 }
 
 // ---------------------------------------------------------------------------
