@@ -285,9 +285,9 @@ static int setup_kernels() {
   static bool done = false;
   if (done) return CSS_OK;
   if (int rc = setup_mt<0, 0>()) return rc;
-  CUDA_TRY(cudaFuncSetAttribute(k_sld<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<4>)));
-  CUDA_TRY(cudaFuncSetAttribute(k_sld<5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<5>)));
-  CUDA_TRY(cudaFuncSetAttribute(k_sld<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<3>)));
+  CUDA_TRY(cudaFuncSetAttribute(k_sld<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<4>)));
+  CUDA_TRY(cudaFuncSetAttribute(k_sld<5, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<5>)));
+  CUDA_TRY(cudaFuncSetAttribute(k_sld<3, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<3>)));
   if (int rc = setup_mt<16, 16>()) return rc;
   if (int rc = setup_mt<32, 16>()) return rc;
   if (int rc = setup_mt<16, 8>()) return rc;
@@ -990,21 +990,26 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
   // the diffused fields are contiguous from varlist[0]; MHD runs them in two
   // launches (the hydro fields, then A) so each carries a register window
   // of at most five fields
-  const int off = g.varlist[0];
+  // the first diffused field is a template argument: 1 without mass
+  // diffusion (4 or 7 fields), 0 with it (5 or 8)
+  if (g.varlist[0] != ((g.nsld == 4 || g.nsld == 7) ? 1 : 0)) {
+    set_err("launch_sld: unexpected diffused-field list");
+    return CSS_ERR_ARG;
+  }
   const unsigned all = (1u << g.nv) - 1u;
   const int th = SLD_TT * SLD_TP;
   switch (g.nsld) {
-    case 4: k_sld<4><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, off, all, tb); break;
-    case 5: k_sld<5><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, off, all, tb); break;
+    case 4: k_sld<4, 1><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, all, tb); break;
+    case 5: k_sld<5, 0><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, all, tb); break;
     case 7:  // fields 1..7: rho is not diffused (its tendency is zero)
-      k_sld<4><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, 1, 0x1Fu, tb);
+      k_sld<4, 1><<<gs, th, sizeof(SldSmem<4>), c->stream>>>(g, v, av, c->vcc, dout, 0x1Fu, tb);
       if (int rc = check_launch(c)) return rc;
-      k_sld<3><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 5, 0xE0u, tb);
+      k_sld<3, 5><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 0xE0u, tb);
       break;
     default:  // fields 0..7
-      k_sld<5><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, 0, 0x1Fu, tb);
+      k_sld<5, 0><<<gs, th, sizeof(SldSmem<5>), c->stream>>>(g, v, av, c->vcc, dout, 0x1Fu, tb);
       if (int rc = check_launch(c)) return rc;
-      k_sld<3><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 5, 0xE0u, tb);
+      k_sld<3, 5><<<gs, th, sizeof(SldSmem<3>), c->stream>>>(g, v, av, c->vcc, dout, 0xE0u, tb);
       break;
   }
   prof_end(c);

@@ -1553,12 +1553,13 @@ __device__ __forceinline__ void sld_issue_plane(const CssGeo &g, const double *_
   cp_async_commit();
 }
 
-template <int NF>
+template <int NF, int OFF>
 __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const double *__restrict__ v,
                                                             const double *__restrict__ av,
                                                             const double *__restrict__ vcc,
-                                                            double *__restrict__ dout, int off, unsigned wmask,
+                                                            double *__restrict__ dout, unsigned wmask,
                                                             const double *__restrict__ tb) {
+  constexpr int off = OFF;  // first diffused field: every field index below is a constant
   extern __shared__ double sm_raw[];
   SldSmem<NF> &S = *reinterpret_cast<SldSmem<NF> *>(sm_raw);
   auto &FT = S.FT;
