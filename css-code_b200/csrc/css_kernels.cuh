@@ -1666,8 +1666,11 @@ __global__ void __launch_bounds__(SLD_TT * SLD_TP, 2) k_sld(CssGeo g, const doub
     else if (lo_t && th_lo_in) s_lo = (g.sld_coef * sqrt(0.5 * (V[tx + 1][1] + V[tx + 1][0]))) * __ldg(g.sld_th + t0);
     // face fluxes of every field: each thread takes the upper theta face and
     // the upper phi face of its cell; warp 0 also the phi faces of row 0,
-    // warp 1 the theta faces of column 0
-#pragma unroll 1
+    // warp 1 the theta faces of column 0.  Unrolled over the fields: their
+    // limiter chains are independent, and with every field index static the
+    // longer code no longer costs instruction-cache stalls (2.21 -> 2.03 ms
+    // on 128x256x512)
+#pragma unroll
     for (int f = 0; f < NF; f++) {
       const double tiny = g.tinyvar[f + off], itiny = g.inv_tinyvar[f + off];
       const double *xr = &X[f][ty + 2][tx + 1];
