@@ -130,7 +130,18 @@ def initial_state(p, prof, info, seed=1234, samp=1e-4, vamp=0.0, b_rel=1e-3):
     rand = rng.standard_normal((nr, nphi, nth))
     xv = math.pi * (theta - p.th1) / (p.th2 - p.th1)
     yv = math.pi * (r - p.r1) / (p.r2 - p.r1)
-    taper = (1.0 - np.cos(yv)[:, None, None] ** 16) * (1.0 - np.cos(xv)[None, None, :] ** 16)
+    # radial taper of the perturbation (mhdsph_mpi.f90:679-714): zero at a
+    # closed face, left free at an open one (top_inout / bot_inout)
+    top_open, bot_open = bool(getattr(p, "top_inout", 0)), bool(getattr(p, "bot_inout", 0))
+    if top_open and bot_open:
+        rtap = np.ones_like(r)
+    elif top_open:
+        rtap = 1.0 - np.cos(0.5 * yv) ** 16
+    elif bot_open:
+        rtap = 1.0 - np.sin(0.5 * yv) ** 16
+    else:
+        rtap = 1.0 - np.cos(yv) ** 16
+    taper = rtap[:, None, None] * (1.0 - np.cos(xv)[None, None, :] ** 16)
     rand = rand * taper
     v = np.zeros((nv, nr, nphi, nth))
     bv = 0.5 * (p.omega_0 * p.r2) ** 2 / (p.cp * p.t0)
@@ -212,9 +223,10 @@ WORKLOADS = {
 }
 
 
-def build(name_or_dims, seed=1234, magnetic=None, decomp=None, n_rho=None):
+def build(name_or_dims, seed=1234, magnetic=None, decomp=None, n_rho=None, top_inout=False, bot_inout=False):
     """(params, profiles, vars0, dt, info) for a named workload or a
-    (nr, nth, nphi) tuple."""
+    (nr, nth, nphi) tuple; top_inout / bot_inout open those radial faces
+    (and leave the initial perturbation untapered there)."""
     from .params import default_params
     if isinstance(name_or_dims, str):
         nr, nth, nphi, dec, mag, nrho = WORKLOADS[name_or_dims]
@@ -228,6 +240,7 @@ def build(name_or_dims, seed=1234, magnetic=None, decomp=None, n_rho=None):
     if n_rho is not None:
         nrho = n_rho
     p = default_params(nr, nth, nphi, dec, magnetic=mag)
+    p.top_inout, p.bot_inout = int(bool(top_inout)), int(bool(bot_inout))
     if mag:
         p.sld_prm = 0.5  # magnetic Prandtl number 2 through the SLD scaling
     prof, info = polytrope(p, nrho, ra=1e6 if mag else 1e5)

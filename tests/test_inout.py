@@ -258,6 +258,19 @@ def test_oracle_clock_and_mass_total():
     assert o.inout_state()["mtot"] == o2.inout_state()["mtot"]
 
 
+def test_initial_perturbation_taper_follows_the_open_faces():
+    """mhdsph_mpi.f90:679-714: the entropy perturbation vanishes on a closed
+    radial face and is left free on an open one."""
+    for top, bot in ((False, False), (True, False), (False, True), (True, True)):
+        p, prof, v0, dt, _ = problem.build((32, 32, 64), decomp=(2, 2, 4), top_inout=top, bot_inout=bot)
+        sr = prof.reshape(-1, p.nr)[6]
+        pert = np.abs(v0[4] / sr[:, None, None] - 1.0)
+        mid = slice(8, 24)
+        assert (pert[-1][:, mid].max() > 1e-7) == top, (top, bot)
+        assert (pert[0][:, mid].max() > 1e-7) == bot, (top, bot)
+        assert p.top_inout == int(top) and p.bot_inout == int(bot)
+
+
 def test_oracle_rejections():
     p, prof, v0, dt = build(bot_inout=1)
     for flags in (dict(magnetic=1), dict(laplacian=1), dict(do_radheat=1), dict(precision=1),
