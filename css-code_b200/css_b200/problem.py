@@ -248,3 +248,20 @@ def build(name_or_dims, seed=1234, magnetic=None, decomp=None, n_rho=None, top_i
     bfield = curl_estimate(p, prof, vars0[5:8]) if mag else None
     dt = cfl_dt(p, prof, vars0, bfield)
     return p, prof, vars0, dt, info
+
+
+def open_from_checkpoint(vars0, bottom=False, top=False, vamp=1.0):
+    """startbio / starttio (mhdsph_mpi.f90:956-976): open radial faces of a
+    state read from a closed-boundary checkpoint.  On an opened bottom u_r
+    becomes vamp times the plane above it, on an opened top vamp times the
+    plane below, each less its plane mean; an opened top also takes the
+    entropy of the plane below.  Returns a new array (nv, nr, nphi, nth)."""
+    v = np.array(vars0, dtype=np.float64, copy=True)
+    if bottom:
+        v[3, 0] = vamp * v[3, 1]
+        v[3, 0] = v[3, 0] - v[3, 0].sum() / v[3, 0].size
+    if top:
+        v[3, -1] = v[3, -2] * vamp
+        v[3, -1] = v[3, -1] - v[3, -1].sum() / v[3, -1].size
+        v[4, -1] = v[4, -2]
+    return v

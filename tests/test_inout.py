@@ -271,6 +271,21 @@ def test_initial_perturbation_taper_follows_the_open_faces():
         assert p.top_inout == int(top) and p.bot_inout == int(bot)
 
 
+def test_open_from_checkpoint():
+    """startbio / starttio: the opened face's u_r copies the neighbouring
+    plane scaled by vamp with zero plane mean; an opened top also copies s."""
+    p, prof, v0, dt, _ = problem.build((32, 32, 64), decomp=(2, 2, 4))
+    v = stirred(v0, 11)
+    o = problem.open_from_checkpoint(v, bottom=True, top=True, vamp=0.5)
+    for face, inner in ((0, 1), (-1, -2)):
+        want = 0.5 * v[3, inner] - (0.5 * v[3, inner]).mean()
+        assert np.allclose(o[3, face], want, rtol=0, atol=1e-15)
+        assert abs(o[3, face].mean()) < 1e-15
+    assert np.array_equal(o[4, -1], v[4, -2]) and np.array_equal(o[4, 0], v[4, 0])
+    assert np.array_equal(o[:, 1:-1], v[:, 1:-1]) and np.array_equal(o[:3], v[:3])
+    assert np.array_equal(problem.open_from_checkpoint(v), v)
+
+
 def test_oracle_rejections():
     p, prof, v0, dt = build(bot_inout=1)
     for flags in (dict(magnetic=1), dict(laplacian=1), dict(do_radheat=1), dict(precision=1),
