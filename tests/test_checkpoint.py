@@ -68,3 +68,28 @@ def test_library_checkpoints_equal_the_host_layout(gpu_available, tmp_path, magn
     sim.step_rk4(dt, 1)
     other.step_rk4(dt, 1)
     assert np.array_equal(sim.download(), other.download())
+
+
+def test_rain_and_ash_header_variants_and_squall_records(tmp_path):
+    """checkpoint.f90:172-181, :290-309: the header's first line carries
+    nsqualls (entropy rain) and iashtime (prescribed bottom); the squalls
+    go to checkpoint.rain_squalls as 12 REAL*8 per record and read back."""
+    from css_b200 import checkpoint as C, problem, rain
+    p, prof, v0, dt, _ = problem.build((24, 32, 64), decomp=(2, 2, 4))
+    r = rain.RainSqualls(p, prof, nsqualls=5, meandur=1.0, meansize=0.05, rhotopin=0.1, stopin=-1e-3,
+                         utopin=-0.02, seed=3)
+    r.scaling[:] = np.linspace(0.1, 0.5, 5)
+    d = str(tmp_path / "ck")
+    C.write(d, v0, p, 17, 1e-3, 2.5, rain=r, iashtime=9)
+    first = open(d + "/header").read().splitlines()[0]
+    assert len(first) == 7 * 9 and first.split()[-2:] == ["5", "9"]
+    assert os.path.getsize(d + "/checkpoint.rain_squalls") == 5 * 12 * 8
+    v, head = C.read(d, rain=True, bottom_specified=True)
+    assert np.array_equal(v, v0) and head["nsqualls"] == 5 and head["iashtime"] == 9 and head["istep"] == 17
+    r2 = rain.RainSqualls(p, prof, nsqualls=5, meandur=1.0, meansize=0.05, rhotopin=0.1, stopin=-1e-3,
+                          utopin=-0.02, seed=99)
+    C.read_rain_squalls(d + "/checkpoint.rain_squalls", r2)
+    for a in ("par", "sigma_t", "start", "scaling", "loct", "locp"):
+        assert np.array_equal(getattr(r2, a), getattr(r, a)), a
+    C.write(str(tmp_path / "plain"), v0, p, 1, dt, 0.0, iashtime=4)
+    assert len(open(str(tmp_path / "plain") + "/header").read().splitlines()[0]) == 6 * 9
