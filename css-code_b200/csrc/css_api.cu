@@ -1239,6 +1239,40 @@ extern "C" int css_deriv(css_ctx *c, int dir, int order, const double *x, double
   return CSS_OK;
 }
 
+// The six derivative routines by the reference's names, with its `var`
+// argument (derivatives.f90:558-562): var >= 1 takes the boundary condition
+// of field var from ibcr (r) or ibct (theta), var <= 0 means bdry = -var.
+// Dbydp / D2bydp2 have no boundary variants and ignore var.
+static int deriv_var(css_ctx *c, int dir, int order, const double *x, double *dx, const double *b1,
+                     const double *b2, int var, const char *who) {
+  if (!c) { set_err("%s: NULL", who); return CSS_ERR_ARG; }
+  int bdry = 1;
+  if (dir < 2) {
+    if (var > 12) { set_err("%s: var %d beyond the 12 fields of the BC tables", who, var); return CSS_ERR_ARG; }
+    bdry = var >= 1 ? (dir == 0 ? c->g.ibcr[var] : c->g.ibct[var]) : -var;
+    if (bdry < 0 || bdry > 4) { set_err("%s: var %d gives no boundary variant 0..4", who, var); return CSS_ERR_ARG; }
+  }
+  return css_deriv(c, dir, order, x, dx, b1, b2, bdry);
+}
+extern "C" int css_dbydr(css_ctx *c, const double *x, double *dx, const double *b1, const double *b2, int var) {
+  return deriv_var(c, 0, 1, x, dx, b1, b2, var, "css_dbydr");
+}
+extern "C" int css_d2bydr2(css_ctx *c, const double *x, double *dx, const double *b1, const double *b2, int var) {
+  return deriv_var(c, 0, 2, x, dx, b1, b2, var, "css_d2bydr2");
+}
+extern "C" int css_dbydt(css_ctx *c, const double *x, double *dx, const double *b1, const double *b2, int var) {
+  return deriv_var(c, 1, 1, x, dx, b1, b2, var, "css_dbydt");
+}
+extern "C" int css_d2bydt2(css_ctx *c, const double *x, double *dx, const double *b1, const double *b2, int var) {
+  return deriv_var(c, 1, 2, x, dx, b1, b2, var, "css_d2bydt2");
+}
+extern "C" int css_dbydp(css_ctx *c, const double *x, double *dx, int var) {
+  return deriv_var(c, 2, 1, x, dx, nullptr, nullptr, var, "css_dbydp");
+}
+extern "C" int css_d2bydp2(css_ctx *c, const double *x, double *dx, int var) {
+  return deriv_var(c, 2, 2, x, dx, nullptr, nullptr, var, "css_d2bydp2");
+}
+
 // Lines with explicit closures; used by css_dbyd1_dt0 and css_compact_lines.
 static int run_lines(const double *x, double *dx, int n, int nlines, int order, int lphys, int rphys, int bdry,
                      const double *bclo, const double *bchi, const double *hlo, const double *hhi, double dnum,

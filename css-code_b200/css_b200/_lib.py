@@ -90,6 +90,10 @@ def lib():
         L.css_mlp_set_stream.argtypes = [vp, vp]
         L.css_mlp_set_fused.argtypes = [vp, ctypes.c_int]
         L.css_download_plane.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+        for nm in ("css_dbydr", "css_d2bydr2", "css_dbydt", "css_d2bydt2"):
+            getattr(L, nm).argtypes = [vp, dp, dp, dp, dp, ctypes.c_int]
+        for nm in ("css_dbydp", "css_d2bydp2"):
+            getattr(L, nm).argtypes = [vp, dp, dp, ctypes.c_int]
         L.css_set_clock.argtypes = [vp, ll, ctypes.c_double, ctypes.c_double]
         L.css_get_clock.argtypes = [vp, ctypes.POINTER(ll), dp]
         L.css_inout_init.argtypes = [vp]
@@ -120,5 +124,6 @@ EXPORTS = [
     "css_mlp_destroy", "css_mlp_dims", "css_mlp_forward", "css_mlp_train_step", "css_mlp_params", "css_mlp_grads",
     "css_mlp_set_stream", "css_mlp_set_fused", "css_set_clock", "css_get_clock", "css_inout_init",
     "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_squalls",
-    "css_set_ash_slices", "css_download_plane",
+    "css_set_ash_slices", "css_download_plane", "css_dbydr", "css_d2bydr2", "css_dbydt", "css_d2bydt2",
+    "css_dbydp", "css_d2bydp2",
 ]

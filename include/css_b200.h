@@ -179,6 +179,22 @@ int css_diffusion(css_ctx *ctx, double *vars1, const double *avec, double *dvars
 int css_deriv(css_ctx *ctx, int dir, int order, const double *x, double *dx,
               const double *bc_lo, const double *bc_hi, int bdry);
 
+/* The six routines by the reference's names and with its `var` argument:
+ * Dbydr, D2bydr2 (derivatives.f90:547, :799), Dbydt, D2bydt2 (:1010,
+ * :1265), Dbydp, D2bydp2 (:1480, :1594).  var >= 1 takes the boundary
+ * condition of field var (1-based, 1..12) from the run's ibcr / ibct
+ * tables, var <= 0 means bdry = -var (derivatives.f90:558-562); the phi
+ * routines have no boundary variants and ignore var.  Whole fields: the
+ * reference's loop of per-pencil calls (one x(mynth, mynr) per phi for r)
+ * becomes one call; b1 / b2 are the physical-face data as in css_deriv.
+ * Host pointers.                                                          */
+int css_dbydr(css_ctx *ctx, const double *x, double *dx, const double *b1, const double *b2, int var);
+int css_d2bydr2(css_ctx *ctx, const double *x, double *dx, const double *b1, const double *b2, int var);
+int css_dbydt(css_ctx *ctx, const double *x, double *dx, const double *b1, const double *b2, int var);
+int css_d2bydt2(css_ctx *ctx, const double *x, double *dx, const double *b1, const double *b2, int var);
+int css_dbydp(css_ctx *ctx, const double *x, double *dx, int var);
+int css_d2bydp2(css_ctx *ctx, const double *x, double *dx, int var);
+
 /* Same on device pointers, enqueued on `stream` (a cudaStream_t, NULL =
  * the context stream); returns after enqueueing.                           */
 int css_deriv_dev(css_ctx *ctx, int dir, int order, const double *x, double *dx,

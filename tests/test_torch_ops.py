@@ -72,3 +72,38 @@ def test_leading_dims_fp32_and_wall_data(field):
     lo = torch.full((p.nr, p.nphi), 3.0, dtype=torch.float64, device="cuda")
     assert torch.equal(T.dbydt(x[0], sim, lo, lo, 1), T.dbydt(x[0], sim, None, None, 1))
     assert not torch.equal(T.dbydt(x[0], sim, lo, lo, 4), T.dbydt(x[0], sim, None, None, 4))
+
+
+@pytest.mark.gpu
+def test_reference_named_entry_points_take_var(field):
+    """css_dbydr ... css_d2bydp2: var >= 1 picks the field's boundary
+    variant from ibcr / ibct (derivatives.f90:558-562), var <= 0 is bdry =
+    -var; the result equals css_deriv with that bdry, bit for bit."""
+    import ctypes
+    from css_b200 import _lib
+    from css_b200._lib import CssError, check
+    p, sim, f, rng = field
+    x = np.ascontiguousarray(f)
+    face_r, face_t = (p.nphi, p.nth), (p.nr, p.nphi)
+    lo_r, hi_r = rng.standard_normal(face_r), rng.standard_normal(face_r)
+    lo_t, hi_t = rng.standard_normal(face_t), rng.standard_normal(face_t)
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    L = _lib.lib()
+    # the run's BC integers for field 2 (w) and 5 (s) under the default flags:
+    # stress-free r faces (lbcr_v 4), constant-temperature top (lbcr_s 2),
+    # theta walls lbct_w 1, lbct_s 0
+    cases = [("css_dbydr", 0, 1, 2, 4, lo_r, hi_r), ("css_d2bydr2", 0, 2, 5, 2, lo_r, hi_r),
+             ("css_dbydt", 1, 1, 2, 1, lo_t, hi_t), ("css_d2bydt2", 1, 2, 5, 0, lo_t, hi_t),
+             ("css_dbydr", 0, 1, -3, 3, lo_r, hi_r), ("css_dbydt", 1, 1, 0, 0, lo_t, hi_t)]
+    for name, d, order, var, bdry, lo, hi in cases:
+        out = np.zeros_like(x)
+        check(getattr(L, name)(sim.h, dp(x), dp(out), dp(np.ascontiguousarray(lo)), dp(np.ascontiguousarray(hi)), var))
+        want = sim.deriv(d, order, x, lo.reshape(-1), hi.reshape(-1), bdry)
+        assert np.array_equal(out, want), (name, var)
+    for name, d, order in (("css_dbydp", 2, 1), ("css_d2bydp2", 2, 2)):
+        out = np.zeros_like(x)
+        check(getattr(L, name)(sim.h, dp(x), dp(out), 7))
+        assert np.array_equal(out, sim.deriv(d, order, x, None, None, 1)), name
+    out = np.zeros_like(x)
+    with pytest.raises(CssError):
+        check(L.css_dbydr(sim.h, dp(x), dp(out), None, None, 13))
