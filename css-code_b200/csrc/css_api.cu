@@ -1169,6 +1169,17 @@ extern "C" int css_rhs(css_ctx *c, double *vars1, double *dvars1, int call_num) 
   return CSS_OK;
 }
 
+extern "C" int css_bound(css_ctx *c, double *vars1) {
+  if (!c || !vars1) { set_err("css_bound: NULL"); return CSS_ERR_ARG; }
+  const size_t sb = c->ncell * c->nv * 8;
+  CUDA_TRY(cudaMemcpyAsync(c->vA, vars1, sb, cudaMemcpyHostToDevice, c->stream));
+  k_bound<<<c->nsm * 4, 256, 0, c->stream>>>(c->g, c->vA);
+  if (int rc = check_launch(c)) return rc;
+  CUDA_TRY(cudaMemcpyAsync(vars1, c->vA, sb, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
 extern "C" int css_diffusion(css_ctx *c, double *vars1, const double *avec, double *dvars1) {
   if (!c || !vars1 || !dvars1 || (c->g.magnetic && !avec)) { set_err("css_diffusion: NULL"); return CSS_ERR_ARG; }
   size_t n = c->ncell, sb = n * c->nv * 8;

@@ -1143,6 +1143,51 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
 }
 
 // ---------------------------------------------------------------------------
+// Bound (rhs_mpi.f90:2395-2491) on a whole state, for callers that change
+// the state themselves (the step kernels apply the same rules inside the
+// stage update).  One thread per (theta, phi) column of the two radial faces
+// and per (phi, r) line of the two theta walls; every rule only sets zeros.
+// ---------------------------------------------------------------------------
+__global__ void k_bound(CssGeo g, double *v) {
+  const size_t n = (size_t)g.ncell, np = (size_t)g.nth * g.nphi;
+  const size_t nwall = (size_t)g.nphi * g.nr;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < np + nwall; k += (size_t)gridDim.x * blockDim.x) {
+    if (k < np) {  // radial faces at this (theta, phi)
+      const size_t lo = k, hi = (size_t)(g.nr - 1) * np + k;
+      if (!g.bottom_stress_free) { v[n + lo] = 0.0; v[2 * n + lo] = 0.0; }
+      if (!g.bot_inout) v[3 * n + lo] = 0.0;
+      if (!g.top_inout) {
+        if (!g.top_stress_free) { v[n + hi] = 0.0; v[2 * n + hi] = 0.0; }
+        v[3 * n + hi] = 0.0;
+      }
+      if (g.magnetic) {
+        if (!g.bot_inout) {
+          if (g.bottom_radial_field) v[7 * n + lo] = 0.0;
+          else if (g.bottom_perfect_cond) { v[5 * n + lo] = 0.0; v[6 * n + lo] = 0.0; }
+        }
+        if (!g.top_inout) {
+          if (g.top_radial_field) v[7 * n + hi] = 0.0;
+          else if (g.top_perfect_cond) { v[5 * n + hi] = 0.0; v[6 * n + hi] = 0.0; }
+        }
+      }
+    } else {  // theta walls of this (phi, r) line
+      const size_t q = k - np, ip = q % g.nphi, ir = q / g.nphi;
+      const size_t a = css_idx(g, 0, (int)ip, (int)ir), b = css_idx(g, g.nth - 1, (int)ip, (int)ir);
+      v[n + a] = 0.0;
+      v[n + b] = 0.0;
+      if (!g.theta_stress_free) { v[3 * n + a] = 0.0; v[3 * n + b] = 0.0; }
+      if (g.magnetic) {
+        if (g.theta_perf_conductor) {
+          v[6 * n + a] = 0.0; v[7 * n + a] = 0.0; v[6 * n + b] = 0.0; v[7 * n + b] = 0.0;
+        } else {
+          v[5 * n + a] = 0.0; v[5 * n + b] = 0.0;
+        }
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 // VectorCurlA (derivatives.f90:2106-2294): out = curl(a), fields ordered
 // (theta, phi, r).  Three kernels, one per sweep direction; the r sweep
 // optionally applies Compute_B's boundary zeroing (:1842-1883).

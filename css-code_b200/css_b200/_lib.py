@@ -90,6 +90,7 @@ def lib():
         L.css_mlp_set_stream.argtypes = [vp, vp]
         L.css_mlp_set_fused.argtypes = [vp, ctypes.c_int]
         L.css_download_plane.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+        L.css_bound.argtypes = [vp, dp]
         for nm in ("css_dbydr", "css_d2bydr2", "css_dbydt", "css_d2bydt2"):
             getattr(L, nm).argtypes = [vp, dp, dp, dp, dp, ctypes.c_int]
         for nm in ("css_dbydp", "css_d2bydp2"):
@@ -125,5 +126,5 @@ EXPORTS = [
     "css_mlp_set_stream", "css_mlp_set_fused", "css_set_clock", "css_get_clock", "css_inout_init",
     "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_squalls",
     "css_set_ash_slices", "css_download_plane", "css_dbydr", "css_d2bydr2", "css_dbydt", "css_d2bydt2",
-    "css_dbydp", "css_d2bydp2",
+    "css_dbydp", "css_d2bydp2", "css_bound",
 ]

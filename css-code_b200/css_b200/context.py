@@ -164,6 +164,12 @@ class Simulation:
         check(_lib.lib().css_rhs(self.h, _p(v), _p(dv), int(call_num)))
         return v, dv
 
+    def bound(self, vars1):
+        """Bound() on a copy of vars1 (css_bound)."""
+        v = np.array(vars1, dtype=np.float64, order="C", copy=True)
+        check(_lib.lib().css_bound(self.h, _p(v)))
+        return v
+
     def diffusion(self, vars1, avec=None):
         v = np.array(vars1, dtype=np.float64, order="C", copy=True)
         dv = np.zeros_like(v)

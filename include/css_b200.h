@@ -159,6 +159,12 @@ int css_step_rk4_host(css_ctx *ctx, double *vars0, double dt, int nsteps);
  * call_num == 1 and A otherwise (rhs_mpi.f90:325, :750-752).              */
 int css_rhs(css_ctx *ctx, double *vars1, double *dvars1, int call_num);
 
+/* Bound() (rhs_mpi.f90:2395-2491) on a host state, in place: the wall and
+ * face zeroing of velocities (and of the vector potential for MHD) that the
+ * step entry points already apply after every stage, for a driver that
+ * changes the state itself.                                               */
+int css_bound(css_ctx *ctx, double *vars1);
+
 /* Compute_Diffusion(1) (diffusion.f90:70-474) on host buffers: dvars1 gets
  * the SLD tendency.  As in the reference, vars1 comes back with the mean
  * state subtracted from rho and s (diffusion.f90:168-175).  For MHD, vars1

@@ -2786,6 +2786,11 @@ int orc_build_squalls(orc_ctx *c, int sstruct, int nsq, const double *sq) {
   return CSS_OK;
 }
 
+int orc_bound(orc_ctx *c, double *vars1) {
+  bound(c, vars1);
+  return CSS_OK;
+}
+
 /* Step_RK2_TVD / Step_RK3_TVD (step_rk4.f90:31-335): the SLD tendency of
    the step's start (forward Euler) is added once, after the last stage's
    combination and before its Bound */

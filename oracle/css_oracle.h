@@ -48,6 +48,7 @@ int orc_deriv(orc_ctx *c, int dir, int order, const double *x, double *dx,
 int orc_rhs(orc_ctx *c, double *vars1, double *dvars1, int call_num);
 int orc_diffusion(orc_ctx *c, double *vars1, const double *avec, double *dvars1);
 int orc_step_rk4(orc_ctx *c, double *vars0, double dt, int nsteps);
+int orc_bound(orc_ctx *c, double *vars1);
 int orc_dbyd1_dt0(const double *x, double *dxdy, const double *bdat1,
                   const double *bdat2, int n1, int ibc, int nlines);
 int orc_compact_lines(const double *x, double *dx, int n, int nlines, int order, int lphys, int rphys,

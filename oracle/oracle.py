@@ -46,6 +46,7 @@ def lib():
         L.orc_step_size.argtypes = [ctypes.c_void_p, _dp, ctypes.c_double, _dp]
         L.orc_shell_averages.argtypes = [ctypes.c_void_p, _dp, ctypes.POINTER(ctypes.c_int), ctypes.c_int, _dp, _dp]
         L.orc_spectrum.argtypes = [ctypes.c_void_p, _dp, ctypes.c_int, _dp]
+        L.orc_bound.argtypes = [ctypes.c_void_p, _dp]
         L.orc_set_clock.argtypes = [ctypes.c_void_p, ctypes.c_longlong, ctypes.c_double, ctypes.c_double]
         L.orc_get_clock.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), _dp]
         L.orc_inout_init.argtypes = [ctypes.c_void_p, _dp]
@@ -166,6 +167,11 @@ class Oracle:
         out = np.zeros((self.p.nr, self.p.nphi // 2))
         _check(lib().orc_spectrum(self.h, _ptr(v), int(kind), _ptr(out)))
         return out
+
+    def bound(self, vars1):
+        v = np.array(vars1, dtype=np.float64, order="C", copy=True)
+        _check(lib().orc_bound(self.h, _ptr(v)))
+        return v
 
     def step(self, vars0, dt, nsteps=1):
         v = np.array(vars0, dtype=np.float64, order="C", copy=True)

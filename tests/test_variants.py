@@ -97,3 +97,26 @@ def test_variant_parity(name, gpu_available):
     o = orc.step(v, dt, 5)
     check(p, prof, v, g, o, bar=1e-10)
     assert np.isfinite(g).all()
+
+
+BOUND_CASES = dict(VARIANTS, **{"default": {}, "mhd-default": dict(_magnetic=True),
+                                "open-top": dict(top_inout=1), "open-bottom": dict(bot_inout=1)})
+
+
+@pytest.mark.parametrize("name", ["default", "no-slip-both", "theta-u-fixed", "mhd-default", "mhd-perfect-conductor",
+                                  "open-top", "open-bottom"])
+def test_bound_entry_point(name, gpu_available):
+    """css_bound applies Bound() (rhs_mpi.f90:2395-2491) to a whole state
+    exactly as the oracle does: the same entries zeroed, the rest untouched."""
+    from css_b200.context import Simulation
+    flags = dict(BOUND_CASES[name])
+    mag = flags.pop("_magnetic", False)
+    p, prof, v0, dt, _ = problem.build((32, 32, 64), decomp=(2, 2, 4), magnetic=mag)
+    for k, val in flags.items():
+        setattr(p, k, val)
+    rng = np.random.default_rng(sum(map(ord, name)))
+    v = v0 + 1e-2 * rng.standard_normal(v0.shape)
+    g = Simulation(p, prof).bound(v)
+    o = O.Oracle(p, prof).bound(v)
+    assert np.array_equal(g, o)
+    assert (g == 0.0).sum() > 0 and np.array_equal(g[:, 1:-1, :, 1:-1], v[:, 1:-1, :, 1:-1])
