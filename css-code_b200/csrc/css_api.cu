@@ -258,14 +258,20 @@ template <int MT, int TLC>
 static int setup_mt() {
   int mx = 200 * 1024;
 #define CSS_SMEM_ATTR(...) CUDA_TRY(cudaFuncSetAttribute(__VA_ARGS__, cudaFuncAttributeMaxDynamicSharedMemorySize, mx))
-  CSS_SMEM_ATTR(k_theta_terms<MT, TLC, double>);
-  CSS_SMEM_ATTR(k_theta_terms<MT, TLC, float>);
-  CSS_SMEM_ATTR(k_phi_terms<MT, TLC, double>);
-  CSS_SMEM_ATTR(k_phi_terms<MT, TLC, float>);
+  CSS_SMEM_ATTR(k_theta_terms<MT, TLC, double, 0>);
+  CSS_SMEM_ATTR(k_theta_terms<MT, TLC, float, 0>);
+  CSS_SMEM_ATTR(k_phi_terms<MT, TLC, double, 0>);
+  CSS_SMEM_ATTR(k_phi_terms<MT, TLC, float, 0>);
+  CSS_SMEM_ATTR(k_theta_terms<MT, TLC, double, 1>);
+  CSS_SMEM_ATTR(k_theta_terms<MT, TLC, float, 1>);
+  CSS_SMEM_ATTR(k_phi_terms<MT, TLC, double, 1>);
+  CSS_SMEM_ATTR(k_phi_terms<MT, TLC, float, 1>);
   CSS_SMEM_ATTR(k_radial_terms<MT, TLC, double, 0>);
   CSS_SMEM_ATTR(k_radial_terms<MT, TLC, float, 0>);
   CSS_SMEM_ATTR(k_radial_terms<MT, TLC, double, 1>);
   CSS_SMEM_ATTR(k_radial_terms<MT, TLC, float, 1>);
+  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, double, 2>);
+  CSS_SMEM_ATTR(k_radial_terms<MT, TLC, float, 2>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, float>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, float>);
@@ -921,7 +927,12 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   int TL = c->tl_theta;
   dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_THETA);
-  LAUNCH_MT(1, TL, k_theta_terms, (TS), gt, smem_theta_terms(mag, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  if (mag)
+    LAUNCH_MT(1, TL, k_theta_terms, (TS, 1), gt, smem_theta_terms(mag, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+              TL);
+  else
+    LAUNCH_MT(1, TL, k_theta_terms, (TS, 0), gt, smem_theta_terms(mag, g.d[1].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+              TL);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   TL = c->tl_phi;
@@ -941,7 +952,14 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
     }
   }
   if (!pers)
-    LAUNCH_MT(2, TL, k_phi_terms, (TS), gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf, TL);
+  {
+    if (mag)
+      LAUNCH_MT(2, TL, k_phi_terms, (TS, 1), gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+                TL);
+    else
+      LAUNCH_MT(2, TL, k_phi_terms, (TS, 0), gp, smem_phi_terms(mag, g.d[2].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+                TL);
+  }
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   if constexpr (sizeof(TS) == 8) {
@@ -953,7 +971,10 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   TL = c->tl_r;
   const dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_RADIAL);
-  if (c->io)
+  if (mag)
+    LAUNCH_MT(0, TL, k_radial_terms, (TS, 2), gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
+              TL);
+  else if (c->io)
     LAUNCH_MT(0, TL, k_radial_terms, (TS, 1), gr, smem_radial_terms(mag, g.d[0].maxm, TL), g, cur, c->bf, c->dv, c->tbuf,
               TL);
   else

@@ -269,7 +269,7 @@ __device__ __forceinline__ int solve_tasks(int nd, int TL) {
 // (vars1), B = curl A (MHD) in bf, dv = dvars1 (written, not read), tbuf =
 // the stage temperature (written here, read by the later kernels).
 // ---------------------------------------------------------------------------
-template <int MT, int TLC, typename TV>
+template <int MT, int TLC, typename TV, int MAG>
 __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const TV *__restrict__ cur,
                                                      const double *__restrict__ bf, double *__restrict__ dv,
                                                      double *__restrict__ tbuf, int TLrt) {
@@ -281,7 +281,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const TV *__restr
   const CssDir &D = g.d[1];
   const int t0 = D.start[bt], m = MT ? MT : D.size[bt];
   const int dtype = dtype_of(D, bt);
-  const int mag = g.magnetic;
+  constexpr int mag = MAG;  // compile-time: a hydro run carries no MHD code
   const int SR = m + 9, SO = m + 1, TS = 3 * (m + 2);
   const size_t n = (size_t)g.ncell;
   const int nh = mag ? 6 : 4;   // w v u s [bp br]
@@ -431,13 +431,13 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const TV *__restr
 // ---------------------------------------------------------------------------
 // tables, line solves and pointwise physics of one phi tile whose fields are
 // in H (shared by the one-tile-per-CTA kernel and the persistent one)
-template <int MT, int TLC>
+template <int MT, int TLC, int MAG>
 __device__ __forceinline__ void phi_tile_compute(const CssGeo &g, const double *__restrict__ bf,
                                                  double *__restrict__ dv, const double *__restrict__ tbuf, int TL,
                                                  int bp, int tb, int ir, double *H, double *O, double *Tb) {
   const CssDir &D = g.d[2];
   const int p0 = D.start[bp], m = MT ? MT : D.size[bp];
-  const int mag = g.magnetic;
+  constexpr int mag = MAG;
   const int SR = TL + 1, TS = 3 * (m + 2);
   const size_t n = (size_t)g.ncell;
   const int nd = mag ? 8 : 6;
@@ -536,7 +536,7 @@ __device__ __forceinline__ void phi_tile_compute(const CssGeo &g, const double *
   }
 }
 
-template <int MT, int TLC, typename TV>
+template <int MT, int TLC, typename TV, int MAG>
 __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restrict__ cur,
                                                    const double *__restrict__ bf, double *__restrict__ dv,
                                                    const double *__restrict__ tbuf, int TLrt) {
@@ -547,7 +547,7 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restric
   const int ir = blockIdx.y;
   const CssDir &D = g.d[2];
   const int p0 = D.start[bp], m = MT ? MT : D.size[bp];
-  const int mag = g.magnetic;
+  constexpr int mag = MAG;
   const int SR = TL + 1;
   const size_t n = (size_t)g.ncell;
   const int nh = mag ? 7 : 5;  // rho v w u s [bt br]
@@ -576,7 +576,7 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restric
     for (int k = 0; k < 5; k++) tile_phi<MT, TLC>(g, fs[k], H + k * HS, SR, p0, m, tb, TL, ir, ms[k]);
     for (int k = 5; k < nh; k++) tile_phi<MT, TLC>(g, fb[k - 5], H + k * HS, SR, p0, m, tb, TL, ir);
   }
-  phi_tile_compute<MT, TLC>(g, bf, dv, tbuf, TL, bp, tb, ir, H, O, Tb);
+  phi_tile_compute<MT, TLC, MAG>(g, bf, dv, tbuf, TL, bp, tb, ir, H, O, Tb);
 }
 
 // Phi_Terms as a persistent kernel (FP64 stage input, compile-time block
@@ -638,7 +638,8 @@ __global__ void __launch_bounds__(128) k_phi_terms_p(CssGeo g, const double *__r
     if (t + gridDim.x < ntile) issue(t + gridDim.x, Hb[(it + 1) & 1]);
     const int ir = (int)(t / per_r), x = (int)(t - (long long)ir * per_r);
     const int bp = x / nchunk, tb = (x - bp * nchunk) * TL;
-    phi_tile_compute<MT, TLC>(g, bf, dv, tbuf, TL, bp, tb, ir, H, O, Tb);
+    if (mag) phi_tile_compute<MT, TLC, 1>(g, bf, dv, tbuf, TL, bp, tb, ir, H, O, Tb);
+    else phi_tile_compute<MT, TLC, 0>(g, bf, dv, tbuf, TL, bp, tb, ir, H, O, Tb);
   }
   cp_async_wait<0>();
 }
@@ -648,6 +649,7 @@ __global__ void __launch_bounds__(128) k_phi_terms_p(CssGeo g, const double *__r
 struct RadIn {
   double u, rho, t, dw_r, dv_r, du_r, ds_r, d2s_r, bt, bp, br, dbt_r, dbp_r;
 };
+template <int MAG>
 __device__ __forceinline__ void radial_point(const CssGeo &g, int ir, const RadIn &q, double &drho, double &dw,
                                              double &dvv, double &du, double &ds) {
   const int nu = g.non_uniform;
@@ -677,7 +679,7 @@ __device__ __forceinline__ void radial_point(const CssGeo &g, int ir, const RadI
     if (nu) d2 = d2 * (w3 * w3);
     ds = ds + g.ks[ir] * d2 * oorho;
   }
-  if (g.magnetic) {
+  if (MAG) {
     double oo = invrho * ONE_OVER_4PI;
     w1 = q.dbt_r;
     if (nu) w1 = w1 * w3;
@@ -741,17 +743,18 @@ __device__ __forceinline__ void inout_face(const CssGeo &g, int j, int m, bool t
 // the datum times the block's unit response (resp) is added afterwards.
 // ---------------------------------------------------------------------------
 // One tile of Radial_Terms + Density_Terms_Radial: r block br, theta lines
-// tb .. tb+TL-1, phi ip; sm is the CTA's shared buffer.  OPEN = 1 compiles
+// tb .. tb+TL-1, phi ip; sm is the CTA's shared buffer.  KIND: 0 a closed
+// hydro run, 1 a hydro run with open radial faces, 2 MHD; KIND 1 compiles
 // the open radial boundaries in (a run with top_inout or bot_inout); the
 // closed instance carries none of their code.
-template <int MT, int TLC, typename TV, int OPEN>
+template <int MT, int TLC, typename TV, int KIND>
 __device__ __forceinline__ void radial_tile(const CssGeo &g, const TV *__restrict__ cur, const double *__restrict__ bf,
                                             double *__restrict__ dv, const double *__restrict__ tbuf, int TL, int br,
                                             int tb, int ip, double *sm) {
   const CssDir &D = g.d[0];
   const int r0 = D.start[br], m = MT ? MT : D.size[br];
   const int dtype = dtype_of(D, br);
-  const int mag = g.magnetic;
+  constexpr int mag = KIND == 2;  // known at compile time: a hydro run carries no MHD code
   const int SR = TL, TS = 3 * (m + 2);  // lines contiguous, unpadded (4 CTAs per SM)
   const size_t n = (size_t)g.ncell;
   const int nh = mag ? 7 : 5;  // w v u s rho [bt bp]
@@ -784,7 +787,7 @@ __device__ __forceinline__ void radial_tile(const CssGeo &g, const TV *__restric
   // open faces (a radial block has at most one physical face): the top one
   // takes d(rho)/dr with bdry 2 and no datum, the bottom one with the datum
   // left in x-space (rhs_mpi.f90:2020-2023, :1895-1898)
-  const bool top_open = OPEN && D.rphys[br] && g.top_inout, bot_open = OPEN && D.lphys[br] && g.bot_inout;
+  const bool top_open = KIND == 1 && D.rphys[br] && g.top_inout, bot_open = KIND == 1 && D.lphys[br] && g.bot_inout;
   auto bdry_of = [&](int k) { return (k == 5 && top_open) ? 2 : g.ibcr[var[k]]; };
   for (int k = 0; k < nd; k++) stage_table(g, 0, br, k == 4 ? 2 : 1, bdry_of(k), m, Tb + k * TS);
   __syncthreads();
@@ -843,7 +846,7 @@ __device__ __forceinline__ void radial_tile(const CssGeo &g, const TV *__restric
       RadIn q;
       size_t id = gather(j, l, q);
       double drho = dv[id], dw = dv[n + id], dvv = dv[2 * n + id], du = dv[3 * n + id], ds = dv[4 * n + id];
-      radial_point(g, r0 + j, q, drho, dw, dvv, du, ds);
+      radial_point<mag>(g, r0 + j, q, drho, dw, dvv, du, ds);
       double d;
       if (bot_open) {
         d = g.invpconst * q.rho * du / q.t;  // rhs_mpi.f90:1894
@@ -892,7 +895,7 @@ __device__ __forceinline__ void radial_tile(const CssGeo &g, const TV *__restric
         q.dbt_r = ol[6 * OS]; q.dbp_r = ol[7 * OS];
       }
       double drho = in_[k][0], dw = in_[k][1], dvv = in_[k][2], du = in_[k][3], ds = in_[k][4];
-      radial_point(g, ir, q, drho, dw, dvv, du, ds);
+      radial_point<mag>(g, ir, q, drho, dw, dvv, du, ds);
       // Density_Terms_Radial
       double w1 = O[5 * OS + (size_t)j * SR + l];
       if (phys) w1 = w1 + datum[l] * resp[j + 1];
@@ -928,7 +931,7 @@ __device__ __forceinline__ void radial_tile(const CssGeo &g, const TV *__restric
 }
 
 // grid: x = r block * nchunk + theta chunk, y = phi; one tile per CTA
-template <int MT, int TLC, typename TV, int OPEN>
+template <int MT, int TLC, typename TV, int KIND>
 __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__restrict__ cur,
                                                       const double *__restrict__ bf, double *__restrict__ dv,
                                                       const double *__restrict__ tbuf, int TLrt) {
@@ -936,7 +939,7 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
   const int TL = TLC ? TLC : TLrt;
   const int nchunk = (g.nth + TL - 1) / TL;
   const int br = blockIdx.x / nchunk;
-  radial_tile<MT, TLC, TV, OPEN>(g, cur, bf, dv, tbuf, TL, br, (blockIdx.x - br * nchunk) * TL, blockIdx.y, sm);
+  radial_tile<MT, TLC, TV, KIND>(g, cur, bf, dv, tbuf, TL, br, (blockIdx.x - br * nchunk) * TL, blockIdx.y, sm);
 }
 
 // ---------------------------------------------------------------------------
