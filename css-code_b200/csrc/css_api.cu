@@ -10,6 +10,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 #include <sys/stat.h>
 
@@ -273,6 +274,10 @@ static int setup_mt() {
   CSS_SMEM_ATTR(k_radial_terms<MT, TLC, double, 2>);
   CSS_SMEM_ATTR(k_radial_terms<MT, TLC, float, 2>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double, 1>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double, 2>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double, 3>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double, 4>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, float>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, float>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, double>);
@@ -991,6 +996,22 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_RHOT_UPDATE);
+  bool staged = false;  // FP64 RK4 stages: the stage is a template argument
+  if constexpr (std::is_same<TS, double>::value && std::is_same<TO, double>::value) {
+    staged = stage >= 1 && stage <= 4;
+    switch (stage) {
+      case 1: LAUNCH_MT(1, TL, k_rhot_update, (TS, TO, 1), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            ca, cb, dsld, TL, c->flag); break;
+      case 2: LAUNCH_MT(1, TL, k_rhot_update, (TS, TO, 2), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            ca, cb, dsld, TL, c->flag); break;
+      case 3: LAUNCH_MT(1, TL, k_rhot_update, (TS, TO, 3), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            ca, cb, dsld, TL, c->flag); break;
+      case 4: LAUNCH_MT(1, TL, k_rhot_update, (TS, TO, 4), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            ca, cb, dsld, TL, c->flag); break;
+      default: break;
+    }
+  }
+  if (!staged)
   LAUNCH_MT(1, TL, k_rhot_update, (TS, TO), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
             ca, cb, dsld, TL, c->flag);
   prof_end(c);

@@ -955,11 +955,14 @@ __global__ void __launch_bounds__(128, 4) k_radial_terms(CssGeo g, const TV *__r
 //   stage 5: nx = ca*v0 + cb*cur + dtcur*dv
 //   stage 6: nx = (ca*v0 + cb*cur + dtcur*dv) + dsld*vs  (nx may be v0)
 // ---------------------------------------------------------------------------
-template <int MT, int TLC, typename TS, typename TO>
+template <int MT, int TLC, typename TS, typename TO, int STG = -1>
 __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restrict__ cur,
                                                      double *__restrict__ dv, const double *v0, double *vs, TO *nx,
-                                                     const double *__restrict__ tbuf, int stage, double dtcur,
+                                                     const double *__restrict__ tbuf, int stage_rt, double dtcur,
                                                      double ca, double cb, double dsld, int TLrt, int *flag) {
+  // STG >= 0: the stage is known at compile time (the RK4 stages of an FP64
+  // run), so the combination carries no per-point stage branches
+  const int stage = STG >= 0 ? STG : stage_rt;
   extern __shared__ double sm[];
   const int TL = TLC ? TLC : TLrt;
   const int nchunk = (g.nphi + TL - 1) / TL;
