@@ -1198,6 +1198,11 @@ extern "C" int css_step_rk4_host(css_ctx *c, double *vars0, double dt, int nstep
 
 extern "C" int css_rhs(css_ctx *c, double *vars1, double *dvars1, int call_num) {
   if (!c || !vars1 || !dvars1) { set_err("css_rhs: NULL"); return CSS_ERR_ARG; }
+  if (c->io && !(c->deltat > 0.0)) {
+    set_err("css_rhs: an open radial boundary's mean-flow terms divide by the step size: set it with "
+            "css_set_clock first");
+    return CSS_ERR_ARG;
+  }
   size_t sb = c->ncell * c->nv * 8;
   CUDA_TRY(cudaMemcpyAsync(c->vA, vars1, sb, cudaMemcpyHostToDevice, c->stream));
   c->rhs_call = call_num;

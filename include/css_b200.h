@@ -156,7 +156,8 @@ int css_step_rk4_host(css_ctx *ctx, double *vars0, double dt, int nsteps);
 
 /* RHS(call_num) (rhs_mpi.f90:279-783) on host buffers.  vars1 is in/out as
  * in the reference: for MHD, slots 5..7 come back holding B = curl A when
- * call_num == 1 and A otherwise (rhs_mpi.f90:325, :750-752).              */
+ * call_num == 1 and A otherwise (rhs_mpi.f90:325, :750-752).  A run with an
+ * open radial boundary needs the clock's deltat set (css_set_clock) first. */
 int css_rhs(css_ctx *ctx, double *vars1, double *dvars1, int call_num);
 
 /* Bound() (rhs_mpi.f90:2395-2491) on a host state, in place: the wall and

@@ -393,3 +393,8 @@ def test_open_boundary_rejections(gpu_available):
     closed = Simulation(build()[0], prof)
     with pytest.raises(CssError):
         closed.inout_init()
+    fresh = Simulation(p, prof)  # open top, clock never set: deltat 0
+    with pytest.raises(CssError):
+        fresh.rhs(v0, 2)
+    fresh.set_clock(1, 0.0, dt)
+    assert np.isfinite(fresh.rhs(v0, 2)[1]).all()
