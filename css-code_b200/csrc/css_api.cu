@@ -278,6 +278,10 @@ static int setup_mt() {
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double, 2>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double, 3>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, double, 4>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, float, 1>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, float, 2>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, float, 3>);
+  CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, double, 4>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, double, float>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, float>);
   CSS_SMEM_ATTR(k_rhot_update<MT, TLC, float, double>);
@@ -996,7 +1000,7 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
   TL = c->tl_theta;
   dim3 gu(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
   prof_begin(c, KI_RHOT_UPDATE);
-  bool staged = false;  // FP64 RK4 stages: the stage is a template argument
+  bool staged = false;  // RK4 stages: the stage is a template argument
   if constexpr (std::is_same<TS, double>::value && std::is_same<TO, double>::value) {
     staged = stage >= 1 && stage <= 4;
     switch (stage) {
@@ -1010,6 +1014,17 @@ static int launch_rhs(css_ctx *c, const TS *cur, TO *nx, int stage, double dtcur
             ca, cb, dsld, TL, c->flag); break;
       default: break;
     }
+  } else if constexpr (std::is_same<TS, double>::value) {  // mixed, stage 1: FP64 vars0 -> FP32 U1
+    if (stage == 1) { staged = true; LAUNCH_MT(1, TL, k_rhot_update, (TS, TO, 1), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            ca, cb, dsld, TL, c->flag);; }
+  } else if constexpr (std::is_same<TO, float>::value) {  // mixed, stages 2-3: FP32 -> FP32
+    if (stage == 2) { staged = true; LAUNCH_MT(1, TL, k_rhot_update, (TS, TO, 2), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            ca, cb, dsld, TL, c->flag);; }
+    else if (stage == 3) { staged = true; LAUNCH_MT(1, TL, k_rhot_update, (TS, TO, 3), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            ca, cb, dsld, TL, c->flag);; }
+  } else {  // mixed, stage 4: FP32 U3 -> FP64 vars0
+    if (stage == 4) { staged = true; LAUNCH_MT(1, TL, k_rhot_update, (TS, TO, 4), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
+            ca, cb, dsld, TL, c->flag);; }
   }
   if (!staged)
   LAUNCH_MT(1, TL, k_rhot_update, (TS, TO), gu, smem_rhot(g.d[1].maxm, TL), g, cur, c->dv, c->v0, c->vs, nx, c->tbuf, stage, dtcur,
