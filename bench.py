@@ -3,21 +3,28 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload NAME]
 
-Default workload: the 128x256x512 hydro polytrope (3 density scale heights,
-FP64, virtual decomposition 4x8x16 = 32^3 blocks), synthetic seeded state.
-One step = one full RK4 step (4 RHS evaluations + slope-limited diffusion).
-`value` is device-timed with CUDA events on the stream the library runs on,
-inputs resident in HBM (the state, 671 MB per buffer, is larger than L2).
-`e2e` is the same metric through the C ABI with host buffers: each step
-uploads the state from pinned host memory, advances it one step and reads
-it back (css_step_rk4_host), as a Fortran driver that keeps vars0 on the
-host would call it.  N > 1: one process per GPU, each advancing its own
-replica (the hot path runs the whole domain on one GPU; no collective),
-time = max over ranks.
+Default workload: the 256x512x1024 MHD shell (nv = 8: rho, u_theta, u_phi,
+u_r, s and the vector potential A; 5 density scale heights, magnetic Prandtl
+number 2 through the SLD scaling, FP64, virtual decomposition 8x16x32 =
+32^3 blocks), synthetic seeded state with the random, tapered vector
+potential of Initialize_Mag.  --workload hydro-128x256x512 runs the hydro
+polytrope (3 scale heights, 4x8x16 blocks).  One step = one full RK4 step
+(4 RHS evaluations + slope-limited diffusion).  `value` is device-timed
+with CUDA events on the stream the library runs on, inputs resident in HBM
+(the state, 8.6 GB per buffer for MHD, is larger than L2).  `e2e` is the
+same metric through the C ABI with host buffers: each step uploads the
+state from pinned host memory, advances it one step and reads it back
+(css_step_rk4_host), as a Fortran driver that keeps vars0 on the host would
+call it.  N > 1: one process per GPU, each advancing its own replica (the
+hot path runs the whole domain on one GPU; no collective), time = max over
+ranks.
 
 --impl reference times the reference's CPU implementation of the same path:
 the FP64 C restatement in oracle/ (the Fortran itself cannot be built here),
-with every host thread, on a bounded number of steps of the same workload.
+with every host thread, on a bounded sample of the workload (for the MHD
+shell: RK4 steps of a 128x256x512 MHD shell with the same physics and the
+same 32^3 virtual blocks; cell-updates/s is per cell, and a full step of
+the 1.3e8-cell shell would take over a minute of host time).
 """
 import argparse
 import json
@@ -54,14 +61,45 @@ def kernel_alg_bytes(name, nv, stage_mix=None):
         "curl_phi": 2 + 3 + 1,
         "curl_r": 2 + 3 + 3,
         "sld_vcc": 3 + (4 if mag else 0) + 1,
-        "sld": nv + 1 + nv,
+        # MHD runs the SLD as two launches (hydro fields, then A), timed as
+        # one, each reading the speed^2: nv + 2 + nv words over the pair
+        "sld": nv + (2 if mag else 1) + nv,
         "sld_ohmic": 2 + 3 + 3 + 2,
     }.get(name)
+    if name == "thph":
+        # the state's five fields [+ B], the tendency of every field and T
+        w = 5 + nb + nv + 1
+    if name == "rstage":
+        # the slab's five fields [+ B_theta, B_phi, B_r], the tendency, T,
+        # vars0 and the accumulator read; the next state written, and the
+        # accumulator in stages 1-3 (average over the four stages)
+        w = 5 + nb + nv + 1 + 2 * nv + (3 * nv) / 4.0 + nv
     if name == "rhot_update":
         # average over the four stages: reads rho,w,s + dv,v0,vs (3 nv), writes
         # vs + next (2 nv) in stages 1-3 and next only (nv) in stage 4
         w = 3 + 3 * nv + (3 * 2 * nv + nv) / 4.0
     return None if w is None else 8.0 * w
+
+
+# The bounded CPU sample of a workload: (dims, build options, description).
+# None: the workload itself (a step takes seconds on the host cores).
+CPU_SAMPLES = {
+    "mhd-256x512x1024": ((128, 256, 512), dict(magnetic=True, decomp=(4, 8, 16), n_rho=5.0),
+                         "a 128x256x512 MHD shell with the workload's physics (n_rho 5, Pm 2) and 32^3 virtual "
+                         "blocks (decomposition 4x8x16)"),
+}
+
+
+def cpu_sample(workload):
+    """(params, profiles, vars0, dt, description) of the CPU sample."""
+    from css_b200 import problem
+    spec = CPU_SAMPLES.get(workload)
+    if spec is None:
+        p, prof, v0, dt, _ = problem.build(workload)
+        return p, prof, v0, dt, "the full %dx%dx%d workload" % (p.nr, p.nth, p.nphi)
+    dims, kw, desc = spec
+    p, prof, v0, dt, _ = problem.build(dims, **kw)
+    return p, prof, v0, dt, desc
 
 
 def step_alg_bytes(nv):
@@ -164,7 +202,14 @@ def max_over_ranks(x, world):
     return float(t.item())
 
 
-def cpu_baseline(p, prof, v0, dt, steps):
+def cpu_baseline(workload, steps):
+    """The oracle (FP64 C restatement, every host thread) on the workload's
+    bounded CPU sample: one warm-up step, then `steps` timed steps."""
+    p, prof, v0, dt, desc = cpu_sample(workload)
+    return cpu_baseline_on(p, prof, v0, dt, steps, desc)
+
+
+def cpu_baseline_on(p, prof, v0, dt, steps, desc):
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     O.set_threads(threads)
@@ -176,8 +221,8 @@ def cpu_baseline(p, prof, v0, dt, steps):
     orc.close()
     cells = p.nr * p.nth * p.nphi
     return {"value": cells * steps / el, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": "%d RK4 steps of the full %dx%dx%d workload (FP64 C restatement, %d OpenMP threads)"
-                      % (steps, p.nr, p.nth, p.nphi, threads), "seconds": el}
+            "sample": "%d RK4 steps of %s (FP64 C restatement, %d OpenMP threads)" % (steps, desc, threads),
+            "seconds": el}
 
 
 def run_reference(args):
@@ -192,7 +237,7 @@ def run_reference(args):
         print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned closure: its SLD "
                           "speed is a prescribed radial profile (diffusion.f90:19-63)"}))
         return 0
-    p, prof, v0, dt, _ = problem.build(args.workload)
+    p, prof, v0, dt, desc = cpu_sample(args.workload)
     from oracle import oracle as O
     threads = os.cpu_count() or 1
     O.set_threads(threads)
@@ -216,12 +261,13 @@ def run_reference(args):
         "impl": "reference", "metric": METRIC, "value": val, "unit": UNIT, "n_gpus": world, "steps": timed,
         "steps_requested": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / timed, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "grid": [p.nr, p.nth, p.nphi], "decomposition": [p.nnr, p.nnt, p.nnp],
-                   "fields": 8 if p.magnetic else 5, "l2": "state larger than L2"},
+        "config": {"workload": args.workload, "sample_grid": [p.nr, p.nth, p.nphi],
+                   "sample_decomposition": [p.nnr, p.nnt, p.nnp], "fields": 8 if p.magnetic else 5,
+                   "l2": "state larger than L2"},
         "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
-                         "sample": "%d RK4 steps of the full workload (bounded to ~%d s of CPU time), FP64 C "
+                         "sample": "%d RK4 steps of %s (bounded to ~%d s of CPU time), FP64 C "
                                    "restatement of the reference (Fortran not buildable here), %d OpenMP threads"
-                                   % (timed, REF_BUDGET_S, threads)},
+                                   % (timed, desc, REF_BUDGET_S, threads)},
         "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out))
@@ -375,9 +421,10 @@ def run_ours(args):
     }
     if clk:
         out["clocks"] = clk
-    if rank == 0 and world == 1 and not args.no_cpu:
-        out["cpu_baseline"] = cpu_baseline(p, prof, v0, dt, args.cpu_steps)
     sim.close()
+    if rank == 0 and world == 1 and not args.no_cpu:
+        del host
+        out["cpu_baseline"] = cpu_baseline(args.workload, args.cpu_steps)
     if rank == 0:
         print(json.dumps(out))
     if world > 1:
@@ -472,9 +519,8 @@ def run_ensemble(args):
         out["clocks"] = clk
     if rank == 0 and world == 1 and not args.no_cpu:
         p, prof, v0, dt = members[0]
-        out["cpu_baseline"] = cpu_baseline(p, prof, v0, dt, 1)
-        out["cpu_baseline"]["sample"] = "1 RK4 step of ensemble member %d (%dx%dx%d) on the FP64 C restatement" % (
-            mine[0], p.nr, p.nth, p.nphi)
+        out["cpu_baseline"] = cpu_baseline_on(p, prof, v0, dt, 1, "ensemble member %d (%dx%dx%d)" % (
+            mine[0], p.nr, p.nth, p.nphi))
     ens.close()
     for sim in sims:
         sim.close()
@@ -624,8 +670,8 @@ def main():
     ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="hydro-128x256x512")
-    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--workload", default="mhd-256x512x1024")
+    ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],

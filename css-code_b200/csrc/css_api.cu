@@ -4,11 +4,13 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <type_traits>
 #include <vector>
@@ -20,6 +22,7 @@
 #include "css_closure.cuh"
 #include "css_lap.cuh"
 #include "css_inout.cuh"
+#include "css_fused.cuh"
 
 using namespace css;
 
@@ -43,10 +46,10 @@ extern "C" const char *css_last_error(void) { return g_err; }
 
 // kernel kinds, for the per-kernel CUDA-event timing of css_profile
 enum KernelId { KI_THETA = 0, KI_PHI, KI_RADIAL, KI_RHOT_UPDATE, KI_CURL_THETA, KI_CURL_PHI, KI_CURL_R,
-                KI_SLD_VCC, KI_SLD, KI_SLD_OHMIC, KI_DERIV, KI_COUNT };
+                KI_SLD_VCC, KI_SLD, KI_SLD_OHMIC, KI_DERIV, KI_THPH, KI_RSTAGE, KI_COUNT };
 static const char *kKernelNames[KI_COUNT] = {"theta_terms", "phi_terms", "radial_terms", "rhot_update",
                                              "curl_theta", "curl_phi", "curl_r", "sld_vcc", "sld", "sld_ohmic",
-                                             "deriv"};
+                                             "deriv", "thph", "rstage"};
 
 struct css_ctx {
   css_params p;
@@ -84,6 +87,8 @@ struct css_ctx {
   long long launches;
   int tl_theta, tl_phi, tl_r;
   int phi_pers = 0;                 // 1: persistent double-buffered phi kernel (autotuned)
+  int fused_ok = 0;                 // the run qualifies for the two-pass RK4 stage (css_fused.cuh)
+  int fused = 0;                    // 1: FP64 RK4 stages run k_thph + k_rstage
   int nsm = 148;                    // SMs of the device
   cudaStream_t own_stream;
   // per-kernel event timing (css_profile)
@@ -308,6 +313,19 @@ static int setup_kernels() {
   if (int rc = setup_mt<16, 8>()) return rc;
   if (int rc = setup_mt<32, 8>()) return rc;
   int mx = 200 * 1024;
+#define CSS_FUSED_ATTR(K, CFG) \
+  CUDA_TRY(cudaFuncSetAttribute(K, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)CFG::SMEM))
+  CSS_FUSED_ATTR(k_thph<0>, ThphCfg<0>);
+  CSS_FUSED_ATTR(k_thph<1>, ThphCfg<1>);
+  CSS_FUSED_ATTR((k_rstage<0, 1>), RstageCfg<0>);
+  CSS_FUSED_ATTR((k_rstage<0, 2>), RstageCfg<0>);
+  CSS_FUSED_ATTR((k_rstage<0, 3>), RstageCfg<0>);
+  CSS_FUSED_ATTR((k_rstage<0, 4>), RstageCfg<0>);
+  CSS_FUSED_ATTR((k_rstage<1, 1>), RstageCfg<1>);
+  CSS_FUSED_ATTR((k_rstage<1, 2>), RstageCfg<1>);
+  CSS_FUSED_ATTR((k_rstage<1, 3>), RstageCfg<1>);
+  CSS_FUSED_ATTR((k_rstage<1, 4>), RstageCfg<1>);
+#undef CSS_FUSED_ATTR
   CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   CUDA_TRY(cudaFuncSetAttribute(k_deriv_theta<2, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
   CUDA_TRY(cudaFuncSetAttribute(k_deriv_phi<1, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
@@ -742,6 +760,14 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   c->tl_theta = pick(c->mt[1], smem_theta_terms, mag, g.d[1].maxm);
   c->tl_phi = pick(c->mt[2], smem_phi_terms, mag, g.d[2].maxm);
   c->tl_r = pick(c->mt[0], smem_radial_terms, mag, g.d[0].maxm);
+  // the two-pass stage (css_fused.cuh): 32-point blocks in every direction,
+  // an FP64 RK4 run with closed radial faces and none of the passes that
+  // sit between the sweeps (explicit viscosity, radiative diffusion, open
+  // faces, prescribed bottom)
+  c->fused_ok = c->mt[0] == 32 && c->mt[1] == 32 && c->mt[2] == 32 && p.precision == 0 &&
+                (p.time_stepper == 4 || p.time_stepper == 0) && !p.laplacian && !p.do_radheat && !p.top_inout &&
+                !p.bot_inout && !p.bottom_specified;
+  c->fused = 0;
   *out = c;
   return CSS_OK;
 }
@@ -1081,6 +1107,42 @@ static int launch_sld(css_ctx *c, const double *v, const double *av, double *dou
   return CSS_OK;
 }
 
+// One RK4 stage in two passes (css_fused.cuh): [curl] -> k_thph -> [SLD
+// of the step's start in stage 1] -> k_rstage<stage>
+static int launch_stage_fused(css_ctx *c, const double *cur, double *nx, int stage, double dtcur, bool with_sld) {
+  const CssGeo &g = c->g;
+  const int mag = g.magnetic;
+  if (mag)
+    if (int rc = launch_curl(c, cur + 5 * c->ncell, c->bf, 1)) return rc;
+  const dim3 ga(g.d[1].nb * g.d[2].nb, g.nr);
+  prof_begin(c, KI_THPH);
+  if (mag) k_thph<1><<<ga, FNT, ThphCfg<1>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf);
+  else k_thph<0><<<ga, FNT, ThphCfg<0>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf);
+  prof_end(c);
+  if (int rc = check_launch(c)) return rc;
+  if (with_sld)
+    if (int rc = launch_sld(c, cur, cur + 5 * c->ncell, c->vs, c->tbuf)) return rc;
+  const dim3 gb(g.d[0].nb * g.d[1].nb, g.nphi);
+  prof_begin(c, KI_RSTAGE);
+#define CSS_RSTAGE(M, S)                                                                                      \
+  k_rstage<M, S><<<gb, FNT, RstageCfg<M>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->v0, c->vs, nx, c->tbuf, \
+                                                             dtcur, c->flag)
+  switch (stage + (mag ? 10 : 0)) {
+    case 1: CSS_RSTAGE(0, 1); break;
+    case 2: CSS_RSTAGE(0, 2); break;
+    case 3: CSS_RSTAGE(0, 3); break;
+    case 4: CSS_RSTAGE(0, 4); break;
+    case 11: CSS_RSTAGE(1, 1); break;
+    case 12: CSS_RSTAGE(1, 2); break;
+    case 13: CSS_RSTAGE(1, 3); break;
+    case 14: CSS_RSTAGE(1, 4); break;
+    default: set_err("launch_stage_fused: stage %d", stage); return CSS_ERR_ARG;
+  }
+#undef CSS_RSTAGE
+  prof_end(c);
+  return check_launch(c);
+}
+
 static int step_stages(css_ctx *c, double dt);
 
 // the prescribed bottom fields at the clock's time (Cubic_Time_Interp)
@@ -1154,6 +1216,12 @@ static int step_stages(css_ctx *c, double dt) {
     if (int rc = launch_rhs(c, (const float *)fB, fA, 3, dt)) return rc;
     if (int rc = launch_rhs(c, (const float *)fA, c->v0, 4, dt)) return rc;
     return CSS_OK;
+  }
+  if (c->fused) {
+    if (int rc = launch_stage_fused(c, c->v0, c->vA, 1, dt / 2.0, sld)) return rc;
+    if (int rc = launch_stage_fused(c, c->vA, c->vB, 2, dt / 2.0, false)) return rc;
+    if (int rc = launch_stage_fused(c, c->vB, c->vA, 3, dt, false)) return rc;
+    return launch_stage_fused(c, c->vA, c->v0, 4, dt, false);
   }
   if (int rc = launch_rhs(c, (const double *)c->v0, c->vA, 1, dt / 2.0, 0.0, 0.0, 0.0, sld)) return rc;
   if (int rc = launch_rhs(c, (const double *)c->vA, c->vB, 2, dt / 2.0)) return rc;
@@ -1524,6 +1592,19 @@ extern "C" int css_autotune(css_ctx *c, int reps, int *chosen) {
 // the autotuner's choices set by hand: tile heights (lines per CTA) of the
 // r, theta and phi kernels and the persistent phi kernel (0/1); a height a
 // direction does not offer is refused
+extern "C" int css_set_fused(css_ctx *c, int on) {
+  if (!c) { set_err("css_set_fused: NULL"); return CSS_ERR_ARG; }
+  if (on && !c->fused_ok) {
+    set_err("css_set_fused: the two-pass stage needs 32-point blocks in r, theta and phi and an FP64 RK4 run "
+            "with closed radial faces, no explicit viscosity, radiative diffusion or prescribed bottom");
+    return CSS_ERR_ARG;
+  }
+  c->fused = on ? 1 : 0;
+  return CSS_OK;
+}
+
+extern "C" int css_get_fused(css_ctx *c) { return c ? c->fused : -1; }
+
 extern "C" int css_set_tiles(css_ctx *c, int tl_r, int tl_theta, int tl_phi, int phi_persistent) {
   if (!c) { set_err("css_set_tiles: NULL"); return CSS_ERR_ARG; }
   const int tl[3] = {tl_r, tl_theta, tl_phi};
@@ -2382,8 +2463,33 @@ extern "C" int css_checkpoint_read(css_ctx *c, const char *dir, int *istep, doub
 // ---------------------------------------------------------------------------
 #define CSS_NOALLOC_DOUBLES (1 << 18)  // 2 MiB of scratch per device
 static __device__ __align__(256) double g_noalloc_scratch[CSS_NOALLOC_DOUBLES];
-static double *g_noalloc_addr[64];     // device address of the array, per device
-static int g_noalloc_ready[64];
+// device address of the array, per device: published with release order
+// once it has been looked up, so a host thread that sees it non-null also
+// sees a finished lookup; the lookup itself runs under g_noalloc_mu
+static std::atomic<double *> g_noalloc_addr[64];
+static std::mutex g_noalloc_mu;
+
+// The array's device address on the current device.  The first lookup on a
+// device loads this library's device code there (under lazy module loading
+// that is when the array itself is placed in device memory), so it must run
+// before the caller hands its device memory to a pool and before any stream
+// capture.
+static int noalloc_scratch(double **out) {
+  int dev = 0;
+  CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) { set_err("css_compact_lines_noalloc: device index %d out of range", dev); return CSS_ERR_ARG; }
+  double *p = g_noalloc_addr[dev].load(std::memory_order_acquire);
+  if (!p) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    p = g_noalloc_addr[dev].load(std::memory_order_relaxed);
+    if (!p) {
+      CUDA_TRY(cudaGetSymbolAddress((void **)&p, g_noalloc_scratch));
+      g_noalloc_addr[dev].store(p, std::memory_order_release);
+    }
+  }
+  *out = p;
+  return CSS_OK;
+}
 
 // LU tables of one (n, lphys, rphys) line for bdry 0..4, written on the
 // device with the same correctly rounded steps as the host's tab_d1/tab_d2
@@ -2456,17 +2562,12 @@ extern "C" int css_compact_lines_noalloc(const double *x, double *dx, int n, int
             need, CSS_NOALLOC_DOUBLES);
     return CSS_ERR_ARG;
   }
+  // the set-up comes first, so a call with nlines == 0 on each device at
+  // start-up does it without launching anything
+  double *T = nullptr;
+  if (int rc = noalloc_scratch(&T)) return rc;
   if (nlines == 0) return CSS_OK;
-  int dev = 0;
-  CUDA_TRY(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) { set_err("css_compact_lines_noalloc: device index %d out of range", dev); return CSS_ERR_ARG; }
-  if (!g_noalloc_ready[dev]) {  // once per device, with that device current
-    double *p = nullptr;
-    CUDA_TRY(cudaGetSymbolAddress((void **)&p, g_noalloc_scratch));
-    g_noalloc_addr[dev] = p;
-    g_noalloc_ready[dev] = 1;
-  }
-  double *T = g_noalloc_addr[dev], *work = T + 15 * ts;
+  double *work = T + 15 * ts;
   cudaStream_t st = (cudaStream_t)stream;
   k_noalloc_tables<<<1, 1, 0, st>>>(T, n, lphys, rphys, order);
   CUDA_TRY(cudaGetLastError());

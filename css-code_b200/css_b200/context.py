@@ -119,6 +119,15 @@ class Simulation:
         check(_lib.lib().css_autotune(self.h, int(reps), ch))
         return tuple(ch)
 
+    def set_fused(self, on):
+        """Two-pass RK4 stage on or off (css_set_fused); on is refused for a
+        run that does not qualify."""
+        check(_lib.lib().css_set_fused(self.h, 1 if on else 0))
+
+    @property
+    def fused(self):
+        return bool(_lib.lib().css_get_fused(self.h))
+
     def set_tiles(self, tl_r, tl_theta, tl_phi, phi_persistent=False):
         """The autotuner's choices by hand (css_set_tiles)."""
         check(_lib.lib().css_set_tiles(self.h, int(tl_r), int(tl_theta), int(tl_phi), 1 if phi_persistent else 0))

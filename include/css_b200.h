@@ -246,10 +246,13 @@ int css_compact_lines(const double *x, double *dx, int n, int nlines, int order,
  * zero: each call writes every table entry and every padded line before
  * reading it.  The array is shared by every call on a device, so calls that
  * overlap on the GPU (other streams, other host threads) race: serialize
- * them on one stream.  The
- * first call on each device looks up the array's device address, so make
- * it before any stream capture.  No memory is allocated, on the device or
- * the host.                                                              */
+ * them on one stream.  The first call on each device (nlines may be 0:
+ * such a call only does this set-up) looks up the array's device address;
+ * under CUDA's lazy module loading that lookup is also when the library's
+ * device code, and with it the array, is placed on that device.  So make
+ * that first call at start-up, before handing device memory to a pool and
+ * before any stream capture.  Later calls allocate nothing, on the device
+ * or the host; concurrent first calls from several host threads are safe. */
 int css_compact_lines_noalloc(const double *x, double *dx, int n, int nlines,
                               int order, int lphys, int rphys, int bdry,
                               const double *bc_lo, const double *bc_hi,
@@ -311,6 +314,21 @@ int css_autotune(css_ctx *ctx, int reps, int *chosen);
  * run Phi_Terms as a persistent kernel that streams the next tile into
  * shared memory while the current one is computed.                         */
 int css_set_tiles(css_ctx *ctx, int tl_r, int tl_theta, int tl_phi, int phi_persistent);
+
+/* The RK4 stage of Step_RK4 (step_rk4.f90:339-493) in two passes over the
+ * device memory instead of four: one kernel per (theta block, phi block,
+ * radius) plane for Source_Theta_Terms, Phi_Terms and Density_Terms_Theta
+ * (rhs_mpi.f90:786-1261, :1522-1605), one per (r block, theta block, phi)
+ * slab for Radial_Terms with Density_Terms_Radial (:1264-1519, :1710-1855),
+ * the theta-wall part of Density_Terms_Theta, the stage combination and
+ * Bound (:2395-2491).  css_create turns it on for runs that qualify: 32-point
+ * virtual blocks in r, theta and phi, FP64 RK4, closed radial faces, no
+ * explicit viscosity, radiative diffusion or prescribed bottom.
+ * css_set_fused(ctx, 0) selects the four-kernel stage (same results to
+ * rounding); css_set_fused(ctx, 1) on a run that does not qualify fails
+ * with CSS_ERR_ARG.  css_get_fused returns the current choice.            */
+int css_set_fused(css_ctx *ctx, int on);
+int css_get_fused(css_ctx *ctx);
 
 /* A batched ensemble of independent runs (many small shells, each with its
  * own grid, decomposition and parameters: hydro and MHD members may mix).

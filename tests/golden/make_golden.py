@@ -1,9 +1,10 @@
 """Generates tests/golden/compact_fd6.npz from the reference's own Python
 operator, CSS-Python/derivatives.py:32 compact_fd6 (with linalg.py:7
-tri_solver), imported from the reference checkout.  Run here, where the
-reference is mounted; the GPU box only reads the committed .npz.
+tri_solver), imported from a checkout of the reference.  Run it where the
+reference is available; tests only read the committed .npz.
 
-    python tests/golden/make_golden.py /root/reference/CSS-Python
+    python tests/golden/make_golden.py <reference checkout>/CSS-Python
+    CSS_PYTHON_DIR=<reference checkout>/CSS-Python python tests/golden/make_golden.py
 
 Cases: dtype=0 (whole line; the only mode of compact_fd6 that is correct,
 its dtype 1-3 closures do not converge), ibc 0..4, n in {16, 33, 64, 128},
@@ -74,4 +75,7 @@ def main(refdir):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/CSS-Python")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("CSS_PYTHON_DIR")
+    if not src:
+        sys.exit("usage: make_golden.py <reference checkout>/CSS-Python (or set CSS_PYTHON_DIR)")
+    main(src)

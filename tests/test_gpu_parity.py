@@ -205,3 +205,38 @@ def test_empty_line_batches(gpu_available):
     x = np.zeros((0, 40))
     assert compact_lines(x, 1, True, True, 1).shape == (0, 40)
     assert dbyd1_dt0(x, np.zeros(0), np.zeros(0), 1).shape == (0, 40)
+
+
+def test_mhd_step_parity_100_steps_32cubed_blocks(gpu_available):
+    """MHD on 32^3 virtual blocks, the block shape of the 256x512x1024 MHD
+    workload (its compile-time 32-point kernels), at 64x64x128 with
+    decomposition 2x2x4, 5 density scale heights and the default walls:
+    100 FP64 RK4 steps from the workload's own kind of initial state
+    (entropy perturbation, random tapered vector potential) within 1e-10 of
+    the oracle in every field."""
+    p, prof, v0, dt, _ = problem.build((64, 64, 128), magnetic=True, decomp=(2, 2, 4), n_rho=5.0)
+    sim, orc = Simulation(p, prof), O.Oracle(p, prof)
+    g1 = sim.step_host(v0, dt, 1)
+    o1 = orc.step(v0, dt, 1)
+    assert max(fieldwise(g1, o1)) < 1e-11, fieldwise(g1, o1)
+    g = sim.step_host(v0, dt, 100)
+    o = orc.step(v0, dt, 100)
+    errs = fieldwise(g, o)
+    sim.close()
+    orc.close()
+    assert np.isfinite(g).all()
+    assert max(errs) < 1e-10, errs
+
+
+def test_hydro_bench_workload_one_step_parity(gpu_available):
+    """The hydro bench workload itself (128x256x512, 4x8x16 blocks): one
+    FP64 RK4 step against the oracle within 1e-11 in every field."""
+    p, prof, v0, dt, _ = problem.build("hydro-128x256x512")
+    sim = Simulation(p, prof)
+    g = sim.step_host(v0, dt, 1)
+    sim.close()
+    orc = O.Oracle(p, prof)
+    o = orc.step(v0, dt, 1)
+    orc.close()
+    errs = fieldwise(g, o)
+    assert max(errs) < 1e-11, errs

@@ -3,14 +3,15 @@ that cannot allocate device memory when they need a derivative (all device
 memory handed to their own pool or a framework's caching allocator, or no
 tolerance for the device-wide synchronization of cudaMalloc/cudaFree).
 
-It must give the same lines as css_compact_lines, which allocates, to the
-tolerance of the other derivative tests, on two calls in a row (the second
-with a different size and closure, so stale scratch contents would show),
-and refuse a request larger than its fixed scratch array.  This file is
-collected last on purpose: if it fails, a run that stops at the first
-failure has already run every other test."""
-import ctypes
-
+It must give the same lines as css_compact_lines, which allocates: bit for
+bit, since both run the same line kernel on tables built by the same
+correctly rounded steps.  Every closure is covered (both ends physical, both
+halo-closed, one of each, bdry 0..4, first and second derivatives), call
+after call on the one shared scratch array, with sizes and closures changing
+between calls so stale scratch contents would show.  An empty batch does
+only the per-device set-up, and a request larger than the fixed scratch
+array is refused.  This file is collected last on purpose: if it fails, a
+run that stops at the first failure has already run every other test."""
 import numpy as np
 import pytest
 
@@ -42,6 +43,14 @@ def rel(a, b):
     return float(np.abs(a - b).max() / np.abs(b).max())
 
 
+def test_noalloc_setup_call_with_no_lines(gpu_available):
+    import torch
+    x = torch.zeros((1, 32), dtype=torch.float64, device="cuda")
+    rc = _lib.lib().css_compact_lines_noalloc(x.data_ptr(), x.data_ptr(), 32, 0, 1, 1, 1, 1, None, None, None,
+                                              None, 1.0, 1.0, None)
+    assert rc == 0
+
+
 def test_noalloc_matches_allocating_entry_point_twice(gpu_available):
     rng = np.random.default_rng(42)
     cases = [  # (n, nlines, order, lphys, rphys, bdry)
@@ -57,6 +66,25 @@ def test_noalloc_matches_allocating_entry_point_twice(gpu_available):
         want = compact_lines(x, order, lphys, rphys, bdry, bl, bh, hl, hh, dnum=dnum, scale=scale)
         got = _noalloc(x, order, lphys, rphys, bdry, bl, bh, hl, hh, dnum, scale)
         assert rel(got, want) < 1e-13, (n, order, rel(got, want))
+        assert np.array_equal(got, want), (n, order, rel(got, want))
+
+
+@pytest.mark.parametrize("order", [1, 2])
+def test_noalloc_every_closure_bit_equal(order, gpu_available):
+    rng = np.random.default_rng(7 + order)
+    for lphys in (0, 1):
+        for rphys in (0, 1):
+            for bdry in range(5):
+                n = 20 + 2 * bdry + 6 * lphys + 3 * rphys  # a different size every call
+                nl = 37 + 11 * bdry
+                x = np.cos(np.linspace(0, 2.5, n))[None, :] + 0.05 * rng.standard_normal((nl, n))
+                bl, bh = rng.standard_normal(nl), rng.standard_normal(nl)
+                hl, hh = rng.standard_normal((nl, 4)), rng.standard_normal((nl, 4))
+                dnum = float(n - 1)
+                scale = dnum ** order
+                want = compact_lines(x, order, lphys, rphys, bdry, bl, bh, hl, hh, dnum=dnum, scale=scale)
+                got = _noalloc(x, order, lphys, rphys, bdry, bl, bh, hl, hh, dnum, scale)
+                assert np.array_equal(got, want), (lphys, rphys, bdry, rel(got, want))
 
 
 def test_noalloc_rejects_requests_beyond_its_scratch(gpu_available):
