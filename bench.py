@@ -323,6 +323,8 @@ def run_ours(args):
     if args.precision == "mixed":
         p.precision = 1
     sim = Simulation(p, prof)
+    if args.stage == "four":
+        sim.set_fused(False)
     stream = torch.cuda.current_stream(dev)
     sim.set_stream(stream.cuda_stream)
     sim.upload(v0)
@@ -405,6 +407,7 @@ def run_ours(args):
         "dtype": "f64" if args.precision == "fp64" else "f32-storage/f64", "data": "synthetic",
         "config": {"workload": args.workload, "grid": [p.nr, p.nth, p.nphi], "decomposition": [p.nnr, p.nnt, p.nnp],
                    "precision": args.precision, "tile_lines_r_theta_phi": list(tiles),
+                   "stage": "two-pass (k_thph + k_rstage)" if sim.fused else "four-kernel",
                    "fields": nv, "dt": dt, "l2": "state (%.0f MB per buffer) larger than L2, no flush" % (state_bytes / 1e6),
                    "parallelism": "replicas" if world > 1 else "single-gpu"},
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": state_bytes, "d2h_bytes_per_step": state_bytes,
@@ -674,6 +677,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--stage", default="auto", choices=["auto", "four"],
+                    help="four: the four-kernel RK4 stage even where the two-pass stage applies")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"],
                     help="mixed: FP32 stage states (rho, s as perturbations), FP64 arithmetic and accumulator")
     args = ap.parse_args()

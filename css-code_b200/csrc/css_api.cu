@@ -767,7 +767,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   c->fused_ok = c->mt[0] == 32 && c->mt[1] == 32 && c->mt[2] == 32 && p.precision == 0 &&
                 (p.time_stepper == 4 || p.time_stepper == 0) && !p.laplacian && !p.do_radheat && !p.top_inout &&
                 !p.bot_inout && !p.bottom_specified;
-  c->fused = 0;
+  c->fused = c->fused_ok;
   *out = c;
   return CSS_OK;
 }

@@ -51,30 +51,28 @@ struct ThphCfg {
   static constexpr size_t SMEM = 8 * ((size_t)NF * FA_FIELD + (size_t)NO * FA_OUT);
 };
 
-// theta line of field F at row p: j = -3..36 -> column j+3
-struct ThLine {
-  const double *F;
-  __device__ __forceinline__ double operator()(int j) const { return F[j + 3]; }
+// index maps of the lines (css_lines.cuh: the solver reads xb[xi(j)] and
+// writes ob[oi(j)])
+// theta line: base = the row start, j = -3..36 -> column j+3
+struct ThIdx {
+  __device__ __forceinline__ int operator()(int j) const { return j + 3; }
 };
-// phi line of field F at theta column t
-struct PhLine {
-  const double *F;
+// phi line at theta column t: base = the field
+struct PhIdx {
   int t;
-  __device__ __forceinline__ double operator()(int j) const {
-    if (j < 1) return F[FA_MAIN + (j + 3) * FM + t];
-    if (j > FM) return F[FA_MAIN + (j - FM + 3) * FM + t];
-    return F[(j - 1) * FA_RW + t + 4];
+  __device__ __forceinline__ int operator()(int j) const {
+    if (j < 1) return FA_MAIN + (j + 3) * FM + t;
+    if (j > FM) return FA_MAIN + (j - FM + 3) * FM + t;
+    return (j - 1) * FA_RW + t + 4;
   }
 };
-struct SwzRow {  // theta line: element (p, j)
-  double *O;
+struct SwzRow {  // theta line p of a derivative tile: element (p, j)
   int p;
-  __device__ __forceinline__ double &operator()(int j) const { return O[p * FM + (j ^ (p & 15))]; }
+  __device__ __forceinline__ int operator()(int j) const { return p * FM + (j ^ (p & 15)); }
 };
-struct SwzCol {  // phi line: element (j, t)
-  double *O;
+struct SwzCol {  // phi line t of a derivative tile: element (j, t)
   int t;
-  __device__ __forceinline__ double &operator()(int j) const { return O[j * FM + (t ^ (j & 15))]; }
+  __device__ __forceinline__ int operator()(int j) const { return j * FM + (t ^ (j & 15)); }
 };
 __device__ __forceinline__ double swz(const double *O, int p, int t) { return O[p * FM + (t ^ (p & 15))]; }
 
@@ -161,11 +159,11 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_thph(CssGeo g, const doubl
       const int slot = (k == nth_t - 1 && !wall) ? C::NO - 1 : k;
       if (order == 2) {
         if (g.slaplacian)
-          line_solve_ua<2, FM>(ThLine{x}, dtype, bdry, lo, hi, tabp(g, 1, bt, 2, bdry), g.tstride,
-                               dnum_d2_theta(g, ir), dn * dn, 0, SwzRow{O + slot * FA_OUT, p});
+          line_solve_ua<2, FM>(x, ThIdx{}, dtype, bdry, lo, hi, tabp(g, 1, bt, 2, bdry), g.tstride,
+                               dnum_d2_theta(g, ir), dn * dn, 0, O + slot * FA_OUT, SwzRow{p});
       } else {
-        line_solve_ua<1, FM>(ThLine{x}, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, dn, dn, 0,
-                             SwzRow{O + slot * FA_OUT, p});
+        line_solve_ua<1, FM>(x, ThIdx{}, dtype, bdry, lo, hi, tabp(g, 1, bt, 1, bdry), g.tstride, dn, dn, 0,
+                             O + slot * FA_OUT, SwzRow{p});
       }
     }
   }
@@ -207,7 +205,6 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_thph(CssGeo g, const doubl
       du = du - w * w1;
       const double t = temp_of(g, rho, s);
       tk[q] = t;
-      tbuf[pl + (size_t)(p0 + p) * nth + it] = t;
       const double invrho = 1.0 / rho;
       const double oorho_t = invrho / t;
       double ds;
@@ -250,6 +247,10 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_thph(CssGeo g, const doubl
       }
       acc[q][0] = drho; acc[q][1] = dw; acc[q][2] = dvv; acc[q][3] = du; acc[q][4] = ds;
     }
+    // global stores after every point's shared-memory reads, so the
+    // compiler need not order those reads behind them
+#pragma unroll
+    for (int q = 0; q < 4; q++) tbuf[pl + (size_t)(p0 + q * 8 + wrp) * nth + it] = tk[q];
   }
   __syncthreads();
 
@@ -263,11 +264,11 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_thph(CssGeo g, const doubl
       const double *x = F + (size_t)f * FA_FIELD;
       if (k == 5) {
         if (g.slaplacian)
-          line_solve_ua<2, FM>(PhLine{x, t}, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 2, 0), g.tstride, dn, dn * dn, 1,
-                               SwzCol{O + k * FA_OUT, t});
+          line_solve_ua<2, FM>(x, PhIdx{t}, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 2, 0), g.tstride, dn, dn * dn, 1,
+                               O + k * FA_OUT, SwzCol{t});
       } else {
-        line_solve_ua<1, FM>(PhLine{x, t}, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, dn, dn, 1,
-                             SwzCol{O + k * FA_OUT, t});
+        line_solve_ua<1, FM>(x, PhIdx{t}, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride, dn, dn, 1,
+                             O + k * FA_OUT, SwzCol{t});
       }
     }
   }
@@ -310,17 +311,13 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_thph(CssGeo g, const doubl
         dvv = dvv - br_ * w1;
         du = du + bp_ * w1;
       }
-      const size_t id = pl + (size_t)(p0 + p) * nth + it;
-      dv[id] = drho;
-      dv[n + id] = dw;
-      dv[2 * n + id] = dvv;
-      dv[3 * n + id] = du;
-      dv[4 * n + id] = ds;
-      if (MAG) {
-        dv[5 * n + id] = acc[q][5];
-        dv[6 * n + id] = acc[q][6];
-        dv[7 * n + id] = acc[q][7];
-      }
+      acc[q][0] = drho; acc[q][1] = dw; acc[q][2] = dvv; acc[q][3] = du; acc[q][4] = ds;
+    }
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      const size_t id = pl + (size_t)(p0 + q * 8 + wrp) * nth + it;
+#pragma unroll
+      for (int f = 0; f < NA; f++) dv[f * n + id] = acc[q][f];
     }
   }
 }
@@ -339,16 +336,6 @@ struct RstageCfg {
 // the theta-wall pass reuses the derivative tiles: rho rows with their theta
 // halo (stride 41) and the d(rho)/dtheta rows (stride 33)
 constexpr int FB_XS = 41, FB_YS = 33;
-
-// a[i] for a run-time i without indexing the register array
-__device__ __forceinline__ double pick5(const double (&a)[5], int i) {
-  double r = a[0];
-  r = i == 1 ? a[1] : r;
-  r = i == 2 ? a[2] : r;
-  r = i == 3 ? a[3] : r;
-  r = i == 4 ? a[4] : r;
-  return r;
-}
 
 // STG: the RK4 stage (1..4), compiled in:
 //   1: vs = (sld ? vs + dv/6 : dv); nx = v0 + dtcur*dv
@@ -375,13 +362,24 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_rstage(CssGeo g, const dou
   const size_t base = (size_t)ip * g.nth + t0;  // (theta t0, phi ip) of plane 0
   const int nr = g.nr;
 
-  // lines the pointwise phase reads (two 128-byte halves per row): the
-  // tendency, T [and B_r]
-  if (tid < 2 * FM) {
-    const size_t id = base + (size_t)(r0 + (tid >> 1)) * ps + (tid & 1) * 16;
-    for (int f = 0; f < 5; f++) prefetch_l2(dv + f * n + id);
-    prefetch_l2(tbuf + id);
-    if (MAG) prefetch_l2(bf + 2 * n + id);
+  // Lines the later phases read, toward L2 now (two 128-byte halves per
+  // row): the tendency, T [and B_r] for the pointwise phase; vars0 and the
+  // accumulator for the stage combination
+  {
+    const int nv = MAG ? 8 : 5;
+    const bool need_s = !(STG == 1 && !g.sldiffusion);
+    const int per = 2 * nv + 1 + (MAG ? 1 : 0) + (need_s ? nv : 0);
+    for (int k = tid; k < 2 * FM * per; k += FNT) {
+      const int row = k / per, f = k - row * per;
+      const size_t id = base + (size_t)(r0 + (row >> 1)) * ps + (row & 1) * 16;
+      const double *src;
+      if (f < nv) src = dv + f * n;
+      else if (f < 2 * nv) src = v0 + (f - nv) * n;
+      else if (f == 2 * nv) src = tbuf;
+      else if (MAG && f == 2 * nv + 1) src = bf + 2 * n;
+      else src = vs + (f - 2 * nv - 1 - (MAG ? 1 : 0)) * n;
+      prefetch_l2(src + id);
+    }
   }
   // ---- stage the slab: 16-byte copies, zero fill outside [0, nr) ----
   {
@@ -423,11 +421,11 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_rstage(CssGeo g, const dou
       }
       const double dn = D.dnum[br];
       if (k == 4)
-        line_solve_ua<2, FM>(StridedIn{x, FM}, dtype, bdry, lo, hi, tabp(g, 0, br, 2, bdry), g.tstride, dn, dn * dn,
-                             0, StridedOut{O + k * FB_OUT + l, FM});
+        line_solve_ua<2, FM>(x, StridedIn{FM}, dtype, bdry, lo, hi, tabp(g, 0, br, 2, bdry), g.tstride, dn, dn * dn,
+                             0, O + k * FB_OUT + l, StridedOut{FM});
       else
-        line_solve_ua<1, FM>(StridedIn{x, FM}, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, dn, dn, 0,
-                             StridedOut{O + k * FB_OUT + l, FM});
+        line_solve_ua<1, FM>(x, StridedIn{FM}, dtype, bdry, lo, hi, tabp(g, 0, br, 1, bdry), g.tstride, dn, dn, 0,
+                             O + k * FB_OUT + l, StridedOut{FM});
     }
   }
   __syncthreads();
@@ -472,8 +470,8 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_rstage(CssGeo g, const dou
     for (int q = 0; q < 4; q++) {
       const int j = q * 8 + wrp;
       const size_t id = base + (size_t)(r0 + j) * ps + lane;
-      in[q][0] = dv[id]; in[q][1] = dv[n + id]; in[q][2] = dv[2 * n + id];
-      in[q][3] = dv[3 * n + id]; in[q][4] = dv[4 * n + id]; in[q][5] = __ldg(tbuf + id);
+      in[q][0] = __ldg(dv + id); in[q][1] = __ldg(dv + n + id); in[q][2] = __ldg(dv + 2 * n + id);
+      in[q][3] = __ldg(dv + 3 * n + id); in[q][4] = __ldg(dv + 4 * n + id); in[q][5] = __ldg(tbuf + id);
       in[q][6] = MAG ? __ldg(bf + 2 * n + id) : 0.0;
     }
 #pragma unroll
@@ -531,8 +529,8 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_rstage(CssGeo g, const dou
       const int bdry = g.ibct[1];
       const double dn = DT.dnum[bt];
       const double lo = lw ? datum[FM + j] : 0.0, hi = hw ? datum[FM + j] : 0.0;
-      line_solve_ua<1, FM>(StridedIn{X + j * FB_XS + 4, 1}, dtype_of(DT, bt), bdry, lo, hi,
-                           tabp(g, 1, bt, 1, bdry), g.tstride, dn, dn, 0, StridedOut{Y + j * FB_YS, 1});
+      line_solve_ua<1, FM>(X + j * FB_XS + 4, StridedIn{1}, dtype_of(DT, bt), bdry, lo, hi,
+                           tabp(g, 1, bt, 1, bdry), g.tstride, dn, dn, 0, Y + j * FB_YS, StridedOut{1});
     }
     __syncthreads();
 #pragma unroll
@@ -555,7 +553,11 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_rstage(CssGeo g, const dou
 #pragma unroll
   for (int q = 0; q < 4; q++)
     if (g.xi_cs < 1.0) d[q][0] = (g.xi_cs * g.xi_cs) * d[q][0];
-#pragma unroll 1
+  // Every value is read once, before the same thread writes that address
+  // (nx is vars0 in stage 4), and no other thread touches it, so the reads
+  // go through the non-coherent path; the compiler may then start the next
+  // field's reads before this field's stores.
+#pragma unroll
   for (int iv = 0; iv < nv; iv++) {
     double dd[4], aa[4], ss[4];
     const bool need_s = !(STG == 1 && !g.sldiffusion);
@@ -563,9 +565,9 @@ __global__ void __launch_bounds__(FNT, MAG ? 1 : 2) k_rstage(CssGeo g, const dou
     for (int q = 0; q < 4; q++) {
       const int j = q * 8 + wrp;
       const size_t qi = (size_t)iv * n + base + (size_t)(r0 + j) * ps + lane;
-      dd[q] = (iv < 5) ? pick5(d[q], iv) : dv[qi];
-      aa[q] = v0[qi];
-      ss[q] = need_s ? vs[qi] : 0.0;
+      dd[q] = (iv < 5) ? d[q][iv < 5 ? iv : 0] : __ldg(dv + qi);
+      aa[q] = __ldg(v0 + qi);
+      ss[q] = need_s ? __ldg(vs + qi) : 0.0;
     }
 #pragma unroll
     for (int q = 0; q < 4; q++) {

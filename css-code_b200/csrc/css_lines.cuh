@@ -40,28 +40,28 @@ struct HaloD1 {
   static constexpr double pb1 = -3.0 * pc;
 };
 
-// Line accessors.  A line is read through x(j), j 1-based (the halo points
-// at j = -3..0 and m+1..m+4), and written through out(j), j 0-based; the
-// strided forms are a pointer and a stride, the fused kernels pass their own
-// (a halo kept apart from the line, or a swizzled output tile).
+// Line addressing.  A line is read as xb[xi(j)], j 1-based (the halo points
+// at j = -3..0 and m+1..m+4), and written as ob[oi(j)], j 0-based.  The
+// base pointers are __restrict__ parameters of the solvers, so the compiler
+// may move the line's loads ahead of the stores of its results; xi and oi
+// only map indices (a stride, or the fused kernels' halo-apart and swizzled
+// tiles).
 struct StridedIn {
-  const double *__restrict__ p;
   int s;
-  __device__ __forceinline__ double operator()(int j) const { return p[(j - 1) * s]; }
+  __device__ __forceinline__ int operator()(int j) const { return (j - 1) * s; }
 };
 struct StridedOut {
-  double *__restrict__ p;
   int s;
-  __device__ __forceinline__ double &operator()(int j) const { return p[j * s]; }
+  __device__ __forceinline__ int operator()(int j) const { return j * s; }
 };
 
-#define CSS_X(j) x(j)
+#define CSS_X(j) xb[xi(j)]
 
 // Right-hand side of the first-derivative system, rows written to d[] (a
 // per-thread scratch that aliases the output buffer).  Returns nothing; the
 // caller runs the sweeps.
 template <class X>
-__device__ __forceinline__ double d1_row_lo1(const X &x, int dtype, int bdry, double bclo,
+__device__ __forceinline__ double d1_row_lo1(const double *__restrict__ xb, const X &xi, int dtype, int bdry, double bclo,
                                              double dnum, double row2) {
   if (dtype == 1 || dtype == 3) {
     return (-HaloD1::c1) * CSS_X(-3) + HaloD1::c2 * CSS_X(-2) + HaloD1::cnst * CSS_X(-1) +
@@ -79,7 +79,7 @@ __device__ __forceinline__ double d1_row_lo1(const X &x, int dtype, int bdry, do
 }
 
 template <class X>
-__device__ __forceinline__ double d1_row_lo2(const X &x, int dtype) {
+__device__ __forceinline__ double d1_row_lo2(const double *__restrict__ xb, const X &xi, int dtype) {
   if (dtype == 1 || dtype == 3)
     return (7.0 / 9.0) * (CSS_X(3) - CSS_X(1)) + (1.0 / 36.0) * (CSS_X(4) - CSS_X(0));
   return (-43.0 / 96.0) * CSS_X(1) + (-5.0 / 6.0) * CSS_X(2) + (9.0 / 8.0) * CSS_X(3) + (1.0 / 6.0) * CSS_X(4) +
@@ -87,7 +87,7 @@ __device__ __forceinline__ double d1_row_lo2(const X &x, int dtype) {
 }
 
 template <class X>
-__device__ __forceinline__ double d1_row_hi1(const X &x, int m, int dtype) {  // row m-1
+__device__ __forceinline__ double d1_row_hi1(const double *__restrict__ xb, const X &xi, int m, int dtype) {  // row m-1
   if (dtype == 2 || dtype == 3)
     return HaloD1::r_c1 * (CSS_X(m) - CSS_X(m - 2)) + HaloD1::r_c2 * (CSS_X(m + 1) - CSS_X(m - 3));
   return (43.0 / 96.0) * CSS_X(m) + (5.0 / 6.0) * CSS_X(m - 1) + (-9.0 / 8.0) * CSS_X(m - 2) +
@@ -95,7 +95,7 @@ __device__ __forceinline__ double d1_row_hi1(const X &x, int m, int dtype) {  //
 }
 
 template <class X>
-__device__ __forceinline__ double d1_row_hi2(const X &x, int m, int dtype, int bdry, double bchi,
+__device__ __forceinline__ double d1_row_hi2(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bchi,
                                              double dnum, double rowm1) {  // row m
   if (dtype == 2 || dtype == 3)
     return HaloD1::r_c1 * CSS_X(m + 1) + HaloD1::r_cnst * CSS_X(m + 2) + HaloD1::r_c4 * CSS_X(m + 3) +
@@ -112,7 +112,7 @@ __device__ __forceinline__ double d1_row_hi2(const X &x, int m, int dtype, int b
 }
 
 template <class X>
-__device__ __forceinline__ double d1_row_int(const X &x, int j) {
+__device__ __forceinline__ double d1_row_int(const double *__restrict__ xb, const X &xi, int j) {
   return (7.0 / 9.0) * (CSS_X(j + 1) - CSS_X(j - 1)) + (1.0 / 36.0) * (CSS_X(j + 2) - CSS_X(j - 2));
 }
 
@@ -122,7 +122,7 @@ struct HaloD2 {
 };
 
 template <class X>
-__device__ __forceinline__ double d2_row_lo1(const X &x, int dtype, int bdry, double bclo, double dnum) {
+__device__ __forceinline__ double d2_row_lo1(const double *__restrict__ xb, const X &xi, int dtype, int bdry, double bclo, double dnum) {
   if (dtype == 1 || dtype == 3) {
     double r = HaloD2::c3 * (2.0 * (CSS_X(-3) + CSS_X(3)) + (-27.0) * (CSS_X(-2) + CSS_X(2)) +
                              270.0 * (CSS_X(-1) + CSS_X(1)) + (-490.0) * CSS_X(0));
@@ -139,14 +139,14 @@ __device__ __forceinline__ double d2_row_lo1(const X &x, int dtype, int bdry, do
 }
 
 template <class X>
-__device__ __forceinline__ double d2_row_lo2(const X &x, int dtype) {
+__device__ __forceinline__ double d2_row_lo2(const double *__restrict__ xb, const X &xi, int dtype) {
   if (dtype == 1 || dtype == 3)
     return HaloD2::c1 * (CSS_X(3) - 2.0 * CSS_X(2) + CSS_X(1)) + HaloD2::c2 * (CSS_X(0) - 2.0 * CSS_X(2) + CSS_X(4));
   return 1.2375 * CSS_X(1) + (-3.0) * CSS_X(2) + 2.325 * CSS_X(3) + (-0.6) * CSS_X(4) + 0.0375 * CSS_X(5);
 }
 
 template <class X>
-__device__ __forceinline__ double d2_row_hi1(const X &x, int m, int dtype) {
+__device__ __forceinline__ double d2_row_hi1(const double *__restrict__ xb, const X &xi, int m, int dtype) {
   if (dtype == 2 || dtype == 3)
     return HaloD2::c1 * (CSS_X(m) - 2.0 * CSS_X(m - 1) + CSS_X(m - 2)) +
            HaloD2::c2 * (CSS_X(m - 3) - 2.0 * CSS_X(m - 1) + CSS_X(m + 1));
@@ -154,7 +154,7 @@ __device__ __forceinline__ double d2_row_hi1(const X &x, int m, int dtype) {
 }
 
 template <class X>
-__device__ __forceinline__ double d2_row_hi2(const X &x, int m, int dtype, int bdry, double bchi,
+__device__ __forceinline__ double d2_row_hi2(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bchi,
                                              double dnum) {
   if (dtype == 2 || dtype == 3) {
     double r = HaloD2::c1 * (CSS_X(m + 1) - 2.0 * CSS_X(m) + CSS_X(m - 1)) +
@@ -172,7 +172,7 @@ __device__ __forceinline__ double d2_row_hi2(const X &x, int m, int dtype, int b
 }
 
 template <class X>
-__device__ __forceinline__ double d2_row_int(const X &x, int j) {
+__device__ __forceinline__ double d2_row_int(const double *__restrict__ xb, const X &xi, int j) {
   return HaloD2::c1 * (CSS_X(j + 1) - 2.0 * CSS_X(j) + CSS_X(j - 1)) +
          HaloD2::c2 * (CSS_X(j - 2) - 2.0 * CSS_X(j) + CSS_X(j + 2));
 }
@@ -180,56 +180,56 @@ __device__ __forceinline__ double d2_row_int(const X &x, int j) {
 // One line: ORDER 1 or 2.  G points at the 1-based tables of this block and
 // bdry: g1 = G, g2 = G + ts, g3 = G + 2 ts.  phi = 1 selects the Dbydp /
 // D2bydp2 sweep form (every row after the first as g2*(d + a*t)).
-// out(j-1) receives scale * solution of row j; the forward values pass
+// ob[oi(j-1)] receives scale * solution of row j; the forward values pass
 // through out on the way.
 template <int ORDER, class X, class O>
-__device__ __forceinline__ void line_solve_a(const X &x, int m, int dtype, int bdry, double bclo, double bchi,
+__device__ __forceinline__ void line_solve_a(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bclo, double bchi,
                                              const double *__restrict__ G, int ts, double dnum, double scale,
-                                             int phi, const O &out) {
+                                             int phi, double *__restrict__ ob, const O &oi) {
   const double *g1 = G, *g2 = G + ts, *g3 = G + 2 * ts;
   const double a1 = (ORDER == 1) ? -1.0 / 3.0 : -2.0 / 11.0;
   double r1, r2, rm1, rm;
   if (ORDER == 1) {
-    r2 = d1_row_lo2(x, dtype);
-    r1 = d1_row_lo1(x, dtype, bdry, bclo, dnum, r2);
-    rm1 = d1_row_hi1(x, m, dtype);
-    rm = d1_row_hi2(x, m, dtype, bdry, bchi, dnum, rm1);
+    r2 = d1_row_lo2(xb, xi, dtype);
+    r1 = d1_row_lo1(xb, xi, dtype, bdry, bclo, dnum, r2);
+    rm1 = d1_row_hi1(xb, xi, m, dtype);
+    rm = d1_row_hi2(xb, xi, m, dtype, bdry, bchi, dnum, rm1);
   } else {
-    r1 = d2_row_lo1(x, dtype, bdry, bclo, dnum);
-    r2 = d2_row_lo2(x, dtype);
-    rm1 = d2_row_hi1(x, m, dtype);
-    rm = d2_row_hi2(x, m, dtype, bdry, bchi, dnum);
+    r1 = d2_row_lo1(xb, xi, dtype, bdry, bclo, dnum);
+    r2 = d2_row_lo2(xb, xi, dtype);
+    rm1 = d2_row_hi1(xb, xi, m, dtype);
+    rm = d2_row_hi2(xb, xi, m, dtype, bdry, bchi, dnum);
   }
   double t = g2[1] * r1;
-  out(0) = t;
+  ob[oi(0)] = t;
   if (phi) {
     t = g2[2] * (r2 + a1 * t);
-    out(1) = t;
+    ob[oi(1)] = t;
     for (int j = 3; j <= m - 2; j++) {
-      double d = (ORDER == 1) ? d1_row_int(x, j) : d2_row_int(x, j);
+      double d = (ORDER == 1) ? d1_row_int(xb, xi, j) : d2_row_int(xb, xi, j);
       t = g2[j] * (d + a1 * t);
-      out(j - 1) = t;
+      ob[oi(j - 1)] = t;
     }
     t = g2[m - 1] * (rm1 + a1 * t);
-    out(m - 2) = t;
+    ob[oi(m - 2)] = t;
     t = g2[m] * (rm + a1 * t);
   } else {
     t = g2[2] * r2 + g3[2] * t;
-    out(1) = t;
+    ob[oi(1)] = t;
     for (int j = 3; j <= m - 2; j++) {
-      double d = (ORDER == 1) ? d1_row_int(x, j) : d2_row_int(x, j);
+      double d = (ORDER == 1) ? d1_row_int(xb, xi, j) : d2_row_int(xb, xi, j);
       t = g2[j] * (d + a1 * t);
-      out(j - 1) = t;
+      ob[oi(j - 1)] = t;
     }
     t = g2[m - 1] * rm1 + g3[m - 1] * t;
-    out(m - 2) = t;
+    ob[oi(m - 2)] = t;
     t = g2[m] * rm + g3[m] * t;
   }
   double sol = t;
-  out(m - 1) = scale * sol;
+  ob[oi(m - 1)] = scale * sol;
   for (int j = m - 1; j >= 1; j--) {
-    sol = out(j - 1) + g1[j + 1] * sol;
-    out(j - 1) = scale * sol;
+    sol = ob[oi(j - 1)] + g1[j + 1] * sol;
+    ob[oi(j - 1)] = scale * sol;
   }
 }
 
@@ -237,49 +237,49 @@ __device__ __forceinline__ void line_solve_a(const X &x, int m, int dtype, int b
 // are fully unrolled (the forward values go through the output buffer, so
 // register use stays low); identical arithmetic to line_solve_a.
 template <int ORDER, int M, class X, class O>
-__device__ __forceinline__ void line_solve_ua(const X &x, int dtype, int bdry, double bclo, double bchi,
+__device__ __forceinline__ void line_solve_ua(const double *__restrict__ xb, const X &xi, int dtype, int bdry, double bclo, double bchi,
                                               const double *__restrict__ G, int ts, double dnum, double scale,
-                                              int phi, const O &out) {
+                                              int phi, double *__restrict__ ob, const O &oi) {
   const double *g1 = G, *g2 = G + ts, *g3 = G + 2 * ts;
   const double a1 = (ORDER == 1) ? -1.0 / 3.0 : -2.0 / 11.0;
   double r1, r2, rm1, rm;
   if (ORDER == 1) {
-    r2 = d1_row_lo2(x, dtype);
-    r1 = d1_row_lo1(x, dtype, bdry, bclo, dnum, r2);
-    rm1 = d1_row_hi1(x, M, dtype);
-    rm = d1_row_hi2(x, M, dtype, bdry, bchi, dnum, rm1);
+    r2 = d1_row_lo2(xb, xi, dtype);
+    r1 = d1_row_lo1(xb, xi, dtype, bdry, bclo, dnum, r2);
+    rm1 = d1_row_hi1(xb, xi, M, dtype);
+    rm = d1_row_hi2(xb, xi, M, dtype, bdry, bchi, dnum, rm1);
   } else {
-    r1 = d2_row_lo1(x, dtype, bdry, bclo, dnum);
-    r2 = d2_row_lo2(x, dtype);
-    rm1 = d2_row_hi1(x, M, dtype);
-    rm = d2_row_hi2(x, M, dtype, bdry, bchi, dnum);
+    r1 = d2_row_lo1(xb, xi, dtype, bdry, bclo, dnum);
+    r2 = d2_row_lo2(xb, xi, dtype);
+    rm1 = d2_row_hi1(xb, xi, M, dtype);
+    rm = d2_row_hi2(xb, xi, M, dtype, bdry, bchi, dnum);
   }
   double t = g2[1] * r1;
-  out(0) = t;
+  ob[oi(0)] = t;
   if (phi) t = g2[2] * (r2 + a1 * t);
   else t = g2[2] * r2 + g3[2] * t;
-  out(1) = t;
+  ob[oi(1)] = t;
 #pragma unroll
   for (int j = 3; j <= M - 2; j++) {
-    double d = (ORDER == 1) ? d1_row_int(x, j) : d2_row_int(x, j);
+    double d = (ORDER == 1) ? d1_row_int(xb, xi, j) : d2_row_int(xb, xi, j);
     t = g2[j] * (d + a1 * t);
-    out(j - 1) = t;
+    ob[oi(j - 1)] = t;
   }
   if (phi) {
     t = g2[M - 1] * (rm1 + a1 * t);
-    out(M - 2) = t;
+    ob[oi(M - 2)] = t;
     t = g2[M] * (rm + a1 * t);
   } else {
     t = g2[M - 1] * rm1 + g3[M - 1] * t;
-    out(M - 2) = t;
+    ob[oi(M - 2)] = t;
     t = g2[M] * rm + g3[M] * t;
   }
   double sol = t;
-  out(M - 1) = scale * sol;
+  ob[oi(M - 1)] = scale * sol;
 #pragma unroll
   for (int j = M - 1; j >= 1; j--) {
-    sol = out(j - 1) + g1[j + 1] * sol;
-    out(j - 1) = scale * sol;
+    sol = ob[oi(j - 1)] + g1[j + 1] * sol;
+    ob[oi(j - 1)] = scale * sol;
   }
 }
 
@@ -289,14 +289,14 @@ __device__ __forceinline__ void line_solve(const double *__restrict__ x, int sx,
                                            double bclo, double bchi, const double *__restrict__ G, int ts,
                                            double dnum, double scale, int phi, double *__restrict__ out,
                                            int so) {
-  line_solve_a<ORDER>(StridedIn{x, sx}, m, dtype, bdry, bclo, bchi, G, ts, dnum, scale, phi, StridedOut{out, so});
+  line_solve_a<ORDER>(x, StridedIn{sx}, m, dtype, bdry, bclo, bchi, G, ts, dnum, scale, phi, out, StridedOut{so});
 }
 
 template <int ORDER, int M>
 __device__ __forceinline__ void line_solve_u(const double *__restrict__ x, int sx, int dtype, int bdry, double bclo,
                                              double bchi, const double *__restrict__ G, int ts, double dnum,
                                              double scale, int phi, double *__restrict__ out, int so) {
-  line_solve_ua<ORDER, M>(StridedIn{x, sx}, dtype, bdry, bclo, bchi, G, ts, dnum, scale, phi, StridedOut{out, so});
+  line_solve_ua<ORDER, M>(x, StridedIn{sx}, dtype, bdry, bclo, bchi, G, ts, dnum, scale, phi, out, StridedOut{so});
 }
 
 // dispatch: compile-time block length when the direction's blocks all have

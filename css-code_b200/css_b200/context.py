@@ -102,11 +102,12 @@ class Simulation:
     def kernel_stats(self):
         """{kernel name: (total ms, launches)} since profile(True)."""
         out = {}
-        for k in range(11):
+        for k in range(64):
             nm = ctypes.c_char_p()
             ms = ctypes.c_double()
             cnt = ctypes.c_longlong()
-            check(_lib.lib().css_kernel_stats(self.h, k, ctypes.byref(nm), ctypes.byref(ms), ctypes.byref(cnt)))
+            if _lib.lib().css_kernel_stats(self.h, k, ctypes.byref(nm), ctypes.byref(ms), ctypes.byref(cnt)):
+                break  # past the last kernel kind
             if cnt.value:
                 out[nm.value.decode()] = (ms.value, cnt.value)
         return out
