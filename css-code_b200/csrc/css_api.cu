@@ -65,6 +65,7 @@ struct css_ctx {
   double *vcc;                      // SLD speed^2
   double *cda;                      // curl of the A-tendency (MHD ohmic heating)
   double *tbuf;                     // temperature of the current stage input
+  double *rtw = nullptr;            // two-pass stage: zero-datum d(rho)/dtheta on the theta-wall blocks
   double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
   double *lapface = nullptr;        // explicit viscosity: face data, 6 x max face size
   double *radbuf = nullptr;         // radiative diffusion: d ln(rho)/dr, ds/dr, 8 derivative fields
@@ -251,7 +252,7 @@ extern "C" void css_destroy(css_ctx *c) {
   if (!c) return;
   cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo); cudaFree(c->resp);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
-  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf);
+  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf); cudaFree(c->rtw);
   cudaFree(c->lapbuf); cudaFree(c->lapface); cudaFree(c->radbuf); cudaFree(c->radface);
   cudaFree(c->io); cudaFree(c->io_part); cudaFree(c->rain); cudaFree(c->ash_slices); cudaFree(c->ashv);
   cudaFree(c->squalls);
@@ -487,14 +488,17 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
       }
     }
   }
-  // unit responses of the first-derivative system of rho (bdry ibcr(1)) to
-  // its face datum on the radial blocks with a physical face: resp = A^-1 e_1
-  // (bottom) / A^-1 e_m (top), by the same sweeps the kernels run
-  std::vector<double> RESP((size_t)2 * g.d[0].nb * ts, 0.0);
-  {
-    int bdry = 4;  // lbcr_rho (Read_Input, mhdsph_mpi.f90:1362)
-    for (int b = 0; b < g.d[0].nb; b++) {
-      CssDir &D = g.d[0];
+  // unit responses of the first-derivative system of rho to its face datum
+  // on the blocks with a physical face: resp = A^-1 e_1 (low face) / A^-1
+  // e_m (high face), by the same sweeps the kernels run.  Radial blocks
+  // (bdry ibcr(1)) first, then theta blocks (bdry ibct(1), for the two-pass
+  // stage's Density_Terms_Theta on the theta walls).
+  std::vector<double> RESP((size_t)2 * (g.d[0].nb + g.d[1].nb) * ts, 0.0);
+  for (int dir = 0; dir < 2; dir++) {
+    const int bdry = 4;  // lbcr_rho, lbct_rho (Read_Input, mhdsph_mpi.f90:1362)
+    const CssDir &D = g.d[dir];
+    const size_t off0 = dir == 0 ? 0 : (size_t)2 * g.d[0].nb * ts;
+    for (int b = 0; b < D.nb; b++) {
       int m = D.size[b];
       const double *g1 = &T[D.tab1[b] + (size_t)bdry * 3 * ts], *g2 = g1 + ts, *g3 = g2 + ts;
       for (int side = 0; side < 2; side++) {
@@ -510,7 +514,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
         t[m] = g2[m] * d[m] + g3[m] * t[m - 1];
         x[m] = t[m];
         for (int j = m - 1; j >= 1; j--) x[j] = t[j] + g1[j + 1] * x[j + 1];
-        double *dst = &RESP[(size_t)(2 * b + side) * ts];
+        double *dst = &RESP[off0 + (size_t)(2 * b + side) * ts];
         for (int j = 1; j <= m; j++) dst[j] = x[j];
       }
     }
@@ -722,7 +726,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   cudaMemcpy(c->rblk, rblk.data(), nr * sizeof(int), cudaMemcpyHostToDevice);
   cudaMemset(c->flag, 0, sizeof(int));
   cudaMemset(c->vs, 0, sb);
-  g.tab = c->tab; g.rblk = c->rblk; g.resp_r = c->resp;
+  g.tab = c->tab; g.rblk = c->rblk; g.resp_r = c->resp; g.resp_t = c->resp + (size_t)2 * g.d[0].nb * ts;
   g.r_ind = c->prof; g.r_inv = c->prof + nr; g.dr_ind = c->prof + 2 * nr; g.dxdr = c->prof + 3 * nr;
   g.d2xdr2 = c->prof + 4 * nr; g.rhor = c->prof + 5 * nr; g.sr = c->prof + 6 * nr; g.grav = c->prof + 7 * nr;
   g.ks = c->prof + 8 * nr; g.dlnks = c->prof + 9 * nr; g.eps = c->prof + 10 * nr; g.dspeed = c->prof + 11 * nr;
@@ -767,6 +771,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
   c->fused_ok = c->mt[0] == 32 && c->mt[1] == 32 && c->mt[2] == 32 && p.precision == 0 &&
                 (p.time_stepper == 4 || p.time_stepper == 0) && !p.laplacian && !p.do_radheat && !p.top_inout &&
                 !p.bot_inout && !p.bottom_specified;
+  if (c->fused_ok) ALLOC(c->rtw, (size_t)nr * nphi * 2 * 32 * sizeof(double));
   c->fused = c->fused_ok;
   *out = c;
   return CSS_OK;
@@ -1114,19 +1119,20 @@ static int launch_stage_fused(css_ctx *c, const double *cur, double *nx, int sta
   const int mag = g.magnetic;
   if (mag)
     if (int rc = launch_curl(c, cur + 5 * c->ncell, c->bf, 1)) return rc;
-  const dim3 ga(g.d[1].nb * g.d[2].nb, g.nr);
+  // persistent kernels: one CTA per SM
+  const dim3 ga(c->nsm);
   prof_begin(c, KI_THPH);
-  if (mag) k_thph<1><<<ga, FNT, ThphCfg<1>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf);
-  else k_thph<0><<<ga, FNT, ThphCfg<0>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf);
+  if (mag) k_thph<1><<<ga, FNT, ThphCfg<1>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf, c->rtw);
+  else k_thph<0><<<ga, FNT, ThphCfg<0>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf, c->rtw);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   if (with_sld)
     if (int rc = launch_sld(c, cur, cur + 5 * c->ncell, c->vs, c->tbuf)) return rc;
-  const dim3 gb(g.d[0].nb * g.d[1].nb, g.nphi);
+  const dim3 gb(g.d[0].nb * g.d[1].nb * g.nphi);  // one tile per CTA
   prof_begin(c, KI_RSTAGE);
 #define CSS_RSTAGE(M, S)                                                                                      \
-  k_rstage<M, S><<<gb, FNT, RstageCfg<M>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->v0, c->vs, nx, c->tbuf, \
-                                                             dtcur, c->flag)
+  k_rstage<M, S><<<gb, FBNT, RstageCfg<M>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->v0, c->vs, nx, c->tbuf, \
+                                                              c->rtw, dtcur, c->flag)
   switch (stage + (mag ? 10 : 0)) {
     case 1: CSS_RSTAGE(0, 1); break;
     case 2: CSS_RSTAGE(0, 2); break;

@@ -28,6 +28,7 @@ struct CssGeo {
   const double *tab;        // [.. bdry][g1|g2|g3][tstride]
   const int *rblk;          // radial block index of each global ir
   const double *resp_r;     // [r block][lo|hi][tstride]: unit response of d/dr to the face datum of rho
+  const double *resp_t;     // [theta block][lo|hi][tstride]: the same for d/dtheta of rho (ibct(1))
   // radial profiles (length nr)
   const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
   const double *mur, *dlnmu;  // viscosity and its log-derivative (explicit-viscosity path)

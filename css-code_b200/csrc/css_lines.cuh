@@ -283,6 +283,55 @@ __device__ __forceinline__ void line_solve_ua(const double *__restrict__ xb, con
   }
 }
 
+// Same arithmetic as line_solve_ua with the forward values held in
+// registers instead of the output buffer: the forward sweep then only
+// loads and the backward sweep only stores, so nothing orders a load
+// behind a store.  The tables are read through the read-only path (G must
+// be global memory).
+template <int ORDER, int M, class X, class O>
+__device__ __forceinline__ void line_solve_r(const double *__restrict__ xb, const X &xi, int dtype, int bdry,
+                                             double bclo, double bchi, const double *__restrict__ G, int ts,
+                                             double dnum, double scale, int phi, double *__restrict__ ob,
+                                             const O &oi) {
+  const double *g1 = G, *g2 = G + ts, *g3 = G + 2 * ts;
+  const double a1 = (ORDER == 1) ? -1.0 / 3.0 : -2.0 / 11.0;
+  double r1, r2, rm1, rm;
+  if (ORDER == 1) {
+    r2 = d1_row_lo2(xb, xi, dtype);
+    r1 = d1_row_lo1(xb, xi, dtype, bdry, bclo, dnum, r2);
+    rm1 = d1_row_hi1(xb, xi, M, dtype);
+    rm = d1_row_hi2(xb, xi, M, dtype, bdry, bchi, dnum, rm1);
+  } else {
+    r1 = d2_row_lo1(xb, xi, dtype, bdry, bclo, dnum);
+    r2 = d2_row_lo2(xb, xi, dtype);
+    rm1 = d2_row_hi1(xb, xi, M, dtype);
+    rm = d2_row_hi2(xb, xi, M, dtype, bdry, bchi, dnum);
+  }
+  double t[M];
+  t[0] = __ldg(g2 + 1) * r1;
+  if (phi) t[1] = __ldg(g2 + 2) * (r2 + a1 * t[0]);
+  else t[1] = __ldg(g2 + 2) * r2 + __ldg(g3 + 2) * t[0];
+#pragma unroll
+  for (int j = 3; j <= M - 2; j++) {
+    const double d = (ORDER == 1) ? d1_row_int(xb, xi, j) : d2_row_int(xb, xi, j);
+    t[j - 1] = __ldg(g2 + j) * (d + a1 * t[j - 2]);
+  }
+  if (phi) {
+    t[M - 2] = __ldg(g2 + M - 1) * (rm1 + a1 * t[M - 3]);
+    t[M - 1] = __ldg(g2 + M) * (rm + a1 * t[M - 2]);
+  } else {
+    t[M - 2] = __ldg(g2 + M - 1) * rm1 + __ldg(g3 + M - 1) * t[M - 3];
+    t[M - 1] = __ldg(g2 + M) * rm + __ldg(g3 + M) * t[M - 2];
+  }
+  double sol = t[M - 1];
+  ob[oi(M - 1)] = scale * sol;
+#pragma unroll
+  for (int j = M - 1; j >= 1; j--) {
+    sol = t[j - 1] + __ldg(g1 + j + 1) * sol;
+    ob[oi(j - 1)] = scale * sol;
+  }
+}
+
 // pointer-and-stride forms: x[(j-1)*sx], out[(j-1)*so]
 template <int ORDER>
 __device__ __forceinline__ void line_solve(const double *__restrict__ x, int sx, int m, int dtype, int bdry,
