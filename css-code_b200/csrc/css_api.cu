@@ -1131,7 +1131,7 @@ static int launch_stage_fused(css_ctx *c, const double *cur, double *nx, int sta
   const dim3 gb(g.d[0].nb * g.d[1].nb * g.nphi);  // one tile per CTA
   prof_begin(c, KI_RSTAGE);
 #define CSS_RSTAGE(M, S)                                                                                      \
-  k_rstage<M, S><<<gb, FBNT, RstageCfg<M>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->v0, c->vs, nx, c->tbuf, \
+  k_rstage<M, S><<<gb, RstageCfg<M>::NT, RstageCfg<M>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->v0, c->vs, nx, c->tbuf, \
                                                               c->rtw, dtcur, c->flag)
   switch (stage + (mag ? 10 : 0)) {
     case 1: CSS_RSTAGE(0, 1); break;

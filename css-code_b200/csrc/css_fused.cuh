@@ -60,9 +60,11 @@ struct ThphCfg {
   // at once; MHD holds one direction's eight at a time
   static constexpr int NO = MAG ? 8 : 12;
   static constexpr int PHI0 = MAG ? 0 : 6;   // first phi tile
-  static constexpr int TW0 = MAG ? 8 : 12;   // first warp of the pointwise-quantity group
-  // + T, 1/rho and 1/(rho T) of the plane's points
-  static constexpr size_t SMEM = 8 * ((size_t)NF * FA_FIELD + (size_t)NO * FA_OUT + 3 * (size_t)FA_OUT);
+  // hydro stages the next tile's plane into a second buffer while it
+  // computes the current one; MHD (eight fields) has room for one plane and
+  // brings the next one toward L2 instead
+  static constexpr int NBUF = MAG ? 1 : 2;
+  static constexpr size_t SMEM = 8 * ((size_t)NBUF * NF * FA_FIELD + (size_t)NO * FA_OUT);
 };
 
 // index maps of the lines (css_lines.cuh: the solver reads xb[xi(j)] and
@@ -214,25 +216,6 @@ __device__ __forceinline__ void thph_phi_solve(const CssGeo &g, const double *F,
   }
 }
 
-// T, 1/rho and 1/(rho T) of the plane's points into Q (three 32x32 tiles,
-// element (p, t) at p*32 + t), T also to tbuf; thread i of n takes the
-// points i, i + n, ...
-__device__ __forceinline__ void thph_point_quantities(const CssGeo &g, const double *F, double *Q,
-                                                      double *__restrict__ tbuf, const ThphTile &T, int i, int n) {
-  const size_t pl = plane(g, T.ir);
-  for (int k = i; k < FM * FM; k += n) {
-    const int p = k >> 5, t = k & 31;
-    const int ic = p * FA_RW + t + 4;
-    const double rho = F[ic], s = F[4 * FA_FIELD + ic];
-    const double tt = temp_of(g, rho, s);
-    const double invrho = 1.0 / rho;
-    Q[k] = tt;
-    Q[FA_OUT + k] = invrho;
-    Q[2 * FA_OUT + k] = invrho / tt;
-    tbuf[pl + (size_t)(T.p0 + p) * g.nth + T.t0 + t] = tt;
-  }
-}
-
 // d(rho)/dtheta with a zero wall datum on a theta-wall block (bdry ibct(1)),
 // line p, into rtw (k_rstage adds the datum times the unit response)
 __device__ __forceinline__ void thph_wall_rho(const CssGeo &g, const double *F, const ThphTile &T, int p,
@@ -252,36 +235,62 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
   using C = ThphCfg<MAG>;
   constexpr int NA = MAG ? 8 : 5;
   extern __shared__ __align__(16) double sm[];
-  double *F = sm;                               // NF fields
-  double *O = F + (size_t)C::NF * FA_FIELD;     // NO derivative tiles
-  double *Q = O + (size_t)C::NO * FA_OUT;       // T, 1/rho, 1/(rho T)
+  double *O = sm + (size_t)C::NBUF * C::NF * FA_FIELD;  // NO derivative tiles
   const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
   const size_t n = (size_t)g.ncell;
   const double *src[8];
   src[0] = cur; src[1] = cur + n; src[2] = cur + 2 * n; src[3] = cur + 3 * n; src[4] = cur + 4 * n;
   if (MAG) { src[5] = bf; src[6] = bf + n; src[7] = bf + 2 * n; }
   const int ntile = g.nr * g.d[1].nb * g.d[2].nb;
-  for (int q = blockIdx.x; q < ntile; q += gridDim.x) {
+  if (C::NBUF == 2 && (int)blockIdx.x < ntile) thph_stage<C::NF>(g, src, thph_tile(g, blockIdx.x), sm);
+  for (int q = blockIdx.x, i = 0; q < ntile; q += gridDim.x, i++) {
     const ThphTile T = thph_tile(g, q);
-    if (q + (int)gridDim.x < ntile) thph_prefetch<C::NF>(g, src, thph_tile(g, q + gridDim.x));
-    thph_stage<C::NF>(g, src, T, F);
-    cp_async_wait<0>();
+    double *F = sm + (size_t)(C::NBUF == 2 ? (i & 1) : 0) * C::NF * FA_FIELD;
+    const bool more = q + (int)gridDim.x < ntile;
+    if (C::NBUF == 2) {
+      // the next plane into the other buffer (its last readers passed the
+      // barrier at the end of the previous tile), then wait for this one
+      if (more) {
+        thph_stage<C::NF>(g, src, thph_tile(g, q + gridDim.x), sm + (size_t)((i + 1) & 1) * C::NF * FA_FIELD);
+        cp_async_wait<1>();
+      } else {
+        cp_async_wait<0>();
+      }
+    } else {
+      if (more) thph_prefetch<C::NF>(g, src, thph_tile(g, q + gridDim.x));
+      thph_stage<C::NF>(g, src, T, F);
+      cp_async_wait<0>();
+    }
     __syncthreads();
     const CssDir &DT = g.d[1];
     const bool wall = DT.lphys[T.bt] || DT.rphys[T.bt];
     const int ir = T.ir, it = T.t0 + lane;
-    // ---- solves [theta, and phi for hydro] | pointwise quantities ----
-    if (wrp < C::TW0) {
+    // ---- T, 1/rho and 1/(rho T) of this thread's two points (rows wrp,
+    // wrp + 16, theta t0 + lane), T also to tbuf ----
+    double tq[2], rq[2], rtq[2];
+    {
+      const size_t pl = plane(g, ir);
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        const int ic = (wrp + 16 * h) * FA_RW + lane + 4;
+        const double rho = F[ic], s = F[4 * FA_FIELD + ic];
+        tq[h] = temp_of(g, rho, s);
+        rq[h] = 1.0 / rho;
+        rtq[h] = rq[h] / tq[h];
+      }
+#pragma unroll
+      for (int h = 0; h < 2; h++) tbuf[pl + (size_t)(T.p0 + wrp + 16 * h) * g.nth + it] = tq[h];
+    }
+    // ---- solves: theta (warps 0-5 hydro, 0-7 MHD), phi (warps 6-11 hydro) ----
+    {
       const int nth_t = (MAG ? 7 : 5) + (wall ? 0 : 1);
       const int nthw = MAG ? 8 : 6;  // theta warps; the last one solves d(rho)/dtheta
       if (wrp < nthw) {
         if (wrp < nth_t) thph_theta_solve<MAG>(g, F, O, T, wrp, lane);
         else thph_wall_rho(g, F, T, lane, rtw);
-      } else {
+      } else if (!MAG && wrp < 12) {
         thph_phi_solve(g, F, O, T, wrp - 6, C::PHI0, lane);
       }
-    } else {
-      thph_point_quantities(g, F, Q, tbuf, T, tid - 32 * C::TW0, FNT - 32 * C::TW0);
     }
     __syncthreads();
     // ---- theta pointwise (Source_Theta_Terms, Lorentz, induction, and
@@ -296,11 +305,9 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int p = wrp + 16 * h;
-        const int ic = p * FA_RW + lane + 4, iq = p * FM + lane;
-        const double rho = F[ic], w = F[FA_FIELD + ic], v = F[2 * FA_FIELD + ic], u = F[3 * FA_FIELD + ic],
-                     s = F[4 * FA_FIELD + ic];
-        const double t = Q[iq], invrho = Q[FA_OUT + iq], oorho_t = Q[2 * FA_OUT + iq];
-        (void)s;
+        const int ic = p * FA_RW + lane + 4;
+        const double rho = F[ic], w = F[FA_FIELD + ic], v = F[2 * FA_FIELD + ic], u = F[3 * FA_FIELD + ic];
+        const double t = tq[h], invrho = rq[h], oorho_t = rtq[h];
         double dw = omsq * sn * cs;
         double du = -g.grav[ir] + omsq * sn * sn;
         double drho = -rho * w * ct * ri;
@@ -372,9 +379,9 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int p = wrp + 16 * h;
-        const int ic = p * FA_RW + lane + 4, iq = p * FM + lane;
+        const int ic = p * FA_RW + lane + 4;
         const double rho = F[ic], v = F[2 * FA_FIELD + ic];
-        const double t = Q[iq], oorho = Q[FA_OUT + iq], oorho_t = Q[2 * FA_OUT + iq];
+        const double t = tq[h], oorho = rq[h], oorho_t = rtq[h];
         double drho = acc[h][0], dw = acc[h][1], dvv = acc[h][2], du = acc[h][3], ds = acc[h][4];
         double w1 = swz(OP, p, lane) * oors;
         drho = drho - v * w1;
@@ -421,17 +428,18 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
 // The slab: field f at H + f*FB_FIELD, row rr = 0..39 (r = r0-4+rr), 32
 // theta values per row.  Derivative tiles O + k*FB_OUT, row r - r0.  On a
 // theta-wall block W holds the zero-datum d(rho)/dtheta rows k_thph left in
-// rtw.  One tile per CTA of 256 threads, two CTAs per SM for hydro (one for
-// MHD): the block scheduler keeps the SM's two tiles in different phases,
-// so one's loads overlap the other's solves.
-constexpr int FBNT = 256;
+// rtw.  One tile per CTA: hydro 256 threads, two CTAs per SM (the block
+// scheduler keeps the SM's two tiles in different phases, so one's loads
+// overlap the other's solves); MHD, with room for one CTA per SM, 512.
 constexpr int FB_FIELD = (FM + 8) * FM;
 constexpr int FB_OUT = FM * FM;
 template <int MAG>
 struct RstageCfg {
   static constexpr int NH = MAG ? 7 : 5;  // w v u s rho [bt bp]
   static constexpr int ND = MAG ? 8 : 6;  // dw dv du ds d2s drho0 [dbt dbp]
-  static constexpr int CPS = MAG ? 1 : 2;  // CTAs per SM
+  static constexpr int NT = MAG ? 512 : 256;  // threads per CTA
+  static constexpr int NW = NT / 32;           // warps
+  static constexpr int PPT = FM * FM / NT;     // points per thread
   static constexpr size_t SMEM = 8 * ((size_t)NH * FB_FIELD + (size_t)ND * FB_OUT + FB_OUT + 2 * FM);
 };
 
@@ -455,7 +463,7 @@ __device__ __forceinline__ RstageTile rstage_tile(const CssGeo &g, int q) {
 //   2,3: vs = vs + dv/3;            nx = v0 + dtcur*dv
 //   4: vs + dv/6 accumulated;       nx = v0 + dtcur*(vs + dv/6)  (nx is v0)
 template <int MAG, int STG>
-__global__ void __launch_bounds__(FBNT, MAG ? 1 : 2) k_rstage(CssGeo g, const double *__restrict__ cur,
+__global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssGeo g, const double *__restrict__ cur,
                                                               const double *__restrict__ bf, const double *dv,
                                                               const double *v0, double *vs, double *nx,
                                                               const double *__restrict__ tbuf,
@@ -483,7 +491,7 @@ __global__ void __launch_bounds__(FBNT, MAG ? 1 : 2) k_rstage(CssGeo g, const do
     // accumulator]
     {
       const int ns = 6 + (MAG ? 1 : 0) + nv + (need_s ? nv : 0);
-      for (int k = tid; k < ns * FM * 2; k += FBNT) {
+      for (int k = tid; k < ns * FM * 2; k += C::NT) {
         const int f = k / (FM * 2), rr = (k >> 1) % FM;
         const double *b;
         if (f < 5) b = dv + (size_t)f * n;
@@ -502,7 +510,7 @@ __global__ void __launch_bounds__(FBNT, MAG ? 1 : 2) k_rstage(CssGeo g, const do
       constexpr int PH = (FM + 8) * 16;
       const int nw = (lw || hw) ? FM * 16 : 0;
       const int side = lw ? 0 : 1;
-      for (int k = tid; k < C::NH * PH + nw; k += FBNT) {
+      for (int k = tid; k < C::NH * PH + nw; k += C::NT) {
         if (k < C::NH * PH) {
           const int f = k / PH, qq = k - f * PH;
           const int rr = qq >> 4, c = (qq & 15) * 2;
@@ -585,21 +593,21 @@ __global__ void __launch_bounds__(FBNT, MAG ? 1 : 2) k_rstage(CssGeo g, const do
       __syncthreads();
     }
 
-    // ---- radial pointwise: 4 points per thread (row j = warp + 8 h, t = lane) ----
+    // ---- radial pointwise: PPT points per thread (row j = warp + NW h, t = lane) ----
     const double *resp = g.resp_r + (size_t)(2 * T.br + (phys == 2 ? 1 : 0)) * g.tstride;
-    double d[4][5], tk[4];
+    double d[C::PPT][5], tk[C::PPT];
     {
-      double in[4][7];
+      double in[C::PPT][7];
 #pragma unroll
-      for (int h = 0; h < 4; h++) {
-        const size_t id = base + (size_t)(T.r0 + wrp + 8 * h) * ps + lane;
+      for (int h = 0; h < C::PPT; h++) {
+        const size_t id = base + (size_t)(T.r0 + wrp + C::NW * h) * ps + lane;
         in[h][0] = __ldg(dv + id); in[h][1] = __ldg(dv + n + id); in[h][2] = __ldg(dv + 2 * n + id);
         in[h][3] = __ldg(dv + 3 * n + id); in[h][4] = __ldg(dv + 4 * n + id); in[h][5] = __ldg(tbuf + id);
         in[h][6] = MAG ? __ldg(bf + 2 * n + id) : 0.0;
       }
 #pragma unroll
-      for (int h = 0; h < 4; h++) {
-        const int j = wrp + 8 * h, ir = T.r0 + j;
+      for (int h = 0; h < C::PPT; h++) {
+        const int j = wrp + C::NW * h, ir = T.r0 + j;
         RadIn qq;
         gather(j, lane, qq, in[h][5], in[h][6]);
         double drho = in[h][0], dw = in[h][1], dvv = in[h][2], du = in[h][3], ds = in[h][4];
@@ -628,8 +636,8 @@ __global__ void __launch_bounds__(FBNT, MAG ? 1 : 2) k_rstage(CssGeo g, const do
       const int tw = lw ? 0 : FM - 1;
       if (lane == tw) {
 #pragma unroll
-        for (int h = 0; h < 4; h++) {
-          const int j = wrp + 8 * h;
+        for (int h = 0; h < C::PPT; h++) {
+          const int j = wrp + C::NW * h;
           const double rho = H[4 * FB_FIELD + (size_t)(j + 4) * FM + tw];
           datum[FM + j] = g.r_ind[T.r0 + j] * g.invpconst * d[h][1] * rho / tk[h];
         }
@@ -638,8 +646,8 @@ __global__ void __launch_bounds__(FBNT, MAG ? 1 : 2) k_rstage(CssGeo g, const do
       const double *rt = g.resp_t + (size_t)(2 * T.bt + (lw ? 0 : 1)) * g.tstride;
       const double rl = rt[lane + 1];
 #pragma unroll
-      for (int h = 0; h < 4; h++) {
-        const int j = wrp + 8 * h;
+      for (int h = 0; h < C::PPT; h++) {
+        const int j = wrp + C::NW * h;
         const double w = H[(size_t)(j + 4) * FM + lane], rho = H[4 * FB_FIELD + (size_t)(j + 4) * FM + lane];
         double w1 = g.r_inv[T.r0 + j] * (W[j * FM + lane] + datum[FM + j] * rl);
         d[h][0] = d[h][0] - w * w1;
@@ -656,21 +664,21 @@ __global__ void __launch_bounds__(FBNT, MAG ? 1 : 2) k_rstage(CssGeo g, const do
     const int it = T.t0 + lane;
     const bool twall = (it == 0 || it == g.nth - 1);
 #pragma unroll
-    for (int h = 0; h < 4; h++)
+    for (int h = 0; h < C::PPT; h++)
       if (g.xi_cs < 1.0) d[h][0] = (g.xi_cs * g.xi_cs) * d[h][0];
 #pragma unroll
     for (int iv = 0; iv < nv; iv++) {
-      double dd[4], aa[4], ss[4];
+      double dd[C::PPT], aa[C::PPT], ss[C::PPT];
 #pragma unroll
-      for (int h = 0; h < 4; h++) {
-        const size_t qi = (size_t)iv * n + base + (size_t)(T.r0 + wrp + 8 * h) * ps + lane;
+      for (int h = 0; h < C::PPT; h++) {
+        const size_t qi = (size_t)iv * n + base + (size_t)(T.r0 + wrp + C::NW * h) * ps + lane;
         dd[h] = (iv < 5) ? d[h][iv < 5 ? iv : 0] : __ldg(dv + qi);
         aa[h] = __ldg(v0 + qi);
         ss[h] = need_s ? __ldg(vs + qi) : 0.0;
       }
 #pragma unroll
-      for (int h = 0; h < 4; h++) {
-        const int ir = T.r0 + wrp + 8 * h;
+      for (int h = 0; h < C::PPT; h++) {
+        const int ir = T.r0 + wrp + C::NW * h;
         const size_t qi = (size_t)iv * n + base + (size_t)ir * ps + lane;
         const double dd_ = dd[h], a = aa[h];
         double o;
