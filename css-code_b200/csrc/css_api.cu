@@ -1,7 +1,9 @@
 // css_api.cu -- C ABI of the CSS B200 library (include/css_b200.h): context
 // set-up (virtual decomposition, LU tables, profiles), device buffers, the
 // RK4 step loop and the parity entry points.
+#include <cuda.h>
 #include <cuda_runtime.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 #include <atomic>
@@ -66,6 +68,7 @@ struct css_ctx {
   double *cda;                      // curl of the A-tendency (MHD ohmic heating)
   double *tbuf;                     // temperature of the current stage input
   double *rtw = nullptr;            // two-pass stage: zero-datum d(rho)/dtheta on the theta-wall blocks
+  PlaneMaps pmaps[4];               // two-pass stage: TMA maps of v0, vA, vB and bf
   double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
   double *lapface = nullptr;        // explicit viscosity: face data, 6 x max face size
   double *radbuf = nullptr;         // radiative diffusion: d ln(rho)/dr, ds/dr, 8 derivative fields
@@ -351,6 +354,41 @@ static int setup_kernels() {
       default: KERNEL<0, 0, CSS_STRIP XT><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;     \
     }                                                                                     \
   } while (0)
+
+// TMA maps of the two-pass stage's plane staging (css_fused.cuh
+// thph_stage_tma): for each state buffer (vars0, the two stage buffers) and
+// B, a 4-D FP64 map (theta, phi, r, field) with a 42x32 main-row box and a
+// 32x4 phi-halo box.  Returns false when the driver offers no encoder (the
+// run then keeps the four-kernel stage).
+static bool plane_maps(css_ctx *c) {
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  if (!encode) {
+    cudaDriverEntryPointQueryResult q;
+    void *fn = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return false;
+    encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  }
+  const CssGeo &g = c->g;
+  double *bufs[4] = {c->v0, c->vA, c->vB, c->bf};
+  for (int k = 0; k < 4; k++) {
+    if (!bufs[k]) { memset(&c->pmaps[k], 0, sizeof(PlaneMaps)); continue; }
+    const cuuint64_t dims[4] = {(cuuint64_t)g.nth, (cuuint64_t)g.nphi, (cuuint64_t)g.nr, (cuuint64_t)(k < 3 ? c->nv : 3)};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.nth * 8, (cuuint64_t)g.nth * g.nphi * 8, (cuuint64_t)c->ncell * 8};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    const cuuint32_t bmain[4] = {FA_RW, FM, 1, 1}, bhalo[4] = {FM, 4, 1, 1};
+    if (encode(&c->pmaps[k].main, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, bufs[k], dims, strides, bmain, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    if (encode(&c->pmaps[k].halo, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, bufs[k], dims, strides, bhalo, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  return true;
+}
 
 extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **out) {
   if (!out) { set_err("css_create: NULL out"); return CSS_ERR_ARG; }
@@ -772,6 +810,7 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
                 (p.time_stepper == 4 || p.time_stepper == 0) && !p.laplacian && !p.do_radheat && !p.top_inout &&
                 !p.bot_inout && !p.bottom_specified;
   if (c->fused_ok) ALLOC(c->rtw, (size_t)nr * nphi * 2 * 32 * sizeof(double));
+  if (c->fused_ok && !plane_maps(c)) c->fused_ok = 0;
   c->fused = c->fused_ok;
   *out = c;
   return CSS_OK;
@@ -1122,8 +1161,11 @@ static int launch_stage_fused(css_ctx *c, const double *cur, double *nx, int sta
   // persistent kernels: one CTA per SM
   const dim3 ga(c->nsm);
   prof_begin(c, KI_THPH);
-  if (mag) k_thph<1><<<ga, FNT, ThphCfg<1>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf, c->rtw);
-  else k_thph<0><<<ga, FNT, ThphCfg<0>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf, c->rtw);
+  const int mi = cur == c->v0 ? 0 : (cur == c->vA ? 1 : (cur == c->vB ? 2 : -1));
+  if (mi < 0) { set_err("launch_stage_fused: stage input is not a state buffer"); return CSS_ERR_ARG; }
+  const PlaneMaps &mc = c->pmaps[mi], &mb = c->pmaps[3];
+  if (mag) k_thph<1><<<ga, FNT, ThphCfg<1>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf, c->rtw, mc, mb, c->flag);
+  else k_thph<0><<<ga, FNT, ThphCfg<0>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->tbuf, c->rtw, mc, mb, c->flag);
   prof_end(c);
   if (int rc = check_launch(c)) return rc;
   if (with_sld)
@@ -1273,6 +1315,10 @@ extern "C" int css_step_rk4(css_ctx *c, double dt, int nsteps) {
   int h = 0;
   CUDA_TRY(cudaMemcpyAsync(&h, c->flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
+  if (h & kFlagTimeout) {
+    set_err("css_step_rk4: a tile's staged copies did not arrive within the kernel's bounded wait");
+    return CSS_ERR_CUDA;
+  }
   if (h) { set_err("css_step_rk4: non-finite value in the state"); return CSS_ERR_NAN; }
   return CSS_OK;
 }
@@ -1764,6 +1810,11 @@ extern "C" int css_ensemble_step(css_ensemble *e, const double *dt, int nsteps) 
   float ms = 0.f;
   CUDA_TRY(cudaEventElapsedTime(&ms, e->t0, e->t1));
   e->last_ms = ms;
+  for (int i = 0; i < nm; i++)
+    if (h[i] & kFlagTimeout) {
+      set_err("css_ensemble_step: member %d: a tile's staged copies did not arrive within the kernel's bounded wait", i);
+      return CSS_ERR_CUDA;
+    }
   for (int i = 0; i < nm; i++)
     if (h[i]) { set_err("css_ensemble_step: non-finite value in member %d", i); return CSS_ERR_NAN; }
   return CSS_OK;

@@ -33,6 +33,8 @@
 // k_rhot_update; only the order in which the density-theta term joins the
 // sums differs (it follows the theta terms here), a rounding-level change.
 #pragma once
+#include <cuda.h>  // CUtensorMap
+#include <cstdint>
 #include "css_kernels.cuh"
 
 namespace css {
@@ -64,7 +66,10 @@ struct ThphCfg {
   // computes the current one; MHD (eight fields) has room for one plane and
   // brings the next one toward L2 instead
   static constexpr int NBUF = MAG ? 1 : 2;
-  static constexpr size_t SMEM = 8 * ((size_t)NBUF * NF * FA_FIELD + (size_t)NO * FA_OUT);
+  // + one mbarrier per plane buffer
+  static constexpr size_t SMEM = 8 * ((size_t)NBUF * NF * FA_FIELD + (size_t)NO * FA_OUT + NBUF);
+  // bytes one plane's copies deliver
+  static constexpr unsigned TX = 8u * NF * FA_FIELD;
 };
 
 // index maps of the lines (css_lines.cuh: the solver reads xb[xi(j)] and
@@ -91,6 +96,64 @@ struct SwzCol {  // phi line t of a derivative tile: element (j, t)
   __device__ __forceinline__ int operator()(int j) const { return j * FM + (t ^ (j & 15)); }
 };
 __device__ __forceinline__ double swz(const double *O, int p, int t) { return O[p * FM + (t ^ (p & 15))]; }
+
+// ---- TMA tile copies completing on an mbarrier (this CTA's own shared
+// memory; no cluster multicast) ----------------------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+// orders the barrier initialisation (generic proxy) before the async proxy's
+// use of it
+__device__ __forceinline__ void mbar_fence_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+// orders this thread's earlier shared-memory accesses (and those the barrier
+// before it made visible) before later async-proxy copies into that memory
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// waits for the phase of the given parity, for at most about `cycles` SM
+// clocks; false when the limit ran out
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, unsigned parity, long long cycles) {
+  const long long t0 = clock64();
+  while (!mbar_try_wait(bar, parity))
+    if (clock64() - t0 > cycles) return false;
+  return true;
+}
+// one 4-D box of a tiled tensor map into shared memory; x (the innermost,
+// theta) start is a multiple of 2 doubles, so 16-byte aligned
+__device__ __forceinline__ void tma_load_4d(void *dst, const CUtensorMap *tm, int x, int y, int z, int w,
+                                            uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(tm)), "r"(x), "r"(y), "r"(z), "r"(w), "r"(smem_u32(bar))
+      : "memory");
+}
+// about two seconds at the B200's clocks: a bound no healthy copy reaches
+constexpr long long kWaitCycles = 4000000000ll;
+// bit of the step flag a timed-out wait sets (bit 0 is a non-finite state)
+constexpr int kFlagTimeout = 2;
+
+// The tensor maps of one state buffer: 4-D (theta, phi, r, field) FP64,
+// boxes of the plane's main rows (42 theta x 32 phi) and of its phi halo
+// (32 theta x 4 phi).
+struct PlaneMaps {
+  CUtensorMap main, halo;
+};
 
 // ---------------------------------------------------------------------------
 // k_thph.  Persistent: CTA b takes tiles b, b + gridDim.x, ...; a tile is
@@ -136,31 +199,24 @@ __device__ __forceinline__ void thph_prefetch(const CssGeo &g, const double *con
   }
 }
 
-// stage the plane: 16-byte copies, zero fill outside [0, nth)
+// stage the plane with TMA boxes (called by one thread): per field the main
+// rows over theta t0-4 .. t0+37 (zero outside [0, nth)) and the two 4-row
+// phi halos (periodic; blocks are 32 long, so a halo box never wraps)
 template <int NF>
-__device__ __forceinline__ void thph_stage(const CssGeo &g, const double *const *src, const ThphTile &T, double *F) {
-  const size_t pl = plane(g, T.ir);
-  constexpr int MAINP = FM * 20, HALOP = 8 * 16, PER = MAINP + HALOP;
-  for (int k = threadIdx.x; k < NF * PER; k += FNT) {
-    const int f = k / PER, q = k - f * PER;
-    int p, tt, dst;
-    if (q < MAINP) {
-      const int row = q / 20, c = (q - row * 20) * 2;
-      tt = T.t0 - 4 + c;
-      p = T.p0 + row;
-      dst = row * FA_RW + c;
-    } else {
-      const int h = (q - MAINP) / 16, c = (q - MAINP - h * 16) * 2;
-      p = h < 4 ? T.p0 - 4 + h : T.p0 + FM + (h - 4);
-      if (p < 0) p += g.nphi;
-      else if (p >= g.nphi) p -= g.nphi;
-      tt = T.t0 + c;
-      dst = FA_MAIN + h * FM + c;
-    }
-    const bool in = tt >= 0 && tt < g.nth;
-    cp_async16(F + (size_t)f * FA_FIELD + dst, src[f] + pl + (size_t)p * g.nth + (in ? tt : 0), in ? 16 : 0);
+__device__ __forceinline__ void thph_stage_tma(const CssGeo &g, const PlaneMaps &mc, const PlaneMaps &mb,
+                                               const ThphTile &T, double *F, uint64_t *bar) {
+  const int plo = T.p0 >= 4 ? T.p0 - 4 : g.nphi - 4;
+  const int phi = T.p0 + FM < g.nphi ? T.p0 + FM : 0;
+  mbar_expect_tx(bar, 8u * NF * FA_FIELD);
+#pragma unroll
+  for (int f = 0; f < NF; f++) {
+    const PlaneMaps &m = f < 5 ? mc : mb;
+    const int w = f < 5 ? f : f - 5;
+    double *Fd = F + (size_t)f * FA_FIELD;
+    tma_load_4d(Fd, &m.main, T.t0 - 4, T.p0, T.ir, w, bar);
+    tma_load_4d(Fd + FA_MAIN, &m.halo, T.t0, plo, T.ir, w, bar);
+    tma_load_4d(Fd + FA_MAIN + 4 * FM, &m.halo, T.t0, phi, T.ir, w, bar);
   }
-  cp_async_commit();
 }
 
 // theta line solve of derivative tile k (0 dw 1 dv 2 du 3 ds 4 d2s [5 dbp
@@ -231,37 +287,62 @@ __device__ __forceinline__ void thph_wall_rho(const CssGeo &g, const double *F, 
 template <int MAG>
 __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restrict__ cur,
                                                  const double *__restrict__ bf, double *__restrict__ dv,
-                                                 double *__restrict__ tbuf, double *__restrict__ rtw) {
+                                                 double *__restrict__ tbuf, double *__restrict__ rtw,
+                                                 const __grid_constant__ PlaneMaps mc,
+                                                 const __grid_constant__ PlaneMaps mb, int *flag) {
   using C = ThphCfg<MAG>;
   constexpr int NA = MAG ? 8 : 5;
-  extern __shared__ __align__(16) double sm[];
+  // plane buffers (128-byte aligned boxes: a field is 12800 bytes), the
+  // derivative tiles, the buffers' mbarriers
+  extern __shared__ __align__(128) double sm[];
   double *O = sm + (size_t)C::NBUF * C::NF * FA_FIELD;  // NO derivative tiles
+  uint64_t *bar = reinterpret_cast<uint64_t *>(O + (size_t)C::NO * FA_OUT);
   const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
   const size_t n = (size_t)g.ncell;
   const double *src[8];
   src[0] = cur; src[1] = cur + n; src[2] = cur + 2 * n; src[3] = cur + 3 * n; src[4] = cur + 4 * n;
   if (MAG) { src[5] = bf; src[6] = bf + n; src[7] = bf + 2 * n; }
   const int ntile = g.nr * g.d[1].nb * g.d[2].nb;
-  if (C::NBUF == 2 && (int)blockIdx.x < ntile) thph_stage<C::NF>(g, src, thph_tile(g, blockIdx.x), sm);
+  if (tid == 0) {
+    for (int b = 0; b < C::NBUF; b++) mbar_init(bar + b, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (C::NBUF == 2 && tid == 0 && (int)blockIdx.x < ntile)
+    thph_stage_tma<C::NF>(g, mc, mb, thph_tile(g, blockIdx.x), sm, bar);
   for (int q = blockIdx.x, i = 0; q < ntile; q += gridDim.x, i++) {
     const ThphTile T = thph_tile(g, q);
-    double *F = sm + (size_t)(C::NBUF == 2 ? (i & 1) : 0) * C::NF * FA_FIELD;
+    const int b = C::NBUF == 2 ? (i & 1) : 0;
+    double *F = sm + (size_t)b * C::NF * FA_FIELD;
     const bool more = q + (int)gridDim.x < ntile;
     if (C::NBUF == 2) {
-      // the next plane into the other buffer (its last readers passed the
-      // barrier at the end of the previous tile), then wait for this one
-      if (more) {
-        thph_stage<C::NF>(g, src, thph_tile(g, q + gridDim.x), sm + (size_t)((i + 1) & 1) * C::NF * FA_FIELD);
-        cp_async_wait<1>();
-      } else {
-        cp_async_wait<0>();
+      // the next plane into the other buffer: its last readers passed the
+      // barrier that ended the previous tile
+      if (more && tid == 0) {
+        fence_proxy_async();
+        thph_stage_tma<C::NF>(g, mc, mb, thph_tile(g, q + gridDim.x), sm + (size_t)(b ^ 1) * C::NF * FA_FIELD,
+                              bar + (b ^ 1));
       }
     } else {
       if (more) thph_prefetch<C::NF>(g, src, thph_tile(g, q + gridDim.x));
-      thph_stage<C::NF>(g, src, T, F);
-      cp_async_wait<0>();
+      if (tid == 0) {
+        fence_proxy_async();
+        thph_stage_tma<C::NF>(g, mc, mb, T, F, bar);
+      }
     }
-    __syncthreads();
+    // this plane's copies: buffer b's (i >> 1)-th use (every use for MHD)
+    const unsigned parity = C::NBUF == 2 ? ((unsigned)(i >> 1) & 1u) : ((unsigned)i & 1u);
+    const bool late = !mbar_wait_bounded(bar + b, parity, kWaitCycles);
+    if (__syncthreads_or(late)) {
+      // a copy that never completes: report it and stop, after giving the
+      // copies still in flight the same bound to land
+      if (tid == 0) {
+        atomicOr(flag, kFlagTimeout);
+        mbar_wait_bounded(bar + b, parity, kWaitCycles);
+        if (C::NBUF == 2 && more) mbar_wait_bounded(bar + (b ^ 1), (unsigned)((i + 1) >> 1) & 1u, kWaitCycles);
+      }
+      return;
+    }
     const CssDir &DT = g.d[1];
     const bool wall = DT.lphys[T.bt] || DT.rphys[T.bt];
     const int ir = T.ir, it = T.t0 + lane;
