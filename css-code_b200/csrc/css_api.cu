@@ -68,7 +68,8 @@ struct css_ctx {
   double *cda;                      // curl of the A-tendency (MHD ohmic heating)
   double *tbuf;                     // temperature of the current stage input
   double *rtw = nullptr;            // two-pass stage: zero-datum d(rho)/dtheta on the theta-wall blocks
-  PlaneMaps pmaps[4];               // two-pass stage: TMA maps of v0, vA, vB and bf
+  PlaneMaps pmaps[4];               // two-pass stage: TMA maps of v0, vA, vB and bf (plane kernel)
+  SlabMaps smaps[5];                // the same for the stage kernel's slabs, then rtw
   double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
   double *lapface = nullptr;        // explicit viscosity: face data, 6 x max face size
   double *radbuf = nullptr;         // radiative diffusion: d ln(rho)/dr, ds/dr, 8 derivative fields
@@ -373,7 +374,11 @@ static bool plane_maps(css_ctx *c) {
   const CssGeo &g = c->g;
   double *bufs[4] = {c->v0, c->vA, c->vB, c->bf};
   for (int k = 0; k < 4; k++) {
-    if (!bufs[k]) { memset(&c->pmaps[k], 0, sizeof(PlaneMaps)); continue; }
+    if (!bufs[k]) {
+      memset(&c->pmaps[k], 0, sizeof(PlaneMaps));
+      memset(&c->smaps[k], 0, sizeof(SlabMaps));
+      continue;
+    }
     const cuuint64_t dims[4] = {(cuuint64_t)g.nth, (cuuint64_t)g.nphi, (cuuint64_t)g.nr, (cuuint64_t)(k < 3 ? c->nv : 3)};
     const cuuint64_t strides[3] = {(cuuint64_t)g.nth * 8, (cuuint64_t)g.nth * g.nphi * 8, (cuuint64_t)c->ncell * 8};
     const cuuint32_t estr[4] = {1, 1, 1, 1};
@@ -383,6 +388,21 @@ static bool plane_maps(css_ctx *c) {
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return false;
     if (encode(&c->pmaps[k].halo, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, bufs[k], dims, strides, bhalo, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+    // the stage kernel's slab box: 32 theta x 1 phi x 40 r
+    const cuuint32_t bslab[4] = {FM, 1, FM + 8, 1};
+    if (encode(&c->smaps[k].slab, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, bufs[k], dims, strides, bslab, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return false;
+  }
+  {  // rtw: (theta 32, side 2, phi, r), box 32 x 1 x 1 x 32
+    const cuuint64_t dims[4] = {32, 2, (cuuint64_t)g.nphi, (cuuint64_t)g.nr};
+    const cuuint64_t strides[3] = {32 * 8, 64 * 8, (cuuint64_t)g.nphi * 64 * 8};
+    const cuuint32_t estr[4] = {1, 1, 1, 1}, box[4] = {FM, 1, 1, FM};
+    if (encode(&c->smaps[4].slab, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, c->rtw, dims, strides, box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return false;
@@ -1174,7 +1194,8 @@ static int launch_stage_fused(css_ctx *c, const double *cur, double *nx, int sta
   prof_begin(c, KI_RSTAGE);
 #define CSS_RSTAGE(M, S)                                                                                      \
   k_rstage<M, S><<<gb, RstageCfg<M>::NT, RstageCfg<M>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->v0, c->vs, nx, c->tbuf, \
-                                                              c->rtw, dtcur, c->flag)
+                                                              c->rtw, dtcur, c->flag, c->smaps[mi], c->smaps[3], \
+                                                              c->smaps[4])
   switch (stage + (mag ? 10 : 0)) {
     case 1: CSS_RSTAGE(0, 1); break;
     case 2: CSS_RSTAGE(0, 2); break;

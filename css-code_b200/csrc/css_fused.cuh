@@ -154,6 +154,12 @@ constexpr int kFlagTimeout = 2;
 struct PlaneMaps {
   CUtensorMap main, halo;
 };
+// The tensor maps of the stage kernel's slab: the state buffer (or B) with
+// a 32 theta x 1 phi x 40 r box, and the wall d(rho)/dtheta rows (theta 32,
+// side 2, phi, r) with a 32 x 1 x 1 x 32 box.
+struct SlabMaps {
+  CUtensorMap slab;
+};
 
 // ---------------------------------------------------------------------------
 // k_thph.  Persistent: CTA b takes tiles b, b + gridDim.x, ...; a tile is
@@ -521,7 +527,8 @@ struct RstageCfg {
   static constexpr int NT = MAG ? 512 : 256;  // threads per CTA
   static constexpr int NW = NT / 32;           // warps
   static constexpr int PPT = FM * FM / NT;     // points per thread
-  static constexpr size_t SMEM = 8 * ((size_t)NH * FB_FIELD + (size_t)ND * FB_OUT + FB_OUT + 2 * FM);
+  // + the slab's mbarrier
+  static constexpr size_t SMEM = 8 * ((size_t)NH * FB_FIELD + (size_t)ND * FB_OUT + FB_OUT + 2 * FM + 1);
 };
 
 struct RstageTile {
@@ -549,19 +556,21 @@ __global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssG
                                                               const double *v0, double *vs, double *nx,
                                                               const double *__restrict__ tbuf,
                                                               const double *__restrict__ rtw, double dtcur,
-                                                              int *flag) {
+                                                              int *flag, const __grid_constant__ SlabMaps sc,
+                                                              const __grid_constant__ SlabMaps sb,
+                                                              const __grid_constant__ SlabMaps sw) {
   using C = RstageCfg<MAG>;
   constexpr int nv = MAG ? 8 : 5;
-  extern __shared__ __align__(16) double sm[];
-  double *H = sm;
+  extern __shared__ __align__(128) double sm[];
+  double *H = sm;  // fields of 10240 bytes: every TMA box lands 128-byte aligned
   double *O = H + (size_t)C::NH * FB_FIELD;
   double *W = O + (size_t)C::ND * FB_OUT;
   double *datum = W + FB_OUT;  // [0, 32): radial face datum per line; [32, 64): theta wall datum per row
+  uint64_t *bar = reinterpret_cast<uint64_t *>(datum + 2 * FM);
   const CssDir &D = g.d[0], &DT = g.d[1];
   const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
   const size_t n = (size_t)g.ncell, ps = (size_t)g.nth * g.nphi;
   const int nr = g.nr;
-  const double *hsrc[7] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, cur, MAG ? bf : cur, MAG ? bf + n : cur};
   const bool need_s = !(STG == 1 && !g.sldiffusion);
   int bad = 0;
   {
@@ -585,29 +594,35 @@ __global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssG
         prefetch_l2(b + (size_t)(T.r0 + rr) * ps + base + (k & 1) * 16);
       }
     }
-    // ---- stage the slab [and the wall rows of d(rho)/dtheta] ----
+    // ---- stage the slab [and the wall rows of d(rho)/dtheta] with TMA
+    // boxes: per field the 40 radial rows r0-4 .. r0+35 of the 32 theta
+    // values (zero outside [0, nr)) ----
     const bool lw = DT.lphys[T.bt], hw = DT.rphys[T.bt];
-    {
-      constexpr int PH = (FM + 8) * 16;
-      const int nw = (lw || hw) ? FM * 16 : 0;
-      const int side = lw ? 0 : 1;
-      for (int k = tid; k < C::NH * PH + nw; k += C::NT) {
-        if (k < C::NH * PH) {
-          const int f = k / PH, qq = k - f * PH;
-          const int rr = qq >> 4, c = (qq & 15) * 2;
-          const int gr = T.r0 - 4 + rr;
-          const bool in = gr >= 0 && gr < nr;
-          cp_async16(H + (size_t)f * FB_FIELD + rr * FM + c, hsrc[f] + (in ? (size_t)gr * ps + base + c : 0),
-                     in ? 16 : 0);
-        } else {
-          const int kk = k - C::NH * PH, rr = kk >> 4, c = (kk & 15) * 2;
-          cp_async16(W + rr * FM + c, rtw + (((size_t)(T.r0 + rr) * g.nphi + T.ip) * 2 + side) * FM + c, 16);
-        }
-      }
-      cp_async_commit();
-      cp_async_wait<0>();
+    if (tid == 0) {
+      mbar_init(bar, 1);
+      mbar_fence_init();
     }
-    __syncthreads();
+    __syncthreads();  // the barrier is initialised before anyone waits on it
+    if (tid == 0) {
+      mbar_expect_tx(bar, 8u * (C::NH * FB_FIELD + ((lw || hw) ? FB_OUT : 0)));
+#pragma unroll
+      for (int f = 0; f < C::NH; f++) {
+        // H order w v u s rho [bt bp]: fields 1 2 3 4 0 of the state, 0 1 of B
+        const CUtensorMap *m = f < 5 ? &sc.slab : &sb.slab;
+        const int w = f < 4 ? f + 1 : (f == 4 ? 0 : f - 5);
+        tma_load_4d(H + (size_t)f * FB_FIELD, m, T.t0, T.ip, T.r0 - 4, w, bar);
+      }
+      if (lw || hw) tma_load_4d(W, &sw.slab, 0, lw ? 0 : 1, T.ip, T.r0, bar);
+    }
+    if (__syncthreads_or(!mbar_wait_bounded(bar, 0u, kWaitCycles))) {
+      // copies that never complete: report them and stop, after giving the
+      // ones still in flight the same bound to land
+      if (tid == 0) {
+        atomicOr(flag, kFlagTimeout);
+        mbar_wait_bounded(bar, 0u, kWaitCycles);
+      }
+      return;
+    }
 
     // ---- radial solves: tile k = warp, line = lane ----
     const int dtype = dtype_of(D, T.br);
