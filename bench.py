@@ -328,7 +328,9 @@ def run_ours(args):
     stream = torch.cuda.current_stream(dev)
     sim.set_stream(stream.cuda_stream)
     sim.upload(v0)
-    tiles = sim.autotune(reps=3)  # lines per CTA for r, theta, phi (no result changes)
+    # lines per CTA of the four-kernel stage's sweeps (no result changes);
+    # the two-pass stage has fixed tiles
+    tiles = (0, 0, 0) if sim.fused else sim.autotune(reps=3)
     for _ in range(args.warmup):
         sim.step_rk4(dt, 1)
     torch.cuda.synchronize()
@@ -386,6 +388,7 @@ def run_ours(args):
         per_launch_cells = cells
         achieved = alg * per_launch_cells / (kms / cnt / 1e3) / 1e9 if alg else None
         traffic = None
+        fp64 = None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
             try:
@@ -393,13 +396,18 @@ def run_ours(args):
                 key = "%s/%s" % ("mhd" if p.magnetic else "hydro", name)
                 if key in tj:
                     traffic = tj[key]["dram_bytes_per_cell"] * per_launch_cells
+                    fp64 = tj[key].get("fp64_pipe_pct_of_peak")
             except Exception:
                 traffic = None
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "algorithmic_bytes_per_launch": alg * per_launch_cells if alg else None,
                 "avg_launch_ms": kms / cnt, "peak_source": peak_src,
-                "time_share": kms / sum(v[0] for v in stats.values())}
+                "time_share": kms / sum(v[0] for v in stats.values()),
+                # the FP64 bound beside the HBM one: ncu's FP64-pipe activity
+                # of this kernel (profiles/traffic.json, captured on the
+                # 128x128x256 case of the same kind of run)
+                "fp64_pipe_frac": (fp64 / 100.0) if fp64 is not None else None}
     step_ach = step_alg_bytes(nv) * cells * args.steps / (ms / 1e3) / 1e9
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
