@@ -460,7 +460,8 @@ def run_ensemble(args):
     count = int(args.workload.split("-")[1])
     specs = E.shell_specs(count, seed=7)
     mine = E.lpt_partition([E.member_cost(s) for s in specs], world)[rank]
-    members = [E.build_member(specs[i], seed=1000 + i) for i in mine]
+    prec = 1 if args.precision == "mixed" else 0
+    members = [E.build_member(specs[i], seed=1000 + i, precision=prec) for i in mine]
     sims = []
     for p, prof, v0, dt in members:
         sim = Simulation(p, prof)
@@ -513,8 +514,9 @@ def run_ensemble(args):
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
-        "dtype": "f64", "data": "synthetic",
+        "dtype": "f64" if not prec else "f32-storage/f64", "data": "synthetic",
         "config": {"workload": args.workload, "members": summ["members"], "mhd_members": summ["mhd"],
+                   "precision": args.precision, "ro_range": list(E.RO_RANGE), "pm_range": list(E.PM_RANGE),
                    "cells": total_cells, "members_on_rank0": len(mine),
                    "l2": "states (%.1f GB) larger than L2, no flush" % (state_bytes / 1e9),
                    "parallelism": "lpt over %d ranks, one CUDA graph per rank" % world},
@@ -524,7 +526,10 @@ def run_ensemble(args):
         "gpu_launches": launches,
         "step_roofline": {"algorithmic_bytes_per_cell_step": "17 nv words", "achieved": step_ach, "peak": peak,
                           "unit": "GB/s", "frac": step_ach / peak, "peak_source": peak_src},
-        "error_vs_oracle": "bit-identical to the members stepped alone (tests/test_ensemble.py)",
+        "error_vs_oracle": ("bit-identical to the members stepped alone, 200 steps (tests/test_ensemble.py)"
+                            if not prec else
+                            "every member within the mixed form's bounds of its own unbatched FP64 run after "
+                            "200 steps (tests/test_ensemble.py)"),
     }
     if clk:
         out["clocks"] = clk

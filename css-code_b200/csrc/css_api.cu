@@ -68,6 +68,7 @@ struct css_ctx {
   double *cda;                      // curl of the A-tendency (MHD ohmic heating)
   double *tbuf;                     // temperature of the current stage input
   double *rtw = nullptr;            // two-pass stage: zero-datum d(rho)/dtheta on the theta-wall blocks
+  double *cyc = nullptr;            // cyclic phi derivative tables, per order: w, piv, z (nphi each), v.z
   PlaneMaps pmaps[4];               // two-pass stage: TMA maps of v0, vA, vB and bf (plane kernel)
   SlabMaps smaps[5];                // the same for the stage kernel's slabs, then rtw
   double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
@@ -256,7 +257,7 @@ extern "C" void css_destroy(css_ctx *c) {
   if (!c) return;
   cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo); cudaFree(c->resp);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
-  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf); cudaFree(c->rtw);
+  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf); cudaFree(c->rtw); cudaFree(c->cyc);
   cudaFree(c->lapbuf); cudaFree(c->lapface); cudaFree(c->radbuf); cudaFree(c->radface);
   cudaFree(c->io); cudaFree(c->io_part); cudaFree(c->rain); cudaFree(c->ash_slices); cudaFree(c->ashv);
   cudaFree(c->squalls);
@@ -355,6 +356,28 @@ static int setup_kernels() {
       default: KERNEL<0, 0, CSS_STRIP XT><<<GRID, 128, SMEM, c->stream>>>(__VA_ARGS__); break;     \
     }                                                                                     \
   } while (0)
+
+// Tables of the cyclic phi derivative (k_dbydp_cyclic) for n points:
+// B = tridiag(alpha, 1, alpha) with first diagonal 1 - gamma and last
+// 1 - alpha^2/gamma (gamma = -1); elimination factors w[j] = alpha /
+// piv[j-1], pivots piv[j] = b_j - alpha w[j], z = B^-1 u with u = (gamma,
+// 0.., alpha), and v.z = z[0] + (alpha/gamma) z[n-1].  out: w | piv | z | v.z
+static void cyclic_tables(int n, int order, double *out) {
+  const double alpha = order == 1 ? 1.0 / 3.0 : 2.0 / 11.0, gamma = -1.0;
+  double *w = out, *piv = out + n, *z = out + 2 * n;
+  w[0] = 0.0;
+  piv[0] = 1.0 - gamma;
+  for (int j = 1; j < n; j++) {
+    w[j] = alpha / piv[j - 1];
+    const double bj = j == n - 1 ? 1.0 - alpha * alpha / gamma : 1.0;
+    piv[j] = bj - alpha * w[j];
+  }
+  // z: forward then back substitution on u
+  z[0] = gamma / piv[0];
+  for (int j = 1; j < n; j++) z[j] = ((j == n - 1 ? alpha : 0.0) - alpha * z[j - 1]) / piv[j];
+  for (int j = n - 2; j >= 0; j--) z[j] -= w[j + 1] * z[j + 1];
+  out[3 * n] = z[0] + (alpha / gamma) * z[n - 1];
+}
 
 // TMA maps of the two-pass stage's plane staging (css_fused.cuh
 // thph_stage_tma): for each state buffer (vars0, the two stage buffers) and
@@ -830,6 +853,13 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
                 (p.time_stepper == 4 || p.time_stepper == 0) && !p.laplacian && !p.do_radheat && !p.top_inout &&
                 !p.bot_inout && !p.bottom_specified;
   if (c->fused_ok) ALLOC(c->rtw, (size_t)nr * nphi * 2 * 32 * sizeof(double));
+  {  // cyclic phi derivative tables (css_dbydp_cyclic)
+    const size_t per = 3 * (size_t)nphi + 1;
+    std::vector<double> CY(2 * per);
+    for (int order = 1; order <= 2; order++) cyclic_tables(nphi, order, &CY[(order - 1) * per]);
+    ALLOC(c->cyc, CY.size() * sizeof(double));
+    cudaMemcpy(c->cyc, CY.data(), CY.size() * sizeof(double), cudaMemcpyHostToDevice);
+  }
   if (c->fused_ok && !plane_maps(c)) c->fused_ok = 0;
   c->fused = c->fused_ok;
   *out = c;
@@ -1435,6 +1465,28 @@ extern "C" int css_deriv_dev(css_ctx *c, int dir, int order, const double *x, do
     else k_deriv_r<2, 0><<<gr, 128, sm, st>>>(g, x, dx, bc_lo, bc_hi, bdry, TL);
   }
   return check_launch(c);
+}
+
+extern "C" int css_dbydp_cyclic_dev(css_ctx *c, const double *x, double *dx, int order, void *stream) {
+  if (!c || !x || !dx || order < 1 || order > 2) { set_err("css_dbydp_cyclic: bad argument"); return CSS_ERR_ARG; }
+  if (x == dx) { set_err("css_dbydp_cyclic: x and dx must not overlap"); return CSS_ERR_ARG; }
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  const CssGeo &g = c->g;
+  const size_t nl = (size_t)g.nth * g.nr;
+  const double dpi = 1.0 / c->g.dphi;
+  const double *T = c->cyc + (size_t)(order - 1) * (3 * (size_t)g.nphi + 1);
+  k_dbydp_cyclic<<<(unsigned)((nl + 127) / 128), 128, 0, st>>>(g, x, dx, T, order, order == 1 ? dpi : dpi * dpi);
+  return check_launch(c);
+}
+
+extern "C" int css_dbydp_cyclic(css_ctx *c, const double *x, double *dx, int order) {
+  if (!c || !x || !dx) { set_err("css_dbydp_cyclic: NULL"); return CSS_ERR_ARG; }
+  const size_t n = c->ncell;
+  CUDA_TRY(cudaMemcpyAsync(c->vA, x, n * 8, cudaMemcpyHostToDevice, c->stream));
+  if (int rc = css_dbydp_cyclic_dev(c, c->vA, c->dv, order, nullptr)) return rc;
+  CUDA_TRY(cudaMemcpyAsync(dx, c->dv, n * 8, cudaMemcpyDeviceToHost, c->stream));
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
 }
 
 extern "C" int css_deriv(css_ctx *c, int dir, int order, const double *x, double *dx, const double *bc_lo,

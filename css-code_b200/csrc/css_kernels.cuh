@@ -1915,6 +1915,53 @@ __global__ void __launch_bounds__(128) k_deriv_r(CssGeo g, const double *__restr
 
 // independent lines with explicit closures (css_compact_lines /
 // Dbyd1_dt0): one thread per line on global memory, lines contiguous.
+// Cyclic phi derivative of one field (css_dbydp_cyclic; an extension with
+// no counterpart in the reference, whose Dbydp closes each block with halo
+// rows, derivatives.f90:1480-1591): every whole phi line is periodic and
+// takes Dbydp's interior rows at every point; the cyclic tridiagonal
+// system is solved by Sherman-Morrison, A = B + u v^T with gamma = -1, as
+// x = y - (v.y)/(1 + v.z) z.  T holds, for this order and nphi, B's
+// elimination factors w[j], pivots piv[j], the vector z = B^-1 u and v.z.
+// One thread per (theta, r) line; consecutive threads take consecutive
+// theta, so every load and store is coalesced.
+__global__ void k_dbydp_cyclic(CssGeo g, const double *__restrict__ x, double *__restrict__ out,
+                               const double *__restrict__ T, int order, double scale) {
+  const int nth = g.nth, n = g.nphi;
+  const size_t line = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (line >= (size_t)nth * g.nr) return;
+  const int t = (int)(line % nth), r = (int)(line / nth);
+  const size_t base = (size_t)r * nth * n + t;
+  const double *w = T, *piv = T + n, *z = T + 2 * n;
+  const double vz = T[3 * n];
+  const double alpha = order == 1 ? 1.0 / 3.0 : 2.0 / 11.0, ag = -alpha;  // alpha / gamma, gamma = -1
+  auto X = [&](int j) { return __ldg(x + base + (size_t)j * nth); };
+  double fm2 = X(n - 2), fm1 = X(n - 1), f0 = X(0), fp1 = X(1), fp2 = X(2);
+  double prev = 0.0;
+  for (int j = 0; j < n; j++) {
+    const double rhs = order == 1 ? (7.0 / 9.0) * (fp1 - fm1) + (1.0 / 36.0) * (fp2 - fm2)
+                                  : (12.0 / 11.0) * (fp1 - 2.0 * f0 + fm1) + (3.0 / 44.0) * (fp2 - 2.0 * f0 + fm2);
+    const double y = j == 0 ? rhs / __ldg(piv) : (rhs - alpha * prev) / __ldg(piv + j);
+    out[base + (size_t)j * nth] = y;
+    prev = y;
+    fm2 = fm1; fm1 = f0; f0 = fp1; fp1 = fp2;
+    int k = j + 3;
+    if (k >= n) k -= n;
+    fp2 = X(k);
+  }
+  const double yl = prev;
+  double next = prev;
+  for (int j = n - 2; j >= 0; j--) {
+    const double y = out[base + (size_t)j * nth] - __ldg(w + j + 1) * next;
+    out[base + (size_t)j * nth] = y;
+    next = y;
+  }
+  const double fact = (next + ag * yl) / (1.0 + vz);
+  for (int j = 0; j < n; j++) {
+    const size_t q = base + (size_t)j * nth;
+    out[q] = scale * (out[q] - fact * __ldg(z + j));
+  }
+}
+
 __global__ void k_lines(const double *__restrict__ x, double *__restrict__ out, int n, int nlines, int order,
                         int dtype, int bdry, const double *__restrict__ bclo, const double *__restrict__ bchi,
                         const double *__restrict__ hlo, const double *__restrict__ hhi, const double *__restrict__ tab,

@@ -120,6 +120,16 @@ class Simulation:
         check(_lib.lib().css_autotune(self.h, int(reps), ch))
         return tuple(ch)
 
+    def dbydp_cyclic(self, field, order=1):
+        """Cyclic phi derivative of one field (nr, nphi, nth): every whole
+        phi line periodic, Sherman-Morrison (css_dbydp_cyclic; an extension
+        beside the reference's block-closed Dbydp)."""
+        f = np.ascontiguousarray(field, dtype=np.float64)
+        assert f.shape == self.shape[1:], (f.shape, self.shape)
+        out = np.empty_like(f)
+        check(_lib.lib().css_dbydp_cyclic(self.h, _p(f), _p(out), int(order)))
+        return out
+
     def set_fused(self, on):
         """Two-pass RK4 stage on or off (css_set_fused); on is refused for a
         run that does not qualify."""

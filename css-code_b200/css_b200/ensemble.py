@@ -19,12 +19,15 @@ import numpy as np
 from . import _lib
 from ._lib import check, dp
 
-# ranges of the shell study: nr, ntheta, nphi; log10 Ra; Rossby number
+# ranges of the shell study: nr, ntheta, nphi; log10 Ra; Rossby number;
+# magnetic Prandtl number of the MHD members (through the SLD scaling
+# sld_prm = 1/Pm, as the MHD workload's Pm 2 is sld_prm 0.5)
 NR_RANGE = (48, 160)
 NTH_RANGE = (64, 256)
 NPHI_RANGE = (128, 512)
 LOG_RA_RANGE = (4.0, 6.0)
-RO_RANGE = (0.25, 2.0)
+RO_RANGE = (0.3, 3.0)
+PM_RANGE = (1.0, 4.0)
 
 
 def _blocks(n, min_blocks):
@@ -51,7 +54,7 @@ def _blocks(n, min_blocks):
 def shell_specs(count=48, seed=7):
     """Seeded member descriptions: sizes uniform in the ranges (theta and phi
     rounded to multiples of 16, r to a multiple of 4), Ra log-uniform, Ro
-    uniform, every second member magnetic."""
+    uniform, every second member magnetic with Pm uniform."""
     rng = np.random.default_rng(seed)
     specs = []
     for i in range(count):
@@ -61,8 +64,10 @@ def shell_specs(count=48, seed=7):
         nphi = int(min(NPHI_RANGE[1], max(NPHI_RANGE[0], 16 * round(rng.uniform(*NPHI_RANGE) / 16))))
         ra = 10.0 ** rng.uniform(*LOG_RA_RANGE)
         ro = rng.uniform(*RO_RANGE)
-        specs.append({"nr": nr, "nth": nth, "nphi": nphi, "ra": ra, "ro": ro, "magnetic": i % 2 == 1,
-                      "decomp": (_blocks(nr, 2), _blocks(nth, 2), _blocks(nphi, 3))})
+        mag = i % 2 == 1
+        pm = rng.uniform(*PM_RANGE)
+        specs.append({"nr": nr, "nth": nth, "nphi": nphi, "ra": ra, "ro": ro, "magnetic": mag,
+                      "pm": pm if mag else None, "decomp": (_blocks(nr, 2), _blocks(nth, 2), _blocks(nphi, 3))})
     return specs
 
 
@@ -85,14 +90,16 @@ def lpt_partition(costs, nranks):
     return [sorted(p) for p in parts]
 
 
-def build_member(spec, seed=1234, n_rho=3.0):
-    """(params, profiles, vars0, dt) of one member."""
+def build_member(spec, seed=1234, n_rho=3.0, precision=0):
+    """(params, profiles, vars0, dt) of one member; precision 1 stores its
+    RK4 stage states in FP32 (the mixed form)."""
     from . import problem
     from .params import default_params
     p = default_params(spec["nr"], spec["nth"], spec["nphi"], spec["decomp"], magnetic=spec["magnetic"])
     p.omega_0 = 0.5 / spec["ro"]
+    p.precision = int(precision)
     if spec["magnetic"]:
-        p.sld_prm = 0.5
+        p.sld_prm = 1.0 / (spec.get("pm") or 2.0)
     prof, info = problem.polytrope(p, n_rho, ra=spec["ra"])
     vars0 = problem.initial_state(p, prof, info, seed=seed)
     bfield = problem.curl_estimate(p, prof, vars0[5:8]) if spec["magnetic"] else None

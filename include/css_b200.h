@@ -207,6 +207,19 @@ int css_d2bydp2(css_ctx *ctx, const double *x, double *dx, int var);
 int css_deriv_dev(css_ctx *ctx, int dir, int order, const double *x, double *dx,
                   const double *bc_lo, const double *bc_hi, int bdry, void *stream);
 
+/* Cyclic phi derivative (an extension, off the reference path: the
+ * reference's Dbydp / D2bydp2, derivatives.f90:1480-1684, close every phi
+ * block with halo rows, and css_dbydp / css_deriv reproduce that).  Here
+ * every whole phi line is one periodic system: Dbydp's interior rows at
+ * every point (alpha 1/3 or 2/11), the cyclic tridiagonal system solved by
+ * Sherman-Morrison; order 1 or 2, times 1/dphi or 1/dphi^2.  It differs from
+ * the reference's blocked operator at truncation level only.  x, dx: one
+ * field (nth, nphi, nr) in Fortran order, host arrays; the _dev form takes
+ * device pointers (not overlapping) and enqueues on `stream` (NULL = the
+ * context stream).                                                         */
+int css_dbydp_cyclic(css_ctx *ctx, const double *x, double *dx, int order);
+int css_dbydp_cyclic_dev(css_ctx *ctx, const double *x, double *dx, int order, void *stream);
+
 /* Batched 1D whole-line first derivative Dbyd1_dt0 (derivatives.f90:2296)
  * on nlines contiguous lines of n1 points, host pointers; bdat1/bdat2 per
  * line (may be NULL).  Returns d/dx in grid units, as the Fortran does.

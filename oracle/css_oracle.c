@@ -3156,3 +3156,70 @@ int orc_spectrum(orc_ctx *c, const double *vars0, int kind, double *out) {
   free(cp_); free(sp_); free(ct_); free(st_);
   return CSS_OK;
 }
+
+/* ------------------------------------------------------------------------
+ * Cyclic phi derivative (an extension with no counterpart in the
+ * reference, whose Dbydp / D2bydp2, derivatives.f90:1480-1684, close every
+ * block with halo rows).  The whole periodic line of n points takes the
+ * interior rows of Dbydp / D2bydp2 at every point:
+ *   alpha f'_{j-1} + f'_j + alpha f'_{j+1} = rhs_j (periodic indices),
+ * alpha = 1/3, rhs = 7/9 (f_{j+1}-f_{j-1}) + 1/36 (f_{j+2}-f_{j-2}) for the
+ * first derivative; alpha = 2/11, rhs = 12/11 (f_{j+1}-2f_j+f_{j-1}) + 3/44
+ * (f_{j+2}-2f_j+f_{j-2}) for the second; times dnum (dnum^2).  The cyclic
+ * tridiagonal system is split as A = B + u v^T (Sherman-Morrison, with
+ * gamma = -1: B's first diagonal 1 - gamma, its last 1 - alpha^2/gamma,
+ * u = (gamma, 0.., alpha), v = (1, 0.., alpha/gamma)) and solved as
+ * x = y - (v.y)/(1 + v.z) z with B y = rhs, B z = u by Gaussian
+ * elimination without pivoting (B is diagonally dominant).
+ * ------------------------------------------------------------------------ */
+static void orc_tridiag(int n, double alpha, double b0, double bn, const double *d, double *x, double *w) {
+  /* solves B x = d, B = tridiag(alpha, b, alpha), b = 1 but b[0] = b0, b[n-1] = bn;
+   * w is scratch of n */
+  double piv = b0;
+  x[0] = d[0] / piv;
+  for (int j = 1; j < n; j++) {
+    w[j] = alpha / piv;
+    const double bj = (j == n - 1) ? bn : 1.0;
+    piv = bj - alpha * w[j];
+    x[j] = (d[j] - alpha * x[j - 1]) / piv;
+  }
+  for (int j = n - 2; j >= 0; j--) x[j] -= w[j + 1] * x[j + 1];
+}
+
+int orc_cyclic_lines(const double *x, double *dx, int n, int nlines, int order, double dnum) {
+  if (!x || !dx || n < 5 || nlines < 0 || order < 1 || order > 2) {
+    set_err("orc_cyclic_lines: bad argument");
+    return CSS_ERR_ARG;
+  }
+  const double alpha = order == 1 ? 1.0 / 3.0 : 2.0 / 11.0, gamma = -1.0;
+  const double b0 = 1.0 - gamma, bn = 1.0 - alpha * alpha / gamma;
+  const double scale = order == 1 ? dnum : dnum * dnum;
+  double *u = malloc(sizeof(double) * n), *z = malloc(sizeof(double) * n), *w = malloc(sizeof(double) * n);
+  for (int j = 0; j < n; j++) u[j] = 0.0;
+  u[0] = gamma;
+  u[n - 1] = alpha;
+  orc_tridiag(n, alpha, b0, bn, u, z, w);
+  const double vz = z[0] + (alpha / gamma) * z[n - 1];
+  free(u);
+  free(w);
+#pragma omp parallel for schedule(static)
+  for (int l = 0; l < nlines; l++) {
+    const double *f = x + (size_t)l * n;
+    double *o = dx + (size_t)l * n;
+    double *r = malloc(sizeof(double) * n), *y = malloc(sizeof(double) * n), *ws = malloc(sizeof(double) * n);
+    for (int j = 0; j < n; j++) {
+      const double fm2 = f[(j - 2 + n) % n], fm1 = f[(j - 1 + n) % n], f0 = f[j], fp1 = f[(j + 1) % n],
+                   fp2 = f[(j + 2) % n];
+      if (order == 1) r[j] = (7.0 / 9.0) * (fp1 - fm1) + (1.0 / 36.0) * (fp2 - fm2);
+      else r[j] = (12.0 / 11.0) * (fp1 - 2.0 * f0 + fm1) + (3.0 / 44.0) * (fp2 - 2.0 * f0 + fm2);
+    }
+    orc_tridiag(n, alpha, b0, bn, r, y, ws);
+    const double fact = (y[0] + (alpha / gamma) * y[n - 1]) / (1.0 + vz);
+    for (int j = 0; j < n; j++) o[j] = scale * (y[j] - fact * z[j]);
+    free(r);
+    free(y);
+    free(ws);
+  }
+  free(z);
+  return CSS_OK;
+}

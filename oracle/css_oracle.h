@@ -54,6 +54,9 @@ int orc_dbyd1_dt0(const double *x, double *dxdy, const double *bdat1,
 int orc_compact_lines(const double *x, double *dx, int n, int nlines, int order, int lphys, int rphys,
                       int bdry, const double *bc_lo, const double *bc_hi, const double *halo_lo,
                       const double *halo_hi, double dnum, double scale);
+/* cyclic (Sherman-Morrison) compact derivative of whole periodic lines: the
+ * phi extension css_dbydp_cyclic; x, dx: nlines x n, line-contiguous */
+int orc_cyclic_lines(const double *x, double *dx, int n, int nlines, int order, double dnum);
 /* curl of A (VectorCurlA + Compute_B boundary zeroing): b = curl(a), 3 fields */
 int orc_curl_b(orc_ctx *c, const double *a, double *b);
 /* diagnostics of vars0, same outputs as css_scalars / css_step_size /

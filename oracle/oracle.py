@@ -55,6 +55,7 @@ def lib():
         L.orc_rain_fields.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.orc_set_ash_slices.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double]
         L.orc_build_squalls.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_cyclic_lines.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
         _LIB = L
     return _LIB
 
@@ -232,3 +233,23 @@ def compact_lines(x, order=1, lphys=True, rphys=True, bdry=1, bc_lo=None, bc_hi=
                                    int(bdry), _ptr(vec(bc_lo, 1)), _ptr(vec(bc_hi, 1)), _ptr(vec(halo_lo, 4)),
                                    _ptr(vec(halo_hi, 4)), float(dnum), float(scale)))
     return out.reshape(x.shape)
+
+
+def cyclic_lines(x, order=1, dnum=1.0):
+    """Cyclic compact derivative along the last axis (orc_cyclic_lines):
+    every line periodic, Sherman-Morrison on the cyclic tridiagonal system."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    n = x.shape[-1]
+    lines = x.reshape(-1, n)
+    out = np.zeros_like(lines)
+    _check(lib().orc_cyclic_lines(_ptr(lines), _ptr(out), n, lines.shape[0], int(order), float(dnum)))
+    return out.reshape(x.shape)
+
+
+def dbydp_cyclic(p, field, order=1):
+    """The cyclic phi derivative of one field (nr, nphi, nth) of run p, the
+    oracle of css_dbydp_cyclic: lines along phi, dnum = 1/dphi."""
+    f = np.ascontiguousarray(np.moveaxis(np.asarray(field, dtype=np.float64), 1, 2))  # (nr, nth, nphi)
+    dphi = (p.phi2 - p.phi1) / p.nphi
+    d = cyclic_lines(f, order, 1.0 / dphi)
+    return np.ascontiguousarray(np.moveaxis(d, 2, 1))

@@ -24,7 +24,11 @@ def test_shell_specs_follow_the_study_ranges():
         assert E.NR_RANGE[0] <= s["nr"] <= E.NR_RANGE[1]
         assert E.NTH_RANGE[0] <= s["nth"] <= E.NTH_RANGE[1] and s["nth"] % 16 == 0
         assert E.NPHI_RANGE[0] <= s["nphi"] <= E.NPHI_RANGE[1] and s["nphi"] % 16 == 0
-        assert 1e4 <= s["ra"] <= 1e6 and E.RO_RANGE[0] <= s["ro"] <= E.RO_RANGE[1]
+        assert 1e4 <= s["ra"] <= 1e6 and 0.3 <= s["ro"] <= 3.0
+        if s["magnetic"]:
+            assert E.PM_RANGE[0] <= s["pm"] <= E.PM_RANGE[1]
+        else:
+            assert s["pm"] is None
         nnr, nnt, nnp = s["decomp"]
         assert nnr >= 2 and nnt >= 2 and nnp >= 3
         for n, nb in ((s["nr"], nnr), (s["nth"], nnt), (s["nphi"], nnp)):
@@ -76,6 +80,66 @@ def test_lpt_partition_over_two_gloo_ranks():
         assert p.exitcode == 0
     a, b = set(got[0]), set(got[1])
     assert not (a & b) and a | b == set(range(48))
+
+
+TINY = [  # oracle-sized members: blocks of 10 points
+    {"nr": 20, "nth": 20, "nphi": 30, "ra": 1e5, "ro": 0.5, "magnetic": False, "pm": None, "decomp": (2, 2, 3)},
+    {"nr": 20, "nth": 20, "nphi": 30, "ra": 3e5, "ro": 1.5, "magnetic": True, "pm": 3.0, "decomp": (2, 2, 3)},
+    {"nr": 20, "nth": 30, "nphi": 40, "ra": 1e4, "ro": 2.5, "magnetic": False, "pm": None, "decomp": (2, 3, 4)},
+    {"nr": 30, "nth": 20, "nphi": 30, "ra": 2e4, "ro": 0.4, "magnetic": True, "pm": 1.2, "decomp": (3, 2, 3)},
+]
+
+
+def _oracle_rank_main(rank, world, port, out):
+    """One rank of a CPU ensemble run: LPT share of TINY, each member stepped
+    through the oracle; the final states gathered on rank 0."""
+    import torch.distributed as dist
+    from oracle import oracle as O
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    O.set_threads(2)
+    mine = E.lpt_partition([E.member_cost(s) for s in TINY], world)[rank]
+    states = {}
+    for i in mine:
+        p, prof, v0, dt = E.build_member(TINY[i], seed=100 + i)
+        orc = O.Oracle(p, prof)
+        states[i] = orc.step(v0, dt, 3)
+        orc.close()
+    got = [None] * world
+    dist.all_gather_object(got, states)
+    if rank == 0:
+        out.put(got)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_ensemble_stepped_over_two_gloo_ranks_through_the_oracle():
+    """Each of two gloo ranks steps its LPT share of the members (3 RK4
+    steps, the FP64 oracle); every member comes back once and equals the
+    same member stepped in one process."""
+    import multiprocessing as mp
+    import socket
+    from oracle import oracle as O
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_oracle_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    got = q.get(timeout=600)
+    for p in procs:
+        p.join(timeout=120)
+        assert p.exitcode == 0
+    assert not (set(got[0]) & set(got[1])) and set(got[0]) | set(got[1]) == set(range(len(TINY)))
+    states = {**got[0], **got[1]}
+    for i, spec in enumerate(TINY):
+        p, prof, v0, dt = E.build_member(spec, seed=100 + i)
+        want = O.Oracle(p, prof).step(v0, dt, 3)
+        assert np.array_equal(states[i], want), i
 
 
 # ---------------------------------------------------------------------------
@@ -176,4 +240,47 @@ def test_every_tile_variant_gives_the_same_bits(gpu_available, spec):
             sim.upload(v0)
             sim.step_rk4(dt, 2)
             assert np.array_equal(sim.download(), want), (tl, pers)
+            sim.close()
+
+
+MIX = SMALL + [  # a member on 32^3 blocks (the two-pass stage for FP64)
+    {"nr": 64, "nth": 64, "nphi": 96, "ra": 1e5, "ro": 0.8, "magnetic": True, "pm": 2.5, "decomp": (2, 2, 3)},
+]
+
+
+@pytest.mark.gpu
+def test_ensemble_200_steps_fp64_and_mixed_against_each_member_alone(gpu_available):
+    """200 steps of the ensemble, each member checked against its own
+    unbatched FP64 run: the FP64 ensemble bit for bit, the mixed-precision
+    ensemble (FP32 stage states) within the mixed form's bounds (rho and s
+    1e-6, velocities and A 1e-3 of each field's size, tests/test_mixed.py)."""
+    from css_b200.context import Simulation
+    n = 200
+    alone = []
+    for i, spec in enumerate(MIX):
+        p, prof, v0, dt = E.build_member(spec, seed=31 + i)
+        sim = Simulation(p, prof)
+        sim.upload(v0)
+        sim.step_rk4(dt, n)
+        alone.append(sim.download())
+        sim.close()
+    for precision in (0, 1):
+        members = [E.build_member(spec, seed=31 + i, precision=precision) for i, spec in enumerate(MIX)]
+        sims = [Simulation(p, prof) for p, prof, _, _ in members]
+        for sim, (_, _, v0, _) in zip(sims, members):
+            sim.upload(v0)
+        ens = E.Ensemble(sims)
+        ens.step([m[3] for m in members], n)
+        for k, (sim, ref) in enumerate(zip(sims, alone)):
+            got = sim.download()
+            assert np.isfinite(got).all()
+            if precision == 0:
+                assert np.array_equal(got, ref), k
+            else:
+                for iv in range(got.shape[0]):
+                    err = np.abs(got[iv] - ref[iv]).max() / np.abs(ref[iv]).max()
+                    bar = 1e-6 if iv in (0, 4) else 1e-3
+                    assert err < bar, (k, iv, err)
+        ens.close()
+        for sim in sims:
             sim.close()
