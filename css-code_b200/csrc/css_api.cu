@@ -69,6 +69,7 @@ struct css_ctx {
   double *tbuf;                     // temperature of the current stage input
   double *rtw = nullptr;            // two-pass stage: zero-datum d(rho)/dtheta on the theta-wall blocks
   double *cyc = nullptr;            // cyclic phi derivative tables, per order: w, piv, z (nphi each), v.z
+  double *bg2 = nullptr;            // mixed precision: rho and s backgrounds, [2][nr][nth]
   PlaneMaps pmaps[4];               // two-pass stage: TMA maps of v0, vA, vB and bf (plane kernel)
   SlabMaps smaps[5];                // the same for the stage kernel's slabs, then rtw
   double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
@@ -257,7 +258,7 @@ extern "C" void css_destroy(css_ctx *c) {
   if (!c) return;
   cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo); cudaFree(c->resp);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
-  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf); cudaFree(c->rtw); cudaFree(c->cyc);
+  cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf); cudaFree(c->rtw); cudaFree(c->cyc); cudaFree(c->bg2);
   cudaFree(c->lapbuf); cudaFree(c->lapface); cudaFree(c->radbuf); cudaFree(c->radface);
   cudaFree(c->io); cudaFree(c->io_part); cudaFree(c->rain); cudaFree(c->ash_slices); cudaFree(c->ashv);
   cudaFree(c->squalls);
@@ -853,6 +854,11 @@ extern "C" int css_create(const css_params *pp, const double *prof, css_ctx **ou
                 (p.time_stepper == 4 || p.time_stepper == 0) && !p.laplacian && !p.do_radheat && !p.top_inout &&
                 !p.bot_inout && !p.bottom_specified;
   if (c->fused_ok) ALLOC(c->rtw, (size_t)nr * nphi * 2 * 32 * sizeof(double));
+  if (p.precision == 1) {  // backgrounds of the FP32 stage states, refreshed at every upload
+    ALLOC(c->bg2, 2 * (size_t)nr * nth * sizeof(double));
+    cudaMemset(c->bg2, 0, 2 * (size_t)nr * nth * sizeof(double));
+    c->g.bg2 = c->bg2;
+  }
   {  // cyclic phi derivative tables (css_dbydp_cyclic)
     const size_t per = 3 * (size_t)nphi + 1;
     std::vector<double> CY(2 * per);
@@ -1332,9 +1338,32 @@ static int step_stages(css_ctx *c, double dt) {
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
+// phi means of rho and s at every (r, theta): the backgrounds about which
+// the mixed path stores its FP32 stage states (one thread per (r, theta),
+// phi summed in order)
+__global__ void k_phi_mean(CssGeo g, const double *__restrict__ v, double *__restrict__ bg2) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x, nrt = (size_t)g.nr * g.nth;
+  if (k >= nrt) return;
+  const int t = (int)(k % g.nth), r = (int)(k / g.nth);
+  const size_t n = (size_t)g.ncell;
+  double a = 0.0, b = 0.0;
+  for (int p = 0; p < g.nphi; p++) {
+    const size_t id = css_idx(g, t, p, r);
+    a += __ldg(v + id);
+    b += __ldg(v + 4 * n + id);
+  }
+  bg2[k] = a / g.nphi;
+  bg2[nrt + k] = b / g.nphi;
+}
+
 extern "C" int css_upload_state(css_ctx *c, const double *vars) {
   if (!c || !vars) { set_err("css_upload_state: NULL"); return CSS_ERR_ARG; }
   CUDA_TRY(cudaMemcpyAsync(c->v0, vars, c->ncell * c->nv * 8, cudaMemcpyHostToDevice, c->stream));
+  if (c->bg2) {
+    const size_t nrt = (size_t)c->p.nr * c->p.nth;
+    k_phi_mean<<<(unsigned)((nrt + 127) / 128), 128, 0, c->stream>>>(c->g, c->v0, c->bg2);
+    if (int rc = check_launch(c)) return rc;
+  }
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return CSS_OK;
 }

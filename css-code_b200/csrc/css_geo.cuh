@@ -29,6 +29,10 @@ struct CssGeo {
   const int *rblk;          // radial block index of each global ir
   const double *resp_r;     // [r block][lo|hi][tstride]: unit response of d/dr to the face datum of rho
   const double *resp_t;     // [theta block][lo|hi][tstride]: the same for d/dtheta of rho (ibct(1))
+  // mixed precision: backgrounds of rho and s about which FP32 stage states
+  // are stored, [2][nr][nth] (phi means of the state last uploaded); NULL
+  // for FP64 runs
+  const double *bg2;
   // radial profiles (length nr)
   const double *r_ind, *r_inv, *dr_ind, *dxdr, *d2xdr2, *rhor, *sr, *grav, *ks, *dlnks, *eps, *dspeed;
   const double *mur, *dlnmu;  // viscosity and its log-derivative (explicit-viscosity path)

@@ -47,18 +47,25 @@ __device__ __forceinline__ double dnum_d2_theta(const CssGeo &g, int ir) {
 }
 
 // A stage state is stored either as FP64 values (the FP64 path, and vars0)
-// or as FP32 perturbations of rho and s about the background rhor(r), sr(r)
-// (the mixed path; the other fields are plain FP32).  st_val returns the
-// FP64 value: the stored number, plus the background when it is FP32 and a
-// background profile is given.
+// or as FP32 perturbations of rho and s about a background that depends on
+// r and theta (CssGeo::bg2: the phi means of the state last uploaded; the
+// mixed path, the other fields plain FP32).  st_val returns the FP64 value:
+// the stored number, plus the background at (r, theta) -- bidx = r*nth +
+// theta -- when it is FP32 and a background is given.
 template <typename TS>
-__device__ __forceinline__ double st_val(const TS *p, size_t off, const double *mean, int r) {
+__device__ __forceinline__ double st_val(const TS *p, size_t off, const double *mean, size_t bidx) {
   double x = (double)__ldg(p + off);
   if constexpr (sizeof(TS) == 4) {
-    if (mean) x += mean[r];
+    if (mean) x += mean[bidx];
   }
   return x;
 }
+// backgrounds of rho and s for the FP32 stage states (2-D, nr x nth)
+__device__ __forceinline__ const double *bg_rho(const CssGeo &g) { return g.bg2; }
+__device__ __forceinline__ const double *bg_s(const CssGeo &g) {
+  return g.bg2 ? g.bg2 + (size_t)g.nr * g.nth : nullptr;
+}
+__device__ __forceinline__ size_t bgi(const CssGeo &g, int r, int t) { return (size_t)r * g.nth + t; }
 
 // the stored form of a new stage value (inverse of st_val)
 template <typename TO>
@@ -151,7 +158,7 @@ __device__ __forceinline__ void tile_theta(const CssGeo &g, const TS *__restrict
     int l = idx / w, jj = idx - l * w;
     int gt = t0 + jj - 4, gp = pb + l;
     if (gt < 0 || gt >= g.nth || gp >= g.nphi) continue;
-    S[l * SR + jj] = st_val(fp, (size_t)gp * g.nth + gt, mean, ir);
+    S[l * SR + jj] = st_val(fp, (size_t)gp * g.nth + gt, mean, bgi(g, ir, gt));
   }
 }
 
@@ -167,7 +174,7 @@ __device__ __forceinline__ void tile_phi(const CssGeo &g, const TS *__restrict__
     if (gp < 0) gp += g.nphi;
     else if (gp >= g.nphi) gp -= g.nphi;
     if (gt >= g.nth) continue;
-    S[jj * SR + l] = st_val(fp, (size_t)gp * g.nth + gt, mean, ir);
+    S[jj * SR + l] = st_val(fp, (size_t)gp * g.nth + gt, mean, bgi(g, ir, gt));
   }
 }
 
@@ -182,7 +189,7 @@ __device__ __forceinline__ void tile_r(const CssGeo &g, const TS *__restrict__ f
     int jj = idx / TL, l = idx - jj * TL;
     int gr = r0 + jj - 4;
     if (gr < 0 || gr >= g.nr || tb + l >= g.nth) continue;
-    S[jj * SR + l] = st_val(fp, (size_t)gr * ps + l, mean, gr);
+    S[jj * SR + l] = st_val(fp, (size_t)gr * ps + l, mean, bgi(g, gr, tb + l));
   }
 }
 
@@ -202,8 +209,8 @@ __device__ __forceinline__ void tiles_ct(const CssGeo &g, const TS *const *f, do
                                          int a0, int lb, int fixed, const double *const *mp = nullptr) {
   constexpr int W = MT + 8, N = TLC * W, IT = (N + NT - 1) / NT;
   double val[NF][IT];
-  int so[IT], rr[IT];
-  size_t go[IT];
+  int so[IT];
+  size_t go[IT], bb[IT];
 #pragma unroll
   for (int k = 0; k < IT; k++) {
     const int idx = threadIdx.x + k * NT;
@@ -231,14 +238,18 @@ __device__ __forceinline__ void tiles_ct(const CssGeo &g, const TS *const *f, do
       off = plane(g, gr < 0 ? 0 : gr) + (size_t)fixed * g.nth + gt;
       so[k] = jj * SR + l;
     }
-    rr[k] = DIR == 0 ? (ok ? a0 + jj - 4 : 0) : fixed;
+    {
+      const int r_ = DIR == 0 ? (ok ? a0 + jj - 4 : 0) : fixed;
+      const int t_ = DIR == 1 ? a0 + jj - 4 : lb + l;
+      bb[k] = ok ? bgi(g, r_, t_) : 0;
+    }
     if (!ok) so[k] = -1;
     go[k] = ok ? off : 0;
   }
 #pragma unroll
   for (int q = 0; q < NF; q++)
 #pragma unroll
-    for (int k = 0; k < IT; k++) val[q][k] = (so[k] >= 0) ? st_val(f[q], go[k], mp ? mp[q] : nullptr, rr[k]) : 0.0;
+    for (int k = 0; k < IT; k++) val[q][k] = (so[k] >= 0) ? st_val(f[q], go[k], mp ? mp[q] : nullptr, bb[k]) : 0.0;
 #pragma unroll
   for (int q = 0; q < NF; q++)
 #pragma unroll
@@ -290,7 +301,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const TV *__restr
   double *O = H + (size_t)nh * TL * SR;
   double *Tb = O + (size_t)nd * TL * SO;
   const TV *fs[4] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n};
-  const double *ms[4] = {nullptr, nullptr, nullptr, g.sr};
+  const double *ms[4] = {nullptr, nullptr, nullptr, bg_s(g)};
   const double *fb[2] = {bf + n, bf + 2 * n};
   if constexpr (MT > 0 && TLC > 0) {
     tiles_ct<4, MT, TLC, 1>(g, fs, H, (size_t)TL * SR, SR, t0, pb, ir, ms);
@@ -343,7 +354,7 @@ __global__ void __launch_bounds__(128) k_theta_terms(CssGeo g, const TV *__restr
     const int l = pt / m, j = pt - l * m;
     const bool ok = pt < TL * m && pb + l < g.nphi;
     const size_t id = pl + (size_t)(pb + l) * g.nth + t0 + j;
-    rho_[k] = ok ? st_val(cur, id, g.rhor, ir) : 1.0;
+    rho_[k] = ok ? st_val(cur, id, bg_rho(g), bgi(g, ir, t0 + j)) : 1.0;
     bt_in[k] = (ok && mag) ? __ldg(bf + id) : 0.0;
   }
 #pragma unroll
@@ -567,7 +578,7 @@ __global__ void __launch_bounds__(128) k_phi_terms(CssGeo g, const TV *__restric
     }
   }
   const TV *fs[5] = {cur, cur + 2 * n, cur + n, cur + 3 * n, cur + 4 * n};
-  const double *ms[5] = {g.rhor, nullptr, nullptr, nullptr, g.sr};
+  const double *ms[5] = {bg_rho(g), nullptr, nullptr, nullptr, bg_s(g)};
   const double *fb[2] = {bf, bf + 2 * n};
   if constexpr (MT > 0 && TLC > 0) {
     tiles_ct<5, MT, TLC, 2>(g, fs, H, HS, SR, p0, tb, ir, ms);
@@ -774,7 +785,7 @@ __device__ __forceinline__ void radial_tile(const CssGeo &g, const TV *__restric
     }
   }
   const TV *fs[5] = {cur + n, cur + 2 * n, cur + 3 * n, cur + 4 * n, cur};
-  const double *ms[5] = {nullptr, nullptr, nullptr, g.sr, g.rhor};
+  const double *ms[5] = {nullptr, nullptr, nullptr, bg_s(g), bg_rho(g)};
   const double *fb[2] = {bf, bf + n};
   if constexpr (MT > 0 && TLC > 0) {
     tiles_ct<5, MT, TLC, 0>(g, fs, H, HS, SR, r0, tb, ip, ms);
@@ -999,10 +1010,10 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
   }
   if constexpr (MT > 0 && TLC > 0) {
     const TS *f1[1] = {cur};
-    const double *m1[1] = {g.rhor};
+    const double *m1[1] = {bg_rho(g)};
     tiles_ct<1, MT, TLC, 1>(g, f1, H, 0, SR, t0, pb, ir, m1);
   } else {
-    tile_theta<MT, TLC>(g, cur, H, SR, t0, m, pb, TL, ir, g.rhor);
+    tile_theta<MT, TLC>(g, cur, H, SR, t0, m, pb, TL, ir, bg_rho(g));
   }
   const int bdry = g.ibct[1];
   stage_table(g, 1, bt, 1, bdry, m, Tb);
@@ -1044,7 +1055,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
       itk[k] = t0 + j;
       idk[k] = pl + (size_t)(pb + l) * g.nth + t0 + j;
       if (okk[k]) {
-        wk[k] = st_val(cur + n, idk[k], nullptr, ir);
+        wk[k] = st_val(cur + n, idk[k], nullptr, 0);
         tk[k] = __ldg(tbuf + idk[k]);
         d0k[k] = dv[idk[k]];
         d1k[k] = dv[n + idk[k]];
@@ -1080,7 +1091,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
       double dd[PPT], aa[PPT], ss[PPT], cc[PPT];
       const bool need_s = stage <= 4 ? !(stage == 1 && !g.sldiffusion) : (stage == 6 && dsld != 0.0);
       const bool need_c = stage >= 5 && cb != 0.0;
-      const double *bg = iv == 0 ? g.rhor : (iv == 4 ? g.sr : nullptr);  // background of an FP32 stage state
+      const double *bg = iv == 0 ? bg_rho(g) : (iv == 4 ? bg_s(g) : nullptr);  // background of an FP32 stage state
 #pragma unroll
       for (int k = 0; k < PPT; k++) {
         if (!okk[k]) continue;
@@ -1088,7 +1099,7 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
         dd[k] = (iv == 0) ? d0k[k] : (iv == 1) ? d1k[k] : dv[q];
         aa[k] = v0[q];
         ss[k] = need_s ? vs[q] : 0.0;
-        cc[k] = need_c ? st_val(cur + (size_t)iv * n, idk[k], bg, ir) : 0.0;
+        cc[k] = need_c ? st_val(cur + (size_t)iv * n, idk[k], bg, bgi(g, ir, itk[k])) : 0.0;
       }
 #pragma unroll
       for (int k = 0; k < PPT; k++) {
@@ -1141,7 +1152,12 @@ __global__ void __launch_bounds__(128) k_rhot_update(CssGeo g, const TS *__restr
           }
         }
         if (!isfinite(o)) bad = 1;
-        nx[q] = st_store<TO>(o, iv == 0 ? g.rhor[ir] : (iv == 4 ? g.sr[ir] : 0.0));
+        double bgv = 0.0;
+        if constexpr (sizeof(TO) == 4) {
+          if (iv == 0) bgv = bg_rho(g)[bgi(g, ir, itk[k])];
+          else if (iv == 4) bgv = bg_s(g)[bgi(g, ir, itk[k])];
+        }
+        nx[q] = st_store<TO>(o, bgv);
       }
     }
   }

@@ -1,14 +1,20 @@
 """Mixed precision (precision = 1): the stage states U1..U3 of every RK4 step
-are stored in FP32, rho and s as perturbations about the background
-rhor(r), sr(r); vars0, the RK accumulator, the tendency, the tables and all
-arithmetic stay FP64.  Its error against the FP64 oracle is the stated
-error of the mixed path, normwise per field (max|mixed - oracle| /
-max|oracle|), measured after 1 and 100 steps of the 64x64x128 workload:
-rho and s stay within 1e-6 (observed <= 9e-8), the velocities within 1e-3
-(observed <= 1.4e-4: they start at rest and grow from a residual of
-hydrostatic balance, so the FP32 rounding of the stage perturbations --
-the initial rho departs from the background by up to 7% -- weighs more on
-them).  MHD after 5 steps: velocities within 1e-4, A within 1e-6."""
+are stored in FP32, rho and s as perturbations about backgrounds that depend
+on r and theta (the phi means of the state at its last upload); vars0, the
+RK accumulator, the tendency, the tables and all arithmetic stay FP64.  Its
+error against FP64 is the stated error of the mixed path, normwise per
+field (max|mixed - fp64| / max|fp64|):
+
+- from the seeded 64x64x128 state, 1 and 100 steps against the FP64 oracle:
+  rho and s within 1e-6 (observed 1e-9 / 1.2e-8); the velocities, which start
+  at rest and after 100 steps are still small residuals of hydrostatic
+  balance, within 1e-5 (observed 6.1e-6);
+- from a developed flow (2000 FP64 steps first, |u| up to 0.03), 100 mixed
+  steps against 100 FP64 steps on the device: every field within 1e-6
+  (observed 2.6e-7 at most, u_r); the FP64 device path itself is held to the
+  oracle at 1e-10 over 100 steps elsewhere (tests/test_gpu_parity.py);
+- MHD 32x64x128: 5 steps from the seeded state against the oracle, every
+  field within 1e-6, and 100 steps of a developed flow within 1e-6."""
 import numpy as np
 import pytest
 
@@ -26,39 +32,50 @@ def cfg1():
     return problem.build("hydro-64x64x128")
 
 
-@pytest.mark.parametrize("nsteps", [1, 100])
-def test_mixed_state_within_stated_error_of_fp64_oracle(gpu_available, cfg1, nsteps):
+def run(p, prof, v0, dt, nsteps, precision):
     from css_b200.context import Simulation
-    from oracle import oracle as O
-    p, prof, v0, dt, _ = cfg1
-    pm = p.copy()
-    pm.precision = 1
-    sim = Simulation(pm, prof)
+    q = p.copy()
+    q.precision = precision
+    sim = Simulation(q, prof)
     sim.upload(v0)
     sim.step_rk4(dt, nsteps)
-    got = sim.download()
+    out = sim.download()
+    sim.close()
+    return out
+
+
+@pytest.mark.parametrize("nsteps", [1, 100])
+def test_mixed_state_within_stated_error_of_fp64_oracle(gpu_available, cfg1, nsteps):
+    from oracle import oracle as O
+    p, prof, v0, dt, _ = cfg1
+    got = run(p, prof, v0, dt, nsteps, 1)
     want = O.Oracle(p, prof).step(v0, dt, nsteps)
     err = fieldwise(got, want)
     print("mixed vs FP64 oracle after %d steps:" % nsteps, ["%.2e" % e for e in err])
     assert max(err[0], err[4]) < 1e-6, err
-    assert max(err[1:4]) < 1e-3, err
+    assert max(err[1:4]) < 1e-5, err
     # and it is not the FP64 path: the FP32 stage states leave a trace
-    sim64 = Simulation(p, prof)
-    sim64.upload(v0)
-    sim64.step_rk4(dt, nsteps)
-    assert not np.array_equal(sim64.download(), got)
+    assert not np.array_equal(run(p, prof, v0, dt, nsteps, 0), got)
+
+
+@pytest.mark.parametrize("mag", [False, True])
+def test_mixed_developed_flow_every_field_within_1e6(gpu_available, mag):
+    if mag:
+        p, prof, v0, dt, _ = problem.build((32, 64, 128), magnetic=True)
+    else:
+        p, prof, v0, dt, _ = problem.build("hydro-64x64x128")
+    developed = run(p, prof, v0, dt, 2000, 0)
+    assert np.abs(developed[1:4]).max() > 1e-3  # a flow, not a resting state
+    want = run(p, prof, developed, dt, 100, 0)
+    got = run(p, prof, developed, dt, 100, 1)
+    err = fieldwise(got, want)
+    print("mixed vs FP64, 100 steps of a developed flow:", ["%.2e" % e for e in err])
+    assert max(err) < 1e-6, err
 
 
 def test_mixed_magnetic_runs_within_stated_error(gpu_available):
-    from css_b200.context import Simulation
     from oracle import oracle as O
     p, prof, v0, dt, _ = problem.build((32, 64, 128), magnetic=True)
-    pm = p.copy()
-    pm.precision = 1
-    sim = Simulation(pm, prof)
-    sim.upload(v0)
-    sim.step_rk4(dt, 5)
-    err = fieldwise(sim.download(), O.Oracle(p, prof).step(v0, dt, 5))
+    err = fieldwise(run(p, prof, v0, dt, 5, 1), O.Oracle(p, prof).step(v0, dt, 5))
     print("mixed MHD vs FP64 oracle after 5 steps:", ["%.2e" % e for e in err])
-    assert max(err[0], err[4]) < 1e-6 and max(err[5:]) < 1e-6, err
-    assert max(err[1:4]) < 1e-4, err
+    assert max(err) < 1e-6, err
