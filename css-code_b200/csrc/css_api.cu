@@ -70,6 +70,10 @@ struct css_ctx {
   double *rtw = nullptr;            // two-pass stage: zero-datum d(rho)/dtheta on the theta-wall blocks
   double *cyc = nullptr;            // cyclic phi derivative tables, per order: w, piv, z (nphi each), v.z
   double *bg2 = nullptr;            // mixed precision: rho and s backgrounds, [2][nr][nth]
+  // adjoints of css_deriv (torch backward): dense block operators per
+  // (direction, order, bdry), built on first use, and their block offsets
+  double *adjM[3][2][5] = {};
+  int *adjOff[3][2][5] = {};
   PlaneMaps pmaps[4];               // two-pass stage: TMA maps of v0, vA, vB and bf (plane kernel)
   SlabMaps smaps[5];                // the same for the stage kernel's slabs, then rtw
   double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
@@ -258,6 +262,9 @@ extern "C" void css_destroy(css_ctx *c) {
   if (!c) return;
   cudaFree(c->tab); cudaFree(c->prof); cudaFree(c->theta_prof); cudaFree(c->rblk); cudaFree(c->sld_geo); cudaFree(c->resp);
   cudaFree(c->v0); cudaFree(c->vA); cudaFree(c->vB); cudaFree(c->dv); cudaFree(c->vs);
+  for (int d = 0; d < 3; d++)
+    for (int o = 0; o < 2; o++)
+      for (int b = 0; b < 5; b++) { cudaFree(c->adjM[d][o][b]); cudaFree(c->adjOff[d][o][b]); }
   cudaFree(c->bf); cudaFree(c->vcc); cudaFree(c->cda); cudaFree(c->flag); cudaFree(c->tbuf); cudaFree(c->rtw); cudaFree(c->cyc); cudaFree(c->bg2);
   cudaFree(c->lapbuf); cudaFree(c->lapface); cudaFree(c->radbuf); cudaFree(c->radface);
   cudaFree(c->io); cudaFree(c->io_part); cudaFree(c->rain); cudaFree(c->ash_slices); cudaFree(c->ashv);
@@ -1516,6 +1523,66 @@ extern "C" int css_dbydp_cyclic(css_ctx *c, const double *x, double *dx, int ord
   CUDA_TRY(cudaMemcpyAsync(dx, c->dv, n * 8, cudaMemcpyDeviceToHost, c->stream));
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return CSS_OK;
+}
+
+// dense block operators of css_deriv along dir (zero boundary data): block
+// b's m x (m + 8) matrix is the solver applied, on the host, to each unit
+// input of the block and its halos, with the run's tables and closures
+static int adjoint_mats(css_ctx *c, int dir, int order, int bdry) {
+  const int ob = dir == 2 ? 0 : bdry;
+  if (c->adjM[dir][order - 1][ob]) return CSS_OK;
+  const CssDir &D = c->g.d[dir];
+  std::vector<double> M;
+  std::vector<int> off(D.nb);
+  for (int b = 0; b < D.nb; b++) {
+    const int m = D.size[b], ts = m + 2, w = m + 8;
+    off[b] = (int)M.size();
+    M.resize(M.size() + (size_t)m * w);
+    std::vector<double> T(3 * (size_t)ts, 0.0), x(w), o(m);
+    double *g1 = T.data(), *g2 = g1 + ts, *g3 = g2 + ts;
+    if (dir == 2) tab_p(m, order == 1 ? 1.0 / 3.0 : 2.0 / 11.0, g1, g2, g3);
+    else if (order == 1) tab_d1(m, D.lphys[b], D.rphys[b], bdry, g1, g2, g3);
+    else tab_d2(m, D.lphys[b], D.rphys[b], bdry, g1, g2, g3);
+    const int dtype = dir == 2 ? 3 : (D.lphys[b] ? (D.rphys[b] ? 0 : 2) : (D.rphys[b] ? 1 : 3));
+    const double dn = D.dnum[b], sc = order == 1 ? dn : dn * dn;
+    for (int col = 0; col < w; col++) {
+      std::fill(x.begin(), x.end(), 0.0);
+      x[col] = 1.0;
+      if (order == 1)
+        line_solve_a<1>(x.data() + 4, StridedIn{1}, m, dtype, ob, 0.0, 0.0, T.data(), ts, dn, sc, dir == 2,
+                        o.data(), StridedOut{1});
+      else
+        line_solve_a<2>(x.data() + 4, StridedIn{1}, m, dtype, ob, 0.0, 0.0, T.data(), ts, dn, sc, dir == 2,
+                        o.data(), StridedOut{1});
+      for (int q = 0; q < m; q++) M[(size_t)off[b] + (size_t)q * w + col] = o[q];
+    }
+  }
+  double *dM = nullptr;
+  int *dO = nullptr;
+  if (cudaMalloc(&dM, M.size() * 8) != cudaSuccess || cudaMalloc(&dO, off.size() * sizeof(int)) != cudaSuccess) {
+    cudaFree(dM);
+    set_err("css_deriv_adjoint: device allocation failed");
+    return CSS_ERR_NOMEM;
+  }
+  CUDA_TRY(cudaMemcpy(dM, M.data(), M.size() * 8, cudaMemcpyHostToDevice));
+  CUDA_TRY(cudaMemcpy(dO, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice));
+  c->adjM[dir][order - 1][ob] = dM;
+  c->adjOff[dir][order - 1][ob] = dO;
+  return CSS_OK;
+}
+
+extern "C" int css_deriv_adjoint_dev(css_ctx *c, int dir, int order, const double *g, double *gx, int bdry,
+                                     void *stream) {
+  if (!c || !g || !gx || dir < 0 || dir > 2 || order < 1 || order > 2 || bdry < 0 || bdry > 4 || g == gx) {
+    set_err("css_deriv_adjoint: bad argument");
+    return CSS_ERR_ARG;
+  }
+  if (int rc = adjoint_mats(c, dir, order, bdry)) return rc;
+  const int ob = dir == 2 ? 0 : bdry;
+  cudaStream_t st = stream ? (cudaStream_t)stream : c->stream;
+  k_deriv_adjoint<<<(unsigned)((c->ncell + 255) / 256), 256, 0, st>>>(c->g, dir, c->adjM[dir][order - 1][ob],
+                                                                       c->adjOff[dir][order - 1][ob], g, gx);
+  return check_launch(c);
 }
 
 extern "C" int css_deriv(css_ctx *c, int dir, int order, const double *x, double *dx, const double *bc_lo,

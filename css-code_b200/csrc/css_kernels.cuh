@@ -1929,8 +1929,6 @@ __global__ void __launch_bounds__(128) k_deriv_r(CssGeo g, const double *__restr
   }
 }
 
-// independent lines with explicit closures (css_compact_lines /
-// Dbyd1_dt0): one thread per line on global memory, lines contiguous.
 // Cyclic phi derivative of one field (css_dbydp_cyclic; an extension with
 // no counterpart in the reference, whose Dbydp closes each block with halo
 // rows, derivatives.f90:1480-1591): every whole phi line is periodic and
@@ -1978,6 +1976,51 @@ __global__ void k_dbydp_cyclic(CssGeo g, const double *__restrict__ x, double *_
   }
 }
 
+// Adjoint of the whole-field compact derivative along direction dir (the
+// backward of torch.ops.css.deriv): gx = D^T g with zero boundary data.
+// M holds every block's dense operator, rows = the block's m outputs,
+// columns = its m + 8 inputs (4 halo points below, the block, 4 above),
+// at M + off[b].  A point is an input of its own block and, within four
+// points of a block face, a halo input of the neighbouring block (phi
+// periodic), so gx at that point gathers one column of each: a fixed-order
+// sum, deterministic.  One thread per point.
+__global__ void k_deriv_adjoint(CssGeo g, int dir, const double *__restrict__ M, const int *__restrict__ off,
+                                const double *__restrict__ gin, double *__restrict__ gout) {
+  const size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (id >= (size_t)g.ncell) return;
+  const int it = (int)(id % g.nth), ip = (int)((id / g.nth) % g.nphi), ir = (int)(id / ((size_t)g.nth * g.nphi));
+  const CssDir &D = g.d[dir];
+  const int a = dir == 0 ? ir : (dir == 1 ? it : ip);
+  int b = 0;
+  while (b + 1 < D.nb && D.start[b + 1] <= a) b++;
+  const int i = a - D.start[b], m = D.size[b];
+  auto gat = [&](int aa) -> double {
+    return __ldg(gin + (dir == 0 ? css_idx(g, it, ip, aa) : (dir == 1 ? css_idx(g, aa, ip, ir) : css_idx(g, it, aa, ir))));
+  };
+  auto col = [&](int bb, int c) -> double {
+    const int mb = D.size[bb], s0 = D.start[bb];
+    const double *Mb = M + off[bb];
+    double acc = 0.0;
+    for (int q = 0; q < mb; q++) acc += __ldg(Mb + (size_t)q * (mb + 8) + c) * gat(s0 + q);
+    return acc;
+  };
+  double acc = col(b, i + 4);
+  const bool periodic = dir == 2;
+  if (i < 4) {
+    int bb = b - 1;
+    if (bb < 0 && periodic) bb = D.nb - 1;
+    if (bb >= 0) acc += col(bb, D.size[bb] + 4 + i);
+  }
+  if (i >= m - 4) {
+    int bb = b + 1;
+    if (bb >= D.nb && periodic) bb = 0;
+    if (bb < D.nb) acc += col(bb, i - (m - 4));
+  }
+  gout[id] = acc;
+}
+
+// independent lines with explicit closures (css_compact_lines /
+// Dbyd1_dt0): one thread per line on global memory, lines contiguous.
 __global__ void k_lines(const double *__restrict__ x, double *__restrict__ out, int n, int nlines, int order,
                         int dtype, int bdry, const double *__restrict__ bclo, const double *__restrict__ bchi,
                         const double *__restrict__ hlo, const double *__restrict__ hhi, const double *__restrict__ tab,

@@ -48,11 +48,11 @@ struct HaloD1 {
 // tiles).
 struct StridedIn {
   int s;
-  __device__ __forceinline__ int operator()(int j) const { return (j - 1) * s; }
+  __host__ __device__ __forceinline__ int operator()(int j) const { return (j - 1) * s; }
 };
 struct StridedOut {
   int s;
-  __device__ __forceinline__ int operator()(int j) const { return j * s; }
+  __host__ __device__ __forceinline__ int operator()(int j) const { return j * s; }
 };
 
 #define CSS_X(j) xb[xi(j)]
@@ -61,7 +61,7 @@ struct StridedOut {
 // per-thread scratch that aliases the output buffer).  Returns nothing; the
 // caller runs the sweeps.
 template <class X>
-__device__ __forceinline__ double d1_row_lo1(const double *__restrict__ xb, const X &xi, int dtype, int bdry, double bclo,
+__host__ __device__ __forceinline__ double d1_row_lo1(const double *__restrict__ xb, const X &xi, int dtype, int bdry, double bclo,
                                              double dnum, double row2) {
   if (dtype == 1 || dtype == 3) {
     return (-HaloD1::c1) * CSS_X(-3) + HaloD1::c2 * CSS_X(-2) + HaloD1::cnst * CSS_X(-1) +
@@ -79,7 +79,7 @@ __device__ __forceinline__ double d1_row_lo1(const double *__restrict__ xb, cons
 }
 
 template <class X>
-__device__ __forceinline__ double d1_row_lo2(const double *__restrict__ xb, const X &xi, int dtype) {
+__host__ __device__ __forceinline__ double d1_row_lo2(const double *__restrict__ xb, const X &xi, int dtype) {
   if (dtype == 1 || dtype == 3)
     return (7.0 / 9.0) * (CSS_X(3) - CSS_X(1)) + (1.0 / 36.0) * (CSS_X(4) - CSS_X(0));
   return (-43.0 / 96.0) * CSS_X(1) + (-5.0 / 6.0) * CSS_X(2) + (9.0 / 8.0) * CSS_X(3) + (1.0 / 6.0) * CSS_X(4) +
@@ -87,7 +87,7 @@ __device__ __forceinline__ double d1_row_lo2(const double *__restrict__ xb, cons
 }
 
 template <class X>
-__device__ __forceinline__ double d1_row_hi1(const double *__restrict__ xb, const X &xi, int m, int dtype) {  // row m-1
+__host__ __device__ __forceinline__ double d1_row_hi1(const double *__restrict__ xb, const X &xi, int m, int dtype) {  // row m-1
   if (dtype == 2 || dtype == 3)
     return HaloD1::r_c1 * (CSS_X(m) - CSS_X(m - 2)) + HaloD1::r_c2 * (CSS_X(m + 1) - CSS_X(m - 3));
   return (43.0 / 96.0) * CSS_X(m) + (5.0 / 6.0) * CSS_X(m - 1) + (-9.0 / 8.0) * CSS_X(m - 2) +
@@ -95,7 +95,7 @@ __device__ __forceinline__ double d1_row_hi1(const double *__restrict__ xb, cons
 }
 
 template <class X>
-__device__ __forceinline__ double d1_row_hi2(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bchi,
+__host__ __device__ __forceinline__ double d1_row_hi2(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bchi,
                                              double dnum, double rowm1) {  // row m
   if (dtype == 2 || dtype == 3)
     return HaloD1::r_c1 * CSS_X(m + 1) + HaloD1::r_cnst * CSS_X(m + 2) + HaloD1::r_c4 * CSS_X(m + 3) +
@@ -112,7 +112,7 @@ __device__ __forceinline__ double d1_row_hi2(const double *__restrict__ xb, cons
 }
 
 template <class X>
-__device__ __forceinline__ double d1_row_int(const double *__restrict__ xb, const X &xi, int j) {
+__host__ __device__ __forceinline__ double d1_row_int(const double *__restrict__ xb, const X &xi, int j) {
   return (7.0 / 9.0) * (CSS_X(j + 1) - CSS_X(j - 1)) + (1.0 / 36.0) * (CSS_X(j + 2) - CSS_X(j - 2));
 }
 
@@ -122,7 +122,7 @@ struct HaloD2 {
 };
 
 template <class X>
-__device__ __forceinline__ double d2_row_lo1(const double *__restrict__ xb, const X &xi, int dtype, int bdry, double bclo, double dnum) {
+__host__ __device__ __forceinline__ double d2_row_lo1(const double *__restrict__ xb, const X &xi, int dtype, int bdry, double bclo, double dnum) {
   if (dtype == 1 || dtype == 3) {
     double r = HaloD2::c3 * (2.0 * (CSS_X(-3) + CSS_X(3)) + (-27.0) * (CSS_X(-2) + CSS_X(2)) +
                              270.0 * (CSS_X(-1) + CSS_X(1)) + (-490.0) * CSS_X(0));
@@ -139,14 +139,14 @@ __device__ __forceinline__ double d2_row_lo1(const double *__restrict__ xb, cons
 }
 
 template <class X>
-__device__ __forceinline__ double d2_row_lo2(const double *__restrict__ xb, const X &xi, int dtype) {
+__host__ __device__ __forceinline__ double d2_row_lo2(const double *__restrict__ xb, const X &xi, int dtype) {
   if (dtype == 1 || dtype == 3)
     return HaloD2::c1 * (CSS_X(3) - 2.0 * CSS_X(2) + CSS_X(1)) + HaloD2::c2 * (CSS_X(0) - 2.0 * CSS_X(2) + CSS_X(4));
   return 1.2375 * CSS_X(1) + (-3.0) * CSS_X(2) + 2.325 * CSS_X(3) + (-0.6) * CSS_X(4) + 0.0375 * CSS_X(5);
 }
 
 template <class X>
-__device__ __forceinline__ double d2_row_hi1(const double *__restrict__ xb, const X &xi, int m, int dtype) {
+__host__ __device__ __forceinline__ double d2_row_hi1(const double *__restrict__ xb, const X &xi, int m, int dtype) {
   if (dtype == 2 || dtype == 3)
     return HaloD2::c1 * (CSS_X(m) - 2.0 * CSS_X(m - 1) + CSS_X(m - 2)) +
            HaloD2::c2 * (CSS_X(m - 3) - 2.0 * CSS_X(m - 1) + CSS_X(m + 1));
@@ -154,7 +154,7 @@ __device__ __forceinline__ double d2_row_hi1(const double *__restrict__ xb, cons
 }
 
 template <class X>
-__device__ __forceinline__ double d2_row_hi2(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bchi,
+__host__ __device__ __forceinline__ double d2_row_hi2(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bchi,
                                              double dnum) {
   if (dtype == 2 || dtype == 3) {
     double r = HaloD2::c1 * (CSS_X(m + 1) - 2.0 * CSS_X(m) + CSS_X(m - 1)) +
@@ -172,7 +172,7 @@ __device__ __forceinline__ double d2_row_hi2(const double *__restrict__ xb, cons
 }
 
 template <class X>
-__device__ __forceinline__ double d2_row_int(const double *__restrict__ xb, const X &xi, int j) {
+__host__ __device__ __forceinline__ double d2_row_int(const double *__restrict__ xb, const X &xi, int j) {
   return HaloD2::c1 * (CSS_X(j + 1) - 2.0 * CSS_X(j) + CSS_X(j - 1)) +
          HaloD2::c2 * (CSS_X(j - 2) - 2.0 * CSS_X(j) + CSS_X(j + 2));
 }
@@ -183,7 +183,7 @@ __device__ __forceinline__ double d2_row_int(const double *__restrict__ xb, cons
 // ob[oi(j-1)] receives scale * solution of row j; the forward values pass
 // through out on the way.
 template <int ORDER, class X, class O>
-__device__ __forceinline__ void line_solve_a(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bclo, double bchi,
+__host__ __device__ __forceinline__ void line_solve_a(const double *__restrict__ xb, const X &xi, int m, int dtype, int bdry, double bclo, double bchi,
                                              const double *__restrict__ G, int ts, double dnum, double scale,
                                              int phi, double *__restrict__ ob, const O &oi) {
   const double *g1 = G, *g2 = G + ts, *g3 = G + 2 * ts;

@@ -8,6 +8,9 @@ stream, the result in a new tensor of the input's dtype.  FP64 tensors are
 used as they are; FP32 tensors are computed in FP64 and the result rounded
 back.  Only a CUDA kernel is registered, so CPU tensors raise.  The
 ``dbydr`` ... ``d2bydp2`` functions below name the six reference routines.
+The op is differentiable in x: its backward is ``torch.ops.css.deriv_adjoint``
+(the transpose of the blocked operator, css_deriv_adjoint_dev); boundary
+data are treated as constants.
 
 Like the reference, the r derivatives of a non-uniform grid are returned in
 x-space (the caller multiplies by dxdr).  ``bdry`` is the reference's ibc
@@ -69,6 +72,44 @@ def deriv(x: torch.Tensor, ctx: int, direction: int, order: int, bc_lo: Optional
 @deriv.register_fake
 def _(x, ctx, direction, order, bc_lo, bc_hi, bdry):
     return torch.empty_like(x)
+
+
+@torch.library.custom_op("css::deriv_adjoint", mutates_args=(), device_types="cuda")
+def deriv_adjoint(g: torch.Tensor, ctx: int, direction: int, order: int, bdry: int) -> torch.Tensor:
+    """D^T g for the blocked compact derivative D of css::deriv (zero
+    boundary data): css_deriv_adjoint_dev on every leading index."""
+    gd = g.to(torch.float64).contiguous()
+    out = torch.empty_like(gd)
+    nb = 1
+    for d in gd.shape[:-3]:
+        nb *= d
+    gs, os_ = gd.reshape(nb, *gd.shape[-3:]), out.view(nb, *gd.shape[-3:])
+    stream = ctypes.c_void_p(torch.cuda.current_stream(gd.device).cuda_stream)
+    h = ctypes.c_void_p(ctx)
+    for k in range(nb):
+        check(_lib.lib().css_deriv_adjoint_dev(h, int(direction), int(order), _vp(gs[k]), _vp(os_[k]), int(bdry),
+                                               stream))
+    return out.to(g.dtype)
+
+
+@deriv_adjoint.register_fake
+def _(g, ctx, direction, order, bdry):
+    return torch.empty_like(g)
+
+
+def _deriv_setup(ctx, inputs, output):
+    x, c, direction, order, bc_lo, bc_hi, bdry = inputs
+    ctx.args = (c, direction, order, bdry)
+
+
+def _deriv_backward(ctx, grad):
+    # the derivative is affine in x (the boundary data add a constant), so
+    # its gradient is the adjoint; the boundary data are held fixed
+    c, direction, order, bdry = ctx.args
+    return torch.ops.css.deriv_adjoint(grad, c, direction, order, bdry), None, None, None, None, None, None
+
+
+deriv.register_autograd(_deriv_backward, setup_context=_deriv_setup)
 
 
 def _op(direction, order):

@@ -207,6 +207,17 @@ int css_d2bydp2(css_ctx *ctx, const double *x, double *dx, int var);
 int css_deriv_dev(css_ctx *ctx, int dir, int order, const double *x, double *dx,
                   const double *bc_lo, const double *bc_hi, int bdry, void *stream);
 
+/* Adjoint of css_deriv_dev with zero boundary data: gx = D^T g, where
+ * dx = D x is the blocked compact derivative of direction dir, order and
+ * bdry (the transpose of Dbydr ... D2bydp2, derivatives.f90:547-1684, as
+ * one linear map of the field).  It has no counterpart in the reference;
+ * it is the backward of torch.ops.css.deriv, so networks trained through
+ * the derivatives (the closure) can differentiate them.  Device pointers
+ * (g and gx must differ), enqueued on `stream`; the first call for a
+ * (dir, order, bdry) builds that operator's dense per-block matrices.     */
+int css_deriv_adjoint_dev(css_ctx *ctx, int dir, int order, const double *g, double *gx, int bdry,
+                          void *stream);
+
 /* Cyclic phi derivative (an extension, off the reference path: the
  * reference's Dbydp / D2bydp2, derivatives.f90:1480-1684, close every phi
  * block with halo rows, and css_dbydp / css_deriv reproduce that).  Here

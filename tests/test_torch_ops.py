@@ -107,3 +107,42 @@ def test_reference_named_entry_points_take_var(field):
     out = np.zeros_like(x)
     with pytest.raises(CssError):
         check(L.css_dbydr(sim.h, dp(x), dp(out), None, None, 13))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("direction", [0, 1, 2])
+@pytest.mark.parametrize("order", [1, 2])
+def test_deriv_adjoint_dot_product(direction, order, gpu_available):
+    """<D x, y> = <x, D^T y> for the blocked operator of every direction,
+    order and boundary condition (the backward of torch.ops.css.deriv)."""
+    import torch
+    from css_b200 import problem, torch_ops  # noqa: F401
+    from css_b200.context import Simulation
+    p, prof, v0, dt, _ = problem.build((40, 40, 60), decomp=(2, 2, 3))
+    sim = Simulation(p, prof)
+    g = torch.Generator().manual_seed(direction * 10 + order)
+    x = torch.randn(2, p.nr, p.nphi, p.nth, generator=g, dtype=torch.float64).cuda()
+    y = torch.randn(2, p.nr, p.nphi, p.nth, generator=g, dtype=torch.float64).cuda()
+    for bdry in (range(5) if direction < 2 else [0]):
+        dx = torch.ops.css.deriv(x, sim.h.value, direction, order, None, None, bdry)
+        aty = torch.ops.css.deriv_adjoint(y, sim.h.value, direction, order, bdry)
+        lhs, rhs = float((dx * y).sum()), float((x * aty).sum())
+        scale = float((dx.abs() * y.abs()).sum())
+        assert abs(lhs - rhs) <= 1e-13 * scale, (bdry, lhs, rhs)
+    sim.close()
+
+
+@pytest.mark.gpu
+def test_deriv_gradcheck(gpu_available):
+    """torch.autograd.gradcheck (fast mode: random projections against
+    finite differences) through torch.ops.css.deriv."""
+    import torch
+    from css_b200 import problem, torch_ops  # noqa: F401
+    from css_b200.context import Simulation
+    p, prof, v0, dt, _ = problem.build((40, 40, 60), decomp=(2, 2, 3))
+    sim = Simulation(p, prof)
+    x = torch.randn(p.nr, p.nphi, p.nth, dtype=torch.float64, device="cuda", requires_grad=True)
+    for direction in (0, 1, 2):
+        f = lambda t: torch.ops.css.deriv(t, sim.h.value, direction, 1, None, None, 1)
+        assert torch.autograd.gradcheck(f, (x,), fast_mode=True, eps=1e-6, atol=1e-5, rtol=1e-4)
+    sim.close()
