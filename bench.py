@@ -621,17 +621,21 @@ def run_closure(args):
     barrier(world)
     clk = clocks.stop() if rank == 0 else None
     inf_ms = max_over_ranks(e0.elapsed_time(e1) / args.steps, world)
-    # the per-layer GEMM path, for comparison
-    net.set_fused(False)
-    net.forward(x, nc)
-    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.steps):
+    # the other forward paths, for comparison: the fused mma.sync kernel and
+    # the per-layer GEMMs
+    other_ms = {}
+    for mode in ("mma", "gemm"):
+        net.set_forward(mode)
         net.forward(x, nc)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    net.set_fused(True)
-    gemm_ms = max_over_ranks(f0.elapsed_time(f1) / args.steps, world)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            net.forward(x, nc)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        other_ms[mode] = max_over_ranks(f0.elapsed_time(f1) / args.steps, world)
+    net.set_forward("tcgen05")
+    gemm_ms = other_ms["gemm"]
     tr_ms = max_over_ranks(e1.elapsed_time(e2) / args.steps, world)
     peaks = {}
     try:
@@ -664,7 +668,9 @@ def run_closure(args):
            "training": {"rows_per_s": batch * world / (tr_ms / 1e3), "ms_per_step": tr_ms, "tflops": tr_tf,
                         "own_kernels_per_step": 39},
            "inference_per_layer_gemms": {"ms": gemm_ms, "rows_per_s": nc * world / (gemm_ms / 1e3)},
-           "kernel": "k_mlp_fused (one launch: weights in shared memory, BF16 mma.sync m16n8k16 chain)",
+           "inference_fused_mma_sync": {"ms": other_ms["mma"], "rows_per_s": nc * world / (other_ms["mma"] / 1e3)},
+           "kernel": "k_mlp_tc (one launch: weights in shared memory, 128-row tiles, tcgen05.mma kind::f16 with "
+                     "FP32 accumulators in tensor memory)",
            "roofline": {"bound": "tensor", "achieved": inf_tf, "peak": peak, "unit": "TFLOP/s",
                         "frac": inf_tf / peak, "traffic": None, "peak_source": "measured" if peaks else "fallback",
                         "flop_per_row": fwd_flop_row},

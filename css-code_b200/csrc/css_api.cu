@@ -2286,7 +2286,9 @@ struct css_mlp {
   float *gpart = nullptr;       // row-chunk partials of the weight gradients
   cudaStream_t st = nullptr, own_st = nullptr;
   unsigned char *packed = nullptr;  // weights for the fused forward kernel
-  bool packed_ok = false, fused = true;
+  bool packed_ok = false;
+  int fused = 2;                    // 0 per-layer GEMMs, 1 fused mma.sync kernel, 2 fused tcgen05 kernel
+  int *flag = nullptr;              // set by the tcgen05 kernel when its bounded wait runs out
 };
 
 // the products of a pass, on k_gemm_bf16 (row-major; see css_closure.cuh)
@@ -2330,6 +2332,7 @@ extern "C" void css_mlp_destroy(css_mlp *m) {
     cudaFree(m->Z[l]); cudaFree(m->H[l]);
   }
   cudaFree(m->dH); cudaFree(m->dZb); cudaFree(m->part); cudaFree(m->gpart); cudaFree(m->packed);
+  cudaFree(m->flag);
   if (m->own_st) cudaStreamDestroy(m->own_st);
   else if (m->st) cudaStreamDestroy(m->st);
   delete m;
@@ -2464,14 +2467,38 @@ static int mlp_pack(css_mlp *m) {
 // 1: forward passes use the fused kernel (the default when the widths are
 // 144/128/128/128/16); 0: the per-layer GEMM path
 extern "C" int css_mlp_set_fused(css_mlp *m, int on) {
-  if (!m) { set_err("css_mlp_set_fused: NULL"); return CSS_ERR_ARG; }
-  m->fused = on != 0;
+  if (!m || on < 0 || on > 2) { set_err("css_mlp_set_fused: bad argument"); return CSS_ERR_ARG; }
+  m->fused = on;
   return CSS_OK;
 }
 
 extern "C" int css_mlp_forward(css_mlp *m, const void *x, long long n, float *y) {
   if (!m || !x || !y || n < 1) { set_err("css_mlp_forward: bad argument"); return CSS_ERR_ARG; }
   const int K0 = m->dims[0], MO = m->dims[4];
+  if (m->fused == 2 && mlp_fusable(m)) {
+    static bool attr_tc = false;
+    if (!attr_tc) {
+      CUDA_TRY(cudaFuncSetAttribute(k_mlp_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_BYTES));
+      attr_tc = true;
+    }
+    if (!m->packed_ok)
+      if (int rc = mlp_pack(m)) return rc;
+    if (!m->flag) {
+      CUDA_TRY(cudaMalloc(&m->flag, sizeof(int)));
+    }
+    CUDA_TRY(cudaMemsetAsync(m->flag, 0, sizeof(int), m->st));
+    const long long ntiles = (n + TC_ROWS - 1) / TC_ROWS;
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int grid = (int)std::min<long long>(nsm, ntiles);
+    k_mlp_tc<<<grid, TC_NT, TC_SMEM_BYTES, m->st>>>((const __nv_bfloat16 *)x, n, m->packed, y, m->flag);
+    CUDA_TRY(cudaGetLastError());
+    int h = 0;
+    CUDA_TRY(cudaMemcpyAsync(&h, m->flag, sizeof(int), cudaMemcpyDeviceToHost, m->st));
+    CUDA_TRY(cudaStreamSynchronize(m->st));
+    if (h) { set_err("css_mlp_forward: tensor-core products did not complete within the kernel's bounded wait"); return CSS_ERR_CUDA; }
+    return CSS_OK;
+  }
   if (m->fused && mlp_fusable(m)) {
     static bool attr_done = false;
     if (!attr_done) {

@@ -416,6 +416,252 @@ __global__ void __launch_bounds__(FM_WARPS * 32, 1) k_mlp_fused(const __nv_bfloa
 }
 
 // ---------------------------------------------------------------------------
+// The fused forward pass on the 5th-generation tensor cores (tcgen05): a
+// persistent CTA per SM keeps all four layers' BF16 weights in shared memory
+// in the UMMA K-major core-matrix layout (8 rows x 16 bytes per core matrix:
+// the canonical no-swizzle layout; leading byte offset = the distance
+// between the two K halves of one K=16 step, stride byte offset = 128
+// between 8-row groups).  Its three warpgroups each take 128-row tiles in
+// turn, with a shared-memory slot, 128 tensor-memory columns and an
+// mbarrier of their own, so one group's products run on the tensor core
+// while the other applies its activations:
+//   features -> the slot (16-byte copies, the same layout) -> one thread
+//   issues the layer's tcgen05.mma (M 128, N 128 or 16, K 16 each; BF16 x
+//   BF16 -> FP32 accumulators in tensor memory) and commits them to the
+//   mbarrier -> each thread reads its row's accumulators (tcgen05.ld), adds
+//   the bias, applies GELU, rounds to BF16 and writes the next layer's A
+//   operand into the slot (the features are consumed by then).
+// Waits are bounded: a group whose products never complete sets `flag` and
+// stops; the tensor memory is released before the CTA exits.
+// ---------------------------------------------------------------------------
+#define TC_ROWS 128
+#define TC_GROUPS 3               // warpgroups, each with its own tile, slot, accumulator and mbarrier
+#define TC_NT (128 * TC_GROUPS)
+// shared layout (bytes): W0 (128 x 144) | W1 | W2 (128 x 128) | W3 (16 x 128) | a slot per group (128 x 144
+// each) | biases (FP32) | an mbarrier per group | tensor-memory address
+#define TC_OFF_W1 (FM_W * FM_IN * 2)
+#define TC_OFF_W2 (TC_OFF_W1 + FM_W * FM_W * 2)
+#define TC_OFF_W3 (TC_OFF_W2 + FM_W * FM_W * 2)
+#define TC_OFF_S (TC_OFF_W3 + FM_OUT * FM_W * 2)
+#define TC_SLOT (TC_ROWS * FM_IN * 2)
+#define TC_OFF_B (TC_OFF_S + TC_GROUPS * TC_SLOT)
+#define TC_OFF_BAR (TC_OFF_B + (3 * FM_W + FM_OUT) * 4)
+#define TC_SMEM_BYTES (TC_OFF_BAR + 8 * TC_GROUPS + 8)
+
+// byte offset of element (row r, k) of an R-row K-major operand tile in the
+// core-matrix layout: core matrix (k/8, r/8) at ((k/8) * R/8 + r/8) * 128
+__host__ __device__ __forceinline__ unsigned tc_off(int r, int k, int R) {
+  return (unsigned)(((k >> 3) * (R >> 3) + (r >> 3)) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// UMMA shared-memory descriptor: no swizzle, version 1 (sm_100)
+__device__ __forceinline__ uint64_t tc_desc(unsigned saddr, unsigned lbo, unsigned sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // version
+  return d;               // base offset 0, layout type 0 (no swizzle)
+}
+// instruction descriptor of kind::f16: BF16 A and B (K-major), FP32 D
+__host__ __device__ constexpr uint32_t tc_idesc(int M, int N) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, int acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(acc)
+      : "memory");
+}
+__device__ __forceinline__ void tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+                   (unsigned)__cvta_generic_to_shared(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_proxy() { asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory"); }
+// 16 FP32 accumulator columns of this thread's lane (no wait)
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, uint32_t (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tc_ld_wait() { asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory"); }
+__device__ __forceinline__ bool tc_wait(uint64_t *bar, unsigned parity) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(bar);
+  const long long t0 = clock64();
+  for (;;) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (ok) return true;
+    if (clock64() - t0 > 4000000000ll) return false;
+  }
+}
+// barrier of one warpgroup (named barrier 1 + group, 128 threads)
+__device__ __forceinline__ void tc_group_sync(int grp) {
+  asm volatile("bar.sync %0, 128;\n" ::"r"(1 + grp) : "memory");
+}
+// the same barrier, returning whether any of the group's threads passed pred
+__device__ __forceinline__ bool tc_group_any(int grp, bool pred) {
+  unsigned r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n barrier.red.or.pred p, %2, 128, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(r)
+      : "r"((unsigned)pred), "r"(1 + grp)
+      : "memory");
+  return r != 0;
+}
+
+// a group stages a 128-row feature tile (rows past n zero) into its slot
+__device__ __forceinline__ void tc_stage_x(const __nv_bfloat16 *__restrict__ X, long long n, long long r0,
+                                           unsigned char *xs, int gt) {
+  for (int k = gt; k < TC_ROWS * (FM_IN / 8); k += 128) {
+    const int r = k / (FM_IN / 8), kc = k - r * (FM_IN / 8);
+    const bool in = r0 + r < n;
+    const __nv_bfloat16 *src = in ? X + (size_t)(r0 + r) * FM_IN + kc * 8 : X;
+    cp_async16(xs + tc_off(r, kc * 8, TC_ROWS), src, in ? 16 : 0);
+  }
+  cp_async_commit();
+}
+
+__global__ void __launch_bounds__(TC_NT, 1) k_mlp_tc(const __nv_bfloat16 *__restrict__ X, long long n,
+                                                    const unsigned char *__restrict__ params, float *__restrict__ Y,
+                                                    int *flag) {
+  extern __shared__ __align__(128) unsigned char tc_sm[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int grp = warp >> 2, gt = tid & 127;  // warpgroup and its thread
+  uint64_t *bars = reinterpret_cast<uint64_t *>(tc_sm + TC_OFF_BAR);
+  uint32_t *tslot = reinterpret_cast<uint32_t *>(tc_sm + TC_OFF_BAR + 8 * TC_GROUPS);
+  // weights: packed rows (transposed, k contiguous, padded) -> core-matrix layout
+  {
+    const int Kl[4] = {FM_IN, FM_W, FM_W, FM_W}, Nl[4] = {FM_W, FM_W, FM_W, FM_OUT};
+    const int KPl[4] = {FM_KP0, FM_KP, FM_KP, FM_KP};
+    const size_t srco[4] = {0, FM_OFF_W1, FM_OFF_W2, FM_OFF_W3};
+    const unsigned dsto[4] = {0, TC_OFF_W1, TC_OFF_W2, TC_OFF_W3};
+#pragma unroll
+    for (int l = 0; l < 4; l++) {
+      const int nch = Kl[l] / 8;
+      for (int k = tid; k < Nl[l] * nch; k += TC_NT) {
+        const int r = k / nch, kc = k - r * nch;
+        *reinterpret_cast<uint4 *>(tc_sm + dsto[l] + tc_off(r, kc * 8, Nl[l])) =
+            __ldg(reinterpret_cast<const uint4 *>(params + srco[l] + ((size_t)r * KPl[l] + kc * 8) * 2));
+      }
+    }
+    for (int k = tid; k < 3 * FM_W + FM_OUT; k += TC_NT)
+      reinterpret_cast<float *>(tc_sm + TC_OFF_B)[k] = reinterpret_cast<const float *>(params + FM_OFF_B)[k];
+  }
+  if (warp == 0) {  // 512 tensor-memory columns (a power of two): a 128 x 128 FP32 accumulator per group
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;\n" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(tslot))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int b = 0; b < TC_GROUPS; b++)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"((unsigned)__cvta_generic_to_shared(bars + b))
+                   : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_proxy();  // the weights, written here, are read by the tensor core
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot + (uint32_t)(grp * 128);
+  const unsigned sbase = (unsigned)__cvta_generic_to_shared(tc_sm);
+  const float *bias = reinterpret_cast<const float *>(tc_sm + TC_OFF_B);
+  unsigned char *slot = tc_sm + TC_OFF_S + grp * TC_SLOT;
+  const unsigned slot_s = sbase + TC_OFF_S + grp * TC_SLOT;
+  uint64_t *bar = bars + grp;
+  const long long ntiles = (n + TC_ROWS - 1) / TC_ROWS;
+  unsigned phase = 0;
+  bool failed = false;
+  // this thread's row: lane quarter (warp % 4) of its group's accumulator
+  const int row = (warp & 3) * 32 + lane;
+  const uint32_t trow = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+  for (long long tile = blockIdx.x + (long long)grp * gridDim.x; tile < ntiles && !failed;
+       tile += (long long)TC_GROUPS * gridDim.x) {
+    const long long r0 = tile * TC_ROWS;
+    tc_stage_x(X, n, r0, slot, gt);
+    cp_async_wait<0>();
+    tc_fence_proxy();
+    tc_fence_before();
+    tc_group_sync(grp);
+    for (int l = 0; l < 4; l++) {
+      const int K = l == 0 ? FM_IN : FM_W, N = l == 3 ? FM_OUT : FM_W;
+      if (gt == 0) {
+        tc_fence_after();
+        const unsigned b0 = sbase + (l == 0 ? 0u : l == 1 ? (unsigned)TC_OFF_W1 : l == 2 ? (unsigned)TC_OFF_W2 : (unsigned)TC_OFF_W3);
+        const uint32_t idesc = tc_idesc(TC_ROWS, N);
+        for (int kk = 0; kk < K / 16; kk++) {
+          const uint64_t da = tc_desc(slot_s + kk * 2 * (TC_ROWS / 8) * 128, (TC_ROWS / 8) * 128, 128);
+          const uint64_t db = tc_desc(b0 + kk * 2 * (N / 8) * 128, (N / 8) * 128, 128);
+          tc_mma(tmem, da, db, idesc, kk > 0);
+        }
+        tc_commit(bar);
+      }
+      const bool ok = tc_wait(bar, phase);
+      phase ^= 1u;
+      if (tc_group_any(grp, !ok)) {  // the whole group stops together
+        failed = true;
+        break;
+      }
+      tc_fence_after();
+      if (l < 3) {
+        const float *b = bias + l * FM_W;
+#pragma unroll
+        for (int half = 0; half < 2; half++) {
+          uint32_t r[4][16];
+#pragma unroll
+          for (int q = 0; q < 4; q++) tc_ld16(trow + half * 64 + q * 16, r[q]);
+          tc_ld_wait();
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            const int c0 = half * 64 + q * 16;
+            __align__(16) __nv_bfloat16 hv[16];
+#pragma unroll
+            for (int e = 0; e < 16; e++) hv[e] = __float2bfloat16_rn(gelu_f(__uint_as_float(r[q][e]) + b[c0 + e]));
+            *reinterpret_cast<uint4 *>(slot + tc_off(row, c0, TC_ROWS)) = *reinterpret_cast<const uint4 *>(hv);
+            *reinterpret_cast<uint4 *>(slot + tc_off(row, c0 + 8, TC_ROWS)) = *reinterpret_cast<const uint4 *>(hv + 8);
+          }
+        }
+        tc_fence_proxy();
+      } else {
+        uint32_t r[16];
+        tc_ld16(trow, r);
+        tc_ld_wait();
+        const float *b3 = bias + 3 * FM_W;
+        if (r0 + row < n) {
+          float4 *y = reinterpret_cast<float4 *>(Y + (size_t)(r0 + row) * FM_OUT);
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            y[q] = make_float4(__uint_as_float(r[4 * q]) + b3[4 * q], __uint_as_float(r[4 * q + 1]) + b3[4 * q + 1],
+                               __uint_as_float(r[4 * q + 2]) + b3[4 * q + 2],
+                               __uint_as_float(r[4 * q + 3]) + b3[4 * q + 3]);
+        }
+      }
+      tc_fence_before();
+      tc_group_sync(grp);
+    }
+  }
+  if (failed) atomicOr(flag, 1);
+  cp_async_wait<0>();
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;\n" ::"r"(*tslot) : "memory");
+}
+
+// ---------------------------------------------------------------------------
 // The products of a training step on the tensor cores: BF16 mma.sync
 // m16n8k16 with FP32 accumulation, row-major operands.
 //   GM_FWD: C[n][i] = sum_k X[n][k] W[k][i]             (Z = X W)

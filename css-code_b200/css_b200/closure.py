@@ -92,9 +92,18 @@ class Mlp:
         check(_lib.lib().css_mlp_train_step(self.h, _ptr(x), _ptr(t), n, float(lr), ctypes.byref(loss)))
         return loss.value
 
+    FORWARD_MODES = {"gemm": 0, "mma": 1, "tcgen05": 2}
+
     def set_fused(self, on=True):
-        """Fused one-kernel forward (default) or the per-layer GEMM path."""
-        check(_lib.lib().css_mlp_set_fused(self.h, 1 if on else 0))
+        """Fused one-kernel forward on the tcgen05 tensor cores (default) or
+        the per-layer GEMM path."""
+        check(_lib.lib().css_mlp_set_fused(self.h, 2 if on else 0))
+
+    def set_forward(self, mode):
+        """Forward path: "tcgen05" (fused, 5th-generation tensor cores with
+        tensor-memory accumulators; the default), "mma" (fused, BF16
+        mma.sync) or "gemm" (one product kernel per layer)."""
+        check(_lib.lib().css_mlp_set_fused(self.h, self.FORWARD_MODES[mode]))
 
     def set_stream(self, stream_handle):
         check(_lib.lib().css_mlp_set_stream(self.h, stream_handle))

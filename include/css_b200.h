@@ -434,9 +434,11 @@ int css_mlp_params(css_mlp *mlp, int layer, float *w, float *b, int set);
 int css_mlp_grads(css_mlp *mlp, int layer, float *gw, float *gb);
 /* run the network's work on the caller's cudaStream_t (NULL: its own) */
 int css_mlp_set_stream(css_mlp *mlp, void *stream);
-/* forward passes of a 144/128/128/128/16 network run as one fused kernel
- * (weights in shared memory, the four layers chained in registers on BF16
- * tensor-core MMAs) unless on = 0 selects the per-layer GEMM path          */
+/* forward passes of a 144/128/128/128/16 network run as one fused kernel:
+ * on = 2 (the default) on the tcgen05 tensor cores (weights in shared
+ * memory, 128-row tiles, FP32 accumulators in tensor memory), on = 1 on
+ * BF16 mma.sync with the layers chained in registers, on = 0 the per-layer
+ * GEMM path                                                               */
 int css_mlp_set_fused(css_mlp *mlp, int on);
 
 /* ---- diagnostics of the current state (vars0), computed on the device ----
