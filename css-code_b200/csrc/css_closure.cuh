@@ -159,6 +159,46 @@ __device__ __forceinline__ float gelu_f(float x) {
   const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
   return 0.5f * x * (1.0f + tanh_hw(u));
 }
+// Packed FP32x2 arithmetic (add/mul/fma .f32x2, sm_100): two lanes per
+// instruction, each rounded as its scalar form.
+typedef unsigned long long f32x2_t;
+__device__ __forceinline__ f32x2_t f2_pack(float a, float b) {
+  f32x2_t r;
+  asm("mov.b64 %0, {%1,%2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(f32x2_t v, float &a, float &b) {
+  asm("mov.b64 {%0,%1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ f32x2_t f2_add(f32x2_t a, f32x2_t b) {
+  f32x2_t r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2_t f2_mul(f32x2_t a, f32x2_t b) {
+  f32x2_t r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ f32x2_t f2_fma(f32x2_t a, f32x2_t b, f32x2_t c) {
+  f32x2_t r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+// gelu_f of (z + bias) for two values, the same operations in the same
+// order (so the same roundings) in packed arithmetic, rounded to BF16x2
+__device__ __forceinline__ uint32_t gelu2_bf16(f32x2_t z, f32x2_t bias) {
+  const f32x2_t x = f2_add(z, bias);
+  const f32x2_t u = f2_mul(f2_pack(0.7978845608028654f, 0.7978845608028654f),
+                           f2_fma(f2_mul(f2_pack(0.044715f, 0.044715f), x), f2_mul(x, x), x));
+  float u0, u1;
+  f2_unpack(u, u0, u1);
+  const f32x2_t t = f2_add(f2_pack(1.0f, 1.0f), f2_pack(tanh_hw(u0), tanh_hw(u1)));
+  float g0, g1;
+  f2_unpack(f2_mul(f2_mul(f2_pack(0.5f, 0.5f), x), t), g0, g1);
+  const __nv_bfloat162 h = __floats2bfloat162_rn(g0, g1);
+  return *reinterpret_cast<const uint32_t *>(&h);
+}
 __device__ __forceinline__ float gelu_df(float x) {
   const float u = 0.7978845608028654f * fmaf(0.044715f * x, x * x, x);
   const float t = tanh_hw(u);
@@ -626,11 +666,13 @@ __global__ void __launch_bounds__(TC_NT, 1) k_mlp_tc(const __nv_bfloat16 *__rest
 #pragma unroll
           for (int q = 0; q < 4; q++) {
             const int c0 = half * 64 + q * 16;
-            __align__(16) __nv_bfloat16 hv[16];
+            const f32x2_t *b2 = reinterpret_cast<const f32x2_t *>(b + c0);
+            uint32_t hv[8];
 #pragma unroll
-            for (int e = 0; e < 16; e++) hv[e] = __float2bfloat16_rn(gelu_f(__uint_as_float(r[q][e]) + b[c0 + e]));
-            *reinterpret_cast<uint4 *>(slot + tc_off(row, c0, TC_ROWS)) = *reinterpret_cast<const uint4 *>(hv);
-            *reinterpret_cast<uint4 *>(slot + tc_off(row, c0 + 8, TC_ROWS)) = *reinterpret_cast<const uint4 *>(hv + 8);
+            for (int e = 0; e < 8; e++)
+              hv[e] = gelu2_bf16(((f32x2_t)r[q][2 * e + 1] << 32) | r[q][2 * e], b2[e]);
+            *reinterpret_cast<uint4 *>(slot + tc_off(row, c0, TC_ROWS)) = make_uint4(hv[0], hv[1], hv[2], hv[3]);
+            *reinterpret_cast<uint4 *>(slot + tc_off(row, c0 + 8, TC_ROWS)) = make_uint4(hv[4], hv[5], hv[6], hv[7]);
           }
         }
         tc_fence_proxy();
