@@ -545,29 +545,47 @@ def run_ensemble(args):
     return 0
 
 
+CLOSURE_STUDIES = {
+    # workload: fine grid, coarse grid, magnetic, n_rho, decompositions, study steps
+    "closure-study": ((96, 128, 256), (24, 32, 64), False, 3.0, (3, 4, 8), (2, 2, 4),
+                      dict(n_pre=5000, n_adjust=500, n_train=400, nsnap=8, n_win=1000, nstat=10, train_steps=400)),
+    "closure-study-mhd": ((256, 512, 1024), (64, 128, 256), True, 5.0, (8, 16, 32), (2, 4, 8),
+                          dict(n_pre=20000, n_adjust=500, n_train=500, nsnap=10, n_win=2000, nstat=20,
+                               train_steps=600)),
+}
+
+
 def run_closure_study(args):
-    """The closure judged by a resolved run: hydro 96x128x256 box-filtered
-    4x in every direction onto 24x32x64 (closure.study).  Prints one JSON line
-    with the relative errors of the time-averaged kinetic-energy spectrum and
-    enthalpy-flux profile of the prescribed-profile and the learned-closure
-    coarse runs against the filtered fine run, and the wall-time ratio of the
-    fine to the closure-driven coarse window."""
+    """The closure judged by a resolved run (closure.study): a fine run
+    box-filtered 4x in every direction trains the network; coarse runs from
+    the filtered fine state (prescribed profile, and the closure's two
+    couplings) cover the window of the fine run and are compared with its
+    filtered statistics.  ``closure-study``: hydro 96x128x256 onto 24x32x64.
+    ``closure-study-mhd``: MHD 256x512x1024 onto 64x128x256, a 2000-step
+    window (the learned-closure configuration).  Prints one JSON line: the
+    relative errors of the time-averaged KE (and ME) spectra (m >= 1),
+    enthalpy and kinetic-energy flux profiles of every coarse run, and the
+    wall-time ratio of the fine to the coarse window."""
     import torch
     from css_b200 import closure as C
     from css_b200 import problem
     torch.cuda.set_device(0)
-    fp, fprof, fv0, fdt, _ = problem.build((96, 128, 256), decomp=(3, 4, 8))
-    cp, cprof, cv0, cdt, _ = problem.build((24, 32, 64), decomp=(2, 2, 4))
-    r = C.study((fp, fprof, fv0, fdt), (cp, cprof, cv0, cdt), factor=4, t_spin=10.0, t_win=2.0, nsnap=20)
-    out = {"metric": "closure study: relative error of the time-averaged kinetic-energy spectrum (m >= 1) and "
-                     "enthalpy flux of the coarse run against the filtered fine run",
-           "value": r["flux_err_closure"], "unit": "relative L2 error (enthalpy flux, learned closure)",
+    fdims, cdims, mag, nrho, fdec, cdec, kw = CLOSURE_STUDIES[args.workload]
+    fp, fprof, fv0, fdt, fi = problem.build(fdims, magnetic=mag, decomp=fdec, n_rho=nrho)
+    cp, cprof, cv0, cdt, ci = problem.build(cdims, magnetic=mag, decomp=cdec, n_rho=nrho)
+    r = C.study((fp, fprof, fv0, fdt, problem.background(fp, fprof, fi)),
+                (cp, cprof, cv0, cdt, problem.background(cp, cprof, ci)), factor=4, **kw)
+    out = {"metric": "closure study: relative error of time-averaged spectra (m >= 1) and radial flux profiles "
+                     "of coarse runs against the filtered fine run",
+           "value": r["errors"]["variance"]["E_K"], "unit": "relative L2 error (KE spectrum, learned closure)",
            "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
-           "config": {"workload": "closure-study", "fine": [96, 128, 256], "coarse": [24, 32, 64], "filter": 4,
-                      "t_spin": r["t_spin"], "t_window": r["t_win"], "snapshots": r["nsnap"]},
-           "result": {k: r[k] for k in ("spectrum_err_prescribed", "spectrum_err_closure", "flux_err_prescribed",
-                                        "flux_err_closure", "fine_window_s", "coarse_window_s",
-                                        "coarse_prescribed_window_s", "wall_ratio", "loss_first", "loss_last")}}
+           "config": {"workload": args.workload, "fine": list(fdims), "coarse": list(cdims), "filter": 4,
+                      "magnetic": mag, "n_rho": nrho, **kw},
+           "result": {k: r[k] for k in ("errors", "end_state_error", "fine_window_s", "coarse_window_s",
+                                        "pre_spin_s", "wall_ratio", "loss_first", "loss_last", "fine_steps",
+                                        "coarse_steps", "fine_dt", "coarse_dt", "t_window")},
+           "spectra": {name: {k: [float(x) for x in v[:33]] for k, v in st.items()}
+                       for name, st in r["stats"].items()}}
     print(json.dumps(out))
     return 0
 
@@ -707,7 +725,7 @@ def main():
         return run_reference(args)
     if args.workload.startswith("ensemble-"):
         return run_ensemble(args)
-    if args.workload == "closure-study":
+    if args.workload in CLOSURE_STUDIES:
         return run_closure_study(args)
     if args.workload.startswith("closure-"):
         return run_closure(args)

@@ -2269,6 +2269,59 @@ extern "C" int css_closure_speed2(long long nc, const float *y, const float *tsc
   return CSS_OK;
 }
 
+extern "C" int css_closure_speed2_shaped(css_ctx *c, const float *y, const float *tscale, double *speed2) {
+  if (!c || !y || !tscale || !speed2) { set_err("css_closure_speed2_shaped: bad argument"); return CSS_ERR_ARG; }
+  k_closure_speed2_shaped<<<c->p.nr, 256, 0, c->stream>>>(c->g, y, tscale, speed2);
+  if (int rc = check_launch(c)) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+// the two grids of a restriction / prolongation: same variables, the fine
+// one f times the coarse one in every direction
+static bool grid_pair(const css_ctx *fine, const css_ctx *coarse, int f) {
+  return fine && coarse && f >= 1 && fine->nv == coarse->nv && coarse->p.nr * f == fine->p.nr &&
+         coarse->p.nth * f == fine->p.nth && coarse->p.nphi * f == fine->p.nphi;
+}
+
+extern "C" int css_restrict_state(css_ctx *fine, const double *fine_base, int f, css_ctx *coarse,
+                                  const double *coarse_base) {
+  if (!grid_pair(fine, coarse, f)) {
+    set_err("css_restrict_state: the fine grid must be f times the coarse grid in every direction, same variables");
+    return CSS_ERR_ARG;
+  }
+  CUDA_TRY(cudaStreamSynchronize(coarse->stream));
+  k_restrict_state<<<148 * 8, 256, 0, fine->stream>>>(fine->v0, fine_base, fine->p.nth, fine->p.nphi, fine->p.nr, f,
+                                                       fine->nv, coarse_base, coarse->v0);
+  if (int rc = check_launch(fine)) return rc;
+  CUDA_TRY(cudaStreamSynchronize(fine->stream));
+  if (coarse->bg2) {
+    const size_t nrt = (size_t)coarse->p.nr * coarse->p.nth;
+    k_phi_mean<<<(unsigned)((nrt + 127) / 128), 128, 0, coarse->stream>>>(coarse->g, coarse->v0, coarse->bg2);
+    if (int rc = check_launch(coarse)) return rc;
+    CUDA_TRY(cudaStreamSynchronize(coarse->stream));
+  }
+  return CSS_OK;
+}
+
+extern "C" int css_prolong_add(css_ctx *coarse, const double *coarse_base, int f, css_ctx *fine) {
+  if (!grid_pair(fine, coarse, f)) {
+    set_err("css_prolong_add: the fine grid must be f times the coarse grid in every direction, same variables");
+    return CSS_ERR_ARG;
+  }
+  CUDA_TRY(cudaStreamSynchronize(coarse->stream));
+  k_prolong_add<<<148 * 8, 256, 0, fine->stream>>>(coarse->v0, coarse_base, coarse->p.nth, coarse->p.nphi,
+                                                    coarse->p.nr, f, fine->nv, fine->v0);
+  if (int rc = check_launch(fine)) return rc;
+  if (fine->bg2) {
+    const size_t nrt = (size_t)fine->p.nr * fine->p.nth;
+    k_phi_mean<<<(unsigned)((nrt + 127) / 128), 128, 0, fine->stream>>>(fine->g, fine->v0, fine->bg2);
+    if (int rc = check_launch(fine)) return rc;
+  }
+  CUDA_TRY(cudaStreamSynchronize(fine->stream));
+  return CSS_OK;
+}
+
 struct css_mlp {
   int dims[5];          // padded widths: input, hidden x3, output
   int nreal_in, nreal_out;

@@ -287,6 +287,124 @@ __global__ void k_adam(float *__restrict__ w, const float *__restrict__ gr, floa
   }
 }
 
+// Fine -> coarse restriction of the whole state (the evaluation of a coarse
+// run starts from the filtered fine state): vc[iv][c] = base_c[iv][c] + the
+// f x f x f box average of vf - base_f over the fine cells of coarse cell c,
+// summed in (r, phi, theta) order (a NULL base is zero).  The perturbation
+// about each grid's own background is what is filtered, so the coarse
+// state stays in its own grid's hydrostatic balance.  Layout
+// [iv][r][phi][theta] on both grids.
+__global__ void k_restrict_state(const double *__restrict__ vf, const double *__restrict__ base_f, int nthf,
+                                 int nphif, int nrf, int f, int nv, const double *__restrict__ base_c,
+                                 double *__restrict__ vc) {
+  const int nct = nthf / f, ncp = nphif / f, ncr = nrf / f;
+  const size_t nc = (size_t)nct * ncp * ncr, nf = (size_t)nthf * nphif * nrf;
+  const double w = 1.0 / ((double)f * f * f);
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nc * nv; k += (size_t)gridDim.x * blockDim.x) {
+    const int iv = (int)(k / nc);
+    const size_t c = k - (size_t)iv * nc;
+    const int it = (int)(c % nct), ip = (int)((c / nct) % ncp), ir = (int)(c / ((size_t)nct * ncp));
+    double s = 0.0;
+    for (int dr = 0; dr < f; dr++)
+      for (int dp = 0; dp < f; dp++) {
+        const size_t row = (size_t)iv * nf + (size_t)(f * it) +
+                           (size_t)nthf * ((size_t)(f * ip + dp) + (size_t)nphif * (f * ir + dr));
+        for (int dt = 0; dt < f; dt++) s += base_f ? vf[row + dt] - base_f[row + dt] : vf[row + dt];
+      }
+    vc[k] = (base_c ? base_c[k] : 0.0) + s * w;
+  }
+}
+
+// linear interpolation weights of fine index i from a grid f times coarser
+// (cell-centred: fine i sits at coarse coordinate (i + 0.5) / f - 0.5);
+// clamped at the ends, or periodic
+__device__ __forceinline__ void prolong_w(int i, int f, int nc, bool periodic, int &i0, int &i1, double &w) {
+  const double x = (i + 0.5) / f - 0.5;
+  int j = (int)floor(x);
+  w = x - j;
+  if (periodic) {
+    i0 = (j % nc + nc) % nc;
+    i1 = (i0 + 1) % nc;
+  } else if (j < 0) {
+    i0 = i1 = 0;
+    w = 0.0;
+  } else if (j >= nc - 1) {
+    i0 = i1 = nc - 1;
+    w = 0.0;
+  } else {
+    i0 = j;
+    i1 = j + 1;
+  }
+}
+
+// Coarse -> fine: vf += P(vc - base), P trilinear in index space (theta and
+// r clamped, phi periodic); base NULL means zero.  A state developed on the
+// coarse grid is carried to the fine grid as a perturbation of the fine
+// grid's own state.
+__global__ void k_prolong_add(const double *__restrict__ vc, const double *__restrict__ base, int nct, int ncp,
+                              int ncr, int f, int nv, double *__restrict__ vf) {
+  const int nthf = nct * f, nphif = ncp * f, nrf = ncr * f;
+  const size_t nf = (size_t)nthf * nphif * nrf, nc = (size_t)nct * ncp * ncr;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < nf * nv; k += (size_t)gridDim.x * blockDim.x) {
+    const int iv = (int)(k / nf);
+    const size_t id = k - (size_t)iv * nf;
+    const int it = (int)(id % nthf), ip = (int)((id / nthf) % nphif), ir = (int)(id / ((size_t)nthf * nphif));
+    int t0, t1, p0, p1, r0, r1;
+    double wt, wp, wr;
+    prolong_w(it, f, nct, false, t0, t1, wt);
+    prolong_w(ip, f, ncp, true, p0, p1, wp);
+    prolong_w(ir, f, ncr, false, r0, r1, wr);
+    const double *c = vc + (size_t)iv * nc;
+    const double *b = base ? base + (size_t)iv * nc : nullptr;
+    auto at = [&](int t, int p, int r) {
+      const size_t q = (size_t)t + (size_t)nct * ((size_t)p + (size_t)ncp * r);
+      return b ? c[q] - b[q] : c[q];
+    };
+    const double v00 = (1.0 - wt) * at(t0, p0, r0) + wt * at(t1, p0, r0);
+    const double v10 = (1.0 - wt) * at(t0, p1, r0) + wt * at(t1, p1, r0);
+    const double v01 = (1.0 - wt) * at(t0, p0, r1) + wt * at(t1, p0, r1);
+    const double v11 = (1.0 - wt) * at(t0, p1, r1) + wt * at(t1, p1, r1);
+    vf[k] += (1.0 - wr) * ((1.0 - wp) * v00 + wp * v10) + wr * ((1.0 - wp) * v01 + wp * v11);
+  }
+}
+
+// closure -> SLD speed^2 shaped by the prescribed profile: the predicted
+// subgrid variance k = tau_tt + tau_pp + tau_rr of each cell, divided by its
+// shell mean and multiplied by the prescribed speed^2 of that radius, so a
+// shell keeps the prescribed mean diffusion speed^2 and the network moves it
+// to where the subgrid motions are.  One CTA per radius; the shell sum is a
+// fixed-order block reduction.  -1 (the prescribed profile) where the output
+// is not finite or the shell mean is not positive.
+__global__ void __launch_bounds__(256) k_closure_speed2_shaped(CssGeo g, const float *__restrict__ Y,
+                                                               const float *__restrict__ tscale,
+                                                               double *__restrict__ speed2) {
+  __shared__ double red[2][8];
+  const int ir = blockIdx.x, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const size_t np = (size_t)g.nth * g.nphi, c0 = (size_t)ir * np;
+  double sum = 0.0, cnt = 0.0;
+  for (size_t q = threadIdx.x; q < np; q += blockDim.x) {
+    const float *y = Y + (c0 + q) * CL_YPAD;
+    const double tr = (double)y[0] * tscale[0] + (double)y[3] * tscale[3] + (double)y[5] * tscale[5];
+    if (isfinite(tr)) { sum += fmax(tr, 0.0); cnt += 1.0; }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    sum += __shfl_down_sync(0xffffffffu, sum, o);
+    cnt += __shfl_down_sync(0xffffffffu, cnt, o);
+  }
+  if (lane == 0) { red[0][warp] = sum; red[1][warp] = cnt; }
+  __syncthreads();
+  double tot = 0.0, n = 0.0;
+  for (int w = 0; w < 8; w++) { tot += red[0][w]; n += red[1][w]; }
+  const double mean = n > 0.0 ? tot / n : 0.0;
+  const double prof = g.dspeed[ir];
+  for (size_t q = threadIdx.x; q < np; q += blockDim.x) {
+    const float *y = Y + (c0 + q) * CL_YPAD;
+    const double tr = (double)y[0] * tscale[0] + (double)y[3] * tscale[3] + (double)y[5] * tscale[5];
+    speed2[c0 + q] = (isfinite(tr) && mean > 0.0) ? prof * fmax(tr, 0.0) / mean : -1.0;
+  }
+}
+
 // closure -> SLD speed^2 of each coarse cell: the subgrid velocity variance
 // tau_tt + tau_pp + tau_rr (network outputs times their target scales),
 // floored at zero; -1 (the prescribed profile is used) where the output is

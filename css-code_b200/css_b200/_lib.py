@@ -85,6 +85,9 @@ def lib():
         L.css_closure_features.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, vp, vp, vp]
         L.css_closure_targets.argtypes = [ll, vp, vp, vp]
         L.css_closure_speed2.argtypes = [ll, vp, vp, vp]
+        L.css_closure_speed2_shaped.argtypes = [vp, vp, vp, vp]
+        L.css_restrict_state.argtypes = [vp, vp, ctypes.c_int, vp, vp]
+        L.css_prolong_add.argtypes = [vp, vp, ctypes.c_int, vp]
         L.css_mlp_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_ulonglong,
                                      ctypes.POINTER(vp)]
         L.css_mlp_destroy.argtypes = [vp]
@@ -128,7 +131,8 @@ EXPORTS = [
     "css_profile", "css_kernel_stats", "css_compact_lines_noalloc", "css_scalars", "css_step_size",
     "css_shell_averages", "css_spectrum", "css_autotune", "css_set_tiles", "css_set_fused", "css_get_fused", "css_dbydp_cyclic", "css_dbydp_cyclic_dev", "css_deriv_adjoint_dev", "css_ensemble_create", "css_ensemble_step",
     "css_ensemble_launches", "css_ensemble_last_ms", "css_ensemble_destroy", "css_set_sld_speed2", "css_box_filter",
-    "css_closure_scales", "css_closure_features", "css_closure_targets", "css_closure_speed2", "css_mlp_create",
+    "css_closure_scales", "css_closure_features", "css_closure_targets", "css_closure_speed2",
+    "css_closure_speed2_shaped", "css_restrict_state", "css_prolong_add", "css_mlp_create",
     "css_mlp_destroy", "css_mlp_dims", "css_mlp_forward", "css_mlp_train_step", "css_mlp_params", "css_mlp_grads",
     "css_mlp_set_stream", "css_mlp_set_fused", "css_set_clock", "css_get_clock", "css_inout_init",
     "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_squalls",

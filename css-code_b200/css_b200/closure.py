@@ -170,13 +170,28 @@ class Closure:
     def predict(self, data):
         return self.net.forward(data["x"], data["nc"])
 
-    def speed2(self, data):
-        """Per-cell SLD speed^2 of the coarse cells of ``data`` (device FP64)."""
+    COUPLINGS = ("variance", "shaped")
+
+    def speed2(self, data, coupling="variance", sim=None):
+        """Per-cell SLD speed^2 of the coarse cells of ``data`` (device FP64).
+
+        ``variance``: the predicted subgrid variance tau_tt + tau_pp + tau_rr
+        itself (css_closure_speed2).  ``shaped``: the prescribed speed^2 of
+        each radius times the prediction over its shell mean
+        (css_closure_speed2_shaped; needs the coarse run ``sim``): the
+        prescribed level per shell, placed by the network."""
         import torch
         y = self.predict(data)
         ts = torch.tensor(self.tscale, device=y.device)
         s2 = torch.empty(data["nc"], dtype=torch.float64, device=y.device)
-        check(_lib.lib().css_closure_speed2(data["nc"], _ptr(y), _ptr(ts), _ptr(s2)))
+        if coupling == "variance":
+            check(_lib.lib().css_closure_speed2(data["nc"], _ptr(y), _ptr(ts), _ptr(s2)))
+        elif coupling == "shaped":
+            if sim is None:
+                raise ValueError("the shaped coupling needs the coarse run")
+            check(_lib.lib().css_closure_speed2_shaped(sim.h, _ptr(y), _ptr(ts), _ptr(s2)))
+        else:
+            raise ValueError("coupling %r (one of %s)" % (coupling, ", ".join(self.COUPLINGS)))
         return s2
 
     @staticmethod
@@ -191,112 +206,204 @@ class Closure:
 # Evaluation: the closure against the prescribed profile, both judged by the
 # filtered fine run
 # ---------------------------------------------------------------------------
-def coarse_statistics(u_t, u_p, u_r, s_pert, rhor, tr):
-    """Statistics a coarse run is judged by, from (nr, nphi, nth) fields:
-    the kinetic-energy spectrum in azimuthal wavenumber m summed over r and
-    theta, E(m) = sum rhor |u_hat(m)|^2 over the three components, and the
-    enthalpy-flux profile F(r) = rhor T ⟨u_r s'⟩ over theta and phi (the
-    entropy form of rho c_p ⟨u_r T'⟩ about an adiabatic background)."""
-    E = 0.0
-    for u in (u_t, u_p, u_r):
-        uh = np.fft.rfft(u, axis=1) / u.shape[1]
-        E = E + (rhor[:, None, None] * np.abs(uh) ** 2).sum(axis=(0, 2))
-    F = rhor * tr * (u_r * s_pert).mean(axis=(1, 2))
-    return E, F
+def restrict(fine_sim, coarse_sim, factor, fine_base=None, coarse_base=None):
+    """Coarse state := coarse_base + the factor^3 box average of (fine state -
+    fine_base) (css_restrict_state; bases are device tensors of each grid's
+    state layout, None for zero)."""
+    import torch
+    torch.cuda.synchronize()
+    check(_lib.lib().css_restrict_state(fine_sim.h, None if fine_base is None else _ptr(fine_base), int(factor),
+                                        coarse_sim.h, None if coarse_base is None else _ptr(coarse_base)))
+
+
+def prolong_add(coarse_sim, coarse_base, factor, fine_sim):
+    """Fine state += trilinear interpolation of (coarse state - coarse_base)
+    (css_prolong_add; coarse_base a device tensor of the state's layout or None)."""
+    import torch
+    torch.cuda.synchronize()
+    check(_lib.lib().css_prolong_add(coarse_sim.h, None if coarse_base is None else _ptr(coarse_base),
+                                     int(factor), fine_sim.h))
+
+
+def statistics(sim, rhor):
+    """What a run is judged by, from its resident state: the kinetic-energy
+    spectrum in azimuthal wavenumber m, E_K(m) = sum over r, theta and the
+    three components of rhor(r) |u_hat(m)|^2 / 2, the magnetic one
+    E_M(m) = sum |B_hat(m)|^2 / (8 pi) (B = curl A), and the enthalpy- and
+    kinetic-energy-flux profiles (Shell_Average codes 16 and 17,
+    report_mpi.f90:949-960).  u and B come from the library (a factor-1
+    css_box_filter); the transforms and sums are torch's."""
+    import torch
+    p = sim.p
+    nc = p.nr * p.nth * p.nphi
+    fields = torch.empty(7 * nc, dtype=torch.float64, device="cuda")
+    targ = torch.empty(NTARGET * nc, dtype=torch.float64, device="cuda")
+    check(_lib.lib().css_box_filter(sim.h, 1, _ptr(fields), _ptr(targ)))
+    f = fields.view(7, p.nr, p.nphi, p.nth)
+    w = torch.as_tensor(np.asarray(rhor, dtype=np.float64), device="cuda")[None, :, None, None]
+
+    def spec(q, weight):
+        h = torch.fft.rfft(q, dim=2) / p.nphi
+        e = (weight * h.abs() ** 2).sum(dim=(0, 1, 3))
+        e[1:] *= 2.0  # m and -m
+        return e.cpu().numpy()
+
+    out = {"E_K": spec(f[0:3], 0.5 * w)}
+    if p.magnetic:
+        out["E_M"] = spec(f[4:7], 1.0 / (8.0 * np.pi))
+    fl = sim.shell_averages([16, 17])
+    out["F_en"], out["F_ke"] = fl[0], fl[1]
+    return out
 
 
 def rel_err(a, b, lo=0):
     return float(np.linalg.norm(a[lo:] - b[lo:]) / max(np.linalg.norm(b[lo:]), 1e-300))
 
 
-def study(fine, coarse, factor=4, t_spin=10.0, t_win=2.0, nsnap=20, train_steps=400, refresh=20, seed=4):
-    """Trains a closure on a fine run and compares two coarse runs with it.
+def _mean_stats(samples):
+    return {k: np.mean([s[k] for s in samples], axis=0) for k in samples[0]}
 
-    ``fine`` and ``coarse`` are (params, profiles, vars0, dt) of the two grids
-    (coarse = fine / factor in every direction).  The fine run is spun up for
-    t_spin time units, then over t_win it is box-filtered ``nsnap`` times:
-    the snapshots are the training set and their statistics (time-averaged
-    E(m) and F(r), see coarse_statistics) the reference.  Two coarse runs from
-    the coarse seeded state then cover the same physical time: one with the
-    prescribed SLD profile, one whose SLD speed^2 is the closure's prediction
-    from its own state, refreshed every ``refresh`` steps.  Returns the
-    relative errors of both against the filtered fine statistics (E over
-    m >= 1, F over r) and the wall times of the fine and coarse windows."""
+
+def study(fine, coarse, factor=4, n_pre=0, n_adjust=0, n_train=200, nsnap=4, n_win=200, nstat=4,
+          train_steps=400, batch=16384, refresh=20, couplings=("variance", "shaped"), seed=4, cfl=0.4):
+    """A posteriori evaluation of the closure on a fine run.
+
+    ``fine`` and ``coarse`` are (params, profiles, vars0, dt, background) of
+    the two grids (coarse = fine / factor in every direction; background =
+    problem.background of that grid).  States move between the grids as
+    perturbations about each grid's background.  Steps, in this order:
+
+    1. optional pre-spin: ``n_pre`` coarse steps from the coarse seeded
+       state, the developed coarse perturbation then added to the fine
+       seeded state (css_prolong_add) -- a fine run that starts developed;
+    2. ``n_adjust`` fine steps;
+    3. ``n_train`` fine steps, box-filtered ``nsnap`` times: the training set;
+       the network is trained on it (``train_steps`` Adam steps);
+    4. the window: every coarse run starts from the filtered fine state at
+       its start (css_restrict_state) and covers the physical time of
+       ``n_win`` fine steps, sampled ``nstat`` times at the same times as
+       the fine run, whose filtered state is judged by the same diagnostics
+       (statistics()) on a coarse probe run.
+
+    The coarse runs are the prescribed profile and one per coupling of the
+    closure (Closure.speed2), the closure's speed^2 recomputed from the
+    run's own state every ``refresh`` coarse steps.  Returns the
+    time-averaged statistics of each run, their relative errors against the
+    filtered fine run (spectra over m >= 1), the state error of each run at
+    the end of the window against the filtered fine state (per field,
+    relative to how far the filtered fine state moved in the window), and
+    the wall times of the fine and coarse windows (stepping only).  Time
+    steps are the given ones, lowered where the state's Courant limit at
+    ``cfl`` (css_step_size) is below them: in chunks of 500 during the
+    pre-spin, for the fine run after the pre-spin and the adjustment, for
+    the coarse runs at the start of the window."""
     import time
     import torch
     from .context import Simulation
     from .params import PROF_NAMES
-    fp, fprof, fv0, fdt = fine
-    cp, cprof, cv0, cdt = coarse
-    cpr = np.asarray(cprof).reshape(len(PROF_NAMES), cp.nr)
-    rhor, sr = cpr[PROF_NAMES.index("rhor")], cpr[PROF_NAMES.index("sr")]
-    g, cv = cp.gamma, cp.cp / cp.gamma
-    tr = (1.0 / (cv * (g - 1.0))) * rhor ** (g - 1.0) * np.exp(sr / cv)
+    fp, fprof, fv0, fdt, fbg = fine
+    cp, cprof, cv0, cdt, cbg = coarse
     dims = (cp.nth, cp.nphi, cp.nr)
+    nc = cp.nr * cp.nth * cp.nphi
+    rhor = np.asarray(cprof).reshape(len(PROF_NAMES), cp.nr)[PROF_NAMES.index("rhor")]
 
+    def timed_steps(sim, dt, n):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.step_rk4(dt, n)
+        torch.cuda.synchronize()
+        return time.perf_counter() - t0
+
+    cbase = torch.from_numpy(np.ascontiguousarray(cbg, dtype=np.float64)).cuda()
+    fbase = torch.from_numpy(np.ascontiguousarray(fbg, dtype=np.float64)).cuda()
     fsim = Simulation(fp, fprof)
     fsim.upload(fv0)
-    fsim.step_rk4(fdt, int(round(t_spin / fdt)))
-    every = max(1, int(round(t_win / fdt)) // nsnap)
-    Ef, Ff, snaps = [], [], []
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    pre_s = 0.0
+    if n_pre > 0:
+        pre = Simulation(cp, cprof)
+        pre.upload(cv0)
+        n = n_pre
+        while n > 0:  # the developing flow tightens the Courant limit: dt follows it
+            k = min(500, n)
+            pre_s += timed_steps(pre, min(cdt, pre.step_size(cfl)["dtmax"]), k)
+            n -= k
+        prolong_add(pre, cbase, factor, fsim)
+        pre.close()
+    fdt = min(fdt, fsim.step_size(cfl)["dtmax"])
+    if n_adjust > 0:
+        fsim.step_rk4(fdt, n_adjust)
+        fdt = min(fdt, fsim.step_size(cfl)["dtmax"])
+    every = max(1, n_train // max(1, nsnap))
+    snaps = []
     for _ in range(nsnap):
         fsim.step_rk4(fdt, every)
-        d = dataset(fsim, factor)
-        f = d["fields"].cpu().numpy().reshape(7, cp.nr, cp.nphi, cp.nth)
-        e, fl = coarse_statistics(f[0], f[1], f[2], f[3], rhor, tr)
-        Ef.append(e)
-        Ff.append(fl)
-        snaps.append(d)
-    torch.cuda.synchronize()
-    fine_wall = time.perf_counter() - t0
-    Ef, Ff = np.mean(Ef, axis=0), np.mean(Ff, axis=0)
+        snaps.append(dataset(fsim, factor))
     x = torch.cat([d["x"].view(d["nc"], XPAD) for d in snaps]).contiguous()
     t = torch.cat([d["t"].view(d["nc"], YPAD) for d in snaps]).contiguous()
     data = dict(snaps[-1])
     data.update({"x": x.view(-1), "t": t.view(-1), "nc": x.shape[0]})
-    clo = Closure(seed=seed)
-    losses = clo.fit(data, steps=train_steps, batch=16384, lr=2e-3, seed=seed)
-    nc = cp.nr * cp.nth * cp.nphi
+    clo = Closure(seed=seed, max_rows=batch)
+    losses = clo.fit(data, steps=train_steps, batch=batch, lr=2e-3, seed=seed)
+    del x, t, data, snaps
 
-    def coarse_run(learned):
-        sim = Simulation(cp, cprof)
-        sim.upload(cv0)
-        fields = torch.empty(7 * nc, dtype=torch.float64, device="cuda")
-        targ = torch.empty(NTARGET * nc, dtype=torch.float64, device="cuda")
-
-        def advance(n):
+    # the window: coarse runs from the filtered fine state at its start
+    runs = {"prescribed": None}
+    runs.update({c: c for c in couplings})
+    sims = {}
+    for name in runs:
+        sims[name] = Simulation(cp, cprof)
+        restrict(fsim, sims[name], factor, fbase, cbase)
+    probe = Simulation(cp, cprof)
+    restrict(fsim, probe, factor, fbase, cbase)
+    start = probe.download()
+    cdt = min(cdt, probe.step_size(cfl)["dtmax"])
+    fstats, fine_s = [], 0.0
+    fev = max(1, n_win // max(1, nstat))
+    for _ in range(nstat):
+        fine_s += timed_steps(fsim, fdt, fev)
+        restrict(fsim, probe, factor, fbase, cbase)
+        fstats.append(statistics(probe, rhor))
+    fine_end = probe.download()
+    t_win = fev * nstat * fdt
+    ncs = nstat * int(np.ceil(t_win / (nstat * cdt)))  # coarse steps, a multiple of nstat
+    cdt_run = t_win / ncs
+    fields = torch.empty(7 * nc, dtype=torch.float64, device="cuda")
+    targ = torch.empty(NTARGET * nc, dtype=torch.float64, device="cuda")
+    out = {"fine": _mean_stats(fstats)}
+    walls, end_err = {}, {}
+    scale = [max(np.abs(fine_end[i] - start[i]).max(), 1e-300) for i in range(fine_end.shape[0])]
+    for name, coupling in runs.items():
+        sim = sims[name]
+        stats, wall = [], 0.0
+        for _ in range(nstat):
+            n = ncs // nstat
             while n > 0:
-                if learned:  # the closure's speed^2 from this run's own state
+                if coupling is not None:  # the closure's speed^2 from this run's own state
                     check(_lib.lib().css_box_filter(sim.h, 1, _ptr(fields), _ptr(targ)))
-                    Closure.attach(sim, clo.speed2(build_inputs(fields, dims, clo.qscale)))
+                    Closure.attach(sim, clo.speed2(build_inputs(fields, dims, clo.qscale), coupling, sim))
                 k = min(refresh, n)
-                sim.step_rk4(cdt, k)
+                wall += timed_steps(sim, cdt_run, k)
                 n -= k
-
-        advance(int(round(t_spin / cdt)))
-        cev = max(1, int(round(t_win / cdt)) // nsnap)
-        E, F = [], []
-        torch.cuda.synchronize()
-        t1 = time.perf_counter()
-        for _ in range(nsnap):
-            advance(cev)
-            v = sim.download()
-            e, fl = coarse_statistics(v[1], v[2], v[3], v[4] - sr[:, None, None], rhor, tr)
-            E.append(e)
-            F.append(fl)
-        torch.cuda.synchronize()
-        wall = time.perf_counter() - t1
+            stats.append(statistics(sim, rhor))
+        out[name] = _mean_stats(stats)
+        walls[name] = wall
+        v = sim.download()
+        end_err[name] = [float(np.abs(v[i] - fine_end[i]).max() / scale[i]) for i in range(v.shape[0])]
+        Closure.attach(sim, None)
         sim.close()
-        return np.mean(E, axis=0), np.mean(F, axis=0), wall
-
-    E0, F0, w0 = coarse_run(False)
-    E1, F1, w1 = coarse_run(True)
+    probe.close()
     fsim.close()
-    return {"spectrum_err_prescribed": rel_err(E0, Ef, 1), "spectrum_err_closure": rel_err(E1, Ef, 1),
-            "flux_err_prescribed": rel_err(F0, Ff), "flux_err_closure": rel_err(F1, Ff),
-            "fine_window_s": fine_wall, "coarse_window_s": w1, "coarse_prescribed_window_s": w0,
-            "wall_ratio": fine_wall / max(w1, 1e-12), "loss_first": float(np.mean(losses[:10])),
-            "loss_last": float(np.mean(losses[-10:])), "t_spin": t_spin, "t_win": t_win, "nsnap": nsnap,
-            "E_fine": Ef, "E_prescribed": E0, "E_closure": E1, "F_fine": Ff, "F_prescribed": F0, "F_closure": F1}
+    errs = {}
+    for name in runs:
+        e = {"E_K": rel_err(out[name]["E_K"], out["fine"]["E_K"], 1),
+             "F_en": rel_err(out[name]["F_en"], out["fine"]["F_en"]),
+             "F_ke": rel_err(out[name]["F_ke"], out["fine"]["F_ke"])}
+        if "E_M" in out["fine"]:
+            e["E_M"] = rel_err(out[name]["E_M"], out["fine"]["E_M"], 1)
+        errs[name] = e
+    return {"errors": errs, "end_state_error": end_err, "stats": out, "fine_window_s": fine_s,
+            "coarse_window_s": walls, "pre_spin_s": pre_s,
+            "wall_ratio": {k: fine_s / max(w, 1e-12) for k, w in walls.items()},
+            "loss_first": float(np.mean(losses[:10])), "loss_last": float(np.mean(losses[-10:])),
+            "fine_steps": fev * nstat, "coarse_steps": ncs, "coarse_dt": cdt_run, "fine_dt": fdt, "t_window": t_win,
+            "n_pre": n_pre, "n_adjust": n_adjust, "n_train": every * nsnap, "nsnap": nsnap, "nstat": nstat}

@@ -144,11 +144,7 @@ def initial_state(p, prof, info, seed=1234, samp=1e-4, vamp=0.0, b_rel=1e-3):
     taper = rtap[:, None, None] * (1.0 - np.cos(xv)[None, None, :] ** 16)
     rand = rand * taper
     v = np.zeros((nv, nr, nphi, nth))
-    bv = 0.5 * (p.omega_0 * p.r2) ** 2 / (p.cp * p.t0)
-    cvar = (rhor / info["rho0"]) ** gamm1
-    sth = np.sin(theta)
-    rs = (r[:, None] * sth[None, :] / p.r2) ** 2 - 1.0  # (nr, nth)
-    v[0] = (info["rho0"] * (cvar[:, None] + bv * rs) ** (1.0 / gamm1))[:, None, :]
+    v[0] = _rho_rotating(p, prof, info)[:, None, :]
     v[3] = vamp * rand
     v[4] = (1.0 + samp * rand) * sr[:, None, None]
     if p.magnetic:
@@ -166,6 +162,32 @@ def initial_state(p, prof, info, seed=1234, samp=1e-4, vamp=0.0, b_rel=1e-3):
         scale = b_rel * beq / brms if brms > 0 else 0.0
         v[5:8] = a * scale
     return np.ascontiguousarray(v)
+
+
+def _rho_rotating(p, prof, info):
+    """Density (nr, nth) of the polytrope in the rotating frame, the density
+    of the seeded initial state."""
+    prof = prof.reshape(NPROF, p.nr)
+    r, rhor = prof[1], prof[5]
+    theta = angles(p)[0]
+    gamm1 = p.gamma - 1.0
+    bv = 0.5 * (p.omega_0 * p.r2) ** 2 / (p.cp * p.t0)
+    cvar = (rhor / info["rho0"]) ** gamm1
+    rs = (r[:, None] * np.sin(theta)[None, :] / p.r2) ** 2 - 1.0
+    return info["rho0"] * (cvar[:, None] + bv * rs) ** (1.0 / gamm1)
+
+
+def background(p, prof, info):
+    """The initial state without its seeds, shape (nv, nr, nphi, nth): the
+    rotating polytrope's density, u = 0, s = sr(r), A = 0.  Each grid's
+    perturbations are measured from its own background when a state moves
+    between resolutions."""
+    nv = 8 if p.magnetic else 5
+    prof = np.asarray(prof).reshape(NPROF, p.nr)
+    v = np.zeros((nv, p.nr, p.nphi, p.nth))
+    v[0] = _rho_rotating(p, prof, info)[:, None, :]
+    v[4] = prof[6][:, None, None]
+    return v
 
 
 def curl_estimate(p, prof, a):

@@ -410,9 +410,31 @@ int css_closure_targets(long long nc, const double *targets,
                         const float *tscale, float *tn);
 int css_closure_speed2(long long nc, const float *y, const float *tscale,
                        double *speed2);
+/* css_closure_speed2_shaped: speed2[ncell of ctx] = the prescribed speed^2
+ * of the cell's radius (diffusion_speed, Initialize_Diffusion,
+ * diffusion.f90:19-63) times k / <k>_shell, k = max(0, tau_tt + tau_pp +
+ * tau_rr) of the cell and <k>_shell its mean over the cell's radius: each
+ * shell keeps the prescribed mean and the network places it; -1 where the
+ * output is not finite or the shell mean is not positive.  y holds one row
+ * per cell of ctx, in the state's cell order. */
+int css_closure_speed2_shaped(css_ctx *ctx, const float *y, const float *tscale,
+                              double *speed2);
+/* Grids of one run at two resolutions (same device, same variables, fine =
+ * f x coarse in r, theta and phi).  Bases are device arrays of the state's
+ * layout on their grid (each grid's background state), NULL meaning zero.
+ * css_restrict_state sets the coarse state to coarse_base + the f^3 box
+ * average of (fine state - fine_base): a coarse run started from the
+ * filtered fine perturbation, in its own grid's balance.  css_prolong_add
+ * adds to the fine state the trilinear (index-space; theta and r clamped,
+ * phi periodic) interpolation of (coarse state - coarse_base): a flow
+ * developed on the coarse grid carried to the fine grid as a perturbation
+ * of the fine grid's own state. */
+int css_restrict_state(css_ctx *fine, const double *fine_base, int f,
+                       css_ctx *coarse, const double *coarse_base);
+int css_prolong_add(css_ctx *coarse, const double *coarse_base, int f, css_ctx *fine);
 
-/* The closure network: n_in -> width -> width -> width -> n_out, exact
- * GELU after the hidden layers, BF16 weights and activations, FP32
+/* The closure network: n_in -> width -> width -> width -> n_out, GELU
+ * (tanh form, hardware tanh) after the hidden layers, BF16 weights and activations, FP32
  * accumulation (the products are tensor-core GEMMs), FP32 master weights
  * and Adam moments.  Rows are padded to multiples of 16 (dims[5] returns
  * the padded widths: the input rows of css_mlp_forward /
