@@ -178,6 +178,42 @@ def test_mlp_forward_and_gradients_match_numpy(gpu_available):
         assert np.abs(gb - rb).max() <= 5e-2 * np.abs(rb).max(), l
 
 
+def test_mlp_gradients_against_fp64_oracle(gpu_available):
+    """The device's gradients of one training step against the FP64 CPU
+    oracle (oracle/mlp.py: the same network and loss in exact arithmetic,
+    its backward pass pinned by finite differences in
+    tests/test_oracle_mlp.py), at the weights the device's products see
+    (the BF16 copies of its FP32 master weights).  The device rounds the
+    activations and the gradients fed to the products to BF16 (relative
+    4e-3 each); normwise, per layer, the weight and bias gradients are held
+    to 2e-2 of the oracle's and the loss to 1e-2."""
+    import torch
+    from css_b200 import closure as C
+    from oracle import mlp as M
+    rng = np.random.default_rng(4)
+    n = 4096
+    net = C.Mlp(135, 128, 12, max_rows=8192, seed=6)
+    x = np.zeros((n, 144), np.float32)
+    x[:, :135] = to_bf16(rng.standard_normal((n, 135)).astype(np.float32))
+    t = np.zeros((n, 16), np.float32)
+    t[:, :12] = rng.standard_normal((n, 12))
+    gloss = net.train_step(torch.from_numpy(x).to(torch.bfloat16).cuda(), torch.from_numpy(t).cuda(), n, 0.0)
+    W, B = [], []
+    for l in range(4):
+        w, b = net.params(l)
+        W.append(to_bf16(w).astype(np.float64))
+        B.append(np.asarray(b, dtype=np.float64))
+    loss64, g64 = M.loss_and_grads(W, B, x.astype(np.float64), t.astype(np.float64), 12)
+    assert abs(gloss - loss64) <= 1e-2 * loss64, (gloss, loss64)
+    for l in range(4):
+        gw, gb = net.grads(l)
+        rw, rb = g64[l]
+        ew = np.linalg.norm(gw - rw) / np.linalg.norm(rw)
+        eb = np.linalg.norm(gb - rb) / np.linalg.norm(rb)
+        print("layer %d: weight gradient %.2e, bias gradient %.2e of the FP64 oracle" % (l, ew, eb))
+        assert ew <= 2e-2 and eb <= 2e-2, (l, ew, eb)
+
+
 def test_mlp_learns_a_smooth_map(gpu_available):
     import torch
     from css_b200 import closure as C
