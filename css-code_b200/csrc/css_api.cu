@@ -25,6 +25,7 @@
 #include "css_lap.cuh"
 #include "css_inout.cuh"
 #include "css_fused.cuh"
+#include "css_voronoi.h"
 
 using namespace css;
 
@@ -86,6 +87,8 @@ struct css_ctx {
   double *io = nullptr, *io_part = nullptr, *rain = nullptr, *ash_slices = nullptr, *ashv = nullptr;
   double *squalls = nullptr;
   int squall_cap = 0;
+  double *lanes = nullptr;  // lane samples (3 per sample) + the running maximum's 8 bytes
+  size_t lane_cap = 0;
   // the run's clock: the step index the RHS sees (Program CSS2's istep),
   // sim_time, deltat; the ASH slice times; the RHS call number in progress
   long long istep = 0;
@@ -269,6 +272,7 @@ extern "C" void css_destroy(css_ctx *c) {
   cudaFree(c->lapbuf); cudaFree(c->lapface); cudaFree(c->radbuf); cudaFree(c->radface);
   cudaFree(c->io); cudaFree(c->io_part); cudaFree(c->rain); cudaFree(c->ash_slices); cudaFree(c->ashv);
   cudaFree(c->squalls);
+  cudaFree(c->lanes);
   for (auto e : c->ev) cudaEventDestroy(e);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -2954,8 +2958,111 @@ extern "C" int css_get_rain_fields(css_ctx *c, double *dvel_rain, double *dent_r
 
 // squalls: 6 per squall (theta_loc, phi_loc, size, scaling, vel, dels); the
 // grid point of each centre follows Find_Position (entropy_rain.f90:817-824)
+static int build_squalls(css_ctx *c, int sstruct, int nsq, const double *squalls, int add);
 extern "C" int css_build_squalls(css_ctx *c, int sstruct, int nsq, const double *squalls) {
   if (int rc = need_open(c, "css_build_squalls")) return rc;
+  return build_squalls(c, sstruct, nsq, squalls, 0);
+}
+extern "C" int css_add_squalls(css_ctx *c, int sstruct, int nsq, const double *squalls) {
+  if (int rc = need_open(c, "css_add_squalls")) return rc;
+  return build_squalls(c, sstruct, nsq, squalls, 1);
+}
+
+extern "C" int css_voronoi(int n, const double *x, const double *y, int *degree, int *start, int *face, int *nvert,
+                           double *vxy) {
+  if (n < 3 || !x || !y || !degree || !start || !face || !nvert || !vxy) {
+    set_err("css_voronoi: bad argument (at least 3 sites)");
+    return CSS_ERR_ARG;
+  }
+  std::vector<int> deg, st, fc;
+  std::vector<double> v;
+  if (vor_cells(n, x, y, deg, st, fc, v)) {
+    set_err("css_voronoi: coincident or degenerate sites (no unique Delaunay triangulation)");
+    return CSS_ERR_ARG;
+  }
+  for (int g = 0; g < n; g++) { degree[g] = deg[g]; start[g] = st[g]; }
+  std::copy(fc.begin(), fc.end(), face);
+  *nvert = (int)(v.size() / 2);
+  std::copy(v.begin(), v.end(), vxy);
+  return CSS_OK;
+}
+
+extern "C" int css_build_lanes(css_ctx *c, int ncells, const double *cells, double meansize, double meanvel,
+                               double meands) {
+  if (int rc = need_open(c, "css_build_lanes")) return rc;
+  if (ncells < 1 || !cells || !(meansize > 0.0)) {
+    set_err("css_build_lanes: bad argument (ncells >= 1, cells, meansize > 0)");
+    return CSS_ERR_ARG;
+  }
+  const css_params &p = c->p;
+  const double dth = (p.th2 - p.th1) / (double)(p.nth - 1), dphi = (p.phi2 - p.phi1) / (double)p.nphi;
+  // the sites and their periodic copies one domain width left and right
+  // (Initialize_Rain_Squalls / Update_Rain_Squalls, entropy_rain.f90:80-89, :374-385)
+  const int n3 = 3 * ncells;
+  std::vector<double> x(n3), y(n3), sc(n3);
+  for (int k = 0; k < ncells; k++) {
+    const double *q = cells + 3 * k;
+    if (!(q[2] >= 0.0)) { set_err("css_build_lanes: cell %d has scaling %g (must be >= 0)", k, q[2]); return CSS_ERR_ARG; }
+    for (int cpy = 0; cpy < 3; cpy++) {
+      const int i = k + cpy * ncells;
+      x[i] = cpy == 0 ? q[0] : cpy == 1 ? q[0] - (p.phi2 - p.phi1) : (p.phi2 - p.phi1) + q[0];
+      y[i] = q[1];
+      sc[i] = q[2];
+    }
+  }
+  std::vector<int> deg, st, fc;
+  std::vector<double> v;
+  if (vor_cells(n3, x.data(), y.data(), deg, st, fc, v)) {
+    set_err("css_build_lanes: coincident or degenerate cell sites");
+    return CSS_ERR_ARG;
+  }
+  // the points along every cell edge (Build_Downflow_Lanes, entropy_rain.f90:667-703)
+  const int nmax = (int)std::sqrt((double)p.nth * p.nth + (double)p.nphi * p.nphi);
+  std::vector<double> smp;
+  for (int ic = 0; ic < n3; ic++)
+    for (int ie = 0; ie < deg[ic]; ie++) {
+      const int a = fc[st[ic] + ie], b = fc[st[ic] + (ie + 1 < deg[ic] ? ie + 1 : 0)];
+      const double x1 = v[2 * a], y1 = v[2 * a + 1];
+      const double dvx = v[2 * b] - x1, dvy = v[2 * b + 1] - y1;
+      const double gx = dvx / dphi, gy = dvy / dth;
+      const double len = std::sqrt(gx * gx + gy * gy);
+      const int my = len >= (double)nmax ? nmax : (int)len;
+      for (int k = 0; k < my; k++) {
+        const double t = (double)k / (double)my;
+        smp.push_back(x1 + dvx * t);
+        smp.push_back(y1 + dvy * t);
+        smp.push_back(sc[ic]);
+      }
+    }
+  const int ns = (int)(smp.size() / 3);
+  const size_t need = smp.size() + 1;
+  if (need > c->lane_cap) {
+    cudaFree(c->lanes);
+    c->lanes = nullptr;
+    c->lane_cap = 0;
+    CUDA_TRY(cudaMalloc(&c->lanes, need * sizeof(double)));
+    c->lane_cap = need;
+  }
+  unsigned long long *maxbits = reinterpret_cast<unsigned long long *>(c->lanes + smp.size());
+  if (ns > 0) CUDA_TRY(cudaMemcpyAsync(c->lanes, smp.data(), smp.size() * 8, cudaMemcpyHostToDevice, c->stream));
+  CUDA_TRY(cudaMemsetAsync(maxbits, 0, 8, c->stream));
+  // isz_max (Initialize_Rain_Squalls, entropy_rain.f90:58): the window margin in cells
+  double smin = 1.0;
+  for (int it = 0; it < p.nth; it++) smin = std::min(smin, std::sin(dth * (double)it + p.th1));
+  const int isz = (int)std::ceil(meansize * std::sqrt(-std::log(1e-5)) / (p.r2 * std::min(dth, dphi * smin)));
+  const double rtmp = (p.r2 / meansize) * (p.r2 / meansize);
+  const size_t np = (size_t)p.nth * p.nphi;
+  k_lanes<<<(unsigned)((np + 255) / 256), 256, 0, c->stream>>>(c->g, c->lanes, ns, p.phi1, isz * dphi, isz * dth,
+                                                               rtmp, c->rain, maxbits);
+  if (int rc = check_launch(c)) return rc;
+  k_lanes_scale<<<(unsigned)((np + 255) / 256), 256, 0, c->stream>>>(np, maxbits, meanvel, meands, c->rain,
+                                                                     c->rain + np);
+  if (int rc = check_launch(c)) return rc;
+  CUDA_TRY(cudaStreamSynchronize(c->stream));
+  return CSS_OK;
+}
+
+static int build_squalls(css_ctx *c, int sstruct, int nsq, const double *squalls, int add) {
   if (nsq < 0 || (nsq > 0 && !squalls) || (sstruct != 0 && sstruct != 1)) {
     set_err("css_build_squalls: bad argument");
     return CSS_ERR_ARG;
@@ -2981,7 +3088,7 @@ extern "C" int css_build_squalls(css_ctx *c, int sstruct, int nsq, const double 
   if (nsq > 0) CUDA_TRY(cudaMemcpyAsync(c->squalls, sq.data(), (size_t)8 * nsq * 8, cudaMemcpyHostToDevice, c->stream));
   const size_t np = (size_t)p.nth * p.nphi;
   k_squalls<<<(unsigned)((np + 255) / 256), 256, 0, c->stream>>>(c->g, c->squalls, nsq, sstruct == 0, p.phi1, p.phi2,
-                                                                    c->rain, c->rain + np);
+                                                                    add, c->rain, c->rain + np);
   if (int rc = check_launch(c)) return rc;
   CUDA_TRY(cudaStreamSynchronize(c->stream));
   return CSS_OK;

@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(IO_NT) k_ash_flux(CssGeo g, const double *__re
 // the periodic images on the first and last phi blocks; terms below 1e-5
 // are dropped (polynomials: beyond the squall's size).
 __global__ void k_squalls(CssGeo g, const double *__restrict__ sq, int nsq, int poly, double phi1, double phi2,
-                          double *__restrict__ dvel, double *__restrict__ dent) {
+                          int add, double *__restrict__ dvel, double *__restrict__ dent) {
   const size_t np = (size_t)g.nth * g.nphi;
   for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < np; id += (size_t)gridDim.x * blockDim.x) {
     const int it = (int)(id % g.nth), ip = (int)(id / g.nth);
@@ -273,8 +273,60 @@ __global__ void k_squalls(CssGeo g, const double *__restrict__ sq, int nsq, int 
         }
       }
     }
-    dvel[id] = acc[1];
-    dent[id] = acc[2];
+    if (add) {  // on top of the downflow lanes, as Update_Rain_Squalls builds them after the lanes
+      dvel[id] += acc[1];
+      dent[id] += acc[2];
+    } else {
+      dvel[id] = acc[1];
+      dent[id] = acc[2];
+    }
+  }
+}
+
+// Build_Downflow_Lanes (entropy_rain.f90:657-713), one thread per top-plane
+// cell.  smp: 3 per lane sample (phi, theta, scaling of its cell), in the
+// reference's order (cell, edge, point along the edge).  A sample counts
+// for a cell when it lies in the window of the cell's block: the block's
+// theta and phi range widened by xsz in phi and ysz in theta, as each top
+// rank's window is.  The cell's sum of scaling * exp(-rtmp * distance^2)
+// runs in sample order; a term whose exponent is below -746 is zero in
+// double precision and is skipped.  *maxbits collects the largest sum
+// (sums are non-negative, so their bit patterns order as the values do).
+__global__ void k_lanes(CssGeo g, const double *__restrict__ smp, int ns, double phi1, double xsz, double ysz,
+                        double rtmp, double *__restrict__ dvel, unsigned long long *__restrict__ maxbits) {
+  const size_t np = (size_t)g.nth * g.nphi;
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < np; id += (size_t)gridDim.x * blockDim.x) {
+    const int it = (int)(id % g.nth), ip = (int)(id / g.nth);
+    int jb = 0, kb = 0;
+    while (jb + 1 < g.d[1].nb && g.d[1].start[jb + 1] <= it) jb++;
+    while (kb + 1 < g.d[2].nb && g.d[2].start[kb + 1] <= ip) kb++;
+    const int t0 = g.d[1].start[jb], t1 = t0 + g.d[1].size[jb] - 1;
+    const int p0 = g.d[2].start[kb], p1 = p0 + g.d[2].size[kb] - 1;
+    const double xlo = g.dphi * (double)p0 + phi1 - xsz, xhi = g.dphi * (double)p1 + phi1 + xsz;
+    const double ylo = g.theta[t0] - ysz, yhi = g.theta[t1] + ysz;
+    const double th = g.theta[it], ph = g.dphi * (double)ip + phi1;
+    double acc = 0.0;
+    for (int s = 0; s < ns; s++) {
+      const double xv = smp[3 * s], yv = smp[3 * s + 1];
+      if (!(xv >= xlo && xv <= xhi && yv >= ylo && yv <= yhi)) continue;
+      const double a = th - yv, b = ph - xv;
+      const double e = rtmp * (a * a + b * b);
+      if (e <= 746.0) acc += smp[3 * s + 2] * exp(-e);
+    }
+    dvel[id] = acc;
+    atomicMax(maxbits, (unsigned long long)__double_as_longlong(acc));
+  }
+}
+
+// the lanes' normalisation: dvel / max(largest, 1), then dent = meands
+// times it and dvel = meanvel times it (entropy_rain.f90:708-712)
+__global__ void k_lanes_scale(size_t np, const unsigned long long *__restrict__ maxbits, double meanvel,
+                              double meands, double *__restrict__ dvel, double *__restrict__ dent) {
+  const double m = fmax(__longlong_as_double((long long)*maxbits), 1.0);
+  for (size_t id = blockIdx.x * (size_t)blockDim.x + threadIdx.x; id < np; id += (size_t)gridDim.x * blockDim.x) {
+    const double d = dvel[id] / m;
+    dent[id] = meands * d;
+    dvel[id] = meanvel * d;
   }
 }
 

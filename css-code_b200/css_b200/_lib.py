@@ -112,6 +112,10 @@ def lib():
         L.css_set_rain_fields.argtypes = [vp, dp, dp]
         L.css_get_rain_fields.argtypes = [vp, dp, dp]
         L.css_build_squalls.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+        L.css_add_squalls.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+        L.css_build_lanes.argtypes = [vp, ctypes.c_int, dp, ctypes.c_double, ctypes.c_double, ctypes.c_double]
+        ip = ctypes.POINTER(ctypes.c_int)
+        L.css_voronoi.argtypes = [ctypes.c_int, dp, dp, ip, ip, ip, ip, dp]
         L.css_set_ash_slices.argtypes = [vp, dp, dp, ctypes.c_double]
         _LIB = L
     return _LIB
@@ -135,7 +139,8 @@ EXPORTS = [
     "css_closure_speed2_shaped", "css_restrict_state", "css_prolong_add", "css_mlp_create",
     "css_mlp_destroy", "css_mlp_dims", "css_mlp_forward", "css_mlp_train_step", "css_mlp_params", "css_mlp_grads",
     "css_mlp_set_stream", "css_mlp_set_fused", "css_set_clock", "css_get_clock", "css_inout_init",
-    "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_squalls",
+    "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_squalls", "css_add_squalls",
+    "css_build_lanes", "css_voronoi",
     "css_set_ash_slices", "css_download_plane", "css_dbydr", "css_d2bydr2", "css_dbydt", "css_d2bydt2",
     "css_dbydp", "css_d2bydp2", "css_bound",
 ]

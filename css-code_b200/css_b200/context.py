@@ -239,6 +239,17 @@ class Simulation:
         sq = np.ascontiguousarray(squalls, dtype=np.float64).reshape(-1, 6)
         check(_lib.lib().css_build_squalls(self.h, int(sstruct), sq.shape[0], _p(sq)))
 
+    def add_squalls(self, squalls, sstruct=1):
+        """The same squalls added to the current rain fields (after the lanes)."""
+        sq = np.ascontiguousarray(squalls, dtype=np.float64).reshape(-1, 6)
+        check(_lib.lib().css_add_squalls(self.h, int(sstruct), sq.shape[0], _p(sq)))
+
+    def build_lanes(self, cells, meansize, meanvel, meands):
+        """Downflow lanes (css_build_lanes): cells (n, 3) phi_loc, theta_loc,
+        scaling of the convection-cell sites; replaces the rain fields."""
+        cl = np.ascontiguousarray(cells, dtype=np.float64).reshape(-1, 3)
+        check(_lib.lib().css_build_lanes(self.h, cl.shape[0], _p(cl), float(meansize), float(meanvel), float(meands)))
+
     def set_ash_slices(self, slices, times, ash_fen_mod):
         """slices: (4 times, 4 fields u_r, u_theta, u_phi, s, nphi, nth)."""
         check(_lib.lib().css_set_ash_slices(self.h, _p(np.ascontiguousarray(slices, dtype=np.float64)),

@@ -5,12 +5,15 @@ top inflow/outflow relaxation that reads its fields.
 As in the reference the squall bookkeeping is host work between steps
 (Update_Rain_Squalls runs after every ufreq/10-th step on the top ranks,
 step_rk4.f90:484-486); only the fields are built on the device.  Restated:
-Initialize_Rain_Squalls for squalls (entropy_rain.f90:113-153; the Voronoi
-downflow lanes are not built), both squall shapes (sstruct 1 Gaussian,
+Initialize_Rain_Squalls for squalls (entropy_rain.f90:113-153), both squall shapes (sstruct 1 Gaussian,
 0 polynomial, built on the device), Update_Rain_Squalls (:316-419),
 Temporal_Structure (:851-880), Find_Position (:817-824),
 Generate_New_Squall_Parameters (:737-814), Place_Cell (:930-945) and
-Random_Exponential (:947-962).
+Random_Exponential (:947-962); for the downflow lanes (build_lanes) the
+convection cells' life cycle (ConvectionCells: Initialize_Rain_Squalls
+:67-111, Update_Rain_Squalls :181-314, Generate_New_Cell_Parameters
+:715-735, Find_Cell_Position :827-834, Temporal_Structure_Cell :836-849),
+their Voronoi cells and lane field being the library's (css_build_lanes).
 
 The reference seeds Fortran's random_number from system_clock
 (:60-61), so its draws differ from run to run; here a seeded numpy
@@ -160,7 +163,116 @@ class RainSqualls:
         return built
 
 
-def advance(sim, rain, dt, nsteps, ufreq):
+class ConvectionCells:
+    """The convection cells whose Voronoi edges are the downflow lanes
+    (build_lanes).  ncells sites placed uniformly (Place_Cell), lasting
+    1e12 (Generate_New_Cell_Parameters), their scaling ramping as
+    sin^2(pi (t - t0) / 2e4) over the first 1e4 time units
+    (Temporal_Structure_Cell), advected by the mean surface flow of their
+    theta row and replaced when they leave the theta range
+    (Update_Rain_Squalls).  meansize, stopin (meands) and utopin (meanvel)
+    are the rain namelist values shared with RainSqualls."""
+
+    def __init__(self, p, ncells, meansize, stopin, utopin, seed=0, sim_time=0.0, rng=None):
+        self.p = p
+        self.rng = rng if rng is not None else np.random.default_rng(seed)
+        self.r2 = p.r2
+        self.dth = (p.th2 - p.th1) / (p.nth - 1)
+        self.dphi = (p.phi2 - p.phi1) / p.nphi
+        self.meansize, self.meands, self.meanvel = float(meansize), float(stopin), float(utopin)
+        n = int(ncells)
+        self.phi, self.theta, self.dur = self.generate(n)
+        self.start = np.full(n, sim_time - 1.0)
+        self.scaling = np.zeros(n)
+        self.loct = np.zeros(n, dtype=np.int64)
+        self.locp = np.zeros(n, dtype=np.int64)
+        for k in range(n):
+            self.find_position(k)
+
+    def place_cell(self):
+        p = self.p
+        th0 = 2.0 * p.th2
+        while th0 > p.th2 or th0 < p.th1:
+            th0 = p.th1 + (p.th2 - p.th1) * (1.1 * self.rng.random() - 0.1)
+        ph0 = 2.0 * p.phi2
+        while ph0 > p.phi2 or ph0 < p.phi1:
+            ph0 = p.phi1 + (p.phi2 - p.phi1) * (1.1 * self.rng.random() - 0.1)
+        return th0, ph0
+
+    def generate(self, n):
+        """Generate_New_Cell_Parameters: positions, duration 1e12."""
+        phi, theta = np.empty(n), np.empty(n)
+        for k in range(n):
+            theta[k], phi[k] = self.place_cell()
+        return phi, theta, np.full(n, 1e12)
+
+    def find_position(self, k):
+        p = self.p
+        self.loct[k] = max(min(math.floor((self.theta[k] - p.th1) / self.dth) + 1, p.nth), 1)
+        self.locp[k] = max(min(math.floor((self.phi[k] - p.phi1) / self.dphi) + 1, p.nphi), 1)
+
+    def temporal_structure(self, k, t):
+        dt_ = t - self.start[k]
+        self.scaling[k] = math.sin(math.pi * dt_ / 2e4) ** 2 if dt_ <= 1e4 else 1.0
+
+    def cells(self):
+        """(n, 3) phi_loc, theta_loc, scaling for build_lanes."""
+        return np.stack([self.phi, self.theta, self.scaling], axis=1)
+
+    def update(self, sim_time, deltat, vs_theta, vs_phi):
+        """The cells' part of Update_Rain_Squalls: vs_theta / vs_phi are the
+        theta profiles (length nth) of u_theta and u_phi averaged over phi
+        and the top block's radii; the sites move by deltat * vs / r2, the
+        ones that left the theta range (or outlived their duration) are
+        replaced after the scalings are set.  Returns the cells to build
+        the lanes from."""
+        p = self.p
+        n = self.phi.size
+        iup = np.zeros(n, dtype=bool)
+        for k in range(n):
+            if self.start[k] + self.dur[k] <= sim_time:
+                iup[k] = True
+                continue
+            lct = self.loct[k]
+            self.temporal_structure(k, sim_time)
+            self.theta[k] = self.theta[k] + deltat * vs_theta[lct - 1] / self.r2
+            if self.theta[k] <= p.th1 or self.theta[k] >= p.th2:
+                self.start[k] = 0.0
+                iup[k] = True
+            self.phi[k] = self.phi[k] + deltat * vs_phi[lct - 1] / self.r2
+            if self.phi[k] <= p.phi1:
+                self.phi[k] = p.phi2 + (self.phi[k] - p.phi1)
+            if self.phi[k] >= p.phi2:
+                self.phi[k] = p.phi1 + (self.phi[k] - p.phi2)
+            self.find_position(k)
+        nup = int(iup.sum())
+        if nup:
+            phi, theta, dur = self.generate(nup)
+            for j, k in enumerate(np.flatnonzero(iup)):
+                self.phi[k], self.theta[k], self.dur[k] = phi[j], theta[j], dur[j]
+                self.start[k] = sim_time
+                self.scaling[k] = 0.0
+                self.find_position(k)
+        return self.cells()
+
+
+def top_block_mean_velocity(sim):
+    """theta profiles of u_theta and u_phi averaged over phi and the radii of
+    the top radial block (what each top rank sums before the all-reduce,
+    entropy_rain.f90:185-196)."""
+    p = sim.p
+    nr, nn = p.nr, p.nnr
+    base, rem = nr // nn, nr % nn
+    size_top = base + 1 if (rem > 0 and nn <= rem) else base  # Partition (parallel_mpi.f90:236-343)
+    vt = np.zeros(p.nth)
+    vp = np.zeros(p.nth)
+    for ir in range(nr - size_top, nr):
+        vt += sim.plane(1, ir).sum(axis=0)
+        vp += sim.plane(2, ir).sum(axis=0)
+    return vt / (size_top * p.nphi), vp / (size_top * p.nphi)
+
+
+def advance(sim, rain, dt, nsteps, ufreq, lanes=None):
     """nsteps steps of a top_inout + do_entropy_rain Simulation with the
     rain model updated after every (ufreq // 10)-th step, as Step_RK4 does
     (step_rk4.f90:484-486): the fields of the update take effect from the
@@ -173,5 +285,11 @@ def advance(sim, rain, dt, nsteps, ufreq):
         sim.step_rk4(dt, 1)
         istep, t_end = sim.clock()
         if istep % every == 0:
+            if lanes is not None:  # the lanes first, the squalls on top of them
+                vt, vp = top_block_mean_velocity(sim)
+                sim.build_lanes(lanes.update(t_end - dt, dt, vt, vp), lanes.meansize, lanes.meanvel, lanes.meands)
             built = rain.update(t_end - dt, dt, sim.plane(1, nr - 1), sim.plane(2, nr - 1))
-            sim.build_squalls(built, rain.sstruct)
+            if lanes is not None:
+                sim.add_squalls(built, rain.sstruct)
+            else:
+                sim.build_squalls(built, rain.sstruct)

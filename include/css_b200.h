@@ -537,6 +537,30 @@ int css_inout_state(css_ctx *ctx, double *out);
 int css_set_rain_fields(css_ctx *ctx, const double *dvel_rain, const double *dent_rain);
 int css_get_rain_fields(css_ctx *ctx, double *dvel_rain, double *dent_rain);
 int css_build_squalls(css_ctx *ctx, int sstruct, int nsq, const double *squalls);
+/* css_add_squalls: the same squalls added to the current fields instead of
+ * replacing them -- Update_Rain_Squalls builds its squalls on top of the
+ * downflow lanes (entropy_rain.f90:171-421). */
+int css_add_squalls(css_ctx *ctx, int sstruct, int nsq, const double *squalls);
+/* Downflow lanes of entropy rain (build_lanes): Build_Downflow_Lanes
+ * (entropy_rain.f90:657-713) on the Voronoi cells of the convection-cell
+ * sites.  cells[3*k ..] = phi_loc, theta_loc, scaling (>= 0) of the ncells
+ * sites; the periodic copies one phi-domain width to each side are added
+ * here (:80-89).  Replaces dvel_rain / dent_rain by meanvel and meands
+ * times the lane field over max(its maximum, 1); meansize sets the lanes'
+ * width (r2/meansize)^2 and, through isz_max (:58), the window a top block
+ * sees.  The Voronoi cells are computed on the host (css_voronoi); the
+ * field on the device.  The cells' life cycle is the caller's. */
+int css_build_lanes(css_ctx *ctx, int ncells, const double *cells, double meansize,
+                    double meanvel, double meands);
+/* css_voronoi: Voronoi cells of n >= 3 distinct sites (x, y) in the form of
+ * Compute_Voronoi (voronoi.f90:30-280): degree[g] vertices of site g's
+ * cell at face[start[g] ..], indices into vxy (2 per vertex, nvert of
+ * them: the circumcentres of the Delaunay triangles); a cell inside the
+ * hull is walked clockwise, one on the hull from its most clockwise
+ * triangle counterclockwise.  face needs room for 6n entries, vxy for 4n.
+ * Host only (no device work). */
+int css_voronoi(int n, const double *x, const double *y, int *degree, int *start,
+                int *face, int *nvert, double *vxy);
 
 /* Prescribed bottom (bottom_specified): the four time slices of the ASH
  * fields after the reader's spatial interpolation and wall taper

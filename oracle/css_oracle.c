@@ -2722,15 +2722,23 @@ int orc_set_ash_slices(orc_ctx *c, const double *slices, const double *times, do
  * squall density 1/(1 + sum) (of |term| for the polynomial) then
  * weights each squall's velocity and entropy.  sq: 6 per squall, theta_loc,
  * phi_loc, size, scaling, vel, dels. */
-int orc_build_squalls(orc_ctx *c, int sstruct, int nsq, const double *sq) {
+static int squalls_into(orc_ctx *c, int sstruct, int nsq, const double *sq, int add);
+int orc_build_squalls(orc_ctx *c, int sstruct, int nsq, const double *sq) { return squalls_into(c, sstruct, nsq, sq, 0); }
+/* the squalls on top of the current fields (after the lanes, as
+   Update_Rain_Squalls adds them, entropy_rain.f90:171-421) */
+int orc_add_squalls(orc_ctx *c, int sstruct, int nsq, const double *sq) { return squalls_into(c, sstruct, nsq, sq, 1); }
+
+static int squalls_into(orc_ctx *c, int sstruct, int nsq, const double *sq, int add) {
   const css_params *p = &c->p;
   if (!c->dvel_rain) { set_err("orc_build_squalls: the run has no open boundary"); return CSS_ERR_ARG; }
   const int poly = sstruct == 0;
   int nth = c->nth, nphi = c->nphi;
   size_t np = (size_t)nth * nphi;
   double *dens = dalloc(np);
-  memset(c->dvel_rain, 0, sizeof(double) * np);
-  memset(c->dent_rain, 0, sizeof(double) * np);
+  if (!add) {
+    memset(c->dvel_rain, 0, sizeof(double) * np);
+    memset(c->dent_rain, 0, sizeof(double) * np);
+  }
   for (int pass = 0; pass < 2; pass++) {
     for (int k = 0; k < c->nblk; k++) {
       const blk_t *B = &c->blk[k];
@@ -3222,4 +3230,166 @@ int orc_cyclic_lines(const double *x, double *dx, int n, int nlines, int order, 
   }
   free(z);
   return CSS_OK;
+}
+
+/* ------------------------------------------------------------------------
+ * Voronoi cells (Compute_Voronoi, voronoi.f90:30-280) and the downflow
+ * lanes of entropy rain (Build_Downflow_Lanes, entropy_rain.f90:657-713).
+ *
+ * The Delaunay triangulation here is the definition itself, by brute
+ * force: every triple of sites whose circumcircle holds no other site,
+ * stored counterclockwise, in lexicographic order of the triple (the
+ * reference builds it incrementally, dtris2 of voronoi.f90:376-681; for
+ * sites in general position the triangles are the same, only their
+ * numbering differs).  The walk around each site restates Compute_Voronoi's
+ * loops (:129-276): from the first triangle holding the site, step to the
+ * triangle across the edge to the next node until the start returns or
+ * the hull is met; then walk again from there, recording the triangles.
+ * ------------------------------------------------------------------------ */
+static double orc_orient(double ax, double ay, double bx, double by, double cx, double cy) {
+  return (bx - ax) * (cy - ay) - (by - ay) * (cx - ax);
+}
+
+int orc_voronoi(int n, const double *x, const double *y, int *degree, int *start, int *face, int *nvert,
+                double *vxy) {
+  if (n < 3) { set_err("orc_voronoi: fewer than 3 sites"); return CSS_ERR_ARG; }
+  int cap = 2 * n + 8, nt = 0;
+  int *tri = (int *)malloc(sizeof(int) * 3 * cap);
+  for (int i = 0; i < n; i++)
+    for (int j = i + 1; j < n; j++)
+      for (int k = j + 1; k < n; k++) {
+        double o = orc_orient(x[i], y[i], x[j], y[j], x[k], y[k]);
+        if (o == 0.0) continue;
+        /* circumcircle of (i, j, k), relative to site i */
+        double bx = x[j] - x[i], by = y[j] - y[i], cx = x[k] - x[i], cy = y[k] - y[i];
+        double d = 2.0 * (bx * cy - by * cx), b2 = bx * bx + by * by, c2 = cx * cx + cy * cy;
+        double ux = x[i] + (cy * b2 - by * c2) / d, uy = y[i] + (bx * c2 - cx * b2) / d;
+        double rr = (x[i] - ux) * (x[i] - ux) + (y[i] - uy) * (y[i] - uy);
+        int empty = 1;
+        for (int m = 0; m < n && empty; m++) {
+          if (m == i || m == j || m == k) continue;
+          double dx = x[m] - ux, dy = y[m] - uy;
+          if (dx * dx + dy * dy < rr) empty = 0;
+        }
+        if (!empty) continue;
+        if (nt == cap) { free(tri); set_err("orc_voronoi: degenerate sites"); return CSS_ERR_ARG; }
+        tri[3 * nt] = i;
+        tri[3 * nt + 1] = o > 0.0 ? j : k;
+        tri[3 * nt + 2] = o > 0.0 ? k : j;
+        vxy[2 * nt] = ux;
+        vxy[2 * nt + 1] = uy;
+        nt++;
+      }
+  *nvert = nt;
+  for (int g = 0; g < n; g++) degree[g] = 0;
+  for (int v = 0; v < nt; v++)
+    for (int s = 0; s < 3; s++) degree[tri[3 * v + s]]++;
+  int count = 0;
+  for (int g = 0; g < n; g++) {
+    int vn = -1, sn = -1;
+    for (int v = 0; v < nt && vn < 0; v++)
+      for (int s = 0; s < 3; s++)
+        if (tri[3 * v + s] == g) { vn = v; sn = s; break; }
+    start[g] = count;
+    if (vn < 0) continue;
+    /* one step: across the edge from g to the node after the current one */
+#define ORC_VOR_STEP()                                                      \
+  do {                                                                      \
+    sn = (sn + 1) % 3;                                                      \
+    gn = tri[3 * vn + sn];                                                  \
+    if (gn == g) { sn = (sn + 1) % 3; gn = tri[3 * vn + sn]; }              \
+    vold = vn;                                                              \
+    vn = -1;                                                                \
+    for (int v = 0; v < nt && vn < 0; v++) {                                \
+      if (v == vold) continue;                                              \
+      for (int s = 0; s < 3; s++)                                           \
+        if (tri[3 * v + s] == g) {                                          \
+          int s1 = (s + 1) % 3;                                             \
+          if (tri[3 * v + s1] == gn) { vn = v; sn = s1; break; }            \
+          s1 = (s + 2) % 3;                                                 \
+          if (tri[3 * v + s1] == gn) { vn = v; sn = s1; break; }            \
+        }                                                                   \
+    }                                                                       \
+  } while (0)
+    int gn, vold, vsave = vn;
+    for (;;) {
+      ORC_VOR_STEP();
+      if (vn == vsave) break;
+      if (vn < 0) { vn = vold; break; }
+    }
+    vsave = vn;
+    face[count++] = vn;
+    for (;;) {
+      ORC_VOR_STEP();
+      if (vn == vsave || vn < 0) break;
+      face[count++] = vn;
+    }
+#undef ORC_VOR_STEP
+  }
+  free(tri);
+  return CSS_OK;
+}
+
+/* Build_Downflow_Lanes (entropy_rain.f90:657-713) with the periodic copies
+   of the sites (:80-89); cells[3k..] = phi_loc, theta_loc, scaling.  Each
+   top block (rank) walks every cell edge and adds the Gaussian of every
+   edge point inside its window to all of its cells. */
+int orc_build_lanes(orc_ctx *c, int ncells, const double *cells, double meansize, double meanvel, double meands) {
+  const css_params *p = &c->p;
+  if (!c->dvel_rain) { set_err("orc_build_lanes: the run has no open boundary"); return CSS_ERR_ARG; }
+  int nth = c->nth, nphi = c->nphi, n3 = 3 * ncells;
+  size_t np = (size_t)nth * nphi;
+  double *x = dalloc(n3), *y = dalloc(n3), *sc = dalloc(n3), *vxy = dalloc(4 * (size_t)n3 + 16);
+  int *deg = (int *)calloc(n3, sizeof(int)), *st = (int *)calloc(n3, sizeof(int));
+  int *fc = (int *)calloc(6 * (size_t)n3 + 32, sizeof(int)), nv = 0;
+  for (int k = 0; k < ncells; k++) {
+    x[k] = cells[3 * k];
+    x[k + ncells] = cells[3 * k] - (p->phi2 - p->phi1);
+    x[k + 2 * ncells] = (p->phi2 - p->phi1) + cells[3 * k];
+    y[k] = y[k + ncells] = y[k + 2 * ncells] = cells[3 * k + 1];
+    sc[k] = sc[k + ncells] = sc[k + 2 * ncells] = cells[3 * k + 2];
+  }
+  int rc = orc_voronoi(n3, x, y, deg, st, fc, &nv, vxy);
+  if (rc == CSS_OK) {
+    double smin = 1.0;
+    for (int it = 0; it < nth; it++) smin = fmin(smin, sin(c->theta[it]));
+    int isz = (int)ceil(meansize * sqrt(-log(1e-5)) / (p->r2 * fmin(c->dth, c->dphi * smin)));
+    int nmax = (int)sqrt((double)nth * nth + (double)nphi * nphi);
+    double xsz = isz * c->dphi, ysz = isz * c->dth, rtmp = (p->r2 / meansize) * (p->r2 / meansize);
+    memset(c->dvel_rain, 0, sizeof(double) * np);
+    for (int b = 0; b < c->nblk; b++) {
+      const blk_t *B = &c->blk[b];
+      if (!B->rhi) continue;
+      double xlo = c->phi[B->p0] - xsz, xhi = c->phi[B->p0 + B->np - 1] + xsz;
+      double ylo = c->theta[B->t0] - ysz, yhi = c->theta[B->t0 + B->nt - 1] + ysz;
+      for (int ic = 0; ic < n3; ic++)
+        for (int ie = 0; ie < deg[ic]; ie++) {
+          int va = fc[st[ic] + ie], vb = fc[st[ic] + (ie + 1 < deg[ic] ? ie + 1 : 0)];
+          double x1 = vxy[2 * va], y1 = vxy[2 * va + 1];
+          double dvx = vxy[2 * vb] - x1, dvy = vxy[2 * vb + 1] - y1;
+          double gx = dvx / c->dphi, gy = dvy / c->dth, len = sqrt(gx * gx + gy * gy);
+          int my = len >= (double)nmax ? nmax : (int)len;
+          for (int k = 0; k < my; k++) {
+            double t = (double)k / (double)my, xv = x1 + dvx * t, yv = y1 + dvy * t;
+            if (!(xv >= xlo && xv <= xhi && yv >= ylo && yv <= yhi)) continue;
+            for (int ip = B->p0; ip < B->p0 + B->np; ip++)
+              for (int it = B->t0; it < B->t0 + B->nt; it++) {
+                double a = c->theta[it] - yv, bb = c->phi[ip] - xv;
+                size_t id = it + (size_t)nth * ip;
+                c->dvel_rain[id] = c->dvel_rain[id] + sc[ic] * exp(-rtmp * (a * a + bb * bb));
+              }
+          }
+        }
+    }
+    double m = 0.0;
+    for (size_t i = 0; i < np; i++) m = fmax(m, c->dvel_rain[i]);
+    m = fmax(m, 1.0);
+    for (size_t i = 0; i < np; i++) {
+      double d = c->dvel_rain[i] / m;
+      c->dent_rain[i] = meands * d;
+      c->dvel_rain[i] = meanvel * d;
+    }
+  }
+  free(x); free(y); free(sc); free(vxy); free(deg); free(st); free(fc);
+  return rc;
 }

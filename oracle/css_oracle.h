@@ -74,6 +74,13 @@ int orc_set_rain_fields(orc_ctx *c, const double *dvel, const double *dent);
 int orc_rain_fields(orc_ctx *c, double *dvel, double *dent);
 int orc_set_ash_slices(orc_ctx *c, const double *slices, const double *times, double ash_fen_mod);
 int orc_build_squalls(orc_ctx *c, int sstruct, int nsq, const double *sq);
+int orc_add_squalls(orc_ctx *c, int sstruct, int nsq, const double *sq);
+/* Voronoi cells (Compute_Voronoi, voronoi.f90:30-280; brute-force
+ * Delaunay) and the downflow lanes (Build_Downflow_Lanes,
+ * entropy_rain.f90:657-713), outputs as css_voronoi / css_build_lanes */
+int orc_voronoi(int n, const double *x, const double *y, int *degree, int *start, int *face, int *nvert,
+                double *vxy);
+int orc_build_lanes(orc_ctx *c, int ncells, const double *cells, double meansize, double meanvel, double meands);
 
 #ifdef __cplusplus
 }

@@ -55,6 +55,11 @@ def lib():
         L.orc_rain_fields.argtypes = [ctypes.c_void_p, _dp, _dp]
         L.orc_set_ash_slices.argtypes = [ctypes.c_void_p, _dp, _dp, ctypes.c_double]
         L.orc_build_squalls.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+        L.orc_add_squalls.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, _dp]
+        _ip = ctypes.POINTER(ctypes.c_int)
+        L.orc_voronoi.argtypes = [ctypes.c_int, _dp, _dp, _ip, _ip, _ip, _ip, _dp]
+        L.orc_build_lanes.argtypes = [ctypes.c_void_p, ctypes.c_int, _dp, ctypes.c_double, ctypes.c_double,
+                                      ctypes.c_double]
         L.orc_cyclic_lines.argtypes = [_dp, _dp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double]
         _LIB = L
     return _LIB
@@ -214,6 +219,14 @@ class Oracle:
         sq = np.ascontiguousarray(squalls, dtype=np.float64).reshape(-1, 6)
         _check(lib().orc_build_squalls(self.h, int(sstruct), sq.shape[0], _ptr(sq)))
 
+    def add_squalls(self, squalls, sstruct=1):
+        sq = np.ascontiguousarray(squalls, dtype=np.float64).reshape(-1, 6)
+        _check(lib().orc_add_squalls(self.h, int(sstruct), sq.shape[0], _ptr(sq)))
+
+    def build_lanes(self, cells, meansize, meanvel, meands):
+        cl = np.ascontiguousarray(cells, dtype=np.float64).reshape(-1, 3)
+        _check(lib().orc_build_lanes(self.h, cl.shape[0], _ptr(cl), float(meansize), float(meanvel), float(meands)))
+
 
 def compact_lines(x, order=1, lphys=True, rphys=True, bdry=1, bc_lo=None, bc_hi=None,
                   halo_lo=None, halo_hi=None, dnum=1.0, scale=1.0):
@@ -253,3 +266,20 @@ def dbydp_cyclic(p, field, order=1):
     dphi = (p.phi2 - p.phi1) / p.nphi
     d = cyclic_lines(f, order, 1.0 / dphi)
     return np.ascontiguousarray(np.moveaxis(d, 2, 1))
+
+
+def voronoi(x, y):
+    """Voronoi cells of sites (x, y) as orc_voronoi / Compute_Voronoi give
+    them: (degree, start, face, vxy) with cell g's vertices
+    vxy[face[start[g]:start[g] + degree[g]]]."""
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    n = x.size
+    deg, st = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    face = np.zeros(6 * n + 32, np.int32)
+    vxy = np.zeros((2 * n + 8, 2))
+    nv = ctypes.c_int()
+    ip = ctypes.POINTER(ctypes.c_int)
+    _check(lib().orc_voronoi(n, _ptr(x), _ptr(y), deg.ctypes.data_as(ip), st.ctypes.data_as(ip),
+                             face.ctypes.data_as(ip), ctypes.byref(nv), _ptr(vxy)))
+    return deg, st, face[:int(deg.sum())], vxy[:nv.value]

@@ -6,7 +6,10 @@ Place_Cell; Temporal_Structure's two forms; Update_Rain_Squalls ages,
 advects (with the periodic phi wrap), kills squalls that leave the theta
 range and replaces dead ones with fresh draws starting now.  GPU: a run
 with the rain model updating every ufreq/10 steps against the oracle driven
-by the same squall lists (five updates), at the FP64 step bar."""
+by the same squall lists (five updates), at the FP64 step bar.  The
+downflow lanes (Build_Downflow_Lanes): the device field against the
+oracle's, alone and with squalls added, and a run with lanes and squalls
+against the oracle."""
 import math
 
 import numpy as np
@@ -125,3 +128,79 @@ def test_advance_drives_the_device(gpu_available):
     assert np.abs(dvel).max() > 0.0 and np.abs(dent).max() > 0.0
     with pytest.raises(ValueError):
         rain.advance(sim, r, dt, 1, 5)
+
+
+def lane_cells(p, n, seed, lo=0.2, hi=1.0):
+    rng = np.random.default_rng(seed)
+    return np.stack([rng.uniform(p.phi1, p.phi2, n), rng.uniform(p.th1, p.th2, n), rng.uniform(lo, hi, n)], axis=1)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("scale", [1.0, 1e-4])
+def test_lanes_match_oracle(gpu_available, scale):
+    """css_build_lanes against orc_build_lanes (1e-12 of the largest value):
+    with full scalings the lane field's maximum exceeds 1 and is normalised
+    away, with small ones it is kept (max(x, 1)).  Squalls added on top
+    match the oracle's too."""
+    from css_b200.context import Simulation
+    p, prof, v0, dt, r = setup()
+    sim, orc = Simulation(p, prof), O.Oracle(p, prof)
+    cells = lane_cells(p, 9, 7)
+    cells[:, 2] *= scale
+    for o in (sim, orc):
+        o.build_lanes(cells, 0.05, -0.02, -1e-3)
+    got, want = sim.rain_fields(), orc.rain_fields()
+    for a, b in zip(got, want):
+        assert np.abs(b).max() > 0.0
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+    if scale == 1.0:
+        assert np.abs(want[0]).max() == pytest.approx(0.02, rel=1e-12)  # normalised: meanvel at the peak
+    r.scaling[:] = 0.5
+    built = r.squalls()
+    sim.add_squalls(built)
+    orc.add_squalls(built)
+    for a, b in zip(sim.rain_fields(), orc.rain_fields()):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+def top_mean(p, v):
+    """theta profiles of u_theta, u_phi over phi and the top block's radii."""
+    size_top = p.nr // p.nnr
+    return (v[1, p.nr - size_top:].sum(axis=(0, 1)) / (size_top * p.nphi),
+            v[2, p.nr - size_top:].sum(axis=(0, 1)) / (size_top * p.nphi))
+
+
+@pytest.mark.gpu
+def test_rain_run_with_lanes_parity(gpu_available):
+    """Ten steps with the rain model updating every ufreq/10 steps, lanes
+    first and the squalls added, against the oracle driven by the same cell
+    and squall lists, at the FP64 step bar."""
+    from css_b200.context import Simulation
+    p, prof, v0, dt, r = setup(seed=6)
+    cc = rain.ConvectionCells(p, 8, meansize=0.05, stopin=-1e-3, utopin=-0.02, seed=9)
+    rng = np.random.default_rng(5)
+    v = v0.copy()
+    v[1:4] = 1e-2 * rng.standard_normal(v[1:4].shape)
+    sim, orc = Simulation(p, prof), O.Oracle(p, prof)
+    dt = min(dt, list(orc.step_size(v, 0.4).values())[0])
+    sim.upload(v)
+    for o in (sim, orc):
+        o.set_clock(0, 0.0, dt)
+    every = p.ufreq // 10
+    o_state = v
+    for step in range(1, 11):
+        sim.step_rk4(dt, 1)
+        o_state = orc.step(o_state, dt, 1)
+        if step % every == 0:
+            _, t_end = orc.clock()
+            cells = cc.update(t_end - dt, dt, *top_mean(p, o_state))
+            cells[:, 2] = 0.3 + 0.7 * cells[:, 2]  # lanes that show in a short run
+            built = r.update(t_end - dt, dt, o_state[1, -1], o_state[2, -1])
+            for o in (sim, orc):
+                o.build_lanes(cells, cc.meansize, cc.meanvel, cc.meands)
+                o.add_squalls(built)
+            for a, b in zip(sim.rain_fields(), orc.rain_fields()):
+                assert np.abs(a - b).max() <= 1e-12 * max(np.abs(b).max(), 1e-300)
+    g = sim.download()
+    errs = [float(np.abs(g[i] - o_state[i]).max() / np.abs(o_state[i]).max()) for i in range(5)]
+    assert max(errs) < 1e-10, errs
