@@ -103,6 +103,7 @@ struct css_ctx {
   int phi_pers = 0;                 // 1: persistent double-buffered phi kernel (autotuned)
   int fused_ok = 0;                 // the run qualifies for the two-pass RK4 stage (css_fused.cuh)
   int fused = 0;                    // 1: FP64 RK4 stages run k_thph + k_rstage
+  int curl_tp = 1;                  // 1: B = curl A's theta and phi parts in one pass (k_curl_tp)
   int nsm = 148;                    // SMs of the device
   cudaStream_t own_stream;
   // per-kernel event timing (css_profile)
@@ -326,6 +327,8 @@ static int setup_kernels() {
   CUDA_TRY(cudaFuncSetAttribute(k_sld<4, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<4>)));
   CUDA_TRY(cudaFuncSetAttribute(k_sld<5, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<5>)));
   CUDA_TRY(cudaFuncSetAttribute(k_sld<3, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SldSmem<3>)));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_tp<32, double>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
+  CUDA_TRY(cudaFuncSetAttribute(k_curl_tp<32, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, 96 * 1024));
   if (int rc = setup_mt<16, 16>()) return rc;
   if (int rc = setup_mt<32, 16>()) return rc;
   if (int rc = setup_mt<16, 8>()) return rc;
@@ -900,18 +903,31 @@ template <typename TS>
 static int launch_curl(css_ctx *c, const TS *a, double *out, int apply_bc) {
   const CssGeo &g = c->g;
   int mt = g.d[1].maxm, mp = g.d[2].maxm, mr = g.d[0].maxm;
-  int TL = c->tl_theta;
-  dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
-  prof_begin(c, KI_CURL_THETA);
-  LAUNCH_MT(1, TL, k_curl_theta, (TS), gt, smem_theta(2, 2, mt, TL), g, a, out, TL);
-  prof_end(c);
-  if (int rc = check_launch(c)) return rc;
-  TL = c->tl_phi;
-  dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
-  prof_begin(c, KI_CURL_PHI);
-  LAUNCH_MT(2, TL, k_curl_phi, (TS), gp, smem_line(2, 2, 0, mp, TL), g, a, out, TL);
-  prof_end(c);
-  if (int rc = check_launch(c)) return rc;
+  int TL;
+  if (c->mt[1] && c->mt[1] == c->mt[2] && c->curl_tp) {  // theta and phi in one pass
+    const int M = c->mt[1];
+    const size_t smem = 8 * (2 * (size_t)M * (M + 9) + 2 * (size_t)(M + 8) * (M + 1) + 2 * (size_t)M * (M + 1) +
+                             2 * (size_t)M * (M + 1));
+    dim3 gtp(g.d[1].nb * g.d[2].nb, g.nr);
+    prof_begin(c, KI_CURL_THETA);
+    if (M == 32) k_curl_tp<32, TS><<<gtp, 128, smem, c->stream>>>(g, a, out);
+    else k_curl_tp<16, TS><<<gtp, 128, smem, c->stream>>>(g, a, out);
+    prof_end(c);
+    if (int rc = check_launch(c)) return rc;
+  } else {
+    TL = c->tl_theta;
+    dim3 gt(g.d[1].nb * ((g.nphi + TL - 1) / TL), g.nr);
+    prof_begin(c, KI_CURL_THETA);
+    LAUNCH_MT(1, TL, k_curl_theta, (TS), gt, smem_theta(2, 2, mt, TL), g, a, out, TL);
+    prof_end(c);
+    if (int rc = check_launch(c)) return rc;
+    TL = c->tl_phi;
+    dim3 gp(g.d[2].nb * ((g.nth + TL - 1) / TL), g.nr);
+    prof_begin(c, KI_CURL_PHI);
+    LAUNCH_MT(2, TL, k_curl_phi, (TS), gp, smem_line(2, 2, 0, mp, TL), g, a, out, TL);
+    prof_end(c);
+    if (int rc = check_launch(c)) return rc;
+  }
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);
   prof_begin(c, KI_CURL_R);
@@ -1846,6 +1862,12 @@ extern "C" int css_set_tiles(css_ctx *c, int tl_r, int tl_theta, int tl_phi, int
   }
   if (phi_persistent && !c->mt[2]) { set_err("css_set_tiles: the persistent phi kernel needs 16- or 32-point blocks"); return CSS_ERR_ARG; }
   c->tl_r = tl_r; c->tl_theta = tl_theta; c->tl_phi = tl_phi; c->phi_pers = phi_persistent ? 1 : 0;
+  return CSS_OK;
+}
+
+extern "C" int css_set_curl_pass(css_ctx *c, int one_pass) {
+  if (!c) { set_err("css_set_curl_pass: NULL context"); return CSS_ERR_ARG; }
+  c->curl_tp = one_pass ? 1 : 0;
   return CSS_OK;
 }
 

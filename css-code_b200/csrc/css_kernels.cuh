@@ -1315,6 +1315,68 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const TS *__restrict
   }
 }
 
+// The theta and phi parts of B = curl A in one pass over a theta block x phi
+// block tile of one radius (both directions MT points per block): the
+// theta lines of sin(theta) A_phi and A_r, the phi lines of A_r and A_theta
+// (VectorCurlA, derivatives.f90:1769-1828, as k_curl_theta and k_curl_phi
+// split it), with B_r complete and the theta / phi parts of B_theta / B_phi
+// written once -- the same expressions in the same order as the two kernels
+// (bit for bit), without the phi kernel's read-modify-write of B_r.
+// grid: x = theta block + phi block * (theta blocks), y = r.
+template <int MT, typename TS>
+__global__ void __launch_bounds__(128) k_curl_tp(CssGeo g, const TS *__restrict__ a, double *__restrict__ out) {
+  extern __shared__ double sm[];
+  constexpr int W = MT + 8, SRT = MT + 9, SOT = MT + 1, SRP = MT + 1;
+  constexpr size_t FT = (size_t)MT * SRT, HSP = (size_t)W * SRP, OT = (size_t)MT * SOT, OP = (size_t)MT * SRP;
+  const int bt = blockIdx.x % g.d[1].nb, bp = blockIdx.x / g.d[1].nb, ir = blockIdx.y;
+  const CssDir &DT = g.d[1], &DP = g.d[2];
+  const int t0 = DT.start[bt], p0 = DP.start[bp];
+  const size_t n = (size_t)g.ncell;
+  double *Ht = sm;               // theta lines: 0 sin*A_phi, 1 A_r   [phi line][theta + halo]
+  double *Hp = Ht + 2 * FT;      // phi lines: 0 A_r, 1 A_theta      [phi + halo][theta line]
+  double *Ot = Hp + 2 * HSP;     // d/dtheta of the theta lines      [phi line][theta]
+  double *Op = Ot + 2 * OT;      // d/dphi of the phi lines          [phi][theta line]
+  {
+    const TS *ft[2] = {a + n, a + 2 * n};
+    tiles_ct<2, MT, MT, 1>(g, ft, Ht, FT, SRT, t0, p0, ir);
+    const TS *fp[2] = {a + 2 * n, a};
+    tiles_ct<2, MT, MT, 2>(g, fp, Hp, HSP, SRP, p0, t0, ir);
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < MT * W; idx += blockDim.x) {
+    const int l = idx / W, jj = idx - l * W, gt = t0 + jj - 4;
+    if (gt < 0 || gt >= g.nth) continue;
+    Ht[(size_t)l * SRT + jj] *= g.sines[gt];
+  }
+  __syncthreads();
+  const int dtype = dtype_of(DT, bt);
+  for (int task = threadIdx.x; task < 4 * MT; task += blockDim.x) {
+    const int k = task / MT, l = task - k * MT;
+    if (k < 2) {
+      const int bdry = g.ibct[k == 0 ? 11 : 12];
+      solve<1, MT>(Ht + ((size_t)k * MT + l) * SRT + 4, 1, MT, dtype, bdry, 0.0, 0.0, tabp(g, 1, bt, 1, bdry),
+                   g.tstride, DT.dnum[bt], DT.dnum[bt], 0, Ot + ((size_t)k * MT + l) * SOT, 1);
+    } else {
+      const int q = k - 2;
+      solve<1, MT>(Hp + q * HSP + 4 * SRP + l, SRP, MT, 3, 0, 0.0, 0.0, tabp(g, 2, bp, 1, 0), g.tstride,
+                   DP.dnum[bp], DP.dnum[bp], 1, Op + q * OP + l, SRP);
+    }
+  }
+  __syncthreads();
+  const double invr = g.r_inv[ir];
+  for (int pt = threadIdx.x; pt < MT * MT; pt += blockDim.x) {
+    const int jp = pt / MT, jt = pt - jp * MT;  // theta fastest: coalesced stores
+    const int it = t0 + jt;
+    const size_t id = css_idx(g, it, p0 + jp, ir);
+    const double csc = g.csc[it];
+    out[id] = invr * Op[(size_t)jp * SRP + jt] * csc;
+    out[n + id] = -Ot[(size_t)(MT + jp) * SOT + jt] * invr;
+    // the theta part rounded on its own, as the two-pass form stores it before the phi pass subtracts
+    const double prev = __dmul_rn(__dmul_rn(Ot[(size_t)jp * SOT + jt], csc), invr);
+    out[2 * n + id] = prev - invr * Op[OP + (size_t)jp * SRP + jt] * csc;
+  }
+}
+
 template <int MT, int TLC, typename TS>
 __global__ void __launch_bounds__(128) k_curl_r(CssGeo g, const TS *__restrict__ a, double *__restrict__ out,
                                                 int TL, int apply_bc) {

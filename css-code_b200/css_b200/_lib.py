@@ -69,6 +69,7 @@ def lib():
         L.css_dbydp_cyclic_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int,
                                            ctypes.c_void_p]
         L.css_get_fused.argtypes = [ctypes.c_void_p]
+        L.css_set_curl_pass.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.css_ensemble_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p),
                                           ctypes.POINTER(ctypes.c_void_p)]
         L.css_ensemble_step.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
@@ -133,7 +134,7 @@ EXPORTS = [
     "css_step_rk4_host", "css_rhs", "css_diffusion", "css_deriv", "css_deriv_dev", "css_dbyd1_dt0",
     "css_compact_lines", "css_checkpoint_write", "css_checkpoint_read", "css_sync", "css_state_device_ptr", "css_kernel_launches", "css_set_stream",
     "css_profile", "css_kernel_stats", "css_compact_lines_noalloc", "css_scalars", "css_step_size",
-    "css_shell_averages", "css_spectrum", "css_autotune", "css_set_tiles", "css_set_fused", "css_get_fused", "css_dbydp_cyclic", "css_dbydp_cyclic_dev", "css_deriv_adjoint_dev", "css_ensemble_create", "css_ensemble_step",
+    "css_shell_averages", "css_spectrum", "css_autotune", "css_set_tiles", "css_set_fused", "css_get_fused", "css_set_curl_pass", "css_dbydp_cyclic", "css_dbydp_cyclic_dev", "css_deriv_adjoint_dev", "css_ensemble_create", "css_ensemble_step",
     "css_ensemble_launches", "css_ensemble_last_ms", "css_ensemble_destroy", "css_set_sld_speed2", "css_box_filter",
     "css_closure_scales", "css_closure_features", "css_closure_targets", "css_closure_speed2",
     "css_closure_speed2_shaped", "css_restrict_state", "css_prolong_add", "css_mlp_create",

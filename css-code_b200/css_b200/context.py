@@ -135,6 +135,11 @@ class Simulation:
         run that does not qualify."""
         check(_lib.lib().css_set_fused(self.h, 1 if on else 0))
 
+    def set_curl_pass(self, one_pass):
+        """B = curl A's theta and phi parts in one pass (default) or two
+        (css_set_curl_pass); bit-identical results."""
+        check(_lib.lib().css_set_curl_pass(self.h, 1 if one_pass else 0))
+
     @property
     def fused(self):
         return bool(_lib.lib().css_get_fused(self.h))
