@@ -106,6 +106,7 @@ def lib():
             getattr(L, nm).argtypes = [vp, dp, dp, dp, dp, ctypes.c_int]
         for nm in ("css_dbydp", "css_d2bydp2"):
             getattr(L, nm).argtypes = [vp, dp, dp, ctypes.c_int]
+        L.css_deriv_pencils.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, ctypes.c_int]
         L.css_set_clock.argtypes = [vp, ll, ctypes.c_double, ctypes.c_double]
         L.css_get_clock.argtypes = [vp, ctypes.POINTER(ll), dp]
         L.css_inout_init.argtypes = [vp]
@@ -143,5 +144,5 @@ EXPORTS = [
     "css_inout_state", "css_set_rain_fields", "css_get_rain_fields", "css_build_squalls", "css_add_squalls",
     "css_build_lanes", "css_voronoi",
     "css_set_ash_slices", "css_download_plane", "css_dbydr", "css_d2bydr2", "css_dbydt", "css_d2bydt2",
-    "css_dbydp", "css_d2bydp2", "css_bound",
+    "css_dbydp", "css_d2bydp2", "css_bound", "css_deriv_pencils",
 ]

@@ -202,6 +202,21 @@ int css_d2bydt2(css_ctx *ctx, const double *x, double *dx, const double *b1, con
 int css_dbydp(css_ctx *ctx, const double *x, double *dx, int var);
 int css_d2bydp2(css_ctx *ctx, const double *x, double *dx, int var);
 
+/* The reference's pencil calls, batched: npencils pencils in one call.
+ * dir 0 (Dbydr / D2bydr2, derivatives.f90:547, :799): a pencil is the
+ * (theta, r) plane of one phi, x(nth, nr) in Fortran order ([ir][it]);
+ * bc_lo / bc_hi hold nth values per pencil (the r faces' datum).  dir 1
+ * (Dbydt / D2bydt2, :1010, :1265) and dir 2 (Dbydp / D2bydp2, :1480,
+ * :1594): a pencil is the (theta, phi) plane of one radius, x(nth, nphi)
+ * ([ip][it]); for dir 1 bc_lo / bc_hi hold nphi values per pencil (the
+ * theta faces' datum), dir 2 has none.  var as in the named routines.
+ * The pencils of a call are consecutive in x and dx (pencil p at
+ * p * nth * nr, or p * nth * nphi); each is differentiated on its own,
+ * with the run's virtual blocks, so a pencil gives what the same plane of
+ * a whole field gives.  Host pointers.                                    */
+int css_deriv_pencils(css_ctx *ctx, int dir, int order, int npencils, const double *x, double *dx,
+                      const double *bc_lo, const double *bc_hi, int var);
+
 /* Same on device pointers, enqueued on `stream` (a cudaStream_t, NULL =
  * the context stream); returns after enqueueing.                           */
 int css_deriv_dev(css_ctx *ctx, int dir, int order, const double *x, double *dx,
