@@ -1657,13 +1657,14 @@ extern "C" int css_d2bydp2(css_ctx *c, const double *x, double *dx, int var) {
 
 // The reference's per-pencil calls, batched: dir 0 pencils are (theta, r)
 // planes of one phi (Dbydr's x(mynth, mynr)), dir 1 / 2 pencils (theta, phi)
-// planes of one radius (Dbydt's and Dbydp's x(mynth, mynphi)).  The pencils
-// go into the field buffer one per phi plane (dir 0) or per radius (1, 2),
-// at most nphi / nr of them per pass; the derivative of a plane of either
-// kind depends on that plane alone, so the other planes of the buffer play
-// no part.
-extern "C" int css_deriv_pencils(css_ctx *c, int dir, int order, int npencils, const double *x, double *dx,
-                                 const double *bc_lo, const double *bc_hi, int var) {
+// planes of one radius (Dbydt's and Dbydp's x(mynth, mynphi)).  Each pencil
+// goes into the field buffer at its own phi plane (dir 0) or radius (1, 2)
+// -- D2bydt2 scales the Neumann datum by the radial block's dri, so a
+// theta pencil's result depends on its radius -- and a pass takes pencils
+// until one repeats an index.  The derivative of a plane depends on that
+// plane alone, so the other planes of the buffer play no part.
+extern "C" int css_deriv_pencils(css_ctx *c, int dir, int order, int npencils, const int *index, const double *x,
+                                 double *dx, const double *bc_lo, const double *bc_hi, int var) {
   if (!c || !x || !dx || npencils < 0 || dir < 0 || dir > 2 || (order != 1 && order != 2)) {
     set_err("css_deriv_pencils: bad argument");
     return CSS_ERR_ARG;
@@ -1678,38 +1679,56 @@ extern "C" int css_deriv_pencils(css_ctx *c, int dir, int order, int npencils, c
   const size_t pen = dir == 0 ? nth * nr : plane_tp;        // doubles per pencil
   const size_t bcn = dir == 0 ? nth : (dir == 1 ? nphi : 0);  // face data per pencil
   const int cap = dir == 0 ? (int)nphi : (int)nr;
+  for (int p = 0; p < npencils; p++) {
+    const int k = index ? index[p] : p % cap;
+    if (k < 0 || k >= cap) {
+      set_err("css_deriv_pencils: pencil %d has index %d outside 0..%d", p, k, cap - 1);
+      return CSS_ERR_ARG;
+    }
+  }
   const size_t face = dir == 0 ? plane_tp : nphi * nr;
   double *bl = c->vB, *bh = c->vB + face;  // scratch
-  for (int p0 = 0; p0 < npencils; p0 += cap) {
-    const int np = std::min(cap, npencils - p0);
-    const double *xs = x + (size_t)p0 * pen;
-    double *ds = dx + (size_t)p0 * pen;
-    CUDA_TRY(cudaMemsetAsync(c->vA, 0, c->ncell * 8, c->stream));
-    if (dir == 0) {  // pencil p -> phi plane p: nr rows of nth
-      for (int p = 0; p < np; p++)
-        CUDA_TRY(cudaMemcpy2DAsync(c->vA + (size_t)p * nth, plane_tp * 8, xs + (size_t)p * pen, nth * 8, nth * 8, nr,
-                                   cudaMemcpyHostToDevice, c->stream));
-    } else {  // pencil p -> radius p: the field layout itself
-      CUDA_TRY(cudaMemcpyAsync(c->vA, xs, (size_t)np * pen * 8, cudaMemcpyHostToDevice, c->stream));
+  std::vector<char> used(cap);
+  for (int p0 = 0; p0 < npencils;) {
+    std::fill(used.begin(), used.end(), 0);
+    int p1 = p0;
+    while (p1 < npencils) {
+      const int k = index ? index[p1] : p1 % cap;
+      if (used[k]) break;
+      used[k] = 1;
+      p1++;
     }
-    if (bcn) {
-      CUDA_TRY(cudaMemsetAsync(bl, 0, 2 * face * 8, c->stream));
-      if (bc_lo)
-        CUDA_TRY(cudaMemcpyAsync(bl, bc_lo + (size_t)p0 * bcn, (size_t)np * bcn * 8, cudaMemcpyHostToDevice, c->stream));
-      if (bc_hi)
-        CUDA_TRY(cudaMemcpyAsync(bh, bc_hi + (size_t)p0 * bcn, (size_t)np * bcn * 8, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemsetAsync(c->vA, 0, c->ncell * 8, c->stream));
+    if (bcn) CUDA_TRY(cudaMemsetAsync(bl, 0, 2 * face * 8, c->stream));
+    for (int p = p0; p < p1; p++) {
+      const int k = index ? index[p] : p % cap;
+      const double *xs = x + (size_t)p * pen;
+      if (dir == 0)  // phi plane k: nr rows of nth
+        CUDA_TRY(cudaMemcpy2DAsync(c->vA + (size_t)k * nth, plane_tp * 8, xs, nth * 8, nth * 8, nr,
+                                   cudaMemcpyHostToDevice, c->stream));
+      else  // radius k: the field layout itself
+        CUDA_TRY(cudaMemcpyAsync(c->vA + (size_t)k * plane_tp, xs, pen * 8, cudaMemcpyHostToDevice, c->stream));
+      if (bcn && bc_lo)
+        CUDA_TRY(cudaMemcpyAsync(bl + (size_t)k * bcn, bc_lo + (size_t)p * bcn, bcn * 8, cudaMemcpyHostToDevice,
+                                 c->stream));
+      if (bcn && bc_hi)
+        CUDA_TRY(cudaMemcpyAsync(bh + (size_t)k * bcn, bc_hi + (size_t)p * bcn, bcn * 8, cudaMemcpyHostToDevice,
+                                 c->stream));
     }
     if (int rc = css_deriv_dev(c, dir, order, c->vA, c->dv, (bcn && bc_lo) ? bl : nullptr,
                                (bcn && bc_hi) ? bh : nullptr, bdry, nullptr))
       return rc;
-    if (dir == 0) {
-      for (int p = 0; p < np; p++)
-        CUDA_TRY(cudaMemcpy2DAsync(ds + (size_t)p * pen, nth * 8, c->dv + (size_t)p * nth, plane_tp * 8, nth * 8, nr,
+    for (int p = p0; p < p1; p++) {
+      const int k = index ? index[p] : p % cap;
+      double *ds = dx + (size_t)p * pen;
+      if (dir == 0)
+        CUDA_TRY(cudaMemcpy2DAsync(ds, nth * 8, c->dv + (size_t)k * nth, plane_tp * 8, nth * 8, nr,
                                    cudaMemcpyDeviceToHost, c->stream));
-    } else {
-      CUDA_TRY(cudaMemcpyAsync(ds, c->dv, (size_t)np * pen * 8, cudaMemcpyDeviceToHost, c->stream));
+      else
+        CUDA_TRY(cudaMemcpyAsync(ds, c->dv + (size_t)k * plane_tp, pen * 8, cudaMemcpyDeviceToHost, c->stream));
     }
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    p0 = p1;
   }
   return CSS_OK;
 }

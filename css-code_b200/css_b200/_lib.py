@@ -106,7 +106,8 @@ def lib():
             getattr(L, nm).argtypes = [vp, dp, dp, dp, dp, ctypes.c_int]
         for nm in ("css_dbydp", "css_d2bydp2"):
             getattr(L, nm).argtypes = [vp, dp, dp, ctypes.c_int]
-        L.css_deriv_pencils.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, dp, dp, dp, dp, ctypes.c_int]
+        L.css_deriv_pencils.argtypes = [vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                        dp, dp, dp, dp, ctypes.c_int]
         L.css_set_clock.argtypes = [vp, ll, ctypes.c_double, ctypes.c_double]
         L.css_get_clock.argtypes = [vp, ctypes.POINTER(ll), dp]
         L.css_inout_init.argtypes = [vp]

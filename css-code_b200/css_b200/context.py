@@ -268,16 +268,19 @@ class Simulation:
         check(_lib.lib().css_deriv(self.h, int(direction), int(order), _p(x), _p(out), _p(lo), _p(hi), int(bdry)))
         return out
 
-    def deriv_pencils(self, direction, order, x, bc_lo=None, bc_hi=None, var=0):
+    def deriv_pencils(self, direction, order, x, index=None, bc_lo=None, bc_hi=None, var=0):
         """The reference's per-pencil derivative calls, batched
-        (css_deriv_pencils): direction 0 pencils are (nr, nth) arrays (a
-        phi plane), 1 and 2 (nphi, nth) arrays (a radius); x has shape
-        (npencils, ...).  var as the named routines take it."""
+        (css_deriv_pencils): direction 0 pencils are (nr, nth) arrays (the
+        plane of phi index[p]), 1 and 2 (nphi, nth) arrays (the plane of
+        radius index[p]); x has shape (npencils, ...).  var as the named
+        routines take it."""
         x = np.ascontiguousarray(x, dtype=np.float64)
         out = np.empty_like(x)
         vec = lambda a: None if a is None else np.ascontiguousarray(a, dtype=np.float64)
         lo, hi = vec(bc_lo), vec(bc_hi)
-        check(_lib.lib().css_deriv_pencils(self.h, int(direction), int(order), int(x.shape[0]), _p(x), _p(out),
+        idx = None if index is None else np.ascontiguousarray(index, dtype=np.int32)
+        ip = None if idx is None else idx.ctypes.data_as(ctypes.POINTER(ctypes.c_int))
+        check(_lib.lib().css_deriv_pencils(self.h, int(direction), int(order), int(x.shape[0]), ip, _p(x), _p(out),
                                            _p(lo), _p(hi), int(var)))
         return out
 

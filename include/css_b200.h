@@ -209,13 +209,16 @@ int css_d2bydp2(css_ctx *ctx, const double *x, double *dx, int var);
  * (Dbydt / D2bydt2, :1010, :1265) and dir 2 (Dbydp / D2bydp2, :1480,
  * :1594): a pencil is the (theta, phi) plane of one radius, x(nth, nphi)
  * ([ip][it]); for dir 1 bc_lo / bc_hi hold nphi values per pencil (the
- * theta faces' datum), dir 2 has none.  var as in the named routines.
- * The pencils of a call are consecutive in x and dx (pencil p at
- * p * nth * nr, or p * nth * nphi); each is differentiated on its own,
- * with the run's virtual blocks, so a pencil gives what the same plane of
- * a whole field gives.  Host pointers.                                    */
-int css_deriv_pencils(css_ctx *ctx, int dir, int order, int npencils, const double *x, double *dx,
-                      const double *bc_lo, const double *bc_hi, int var);
+ * theta faces' datum), dir 2 has none.  index[p] is pencil p's phi index
+ * (dir 0) or radius (dir 1, 2): D2bydt2 divides its Neumann datum by the
+ * radial block's dri (derivatives.f90:1322, :1338), so a theta pencil's
+ * result depends on its radius; NULL means index p (mod nphi or nr).
+ * var as in the named routines.  The pencils of a call are consecutive in
+ * x and dx (pencil p at p * nth * nr, or p * nth * nphi); each comes back
+ * as the same plane of the whole-field derivative.  Host pointers.        */
+int css_deriv_pencils(css_ctx *ctx, int dir, int order, int npencils, const int *index,
+                      const double *x, double *dx, const double *bc_lo, const double *bc_hi,
+                      int var);
 
 /* Same on device pointers, enqueued on `stream` (a cudaStream_t, NULL =
  * the context stream); returns after enqueueing.                           */

@@ -2,7 +2,8 @@
 Dbydr's pencils are (theta, r) planes of one phi, Dbydt's and Dbydp's
 (theta, phi) planes of one radius.  Each pencil's derivative is the same
 plane of the whole-field derivative bit for bit (the same kernels on the
-same values), for both orders, boundary variants from var (<= 0 a bdry,
+same values, each pencil at its own phi index or radius: D2bydt2 scales
+its Neumann datum by the radial block's spacing), for both orders, boundary variants from var (<= 0 a bdry,
 >= 1 the run's tables), physical-face data per pencil, pencils in any
 order and repeated, and more pencils than one pass holds."""
 import numpy as np
@@ -31,7 +32,7 @@ def test_r_pencils_match_whole_field(gpu_available, run, order, var):
     lo, hi = rng.standard_normal((p.nphi, p.nth)), rng.standard_normal((p.nphi, p.nth))
     ips = [5, 0, 63, 17, 17, 40] + list(range(p.nphi))  # repeated, unordered, more than one pass
     x = np.stack([F[:, ip, :] for ip in ips])
-    got = sim.deriv_pencils(0, order, x, lo[ips], hi[ips], var)
+    got = sim.deriv_pencils(0, order, x, ips, lo[ips], hi[ips], var)
     if var <= 0:
         whole = sim.deriv(0, order, F, lo, hi, -var)
     else:  # the named whole-field routine takes var the same way
@@ -56,10 +57,10 @@ def test_theta_phi_pencils_match_whole_field(gpu_available, run, direction, orde
     irs = [47, 3, 3, 20] + list(range(p.nr))
     x = np.stack([F[ir] for ir in irs])
     if direction == 1:
-        got = sim.deriv_pencils(1, order, x, lo[irs], hi[irs], -2)
+        got = sim.deriv_pencils(1, order, x, irs, lo[irs], hi[irs], -2)
         whole = sim.deriv(1, order, F, lo, hi, 2)
     else:
-        got = sim.deriv_pencils(2, order, x, var=0)
+        got = sim.deriv_pencils(2, order, x, irs, var=0)
         whole = sim.deriv(2, order, F)
     for k, ir in enumerate(irs):
         assert np.array_equal(got[k], whole[ir]), (k, ir)
@@ -73,3 +74,5 @@ def test_pencils_refuse_bad_arguments(gpu_available, run):
         sim.deriv_pencils(0, 3, x)
     with pytest.raises(CssError):
         sim.deriv_pencils(0, 1, x, var=13)
+    with pytest.raises(CssError):
+        sim.deriv_pencils(0, 1, x, index=[0, p.nphi])
