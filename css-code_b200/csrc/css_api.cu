@@ -910,8 +910,8 @@ static int launch_curl(css_ctx *c, const TS *a, double *out, int apply_bc) {
                              2 * (size_t)M * (M + 1));
     dim3 gtp(g.d[1].nb * g.d[2].nb, g.nr);
     prof_begin(c, KI_CURL_THETA);
-    if (M == 32) k_curl_tp<32, TS><<<gtp, 128, smem, c->stream>>>(g, a, out);
-    else k_curl_tp<16, TS><<<gtp, 128, smem, c->stream>>>(g, a, out);
+    if (M == 32) k_curl_tp<32, TS><<<gtp, 256, smem, c->stream>>>(g, a, out);
+    else k_curl_tp<16, TS><<<gtp, 256, smem, c->stream>>>(g, a, out);
     prof_end(c);
     if (int rc = check_launch(c)) return rc;
   } else {

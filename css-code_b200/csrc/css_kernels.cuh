@@ -204,16 +204,16 @@ constexpr int NT = 128;
 // periodic in phi, lines = theta indices lb..; DIR 0: r tile S[jj*SR + l]
 // at phi index `fixed`, lines = theta indices lb...  a0 = first point of
 // the block along the sweep; jj = 0..MT+7 covers the 4-point halos.
-template <int NF, int MT, int TLC, int DIR, typename TS>
+template <int NF, int MT, int TLC, int DIR, typename TS, int NTT = NT>
 __device__ __forceinline__ void tiles_ct(const CssGeo &g, const TS *const *f, double *S, size_t FS, int SR,
                                          int a0, int lb, int fixed, const double *const *mp = nullptr) {
-  constexpr int W = MT + 8, N = TLC * W, IT = (N + NT - 1) / NT;
+  constexpr int W = MT + 8, N = TLC * W, IT = (N + NTT - 1) / NTT;
   double val[NF][IT];
   int so[IT];
   size_t go[IT], bb[IT];
 #pragma unroll
   for (int k = 0; k < IT; k++) {
-    const int idx = threadIdx.x + k * NT;
+    const int idx = threadIdx.x + k * NTT;
     int l, jj;
     if (DIR == 1) { l = idx / W; jj = idx - l * W; }
     else { jj = idx / TLC; l = idx - jj * TLC; }
@@ -1322,9 +1322,13 @@ __global__ void __launch_bounds__(128) k_curl_phi(CssGeo g, const TS *__restrict
 // split it), with B_r complete and the theta / phi parts of B_theta / B_phi
 // written once -- the same expressions in the same order as the two kernels
 // (bit for bit), without the phi kernel's read-modify-write of B_r.
-// grid: x = theta block + phi block * (theta blocks), y = r.
+// grid: x = theta block + phi block * (theta blocks), y = r; 256 threads
+// (the loads of a tile spread over 8 warps; 2 CTAs per SM, no register
+// cap below what the unrolled 32-point solves hold: 2.53 ms on MHD
+// 256x512x1024 against 2.64 with 3 CTAs of 80 registers, which spill, and
+// 3.09 with 128 threads).
 template <int MT, typename TS>
-__global__ void __launch_bounds__(128) k_curl_tp(CssGeo g, const TS *__restrict__ a, double *__restrict__ out) {
+__global__ void __launch_bounds__(256, 2) k_curl_tp(CssGeo g, const TS *__restrict__ a, double *__restrict__ out) {
   extern __shared__ double sm[];
   constexpr int W = MT + 8, SRT = MT + 9, SOT = MT + 1, SRP = MT + 1;
   constexpr size_t FT = (size_t)MT * SRT, HSP = (size_t)W * SRP, OT = (size_t)MT * SOT, OP = (size_t)MT * SRP;
@@ -1338,9 +1342,9 @@ __global__ void __launch_bounds__(128) k_curl_tp(CssGeo g, const TS *__restrict_
   double *Op = Ot + 2 * OT;      // d/dphi of the phi lines          [phi][theta line]
   {
     const TS *ft[2] = {a + n, a + 2 * n};
-    tiles_ct<2, MT, MT, 1>(g, ft, Ht, FT, SRT, t0, p0, ir);
+    tiles_ct<2, MT, MT, 1, TS, 256>(g, ft, Ht, FT, SRT, t0, p0, ir);
     const TS *fp[2] = {a + 2 * n, a};
-    tiles_ct<2, MT, MT, 2>(g, fp, Hp, HSP, SRP, p0, t0, ir);
+    tiles_ct<2, MT, MT, 2, TS, 256>(g, fp, Hp, HSP, SRP, p0, t0, ir);
   }
   __syncthreads();
   for (int idx = threadIdx.x; idx < MT * W; idx += blockDim.x) {
