@@ -556,7 +556,7 @@ CLOSURE_STUDIES = {
 
 
 def run_closure_study(args):
-    """The closure judged by a resolved run (closure.study): a fine run
+    """The closure measured against a resolved run (closure.study): a fine run
     box-filtered 4x in every direction trains the network; coarse runs from
     the filtered fine state (prescribed profile, and the closure's two
     couplings) cover the window of the fine run and are compared with its

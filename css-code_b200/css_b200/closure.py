@@ -203,7 +203,7 @@ class Closure:
 
 
 # ---------------------------------------------------------------------------
-# Evaluation: the closure against the prescribed profile, both judged by the
+# Evaluation: the closure against the prescribed profile, both measured against the
 # filtered fine run
 # ---------------------------------------------------------------------------
 def restrict(fine_sim, coarse_sim, factor, fine_base=None, coarse_base=None):
@@ -226,7 +226,7 @@ def prolong_add(coarse_sim, coarse_base, factor, fine_sim):
 
 
 def statistics(sim, rhor):
-    """What a run is judged by, from its resident state: the kinetic-energy
+    """The statistics a run is compared on, from its resident state: the kinetic-energy
     spectrum in azimuthal wavenumber m, E_K(m) = sum over r, theta and the
     three components of rhor(r) |u_hat(m)|^2 / 2, the magnetic one
     E_M(m) = sum |B_hat(m)|^2 / (8 pi) (B = curl A), and the enthalpy- and
@@ -282,7 +282,7 @@ def study(fine, coarse, factor=4, n_pre=0, n_adjust=0, n_train=200, nsnap=4, n_w
     4. the window: every coarse run starts from the filtered fine state at
        its start (css_restrict_state) and covers the physical time of
        ``n_win`` fine steps, sampled ``nstat`` times at the same times as
-       the fine run, whose filtered state is judged by the same diagnostics
+       the fine run, whose filtered state gets the same diagnostics
        (statistics()) on a coarse probe run.
 
     The coarse runs are the prescribed profile and one per coupling of the
