@@ -511,6 +511,128 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
   }
 }
 
+// ---- k_curl_pl: B = curl A's theta and phi parts from TMA-staged planes ----
+// The plane tiles of k_thph (same tile order, same maps) carrying only A:
+// fields 5, 6, 7 (A_theta, A_phi, A_r) of a state buffer; persistent CTAs.
+// Per tile: sin(theta)
+// A_phi in place, the theta lines of sin A_phi and A_r and the phi lines of
+// A_r and A_theta (one warp each, one line per lane), then B_r complete and
+// the theta / phi parts of B_theta / B_phi, with the expressions of
+// k_curl_tp (VectorCurlA, derivatives.f90:1769-1828); k_curl_r adds the
+// radial parts.
+template <int NBUF, int NTH>
+struct CurlCfg {
+  static constexpr int NF = 3;
+  static constexpr int NO = 4;
+  static constexpr int NT = NTH;
+  static constexpr size_t SMEM = 8 * ((size_t)NBUF * NF * FA_FIELD + (size_t)NO * FA_OUT + NBUF);
+};
+
+__device__ __forceinline__ void curl_stage_tma(const CssGeo &g, const PlaneMaps &m, const ThphTile &T, double *F,
+                                               uint64_t *bar) {
+  const int plo = T.p0 >= 4 ? T.p0 - 4 : g.nphi - 4;
+  const int phi = T.p0 + FM < g.nphi ? T.p0 + FM : 0;
+  mbar_expect_tx(bar, 8u * 3 * FA_FIELD);
+#pragma unroll
+  for (int f = 0; f < 3; f++) {
+    double *Fd = F + (size_t)f * FA_FIELD;
+    tma_load_4d(Fd, &m.main, T.t0 - 4, T.p0, T.ir, 5 + f, bar);
+    tma_load_4d(Fd + FA_MAIN, &m.halo, T.t0, plo, T.ir, 5 + f, bar);
+    tma_load_4d(Fd + FA_MAIN + 4 * FM, &m.halo, T.t0, phi, T.ir, 5 + f, bar);
+  }
+}
+
+// NBUF 2: two plane buffers, the next tile's copies under the current
+// tile; NBUF 1: one buffer, the next tile's lines toward L2 at the start of
+// a tile and more CTAs per SM to overlap one CTA's copies with another's
+// solves.  a = A (the state buffer's field 5), for the prefetch.
+template <int NBUF, int NTH>
+__global__ void __launch_bounds__(NTH, NBUF == 2 ? 2 : 3) k_curl_pl(CssGeo g, const double *__restrict__ a,
+                                                                    double *__restrict__ out,
+                                                                    const __grid_constant__ PlaneMaps m, int *flag) {
+  using C = CurlCfg<NBUF, NTH>;
+  extern __shared__ __align__(128) double sm[];
+  double *O = sm + (size_t)NBUF * C::NF * FA_FIELD;
+  uint64_t *bar = reinterpret_cast<uint64_t *>(O + (size_t)C::NO * FA_OUT);
+  const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
+  const size_t n = (size_t)g.ncell;
+  const int ntile = g.nr * g.d[1].nb * g.d[2].nb;
+  if (tid == 0) {
+    for (int k = 0; k < NBUF; k++) mbar_init(bar + k, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  if (NBUF == 2 && tid == 0 && (int)blockIdx.x < ntile) curl_stage_tma(g, m, thph_tile(g, blockIdx.x), sm, bar);
+  for (int q = blockIdx.x, i = 0; q < ntile; q += gridDim.x, i++) {
+    const ThphTile T = thph_tile(g, q);
+    const int b = NBUF == 2 ? (i & 1) : 0;
+    double *F = sm + (size_t)b * C::NF * FA_FIELD;
+    const bool more = q + (int)gridDim.x < ntile;
+    if (NBUF == 2) {
+      // the next planes into the other buffer: its last readers passed the
+      // barrier that ended the previous tile
+      if (more && tid == 0) {
+        fence_proxy_async();
+        curl_stage_tma(g, m, thph_tile(g, q + gridDim.x), sm + (size_t)(b ^ 1) * C::NF * FA_FIELD, bar + (b ^ 1));
+      }
+    } else {
+      if (more) {
+        const double *src[3] = {a, a + n, a + 2 * n};
+        thph_prefetch<3>(g, src, thph_tile(g, q + gridDim.x));
+      }
+      if (tid == 0) {
+        fence_proxy_async();
+        curl_stage_tma(g, m, T, F, bar);
+      }
+    }
+    const unsigned parity = NBUF == 2 ? ((unsigned)(i >> 1) & 1u) : ((unsigned)i & 1u);
+    const bool late = !mbar_wait_bounded(bar + b, parity, kWaitCycles);
+    if (__syncthreads_or(late)) {
+      if (tid == 0) {
+        atomicOr(flag, kFlagTimeout);
+        mbar_wait_bounded(bar + b, parity, kWaitCycles);
+        if (NBUF == 2 && more) mbar_wait_bounded(bar + (b ^ 1), (unsigned)((i + 1) >> 1) & 1u, kWaitCycles);
+      }
+      return;
+    }
+    // sin(theta) A_phi on the main rows (the theta lines' input)
+    double *Fp = F + FA_FIELD;
+    for (int k = tid; k < FM * (FM + 8); k += C::NT) {
+      const int p = k / (FM + 8), c = k - p * (FM + 8), gt = T.t0 - 4 + c;
+      if (gt >= 0 && gt < g.nth) Fp[p * FA_RW + c] *= g.sines[gt];
+    }
+    __syncthreads();
+    if (wrp < 4) {
+      const CssDir &DT = g.d[1];
+      if (wrp < 2) {  // theta lines (line = phi row p = lane): sin A_phi (ibct 11), A_r (ibct 12)
+        const int bdry = g.ibct[wrp == 0 ? 11 : 12];
+        const double dn = DT.dnum[T.bt];
+        line_solve_r<1, FM>(F + (size_t)(1 + wrp) * FA_FIELD + lane * FA_RW, ThIdx{}, dtype_of(DT, T.bt), bdry, 0.0,
+                            0.0, tabp(g, 1, T.bt, 1, bdry), g.tstride, dn, dn, 0, O + wrp * FA_OUT, SwzRow{lane});
+      } else {  // phi lines (line = theta column t = lane): A_r, A_theta
+        const double dn = g.d[2].dnum[T.bp];
+        line_solve_r<1, FM>(F + (size_t)(wrp == 2 ? 2 : 0) * FA_FIELD, PhIdx{lane}, 3, 0, 0.0, 0.0,
+                            tabp(g, 2, T.bp, 1, 0), g.tstride, dn, dn, 1, O + wrp * FA_OUT, SwzCol{lane});
+      }
+    }
+    __syncthreads();
+    const double invr = g.r_inv[T.ir];
+    const size_t pl = plane(g, T.ir);
+#pragma unroll
+    for (int k = 0; k < FM * FM / C::NT; k++) {
+      const int pt = tid + k * C::NT, jp = pt >> 5, jt = pt & 31;
+      const int it = T.t0 + jt;
+      const size_t id = pl + (size_t)(T.p0 + jp) * g.nth + it;
+      const double csc = g.csc[it];
+      out[id] = invr * swz(O + 2 * FA_OUT, jp, jt) * csc;
+      out[n + id] = -swz(O + FA_OUT, jp, jt) * invr;
+      const double prev = __dmul_rn(__dmul_rn(swz(O, jp, jt), csc), invr);
+      out[2 * n + id] = prev - invr * swz(O + 3 * FA_OUT, jp, jt) * csc;
+    }
+    __syncthreads();  // the tiles and this buffer are free for the next tiles
+  }
+}
+
 // ---- k_rstage ----------------------------------------------------------------
 // The slab: field f at H + f*FB_FIELD, row rr = 0..39 (r = r0-4+rr), 32
 // theta values per row.  Derivative tiles O + k*FB_OUT, row r - r0.  On a

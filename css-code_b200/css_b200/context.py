@@ -135,10 +135,11 @@ class Simulation:
         run that does not qualify."""
         check(_lib.lib().css_set_fused(self.h, 1 if on else 0))
 
-    def set_curl_pass(self, one_pass):
-        """B = curl A's theta and phi parts in one pass (default) or two
-        (css_set_curl_pass); bit-identical results."""
-        check(_lib.lib().css_set_curl_pass(self.h, 1 if one_pass else 0))
+    def set_curl_pass(self, mode):
+        """B = curl A's theta and phi parts (css_set_curl_pass): 2 from
+        TMA-staged planes (default), 1 one pass over tiles, 0 two passes
+        (True / False as 1 / 0); bit-identical results."""
+        check(_lib.lib().css_set_curl_pass(self.h, int(mode)))
 
     @property
     def fused(self):

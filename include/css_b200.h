@@ -371,12 +371,14 @@ int css_set_tiles(css_ctx *ctx, int tl_r, int tl_theta, int tl_phi, int phi_pers
  * with CSS_ERR_ARG.  css_get_fused returns the current choice.            */
 int css_set_fused(css_ctx *ctx, int on);
 int css_get_fused(css_ctx *ctx);
-/* B = curl A (VectorCurlA, derivatives.f90:1769-1828) of magnetic runs:
- * with equal theta and phi block sizes of 16 or 32, its theta and phi
- * parts run as one pass over the A tiles (one_pass = 1, the default) or
- * as a theta pass and a phi pass (0); the results are the same bit for
- * bit. */
-int css_set_curl_pass(css_ctx *ctx, int one_pass);
+/* B = curl A (VectorCurlA, derivatives.f90:1769-1828) of magnetic runs,
+ * its theta and phi parts: mode 2 (the default) from planes staged by TMA
+ * in a persistent kernel, for the stage's own state buffers of runs that
+ * take the two-pass stage; mode 1 in one pass over tiles (equal theta and
+ * phi block sizes of 16 or 32); mode 0 a theta pass and a phi pass.  A mode
+ * that does not apply falls back to the next lower one.  The results are
+ * the same bit for bit. */
+int css_set_curl_pass(css_ctx *ctx, int mode);
 
 /* A batched ensemble of independent runs (many small shells, each with its
  * own grid, decomposition and parameters: hydro and MHD members may mix).
