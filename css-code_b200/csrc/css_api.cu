@@ -76,7 +76,8 @@ struct css_ctx {
   double *adjM[3][2][5] = {};
   int *adjOff[3][2][5] = {};
   PlaneMaps pmaps[5];               // two-pass stage: TMA maps of v0, vA, vB, bf (plane kernel) and vs (curl)
-  int vs_map = 0;                   // pmaps[4] holds vs's maps
+  int vs_map = 0;                   // pmaps[4] and vs_slab hold vs's maps
+  SlabMaps vs_slab;
   SlabMaps smaps[5];                // the same for the stage kernel's slabs, then rtw
   double *lapbuf = nullptr;         // explicit viscosity: 6 derivative + 6 kept fields
   double *lapface = nullptr;        // explicit viscosity: face data, 6 x max face size
@@ -453,9 +454,14 @@ static bool plane_maps(css_ctx *c) {
         encode(&c->pmaps[4].halo, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, c->vs, dims, strides, bhalo, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      memset(&c->pmaps[4], 0, sizeof(PlaneMaps));  // the ohmic curl keeps its tile kernel
-    else
-      c->vs_map = 1;
+      memset(&c->pmaps[4], 0, sizeof(PlaneMaps));  // the ohmic curl keeps its tile kernels
+    else {
+      const cuuint32_t bslab[4] = {FM, 1, FM + 8, 1};
+      if (encode(&c->vs_slab.slab, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 4, c->vs, dims, strides, bslab, estr,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS)
+        c->vs_map = 1;
+    }
   }
   {  // rtw: (theta 32, side 2, phi, r), box 32 x 1 x 1 x 32
     const cuuint64_t dims[4] = {32, 2, (cuuint64_t)g.nphi, (cuuint64_t)g.nr};
@@ -963,6 +969,13 @@ static int launch_curl(css_ctx *c, const TS *a, double *out, int apply_bc) {
     LAUNCH_MT(2, TL, k_curl_phi, (TS), gp, smem_line(2, 2, 0, mp, TL), g, a, out, TL);
     prof_end(c);
     if (int rc = check_launch(c)) return rc;
+  }
+  if (c->curl_tp == 2 && c->fused_ok && mi >= 0 && c->mt[0] == 32 && c->mt[1] == 32) {  // radial part from TMA slabs
+    prof_begin(c, KI_CURL_R);
+    k_curl_rs<<<g.d[0].nb * g.d[1].nb * g.nphi, CR_NT, CR_SMEM, c->stream>>>(
+        g, out, mi < 3 ? c->smaps[mi] : c->vs_slab, apply_bc, c->flag);
+    prof_end(c);
+    return check_launch(c);
   }
   TL = c->tl_r;
   dim3 gr(g.d[0].nb * ((g.nth + TL - 1) / TL), g.nphi);

@@ -668,6 +668,105 @@ __device__ __forceinline__ RstageTile rstage_tile(const CssGeo &g, int q) {
   return T;
 }
 
+// ---- k_curl_rs: the radial parts of B = curl A from a TMA-staged slab ------
+// One (r block, theta block, phi) slab per CTA (the tiles of k_rstage):
+// A_theta and A_phi over the block's 32 radii with 4-point halos arrive by
+// TMA (the slab box of the state buffer's maps) while the threads load the
+// theta / phi parts of B that k_curl_pl wrote; r A_theta and r A_phi are
+// solved along r (one warp each, one theta column per lane) and
+// B_phi += d(r A_theta)/dr / r, B_theta -= d(r A_phi)/dr / r (times dxdr on a
+// non-uniform grid), then Compute_B's face zeroing (derivatives.f90:
+// 1830-1892) -- the arithmetic of k_curl_r, in the same order.
+constexpr int CR_NT = 128;
+constexpr int CR_PPT = FM * FM / CR_NT;
+constexpr size_t CR_SMEM = 8 * (2 * (size_t)FB_FIELD + 2 * (size_t)FB_OUT + 1);
+
+// Four CTAs per SM (128 registers, 80 bytes spilled): 2.17 ms per curl on
+// MHD 256x512x1024, against 2.30 with three (164 registers) and 2.33 with
+// six (80 registers, 272 bytes spilled); the two-pass form's k_curl_r takes
+// 2.46.
+__global__ void __launch_bounds__(CR_NT, 4) k_curl_rs(CssGeo g, double *__restrict__ out,
+                                                   const __grid_constant__ SlabMaps ms, int apply_bc, int *flag) {
+  extern __shared__ __align__(128) double sm[];
+  double *H = sm;                   // 0: A_theta, 1: A_phi, then times r
+  double *O = H + 2 * FB_FIELD;     // d/dr of the two lines
+  uint64_t *bar = reinterpret_cast<uint64_t *>(O + 2 * FB_OUT);
+  const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
+  const size_t n = (size_t)g.ncell;
+  const RstageTile T = rstage_tile(g, blockIdx.x);
+  const CssDir &D = g.d[0];
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();  // the barrier is initialised before anyone waits on it
+  if (tid == 0) {
+    mbar_expect_tx(bar, 8u * 2 * FB_FIELD);
+    tma_load_4d(H, &ms.slab, T.t0, T.ip, T.r0 - 4, 5, bar);
+    tma_load_4d(H + FB_FIELD, &ms.slab, T.t0, T.ip, T.r0 - 4, 6, bar);
+  }
+  // this thread's points (row j = r - r0, theta column lane): the theta
+  // and phi parts of B, loaded while the slab arrives
+  double in_t[CR_PPT], in_p[CR_PPT], in_r[CR_PPT];
+#pragma unroll
+  for (int k = 0; k < CR_PPT; k++) {
+    const int j = wrp + 4 * k;
+    const size_t id = css_idx(g, T.t0 + lane, T.ip, T.r0 + j);
+    in_t[k] = out[id];
+    in_p[k] = out[n + id];
+    in_r[k] = out[2 * n + id];
+  }
+  if (__syncthreads_or(!mbar_wait_bounded(bar, 0u, kWaitCycles))) {
+    if (tid == 0) {
+      atomicOr(flag, kFlagTimeout);
+      mbar_wait_bounded(bar, 0u, kWaitCycles);
+    }
+    return;
+  }
+  for (int idx = tid; idx < 2 * FB_FIELD; idx += CR_NT) {
+    const int rr = (idx % FB_FIELD) / FM, gr = T.r0 + rr - 4;
+    if (gr >= 0 && gr < g.nr) H[idx] *= g.r_ind[gr];
+  }
+  __syncthreads();
+  if (wrp < 2) {
+    const int bdry = g.ibcr[wrp == 0 ? 10 : 11];
+    const double dn = D.dnum[T.br];
+    line_solve_r<1, FM>(H + (size_t)wrp * FB_FIELD + 4 * FM + lane, StridedIn{FM}, dtype_of(D, T.br), bdry, 0.0, 0.0,
+                        tabp(g, 0, T.br, 1, bdry), g.tstride, dn, dn, 0, O + wrp * FB_OUT + lane, StridedOut{FM});
+  }
+  __syncthreads();
+  const int it = T.t0 + lane;
+#pragma unroll
+  for (int k = 0; k < CR_PPT; k++) {
+    const int j = wrp + 4 * k, ir = T.r0 + j;
+    const size_t id = css_idx(g, it, T.ip, ir);
+    double d = O[j * FM + lane];
+    if (g.non_uniform) d = d * g.dxdr[ir];
+    double bp_ = in_p[k] + d * g.r_inv[ir];
+    d = O[FB_OUT + j * FM + lane];
+    if (g.non_uniform) d = d * g.dxdr[ir];
+    double bt_ = in_t[k] - d * g.r_inv[ir];
+    double br_ = in_r[k];
+    if (apply_bc) {
+      if (it == 0 || it == g.nth - 1) {
+        if (g.theta_perf_conductor) bt_ = 0.0;
+        else { bp_ = 0.0; br_ = 0.0; }
+      }
+      if (ir == 0) {
+        if (g.bottom_radial_field) { bt_ = 0.0; bp_ = 0.0; }
+        else if (g.bottom_perfect_cond) br_ = 0.0;
+      }
+      if (ir == g.nr - 1) {
+        if (g.top_radial_field) { bt_ = 0.0; bp_ = 0.0; }
+        else if (g.top_perfect_cond) br_ = 0.0;
+      }
+      out[2 * n + id] = br_;
+    }
+    out[id] = bt_;
+    out[n + id] = bp_;
+  }
+}
+
 // STG: the RK4 stage (1..4), compiled in:
 //   1: vs = (sld ? vs + dv/6 : dv); nx = v0 + dtcur*dv
 //   2,3: vs = vs + dv/3;            nx = v0 + dtcur*dv
