@@ -1825,9 +1825,18 @@ static int run_lines(const double *x, double *dx, int n, int nlines, int order, 
     if (bchi) cudaMemcpy(dbh, bchi, nlines * 8, cudaMemcpyHostToDevice);
     if (hlo) cudaMemcpy(dhl, hlo, (size_t)4 * nlines * 8, cudaMemcpyHostToDevice);
     if (hhi) cudaMemcpy(dhh, hhi, (size_t)4 * nlines * 8, cudaMemcpyHostToDevice);
-    k_lines<<<(nlines + 127) / 128, 128>>>(dx_, dy, n, nlines, order, dtype, bdry, bclo ? dbl : nullptr,
-                                           bchi ? dbh : nullptr, hlo ? dhl : nullptr, hhi ? dhh : nullptr, dT, ts, dnum,
-                                           scale, work);
+    if (n <= KL_MAXN) {  // lines staged through shared memory, every global access coalesced
+      const size_t smem = 2 * (size_t)KL_LINES * (n + 9) * 8;
+      cudaFuncSetAttribute(k_lines_tiled, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           2 * KL_LINES * (KL_MAXN + 9) * 8);  // on the current device
+      k_lines_tiled<<<(nlines + KL_LINES - 1) / KL_LINES, 128, smem>>>(
+          dx_, dy, n, nlines, order, dtype, bdry, bclo ? dbl : nullptr, bchi ? dbh : nullptr, hlo ? dhl : nullptr,
+          hhi ? dhh : nullptr, dT, ts, dnum, scale);
+    } else {
+      k_lines<<<(nlines + 127) / 128, 128>>>(dx_, dy, n, nlines, order, dtype, bdry, bclo ? dbl : nullptr,
+                                             bchi ? dbh : nullptr, hlo ? dhl : nullptr, hhi ? dhh : nullptr, dT, ts,
+                                             dnum, scale, work);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) fail("k_lines", e);
     else if ((e = cudaMemcpy(dx, dy, nb, cudaMemcpyDeviceToHost)) != cudaSuccess) fail("lines copy", e);
   }

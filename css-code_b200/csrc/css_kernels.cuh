@@ -2085,6 +2085,52 @@ __global__ void k_deriv_adjoint(CssGeo g, int dir, const double *__restrict__ M,
   gout[id] = acc;
 }
 
+// independent lines with explicit closures, staged through shared memory:
+// a CTA of 128 threads takes KL_LINES consecutive lines (contiguous in
+// memory, so the whole CTA reads and writes them with consecutive
+// addresses), one thread solves each line from its shared row (rows of
+// n + 9 doubles, an odd stride: the solving threads touch distinct banks),
+// and the results go back the same way.  The arithmetic per line is
+// k_lines's.  n <= KL_MAXN.
+#define KL_LINES 16
+#define KL_MAXN 248
+__global__ void __launch_bounds__(128) k_lines_tiled(const double *__restrict__ x, double *__restrict__ out, int n,
+                                                     int nlines, int order, int dtype, int bdry,
+                                                     const double *__restrict__ bclo, const double *__restrict__ bchi,
+                                                     const double *__restrict__ hlo, const double *__restrict__ hhi,
+                                                     const double *__restrict__ tab, int ts, double dnum,
+                                                     double scale) {
+  extern __shared__ double sm[];
+  const int sr = n + 9;  // n + 8 used, odd
+  double *X = sm, *Y = sm + (size_t)KL_LINES * sr;
+  const int l0 = blockIdx.x * KL_LINES, nl = min(KL_LINES, nlines - l0);
+  const size_t base = (size_t)l0 * n;
+  for (int k = threadIdx.x; k < nl * n; k += blockDim.x) {
+    const int l = k / n, j = k - l * n;
+    X[l * sr + 4 + j] = x[base + k];
+  }
+  for (int k = threadIdx.x; k < nl * 8; k += blockDim.x) {
+    const int l = k >> 3, q = k & 7;
+    const double *h = q < 4 ? hlo : hhi;
+    X[l * sr + (q < 4 ? q : n + q)] = h ? h[(size_t)4 * (l0 + l) + (q & 3)] : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x < nl) {
+    const int l = threadIdx.x;
+    const double lo = bclo ? bclo[l0 + l] : 0.0, hi = bchi ? bchi[l0 + l] : 0.0;
+    const double *G = tab + (size_t)bdry * 3 * ts;
+    if (order == 1)
+      line_solve<1>(X + l * sr + 4, 1, n, dtype, bdry, lo, hi, G, ts, dnum, scale, 0, Y + l * sr, 1);
+    else
+      line_solve<2>(X + l * sr + 4, 1, n, dtype, bdry, lo, hi, G, ts, dnum, scale, 0, Y + l * sr, 1);
+  }
+  __syncthreads();
+  for (int k = threadIdx.x; k < nl * n; k += blockDim.x) {
+    const int l = k / n, j = k - l * n;
+    out[base + k] = Y[l * sr + j];
+  }
+}
+
 // independent lines with explicit closures (css_compact_lines /
 // Dbyd1_dt0): one thread per line on global memory, lines contiguous.
 __global__ void k_lines(const double *__restrict__ x, double *__restrict__ out, int n, int nlines, int order,

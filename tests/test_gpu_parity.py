@@ -73,6 +73,22 @@ def test_compact_lines_all_closures(lphys, rphys, order, gpu_available):
         assert rel(g, o) < 1e-13, (bdry, rel(g, o))
 
 
+@pytest.mark.parametrize("n,nl", [(248, 37), (249, 5), (300, 20)])
+def test_compact_lines_both_kernels(n, nl, gpu_available):
+    """Lines up to 248 points run the shared-memory tiled kernel (16 lines
+    per CTA, a partial last CTA here), longer ones the one-thread-per-line
+    kernel; both against the oracle."""
+    rng = np.random.default_rng(n)
+    x = np.cos(np.linspace(0, 4, n))[None, :] + 0.1 * rng.standard_normal((nl, n))
+    hl, hh = rng.standard_normal((nl, 4)), rng.standard_normal((nl, 4))
+    for order in (1, 2):
+        for lphys, rphys in ((True, False), (False, True), (False, False)):
+            bl, bh = rng.standard_normal(nl), rng.standard_normal(nl)
+            g = compact_lines(x, order, lphys, rphys, 2, bl, bh, hl, hh, dnum=7.0, scale=7.0 ** order)
+            o = O.compact_lines(x, order, lphys, rphys, 2, bl, bh, hl, hh, dnum=7.0, scale=7.0 ** order)
+            assert rel(g, o) < 1e-13, (order, lphys, rphys, rel(g, o))
+
+
 @pytest.mark.parametrize("decomp,dims", [((2, 2, 4), (64, 64, 128)), ((3, 2, 3), (60, 64, 96)),
                                          ((2, 4, 3), (48, 80, 60))])
 def test_deriv_parity_all_directions(decomp, dims, gpu_available):
