@@ -555,6 +555,90 @@ CLOSURE_STUDIES = {
 }
 
 
+PRECISION_STUDIES = {
+    # workload: grid, magnetic, mixed steps, FP64 steps, checkpoints, statistics every
+    "precision-study": ("hydro-128x256x512", 1000, 1000, (100, 1000), 20),
+    "precision-study-mhd": ("mhd-256x512x1024", 500, 100, (100,), 20),
+}
+
+
+def run_precision_study(args):
+    """The mixed-precision form beside FP64 from the same seeded state, the
+    two runs stepped side by side.  ``precision-study``: hydro 128x256x512,
+    1000 steps of each; per-field relative error (max |mixed - fp64| / max
+    |fp64|, plane by plane) at steps 100 and 1000, and the time-averaged
+    kinetic energy (Scalar_Output's kinener) and enthalpy-flux profile
+    (Shell_Average code 16) of each run.  ``precision-study-mhd``: MHD
+    256x512x1024, 500 mixed steps with the FP64 run over the first 100 as
+    the reference; the error at step 100 and each run's statistics over its
+    own steps.  Prints one JSON line."""
+    import numpy as np
+    import torch
+    from css_b200 import problem
+    from css_b200.context import Simulation
+    torch.cuda.set_device(0)
+    name, n_mixed, n_fp64, checks, every = PRECISION_STUDIES[args.workload]
+    p, prof, v0, dt, _ = problem.build(name)
+    steps = {"fp64": n_fp64, "mixed": n_mixed}
+    sims, acc = {}, {}
+    for label, prec in (("fp64", 0), ("mixed", 1)):
+        q = p.copy()
+        q.precision = prec
+        sims[label] = Simulation(q, prof)
+        sims[label].upload(v0)
+        acc[label] = {"ke": [], "fen": [], "ms": 0.0}
+    del v0
+    names = ["rho", "u_theta", "u_phi", "u_r", "s", "A_theta", "A_phi", "A_r"]
+    nv = 8 if p.magnetic else 5
+    errors, done = {}, 0
+    while done < max(steps.values()):
+        k = every
+        for label, sim in sims.items():
+            if done >= steps[label]:
+                continue
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            sim.step_rk4(dt, k)
+            torch.cuda.synchronize()
+            acc[label]["ms"] += 1e3 * (time.perf_counter() - t0)
+            acc[label]["ke"].append(sim.scalars()["kinener"])
+            acc[label]["fen"].append(sim.shell_averages([16])[0])
+        done += k
+        if done in checks and done <= min(steps.values()):
+            err = {}
+            for iv in range(nv):
+                dmax = amax = 0.0
+                for ir in range(p.nr):
+                    a, b = sims["mixed"].plane(iv, ir), sims["fp64"].plane(iv, ir)
+                    dmax = max(dmax, float(np.abs(a - b).max()))
+                    amax = max(amax, float(np.abs(b).max()))
+                err[names[iv]] = dmax / max(amax, 1e-300)
+            errors[str(done)] = err
+        for label in list(sims):
+            if done >= steps[label] and label == "fp64" and steps["mixed"] > steps["fp64"]:
+                sims.pop(label).close()  # the reference run ends here; its memory goes back
+    for sim in sims.values():
+        sim.close()
+    res = {k: {"ke": float(np.mean(a["ke"])), "fen": np.mean(a["fen"], axis=0), "ms": a["ms"] / steps[k]}
+           for k, a in acc.items()}
+    out = {"metric": "mixed-precision state error against FP64 and time-averaged statistics",
+           "value": max(max(e.values()) for e in errors.values()), "unit": "max per-field relative error",
+           "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+           "config": {"workload": args.workload, "grid": name, "dt": dt, "mixed_steps": n_mixed,
+                      "fp64_steps": n_fp64, "statistics_every": every},
+           "errors_at_step": errors,
+           "kinetic_energy_time_avg": {k: r["ke"] for k, r in res.items()},
+           "ms_per_step": {k: r["ms"] for k, r in res.items()},
+           "enthalpy_flux_time_avg": {k: [float(x) for x in r["fen"]] for k, r in res.items()}}
+    if steps["fp64"] == steps["mixed"]:
+        f, m = res["fp64"]["fen"], res["mixed"]["fen"]
+        out["enthalpy_flux_rel_diff"] = float(np.linalg.norm(m - f) / max(np.linalg.norm(f), 1e-300))
+        out["kinetic_energy_rel_diff"] = abs(res["mixed"]["ke"] - res["fp64"]["ke"]) / max(abs(res["fp64"]["ke"]),
+                                                                                            1e-300)
+    print(json.dumps(out))
+    return 0
+
+
 def run_closure_study(args):
     """The closure measured against a resolved run (closure.study): a fine run
     box-filtered 4x in every direction trains the network; coarse runs from
@@ -727,6 +811,8 @@ def main():
         return run_ensemble(args)
     if args.workload in CLOSURE_STUDIES:
         return run_closure_study(args)
+    if args.workload in PRECISION_STUDIES:
+        return run_precision_study(args)
     if args.workload.startswith("closure-"):
         return run_closure(args)
     return run_ours(args)
