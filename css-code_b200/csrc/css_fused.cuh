@@ -4,7 +4,8 @@
 //
 //   k_thph    tiles of one (theta block, phi block, radius) plane: the
 //             32x32 plane of the two blocks with 4-point halos in theta and
-//             phi is staged once in shared memory; Source_Theta_Terms
+//             phi is staged once in shared memory, and the theta and phi
+//             line solves of every field run at once; Source_Theta_Terms
 //             (+ Lorentz, + Induction_Terms), Phi_Terms (+ Lorentz) and, on
 //             blocks with no theta wall, Density_Terms_Theta run from it, and
 //             the tendency of every field and the stage temperature are
@@ -56,22 +57,31 @@ constexpr int FA_FIELD = FA_MAIN + 8 * FM;
 // pointwise phase (t across the warp) all touch 16 distinct 8-byte banks
 constexpr int FA_OUT = FM * FM;
 
+// offset of field f in a plane buffer: MHD's B_phi (field 6) has no phi
+// derivative, so it is staged without its phi-halo rows and B_r follows its
+// main rows (10944 doubles in: still 128-byte aligned)
+__host__ __device__ constexpr int thph_foff(int mag, int f) {
+  return f * FA_FIELD - ((mag && f == 7) ? 8 * FM : 0);
+}
+
 template <int MAG>
 struct ThphCfg {
   static constexpr int NF = MAG ? 8 : 5;     // rho w v u s [bt bp br]
-  // derivative tiles: hydro holds both directions' (theta 0-5, phi 6-11)
-  // at once; MHD holds one direction's eight at a time
-  static constexpr int NO = MAG ? 8 : 12;
-  static constexpr int PHI0 = MAG ? 0 : 6;   // first phi tile
+  // derivative tiles: both directions' at once (theta 0-5, phi 6-11 hydro;
+  // theta 0-7, phi 8-15 MHD)
+  static constexpr int NO = MAG ? 16 : 12;
+  static constexpr int PHI0 = MAG ? 8 : 6;   // first phi tile
+  static constexpr int PLANE = MAG ? 7 * FA_FIELD + FA_MAIN : NF * FA_FIELD;  // doubles of one plane buffer
   // hydro stages the next tile's plane into a second buffer while it
   // computes the current one; MHD (eight fields) has room for one plane and
   // brings the next one toward L2 instead
   static constexpr int NBUF = MAG ? 1 : 2;
   // + one mbarrier per plane buffer
-  static constexpr size_t SMEM = 8 * ((size_t)NBUF * NF * FA_FIELD + (size_t)NO * FA_OUT + NBUF);
+  static constexpr size_t SMEM = 8 * ((size_t)NBUF * PLANE + (size_t)NO * FA_OUT + NBUF);
   // bytes one plane's copies deliver
-  static constexpr unsigned TX = 8u * NF * FA_FIELD;
+  static constexpr unsigned TX = 8u * PLANE;
 };
+static_assert(ThphCfg<1>::SMEM <= 232448, "MHD plane pass: one plane and sixteen tiles fit 227 KB");
 
 // index maps of the lines (css_lines.cuh: the solver reads xb[xi(j)] and
 // writes ob[oi(j)])
@@ -191,13 +201,15 @@ __device__ __forceinline__ void thph_stage_tma(const CssGeo &g, const PlaneMaps 
                                                const ThphTile &T, double *F, uint64_t *bar) {
   const int plo = T.p0 >= 4 ? T.p0 - 4 : g.nphi - 4;
   const int phi = T.p0 + FM < g.nphi ? T.p0 + FM : 0;
-  mbar_expect_tx(bar, 8u * NF * FA_FIELD);
+  constexpr int MAGF = NF == 8;
+  mbar_expect_tx(bar, 8u * ThphCfg<MAGF>::PLANE);
 #pragma unroll
   for (int f = 0; f < NF; f++) {
     const PlaneMaps &m = f < 5 ? mc : mb;
     const int w = f < 5 ? f : f - 5;
-    double *Fd = F + (size_t)f * FA_FIELD;
+    double *Fd = F + thph_foff(MAGF, f);
     tma_load_4d(Fd, &m.main, T.t0 - 4, T.p0, T.ir, w, bar);
+    if (MAGF && f == 6) continue;  // B_phi: main rows only
     tma_load_4d(Fd + FA_MAIN, &m.halo, T.t0, plo, T.ir, w, bar);
     tma_load_4d(Fd + FA_MAIN + 4 * FM, &m.halo, T.t0, phi, T.ir, w, bar);
   }
@@ -216,7 +228,7 @@ __device__ __forceinline__ void thph_theta_solve(const CssGeo &g, const double *
   else if (MAG && k < 7) { f = k + 1; var = k + 3; }  // bp (8), br (9)
   else { f = 0; var = 1; }
   const int bdry = g.ibct[var];
-  const double *x = F + (size_t)f * FA_FIELD + p * FA_RW;
+  const double *x = F + thph_foff(MAG, f) + p * FA_RW;
   double lo = 0.0, hi = 0.0;
   const int nth = g.nth;
   if (f == 2) {  // stress-free datum cot(theta)*v on the walls (rhs_mpi.f90:414, :444)
@@ -245,7 +257,7 @@ __device__ __forceinline__ void thph_phi_solve(const CssGeo &g, const double *F,
                                                int k0, int t) {
   const int f = k == 0 ? 0 : k == 1 ? 2 : k == 2 ? 1 : k == 3 ? 3 : k <= 5 ? 4 : (k == 6 ? 5 : 7);
   const double dn = g.d[2].dnum[T.bp];
-  const double *x = F + (size_t)f * FA_FIELD;
+  const double *x = F + thph_foff(1, f);  // fields 0..5, 7: f = 7 only for MHD
   if (k == 5) {
     if (g.slaplacian)
       line_solve_r<2, FM>(x, PhIdx{t}, 3, 0, 0.0, 0.0, tabp(g, 2, T.bp, 2, 0), g.tstride, dn, dn * dn, 1,
@@ -279,7 +291,7 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
   // plane buffers (128-byte aligned boxes: a field is 12800 bytes), the
   // derivative tiles, the buffers' mbarriers
   extern __shared__ __align__(128) double sm[];
-  double *O = sm + (size_t)C::NBUF * C::NF * FA_FIELD;  // NO derivative tiles
+  double *O = sm + (size_t)C::NBUF * C::PLANE;  // NO derivative tiles
   uint64_t *bar = reinterpret_cast<uint64_t *>(O + (size_t)C::NO * FA_OUT);
   const int tid = threadIdx.x, lane = tid & 31, wrp = tid >> 5;
   const size_t n = (size_t)g.ncell;
@@ -294,14 +306,14 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
   for (int q = blockIdx.x, i = 0; q < ntile; q += gridDim.x, i++) {
     const ThphTile T = thph_tile(g, q);
     const int b = C::NBUF == 2 ? (i & 1) : 0;
-    double *F = sm + (size_t)b * C::NF * FA_FIELD;
+    double *F = sm + (size_t)b * C::PLANE;
     const bool more = q + (int)gridDim.x < ntile;
     if (C::NBUF == 2) {
       // the next plane into the other buffer: its last readers passed the
       // barrier that ended the previous tile
       if (more && tid == 0) {
         fence_proxy_async();
-        thph_stage_tma<C::NF>(g, mc, mb, thph_tile(g, q + gridDim.x), sm + (size_t)(b ^ 1) * C::NF * FA_FIELD,
+        thph_stage_tma<C::NF>(g, mc, mb, thph_tile(g, q + gridDim.x), sm + (size_t)(b ^ 1) * C::PLANE,
                               bar + (b ^ 1));
       }
     } else if (tid == 0) {
@@ -342,15 +354,16 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
 #pragma unroll
       for (int h = 0; h < 2; h++) tbuf[pl + (size_t)(T.p0 + wrp + 16 * h) * g.nth + it] = tq[h];
     }
-    // ---- solves: theta (warps 0-5 hydro, 0-7 MHD), phi (warps 6-11 hydro) ----
+    // ---- solves: theta (warps 0-5 hydro, 0-7 MHD), phi (warps 6-11 hydro,
+    // 8-15 MHD), all at once ----
     {
       const int nth_t = (MAG ? 7 : 5) + (wall ? 0 : 1);
       const int nthw = MAG ? 8 : 6;  // theta warps; the last one solves d(rho)/dtheta
       if (wrp < nthw) {
         if (wrp < nth_t) thph_theta_solve<MAG>(g, F, O, T, wrp, lane);
         else thph_wall_rho(g, F, T, lane, rtw);
-      } else if (!MAG && wrp < 12) {
-        thph_phi_solve(g, F, O, T, wrp - 6, C::PHI0, lane);
+      } else if (wrp < nthw + 8 - (MAG ? 0 : 2)) {
+        thph_phi_solve(g, F, O, T, wrp - nthw, C::PHI0, lane);
       }
     }
     __syncthreads();
@@ -403,7 +416,7 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
         if (MAG) {
           double oo = invrho;
           oo = oo * ONE_OVER_4PI * ri;
-          const double bt_ = F[5 * FA_FIELD + ic], bp_ = F[6 * FA_FIELD + ic], br_ = F[7 * FA_FIELD + ic];
+          const double bt_ = F[5 * FA_FIELD + ic], bp_ = F[6 * FA_FIELD + ic], br_ = F[thph_foff(MAG, 7) + ic];
           du = du - bt_ * bt_ * oo;
           dw = dw - bp_ * bp_ * ct * oo;
           dvv = dvv + bp_ * bt_ * ct * oo;
@@ -427,11 +440,6 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
         }
         acc[h][0] = drho; acc[h][1] = dw; acc[h][2] = dvv; acc[h][3] = du; acc[h][4] = ds;
       }
-    }
-    if (MAG) {  // the phi derivatives replace the theta ones
-      __syncthreads();
-      if (wrp < 8) thph_phi_solve(g, F, O, T, wrp, C::PHI0, lane);
-      __syncthreads();
     }
     // ---- phi pointwise (Phi_Terms + Lorentz), then the stores ----
     {
@@ -463,7 +471,7 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
         }
         if (MAG) {
           const double oo = ONE_OVER_4PI * oorho * oors;
-          const double bt_ = F[5 * FA_FIELD + ic], bp_ = F[6 * FA_FIELD + ic], br_ = F[7 * FA_FIELD + ic];
+          const double bt_ = F[5 * FA_FIELD + ic], bp_ = F[6 * FA_FIELD + ic], br_ = F[thph_foff(MAG, 7) + ic];
           w1 = swz(OP + 6 * FA_OUT, p, lane) * oo;
           dvv = dvv - bt_ * w1;
           dw = dw + bp_ * w1;
