@@ -253,11 +253,12 @@ __device__ __forceinline__ void thph_theta_solve(const CssGeo &g, const double *
 
 // phi line solve of derivative tile k (0 drho 1 dv 2 dw 3 du 4 ds 5 d2s
 // [6 dbt 7 dbr]) into O + k0 + k, line (theta column) t
+template <int MAG>
 __device__ __forceinline__ void thph_phi_solve(const CssGeo &g, const double *F, double *O, const ThphTile &T, int k,
                                                int k0, int t) {
   const int f = k == 0 ? 0 : k == 1 ? 2 : k == 2 ? 1 : k == 3 ? 3 : k <= 5 ? 4 : (k == 6 ? 5 : 7);
   const double dn = g.d[2].dnum[T.bp];
-  const double *x = F + thph_foff(1, f);  // fields 0..5, 7: f = 7 only for MHD
+  const double *x = F + thph_foff(MAG, f);
   if (k == 5) {
     if (g.slaplacian)
       line_solve_r<2, FM>(x, PhIdx{t}, 3, 0, 0.0, 0.0, tabp(g, 2, T.bp, 2, 0), g.tstride, dn, dn * dn, 1,
@@ -362,8 +363,8 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
       if (wrp < nthw) {
         if (wrp < nth_t) thph_theta_solve<MAG>(g, F, O, T, wrp, lane);
         else thph_wall_rho(g, F, T, lane, rtw);
-      } else if (wrp < nthw + 8 - (MAG ? 0 : 2)) {
-        thph_phi_solve(g, F, O, T, wrp - nthw, C::PHI0, lane);
+      } else if (wrp < (MAG ? 16 : 12)) {
+        thph_phi_solve<MAG>(g, F, O, T, wrp - nthw, C::PHI0, lane);
       }
     }
     __syncthreads();
