@@ -659,10 +659,11 @@ constexpr int CR_NT = 128;
 constexpr int CR_PPT = FM * FM / CR_NT;
 constexpr size_t CR_SMEM = 8 * (2 * (size_t)FB_FIELD + 2 * (size_t)FB_OUT + 1);
 
-// Four CTAs per SM (128 registers, 80 bytes spilled): 2.17 ms per curl on
-// MHD 256x512x1024, against 2.30 with three (164 registers) and 2.33 with
-// six (80 registers, 272 bytes spilled); the two-pass form's k_curl_r takes
-// 2.46.
+// Four CTAs per SM (128 registers, 80 bytes spilled): 2.13-2.17 ms per curl
+// on MHD 256x512x1024, against 2.30 with three (164 registers), 2.33 with
+// six (80 registers, 272 bytes spilled) and 3.07 with six CTAs of 64
+// threads that load their B parts after the solves; the two-pass form's
+// k_curl_r takes 2.46.
 __global__ void __launch_bounds__(CR_NT, 4) k_curl_rs(CssGeo g, double *__restrict__ out,
                                                    const __grid_constant__ SlabMaps ms, int apply_bc, int *flag) {
   extern __shared__ __align__(128) double sm[];
