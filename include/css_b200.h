@@ -215,7 +215,9 @@ int css_d2bydp2(css_ctx *ctx, const double *x, double *dx, int var);
  * result depends on its radius; NULL means index p (mod nphi or nr).
  * var as in the named routines.  The pencils of a call are consecutive in
  * x and dx (pencil p at p * nth * nr, or p * nth * nphi); each comes back
- * as the same plane of the whole-field derivative.  Host pointers.        */
+ * as the same plane of the whole-field derivative.  Host pointers.  Like
+ * css_deriv it works in the stage buffers, so it must not overlap a step
+ * of the same context on another stream.                                  */
 int css_deriv_pencils(css_ctx *ctx, int dir, int order, int npencils, const int *index,
                       const double *x, double *dx, const double *bc_lo, const double *bc_hi,
                       int var);
