@@ -317,9 +317,11 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
         thph_stage_tma<C::NF>(g, mc, mb, thph_tile(g, q + gridDim.x), sm + (size_t)(b ^ 1) * C::PLANE,
                               bar + (b ^ 1));
       }
-    } else if (tid == 0) {
-      // MHD: this tile's planes now (bringing the next tile's lines toward
-      // L2 first, as an earlier form did, cost 11.6 against 9.8 ms a launch)
+    } else if (tid == 0 && i == 0) {
+      // MHD: the first tile's planes; each later tile's copies start under
+      // the previous tile's pointwise phases, once its plane values are in
+      // registers (bringing the next tile's lines toward L2 instead, as an
+      // earlier form did, cost 11.6 against 9.8 ms a launch)
       fence_proxy_async();
       thph_stage_tma<C::NF>(g, mc, mb, T, F, bar);
     }
@@ -368,6 +370,23 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
       }
     }
     __syncthreads();
+    // this thread's plane values of the pointwise phases; for MHD the plane
+    // buffer is then free and the next tile's copies start under them (8.27
+    // against 6.92 ms a launch at 256x512x1024)
+    double pv[2][7];
+#pragma unroll
+    for (int h = 0; h < 2; h++) {
+      const int ic = (wrp + 16 * h) * FA_RW + lane + 4;
+      pv[h][0] = F[ic]; pv[h][1] = F[FA_FIELD + ic]; pv[h][2] = F[2 * FA_FIELD + ic]; pv[h][3] = F[3 * FA_FIELD + ic];
+      if (MAG) { pv[h][4] = F[5 * FA_FIELD + ic]; pv[h][5] = F[6 * FA_FIELD + ic]; pv[h][6] = F[thph_foff(MAG, 7) + ic]; }
+    }
+    if (C::NBUF == 1) {
+      __syncthreads();
+      if (more && tid == 0) {
+        fence_proxy_async();
+        thph_stage_tma<C::NF>(g, mc, mb, thph_tile(g, q + gridDim.x), F, bar);
+      }
+    }
     // ---- theta pointwise (Source_Theta_Terms, Lorentz, induction, and
     // Density_Terms_Theta off the walls): two points per thread ----
     const double ri = g.r_inv[ir];
@@ -380,8 +399,7 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int p = wrp + 16 * h;
-        const int ic = p * FA_RW + lane + 4;
-        const double rho = F[ic], w = F[FA_FIELD + ic], v = F[2 * FA_FIELD + ic], u = F[3 * FA_FIELD + ic];
+        const double rho = pv[h][0], w = pv[h][1], v = pv[h][2], u = pv[h][3];
         const double t = tq[h], invrho = rq[h], oorho_t = rtq[h];
         double dw = omsq * sn * cs;
         double du = -g.grav[ir] + omsq * sn * sn;
@@ -417,7 +435,7 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
         if (MAG) {
           double oo = invrho;
           oo = oo * ONE_OVER_4PI * ri;
-          const double bt_ = F[5 * FA_FIELD + ic], bp_ = F[6 * FA_FIELD + ic], br_ = F[thph_foff(MAG, 7) + ic];
+          const double bt_ = pv[h][4], bp_ = pv[h][5], br_ = pv[h][6];
           du = du - bt_ * bt_ * oo;
           dw = dw - bp_ * bp_ * ct * oo;
           dvv = dvv + bp_ * bt_ * ct * oo;
@@ -449,8 +467,7 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
 #pragma unroll
       for (int h = 0; h < 2; h++) {
         const int p = wrp + 16 * h;
-        const int ic = p * FA_RW + lane + 4;
-        const double rho = F[ic], v = F[2 * FA_FIELD + ic];
+        const double rho = pv[h][0], v = pv[h][2];
         const double t = tq[h], oorho = rq[h], oorho_t = rtq[h];
         double drho = acc[h][0], dw = acc[h][1], dvv = acc[h][2], du = acc[h][3], ds = acc[h][4];
         double w1 = swz(OP, p, lane) * oors;
@@ -472,7 +489,7 @@ __global__ void __launch_bounds__(FNT, 1) k_thph(CssGeo g, const double *__restr
         }
         if (MAG) {
           const double oo = ONE_OVER_4PI * oorho * oors;
-          const double bt_ = F[5 * FA_FIELD + ic], bp_ = F[6 * FA_FIELD + ic], br_ = F[thph_foff(MAG, 7) + ic];
+          const double bt_ = pv[h][4], bp_ = pv[h][5], br_ = pv[h][6];
           w1 = swz(OP + 6 * FA_OUT, p, lane) * oo;
           dvv = dvv - bt_ * w1;
           dw = dw + bp_ * w1;
