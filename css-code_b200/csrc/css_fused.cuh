@@ -544,8 +544,10 @@ __device__ __forceinline__ void curl_stage_tma(const CssGeo &g, const PlaneMaps 
 
 // NBUF 2: two plane buffers, the next tile's copies under the current
 // tile; NBUF 1: one buffer and more CTAs per SM, so that one CTA's copies
-// overlap another's solves (bringing the next tile's lines toward L2 at the
-// start of a tile, as an earlier form did, cost 1.61 against 1.51 ms).
+// overlap another's solves, and each CTA's next copies start under its own
+// stores (1.51 -> 1.44 ms a launch on MHD 256x512x1024; bringing the next
+// tile's lines toward L2 at the start of a tile instead, as an earlier form
+// did, cost 1.61 against 1.51 ms).
 template <int NBUF, int NTH>
 __global__ void __launch_bounds__(NTH, NBUF == 2 ? 2 : 3) k_curl_pl(CssGeo g, double *__restrict__ out,
                                                                     const __grid_constant__ PlaneMaps m, int *flag) {
@@ -574,11 +576,11 @@ __global__ void __launch_bounds__(NTH, NBUF == 2 ? 2 : 3) k_curl_pl(CssGeo g, do
         fence_proxy_async();
         curl_stage_tma(g, m, thph_tile(g, q + gridDim.x), sm + (size_t)(b ^ 1) * C::NF * FA_FIELD, bar + (b ^ 1));
       }
-    } else {
-      if (tid == 0) {
-        fence_proxy_async();
-        curl_stage_tma(g, m, T, F, bar);
-      }
+    } else if (tid == 0 && i == 0) {
+      // the first tile's planes; each later tile's copies start once the
+      // previous tile's solves are done with the buffer
+      fence_proxy_async();
+      curl_stage_tma(g, m, T, F, bar);
     }
     const unsigned parity = NBUF == 2 ? ((unsigned)(i >> 1) & 1u) : ((unsigned)i & 1u);
     const bool late = !mbar_wait_bounded(bar + b, parity, kWaitCycles);
@@ -611,6 +613,12 @@ __global__ void __launch_bounds__(NTH, NBUF == 2 ? 2 : 3) k_curl_pl(CssGeo g, do
       }
     }
     __syncthreads();
+    // the stores read only the derivative tiles: with one buffer, the next
+    // tile's planes arrive under them
+    if (NBUF == 1 && more && tid == 0) {
+      fence_proxy_async();
+      curl_stage_tma(g, m, thph_tile(g, q + gridDim.x), F, bar);
+    }
     const double invr = g.r_inv[T.ir];
     const size_t pl = plane(g, T.ir);
 #pragma unroll
