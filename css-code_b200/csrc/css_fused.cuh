@@ -20,8 +20,9 @@
 //             the next stage state.
 //
 // The plane pass is persistent (one 512-thread CTA per SM walks the tiles;
-// hydro double-buffers its planes, MHD stages each tile's planes with TMA
-// alone: an L2 prefetch of the next tile's lines made it slower); the slab
+// hydro double-buffers its planes, MHD refills its one plane buffer by TMA
+// under the pointwise phases: an L2 prefetch of the next tile's lines made
+// it slower); the slab
 // pass takes one tile per CTA and brings the tile's per-point lines toward
 // L2 while its slab arrives.  Inside a tile the line solves of different
 // fields and directions run side by side on different warps (forward values in registers, css_lines.cuh
@@ -73,8 +74,8 @@ struct ThphCfg {
   static constexpr int PHI0 = MAG ? 8 : 6;   // first phi tile
   static constexpr int PLANE = MAG ? 7 * FA_FIELD + FA_MAIN : NF * FA_FIELD;  // doubles of one plane buffer
   // hydro stages the next tile's plane into a second buffer while it
-  // computes the current one; MHD (eight fields) has room for one plane and
-  // brings the next one toward L2 instead
+  // computes the current one; MHD (eight fields) has room for one plane,
+  // refilled with the next tile's once the solves are done with it
   static constexpr int NBUF = MAG ? 1 : 2;
   // + one mbarrier per plane buffer
   static constexpr size_t SMEM = 8 * ((size_t)NBUF * PLANE + (size_t)NO * FA_OUT + NBUF);
