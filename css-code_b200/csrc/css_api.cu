@@ -1301,7 +1301,9 @@ static int launch_stage_fused(css_ctx *c, const double *cur, double *nx, int sta
   if (int rc = check_launch(c)) return rc;
   if (with_sld)
     if (int rc = launch_sld(c, cur, cur + 5 * c->ncell, c->vs, c->tbuf)) return rc;
-  const dim3 gb(g.d[0].nb * g.d[1].nb * g.nphi);  // one tile per CTA
+  // hydro: one tile per CTA; MHD: persistent, one CTA per SM
+  const int nrtile = g.d[0].nb * g.d[1].nb * g.nphi;
+  const dim3 gb(mag ? std::min(c->nsm, nrtile) : nrtile);
   prof_begin(c, KI_RSTAGE);
 #define CSS_RSTAGE(M, S)                                                                                      \
   k_rstage<M, S><<<gb, RstageCfg<M>::NT, RstageCfg<M>::SMEM, c->stream>>>(g, cur, c->bf, c->dv, c->v0, c->vs, nx, c->tbuf, \

@@ -23,8 +23,8 @@
 // hydro double-buffers its planes, MHD refills its one plane buffer by TMA
 // under the pointwise phases: an L2 prefetch of the next tile's lines made
 // it slower); the slab
-// pass takes one tile per CTA and brings the tile's per-point lines toward
-// L2 while its slab arrives.  Inside a tile the line solves of different
+// pass brings each tile's per-point lines toward L2 while its slab arrives,
+// one tile per CTA for hydro, persistent for MHD.  Inside a tile the line solves of different
 // fields and directions run side by side on different warps (forward values in registers, css_lines.cuh
 // line_solve_r), with the spare warps computing the pointwise quantities
 // (temperature, 1/rho) the physics phase needs.
@@ -641,9 +641,13 @@ __global__ void __launch_bounds__(NTH, NBUF == 2 ? 2 : 3) k_curl_pl(CssGeo g, do
 // The slab: field f at H + f*FB_FIELD, row rr = 0..39 (r = r0-4+rr), 32
 // theta values per row.  Derivative tiles O + k*FB_OUT, row r - r0.  On a
 // theta-wall block W holds the zero-datum d(rho)/dtheta rows k_thph left in
-// rtw.  One tile per CTA: hydro 256 threads, two CTAs per SM (the block
+// rtw.  Hydro: one tile per CTA, 256 threads, two CTAs per SM (the block
 // scheduler keeps the SM's two tiles in different phases, so one's loads
-// overlap the other's solves); MHD, with room for one CTA per SM, 512.
+// overlap the other's solves).  MHD, with room for one CTA per SM: 512
+// threads, persistent; after the solves each thread holds its points' slab
+// values in registers and the next tile's slab arrives under the pointwise
+// phases and the stage combination (11.66 -> 10.65 ms a launch on
+// 256x512x1024, against one tile per CTA).
 constexpr int FB_FIELD = (FM + 8) * FM;
 constexpr int FB_OUT = FM * FM;
 template <int MAG>
@@ -772,6 +776,26 @@ __global__ void __launch_bounds__(CR_NT, 4) k_curl_rs(CssGeo g, double *__restri
   }
 }
 
+// the slab of tile T [and the wall rows of d(rho)/dtheta] by TMA boxes: per
+// field the 40 radial rows r0-4 .. r0+35 of the 32 theta values (zero
+// outside [0, nr)), on one mbarrier armed with the byte count
+template <int MAG>
+__device__ __forceinline__ void rstage_stage_tma(const CssGeo &g, const RstageTile &T, double *H, double *W,
+                                                 const SlabMaps &sc, const SlabMaps &sb, const SlabMaps &sw,
+                                                 uint64_t *bar) {
+  using C = RstageCfg<MAG>;
+  const bool lw = g.d[1].lphys[T.bt], hw = g.d[1].rphys[T.bt];
+  mbar_expect_tx(bar, 8u * (C::NH * FB_FIELD + ((lw || hw) ? FB_OUT : 0)));
+#pragma unroll
+  for (int f = 0; f < C::NH; f++) {
+    // H order w v u s rho [bt bp]: fields 1 2 3 4 0 of the state, 0 1 of B
+    const CUtensorMap *m = f < 5 ? &sc.slab : &sb.slab;
+    const int w = f < 4 ? f + 1 : (f == 4 ? 0 : f - 5);
+    tma_load_4d(H + (size_t)f * FB_FIELD, m, T.t0, T.ip, T.r0 - 4, w, bar);
+  }
+  if (lw || hw) tma_load_4d(W, &sw.slab, 0, lw ? 0 : 1, T.ip, T.r0, bar);
+}
+
 // STG: the RK4 stage (1..4), compiled in:
 //   1: vs = (sld ? vs + dv/6 : dv); nx = v0 + dtcur*dv
 //   2,3: vs = vs + dv/3;            nx = v0 + dtcur*dv
@@ -799,8 +823,18 @@ __global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssG
   const int nr = g.nr;
   const bool need_s = !(STG == 1 && !g.sldiffusion);
   int bad = 0;
-  {
-    const RstageTile T = rstage_tile(g, blockIdx.x);
+  // hydro: one tile per CTA (the grid covers the tiles); MHD: persistent,
+  // one CTA per SM, the next tile's slab arriving under this tile's
+  // pointwise phases
+  const int ntile = g.d[0].nb * g.d[1].nb * g.nphi;
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();  // the barrier is initialised before anyone waits on it
+  for (int q = blockIdx.x, i = 0; q < ntile; q += gridDim.x, i++) {
+    const RstageTile T = rstage_tile(g, q);
+    const bool more = q + (int)gridDim.x < ntile;
     const size_t base = (size_t)T.ip * g.nth + T.t0;  // (theta t0, phi ip) of plane 0
     // the per-point lines the later phases read, toward L2 now (two
     // 128-byte halves per row): the tendency, T [and B_r], vars0 [and the
@@ -820,32 +854,17 @@ __global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssG
         prefetch_l2(b + (size_t)(T.r0 + rr) * ps + base + (k & 1) * 16);
       }
     }
-    // ---- stage the slab [and the wall rows of d(rho)/dtheta] with TMA
-    // boxes: per field the 40 radial rows r0-4 .. r0+35 of the 32 theta
-    // values (zero outside [0, nr)) ----
+    // ---- the slab: the first tile's copies now, each later tile's issued
+    // under the previous tile's pointwise phases (MHD) ----
     const bool lw = DT.lphys[T.bt], hw = DT.rphys[T.bt];
-    if (tid == 0) {
-      mbar_init(bar, 1);
-      mbar_fence_init();
-    }
-    __syncthreads();  // the barrier is initialised before anyone waits on it
-    if (tid == 0) {
-      mbar_expect_tx(bar, 8u * (C::NH * FB_FIELD + ((lw || hw) ? FB_OUT : 0)));
-#pragma unroll
-      for (int f = 0; f < C::NH; f++) {
-        // H order w v u s rho [bt bp]: fields 1 2 3 4 0 of the state, 0 1 of B
-        const CUtensorMap *m = f < 5 ? &sc.slab : &sb.slab;
-        const int w = f < 4 ? f + 1 : (f == 4 ? 0 : f - 5);
-        tma_load_4d(H + (size_t)f * FB_FIELD, m, T.t0, T.ip, T.r0 - 4, w, bar);
-      }
-      if (lw || hw) tma_load_4d(W, &sw.slab, 0, lw ? 0 : 1, T.ip, T.r0, bar);
-    }
-    if (__syncthreads_or(!mbar_wait_bounded(bar, 0u, kWaitCycles))) {
+    if (i == 0 && tid == 0) rstage_stage_tma<MAG>(g, T, H, W, sc, sb, sw, bar);
+    const unsigned parity = (unsigned)i & 1u;
+    if (__syncthreads_or(!mbar_wait_bounded(bar, parity, kWaitCycles))) {
       // copies that never complete: report them and stop, after giving the
       // ones still in flight the same bound to land
       if (tid == 0) {
         atomicOr(flag, kFlagTimeout);
-        mbar_wait_bounded(bar, 0u, kWaitCycles);
+        mbar_wait_bounded(bar, parity, kWaitCycles);
       }
       return;
     }
@@ -915,6 +934,24 @@ __global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssG
       __syncthreads();
     }
 
+    // MHD: this thread's slab values of the later phases (u rho bt bp w and
+    // the wall row), then the slab buffer is free for the next tile's copies
+    double hv[C::PPT][6];
+    if (MAG) {
+#pragma unroll
+      for (int h = 0; h < C::PPT; h++) {
+        const double *hl = H + (size_t)(wrp + C::NW * h + 4) * FM + lane;
+        hv[h][0] = hl[2 * FB_FIELD]; hv[h][1] = hl[4 * FB_FIELD];
+        hv[h][2] = hl[5 * FB_FIELD]; hv[h][3] = hl[6 * FB_FIELD];
+        hv[h][4] = hl[0];
+        hv[h][5] = (lw || hw) ? W[(wrp + C::NW * h) * FM + lane] : 0.0;
+      }
+      __syncthreads();
+      if (more && tid == 0) {
+        fence_proxy_async();
+        rstage_stage_tma<MAG>(g, rstage_tile(g, q + gridDim.x), H, W, sc, sb, sw, bar);
+      }
+    }
     // ---- radial pointwise: PPT points per thread (row j = warp + NW h, t = lane) ----
     const double *resp = g.resp_r + (size_t)(2 * T.br + (phys == 2 ? 1 : 0)) * g.tstride;
     double d[C::PPT][5], tk[C::PPT];
@@ -931,7 +968,16 @@ __global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssG
       for (int h = 0; h < C::PPT; h++) {
         const int j = wrp + C::NW * h, ir = T.r0 + j;
         RadIn qq;
-        gather(j, lane, qq, in[h][5], in[h][6]);
+        if (MAG) {
+          const double *ol = O + (size_t)j * FM + lane;
+          qq.u = hv[h][0]; qq.rho = hv[h][1]; qq.t = in[h][5];
+          qq.dw_r = ol[0]; qq.dv_r = ol[FB_OUT]; qq.du_r = ol[2 * FB_OUT]; qq.ds_r = ol[3 * FB_OUT];
+          qq.d2s_r = ol[4 * FB_OUT];
+          qq.bt = hv[h][2]; qq.bp = hv[h][3]; qq.br = in[h][6];
+          qq.dbt_r = ol[6 * FB_OUT]; qq.dbp_r = ol[7 * FB_OUT];
+        } else {
+          gather(j, lane, qq, in[h][5], in[h][6]);
+        }
         double drho = in[h][0], dw = in[h][1], dvv = in[h][2], du = in[h][3], ds = in[h][4];
         radial_point<MAG>(g, ir, qq, drho, dw, dvv, du, ds);
         double w1 = O[5 * FB_OUT + j * FM + lane];  // Density_Terms_Radial
@@ -960,7 +1006,7 @@ __global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssG
 #pragma unroll
         for (int h = 0; h < C::PPT; h++) {
           const int j = wrp + C::NW * h;
-          const double rho = H[4 * FB_FIELD + (size_t)(j + 4) * FM + tw];
+          const double rho = MAG ? hv[h][1] : H[4 * FB_FIELD + (size_t)(j + 4) * FM + tw];
           datum[FM + j] = g.r_ind[T.r0 + j] * g.invpconst * d[h][1] * rho / tk[h];
         }
       }
@@ -970,8 +1016,9 @@ __global__ void __launch_bounds__(RstageCfg<MAG>::NT, MAG ? 1 : 2) k_rstage(CssG
 #pragma unroll
       for (int h = 0; h < C::PPT; h++) {
         const int j = wrp + C::NW * h;
-        const double w = H[(size_t)(j + 4) * FM + lane], rho = H[4 * FB_FIELD + (size_t)(j + 4) * FM + lane];
-        double w1 = g.r_inv[T.r0 + j] * (W[j * FM + lane] + datum[FM + j] * rl);
+        const double w = MAG ? hv[h][4] : H[(size_t)(j + 4) * FM + lane],
+                     rho = MAG ? hv[h][1] : H[4 * FB_FIELD + (size_t)(j + 4) * FM + lane];
+        double w1 = g.r_inv[T.r0 + j] * ((MAG ? hv[h][5] : W[j * FM + lane]) + datum[FM + j] * rl);
         d[h][0] = d[h][0] - w * w1;
         w1 = w1 * (1.0 / rho);
         d[h][1] = d[h][1] - g.pconst * w1 * tk[h];
