@@ -109,8 +109,8 @@ struct SwzCol {  // phi line t of a derivative tile: element (j, t)
 };
 __device__ __forceinline__ double swz(const double *O, int p, int t) { return O[p * FM + (t ^ (p & 15))]; }
 
-// ---- TMA tile copies completing on an mbarrier (this CTA's own shared
-// memory; no cluster multicast) ----------------------------------------------
+// ---- TMA tile copies completing on an mbarrier (each into this CTA's own
+// shared memory only) -------------------------------------------------------
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count) : "memory");
