@@ -389,6 +389,7 @@ def run_ours(args):
         achieved = alg * per_launch_cells / (kms / cnt / 1e3) / 1e9 if alg else None
         traffic = None
         fp64 = None
+        traffic_src = None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
         if os.path.exists(tpath):
             try:
@@ -397,10 +398,14 @@ def run_ours(args):
                 if key in tj:
                     traffic = tj[key]["dram_bytes_per_cell"] * per_launch_cells
                     fp64 = tj[key].get("fp64_pipe_pct_of_peak")
+                    note = tj[key].get("note") or ""
+                    traffic_src = "ncu capture on %s%s" % (tj[key].get("captured_on", "?"),
+                                                           "; " + note if note else "")
             except Exception:
                 traffic = None
         roof = {"bound": "hbm", "kernel": name, "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "traffic_source": traffic_src,
                 "algorithmic_bytes_per_launch": alg * per_launch_cells if alg else None,
                 "avg_launch_ms": kms / cnt, "peak_source": peak_src,
                 "time_share": kms / sum(v[0] for v in stats.values()),
